@@ -1,0 +1,241 @@
+"""Python mirror of the reference's solver surface over the C ABI.
+
+``precond_CG`` and ``switching_chol`` keep the reference's argument order and
+meaning (src/mixed_cholesky.cu:76-78, src/switching_chol.cuh:19-22) with torch
+CUDA tensors in place of raw device pointers; ``Factor`` exposes the
+factor-object API of include/mpchol.h.  Every call runs the sm_100a library;
+there is no CPU path here.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import torch
+
+from . import _lib
+from ._lib import check, load
+
+
+def _stream_handle(device: torch.device | None = None) -> int:
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def _ptr(t: torch.Tensor | None) -> int | None:
+    return None if t is None else t.data_ptr()
+
+
+def _require_cuda(t: torch.Tensor, dtype: torch.dtype, name: str) -> None:
+    if not t.is_cuda:
+        raise ValueError(f"{name} must be a CUDA tensor")
+    if t.dtype != dtype:
+        raise ValueError(f"{name} must be {dtype}, got {t.dtype}")
+
+
+def _col_major(A: torch.Tensor) -> tuple[torch.Tensor, int]:
+    """Return a tensor whose storage is column-major n x n and its ld.
+
+    A symmetric matrix given in row-major torch layout has the same lower
+    triangle as its column-major transpose, so A.t() is used without a copy
+    when A is contiguous."""
+    if A.dim() != 2 or A.shape[0] != A.shape[1]:
+        raise ValueError("A must be square")
+    if A.stride(0) == 1 and A.stride(1) >= A.shape[0]:
+        return A, A.stride(1)
+    At = A.t()
+    if At.stride(0) == 1:
+        return At, At.stride(1)
+    At = A.t().contiguous().t()
+    return At, At.stride(1)
+
+
+@dataclass
+class FactorInfo:
+    status: int
+    fail_row: int
+    n_perturbed: int
+    nsteps: int
+    n_fp64_blocks: int
+    steps_by_prec: list
+    step_prec: list
+    step_fp64: list
+
+
+@dataclass
+class Report:
+    iterations: int
+    converged: bool
+    rel_residual: float
+    backward_error: float
+    precond_residual: float
+    status: int
+
+
+class Factor:
+    """A factor object: blocked mixed-precision Cholesky of an SPD matrix."""
+
+    def __init__(self, n: int, **opts):
+        self.lib = load()
+        self.n = n
+        self.opts = _lib.default_opts(**opts)
+        h = ctypes.c_void_p()
+        check(self.lib.mpchol_factor_create(ctypes.byref(self.opts), n, ctypes.byref(h)),
+              "mpchol_factor_create")
+        self.handle = h
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            self.lib.mpchol_factor_destroy(h)
+            self.handle = None
+
+    def compute(self, A: torch.Tensor) -> "Factor":
+        _require_cuda(A, torch.float32, "A")
+        Ac, lda = _col_major(A)
+        check(self.lib.mpchol_factor_compute(self.handle, Ac.data_ptr(), lda, _stream_handle()),
+              "mpchol_factor_compute")
+        self._A_keepalive = Ac
+        return self
+
+    def info(self) -> FactorInfo:
+        fi = _lib.FactorInfo()
+        ns = (self.n + self.opts.block_size - 1) // self.opts.block_size
+        prec = (ctypes.c_int * ns)()
+        f64 = (ctypes.c_int * ns)()
+        check(self.lib.mpchol_factor_info_get(self.handle, ctypes.byref(fi), prec, f64,
+                                              _stream_handle()), "mpchol_factor_info_get")
+        return FactorInfo(fi.status, fi.fail_row, fi.n_perturbed, fi.nsteps, fi.n_fp64_blocks,
+                          list(fi.steps_by_prec), list(prec), list(f64))
+
+    def lower(self) -> torch.Tensor:
+        """The factor L as an n x n torch tensor (lower triangle; a copy)."""
+        p = ctypes.c_void_p()
+        ld = ctypes.c_int()
+        n = ctypes.c_int()
+        check(self.lib.mpchol_factor_lower(self.handle, ctypes.byref(p), ctypes.byref(ld),
+                                           ctypes.byref(n)), "mpchol_factor_lower")
+        buf = torch.empty((self.n, ld.value), dtype=torch.float32, device="cuda")
+        nbytes = self.n * ld.value * 4
+        torch.cuda.current_stream().synchronize()
+        # device-to-device copy via cudaMemcpy through torch: wrap the raw pointer
+        src = _wrap_device(p.value, (self.n, ld.value), torch.float32)
+        buf.copy_(src)
+        del nbytes
+        return buf[:, : self.n].t().tril()
+
+    def diags(self) -> tuple[torch.Tensor, torch.Tensor]:
+        pd = ctypes.c_void_p()
+        pt = ctypes.c_void_p()
+        check(self.lib.mpchol_factor_diags(self.handle, ctypes.byref(pd), ctypes.byref(pt)),
+              "mpchol_factor_diags")
+        torch.cuda.current_stream().synchronize()
+        return (_wrap_device(pd.value, (self.n,), torch.float32).clone(),
+                _wrap_device(pt.value, (self.n,), torch.float32).clone())
+
+    def apply_precond(self, R: torch.Tensor) -> torch.Tensor:
+        _require_cuda(R, torch.float64, "R")
+        R2 = R.reshape(self.n, -1) if R.dim() == 1 else R
+        nrhs = R2.shape[1]
+        Rc = R2.t().contiguous()          # column-major n x nrhs
+        Z = torch.empty_like(Rc)
+        check(self.lib.mpchol_apply_precond(self.handle, Rc.data_ptr(), Z.data_ptr(), nrhs,
+                                            _stream_handle()), "mpchol_apply_precond")
+        Z = Z.t()
+        return Z.reshape(R.shape) if R.dim() == 1 else Z
+
+    def pcg(self, A: torch.Tensor, B: torch.Tensor, rel_tol: float = 1e-10, max_it: int = 200,
+            x0_precond: bool = True, check_every: int = 4) -> tuple[torch.Tensor, Report]:
+        """Solve A X = B (B: n or n x nrhs FP64 CUDA tensor) with PCG on this factor."""
+        if A.dtype not in (torch.float32, torch.float64):
+            raise ValueError("A must be float32 or float64")
+        _require_cuda(B, torch.float64, "B")
+        Ac, lda = _col_major(A)
+        B2 = B.reshape(self.n, 1) if B.dim() == 1 else B
+        nrhs = B2.shape[1]
+        Bc = B2.t().contiguous()
+        X = torch.empty_like(Bc)
+        po = _lib.default_pcg_opts(rel_tol=rel_tol, max_it=max_it, x0_precond=int(x0_precond),
+                                   check_every=check_every)
+        rep = _lib.Report()
+        fn = self.lib.mpchol_pcg if A.dtype == torch.float32 else self.lib.mpchol_pcg_f64
+        st = fn(self.handle, Ac.data_ptr(), lda, Bc.data_ptr(), X.data_ptr(), nrhs,
+                ctypes.byref(po), ctypes.byref(rep), _stream_handle())
+        if st not in (_lib.OK, _lib.PCG_MAXIT):
+            check(st, "mpchol_pcg")
+        Xo = X.t()
+        Xo = Xo.reshape(B.shape) if B.dim() == 1 else Xo
+        return Xo, Report(rep.iterations, bool(rep.converged), rep.rel_residual,
+                          rep.backward_error, rep.precond_residual, st)
+
+
+def _wrap_device(ptr: int, shape: tuple, dtype: torch.dtype) -> torch.Tensor:
+    """View of library-owned device memory as a torch tensor (no copy)."""
+    numel = 1
+    for s in shape:
+        numel *= s
+    itemsize = torch.tensor([], dtype=dtype).element_size()
+
+    class _Holder:
+        __cuda_array_interface__ = {
+            "shape": tuple(shape),
+            "typestr": {torch.float32: "<f4", torch.float64: "<f8"}[dtype],
+            "data": (ptr, False),
+            "version": 3,
+            "strides": None,
+        }
+
+    del numel, itemsize
+    return torch.as_tensor(_Holder(), device="cuda")
+
+
+def factor(A: torch.Tensor, **opts) -> Factor:
+    """Factor the FP32 SPD matrix A (CUDA tensor) with the given options."""
+    f = Factor(A.shape[0], **opts)
+    return f.compute(A)
+
+
+def solve(A: torch.Tensor, B: torch.Tensor, rel_tol: float = 1e-10, max_it: int = 200,
+          **opts) -> tuple[torch.Tensor, Report, Factor]:
+    """Factor A and run PCG on A X = B; returns (X, report, factor)."""
+    f = factor(A if A.dtype == torch.float32 else A.float(), **opts)
+    X, rep = f.pcg(A, B, rel_tol=rel_tol, max_it=max_it)
+    return X, rep, f
+
+
+# ---- reference-shaped entry points ------------------------------------------
+
+def precond_CG(A: torch.Tensor, x: torch.Tensor, b: torch.Tensor, n: int, r: int,
+               normA: float = 0.0, eps_prime: float = 0.0, flr: float = 0.0,
+               perturb_diag: bool = False, microscal_size: int = 32,
+               rel_tol: float = 0.0, max_it: int = 200) -> int:
+    """The reference's precond_CG (src/mixed_cholesky.cu:76-78).
+
+    A: n x n FP64 (column-major device storage; a symmetric row-major tensor is
+    the same matrix), x written, b read, r the block size.  Returns 0 when
+    converged, -1 when not, > 0 when the preconditioner failed (the failing
+    row + 1, the reference's cuSOLVER info convention).  With the reference's
+    rel_tol = 0 the loop runs max_it iterations.
+    """
+    _require_cuda(A, torch.float64, "A")
+    _require_cuda(x, torch.float64, "x")
+    _require_cuda(b, torch.float64, "b")
+    Ac, lda = _col_major(A)
+    if lda != n:
+        Ac = Ac.t().contiguous().t()
+    return load().mpchol_precond_cg(Ac.data_ptr(), x.data_ptr(), b.data_ptr(), n, r, normA,
+                                    eps_prime, flr, int(perturb_diag), microscal_size, rel_tol,
+                                    max_it, _stream_handle())
+
+
+def switching_chol(d_A: torch.Tensor, n: int, b: int, d_diagVals: torch.Tensor,
+                   updated_diag: torch.Tensor, eps_prime: float, perturb_diag: bool = False,
+                   microscal_size: int = 32, scales: torch.Tensor | None = None) -> int:
+    """The reference's switching_chol (src/switching_chol.cuh:19-22): in-place
+    FP32 factor of the n x n column-major matrix d_A with block b.  Returns a
+    status code (0 = ok) where the reference returns nothing."""
+    _require_cuda(d_A, torch.float32, "d_A")
+    if d_A.stride(0) != 1 and not d_A.is_contiguous():
+        raise ValueError("d_A must be column-major or contiguous symmetric")
+    return load().mpchol_switching_chol(d_A.data_ptr(), n, b, _ptr(d_diagVals),
+                                        _ptr(updated_diag), eps_prime, int(perturb_diag),
+                                        microscal_size, _stream_handle(), _ptr(scales))

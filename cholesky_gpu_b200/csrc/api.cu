@@ -1,0 +1,665 @@
+// C-ABI implementation: factor objects, the blocked factorization driver, the
+// PCG driver and the reference-shaped entry points.
+//
+// The driver replaces switching_chol's host loop (src/switching_chol.cuh:76-224)
+// and precond_CG (src/mixed_cholesky.cu:76-229).  Differences that matter to a
+// caller are deliberate: nothing is allocated per step, the precision decision
+// never leaves the device, the caller's stream is the only stream used, and no
+// caller-owned handle or stream is ever destroyed.
+#include <cstdio>
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.cuh"
+#include "pcg.cuh"
+
+using namespace mpchol;
+
+namespace mpchol {
+static std::mutex g_err_mu;
+static std::string g_last_err;
+void record_cuda_error(cudaError_t e, const char* what, const char* file, int line) {
+  std::lock_guard<std::mutex> lk(g_err_mu);
+  char buf[512];
+  snprintf(buf, sizeof(buf), "%s (%d) at %s:%d in %s", cudaGetErrorString(e), (int)e, file, line,
+           what);
+  g_last_err = buf;
+}
+}  // namespace mpchol
+
+struct mpchol_factor {
+  mpchol_opts opts;
+  int n = 0, ld = 0, b = 0, nsteps = 0;
+  int device = 0;
+  float* A = nullptr;         // n columns x ld rows, factor in the lower triangle
+  float* d = nullptr;         // original diagonal
+  float* dtilde = nullptr;    // Schur-complement diagonal tracker
+  float* rowsq = nullptr;     // per-row sum of squares of the latest panel
+  float* sh = nullptr;        // accumulated rounding-shift estimate
+  float* winv = nullptr;      // inverses of the 32x32 diagonal tiles of one block
+  double* scratch64 = nullptr;
+  void* q = nullptr;          // quantized panel (K-major), n x b x 2 bytes
+  int8_t* rowexp = nullptr;
+  uint8_t* mxexp = nullptr;
+  StepState* steps = nullptr;
+  DevStatus* status = nullptr;
+  // solve side
+  float* linv = nullptr;      // 128x128 diagonal-block inverses
+  int* flags = nullptr;
+  int* ticket = nullptr;
+  int epoch = 0;
+  bool solve_ready = false;
+  // PCG workspace (sized for 8 rhs)
+  double* vec = nullptr;      // x, r, z, p, Ap, b, tmp : 7 * n * 8
+  double* partials = nullptr; // 4 * VG * 8
+  double* scal = nullptr;     // rho[2][8], alpha[8], bnorm2[8], misc
+  int* done = nullptr;        // [0] converged flag, [1] iteration counter
+  int* h_done = nullptr;      // pinned
+  double* h_scal = nullptr;   // pinned
+};
+
+namespace {
+
+mpchol_status validate_opts(const mpchol_opts* o, int n) {
+  if (o == nullptr || n <= 0) return MPCHOL_ERR_BAD_ARG;
+  if (o->block_size < 32 || o->block_size > 256 || o->block_size % 32 != 0) return MPCHOL_ERR_BAD_ARG;
+  if (o->precision < 0 || o->precision > MPCHOL_PREC_SWITCHING) return MPCHOL_ERR_BAD_ARG;
+  if (o->left != 0) return MPCHOL_ERR_NOT_SUPPORTED;
+  if (o->diag_pert && !(o->pivot_floor > 0.0f)) return MPCHOL_ERR_BAD_ARG;
+  if (o->switch_mode != 0 && o->switch_mode != 1) return MPCHOL_ERR_BAD_ARG;
+  if (o->ladder_len < 0 || o->ladder_len > 4) return MPCHOL_ERR_BAD_ARG;
+  auto tc_ok = [&](int fmt) { return fmt == MPCHOL_PREC_FP32 || syrk_tc_supported(fmt, o->block_size); };
+  if (o->precision == MPCHOL_PREC_MXFP8) return MPCHOL_ERR_NOT_SUPPORTED;
+  if (o->precision != MPCHOL_PREC_SWITCHING && !tc_ok(o->precision)) return MPCHOL_ERR_NOT_SUPPORTED;
+  if (o->precision == MPCHOL_PREC_SWITCHING) {
+    if (o->switch_mode == 1) {
+      if (!tc_ok(MPCHOL_PREC_FP16) || !tc_ok(MPCHOL_PREC_E4M3)) return MPCHOL_ERR_NOT_SUPPORTED;
+    } else {
+      for (int i = 0; i < o->ladder_len; ++i) {
+        const int p = o->ladder[i];
+        if (p < 0 || p > MPCHOL_PREC_MXFP8) return MPCHOL_ERR_BAD_ARG;
+        if (p == MPCHOL_PREC_MXFP8 || !tc_ok(p)) return MPCHOL_ERR_NOT_SUPPORTED;
+      }
+    }
+  }
+  return MPCHOL_OK;
+}
+
+template <typename T>
+cudaError_t dmalloc(T** p, size_t count) {
+  return cudaMalloc(reinterpret_cast<void**>(p), count * sizeof(T) + 256);
+}
+
+void free_factor(mpchol_factor_t* f) {
+  if (f == nullptr) return;
+  void* ptrs[] = {f->A, f->d, f->dtilde, f->rowsq, f->sh, f->winv, f->scratch64, f->q,
+                  f->rowexp, f->mxexp, f->steps, f->status, f->linv, f->flags, f->ticket,
+                  f->vec, f->partials, f->scal, f->done};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (f->h_done) cudaFreeHost(f->h_done);
+  if (f->h_scal) cudaFreeHost(f->h_scal);
+  delete f;
+}
+
+DecisionParams make_dp(const mpchol_opts& o) {
+  DecisionParams dp;
+  dp.policy = o.precision;
+  dp.switch_mode = o.switch_mode;
+  dp.eps_prime = o.eps_prime;
+  dp.floor_ratio = o.floor;
+  dp.ladder_len = o.ladder_len;
+  for (int i = 0; i < 4; ++i) dp.ladder[i] = o.ladder[i];
+  return dp;
+}
+
+// One factorization of f->A in place, on `stream`.
+mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream) {
+  const mpchol_opts& o = f->opts;
+  const int n = f->n, ld = f->ld, b = f->b;
+  PotrfParams pp{o.diag_pert, o.pert, o.pivot_floor};
+  const DecisionParams dp = make_dp(o);
+  MPCHOL_CUDA_TRY(cudaMemsetAsync(f->status, 0, sizeof(DevStatus), stream));
+  MPCHOL_CUDA_TRY(cudaMemsetAsync(f->steps, 0, sizeof(StepState) * (f->nsteps + 1), stream));
+  MPCHOL_CUDA_TRY(cudaMemsetAsync(f->sh, 0, sizeof(float) * n, stream));
+  MPCHOL_CUDA_TRY(launch_extract_diag(f->A, ld, n, f->d, f->dtilde, stream));
+  const bool fixed = o.precision != MPCHOL_PREC_SWITCHING;
+  std::vector<int> tc_fmts;
+  if (!fixed) {
+    if (o.switch_mode == 1) tc_fmts = {FP16, E4M3};
+    else
+      for (int i = 0; i < o.ladder_len; ++i)
+        if (o.ladder[i] != FP32) tc_fmts.push_back(o.ladder[i]);
+  }
+  for (int k = 0; k < f->nsteps; ++k) {
+    const int s = k * b;
+    const int bs = std::min(b, n - s);
+    const int m = n - s - bs;
+    MPCHOL_CUDA_TRY(launch_potrf(f->A, ld, s, bs, f->d, f->sh, pp, &f->steps[k].fp64_diag,
+                                 f->scratch64, f->winv, f->status, stream));
+    if (m <= 0) break;
+    const int next_bs = std::min(b, m);
+    MPCHOL_CUDA_TRY(launch_trsm_panel(f->A, ld, n, s, bs, f->winv, f->d, f->dtilde, f->rowsq,
+                                      &f->steps[k], &f->steps[k + 1], next_bs, dp, f->status,
+                                      stream));
+    float* P = f->A + (size_t)s * ld + s + bs;
+    float* C = f->A + (size_t)(s + bs) * ld + s + bs;
+    MPCHOL_CUDA_TRY(launch_quantize_panel(P, ld, m, bs, &f->steps[k], dp, f->q, bs, f->rowexp,
+                                          f->mxexp, bs / 32, f->rowsq + s + bs,
+                                          o.diag_pert ? f->sh + s + bs : nullptr, f->status,
+                                          stream));
+    if (fixed) {
+      if (o.precision == FP32)
+        MPCHOL_CUDA_TRY(launch_syrk_f32(C, ld, m, bs, P, ld, nullptr, f->status, stream));
+      else
+        MPCHOL_CUDA_TRY(launch_syrk_tc(C, ld, m, bs, o.precision, f->q, bs, f->rowexp, f->mxexp,
+                                       bs / 32, nullptr, f->status, stream));
+    } else {
+      const int* sel = &f->steps[k].prec;
+      MPCHOL_CUDA_TRY(launch_syrk_f32(C, ld, m, bs, P, ld, sel, f->status, stream));
+      for (int fmt : tc_fmts)
+        MPCHOL_CUDA_TRY(launch_syrk_tc(C, ld, m, bs, fmt, f->q, bs, f->rowexp, f->mxexp, bs / 32,
+                                       sel, f->status, stream));
+    }
+  }
+  f->solve_ready = false;
+  return MPCHOL_OK;
+}
+
+mpchol_status ensure_solve(mpchol_factor_t* f, cudaStream_t stream) {
+  if (f->solve_ready) return MPCHOL_OK;
+  MPCHOL_CUDA_TRY(launch_diag_inverse(f->A, f->ld, f->n, f->linv, stream));
+  f->solve_ready = true;
+  return MPCHOL_OK;
+}
+
+// z = M^-1 r for NR-padded vectors
+mpchol_status apply_precond(mpchol_factor_t* f, const double* r, double* tmp, double* z, int nr,
+                            const int* skip, cudaStream_t stream) {
+  MPCHOL_CUDA_TRY(launch_trsv(false, f->A, f->ld, f->n, f->linv, r, tmp, nr, f->flags, ++f->epoch,
+                              f->ticket, skip, f->status, stream));
+  MPCHOL_CUDA_TRY(launch_trsv(true, f->A, f->ld, f->n, f->linv, tmp, z, nr, f->flags, ++f->epoch,
+                              f->ticket, skip, f->status, stream));
+  return MPCHOL_OK;
+}
+
+int read_status(mpchol_factor_t* f, cudaStream_t stream, DevStatus* out) {
+  if (cudaMemcpyAsync(out, f->status, sizeof(DevStatus), cudaMemcpyDeviceToHost, stream) != cudaSuccess)
+    return -1;
+  if (cudaStreamSynchronize(stream) != cudaSuccess) return -1;
+  return 0;
+}
+
+template <typename TA>
+mpchol_status run_pcg(mpchol_factor_t* f, const TA* dA, int lda, const double* dB, double* dX,
+                      int nrhs, const mpchol_pcg_opts* popts, mpchol_report* rep,
+                      cudaStream_t stream) {
+  if (f == nullptr || dA == nullptr || dB == nullptr || dX == nullptr) return MPCHOL_ERR_BAD_ARG;
+  if (nrhs < 1 || nrhs > 8 || lda < f->n) return MPCHOL_ERR_BAD_ARG;
+  mpchol_pcg_opts po;
+  mpchol_pcg_opts_default(&po);
+  if (popts) po = *popts;
+  if (po.check_every < 1) po.check_every = 1;
+  if (po.max_it < 0) return MPCHOL_ERR_BAD_ARG;
+  const int n = f->n;
+  const int nr = pcg_padded_nrhs(nrhs);
+  const size_t nv = (size_t)n * 8;
+  double* x = f->vec;
+  double* r = x + nv;
+  double* z = r + nv;
+  double* p = z + nv;
+  double* Ap = p + nv;
+  double* bb = Ap + nv;
+  double* tmp = bb + nv;
+  const int VG = pcg_vgrid();
+  double* part_pAp = f->partials;
+  double* part_rr = part_pAp + (size_t)VG * 8;
+  double* part_rz = part_rr + (size_t)VG * 8;
+  double* part_misc = part_rz + (size_t)VG * 8;
+  double* rho[2] = {f->scal, f->scal + 8};
+  double* alpha = f->scal + 16;
+  double* bnorm2 = f->scal + 24;
+  double* misc = f->scal + 32;   // [0..7] rr true, [8..15] xnorm2, [16] frob2
+  mpchol_status ss = ensure_solve(f, stream);
+  if (ss != MPCHOL_OK) return ss;
+  MPCHOL_CUDA_TRY(cudaMemsetAsync(f->status, 0, sizeof(DevStatus), stream));
+  MPCHOL_CUDA_TRY(cudaMemsetAsync(f->done, 0, 2 * sizeof(int), stream));
+  MPCHOL_CUDA_TRY(launch_pad_columns(dB, n, nrhs, bb, nr, stream));
+  MPCHOL_CUDA_TRY(launch_dot(bb, bb, n, nr, part_misc, nullptr, stream));
+  MPCHOL_CUDA_TRY(launch_reduce_partials(part_misc, bnorm2, nr, stream));
+  // x0
+  if (po.x0_precond) {
+    mpchol_status s0 = apply_precond(f, bb, tmp, x, nr, nullptr, stream);
+    if (s0 != MPCHOL_OK) return s0;
+  } else {
+    MPCHOL_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(double) * (size_t)n * nr, stream));
+  }
+  const double tol2 = po.rel_tol * po.rel_tol;
+  int it = 0;
+  bool converged = false;
+  const int max_restarts = 3;
+  for (int restart = 0; restart <= max_restarts; ++restart) {
+    // r = b - A x ; z = M^-1 r ; p = z ; rho = r^T z
+    MPCHOL_CUDA_TRY(launch_symv_skip<TA>(dA, lda, n, x, Ap, nr, nullptr, stream));
+    MPCHOL_CUDA_TRY(launch_residual(bb, Ap, r, n, nr, part_rr, stream));
+    MPCHOL_CUDA_TRY(launch_reduce_partials(part_rr, misc, nr, stream));
+    // convergence of the true residual
+    MPCHOL_CUDA_TRY(cudaMemcpyAsync(f->h_scal, misc, sizeof(double) * 8, cudaMemcpyDeviceToHost, stream));
+    MPCHOL_CUDA_TRY(cudaMemcpyAsync(f->h_scal + 8, bnorm2, sizeof(double) * 8, cudaMemcpyDeviceToHost, stream));
+    MPCHOL_CUDA_TRY(cudaStreamSynchronize(stream));
+    converged = true;
+    for (int k = 0; k < nrhs; ++k)
+      if (!(f->h_scal[k] <= tol2 * f->h_scal[8 + k])) converged = false;
+    if (converged || it >= po.max_it) break;
+    mpchol_status s1 = apply_precond(f, r, tmp, z, nr, nullptr, stream);
+    if (s1 != MPCHOL_OK) return s1;
+    MPCHOL_CUDA_TRY(launch_copy(z, p, n, nr, stream));
+    MPCHOL_CUDA_TRY(launch_dot(r, z, n, nr, part_rz, nullptr, stream));
+    MPCHOL_CUDA_TRY(launch_reduce_partials(part_rz, rho[0], nr, stream));
+    MPCHOL_CUDA_TRY(cudaMemsetAsync(f->done, 0, sizeof(int), stream));
+    int cur = 0;
+    bool stop = false;
+    while (it < po.max_it && !stop) {
+      const int chunk = std::min(po.check_every, po.max_it - it);
+      for (int c = 0; c < chunk; ++c) {
+        MPCHOL_CUDA_TRY(launch_symv_skip<TA>(dA, lda, n, p, Ap, nr, f->done, stream));
+        MPCHOL_CUDA_TRY(launch_dot(p, Ap, n, nr, part_pAp, f->done, stream));
+        MPCHOL_CUDA_TRY(launch_update_xr(x, r, p, Ap, n, nr, part_pAp, rho[cur], alpha, part_rr,
+                                         f->done, f->status, stream));
+        mpchol_status s2 = apply_precond(f, r, tmp, z, nr, f->done, stream);
+        if (s2 != MPCHOL_OK) return s2;
+        MPCHOL_CUDA_TRY(launch_dot(r, z, n, nr, part_rz, f->done, stream));
+        MPCHOL_CUDA_TRY(launch_update_p(p, z, n, nr, part_rz, rho[cur], rho[cur ^ 1], part_rr,
+                                        bnorm2, tol2, f->done, f->done, f->done + 1, stream));
+        cur ^= 1;
+      }
+      MPCHOL_CUDA_TRY(cudaMemcpyAsync(f->h_done, f->done, 2 * sizeof(int), cudaMemcpyDeviceToHost, stream));
+      DevStatus st;
+      MPCHOL_CUDA_TRY(cudaMemcpyAsync(&st, f->status, sizeof(DevStatus), cudaMemcpyDeviceToHost, stream));
+      MPCHOL_CUDA_TRY(cudaStreamSynchronize(stream));
+      if (st.code == MPCHOL_ERR_TIMEOUT) return MPCHOL_ERR_TIMEOUT;
+      it = f->h_done[1];                // iterations actually executed on the device
+      if (f->h_done[0]) stop = true;    // recursive residual met the tolerance
+      if (st.code == MPCHOL_PCG_BREAKDOWN) stop = true;
+    }
+    // the loop exits on max_it or when the recursive residual says done; the
+    // next pass re-checks the true residual (residual replacement restart)
+  }
+  // report
+  DevStatus st;
+  if (read_status(f, stream, &st) != 0) return MPCHOL_ERR_CUDA;
+  MPCHOL_CUDA_TRY(cudaMemcpy2DAsync(dX, sizeof(double) * n, x, sizeof(double) * n,
+                                    sizeof(double) * n, nrhs, cudaMemcpyDeviceToDevice, stream));
+  if (rep != nullptr) {
+    MPCHOL_CUDA_TRY(launch_dot(x, x, n, nr, part_misc, nullptr, stream));
+    MPCHOL_CUDA_TRY(launch_reduce_partials(part_misc, misc + 8, nr, stream));
+    MPCHOL_CUDA_TRY(launch_frob_lower<TA>(dA, lda, n, part_misc, stream));
+    MPCHOL_CUDA_TRY(launch_reduce_partials(part_misc, misc + 16, 1, stream));
+    MPCHOL_CUDA_TRY(launch_dot(r, z, n, nr, part_rz, nullptr, stream));
+    MPCHOL_CUDA_TRY(launch_reduce_partials(part_rz, misc + 24, nr, stream));
+    MPCHOL_CUDA_TRY(cudaMemcpyAsync(f->h_scal, misc, sizeof(double) * 32, cudaMemcpyDeviceToHost, stream));
+    MPCHOL_CUDA_TRY(cudaMemcpyAsync(f->h_scal + 32, bnorm2, sizeof(double) * 8, cudaMemcpyDeviceToHost, stream));
+    MPCHOL_CUDA_TRY(cudaStreamSynchronize(stream));
+    double relmax = 0.0, bemax = 0.0, prmax = 0.0;
+    const double frob = sqrt(f->h_scal[16]);
+    for (int k = 0; k < nrhs; ++k) {
+      const double rr = f->h_scal[k], xx = f->h_scal[8 + k], bb2 = f->h_scal[32 + k];
+      const double rel = bb2 > 0 ? sqrt(rr / bb2) : sqrt(rr);
+      const double be = sqrt(rr) / (frob * sqrt(xx) + sqrt(bb2));
+      const double pr = bb2 > 0 ? sqrt(fabs(f->h_scal[24 + k]) / bb2) : 0.0;
+      relmax = std::max(relmax, rel);
+      bemax = std::max(bemax, be);
+      prmax = std::max(prmax, pr);
+    }
+    rep->iterations = it;
+    rep->converged = converged ? 1 : 0;
+    rep->rel_residual = relmax;
+    rep->backward_error = bemax;
+    rep->precond_residual = prmax;
+  }
+  if (st.code == MPCHOL_PCG_BREAKDOWN) return MPCHOL_PCG_BREAKDOWN;
+  if (st.code != 0) return (mpchol_status)st.code;
+  return converged ? MPCHOL_OK : MPCHOL_PCG_MAXIT;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* mpchol_status_str(int s) {
+  switch (s) {
+    case MPCHOL_OK: return "ok";
+    case MPCHOL_ERR_BAD_ARG: return "bad argument";
+    case MPCHOL_ERR_NOT_SPD: return "matrix not positive definite (non-positive pivot)";
+    case MPCHOL_ERR_CUDA: return "CUDA runtime error";
+    case MPCHOL_ERR_ALLOC: return "device allocation failed";
+    case MPCHOL_PCG_MAXIT: return "PCG reached max_it without converging";
+    case MPCHOL_PCG_BREAKDOWN: return "PCG breakdown (p^T A p <= 0 or not finite)";
+    case MPCHOL_ERR_TIMEOUT: return "bounded device wait timed out";
+    case MPCHOL_ERR_NOT_SUPPORTED: return "option combination not supported";
+    default: return "unknown status";
+  }
+}
+
+const char* mpchol_last_error(void) {
+  std::lock_guard<std::mutex> lk(g_err_mu);
+  static thread_local std::string copy;
+  copy = g_last_err;
+  return copy.c_str();
+}
+
+void mpchol_opts_default(mpchol_opts* o) {
+  if (!o) return;
+  memset(o, 0, sizeof(*o));
+  o->block_size = 256;
+  o->precision = MPCHOL_PREC_SWITCHING;
+  o->eps_prime = 0.5f;
+  o->floor = 0.0f;
+  o->diag_pert = 0;
+  o->pert = 1.0f;
+  o->pivot_floor = 1e-7f;
+  o->switch_mode = 0;
+  o->ladder_len = 3;
+  o->ladder[0] = MPCHOL_PREC_E4M3;
+  o->ladder[1] = MPCHOL_PREC_FP16;
+  o->ladder[2] = MPCHOL_PREC_FP32;
+  o->ladder[3] = MPCHOL_PREC_FP32;
+  o->left = 0;
+}
+
+void mpchol_pcg_opts_default(mpchol_pcg_opts* o) {
+  if (!o) return;
+  o->rel_tol = 1e-10;
+  o->max_it = 200;
+  o->x0_precond = 1;
+  o->check_every = 4;
+}
+
+mpchol_status mpchol_factor_create(const mpchol_opts* opts, int n, mpchol_factor_t** out) {
+  if (out == nullptr) return MPCHOL_ERR_BAD_ARG;
+  *out = nullptr;
+  mpchol_status v = validate_opts(opts, n);
+  if (v != MPCHOL_OK) return v;
+  mpchol_factor_t* f = new mpchol_factor_t();
+  f->opts = *opts;
+  f->n = n;
+  f->ld = (n + 31) / 32 * 32;
+  f->b = opts->block_size;
+  f->nsteps = (n + f->b - 1) / f->b;
+  cudaGetDevice(&f->device);
+  const size_t nv = (size_t)n * 8;
+  const int NB128 = (n + 127) / 128;
+  bool ok = dmalloc(&f->A, (size_t)f->ld * n) == cudaSuccess &&
+            dmalloc(&f->d, n) == cudaSuccess && dmalloc(&f->dtilde, n) == cudaSuccess &&
+            dmalloc(&f->rowsq, n) == cudaSuccess && dmalloc(&f->sh, n) == cudaSuccess &&
+            dmalloc(&f->winv, (size_t)8 * 32 * 32) == cudaSuccess &&
+            dmalloc(&f->scratch64, potrf_scratch64_elems(256)) == cudaSuccess &&
+            dmalloc(reinterpret_cast<uint8_t**>(&f->q), (size_t)n * f->b * 2) == cudaSuccess &&
+            dmalloc(&f->rowexp, n) == cudaSuccess &&
+            dmalloc(&f->mxexp, (size_t)n * (f->b / 32)) == cudaSuccess &&
+            dmalloc(&f->steps, f->nsteps + 1) == cudaSuccess &&
+            dmalloc(&f->status, 1) == cudaSuccess &&
+            dmalloc(&f->linv, (size_t)NB128 * 128 * 128) == cudaSuccess &&
+            dmalloc(&f->flags, NB128) == cudaSuccess && dmalloc(&f->ticket, 1) == cudaSuccess &&
+            dmalloc(&f->vec, 7 * nv) == cudaSuccess &&
+            dmalloc(&f->partials, (size_t)4 * pcg_vgrid() * 8) == cudaSuccess &&
+            dmalloc(&f->scal, 64) == cudaSuccess && dmalloc(&f->done, 2) == cudaSuccess &&
+            cudaMallocHost(reinterpret_cast<void**>(&f->h_done), 2 * sizeof(int)) == cudaSuccess &&
+            cudaMallocHost(reinterpret_cast<void**>(&f->h_scal), sizeof(double) * 64) == cudaSuccess;
+  if (!ok) {
+    cudaGetLastError();
+    free_factor(f);
+    return MPCHOL_ERR_ALLOC;
+  }
+  if (cudaMemset(f->flags, 0, sizeof(int) * NB128) != cudaSuccess) {
+    free_factor(f);
+    return MPCHOL_ERR_CUDA;
+  }
+  *out = f;
+  return MPCHOL_OK;
+}
+
+mpchol_status mpchol_factor_compute(mpchol_factor_t* f, const float* dA, int lda,
+                                    mpchol_stream_t stream) {
+  if (f == nullptr || dA == nullptr || lda < f->n) return MPCHOL_ERR_BAD_ARG;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  MPCHOL_CUDA_TRY(cudaMemcpy2DAsync(f->A, sizeof(float) * f->ld, dA, sizeof(float) * lda,
+                                    sizeof(float) * f->n, f->n, cudaMemcpyDeviceToDevice, s));
+  return run_factor(f, s);
+}
+
+mpchol_status mpchol_factor(const mpchol_opts* opts, int n, const float* dA, int lda,
+                            mpchol_factor_t** out, mpchol_stream_t stream) {
+  mpchol_status s = mpchol_factor_create(opts, n, out);
+  if (s != MPCHOL_OK) return s;
+  s = mpchol_factor_compute(*out, dA, lda, stream);
+  if (s != MPCHOL_OK) {
+    free_factor(*out);
+    *out = nullptr;
+  }
+  return s;
+}
+
+mpchol_status mpchol_factor_destroy(mpchol_factor_t* f) {
+  if (f == nullptr) return MPCHOL_ERR_BAD_ARG;
+  free_factor(f);
+  return MPCHOL_OK;
+}
+
+mpchol_status mpchol_factor_info_get(const mpchol_factor_t* fc, mpchol_factor_info* info,
+                                     int* hStepPrec, int* hStepFp64, mpchol_stream_t stream) {
+  mpchol_factor_t* f = const_cast<mpchol_factor_t*>(fc);
+  if (f == nullptr || info == nullptr) return MPCHOL_ERR_BAD_ARG;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  std::vector<StepState> steps(f->nsteps + 1);
+  DevStatus st;
+  MPCHOL_CUDA_TRY(cudaMemcpyAsync(steps.data(), f->steps, sizeof(StepState) * (f->nsteps + 1),
+                                  cudaMemcpyDeviceToHost, s));
+  MPCHOL_CUDA_TRY(cudaMemcpyAsync(&st, f->status, sizeof(DevStatus), cudaMemcpyDeviceToHost, s));
+  MPCHOL_CUDA_TRY(cudaStreamSynchronize(s));
+  memset(info, 0, sizeof(*info));
+  info->status = st.code;
+  info->fail_row = st.code == MPCHOL_ERR_NOT_SPD ? st.row : -1;
+  info->n_perturbed = st.perturbed;
+  info->nsteps = f->nsteps;
+  for (int k = 0; k < f->nsteps; ++k) {
+    const int m = f->n - k * f->b - std::min(f->b, f->n - k * f->b);
+    const int p = m > 0 ? steps[k].prec : FP32;
+    if (hStepPrec) hStepPrec[k] = p;
+    if (hStepFp64) hStepFp64[k] = steps[k].fp64_diag;
+    if (steps[k].fp64_diag) info->n_fp64_blocks++;
+    if (m > 0 && p >= 0 && p < 5) info->steps_by_prec[p]++;
+  }
+  return MPCHOL_OK;
+}
+
+mpchol_status mpchol_factor_lower(const mpchol_factor_t* f, const float** dL, int* ldl, int* n) {
+  if (f == nullptr) return MPCHOL_ERR_BAD_ARG;
+  if (dL) *dL = f->A;
+  if (ldl) *ldl = f->ld;
+  if (n) *n = f->n;
+  return MPCHOL_OK;
+}
+
+mpchol_status mpchol_factor_diags(const mpchol_factor_t* f, const float** dD, const float** dDt) {
+  if (f == nullptr) return MPCHOL_ERR_BAD_ARG;
+  if (dD) *dD = f->d;
+  if (dDt) *dDt = f->dtilde;
+  return MPCHOL_OK;
+}
+
+mpchol_status mpchol_factor_prepare_solve(mpchol_factor_t* f, mpchol_stream_t stream) {
+  if (f == nullptr) return MPCHOL_ERR_BAD_ARG;
+  return ensure_solve(f, reinterpret_cast<cudaStream_t>(stream));
+}
+
+mpchol_status mpchol_pcg(mpchol_factor_t* f, const float* dA, int lda, const double* dB,
+                         double* dX, int nrhs, const mpchol_pcg_opts* opts, mpchol_report* rep,
+                         mpchol_stream_t stream) {
+  return run_pcg<float>(f, dA, lda, dB, dX, nrhs, opts, rep, reinterpret_cast<cudaStream_t>(stream));
+}
+
+mpchol_status mpchol_pcg_f64(mpchol_factor_t* f, const double* dA, int lda, const double* dB,
+                             double* dX, int nrhs, const mpchol_pcg_opts* opts,
+                             mpchol_report* rep, mpchol_stream_t stream) {
+  return run_pcg<double>(f, dA, lda, dB, dX, nrhs, opts, rep, reinterpret_cast<cudaStream_t>(stream));
+}
+
+mpchol_status mpchol_apply_precond(mpchol_factor_t* f, const double* dR, double* dZ, int nrhs,
+                                   mpchol_stream_t stream) {
+  if (f == nullptr || dR == nullptr || dZ == nullptr || nrhs < 1 || nrhs > 8) return MPCHOL_ERR_BAD_ARG;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  mpchol_status ss = ensure_solve(f, s);
+  if (ss != MPCHOL_OK) return ss;
+  const int nr = pcg_padded_nrhs(nrhs);
+  const size_t nv = (size_t)f->n * 8;
+  double* rp = f->vec + 5 * nv;     // bb slot
+  double* tmp = f->vec + 6 * nv;
+  double* zp = f->vec + 2 * nv;     // z slot
+  MPCHOL_CUDA_TRY(cudaMemsetAsync(f->status, 0, sizeof(DevStatus), s));
+  MPCHOL_CUDA_TRY(launch_pad_columns(dR, f->n, nrhs, rp, nr, s));
+  ss = apply_precond(f, rp, tmp, zp, nr, nullptr, s);
+  if (ss != MPCHOL_OK) return ss;
+  MPCHOL_CUDA_TRY(cudaMemcpy2DAsync(dZ, sizeof(double) * f->n, zp, sizeof(double) * f->n,
+                                    sizeof(double) * f->n, nrhs, cudaMemcpyDeviceToDevice, s));
+  DevStatus st;
+  if (read_status(f, s, &st) != 0) return MPCHOL_ERR_CUDA;
+  return (mpchol_status)st.code;
+}
+
+mpchol_status mpchol_symv(const float* dA, int lda, int n, const double* dX, double* dY, int nrhs,
+                          mpchol_stream_t stream) {
+  if (dA == nullptr || dX == nullptr || dY == nullptr || n <= 0 || lda < n) return MPCHOL_ERR_BAD_ARG;
+  if (nrhs != 1 && nrhs != 2 && nrhs != 4 && nrhs != 8) return MPCHOL_ERR_BAD_ARG;
+  MPCHOL_CUDA_TRY(launch_symv_skip<float>(dA, lda, n, dX, dY, nrhs, nullptr,
+                                          reinterpret_cast<cudaStream_t>(stream)));
+  return MPCHOL_OK;
+}
+
+int mpchol_precond_cg(double* dA, double* dX, double* dB, int n, int r, double normA,
+                      float eps_prime, float flr, int perturb_diag, int microscal_size,
+                      double rel_tol, int max_it, mpchol_stream_t stream) {
+  (void)normA;
+  (void)microscal_size;
+  if (dA == nullptr || dX == nullptr || dB == nullptr || n <= 0) return -(100 + MPCHOL_ERR_BAD_ARG);
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  mpchol_opts o;
+  mpchol_opts_default(&o);
+  o.block_size = r;
+  o.eps_prime = eps_prime;
+  o.floor = flr;
+  o.diag_pert = perturb_diag ? 1 : 0;
+  mpchol_factor_t* f = nullptr;
+  mpchol_status st = mpchol_factor_create(&o, n, &f);
+  if (st != MPCHOL_OK) return -(100 + st);
+  // FP64 -> FP32 directly into the factor's storage (src/mixed_cholesky.cu:122)
+  if (launch_f64_to_f32(dA, n, f->A, f->ld, n, s) != cudaSuccess) {
+    free_factor(f);
+    return -(100 + MPCHOL_ERR_CUDA);
+  }
+  st = run_factor(f, s);
+  mpchol_factor_info info;
+  if (st == MPCHOL_OK) st = mpchol_factor_info_get(f, &info, nullptr, nullptr, stream);
+  if (st != MPCHOL_OK) { free_factor(f); return -(100 + st); }
+  if (info.status == MPCHOL_ERR_NOT_SPD) { free_factor(f); return info.fail_row + 1; }
+  if (info.status != MPCHOL_OK) { free_factor(f); return -(100 + info.status); }
+  mpchol_pcg_opts po;
+  mpchol_pcg_opts_default(&po);
+  po.rel_tol = rel_tol;
+  po.max_it = max_it;
+  po.x0_precond = 1;
+  st = run_pcg<double>(f, dA, n, dB, dX, 1, &po, nullptr, s);
+  free_factor(f);
+  if (st == MPCHOL_OK) return 0;
+  if (st == MPCHOL_PCG_MAXIT) return -1;
+  return -(100 + st);
+}
+
+int mpchol_switching_chol(float* dA, int n, int b, float* d_diagVals, float* updated_diag,
+                          float eps_prime, int perturb_diag, int microscal_size,
+                          mpchol_stream_t stream, uint8_t* scales) {
+  (void)microscal_size;
+  (void)scales;
+  if (dA == nullptr || n <= 0) return MPCHOL_ERR_BAD_ARG;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  mpchol_opts o;
+  mpchol_opts_default(&o);
+  o.block_size = b;
+  o.eps_prime = eps_prime;
+  o.diag_pert = perturb_diag ? 1 : 0;
+  mpchol_factor_t* f = nullptr;
+  mpchol_status st = mpchol_factor(&o, n, dA, n, &f, stream);
+  if (st != MPCHOL_OK) return st;
+  mpchol_factor_info info;
+  st = mpchol_factor_info_get(f, &info, nullptr, nullptr, stream);
+  if (st == MPCHOL_OK) {
+    if (cudaMemcpy2DAsync(dA, sizeof(float) * n, f->A, sizeof(float) * f->ld, sizeof(float) * n, n,
+                          cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+      st = MPCHOL_ERR_CUDA;
+    if (d_diagVals && cudaMemcpyAsync(d_diagVals, f->d, sizeof(float) * n, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+      st = MPCHOL_ERR_CUDA;
+    if (updated_diag && cudaMemcpyAsync(updated_diag, f->dtilde, sizeof(float) * n, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+      st = MPCHOL_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) st = MPCHOL_ERR_CUDA;
+    if (st == MPCHOL_OK) st = (mpchol_status)info.status;
+  }
+  free_factor(f);
+  return st;
+}
+
+mpchol_status mpchol_quantize(const float* dX, void* dQ, long long count, int fmt,
+                              mpchol_stream_t stream) {
+  if (count < 0 || (count > 0 && (dX == nullptr || dQ == nullptr))) return MPCHOL_ERR_BAD_ARG;
+  if (fmt != FP16 && fmt != E4M3 && fmt != E5M2) return MPCHOL_ERR_BAD_ARG;
+  MPCHOL_CUDA_TRY(launch_quantize_elems(dX, dQ, count, fmt, reinterpret_cast<cudaStream_t>(stream)));
+  return MPCHOL_OK;
+}
+
+mpchol_status mpchol_quantize_rows(const float* dP, int m, int k, int ldp, int fmt, void* dQ,
+                                   void* dScale, mpchol_stream_t stream) {
+  if (dP == nullptr || dQ == nullptr || dScale == nullptr || m < 0 || ldp < m) return MPCHOL_ERR_BAD_ARG;
+  if (k < 32 || k > 256 || k % 32 != 0) return MPCHOL_ERR_BAD_ARG;
+  if (fmt != FP16 && fmt != E4M3 && fmt != E5M2 && fmt != MXFP8) return MPCHOL_ERR_BAD_ARG;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (fmt == MXFP8)
+    MPCHOL_CUDA_TRY(launch_quantize_rows(dP, ldp, m, k, fmt, dQ, k, nullptr,
+                                         reinterpret_cast<uint8_t*>(dScale), k / 32, s));
+  else
+    MPCHOL_CUDA_TRY(launch_quantize_rows(dP, ldp, m, k, fmt, dQ, k,
+                                         reinterpret_cast<int8_t*>(dScale), nullptr, 0, s));
+  return MPCHOL_OK;
+}
+
+mpchol_status mpchol_quantize_hash(unsigned long long first, unsigned long long count,
+                                   unsigned long long chunk, int fmt, unsigned long long* dHash,
+                                   mpchol_stream_t stream) {
+  if (dHash == nullptr || chunk == 0 || first + count > (1ull << 32)) return MPCHOL_ERR_BAD_ARG;
+  if (fmt != FP16 && fmt != E4M3 && fmt != E5M2) return MPCHOL_ERR_BAD_ARG;
+  MPCHOL_CUDA_TRY(launch_quantize_hash(first, count, chunk, fmt, dHash,
+                                       reinterpret_cast<cudaStream_t>(stream)));
+  return MPCHOL_OK;
+}
+
+mpchol_status mpchol_syrk_update(float* dC, int ldc, int m, int k, int fmt, const void* dQ,
+                                 const void* dScale, const float* dP, int ldp,
+                                 mpchol_stream_t stream) {
+  if (dC == nullptr || m < 0 || ldc < m || k <= 0) return MPCHOL_ERR_BAD_ARG;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (fmt == FP32) {
+    if (dP == nullptr || ldp < m) return MPCHOL_ERR_BAD_ARG;
+    MPCHOL_CUDA_TRY(launch_syrk_f32(dC, ldc, m, k, dP, ldp, nullptr, nullptr, s));
+    return MPCHOL_OK;
+  }
+  if (!syrk_tc_supported(fmt, k)) return MPCHOL_ERR_NOT_SUPPORTED;
+  if (dQ == nullptr || dScale == nullptr) return MPCHOL_ERR_BAD_ARG;
+  MPCHOL_CUDA_TRY(launch_syrk_tc(dC, ldc, m, k, fmt, dQ, k, reinterpret_cast<const int8_t*>(dScale),
+                                 nullptr, 0, nullptr, nullptr, s));
+  return MPCHOL_OK;
+}
+
+}  // extern "C"

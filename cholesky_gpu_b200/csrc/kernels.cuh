@@ -1,0 +1,85 @@
+// Internal launch interfaces of the mpchol kernels (not part of the C ABI).
+#pragma once
+#include "common.cuh"
+
+namespace mpchol {
+
+struct PotrfParams {
+  int diag_pert;
+  float pert;
+  float pivot_floor;
+};
+
+// Per-step device-side decision state (one slot per factor step).
+struct StepState {
+  unsigned int max_ratio_bits;  // max_i d_i / dtilde_i over trailing rows (float bits, >= 0)
+  int literal_code;             // reference-literal: max over rows of (2 - choice index); choice index 0 FP32, 1 FP16, 2 E4M3
+  int prec;                     // chosen trailing-update precision (Fmt)
+  int fp64_diag;                // 1: factor this step's diagonal block in FP64
+};
+
+struct DecisionParams {
+  int policy;          // Fmt or SWITCHING
+  int switch_mode;     // 0 build criterion, 1 reference-literal
+  float eps_prime;
+  float floor_ratio;   // near-indefinite flag threshold
+  int ladder_len;
+  int ladder[4];
+};
+
+// ---- POTRF of the diagonal block (one CTA) ------------------------------
+size_t potrf_smem_bytes(int bs);
+size_t potrf_scratch64_elems(int bs);
+// Also writes the inverses of the 32x32 diagonal tiles of the factored block
+// to winv (ceil(bs/32) tiles, column-major 32x32 each) for the panel solve.
+cudaError_t launch_potrf(float* A, int lda, int s, int bs, const float* d, const float* sh,
+                         const PotrfParams& p, const int* fp64_flag, double* scratch64,
+                         float* winv, DevStatus* st, cudaStream_t stream);
+
+// ---- panel TRSM + fused diagonal tracker / decision statistics ----------
+// Solves X * L11^T = A21 in place for rows [s+bs, n) of block column s,
+// subtracts each row's sum of squares from dtilde, stores it in rowsq, and
+// folds the switching statistics of the rows into step (and the FP64 flag of
+// the next diagonal block into next).
+cudaError_t launch_trsm_panel(float* A, int lda, int n, int s, int bs, const float* winv,
+                              const float* d, float* dtilde, float* rowsq, StepState* step,
+                              StepState* next, int next_bs, const DecisionParams& dp,
+                              DevStatus* st, cudaStream_t stream);
+
+// ---- decision + panel quantization --------------------------------------
+// Resolves the step precision (from the policy or the statistics in step),
+// then writes the K-major quantized panel q (row stride ldq bytes-or-halfs,
+// see quant.cu) with per-row or per-32-block scales, and accumulates the
+// rounding-shift estimate sh[i] += u_p * rowsq[i] for low-precision steps.
+cudaError_t launch_quantize_panel(const float* P, int ldp, int m, int k, StepState* step,
+                                  const DecisionParams& dp, void* q, int ldq, int8_t* rowexp,
+                                  uint8_t* mxexp, int ldmx, const float* rowsq, float* sh,
+                                  DevStatus* st, cudaStream_t stream);
+// Fixed-format variant (test entry point): no decision, no shift.
+cudaError_t launch_quantize_rows(const float* P, int ldp, int m, int k, int fmt, void* q, int ldq,
+                                 int8_t* rowexp, uint8_t* mxexp, int ldmx, cudaStream_t stream);
+cudaError_t launch_quantize_elems(const float* x, void* q, long long count, int fmt,
+                                  cudaStream_t stream);
+cudaError_t launch_quantize_hash(unsigned long long first, unsigned long long count,
+                                 unsigned long long chunk, int fmt, unsigned long long* hashes,
+                                 cudaStream_t stream);
+
+// ---- trailing update ----------------------------------------------------
+// FP32 SIMT SYRK: C(m x m, lower) -= P P^T, P = m x k column-major (ldp).
+// Skips (returns immediately on device) unless *prec_sel == FP32 when
+// prec_sel is non-null.
+cudaError_t launch_syrk_f32(float* C, int ldc, int m, int k, const float* P, int ldp,
+                            const int* prec_sel, DevStatus* st, cudaStream_t stream);
+// tcgen05 SYRK from the K-major quantized panel (FP16 / E4M3 / E5M2 / MXFP8).
+struct TcPanel;  // defined in syrk_tc.cu
+bool syrk_tc_supported(int fmt, int k);
+cudaError_t launch_syrk_tc(float* C, int ldc, int m, int k, int fmt, const void* q, int ldq,
+                           const int8_t* rowexp, const uint8_t* mxexp, int ldmx,
+                           const int* prec_sel, DevStatus* st, cudaStream_t stream);
+
+// ---- PCG building blocks ------------------------------------------------
+template <typename TA>
+cudaError_t launch_symv(const TA* A, int lda, int n, const double* x, double* y, int nrhs,
+                        cudaStream_t stream);
+
+}  // namespace mpchol

@@ -1,0 +1,43 @@
+// Launchers of the PCG kernels (pcg.cu).
+#pragma once
+#include "common.cuh"
+
+namespace mpchol {
+
+int pcg_padded_nrhs(int nrhs);   // 1, 2, 4 or 8
+int pcg_vgrid();                 // CTAs of the reduction kernels (partials per vector)
+
+template <typename TA>
+cudaError_t launch_symv_skip(const TA* A, int lda, int n, const double* x, double* y, int nrhs,
+                             const int* skip, cudaStream_t stream);
+cudaError_t launch_diag_inverse(const float* L, int ldl, int n, float* linv, cudaStream_t stream);
+cudaError_t launch_trsv(bool backward, const float* L, int ldl, int n, const float* linv,
+                        const double* rhs, double* out, int nrhs, int* flags, int epoch,
+                        int* ticket, const int* skip, DevStatus* st, cudaStream_t stream);
+cudaError_t launch_dot(const double* a, const double* b, int n, int nrhs, double* partials,
+                       const int* skip, cudaStream_t stream);
+cudaError_t launch_update_xr(double* x, double* r, const double* p, const double* Ap, int n,
+                             int nrhs, const double* pAp_partials, const double* rho,
+                             double* alpha_out, double* rr_partials, const int* skip,
+                             DevStatus* st, cudaStream_t stream);
+cudaError_t launch_update_p(double* p, const double* z, int n, int nrhs, const double* rz_partials,
+                            const double* rho_old, double* rho_out, const double* rr_partials,
+                            const double* bnorm2, double tol2, int* done, const int* skip,
+                            int* iters, cudaStream_t stream);
+cudaError_t launch_reduce_partials(const double* partials, double* out, int nrhs,
+                                   cudaStream_t stream);
+cudaError_t launch_residual(const double* b, const double* y, double* r, int n, int nrhs,
+                            double* rr_partials, cudaStream_t stream);
+cudaError_t launch_copy(const double* a, double* b, int n, int nrhs, cudaStream_t stream);
+
+// misc device utilities (util.cu)
+cudaError_t launch_extract_diag(const float* A, int lda, int n, float* d, float* dtilde,
+                                cudaStream_t stream);
+cudaError_t launch_f64_to_f32(const double* src, int lds, float* dst, int ldd, int n,
+                              cudaStream_t stream);
+template <typename TA>
+cudaError_t launch_frob_lower(const TA* A, int lda, int n, double* partials, cudaStream_t stream);
+cudaError_t launch_pad_columns(const double* src, int n, int ncols, double* dst, int ncols_pad,
+                               cudaStream_t stream);
+
+}  // namespace mpchol

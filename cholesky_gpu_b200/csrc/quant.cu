@@ -1,0 +1,215 @@
+// Step-precision decision and panel quantization.
+//
+// Replaces the reference's can_switch decision + host read of the result
+// (src/kernels_macros.cuh:191-211, src/switching_chol.cuh:117-124) and its
+// panel conversions convert_fp32_to_mxe4m3 / convert_transpose_fp32_to_mxe4m3
+// (src/fp8_utils.cuh:27-130) and convertFloatToHalf (src/kernels_macros.cuh:115-124).
+// The decision never leaves the device: every CTA resolves the same precision
+// from the statistics the panel solve reduced, CTA 0 records it, and the
+// trailing-update kernels read it.  The quantized panel is written K-major
+// (row-major m x k) so TMA can stage it for the tensor-core update.
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace mpchol {
+namespace {
+
+constexpr int QROWS = 32;    // rows per CTA
+constexpr int QTHR = 256;
+
+__device__ __forceinline__ int resolve_precision(const StepState* step, const DecisionParams& dp) {
+  if (dp.policy != SWITCHING) return dp.policy;
+  if (dp.switch_mode == 1) {
+    const int code = step->literal_code;            // 2 - min choice index
+    const int choice = 2 - code;
+    return choice == 0 ? FP32 : (choice == 1 ? FP16 : E4M3);
+  }
+  const float ratio = __uint_as_float(step->max_ratio_bits);
+  for (int k = 0; k < dp.ladder_len; ++k) {
+    const int p = dp.ladder[k];
+    if (unit_roundoff(p) * ratio <= dp.eps_prime) return p;
+  }
+  return FP32;
+}
+
+// Quantize one CTA tile of QROWS rows x k columns.  Lane l of a warp owns the
+// contiguous columns [l*c, (l+1)*c), c = k/32 (k is a multiple of 32, <= 256).
+__device__ void quantize_tile(const float* __restrict__ P, int ldp, int m, int k, int fmt,
+                              void* q, int ldq, int8_t* rowexp, uint8_t* mxexp, int ldmx,
+                              float* tile) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int row0 = blockIdx.x * QROWS;
+  const int nr = min(QROWS, m - row0);
+  // stage the rows (coalesced column reads), padded stride QROWS+1
+  for (int e = tid; e < k * QROWS; e += QTHR) {
+    const int c = e / QROWS, r = e % QROWS;
+    tile[c * (QROWS + 1) + r] = (r < nr) ? P[(size_t)c * ldp + row0 + r] : 0.0f;
+  }
+  __syncthreads();
+  const int cpl = k / 32;                   // columns per lane
+  for (int r = warp; r < nr; r += QTHR / 32) {
+    const int gi = row0 + r;
+    float v[8];
+    float amax = 0.0f;
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      v[t] = (t < cpl) ? tile[(lane * cpl + t) * (QROWS + 1) + r] : 0.0f;
+      amax = fmaxf(amax, fabsf(v[t]));
+    }
+    if (fmt == MXFP8) {
+      // one E8M0 scale per 32 consecutive columns = 32/cpl lanes
+      const int lpb = 32 / cpl;
+      float bmax = amax;
+      for (int o = 1; o < lpb; o <<= 1) bmax = fmaxf(bmax, __shfl_xor_sync(0xffffffffu, bmax, o));
+      const int e = mx_scale_exp(bmax);
+      const float inv = pow2f(-e);
+      uint8_t* qr = reinterpret_cast<uint8_t*>(q) + (size_t)gi * ldq + lane * cpl;
+#pragma unroll
+      for (int t = 0; t < 8; ++t)
+        if (t < cpl) qr[t] = f32_to_e4m3(v[t] * inv);
+      if ((lane % lpb) == 0) mxexp[(size_t)gi * ldmx + lane / lpb] = (uint8_t)(e + 127);
+    } else {
+      const float rmax = warp_max(amax);
+      const int e = row_scale_exp(rmax, fmt);
+      const float inv = pow2f(-e);
+      if (fmt == FP16) {
+        uint16_t* qr = reinterpret_cast<uint16_t*>(q) + (size_t)gi * ldq + lane * cpl;
+#pragma unroll
+        for (int t = 0; t < 8; ++t)
+          if (t < cpl) qr[t] = f32_to_f16(v[t] * inv);
+      } else {
+        uint8_t* qr = reinterpret_cast<uint8_t*>(q) + (size_t)gi * ldq + lane * cpl;
+#pragma unroll
+        for (int t = 0; t < 8; ++t)
+          if (t < cpl) qr[t] = (fmt == E4M3) ? f32_to_e4m3(v[t] * inv) : f32_to_e5m2(v[t] * inv);
+      }
+      if (lane == 0) rowexp[gi] = (int8_t)e;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(QTHR)
+quantize_panel_kernel(const float* __restrict__ P, int ldp, int m, int k, StepState* step,
+                      DecisionParams dp, void* q, int ldq, int8_t* rowexp, uint8_t* mxexp, int ldmx,
+                      const float* __restrict__ rowsq, float* sh, DevStatus* st) {
+  if (st->code != 0) return;
+  extern __shared__ __align__(16) float qtile[];
+  const int p = resolve_precision(step, dp);
+  if (blockIdx.x == 0 && threadIdx.x == 0) step->prec = p;
+  if (p == FP32) return;
+  if (sh != nullptr) {
+    const float u = unit_roundoff(p);
+    for (int r = threadIdx.x; r < QROWS; r += QTHR) {
+      const int gi = blockIdx.x * QROWS + r;
+      if (gi < m) sh[gi] += u * rowsq[gi];
+    }
+  }
+  quantize_tile(P, ldp, m, k, p, q, ldq, rowexp, mxexp, ldmx, qtile);
+}
+
+__global__ void __launch_bounds__(QTHR)
+quantize_rows_kernel(const float* __restrict__ P, int ldp, int m, int k, int fmt, void* q, int ldq,
+                     int8_t* rowexp, uint8_t* mxexp, int ldmx) {
+  extern __shared__ __align__(16) float qtile[];
+  quantize_tile(P, ldp, m, k, fmt, q, ldq, rowexp, mxexp, ldmx, qtile);
+}
+
+__global__ void quantize_elems_kernel(const float* __restrict__ x, void* q, long long count, int fmt) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float v = x[i];
+    if (fmt == FP16) reinterpret_cast<uint16_t*>(q)[i] = f32_to_f16(v);
+    else if (fmt == E5M2) reinterpret_cast<uint8_t*>(q)[i] = f32_to_e5m2(v);
+    else reinterpret_cast<uint8_t*>(q)[i] = f32_to_e4m3(v);
+  }
+}
+
+__device__ __forceinline__ unsigned long long mix64(unsigned long long h, unsigned long long v) {
+  return h ^ (v + 0x9e3779b97f4a7c15ull + (h << 6) + (h >> 2));
+}
+
+// One warp per chunk of raw bit patterns: lanes convert 32 consecutive
+// patterns at a time, lane 0 folds them in order (the hash is sequential).
+__global__ void quantize_hash_kernel(unsigned long long first, unsigned long long count,
+                                     unsigned long long chunk, int fmt, unsigned long long* hashes) {
+  const int lane = threadIdx.x & 31;
+  const long long nch = (long long)((count + chunk - 1) / chunk);
+  const long long warp_g = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long c = warp_g; c < nch; c += nwarps) {
+    const unsigned long long lo = first + (unsigned long long)c * chunk;
+    unsigned long long hi = lo + chunk;
+    if (hi > first + count) hi = first + count;
+    unsigned long long h = 0;
+    for (unsigned long long b0 = lo; b0 < hi; b0 += 32) {
+      const unsigned long long b = b0 + lane;
+      unsigned int qv = 0;
+      if (b < hi) {
+        const float x = __uint_as_float((unsigned int)b);
+        if (fmt == FP16) qv = f32_to_f16(x);
+        else if (fmt == E5M2) qv = f32_to_e5m2(x);
+        else qv = f32_to_e4m3(x);
+        if (isnan(x)) qv = 0xffffu;
+        else if (isinf(x)) qv = 0xfffeu;
+      }
+      const int nvalid = (int)min(32ull, hi - b0);
+      for (int l = 0; l < nvalid; ++l) {
+        const unsigned int ql = __shfl_sync(0xffffffffu, qv, l);
+        h = mix64(h, ql);
+      }
+    }
+    if (lane == 0) hashes[c] = h;
+  }
+}
+
+size_t qtile_smem(int k) { return (size_t)k * (QROWS + 1) * sizeof(float); }
+
+}  // namespace
+
+cudaError_t launch_quantize_panel(const float* P, int ldp, int m, int k, StepState* step,
+                                  const DecisionParams& dp, void* q, int ldq, int8_t* rowexp,
+                                  uint8_t* mxexp, int ldmx, const float* rowsq, float* sh,
+                                  DevStatus* st, cudaStream_t stream) {
+  if (m <= 0) return cudaSuccess;
+  const size_t smem = qtile_smem(k);
+  cudaError_t e = cudaFuncSetAttribute(quantize_panel_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  quantize_panel_kernel<<<ceil_div(m, QROWS), QTHR, smem, stream>>>(P, ldp, m, k, step, dp, q, ldq,
+                                                                    rowexp, mxexp, ldmx, rowsq, sh, st);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_quantize_rows(const float* P, int ldp, int m, int k, int fmt, void* q, int ldq,
+                                 int8_t* rowexp, uint8_t* mxexp, int ldmx, cudaStream_t stream) {
+  if (m <= 0) return cudaSuccess;
+  const size_t smem = qtile_smem(k);
+  cudaError_t e = cudaFuncSetAttribute(quantize_rows_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  quantize_rows_kernel<<<ceil_div(m, QROWS), QTHR, smem, stream>>>(P, ldp, m, k, fmt, q, ldq, rowexp,
+                                                                   mxexp, ldmx);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_quantize_elems(const float* x, void* q, long long count, int fmt,
+                                  cudaStream_t stream) {
+  if (count <= 0) return cudaSuccess;
+  long long blocks = (count + 255) / 256;
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  quantize_elems_kernel<<<(int)blocks, 256, 0, stream>>>(x, q, count, fmt);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_quantize_hash(unsigned long long first, unsigned long long count,
+                                 unsigned long long chunk, int fmt, unsigned long long* hashes,
+                                 cudaStream_t stream) {
+  if (count == 0) return cudaSuccess;
+  const long long nch = (long long)((count + chunk - 1) / chunk);
+  long long blocks = (nch * 32 + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  quantize_hash_kernel<<<(int)blocks, 256, 0, stream>>>(first, count, chunk, fmt, hashes);
+  return cudaGetLastError();
+}
+
+}  // namespace mpchol

@@ -1,0 +1,158 @@
+// Panel TRSM with the fused switching epilogue.
+//
+// Replaces the reference's cublasStrsm of the panel (src/switching_chol.cuh:98-110,
+// correct form RIGHT/LOWER/TRANS at src/sChol.cuh:273-280), its update_diag
+// kernel (src/kernels_macros.cuh:177-190) and the per-row part of can_switch
+// (src/kernels_macros.cuh:191-211).
+//
+// X * L11^T = A21 for the m rows below the diagonal block.  Rows are
+// independent, so one CTA owns 64 rows for the whole solve (kept in shared
+// memory) and walks the 32-column tiles J: X_J -= X_{<J} L_{J,<J}^T (a small
+// register-tiled GEMM), then X_J = X_J L_JJ^-T with the tile inverse computed
+// by the POTRF kernel.  The epilogue writes X back, folds each row's sum of
+// squares into the Schur-diagonal tracker dtilde and reduces the switching
+// statistics for the step (max d/dtilde, reference-literal choice) and the
+// near-indefinite flag of the next diagonal block.
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace mpchol {
+namespace {
+
+constexpr int TR = 64;       // rows per CTA
+constexpr int NTHR = 256;
+constexpr int LLD = 33;      // padded stride of the L tile-row in smem
+
+__global__ void __launch_bounds__(NTHR)
+trsm_panel_kernel(float* __restrict__ A, int lda, int n, int s, int bs, const float* __restrict__ winv,
+                  const float* __restrict__ d, float* __restrict__ dtilde, float* __restrict__ rowsq,
+                  StepState* step, StepState* next, int next_bs, DecisionParams dp, DevStatus* st) {
+  if (st->code != 0) return;
+  extern __shared__ __align__(16) float sm[];
+  float* Xs = sm;                          // [bs][TR], column-major in smem
+  float* Ls = Xs + (size_t)bs * TR;        // [bs][LLD] tile-row of L11 (k-major)
+  float* Ws = Ls + (size_t)bs * LLD;       // [32][LLD] inverse of the diagonal tile
+  __shared__ float red_max[NTHR / 32];
+  __shared__ int red_lit[NTHR / 32];
+
+  const int tid = threadIdx.x;
+  const int row0 = s + bs + blockIdx.x * TR;   // first global row of this CTA
+  const int nrows = min(TR, n - row0);
+  if (nrows <= 0) return;
+
+  // load the CTA's rows of the panel
+  for (int e = tid; e < bs * TR; e += NTHR) {
+    const int c = e / TR, r = e % TR;
+    Xs[e] = (r < nrows) ? A[(size_t)(s + c) * lda + row0 + r] : 0.0f;
+  }
+  const int tr = tid % 16, tc = tid / 16;   // 4 rows x 2 cols per thread
+  const int NT = bs / 32;
+  for (int J = 0; J < NT; ++J) {
+    // tile-row J of L11 (columns 0..32J+31) and the inverse of L_JJ
+    const int kend = 32 * J;
+    for (int e = tid; e < (kend + 32) * 32; e += NTHR) {
+      const int k = e / 32, c = e % 32;
+      Ls[k * LLD + c] = A[(size_t)(s + k) * lda + s + 32 * J + c];
+    }
+    for (int e = tid; e < 32 * 32; e += NTHR) {
+      const int m = e / 32, c = e % 32;                // winv column-major: (L^-1)[c][m] at m*32+c
+      Ws[m * LLD + c] = winv[J * 1024 + m * 32 + c];
+    }
+    __syncthreads();
+    // X_J -= X_{<J} L_{J,<J}^T
+    float acc[4][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) acc[i][j] = Xs[(kend + 2 * tc + j) * TR + 4 * tr + i];
+    for (int k = 0; k < kend; ++k) {
+      const float4 xv = *reinterpret_cast<const float4*>(&Xs[k * TR + 4 * tr]);
+      const float l0 = Ls[k * LLD + 2 * tc], l1 = Ls[k * LLD + 2 * tc + 1];
+      acc[0][0] -= xv.x * l0; acc[0][1] -= xv.x * l1;
+      acc[1][0] -= xv.y * l0; acc[1][1] -= xv.y * l1;
+      acc[2][0] -= xv.z * l0; acc[2][1] -= xv.z * l1;
+      acc[3][0] -= xv.w * l0; acc[3][1] -= xv.w * l1;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) Xs[(kend + 2 * tc + j) * TR + 4 * tr + i] = acc[i][j];
+    __syncthreads();
+    // X_J = X_J * L_JJ^-T :  x[r][c] = sum_{m<=c} a[r][m] * (L^-1)[c][m]
+    float out[4][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) { out[i][0] = 0.0f; out[i][1] = 0.0f; }
+    for (int m = 0; m < 32; ++m) {
+      const float4 av = *reinterpret_cast<const float4*>(&Xs[(kend + m) * TR + 4 * tr]);
+      const float w0 = Ws[m * LLD + 2 * tc], w1 = Ws[m * LLD + 2 * tc + 1];
+      out[0][0] += av.x * w0; out[0][1] += av.x * w1;
+      out[1][0] += av.y * w0; out[1][1] += av.y * w1;
+      out[2][0] += av.z * w0; out[2][1] += av.z * w1;
+      out[3][0] += av.w * w0; out[3][1] += av.w * w1;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) Xs[(kend + 2 * tc + j) * TR + 4 * tr + i] = out[i][j];
+    __syncthreads();
+  }
+  // write back the solved rows
+  for (int e = tid; e < bs * TR; e += NTHR) {
+    const int c = e / TR, r = e % TR;
+    if (r < nrows) A[(size_t)(s + c) * lda + row0 + r] = Xs[e];
+  }
+  // fused epilogue: Schur diagonal tracker and switching statistics
+  float ratio = 0.0f;
+  int lit = 0;   // 2 - (reference-literal choice index); max over rows
+  if (tid < nrows) {
+    const int gi = row0 + tid;
+    float sq = 0.0f;
+    for (int c = 0; c < bs; ++c) { const float v = Xs[c * TR + tid]; sq += v * v; }
+    rowsq[gi] = sq;
+    const float dt = dtilde[gi] - sq;
+    dtilde[gi] = dt;
+    const float di = d[gi];
+    ratio = dt > 0.0f ? di / dt : INFINITY;
+    if (isnan(ratio)) ratio = INFINITY;
+    // reference list {FP32, FP16, E4M3} with the reference's machine epsilons
+    const float ref_eps[3] = {1.1920929e-7f, 0.0009765625f, 0.125f};
+    int pick = 0;
+    for (int p = 0; p < 3; ++p)
+      if (ref_eps[p] * dt >= dp.eps_prime * di) { pick = p; break; }
+    lit = 2 - pick;
+    if (next != nullptr && gi - (s + bs) < next_bs && dt <= dp.floor_ratio * di) next->fp64_diag = 1;
+  }
+  float wm = warp_max(ratio);
+  int wl = lit;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) wl = max(wl, __shfl_xor_sync(0xffffffffu, wl, o));
+  if ((tid & 31) == 0) { red_max[tid >> 5] = wm; red_lit[tid >> 5] = wl; }
+  __syncthreads();
+  if (tid == 0) {
+    float bm = 0.0f; int bl = 0;
+    for (int w = 0; w < NTHR / 32; ++w) { bm = fmaxf(bm, red_max[w]); bl = max(bl, red_lit[w]); }
+    atomicMax(&step->max_ratio_bits, __float_as_uint(bm));
+    atomicMax(&step->literal_code, bl);
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_trsm_panel(float* A, int lda, int n, int s, int bs, const float* winv,
+                              const float* d, float* dtilde, float* rowsq, StepState* step,
+                              StepState* next, int next_bs, const DecisionParams& dp,
+                              DevStatus* st, cudaStream_t stream) {
+  const int m = n - s - bs;
+  if (m <= 0) return cudaSuccess;
+  const size_t smem = ((size_t)bs * TR + (size_t)bs * LLD + 32 * LLD) * sizeof(float);
+  cudaError_t e = cudaFuncSetAttribute(trsm_panel_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  trsm_panel_kernel<<<ceil_div(m, TR), NTHR, smem, stream>>>(A, lda, n, s, bs, winv, d, dtilde,
+                                                             rowsq, step, next, next_bs, dp, st);
+  return cudaGetLastError();
+}
+
+}  // namespace mpchol

@@ -1,0 +1,94 @@
+// Small device utilities of the solver: diagonal extraction, FP64 -> FP32
+// cast, Frobenius norm of a symmetric matrix from its lower triangle,
+// zero-padded copies of right-hand sides.
+//
+// extract_diag replaces the reference's extractDiagonal + D2D copy
+// (src/kernels_macros.cuh:161-173, src/mixed_cholesky.cu:128-131);
+// f64_to_f32 its convertDoubleToFloat (src/kernels_macros.cuh:78-86).
+#include "common.cuh"
+#include "pcg.cuh"
+
+namespace mpchol {
+namespace {
+
+__global__ void extract_diag_kernel(const float* __restrict__ A, int lda, int n, float* d,
+                                    float* dtilde) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float v = A[(size_t)i * lda + i];
+    d[i] = v;
+    dtilde[i] = v;
+  }
+}
+
+__global__ void f64_to_f32_kernel(const double* __restrict__ src, int lds, float* __restrict__ dst,
+                                  int ldd, int n) {
+  const long long total = (long long)n * n;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(e / n), r = (int)(e % n);
+    dst[(size_t)c * ldd + r] = (float)src[(size_t)c * lds + r];
+  }
+}
+
+template <typename TA>
+__global__ void frob_lower_kernel(const TA* __restrict__ A, int lda, int n, double* partials) {
+  double s = 0.0;
+  const long long total = (long long)n * n;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(e / n), r = (int)(e % n);
+    if (r >= c) {
+      const double v = (double)A[(size_t)c * lda + r];
+      s += (r == c ? 1.0 : 2.0) * v * v;
+    }
+  }
+  __shared__ double red[8];
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    partials[blockIdx.x] = t;
+  }
+}
+
+__global__ void pad_columns_kernel(const double* __restrict__ src, int n, int ncols,
+                                   double* __restrict__ dst, int ncols_pad) {
+  const long long total = (long long)n * ncols_pad;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(e / n);
+    dst[e] = (c < ncols) ? src[e] : 0.0;
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_extract_diag(const float* A, int lda, int n, float* d, float* dtilde,
+                                cudaStream_t stream) {
+  extract_diag_kernel<<<ceil_div(n, 256), 256, 0, stream>>>(A, lda, n, d, dtilde);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_f64_to_f32(const double* src, int lds, float* dst, int ldd, int n,
+                              cudaStream_t stream) {
+  f64_to_f32_kernel<<<148 * 8, 256, 0, stream>>>(src, lds, dst, ldd, n);
+  return cudaGetLastError();
+}
+
+template <typename TA>
+cudaError_t launch_frob_lower(const TA* A, int lda, int n, double* partials, cudaStream_t stream) {
+  frob_lower_kernel<TA><<<pcg_vgrid(), 256, 0, stream>>>(A, lda, n, partials);
+  return cudaGetLastError();
+}
+template cudaError_t launch_frob_lower<float>(const float*, int, int, double*, cudaStream_t);
+template cudaError_t launch_frob_lower<double>(const double*, int, int, double*, cudaStream_t);
+
+cudaError_t launch_pad_columns(const double* src, int n, int ncols, double* dst, int ncols_pad,
+                               cudaStream_t stream) {
+  pad_columns_kernel<<<148 * 4, 256, 0, stream>>>(src, n, ncols, dst, ncols_pad);
+  return cudaGetLastError();
+}
+
+}  // namespace mpchol

@@ -1,0 +1,210 @@
+/*
+ * mpchol -- mixed-precision blocked Cholesky preconditioner + FP64-checked PCG
+ * for NVIDIA B200 (sm_100a).  Plain C ABI: no C++ or torch types cross it.
+ *
+ * Conventions
+ *   - Matrices are column-major, lower triangle significant (as in the
+ *     reference, src/micro_chol.hpp:18-20, src/sChol.cuh:278-279).
+ *   - All pointers named d* are device pointers; h* are host pointers.
+ *   - Every call is ordered on the caller's stream; the library never
+ *     synchronizes the device except where a call is documented to return a
+ *     host-visible result (reports, info), and then only that stream.
+ *   - Errors are status codes.  The library never calls exit(), never destroys
+ *     caller-owned handles or streams, and its kernels never trap.
+ *   - Objects are re-entrant across different factor objects; one stream per
+ *     object at a time.
+ *
+ * Reference interfaces replaced (paths inside SudhanvaKulkarni123/Cholesky_GPU):
+ *   precond_CG      src/mixed_cholesky.cu:76-78   -> mpchol_precond_cg, mpchol_factor + mpchol_pcg
+ *   switching_chol  src/switching_chol.cuh:19-22  -> mpchol_switching_chol, mpchol_factor
+ *   solveWithCuSolver src/mixed_cholesky.cu:297   -> (oracle only; FP64 dense solve on CPU)
+ *   convert_fp32_to_mxe4m3 / convertFloatToHalf  src/fp8_utils.cuh:27-130,
+ *                   src/kernels_macros.cuh:115-124 -> mpchol_quantize*, fused in the factor
+ */
+#ifndef MPCHOL_H_
+#define MPCHOL_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define MPCHOL_API __attribute__((visibility("default")))
+#else
+#define MPCHOL_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* mpchol_stream_t; /* == cudaStream_t */
+
+typedef enum {
+  MPCHOL_OK = 0,
+  MPCHOL_ERR_BAD_ARG = 1,
+  MPCHOL_ERR_NOT_SPD = 2,      /* non-positive pivot; see info.fail_row */
+  MPCHOL_ERR_CUDA = 3,         /* a CUDA runtime call failed */
+  MPCHOL_ERR_ALLOC = 4,        /* device allocation failed */
+  MPCHOL_PCG_MAXIT = 5,        /* PCG stopped at max_it without reaching rel_tol */
+  MPCHOL_PCG_BREAKDOWN = 6,    /* p^T A p <= 0 or NaN, or rho NaN */
+  MPCHOL_ERR_TIMEOUT = 7,      /* a bounded device-side wait ran out */
+  MPCHOL_ERR_NOT_SUPPORTED = 8 /* option combination not built */
+} mpchol_status;
+
+/* Storage precision of a trailing update (and policy ids). */
+typedef enum {
+  MPCHOL_PREC_FP32 = 0,
+  MPCHOL_PREC_FP16 = 1,
+  MPCHOL_PREC_E4M3 = 2,   /* per-row power-of-two scaled E4M3 (RNE, satfinite) */
+  MPCHOL_PREC_E5M2 = 3,   /* per-row power-of-two scaled E5M2 */
+  MPCHOL_PREC_MXFP8 = 4,  /* OCP MX: E4M3 + E8M0 scale per 32 elements along K */
+  MPCHOL_PREC_SWITCHING = 5 /* per-step choice by the switching criterion */
+} mpchol_precision;
+
+/* Factorization options.  Field names follow the reference's settings.json
+ * "factorization_settings" keys (src/settings.json:7-12) where one exists. */
+typedef struct {
+  int block_size;      /* b: diagonal block / panel width (64..256, multiple of 32) */
+  int precision;       /* mpchol_precision policy */
+  float eps_prime;     /* switching threshold eps' */
+  float floor;         /* rows with dtilde_i <= floor * d_i flag their diagonal block for FP64 POTRF */
+  int diag_pert;       /* 1: shift pivots by pert * (accumulated rounding estimate) and floor them */
+  float pert;          /* shift multiplier (diag_pert) */
+  float pivot_floor;   /* diag_pert: pivots <= pivot_floor * d_i are raised to pivot_floor * d_i */
+  int switch_mode;     /* 0: build criterion (lowest ladder precision with u_p*max(d/dtilde) <= eps');
+                          1: reference-literal can_switch comparison (src/kernels_macros.cuh:191-211) */
+  int ladder_len;      /* switching ladder, lowest precision first (default {E4M3, FP16, FP32}) */
+  int ladder[4];
+  int left;            /* 0: right-looking (only value built); settings.json "left" */
+} mpchol_opts;
+
+/* Per-factor results, filled by mpchol_factor_info (synchronizes the stream). */
+typedef struct {
+  int status;          /* mpchol_status of the factorization */
+  int fail_row;        /* NOT_SPD: global row of the failed pivot */
+  int n_perturbed;     /* pivots raised by diag_pert */
+  int nsteps;          /* ceil(n / b) */
+  int n_fp64_blocks;   /* diagonal blocks factored in FP64 */
+  int steps_by_prec[5];/* number of trailing updates done in each mpchol_precision */
+} mpchol_factor_info;
+
+typedef struct {
+  double rel_tol;      /* stop when the FP64 true residual ||b-Ax||/||b|| <= rel_tol (every rhs) */
+  int max_it;          /* iteration cap (the reference uses 200, src/mixed_cholesky.cu:82) */
+  int x0_precond;      /* 1: x0 = M^-1 b as the reference (src/mixed_cholesky.cu:145-149); 0: x0 = 0 */
+  int check_every;     /* iterations between host convergence checks (>= 1) */
+} mpchol_pcg_opts;
+
+typedef struct {
+  int iterations;          /* PCG iterations taken */
+  int converged;           /* 1 if every rhs met rel_tol on the true residual */
+  double rel_residual;     /* max over rhs of ||b - A x|| / ||b||, FP64, recomputed from x */
+  double backward_error;   /* max over rhs of ||b - A x|| / (||A||_F ||x|| + ||b||) */
+  double precond_residual; /* max over rhs of sqrt(r^T z)/||b|| (the reference's stopping quantity) */
+} mpchol_report;
+
+typedef struct mpchol_factor mpchol_factor_t;
+
+/* ---- status / defaults ------------------------------------------------- */
+MPCHOL_API const char* mpchol_status_str(int status);
+MPCHOL_API void mpchol_opts_default(mpchol_opts* opts);
+MPCHOL_API void mpchol_pcg_opts_default(mpchol_pcg_opts* opts);
+/* Last CUDA error text recorded by the library in this process ("" if none). */
+MPCHOL_API const char* mpchol_last_error(void);
+
+/* ---- factorization (switching_chol, src/switching_chol.cuh:19-227) ---- */
+/* Allocate a factor object (device workspace for order n). */
+MPCHOL_API mpchol_status mpchol_factor_create(const mpchol_opts* opts, int n, mpchol_factor_t** out);
+/* Copy the lower triangle of dA (n x n, lda >= n) into the object and factor
+ * it on `stream`.  Asynchronous: failures inside kernels are reported by
+ * mpchol_factor_info. */
+MPCHOL_API mpchol_status mpchol_factor_compute(mpchol_factor_t* f, const float* dA, int lda, mpchol_stream_t stream);
+/* create + compute. */
+MPCHOL_API mpchol_status mpchol_factor(const mpchol_opts* opts, int n, const float* dA, int lda,
+                            mpchol_factor_t** out, mpchol_stream_t stream);
+MPCHOL_API mpchol_status mpchol_factor_destroy(mpchol_factor_t* f);
+/* Synchronizes `stream`; fills info; hStepPrec (nullable, length nsteps)
+ * receives each step's trailing-update precision, hStepFp64 (nullable) the
+ * FP64-diagonal flags. */
+MPCHOL_API mpchol_status mpchol_factor_info_get(const mpchol_factor_t* f, mpchol_factor_info* info,
+                                     int* hStepPrec, int* hStepFp64, mpchol_stream_t stream);
+/* Device pointer to the factor L (lower triangle valid; upper unspecified). */
+MPCHOL_API mpchol_status mpchol_factor_lower(const mpchol_factor_t* f, const float** dL, int* ldl, int* n);
+/* Device pointers to the tracked diagonals d (original) and dtilde (Schur). */
+MPCHOL_API mpchol_status mpchol_factor_diags(const mpchol_factor_t* f, const float** dD, const float** dDtilde);
+/* Prepare the solve-side data (diagonal-block inverses).  Called implicitly
+ * by the first mpchol_pcg / mpchol_apply_precond. */
+MPCHOL_API mpchol_status mpchol_factor_prepare_solve(mpchol_factor_t* f, mpchol_stream_t stream);
+
+/* ---- PCG (precond_CG, src/mixed_cholesky.cu:76-229) ---------------------- */
+/* Solve A X = B for nrhs (1..8) right-hand sides with M = L L^T.  dA is the
+ * FP32 operator (full symmetric storage), dB/dX are n x nrhs FP64 (ld = n).
+ * Synchronizes `stream` every check_every iterations (convergence test on
+ * the recursive residual; the final answer is re-checked on the true
+ * residual).  report may be NULL. */
+MPCHOL_API mpchol_status mpchol_pcg(mpchol_factor_t* f, const float* dA, int lda, const double* dB,
+                         double* dX, int nrhs, const mpchol_pcg_opts* opts, mpchol_report* report,
+                         mpchol_stream_t stream);
+/* Same with an FP64 operator (the reference's Dgemv on FP64 A). */
+MPCHOL_API mpchol_status mpchol_pcg_f64(mpchol_factor_t* f, const double* dA, int lda, const double* dB,
+                             double* dX, int nrhs, const mpchol_pcg_opts* opts,
+                             mpchol_report* report, mpchol_stream_t stream);
+/* dZ = (L L^T)^-1 dR for nrhs vectors (n x nrhs, ld = n), i.e. Dpotrs
+ * (src/mixed_cholesky.cu:204-206) on the FP32 factor with FP64 vectors. */
+MPCHOL_API mpchol_status mpchol_apply_precond(mpchol_factor_t* f, const double* dR, double* dZ, int nrhs,
+                                   mpchol_stream_t stream);
+/* dY = A dX for symmetric FP32 A (lower triangle read), FP64 vectors,
+ * nrhs columns (ld = n): the Dgemv of src/mixed_cholesky.cu:185-191. */
+MPCHOL_API mpchol_status mpchol_symv(const float* dA, int lda, int n, const double* dX, double* dY, int nrhs,
+                          mpchol_stream_t stream);
+
+/* ---- reference-shaped entry points (used by include/mpchol_refcompat.h) -- */
+/* precond_CG semantics: dA FP64 n x n (device, ld = n), dX written, dB read,
+ * block size r.  Returns 0 if converged, -1 if not, > 0 if the
+ * preconditioner failed (the reference's convention, src/mixed_cholesky.cu:149,225),
+ * and -(100 + status) for library errors.  normA is accepted and unused, as
+ * in the reference.  Convergence uses the FP64 true residual with tolerance
+ * rel_tol (the reference's rel_tol = 0 means "run max_it iterations"). */
+MPCHOL_API int mpchol_precond_cg(double* dA, double* dX, double* dB, int n, int r, double normA,
+                      float eps_prime, float flr, int perturb_diag, int microscal_size,
+                      double rel_tol, int max_it, mpchol_stream_t stream);
+/* switching_chol semantics: in-place factor of the FP32 matrix dA (ld = n)
+ * with block b; d_diagVals (n) receives the original diagonal and
+ * updated_diag (n) the Schur-complement diagonal tracker (the reference's
+ * caller fills both, src/mixed_cholesky.cu:128-131; here the library fills
+ * them).  scales (nullable) receives the last MX step's E8M0 codes.
+ * Returns an mpchol_status (the reference returns void). */
+MPCHOL_API int mpchol_switching_chol(float* dA, int n, int b, float* d_diagVals, float* updated_diag,
+                          float eps_prime, int perturb_diag, int microscal_size,
+                          mpchol_stream_t stream, uint8_t* scales);
+
+/* ---- quantizers (bit-exact vs lo_float ConvertFrom<kSaturate=true>) ----- */
+/* Elementwise FP32 -> fmt (E4M3/E5M2: 1 byte, FP16: 2 bytes) with RNE +
+ * satfinite, no scaling. */
+MPCHOL_API mpchol_status mpchol_quantize(const float* dX, void* dQ, long long count, int fmt,
+                              mpchol_stream_t stream);
+/* Panel quantization as done inside the factor: dP is m x k column-major
+ * (ld = ldp); dQ receives a row-major (K-major) m x k copy in fmt; dScale
+ * receives per-row int8 exponents (E4M3/E5M2/FP16, scale = 2^e, m bytes) or
+ * per-32-block E8M0 codes (MXFP8, m x ceil(k/32) bytes, row-major). */
+MPCHOL_API mpchol_status mpchol_quantize_rows(const float* dP, int m, int k, int ldp, int fmt, void* dQ,
+                                   void* dScale, mpchol_stream_t stream);
+/* Exhaustive-sweep helper: converts the raw bit patterns [first, first+count)
+ * and folds each chunk of `chunk` codes into one 64-bit hash (non-finite
+ * inputs folded as class tokens), dHash receives ceil(count/chunk) words. */
+MPCHOL_API mpchol_status mpchol_quantize_hash(unsigned long long first, unsigned long long count,
+                                   unsigned long long chunk, int fmt, unsigned long long* dHash,
+                                   mpchol_stream_t stream);
+
+/* ---- kernel-level entry points (tests and micro-benchmarks) ------------- */
+/* Trailing update C -= s_i s_j (Q Q^T) on the lower triangle of the m x m
+ * block dC (ld = ldc) from a quantized panel produced by
+ * mpchol_quantize_rows (fmt) or, for FP32, from the column-major panel dP. */
+MPCHOL_API mpchol_status mpchol_syrk_update(float* dC, int ldc, int m, int k, int fmt, const void* dQ,
+                                 const void* dScale, const float* dP, int ldp,
+                                 mpchol_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MPCHOL_H_ */

@@ -1,0 +1,164 @@
+"""Factor and solver parity against the CPU oracle and the FP64 dense solve.
+
+Factor parity: the GPU factor is compared with the oracle's blocked
+restatement run with the same per-step precisions and FP64-diagonal flags (read
+back from the GPU), by relative Frobenius error of the lower triangle with a
+per-precision bar.  Solutions are checked against the FP64 dense Cholesky
+solve, with the FP64 true residual, backward error and iteration count.
+"""
+import numpy as np
+import pytest
+import torch
+
+import cholesky_gpu_b200 as mp
+from cholesky_gpu_b200 import _lib, matgen
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+# relative Frobenius bar of ||L_gpu - L_oracle|| / ||L_oracle|| per step precision
+FACTOR_TOL = {O.FP32: 1e-5, O.FP16: 1e-3, O.E4M3: 5e-2, O.E5M2: 5e-2, O.MXFP8: 5e-2}
+
+
+def factor_parity(A: np.ndarray, **opts):
+    f = mp.factor(torch.from_numpy(A).cuda(), **opts)
+    info = f.info()
+    Lg = f.lower().cpu().numpy()
+    ref = O.blocked_chol(A, block_size=opts.get("block_size", 256),
+                         precision=O.SWITCHING, force_prec=info.step_prec,
+                         force_fp64=info.step_fp64,
+                         eps_prime=opts.get("eps_prime", 0.5), floor=opts.get("floor", 0.0),
+                         diag_pert=opts.get("diag_pert", 0), pert=opts.get("pert", 1.0),
+                         pivot_floor=opts.get("pivot_floor", 1e-7))
+    Lo = ref["L"]
+    err = np.linalg.norm(Lg - Lo) / np.linalg.norm(Lo)
+    return f, info, ref, err
+
+
+@pytest.mark.parametrize("n,b,prec", [
+    (1024, 128, "fp16"),    # the small plain-method workload (block 128, FP16 trailing)
+    (1000, 128, "fp32"),    # ragged: n not a multiple of b
+    (512, 256, "fp32"),
+    (768, 256, "e4m3"),
+    (640, 128, "e5m2"),
+    (96, 256, "fp32"),      # n < b: a single diagonal block
+])
+def test_factor_matches_oracle(cuda, n, b, prec):
+    A = matgen.spd_matrix(n, 1e2 if prec in ("e4m3", "e5m2") else 1e4, 1).numpy()
+    f, info, ref, err = factor_parity(A, block_size=b, precision=prec)
+    assert info.status == 0 and ref["status"] == 0
+    worst = max([O.FP32] + [p for p in info.step_prec[:-1]], key=lambda p: FACTOR_TOL[p])
+    print(f"n={n} b={b} {prec}: steps {info.step_prec} rel Frobenius {err:.2e}")
+    assert err < FACTOR_TOL[worst], err
+
+
+def test_switching_decisions_match_oracle_rule(cuda):
+    n, b = 1536, 256
+    A = matgen.spd_matrix(n, 1e6, 3).numpy()
+    f, info, ref, err = factor_parity(A, block_size=b, eps_prime=0.05)
+    assert info.status == 0
+    assert err < 1e-3
+    # re-derive each step's choice from the oracle's own tracker on the GPU's
+    # precision path: the rule must agree step by step
+    r2 = O.blocked_chol(A, block_size=b, precision=O.SWITCHING, eps_prime=0.05)
+    assert list(r2["step_prec"][:-1]) == list(info.step_prec[:-1])
+    d, dt = f.diags()
+    np.testing.assert_allclose(dt.cpu().numpy(), ref["dtilde"], rtol=1e-3, atol=1e-6)
+
+
+def test_not_spd_reports_failing_row(cuda):
+    A = matgen.spd_matrix(512, 10.0, 4).numpy()
+    A[300, 300] = -1.0
+    f = mp.factor(torch.from_numpy(A).cuda(), block_size=128, precision="fp32")
+    info = f.info()
+    assert info.status == _lib.ERR_NOT_SPD and info.fail_row == 300
+
+
+def test_fp64_diagonal_fallback_flags_blocks(cuda):
+    A = matgen.spd_matrix(768, 1e6, 6).numpy()
+    f, info, ref, err = factor_parity(A, block_size=128, precision="fp32", floor=0.5)
+    assert info.n_fp64_blocks > 0
+    assert err < 1e-5
+
+
+def test_apply_precond_matches_oracle_potrs(cuda):
+    n = 1000
+    A = matgen.spd_matrix(n, 1e4, 2).numpy()
+    f = mp.factor(torch.from_numpy(A).cuda(), block_size=128, precision="fp16")
+    L = f.lower().cpu().numpy()
+    R = np.random.default_rng(0).standard_normal((n, 3))
+    Z = f.apply_precond(torch.from_numpy(R).cuda()).cpu().numpy()
+    want = O.potrs(L, R)
+    assert np.abs(Z - want).max() / np.abs(want).max() < 1e-9
+
+
+@pytest.mark.parametrize("n,b,prec,kappa,nrhs", [
+    (1024, 128, "fp16", 1e4, 1),     # plain-method workload
+    (1024, 128, "fp32", 1e4, 2),
+    (2048, 256, "switching", 1e6, 1),
+    (1000, 128, "fp32", 1e3, 8),
+])
+def test_pcg_reaches_1e10_and_matches_dense_solve(cuda, n, b, prec, kappa, nrhs):
+    A = matgen.spd_matrix(n, kappa, 1).numpy()
+    B = matgen.rhs(n, nrhs, 2).numpy()
+    Ad = torch.from_numpy(A).cuda()
+    f = mp.factor(Ad, block_size=b, precision=prec, eps_prime=0.05)
+    X, rep = f.pcg(Ad, torch.from_numpy(B).cuda(), rel_tol=1e-10, max_it=300)
+    X = X.cpu().numpy()
+    print(f"n={n} {prec} kappa={kappa:.0e}: it={rep.iterations} rel={rep.rel_residual:.2e} "
+          f"be={rep.backward_error:.2e}")
+    assert rep.converged and rep.rel_residual <= 1e-10
+    res = np.linalg.norm(B - A.astype(np.float64) @ X, axis=0) / np.linalg.norm(B, axis=0)
+    assert res.max() <= 1.5e-10
+    Xd = O.dense_solve(A, B)
+    assert np.linalg.norm(X - Xd) / np.linalg.norm(Xd) < kappa * 1e-9
+    # the oracle's PCG on the GPU's factor takes a comparable number of iterations
+    _, it_o, _ = O.pcg(A, f.lower().cpu().numpy(), B if nrhs > 1 else B, 1e-10, 300)
+    assert abs(rep.iterations - it_o) <= max(3, it_o // 5)
+
+
+def test_pcg_fp64_operator(cuda):
+    n = 512
+    A32 = matgen.spd_matrix(n, 1e3, 9)
+    A64 = A32.double().cuda()
+    B = matgen.rhs(n, 1, 3).cuda()
+    f = mp.factor(A32.cuda(), block_size=128, precision="fp16")
+    X, rep = f.pcg(A64, B, rel_tol=1e-12)
+    assert rep.converged and rep.rel_residual <= 1e-12
+
+
+def test_pcg_maxit_is_reported(cuda):
+    n = 512
+    A = matgen.spd_matrix(n, 1e6, 9).cuda()
+    B = matgen.rhs(n, 1, 3).cuda()
+    f = mp.factor(A, block_size=128, precision="fp16")
+    X, rep = f.pcg(A, B, rel_tol=1e-14, max_it=2, check_every=1)
+    assert rep.status == _lib.PCG_MAXIT and not rep.converged and rep.iterations == 2
+
+
+def test_reference_shaped_precond_cg(cuda):
+    n = 768
+    A = matgen.spd_matrix(n, 1e4, 12).double().cuda()
+    b = matgen.rhs(n, 1, 13).cuda()
+    x = torch.zeros_like(b)
+    rc = mp.precond_CG(A, x, b, n, 128, 0.0, eps_prime=0.05, rel_tol=1e-10, max_it=200)
+    assert rc == 0
+    r = b - A @ x
+    assert (r.norm() / b.norm()).item() <= 1e-10
+    # reference default rel_tol = 0: runs max_it and reports "not converged"
+    x2 = torch.zeros_like(b)
+    assert mp.precond_CG(A, x2, b, n, 128, 0.0, eps_prime=0.05, rel_tol=0.0, max_it=5) == -1
+
+
+def test_reference_shaped_switching_chol(cuda):
+    n = 512
+    A = matgen.spd_matrix(n, 1e3, 14)
+    dA = A.clone().cuda()            # symmetric: row-major storage == column-major
+    d = torch.zeros(n, device="cuda")
+    dt = torch.zeros(n, device="cuda")
+    assert mp.switching_chol(dA, n, 128, d, dt, 0.05) == 0
+    Lg = dA.cpu().numpy().T          # column-major result viewed back
+    Lg = np.tril(Lg)
+    L64 = np.linalg.cholesky(A.double().numpy())
+    assert np.linalg.norm(Lg - L64) / np.linalg.norm(L64) < 2e-3
+    np.testing.assert_allclose(d.cpu().numpy(), np.diag(A.numpy()))
