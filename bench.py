@@ -1,0 +1,380 @@
+"""Time-to-solution benchmark for the mixed-precision Cholesky-preconditioned PCG.
+
+Metric: time to a 1e-10 FP64-checked relative residual ||b - A x|| / ||b|| on
+one B200, for the switching mixed-precision factor (E4M3 / FP16 / FP32 trailing
+updates chosen per step) next to the plain FP32-factor PCG on the same GPU.
+
+Workload (default): n = 8192 dense SPD A = Q diag(sigma) Q^T in FP32 storage,
+Q from QR of a seeded N(0,1) matrix, sigma geometric 1 -> 1e-6 (kappa = 1e6),
+block 256, one right-hand side b ~ N(0,1).  Synthetic seeded inputs stand in
+for the reference's generated matrices.  One "step" = factor + PCG to 1e-10 of
+that system.  A (256 MiB) is larger than the 126 MB L2, so every step streams
+it from HBM; no separate L2 flush is needed.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mpchol|reference]
+
+Under torchrun with N > 1 every rank solves its own system (replicas, no
+collective on the data path): value = max over ranks of the time to solution.
+`--impl reference` times the reference's own CPU path (its micro_cholesky,
+src/micro_chol.hpp, built from the reference sources into oracle/_ref, or the
+oracle's restatement of it) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+METRIC = "time to 1e-10 FP64 residual: FP8/MXFP8-chol PCG vs FP32-chol PCG, one B200"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="mpchol", choices=["mpchol", "reference"])
+    ap.add_argument("--n", type=int, default=8192)
+    ap.add_argument("--kappa", type=float, default=1e6)
+    ap.add_argument("--block", type=int, default=256)
+    ap.add_argument("--eps-prime", type=float, default=0.05)
+    ap.add_argument("--tol", type=float, default=1e-10)
+    ap.add_argument("--max-it", type=int, default=400)
+    ap.add_argument("--check-every", type=int, default=4)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- peaks
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------- GPU arm
+def run_gpu(args, world, rank, local):
+    import torch
+    import cholesky_gpu_b200 as mp
+    from cholesky_gpu_b200 import _lib, matgen
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+        pg = dist
+    lib = _lib.load()
+    n, b = args.n, args.block
+    seed = 3 + rank
+    A = matgen.spd_matrix(n, args.kappa, seed, device=dev)
+    B = matgen.rhs(n, 1, 100 + rank, device=dev)
+    A_host = A.cpu().pin_memory()
+    B_host = B.cpu().pin_memory()
+    stream = torch.cuda.current_stream(dev)
+
+    def solve_once(precision, Ad, Bd):
+        f = mp.Factor(n, block_size=b, precision=precision, eps_prime=args.eps_prime)
+        f.compute(Ad)
+        X, rep = f.pcg(Ad, Bd, rel_tol=args.tol, max_it=args.max_it, check_every=args.check_every)
+        return f, X, rep
+
+    # factor objects are created outside the timed region (allocation is setup)
+    fobj = {p: mp.Factor(n, block_size=b, precision=p, eps_prime=args.eps_prime)
+            for p in ("switching", "fp32")}
+
+    def step(precision):
+        f = fobj[precision]
+        f.compute(A)
+        X, rep = f.pcg(A, B, rel_tol=args.tol, max_it=args.max_it, check_every=args.check_every)
+        return X, rep
+
+    def timed(precision, k):
+        times, reps = [], []
+        for _ in range(k):
+            if pg:
+                pg.barrier()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            X, rep = step(precision)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+            reps.append(rep)
+        return times, reps
+
+    for _ in range(args.warmup):
+        step("switching")
+        step("fp32")
+    launches0 = lib.mpchol_kernel_launches()
+    with ClockSampler(local) as clk:
+        t_sw, r_sw = timed("switching", args.steps)
+        launches_sw = lib.mpchol_kernel_launches() - launches0
+        t_32, r_32 = timed("fp32", args.steps)
+    info_sw = fobj["switching"].info()
+
+    def mx(v):
+        if pg:
+            t = torch.tensor([v], dtype=torch.float64, device=dev)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            return t.item()
+        return v
+
+    ms_sw = mx(statistics.median(t_sw))
+    ms_32 = mx(statistics.median(t_32))
+
+    # end-to-end through the public API with host buffers (H2D + factor + PCG + D2H)
+    e2e_times = []
+    for i in range(max(2, min(args.steps, 3)) + 1):
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        Ad = A_host.to(dev, non_blocking=True)
+        Bd = B_host.to(dev, non_blocking=True)
+        f = fobj["switching"]
+        f.compute(Ad)
+        X, rep = f.pcg(Ad, Bd, rel_tol=args.tol, max_it=args.max_it, check_every=args.check_every)
+        xh = X.to("cpu", non_blocking=False)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if i > 0:
+            e2e_times.append(e0.elapsed_time(e1))
+    e2e_ms = mx(statistics.median(e2e_times))
+
+    # per-phase breakdown of one profiled step (events inside the library)
+    lib.mpchol_profile_enable(1)
+    prof0 = _lib.Profile()
+    lib.mpchol_profile_read(prof0, 1)
+    _, rep_p = step("switching")
+    torch.cuda.synchronize()
+    prof = _lib.Profile()
+    lib.mpchol_profile_read(prof, 1)
+    lib.mpchol_profile_enable(0)
+    phases = {nm: round(prof.ms[i], 4) for i, nm in enumerate(_lib.PHASE_NAMES) if prof.calls[i]}
+    calls = {nm: int(prof.calls[i]) for i, nm in enumerate(_lib.PHASE_NAMES) if prof.calls[i]}
+
+    # roofline of the dominant kernel group (PCG preconditioner solves or SYRK)
+    hbm, peak_kind = measured_peaks()
+    it = rep_p.iterations
+    dom = max(phases, key=phases.get)
+    nb128 = (n + 127) // 128
+    if dom == "trsv":
+        # one triangular solve reads the lower triangle of L (FP32) + the 128x128
+        # FP32 diagonal-block inverses, and reads/writes the n-vectors (FP64)
+        per_launch = (n * (n + 1) / 2) * 4 + nb128 * 128 * 128 * 4 + 3 * n * 8
+        achieved = per_launch / (phases[dom] / calls[dom] * 1e-3) / 1e9
+        bound, unit, peak = "hbm", "GB/s", hbm
+    elif dom == "symv":
+        per_launch = (n * (n + 1) / 2) * 4 + 2 * n * 8
+        achieved = per_launch / (phases[dom] / calls[dom] * 1e-3) / 1e9
+        bound, unit, peak = "hbm", "GB/s", hbm
+    else:
+        per_launch = None
+        achieved, bound, unit, peak = None, "hbm", "GB/s", hbm
+    roof = {"kernel": dom, "bound": bound, "achieved": achieved and round(achieved, 1),
+            "peak": peak, "peak_kind": peak_kind, "unit": unit,
+            "frac": achieved and round(achieved / peak, 4),
+            "algorithmic_bytes_per_launch": per_launch, "traffic": None}
+
+    result = {
+        "metric": METRIC,
+        "value": round(ms_sw, 3),
+        "unit": "ms",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms_sw, 3),
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "e4m3/fp16/fp32 factor, fp64 pcg",
+        "data": "synthetic (seeded Q diag(sigma) Q^T, geometric spectrum)",
+        "config": {"workload": f"spd n={n} kappa={args.kappa:g} block={b} switching eps'={args.eps_prime}",
+                   "n": n, "kappa": args.kappa, "block": b, "rhs": 1, "tol": args.tol,
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "inputs larger than L2 (A = %d MiB)" % (n * n * 4 // (1 << 20))},
+        "comparator_fp32_factor_ms": round(ms_32, 3),
+        "speedup_vs_fp32_factor": round(ms_32 / ms_sw, 3),
+        "iterations": {"switching": r_sw[-1].iterations, "fp32": r_32[-1].iterations},
+        "rel_residual": {"switching": r_sw[-1].rel_residual, "fp32": r_32[-1].rel_residual},
+        "backward_error": {"switching": r_sw[-1].backward_error, "fp32": r_32[-1].backward_error},
+        "step_precisions": {"fp32": info_sw.steps_by_prec[0], "fp16": info_sw.steps_by_prec[1],
+                            "e4m3": info_sw.steps_by_prec[2], "e5m2": info_sw.steps_by_prec[3]},
+        "phase_ms_switching_step": phases,
+        "phase_calls_switching_step": calls,
+        "e2e": {"value": round(e2e_ms, 3), "unit": "ms",
+                "h2d_bytes_per_step": int(A_host.numel() * 4 + B_host.numel() * 8),
+                "d2h_bytes_per_step": int(n * 8)},
+        "gpu_launches": int(launches_sw),
+        "roofline": roof,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        result["cpu_baseline"] = cpu_baseline(args, A_host.numpy(), B_host.numpy(),
+                                              r_32[-1].iterations)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return result if rank == 0 else None
+
+
+# ---------------------------------------------------------------- CPU side
+def cpu_baseline(args, A: np.ndarray, b: np.ndarray, iters: int, budget_s: float = 20.0):
+    """Reference CPU path on a bounded sample: micro_cholesky (FP32,
+    unblocked, single thread) on the leading n_s x n_s block, extrapolated by
+    (n/n_s)^3, plus the measured cost of one FP64 PCG iteration at full n
+    (FP32 GEMV + FP32-factor triangular solves) times the FP32 path's GPU
+    iteration count."""
+    from oracle import oracle as O
+
+    n = A.shape[0]
+    kind = "reference" if O.REF_MICRO.exists() else "port"
+    ns = min(n, 1536)
+    sub = np.array(A[:ns, :ns], dtype=np.float32, order="F")
+    t0 = time.perf_counter()
+    if kind == "reference":
+        L, rc = O.ref_micro_cholesky(sub)
+    else:
+        L, rc = O.micro_cholesky(sub)
+    t_sub = time.perf_counter() - t0
+    t_factor = t_sub * (n / ns) ** 3
+    # one PCG iteration at full n: GEMV (n^2 FP32) + two triangular solves
+    F = np.asfortranarray(A.astype(np.float32))
+    lib = O.lib()
+    import ctypes
+    x = np.ascontiguousarray(b, dtype=np.float64)
+    y = np.zeros(n)
+    dp = ctypes.POINTER(ctypes.c_double)
+    t0 = time.perf_counter()
+    lib.orc_gemv_f32_f64(F.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), n, n,
+                         x.ctypes.data_as(dp), y.ctypes.data_as(dp))
+    lib.orc_potrs_f32_f64(F.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), n, n,
+                          x.ctypes.data_as(dp), y.ctypes.data_as(dp))
+    t_it = time.perf_counter() - t0
+    total_ms = (t_factor + (iters + 1) * t_it) * 1e3
+    return {"value": round(total_ms, 1), "unit": "ms", "cores": 1, "kind": kind,
+            "sample": (f"micro_cholesky on the leading {ns}x{ns} block ({t_sub:.2f} s) "
+                       f"extrapolated by (n/{ns})^3 to n={n}, plus {iters + 1} x one measured "
+                       f"FP64 PCG iteration at full n ({t_it * 1e3:.0f} ms)")}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return None
+    from cholesky_gpu_b200 import matgen
+    n = args.n
+    A = matgen.spd_matrix(n, args.kappa, 3).numpy()
+    b = matgen.rhs(n, 1, 100).numpy()
+    vals = []
+    for _ in range(max(1, args.steps)):
+        cb = cpu_baseline(args, A, b, iters=8)
+        vals.append(cb["value"])
+    v = statistics.median(vals)
+    cb["value"] = v
+    return {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "ms", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32 factor, fp64 pcg",
+        "data": "synthetic (seeded Q diag(sigma) Q^T, geometric spectrum)",
+        "config": {"workload": f"spd n={n} kappa={args.kappa:g} block={args.block} (CPU micro_cholesky)",
+                   "n": n, "kappa": args.kappa},
+        "cpu_baseline": cb,
+        "e2e": {"value": v, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_init(args)
+    if args.impl == "reference":
+        out = run_reference(args, world, rank)
+    else:
+        out = run_gpu(args, world, rank, local)
+    if out is not None:
+        print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

@@ -80,6 +80,19 @@ class Report(ctypes.Structure):
     ]
 
 
+NPHASES = 10
+PHASE_NAMES = ["potrf", "trsm", "quant", "syrk_f32", "syrk_tc", "symv", "trsv", "pcg_vec",
+               "setup", "test"]
+
+
+class Profile(ctypes.Structure):
+    _fields_ = [
+        ("ms", ctypes.c_double * NPHASES),
+        ("calls", ctypes.c_longlong * NPHASES),
+        ("launches", ctypes.c_longlong * NPHASES),
+    ]
+
+
 _vp = ctypes.c_void_p
 _i = ctypes.c_int
 _f = ctypes.c_float
@@ -93,6 +106,9 @@ SIGNATURES = {
     "mpchol_opts_default": (None, [ctypes.POINTER(Opts)]),
     "mpchol_pcg_opts_default": (None, [ctypes.POINTER(PcgOpts)]),
     "mpchol_last_error": (ctypes.c_char_p, []),
+    "mpchol_profile_enable": (None, [_i]),
+    "mpchol_profile_read": (_i, [ctypes.POINTER(Profile), _i]),
+    "mpchol_kernel_launches": (ctypes.c_longlong, []),
     "mpchol_factor_create": (_i, [ctypes.POINTER(Opts), _i, ctypes.POINTER(_vp)]),
     "mpchol_factor_compute": (_i, [_vp, _vp, _i, _vp]),
     "mpchol_factor": (_i, [ctypes.POINTER(Opts), _i, _vp, _i, ctypes.POINTER(_vp), _vp]),

@@ -32,6 +32,68 @@ void record_cuda_error(cudaError_t e, const char* what, const char* file, int li
 }
 }  // namespace mpchol
 
+// ---- per-phase profiling (the reference's cudaEvent phase timers,
+// src/hChol.cuh:22-31,112-117, src/sChol.cuh:150-154) and launch counting ----
+namespace {
+struct ProfRec {
+  int phase;
+  cudaEvent_t a, b;
+};
+struct Profiler {
+  std::mutex mu;
+  bool on = false;
+  std::vector<cudaEvent_t> pool;
+  size_t next = 0;
+  std::vector<ProfRec> recs;
+};
+Profiler g_prof;
+long long g_launches[MPCHOL_NPHASES] = {};
+std::mutex g_launch_mu;
+
+cudaEvent_t prof_event() {
+  if (g_prof.next >= g_prof.pool.size()) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    g_prof.pool.push_back(e);
+  }
+  return g_prof.pool[g_prof.next++];
+}
+
+struct PhaseScope {
+  int ph;
+  cudaStream_t s;
+  cudaEvent_t a = nullptr;
+  PhaseScope(int phase, cudaStream_t stream, int nkernels) : ph(phase), s(stream) {
+    {
+      std::lock_guard<std::mutex> lk(g_launch_mu);
+      g_launches[phase] += nkernels;
+    }
+    if (g_prof.on) {
+      std::lock_guard<std::mutex> lk(g_prof.mu);
+      a = prof_event();
+      if (a) cudaEventRecord(a, s);
+    }
+  }
+  ~PhaseScope() {
+    if (a) {
+      std::lock_guard<std::mutex> lk(g_prof.mu);
+      cudaEvent_t b = prof_event();
+      if (b) {
+        cudaEventRecord(b, s);
+        g_prof.recs.push_back({ph, a, b});
+      }
+    }
+  }
+};
+}  // namespace
+
+// Run `expr` (which launches `nk` library kernels) as phase `ph`.
+#define PHASE(ph, nk, stream, expr)                 \
+  do {                                              \
+    PhaseScope _scope((ph), (stream), (nk));        \
+    MPCHOL_CUDA_TRY(expr);                          \
+  } while (0)
+
 struct mpchol_factor {
   mpchol_opts opts;
   int n = 0, ld = 0, b = 0, nsteps = 0;
@@ -127,7 +189,7 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream) {
   MPCHOL_CUDA_TRY(cudaMemsetAsync(f->status, 0, sizeof(DevStatus), stream));
   MPCHOL_CUDA_TRY(cudaMemsetAsync(f->steps, 0, sizeof(StepState) * (f->nsteps + 1), stream));
   MPCHOL_CUDA_TRY(cudaMemsetAsync(f->sh, 0, sizeof(float) * n, stream));
-  MPCHOL_CUDA_TRY(launch_extract_diag(f->A, ld, n, f->d, f->dtilde, stream));
+  PHASE(MPCHOL_PH_SETUP, 1, stream, launch_extract_diag(f->A, ld, n, f->d, f->dtilde, stream));
   const bool fixed = o.precision != MPCHOL_PREC_SWITCHING;
   std::vector<int> tc_fmts;
   if (!fixed) {
@@ -140,30 +202,30 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream) {
     const int s = k * b;
     const int bs = std::min(b, n - s);
     const int m = n - s - bs;
-    MPCHOL_CUDA_TRY(launch_potrf(f->A, ld, s, bs, f->d, f->sh, pp, &f->steps[k].fp64_diag,
+    PHASE(MPCHOL_PH_POTRF, 1, stream, launch_potrf(f->A, ld, s, bs, f->d, f->sh, pp, &f->steps[k].fp64_diag,
                                  f->scratch64, f->winv, f->status, stream));
     if (m <= 0) break;
     const int next_bs = std::min(b, m);
-    MPCHOL_CUDA_TRY(launch_trsm_panel(f->A, ld, n, s, bs, f->winv, f->d, f->dtilde, f->rowsq,
+    PHASE(MPCHOL_PH_TRSM, 1, stream, launch_trsm_panel(f->A, ld, n, s, bs, f->winv, f->d, f->dtilde, f->rowsq,
                                       &f->steps[k], &f->steps[k + 1], next_bs, dp, f->status,
                                       stream));
     float* P = f->A + (size_t)s * ld + s + bs;
     float* C = f->A + (size_t)(s + bs) * ld + s + bs;
-    MPCHOL_CUDA_TRY(launch_quantize_panel(P, ld, m, bs, &f->steps[k], dp, f->q, bs, f->rowexp,
+    PHASE(MPCHOL_PH_QUANT, 1, stream, launch_quantize_panel(P, ld, m, bs, &f->steps[k], dp, f->q, bs, f->rowexp,
                                           f->mxexp, bs / 32, f->rowsq + s + bs,
                                           o.diag_pert ? f->sh + s + bs : nullptr, f->status,
                                           stream));
     if (fixed) {
       if (o.precision == FP32)
-        MPCHOL_CUDA_TRY(launch_syrk_f32(C, ld, m, bs, P, ld, nullptr, f->status, stream));
+        PHASE(MPCHOL_PH_SYRK_F32, 1, stream, launch_syrk_f32(C, ld, m, bs, P, ld, nullptr, f->status, stream));
       else
-        MPCHOL_CUDA_TRY(launch_syrk_tc(C, ld, m, bs, o.precision, f->q, bs, f->rowexp, f->mxexp,
+        PHASE(MPCHOL_PH_SYRK_TC, 1, stream, launch_syrk_tc(C, ld, m, bs, o.precision, f->q, bs, f->rowexp, f->mxexp,
                                        bs / 32, nullptr, f->status, stream));
     } else {
       const int* sel = &f->steps[k].prec;
-      MPCHOL_CUDA_TRY(launch_syrk_f32(C, ld, m, bs, P, ld, sel, f->status, stream));
+      PHASE(MPCHOL_PH_SYRK_F32, 1, stream, launch_syrk_f32(C, ld, m, bs, P, ld, sel, f->status, stream));
       for (int fmt : tc_fmts)
-        MPCHOL_CUDA_TRY(launch_syrk_tc(C, ld, m, bs, fmt, f->q, bs, f->rowexp, f->mxexp, bs / 32,
+        PHASE(MPCHOL_PH_SYRK_TC, 1, stream, launch_syrk_tc(C, ld, m, bs, fmt, f->q, bs, f->rowexp, f->mxexp, bs / 32,
                                        sel, f->status, stream));
     }
   }
@@ -173,7 +235,7 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream) {
 
 mpchol_status ensure_solve(mpchol_factor_t* f, cudaStream_t stream) {
   if (f->solve_ready) return MPCHOL_OK;
-  MPCHOL_CUDA_TRY(launch_diag_inverse(f->A, f->ld, f->n, f->linv, stream));
+  PHASE(MPCHOL_PH_SETUP, 1, stream, launch_diag_inverse(f->A, f->ld, f->n, f->linv, stream));
   f->solve_ready = true;
   return MPCHOL_OK;
 }
@@ -181,9 +243,9 @@ mpchol_status ensure_solve(mpchol_factor_t* f, cudaStream_t stream) {
 // z = M^-1 r for NR-padded vectors
 mpchol_status apply_precond(mpchol_factor_t* f, const double* r, double* tmp, double* z, int nr,
                             const int* skip, cudaStream_t stream) {
-  MPCHOL_CUDA_TRY(launch_trsv(false, f->A, f->ld, f->n, f->linv, r, tmp, nr, f->flags, ++f->epoch,
+  PHASE(MPCHOL_PH_TRSV, 1, stream, launch_trsv(false, f->A, f->ld, f->n, f->linv, r, tmp, nr, f->flags, ++f->epoch,
                               f->ticket, skip, f->status, stream));
-  MPCHOL_CUDA_TRY(launch_trsv(true, f->A, f->ld, f->n, f->linv, tmp, z, nr, f->flags, ++f->epoch,
+  PHASE(MPCHOL_PH_TRSV, 1, stream, launch_trsv(true, f->A, f->ld, f->n, f->linv, tmp, z, nr, f->flags, ++f->epoch,
                               f->ticket, skip, f->status, stream));
   return MPCHOL_OK;
 }
@@ -229,9 +291,9 @@ mpchol_status run_pcg(mpchol_factor_t* f, const TA* dA, int lda, const double* d
   if (ss != MPCHOL_OK) return ss;
   MPCHOL_CUDA_TRY(cudaMemsetAsync(f->status, 0, sizeof(DevStatus), stream));
   MPCHOL_CUDA_TRY(cudaMemsetAsync(f->done, 0, 2 * sizeof(int), stream));
-  MPCHOL_CUDA_TRY(launch_pad_columns(dB, n, nrhs, bb, nr, stream));
-  MPCHOL_CUDA_TRY(launch_dot(bb, bb, n, nr, part_misc, nullptr, stream));
-  MPCHOL_CUDA_TRY(launch_reduce_partials(part_misc, bnorm2, nr, stream));
+  PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_pad_columns(dB, n, nrhs, bb, nr, stream));
+  PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_dot(bb, bb, n, nr, part_misc, nullptr, stream));
+  PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_reduce_partials(part_misc, bnorm2, nr, stream));
   // x0
   if (po.x0_precond) {
     mpchol_status s0 = apply_precond(f, bb, tmp, x, nr, nullptr, stream);
@@ -243,11 +305,11 @@ mpchol_status run_pcg(mpchol_factor_t* f, const TA* dA, int lda, const double* d
   int it = 0;
   bool converged = false;
   const int max_restarts = 3;
-  for (int restart = 0; restart <= max_restarts; ++restart) {
+  for (int restart = 0;; ++restart) {
     // r = b - A x ; z = M^-1 r ; p = z ; rho = r^T z
-    MPCHOL_CUDA_TRY(launch_symv_skip<TA>(dA, lda, n, x, Ap, nr, nullptr, stream));
-    MPCHOL_CUDA_TRY(launch_residual(bb, Ap, r, n, nr, part_rr, stream));
-    MPCHOL_CUDA_TRY(launch_reduce_partials(part_rr, misc, nr, stream));
+    PHASE(MPCHOL_PH_SYMV, 1, stream, launch_symv_skip<TA>(dA, lda, n, x, Ap, nr, nullptr, stream));
+    PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_residual(bb, Ap, r, n, nr, part_rr, stream));
+    PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_reduce_partials(part_rr, misc, nr, stream));
     // convergence of the true residual
     MPCHOL_CUDA_TRY(cudaMemcpyAsync(f->h_scal, misc, sizeof(double) * 8, cudaMemcpyDeviceToHost, stream));
     MPCHOL_CUDA_TRY(cudaMemcpyAsync(f->h_scal + 8, bnorm2, sizeof(double) * 8, cudaMemcpyDeviceToHost, stream));
@@ -255,26 +317,26 @@ mpchol_status run_pcg(mpchol_factor_t* f, const TA* dA, int lda, const double* d
     converged = true;
     for (int k = 0; k < nrhs; ++k)
       if (!(f->h_scal[k] <= tol2 * f->h_scal[8 + k])) converged = false;
-    if (converged || it >= po.max_it) break;
+    if (converged || it >= po.max_it || restart > max_restarts) break;
     mpchol_status s1 = apply_precond(f, r, tmp, z, nr, nullptr, stream);
     if (s1 != MPCHOL_OK) return s1;
-    MPCHOL_CUDA_TRY(launch_copy(z, p, n, nr, stream));
-    MPCHOL_CUDA_TRY(launch_dot(r, z, n, nr, part_rz, nullptr, stream));
-    MPCHOL_CUDA_TRY(launch_reduce_partials(part_rz, rho[0], nr, stream));
+    PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_copy(z, p, n, nr, stream));
+    PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_dot(r, z, n, nr, part_rz, nullptr, stream));
+    PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_reduce_partials(part_rz, rho[0], nr, stream));
     MPCHOL_CUDA_TRY(cudaMemsetAsync(f->done, 0, sizeof(int), stream));
     int cur = 0;
     bool stop = false;
     while (it < po.max_it && !stop) {
       const int chunk = std::min(po.check_every, po.max_it - it);
       for (int c = 0; c < chunk; ++c) {
-        MPCHOL_CUDA_TRY(launch_symv_skip<TA>(dA, lda, n, p, Ap, nr, f->done, stream));
-        MPCHOL_CUDA_TRY(launch_dot(p, Ap, n, nr, part_pAp, f->done, stream));
-        MPCHOL_CUDA_TRY(launch_update_xr(x, r, p, Ap, n, nr, part_pAp, rho[cur], alpha, part_rr,
+        PHASE(MPCHOL_PH_SYMV, 1, stream, launch_symv_skip<TA>(dA, lda, n, p, Ap, nr, f->done, stream));
+        PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_dot(p, Ap, n, nr, part_pAp, f->done, stream));
+        PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_update_xr(x, r, p, Ap, n, nr, part_pAp, rho[cur], alpha, part_rr,
                                          f->done, f->status, stream));
         mpchol_status s2 = apply_precond(f, r, tmp, z, nr, f->done, stream);
         if (s2 != MPCHOL_OK) return s2;
-        MPCHOL_CUDA_TRY(launch_dot(r, z, n, nr, part_rz, f->done, stream));
-        MPCHOL_CUDA_TRY(launch_update_p(p, z, n, nr, part_rz, rho[cur], rho[cur ^ 1], part_rr,
+        PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_dot(r, z, n, nr, part_rz, f->done, stream));
+        PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_update_p(p, z, n, nr, part_rz, rho[cur], rho[cur ^ 1], part_rr,
                                         bnorm2, tol2, f->done, f->done, f->done + 1, stream));
         cur ^= 1;
       }
@@ -296,12 +358,12 @@ mpchol_status run_pcg(mpchol_factor_t* f, const TA* dA, int lda, const double* d
   MPCHOL_CUDA_TRY(cudaMemcpy2DAsync(dX, sizeof(double) * n, x, sizeof(double) * n,
                                     sizeof(double) * n, nrhs, cudaMemcpyDeviceToDevice, stream));
   if (rep != nullptr) {
-    MPCHOL_CUDA_TRY(launch_dot(x, x, n, nr, part_misc, nullptr, stream));
-    MPCHOL_CUDA_TRY(launch_reduce_partials(part_misc, misc + 8, nr, stream));
-    MPCHOL_CUDA_TRY(launch_frob_lower<TA>(dA, lda, n, part_misc, stream));
-    MPCHOL_CUDA_TRY(launch_reduce_partials(part_misc, misc + 16, 1, stream));
-    MPCHOL_CUDA_TRY(launch_dot(r, z, n, nr, part_rz, nullptr, stream));
-    MPCHOL_CUDA_TRY(launch_reduce_partials(part_rz, misc + 24, nr, stream));
+    PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_dot(x, x, n, nr, part_misc, nullptr, stream));
+    PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_reduce_partials(part_misc, misc + 8, nr, stream));
+    PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_frob_lower<TA>(dA, lda, n, part_misc, stream));
+    PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_reduce_partials(part_misc, misc + 16, 1, stream));
+    PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_dot(r, z, n, nr, part_rz, nullptr, stream));
+    PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_reduce_partials(part_rz, misc + 24, nr, stream));
     MPCHOL_CUDA_TRY(cudaMemcpyAsync(f->h_scal, misc, sizeof(double) * 32, cudaMemcpyDeviceToHost, stream));
     MPCHOL_CUDA_TRY(cudaMemcpyAsync(f->h_scal + 32, bnorm2, sizeof(double) * 8, cudaMemcpyDeviceToHost, stream));
     MPCHOL_CUDA_TRY(cudaStreamSynchronize(stream));
@@ -344,6 +406,40 @@ const char* mpchol_status_str(int s) {
     case MPCHOL_ERR_NOT_SUPPORTED: return "option combination not supported";
     default: return "unknown status";
   }
+}
+
+void mpchol_profile_enable(int on) {
+  std::lock_guard<std::mutex> lk(g_prof.mu);
+  g_prof.on = on != 0;
+}
+
+mpchol_status mpchol_profile_read(mpchol_profile* out, int reset) {
+  if (out == nullptr) return MPCHOL_ERR_BAD_ARG;
+  std::lock_guard<std::mutex> lk(g_prof.mu);
+  memset(out, 0, sizeof(*out));
+  for (const ProfRec& r : g_prof.recs) {
+    if (cudaEventSynchronize(r.b) != cudaSuccess) return MPCHOL_ERR_CUDA;
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, r.a, r.b) != cudaSuccess) return MPCHOL_ERR_CUDA;
+    out->ms[r.phase] += ms;
+    out->calls[r.phase] += 1;
+  }
+  {
+    std::lock_guard<std::mutex> lk2(g_launch_mu);
+    for (int i = 0; i < MPCHOL_NPHASES; ++i) out->launches[i] = g_launches[i];
+  }
+  if (reset) {
+    g_prof.recs.clear();
+    g_prof.next = 0;
+  }
+  return MPCHOL_OK;
+}
+
+long long mpchol_kernel_launches(void) {
+  std::lock_guard<std::mutex> lk(g_launch_mu);
+  long long t = 0;
+  for (int i = 0; i < MPCHOL_NPHASES; ++i) t += g_launches[i];
+  return t;
 }
 
 const char* mpchol_last_error(void) {
@@ -522,7 +618,7 @@ mpchol_status mpchol_apply_precond(mpchol_factor_t* f, const double* dR, double*
   double* tmp = f->vec + 6 * nv;
   double* zp = f->vec + 2 * nv;     // z slot
   MPCHOL_CUDA_TRY(cudaMemsetAsync(f->status, 0, sizeof(DevStatus), s));
-  MPCHOL_CUDA_TRY(launch_pad_columns(dR, f->n, nrhs, rp, nr, s));
+  PHASE(MPCHOL_PH_PCG_VEC, 1, s, launch_pad_columns(dR, f->n, nrhs, rp, nr, s));
   ss = apply_precond(f, rp, tmp, zp, nr, nullptr, s);
   if (ss != MPCHOL_OK) return ss;
   MPCHOL_CUDA_TRY(cudaMemcpy2DAsync(dZ, sizeof(double) * f->n, zp, sizeof(double) * f->n,
@@ -536,7 +632,7 @@ mpchol_status mpchol_symv(const float* dA, int lda, int n, const double* dX, dou
                           mpchol_stream_t stream) {
   if (dA == nullptr || dX == nullptr || dY == nullptr || n <= 0 || lda < n) return MPCHOL_ERR_BAD_ARG;
   if (nrhs != 1 && nrhs != 2 && nrhs != 4 && nrhs != 8) return MPCHOL_ERR_BAD_ARG;
-  MPCHOL_CUDA_TRY(launch_symv_skip<float>(dA, lda, n, dX, dY, nrhs, nullptr,
+  PHASE(MPCHOL_PH_SYMV, 1, reinterpret_cast<cudaStream_t>(stream), launch_symv_skip<float>(dA, lda, n, dX, dY, nrhs, nullptr,
                                           reinterpret_cast<cudaStream_t>(stream)));
   return MPCHOL_OK;
 }
@@ -616,7 +712,7 @@ mpchol_status mpchol_quantize(const float* dX, void* dQ, long long count, int fm
                               mpchol_stream_t stream) {
   if (count < 0 || (count > 0 && (dX == nullptr || dQ == nullptr))) return MPCHOL_ERR_BAD_ARG;
   if (fmt != FP16 && fmt != E4M3 && fmt != E5M2) return MPCHOL_ERR_BAD_ARG;
-  MPCHOL_CUDA_TRY(launch_quantize_elems(dX, dQ, count, fmt, reinterpret_cast<cudaStream_t>(stream)));
+  PHASE(MPCHOL_PH_TEST, 1, reinterpret_cast<cudaStream_t>(stream), launch_quantize_elems(dX, dQ, count, fmt, reinterpret_cast<cudaStream_t>(stream)));
   return MPCHOL_OK;
 }
 
@@ -627,10 +723,10 @@ mpchol_status mpchol_quantize_rows(const float* dP, int m, int k, int ldp, int f
   if (fmt != FP16 && fmt != E4M3 && fmt != E5M2 && fmt != MXFP8) return MPCHOL_ERR_BAD_ARG;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   if (fmt == MXFP8)
-    MPCHOL_CUDA_TRY(launch_quantize_rows(dP, ldp, m, k, fmt, dQ, k, nullptr,
+    PHASE(MPCHOL_PH_QUANT, 1, s, launch_quantize_rows(dP, ldp, m, k, fmt, dQ, k, nullptr,
                                          reinterpret_cast<uint8_t*>(dScale), k / 32, s));
   else
-    MPCHOL_CUDA_TRY(launch_quantize_rows(dP, ldp, m, k, fmt, dQ, k,
+    PHASE(MPCHOL_PH_QUANT, 1, s, launch_quantize_rows(dP, ldp, m, k, fmt, dQ, k,
                                          reinterpret_cast<int8_t*>(dScale), nullptr, 0, s));
   return MPCHOL_OK;
 }
@@ -640,7 +736,7 @@ mpchol_status mpchol_quantize_hash(unsigned long long first, unsigned long long 
                                    mpchol_stream_t stream) {
   if (dHash == nullptr || chunk == 0 || first + count > (1ull << 32)) return MPCHOL_ERR_BAD_ARG;
   if (fmt != FP16 && fmt != E4M3 && fmt != E5M2) return MPCHOL_ERR_BAD_ARG;
-  MPCHOL_CUDA_TRY(launch_quantize_hash(first, count, chunk, fmt, dHash,
+  PHASE(MPCHOL_PH_TEST, 1, reinterpret_cast<cudaStream_t>(stream), launch_quantize_hash(first, count, chunk, fmt, dHash,
                                        reinterpret_cast<cudaStream_t>(stream)));
   return MPCHOL_OK;
 }
@@ -652,12 +748,12 @@ mpchol_status mpchol_syrk_update(float* dC, int ldc, int m, int k, int fmt, cons
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   if (fmt == FP32) {
     if (dP == nullptr || ldp < m) return MPCHOL_ERR_BAD_ARG;
-    MPCHOL_CUDA_TRY(launch_syrk_f32(dC, ldc, m, k, dP, ldp, nullptr, nullptr, s));
+    PHASE(MPCHOL_PH_SYRK_F32, 1, s, launch_syrk_f32(dC, ldc, m, k, dP, ldp, nullptr, nullptr, s));
     return MPCHOL_OK;
   }
   if (!syrk_tc_supported(fmt, k)) return MPCHOL_ERR_NOT_SUPPORTED;
   if (dQ == nullptr || dScale == nullptr) return MPCHOL_ERR_BAD_ARG;
-  MPCHOL_CUDA_TRY(launch_syrk_tc(dC, ldc, m, k, fmt, dQ, k, reinterpret_cast<const int8_t*>(dScale),
+  PHASE(MPCHOL_PH_SYRK_TC, 1, s, launch_syrk_tc(dC, ldc, m, k, fmt, dQ, k, reinterpret_cast<const int8_t*>(dScale),
                                  nullptr, 0, nullptr, nullptr, s));
   return MPCHOL_OK;
 }

@@ -105,10 +105,39 @@ typedef struct {
 
 typedef struct mpchol_factor mpchol_factor_t;
 
+/* Phases of the per-phase event timers (mpchol_profile_*). */
+enum {
+  MPCHOL_PH_POTRF = 0,     /* diagonal-block Cholesky */
+  MPCHOL_PH_TRSM = 1,      /* panel solve + Schur-diagonal / switching statistics */
+  MPCHOL_PH_QUANT = 2,     /* precision decision + panel quantization */
+  MPCHOL_PH_SYRK_F32 = 3,  /* FP32 trailing update */
+  MPCHOL_PH_SYRK_TC = 4,   /* tensor-core trailing update */
+  MPCHOL_PH_SYMV = 5,      /* PCG operator A p */
+  MPCHOL_PH_TRSV = 6,      /* PCG preconditioner triangular solves */
+  MPCHOL_PH_PCG_VEC = 7,   /* PCG FP64 dots / updates */
+  MPCHOL_PH_SETUP = 8,     /* diagonal extraction, solve-side setup */
+  MPCHOL_PH_TEST = 9,      /* kernel-level test entry points */
+  MPCHOL_NPHASES = 10
+};
+
+typedef struct {
+  double ms[MPCHOL_NPHASES];          /* summed event time per phase */
+  long long calls[MPCHOL_NPHASES];    /* timed calls per phase */
+  long long launches[MPCHOL_NPHASES]; /* kernels launched per phase since load (all calls) */
+} mpchol_profile;
+
 /* ---- status / defaults ------------------------------------------------- */
 MPCHOL_API const char* mpchol_status_str(int status);
 MPCHOL_API void mpchol_opts_default(mpchol_opts* opts);
 MPCHOL_API void mpchol_pcg_opts_default(mpchol_pcg_opts* opts);
+/* Per-phase CUDA-event timers (the reference's phase timers,
+ * src/hChol.cuh:22-31, src/sChol.cuh:150-154).  While enabled, every kernel
+ * group the library launches is bracketed by events on its stream;
+ * mpchol_profile_read waits for those events and sums them per phase. */
+MPCHOL_API void mpchol_profile_enable(int on);
+MPCHOL_API mpchol_status mpchol_profile_read(mpchol_profile* out, int reset);
+/* Total number of kernels the library has launched in this process. */
+MPCHOL_API long long mpchol_kernel_launches(void);
 /* Last CUDA error text recorded by the library in this process ("" if none). */
 MPCHOL_API const char* mpchol_last_error(void);
 
