@@ -456,7 +456,7 @@ void mpchol_opts_default(mpchol_opts* o) {
   o->precision = MPCHOL_PREC_SWITCHING;
   o->eps_prime = 0.5f;
   o->floor = 0.0f;
-  o->diag_pert = 0;
+  o->diag_pert = 1;
   o->pert = 1.0f;
   o->pivot_floor = 1e-7f;
   o->switch_mode = 0;

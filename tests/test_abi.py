@@ -43,7 +43,7 @@ def test_status_strings():
 
 def test_default_options():
     o = _lib.default_opts()
-    assert o.block_size == 256
+    assert o.block_size == 256 and o.diag_pert == 1
     assert o.precision == _lib.PREC_SWITCHING
     assert list(o.ladder)[: o.ladder_len] == [_lib.PREC_E4M3, _lib.PREC_FP16, _lib.PREC_FP32]
     p = _lib.default_pcg_opts()

@@ -28,7 +28,7 @@ def factor_parity(A: np.ndarray, **opts):
                          precision=O.SWITCHING, force_prec=info.step_prec,
                          force_fp64=info.step_fp64,
                          eps_prime=opts.get("eps_prime", 0.5), floor=opts.get("floor", 0.0),
-                         diag_pert=opts.get("diag_pert", 0), pert=opts.get("pert", 1.0),
+                         diag_pert=opts.get("diag_pert", 1), pert=opts.get("pert", 1.0),
                          pivot_floor=opts.get("pivot_floor", 1e-7))
     Lo = ref["L"]
     err = np.linalg.norm(Lg - Lo) / np.linalg.norm(Lo)
@@ -55,12 +55,15 @@ def test_factor_matches_oracle(cuda, n, b, prec):
 def test_switching_decisions_match_oracle_rule(cuda):
     n, b = 1536, 256
     A = matgen.spd_matrix(n, 1e6, 3).numpy()
-    f, info, ref, err = factor_parity(A, block_size=b, eps_prime=0.05)
-    assert info.status == 0
+    # rounding-error diagonal shifts on (without them FP16 steps make this
+    # kappa = 1e6 factor indefinite; the oracle breaks down the same way)
+    f, info, ref, err = factor_parity(A, block_size=b, eps_prime=0.05, diag_pert=1, pert=1.0)
+    assert info.status == 0 and info.n_perturbed == 0
     assert err < 1e-3
     # re-derive each step's choice from the oracle's own tracker on the GPU's
     # precision path: the rule must agree step by step
-    r2 = O.blocked_chol(A, block_size=b, precision=O.SWITCHING, eps_prime=0.05)
+    r2 = O.blocked_chol(A, block_size=b, precision=O.SWITCHING, eps_prime=0.05, diag_pert=1,
+                        pert=1.0)
     assert list(r2["step_prec"][:-1]) == list(info.step_prec[:-1])
     d, dt = f.diags()
     np.testing.assert_allclose(dt.cpu().numpy(), ref["dtilde"], rtol=1e-3, atol=1e-6)
@@ -69,7 +72,7 @@ def test_switching_decisions_match_oracle_rule(cuda):
 def test_not_spd_reports_failing_row(cuda):
     A = matgen.spd_matrix(512, 10.0, 4).numpy()
     A[300, 300] = -1.0
-    f = mp.factor(torch.from_numpy(A).cuda(), block_size=128, precision="fp32")
+    f = mp.factor(torch.from_numpy(A).cuda(), block_size=128, precision="fp32", diag_pert=0)
     info = f.info()
     assert info.status == _lib.ERR_NOT_SPD and info.fail_row == 300
 
