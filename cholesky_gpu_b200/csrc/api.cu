@@ -85,6 +85,27 @@ struct PhaseScope {
     }
   }
 };
+bool profiling_on() {
+  std::lock_guard<std::mutex> lk(g_prof.mu);
+  return g_prof.on;
+}
+void launch_counts(long long (&out)[MPCHOL_NPHASES]) {
+  std::lock_guard<std::mutex> lk(g_launch_mu);
+  for (int i = 0; i < MPCHOL_NPHASES; ++i) out[i] = g_launches[i];
+}
+void add_launch_counts(const long long* nk, long long times) {
+  std::lock_guard<std::mutex> lk(g_launch_mu);
+  for (int i = 0; i < MPCHOL_NPHASES; ++i) g_launches[i] += nk[i] * times;
+}
+
+// A captured pair of PCG iterations and what it was captured for.
+struct PcgGraph {
+  cudaGraphExec_t exec = nullptr;
+  const void* A = nullptr;
+  int lda = 0, nr = 0, elem = 0;
+  double tol2 = 0.0;
+  long long nk[MPCHOL_NPHASES] = {};
+};
 }  // namespace
 
 // Run `expr` (which launches `nk` library kernels) as phase `ph`.
@@ -111,18 +132,17 @@ struct mpchol_factor {
   StepState* steps = nullptr;
   DevStatus* status = nullptr;
   // solve side
-  float* linv = nullptr;      // 128x128 diagonal-block inverses
-  int* flags = nullptr;
-  int* ticket = nullptr;
-  int epoch = 0;
+  float* blkinv = nullptr;    // inverses of the 128-row diagonal blocks
+  float* wsup = nullptr;      // inverses of the 1024-row diagonal super-blocks
   bool solve_ready = false;
   // PCG workspace (sized for 8 rhs)
-  double* vec = nullptr;      // x, r, z, p, Ap, b, tmp : 7 * n * 8
+  double* vec = nullptr;      // x, r, z, p, Ap, b, tmp, work : 8 * n * 8
   double* partials = nullptr; // 4 * VG * 8
   double* scal = nullptr;     // rho[2][8], alpha[8], bnorm2[8], misc
   int* done = nullptr;        // [0] converged flag, [1] iteration counter
   int* h_done = nullptr;      // pinned
   double* h_scal = nullptr;   // pinned
+  PcgGraph graph;             // captured iteration pair (see run_pcg)
 };
 
 namespace {
@@ -160,10 +180,11 @@ cudaError_t dmalloc(T** p, size_t count) {
 void free_factor(mpchol_factor_t* f) {
   if (f == nullptr) return;
   void* ptrs[] = {f->A, f->d, f->dtilde, f->rowsq, f->sh, f->winv, f->scratch64, f->q,
-                  f->rowexp, f->mxexp, f->steps, f->status, f->linv, f->flags, f->ticket,
+                  f->rowexp, f->mxexp, f->steps, f->status, f->blkinv, f->wsup,
                   f->vec, f->partials, f->scal, f->done};
   for (void* p : ptrs)
     if (p) cudaFree(p);
+  if (f->graph.exec) cudaGraphExecDestroy(f->graph.exec);
   if (f->h_done) cudaFreeHost(f->h_done);
   if (f->h_scal) cudaFreeHost(f->h_scal);
   delete f;
@@ -203,7 +224,7 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream) {
     const int bs = std::min(b, n - s);
     const int m = n - s - bs;
     PHASE(MPCHOL_PH_POTRF, 1, stream, launch_potrf(f->A, ld, s, bs, f->d, f->sh, pp, &f->steps[k].fp64_diag,
-                                 f->scratch64, f->winv, f->status, stream));
+                                 f->scratch64, f->winv, f->status, o.floor > 0.0f, stream));
     if (m <= 0) break;
     const int next_bs = std::min(b, m);
     PHASE(MPCHOL_PH_TRSM, 1, stream, launch_trsm_panel(f->A, ld, n, s, bs, f->winv, f->d, f->dtilde, f->rowsq,
@@ -235,18 +256,26 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream) {
 
 mpchol_status ensure_solve(mpchol_factor_t* f, cudaStream_t stream) {
   if (f->solve_ready) return MPCHOL_OK;
-  PHASE(MPCHOL_PH_SETUP, 1, stream, launch_diag_inverse(f->A, f->ld, f->n, f->linv, stream));
+  PHASE(MPCHOL_PH_SETUP, solve_setup_launches(f->n), stream,
+        launch_solve_setup(f->A, f->ld, f->n, f->blkinv, f->wsup, stream));
   f->solve_ready = true;
   return MPCHOL_OK;
 }
 
-// z = M^-1 r for NR-padded vectors
+int trsv_launch_count(int n) {
+  const int nbs = (n + solve_super_rows() - 1) / solve_super_rows();
+  return 2 + 2 * nbs - 1;
+}
+
+// z = M^-1 r for NR-padded vectors (tmp, work: n x nr scratch)
 mpchol_status apply_precond(mpchol_factor_t* f, const double* r, double* tmp, double* z, int nr,
                             const int* skip, cudaStream_t stream) {
-  PHASE(MPCHOL_PH_TRSV, 1, stream, launch_trsv(false, f->A, f->ld, f->n, f->linv, r, tmp, nr, f->flags, ++f->epoch,
-                              f->ticket, skip, f->status, stream));
-  PHASE(MPCHOL_PH_TRSV, 1, stream, launch_trsv(true, f->A, f->ld, f->n, f->linv, tmp, z, nr, f->flags, ++f->epoch,
-                              f->ticket, skip, f->status, stream));
+  double* work = f->vec + 7 * (size_t)f->n * 8;
+  const int nk = trsv_launch_count(f->n);
+  PHASE(MPCHOL_PH_TRSV, nk, stream,
+        launch_trsv_super(false, f->A, f->ld, f->n, f->wsup, r, tmp, work, nr, skip, stream, nullptr));
+  PHASE(MPCHOL_PH_TRSV, nk, stream,
+        launch_trsv_super(true, f->A, f->ld, f->n, f->wsup, tmp, z, work, nr, skip, stream, nullptr));
   return MPCHOL_OK;
 }
 
@@ -302,7 +331,8 @@ mpchol_status run_pcg(mpchol_factor_t* f, const TA* dA, int lda, const double* d
     MPCHOL_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(double) * (size_t)n * nr, stream));
   }
   const double tol2 = po.rel_tol * po.rel_tol;
-  int it = 0;
+  int it = 0;         // iterations executed on the device
+  int launched = 0;   // iterations enqueued (later ones return at once after convergence)
   bool converged = false;
   const int max_restarts = 3;
   for (int restart = 0;; ++restart) {
@@ -317,29 +347,78 @@ mpchol_status run_pcg(mpchol_factor_t* f, const TA* dA, int lda, const double* d
     converged = true;
     for (int k = 0; k < nrhs; ++k)
       if (!(f->h_scal[k] <= tol2 * f->h_scal[8 + k])) converged = false;
-    if (converged || it >= po.max_it || restart > max_restarts) break;
+    if (converged || launched >= po.max_it || restart > max_restarts) break;
     mpchol_status s1 = apply_precond(f, r, tmp, z, nr, nullptr, stream);
     if (s1 != MPCHOL_OK) return s1;
     PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_copy(z, p, n, nr, stream));
     PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_dot(r, z, n, nr, part_rz, nullptr, stream));
     PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_reduce_partials(part_rz, rho[0], nr, stream));
     MPCHOL_CUDA_TRY(cudaMemsetAsync(f->done, 0, sizeof(int), stream));
+    // One PCG iteration; rho[cur] is the current r^T z, rho[cur^1] receives
+    // the next one.  Every kernel returns at once after *done is set.
+    auto iteration = [&](int cur) -> mpchol_status {
+      PHASE(MPCHOL_PH_SYMV, 2, stream, launch_symv_skip<TA>(dA, lda, n, p, Ap, nr, f->done, stream));
+      PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_dot(p, Ap, n, nr, part_pAp, f->done, stream));
+      PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_update_xr(x, r, p, Ap, n, nr, part_pAp, rho[cur], alpha, part_rr,
+                                       f->done, f->status, stream));
+      mpchol_status s2 = apply_precond(f, r, tmp, z, nr, f->done, stream);
+      if (s2 != MPCHOL_OK) return s2;
+      PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_dot(r, z, n, nr, part_rz, f->done, stream));
+      PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_update_p(p, z, n, nr, part_rz, rho[cur], rho[cur ^ 1], part_rr,
+                                      bnorm2, tol2, f->done, f->done, f->done + 1, stream));
+      return MPCHOL_OK;
+    };
+    // Iteration pairs (which return the rho buffers to their starting roles)
+    // run as one CUDA graph, captured once per operator / rhs-count / tolerance.
+    const bool use_graph = !profiling_on();
+    if (use_graph) {
+      PcgGraph& g = f->graph;
+      if (g.exec == nullptr || g.A != (const void*)dA || g.lda != lda || g.nr != nr ||
+          g.elem != (int)sizeof(TA) || g.tol2 != tol2) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        g.exec = nullptr;
+        long long before[MPCHOL_NPHASES];
+        launch_counts(before);
+        cudaGraph_t graph = nullptr;
+        MPCHOL_CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        mpchol_status s0 = iteration(0);
+        if (s0 == MPCHOL_OK) s0 = iteration(1);
+        cudaError_t ce = cudaStreamEndCapture(stream, &graph);
+        if (s0 != MPCHOL_OK) return s0;
+        MPCHOL_CUDA_TRY(ce);
+        long long after[MPCHOL_NPHASES];
+        launch_counts(after);
+        for (int i = 0; i < MPCHOL_NPHASES; ++i) g.nk[i] = after[i] - before[i];
+        add_launch_counts(g.nk, -1);   // nothing ran during capture
+        ce = cudaGraphInstantiate(&g.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        MPCHOL_CUDA_TRY(ce);
+        g.A = dA; g.lda = lda; g.nr = nr; g.elem = (int)sizeof(TA); g.tol2 = tol2;
+      }
+    }
     int cur = 0;
     bool stop = false;
-    while (it < po.max_it && !stop) {
-      const int chunk = std::min(po.check_every, po.max_it - it);
-      for (int c = 0; c < chunk; ++c) {
-        PHASE(MPCHOL_PH_SYMV, 1, stream, launch_symv_skip<TA>(dA, lda, n, p, Ap, nr, f->done, stream));
-        PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_dot(p, Ap, n, nr, part_pAp, f->done, stream));
-        PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_update_xr(x, r, p, Ap, n, nr, part_pAp, rho[cur], alpha, part_rr,
-                                         f->done, f->status, stream));
-        mpchol_status s2 = apply_precond(f, r, tmp, z, nr, f->done, stream);
-        if (s2 != MPCHOL_OK) return s2;
-        PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_dot(r, z, n, nr, part_rz, f->done, stream));
-        PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_update_p(p, z, n, nr, part_rz, rho[cur], rho[cur ^ 1], part_rr,
-                                        bnorm2, tol2, f->done, f->done, f->done + 1, stream));
+    while (launched < po.max_it && !stop) {
+      const int chunk = std::min(po.check_every, po.max_it - launched);
+      int c = 0;
+      if (use_graph) {
+        if (cur == 1 && c < chunk) {
+          mpchol_status s3 = iteration(cur);
+          if (s3 != MPCHOL_OK) return s3;
+          cur ^= 1;
+          ++c;
+        }
+        for (; chunk - c >= 2; c += 2) {
+          MPCHOL_CUDA_TRY(cudaGraphLaunch(f->graph.exec, stream));
+          add_launch_counts(f->graph.nk, 1);
+        }
+      }
+      for (; c < chunk; ++c) {
+        mpchol_status s3 = iteration(cur);
+        if (s3 != MPCHOL_OK) return s3;
         cur ^= 1;
       }
+      launched += chunk;
       MPCHOL_CUDA_TRY(cudaMemcpyAsync(f->h_done, f->done, 2 * sizeof(int), cudaMemcpyDeviceToHost, stream));
       DevStatus st;
       MPCHOL_CUDA_TRY(cudaMemcpyAsync(&st, f->status, sizeof(DevStatus), cudaMemcpyDeviceToHost, stream));
@@ -489,7 +568,6 @@ mpchol_status mpchol_factor_create(const mpchol_opts* opts, int n, mpchol_factor
   f->nsteps = (n + f->b - 1) / f->b;
   cudaGetDevice(&f->device);
   const size_t nv = (size_t)n * 8;
-  const int NB128 = (n + 127) / 128;
   bool ok = dmalloc(&f->A, (size_t)f->ld * n) == cudaSuccess &&
             dmalloc(&f->d, n) == cudaSuccess && dmalloc(&f->dtilde, n) == cudaSuccess &&
             dmalloc(&f->rowsq, n) == cudaSuccess && dmalloc(&f->sh, n) == cudaSuccess &&
@@ -500,9 +578,9 @@ mpchol_status mpchol_factor_create(const mpchol_opts* opts, int n, mpchol_factor
             dmalloc(&f->mxexp, (size_t)n * (f->b / 32)) == cudaSuccess &&
             dmalloc(&f->steps, f->nsteps + 1) == cudaSuccess &&
             dmalloc(&f->status, 1) == cudaSuccess &&
-            dmalloc(&f->linv, (size_t)NB128 * 128 * 128) == cudaSuccess &&
-            dmalloc(&f->flags, NB128) == cudaSuccess && dmalloc(&f->ticket, 1) == cudaSuccess &&
-            dmalloc(&f->vec, 7 * nv) == cudaSuccess &&
+            dmalloc(&f->blkinv, solve_winv_elems(n)) == cudaSuccess &&
+            dmalloc(&f->wsup, solve_wsup_elems(n)) == cudaSuccess &&
+            dmalloc(&f->vec, 8 * nv) == cudaSuccess &&
             dmalloc(&f->partials, (size_t)4 * pcg_vgrid() * 8) == cudaSuccess &&
             dmalloc(&f->scal, 64) == cudaSuccess && dmalloc(&f->done, 2) == cudaSuccess &&
             cudaMallocHost(reinterpret_cast<void**>(&f->h_done), 2 * sizeof(int)) == cudaSuccess &&
@@ -512,7 +590,7 @@ mpchol_status mpchol_factor_create(const mpchol_opts* opts, int n, mpchol_factor
     free_factor(f);
     return MPCHOL_ERR_ALLOC;
   }
-  if (cudaMemset(f->flags, 0, sizeof(int) * NB128) != cudaSuccess) {
+  if (solve_init_attributes() != cudaSuccess) {
     free_factor(f);
     return MPCHOL_ERR_CUDA;
   }

@@ -34,7 +34,7 @@ size_t potrf_scratch64_elems(int bs);
 // to winv (ceil(bs/32) tiles, column-major 32x32 each) for the panel solve.
 cudaError_t launch_potrf(float* A, int lda, int s, int bs, const float* d, const float* sh,
                          const PotrfParams& p, const int* fp64_flag, double* scratch64,
-                         float* winv, DevStatus* st, cudaStream_t stream);
+                         float* winv, DevStatus* st, bool may_fp64, cudaStream_t stream);
 
 // ---- panel TRSM + fused diagonal tracker / decision statistics ----------
 // Solves X * L11^T = A21 in place for rows [s+bs, n) of block column s,

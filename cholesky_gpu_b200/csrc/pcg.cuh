@@ -7,13 +7,23 @@ namespace mpchol {
 int pcg_padded_nrhs(int nrhs);   // 1, 2, 4 or 8
 int pcg_vgrid();                 // CTAs of the reduction kernels (partials per vector)
 
+// ---- operator and preconditioner (solve.cu) ----
+cudaError_t solve_init_attributes();
+int solve_super_rows();
+size_t solve_wsup_elems(int n);
+size_t solve_winv_elems(int n);
+int solve_setup_launches(int n);
 template <typename TA>
 cudaError_t launch_symv_skip(const TA* A, int lda, int n, const double* x, double* y, int nrhs,
                              const int* skip, cudaStream_t stream);
-cudaError_t launch_diag_inverse(const float* L, int ldl, int n, float* linv, cudaStream_t stream);
-cudaError_t launch_trsv(bool backward, const float* L, int ldl, int n, const float* linv,
-                        const double* rhs, double* out, int nrhs, int* flags, int epoch,
-                        int* ticket, const int* skip, DevStatus* st, cudaStream_t stream);
+// 128-block inverses into winv, then the super-block inverses into wsup.
+cudaError_t launch_solve_setup(const float* L, int ldl, int n, float* winv, float* wsup,
+                               cudaStream_t stream);
+// out = L^-1 in (forward) or L^-T in (backward); work is an n x nrhs scratch.
+// *launches receives the number of kernels launched.
+cudaError_t launch_trsv_super(bool backward, const float* L, int ldl, int n, const float* wsup,
+                              const double* in, double* out, double* work, int nrhs,
+                              const int* skip, cudaStream_t stream, int* launches);
 cudaError_t launch_dot(const double* a, const double* b, int n, int nrhs, double* partials,
                        const int* skip, cudaStream_t stream);
 cudaError_t launch_update_xr(double* x, double* r, const double* p, const double* Ap, int n,

@@ -201,14 +201,24 @@ __device__ void potrf_block(T* tiles, float* A, int lda, int s, int bs, const fl
   if (tid == 0 && s_pert) atomicAdd(&st->perturbed, s_pert);
 }
 
-__global__ void __launch_bounds__(512, 1)
-potrf_kernel(float* A, int lda, int s, int bs, const float* d, const float* sh, PotrfParams p,
-             const int* fp64_flag, double* scratch64, float* winv, DevStatus* st) {
+// FP32 blocks: tiles in shared memory.  Separate kernels for the two
+// precisions keep the FP64 register footprint out of the FP32 path.
+__global__ void __launch_bounds__(256, 1)
+potrf_f32_kernel(float* A, int lda, int s, int bs, const float* d, const float* sh, PotrfParams p,
+                 const int* fp64_flag, float* winv, DevStatus* st) {
   if (st->code != 0) return;
+  if (fp64_flag != nullptr && *fp64_flag != 0) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const bool use64 = fp64_flag != nullptr && *fp64_flag != 0;
-  if (use64) potrf_block<double>(scratch64, A, lda, s, bs, d, sh, p, winv, st);
-  else potrf_block<float>(reinterpret_cast<float*>(smem_raw), A, lda, s, bs, d, sh, p, winv, st);
+  potrf_block<float>(reinterpret_cast<float*>(smem_raw), A, lda, s, bs, d, sh, p, winv, st);
+}
+
+// FP64 blocks (flagged near-indefinite): tiles in a global scratch.
+__global__ void __launch_bounds__(256, 1)
+potrf_f64_kernel(float* A, int lda, int s, int bs, const float* d, const float* sh, PotrfParams p,
+                 const int* fp64_flag, double* scratch64, float* winv, DevStatus* st) {
+  if (st->code != 0) return;
+  if (fp64_flag == nullptr || *fp64_flag == 0) return;
+  potrf_block<double>(scratch64, A, lda, s, bs, d, sh, p, winv, st);
 }
 
 }  // namespace
@@ -224,12 +234,14 @@ size_t potrf_scratch64_elems(int bs) {
 
 cudaError_t launch_potrf(float* A, int lda, int s, int bs, const float* d, const float* sh,
                          const PotrfParams& p, const int* fp64_flag, double* scratch64,
-                         float* winv, DevStatus* st, cudaStream_t stream) {
+                         float* winv, DevStatus* st, bool may_fp64, cudaStream_t stream) {
   const size_t smem = potrf_smem_bytes(256);
-  cudaError_t e = cudaFuncSetAttribute(potrf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem);
+  cudaError_t e = cudaFuncSetAttribute(potrf_f32_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  potrf_kernel<<<1, 512, smem, stream>>>(A, lda, s, bs, d, sh, p, fp64_flag, scratch64, winv, st);
+  potrf_f32_kernel<<<1, 256, smem, stream>>>(A, lda, s, bs, d, sh, p, fp64_flag, winv, st);
+  if (may_fp64)
+    potrf_f64_kernel<<<1, 256, 0, stream>>>(A, lda, s, bs, d, sh, p, fp64_flag, scratch64, winv, st);
   return cudaGetLastError();
 }
 

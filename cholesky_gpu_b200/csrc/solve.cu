@@ -1,0 +1,503 @@
+// PCG operator and preconditioner: y = A x and z = (L L^T)^-1 r.
+//
+// Replaces the reference's per-iteration cublasDgemv on FP64 A
+// (src/mixed_cholesky.cu:185-191) and cusolverDnDpotrs on an FP64 copy of L
+// (src/mixed_cholesky.cu:141,204-206).  Both read the FP32 lower triangle once
+// per application, in 128 x 128 tiles, with FP64 vectors and accumulation.
+//
+// Triangular solves.  A row-by-row (or 128-block-by-block) substitution is a
+// chain of n/128 dependent steps and runs at a few GB/s on one B200.  Instead,
+// once per factor, the inverses W_S of the 1024-row diagonal super-blocks
+// L_SS are formed (FP32, from FP64 128-block inverses and FP32 GEMMs).  A
+// forward solve is then n/1024 steps of two fully parallel kernels:
+//     y_S  = W_S w_S                      (TRMV over the super-block's lower tiles)
+//     w_T -= L_TS y_S   for T > S         (GEMV over the panel below)
+// and the backward solve mirrors it with transposes.  The applied operator is
+// (Lt Lt^T)^-1 with Lt = blockdiag(W_S^-1) + strictly-block-lower(L), which is
+// symmetric positive definite whenever the W_S are nonsingular, so PCG stays
+// well defined; it equals (L L^T)^-1 up to the FP32 rounding of the W_S.
+// Partial sums are combined with FP64 atomics.
+#include "common.cuh"
+#include "pcg.cuh"
+
+namespace mpchol {
+namespace {
+
+constexpr int RB = 128;     // tile size
+constexpr int NTH = 256;    // 8 warps: warp w owns tile columns 16w..16w+15
+constexpr int RS = 1024;    // super-block rows
+
+template <typename TA>
+__device__ __forceinline__ void load4(const TA* p, int nvalid, float out[4]);
+template <>
+__device__ __forceinline__ void load4<float>(const float* p, int nvalid, float out[4]) {
+  if (nvalid >= 4 && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+    const float4 a = __ldg(reinterpret_cast<const float4*>(p));
+    out[0] = a.x; out[1] = a.y; out[2] = a.z; out[3] = a.w;
+  } else {
+#pragma unroll
+    for (int r = 0; r < 4; ++r) out[r] = (r < nvalid) ? __ldg(p + r) : 0.0f;
+  }
+}
+
+// Tile loaded into registers: lane covers rows 4*lane..4*lane+3, warp covers
+// CH consecutive columns starting at col0.  Elements outside (rows_valid,
+// cols_valid) are zero.  Every load of the batch is issued before any use.
+template <typename TA, int CH>
+struct TileRegs {
+  double v[CH][4];
+};
+
+template <int CH>
+__device__ __forceinline__ void load_cols(const float* T, int ld, int rloc, int rows_valid,
+                                          int col0, int cols_valid, double (&v)[CH][4]) {
+  float f[CH][4];
+  const int nv = min(4, rows_valid - rloc);
+#pragma unroll
+  for (int cc = 0; cc < CH; ++cc) {
+    const int c = col0 + cc;
+    if (c < cols_valid && nv > 0) load4<float>(T + (size_t)c * ld + rloc, nv, f[cc]);
+    else f[cc][0] = f[cc][1] = f[cc][2] = f[cc][3] = 0.0f;
+  }
+#pragma unroll
+  for (int cc = 0; cc < CH; ++cc)
+#pragma unroll
+    for (int r = 0; r < 4; ++r) v[cc][r] = f[cc][r];
+}
+
+template <int CH>
+__device__ __forceinline__ void load_cols(const double* T, int ld, int rloc, int rows_valid,
+                                          int col0, int cols_valid, double (&v)[CH][4]) {
+  const int nv = min(4, rows_valid - rloc);
+#pragma unroll
+  for (int cc = 0; cc < CH; ++cc) {
+    const int c = col0 + cc;
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+      v[cc][r] = (c < cols_valid && r < nv) ? __ldg(T + (size_t)c * ld + rloc + r) : 0.0;
+  }
+}
+
+// Accumulate a 128 x 128 tile times a vector segment.
+//   NOTRANS: part[r][k] += T[r][c] * vin[c][k]   (per-thread rows, summed over the warp's columns)
+//   TRANS  : colsum[c][k] = sum_r T[r][c] * vin[r][k], reduced over the warp -> lane 0
+// `mask`: 0 none, 1 keep r >= c (lower incl. diagonal), 2 keep r > c.
+template <typename TA, int NR, int CH>
+__device__ __forceinline__ void tile_pass(const TA* T, int ld, int rows_valid, int cols_valid,
+                                          const double* vin_cols, const double* vin_rows,
+                                          double (&acc)[4][NR], double* colsum_smem, int mask_nt,
+                                          int mask_t, bool do_nt, bool do_t) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int rloc = 4 * lane;
+#pragma unroll 1
+  for (int cb = 0; cb < 16; cb += CH) {
+    double v[CH][4];
+    load_cols<CH>(T, ld, rloc, rows_valid, warp * 16 + cb, cols_valid, v);
+#pragma unroll
+    for (int cc = 0; cc < CH; ++cc) {
+      const int c = warp * 16 + cb + cc;
+      if (do_nt) {
+#pragma unroll
+        for (int k = 0; k < NR; ++k) {
+          const double xc = vin_cols[c * NR + k];
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            const bool keep = mask_nt == 0 || (mask_nt == 1 ? (rloc + r >= c) : (rloc + r > c));
+            if (keep) acc[r][k] = fma(v[cc][r], xc, acc[r][k]);
+          }
+        }
+      }
+      if (do_t) {
+#pragma unroll
+        for (int k = 0; k < NR; ++k) {
+          double s = 0.0;
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            const bool keep = mask_t == 0 || (mask_t == 1 ? (rloc + r >= c) : (rloc + r > c));
+            if (keep) s = fma(v[cc][r], vin_rows[(rloc + r) * NR + k], s);
+          }
+          s = warp_sum(s);
+          if (lane == 0) colsum_smem[c * NR + k] = s;
+        }
+      }
+    }
+  }
+}
+
+// Reduce the per-warp row partials of tile_pass(NOTRANS) and add sign * sum
+// into out[row0 + r] (rows < nvalid) with FP64 atomics.
+template <int NR>
+__device__ __forceinline__ void flush_rows(double (&acc)[4][NR], double* red, double* out, int n,
+                                           int row0, int nvalid, double sign) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int k = 0; k < NR; ++k) red[(warp * RB + 4 * lane + r) * NR + k] = acc[r][k];
+  __syncthreads();
+  for (int e = threadIdx.x; e < RB * NR; e += NTH) {
+    const int r = e / NR, k = e % NR;
+    if (r < nvalid) {
+      double s = 0.0;
+#pragma unroll
+      for (int w = 0; w < NTH / 32; ++w) s += red[(w * RB + r) * NR + k];
+      atomicAdd(&out[(size_t)k * n + row0 + r], sign * s);
+    }
+  }
+}
+
+template <int NR>
+__device__ __forceinline__ void load_vec(const double* x, int n, int row0, int nvalid, double* s) {
+  for (int e = threadIdx.x; e < RB * NR; e += NTH) {
+    const int r = e / NR, k = e % NR;
+    s[e] = (r < nvalid) ? x[(size_t)k * n + row0 + r] : 0.0;
+  }
+}
+
+__device__ __forceinline__ void tri_of(int t, int& i, int& j) {
+  int a = (int)((sqrtf(8.0f * t + 1.0f) - 1.0f) * 0.5f);
+  while (a * (a + 1) / 2 > t) --a;
+  while ((a + 1) * (a + 2) / 2 <= t) ++a;
+  i = a;
+  j = t - a * (a + 1) / 2;
+}
+
+template <typename TA> struct ChunkOf { static constexpr int value = 16; };
+template <> struct ChunkOf<double> { static constexpr int value = 8; };
+
+// ---- y += A x, symmetric A, lower triangle only (one CTA per lower tile) ----
+template <typename TA, int NR>
+__global__ void __launch_bounds__(NTH)
+symv_kernel(const TA* __restrict__ A, int lda, int n, const double* __restrict__ x,
+            double* __restrict__ y, const int* skip) {
+  if (skip != nullptr && *skip) return;
+  __shared__ double s_xJ[RB * NR];
+  __shared__ double s_xI[RB * NR];
+  __shared__ double s_col[RB * NR];
+  extern __shared__ double s_red[];
+  int I, J;
+  tri_of(blockIdx.x, I, J);
+  const int i0 = I * RB, j0 = J * RB;
+  const int ni = min(RB, n - i0), nj = min(RB, n - j0);
+  load_vec<NR>(x, n, j0, nj, s_xJ);
+  load_vec<NR>(x, n, i0, ni, s_xI);
+  __syncthreads();
+  double acc[4][NR] = {};
+  const bool diag = (I == J);
+  tile_pass<TA, NR, ChunkOf<TA>::value>(A + (size_t)j0 * lda + i0, lda, ni, nj, s_xJ, s_xI, acc,
+                                        s_col, diag ? 1 : 0, diag ? 2 : 0, true, true);
+  __syncthreads();
+  // column sums go to y_J
+  for (int e = threadIdx.x; e < RB * NR; e += NTH) {
+    const int c = e / NR, k = e % NR;
+    if (c < nj) atomicAdd(&y[(size_t)k * n + j0 + c], s_col[e]);
+  }
+  flush_rows<NR>(acc, s_red, y, n, i0, ni, 1.0);
+}
+
+// ---- setup: 128-block inverses (FP64 arithmetic, FP32 result) ------------
+// winv + I*RB*RB = inv(L_II), column-major, padded with identity past n.
+__global__ void __launch_bounds__(RB)
+block_inverse_kernel(const float* __restrict__ L, int ldl, int n, float* __restrict__ winv) {
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  double* W = reinterpret_cast<double*>(sm_raw);            // [RB][RB+1]
+  float* Ls = reinterpret_cast<float*>(W + RB * (RB + 1));  // [RB][RB+1]
+  const int I = blockIdx.x, c = threadIdx.x;
+  const int i0 = I * RB;
+  const int nb = min(RB, n - i0);
+  for (int e = c; e < RB * RB; e += RB) {
+    const int col = e / RB, row = e % RB;
+    float v;
+    if (row < nb && col < nb) v = L[(size_t)(i0 + col) * ldl + i0 + row];
+    else v = (row == col) ? 1.0f : 0.0f;
+    Ls[col * (RB + 1) + row] = v;
+  }
+  __syncthreads();
+  for (int i = 0; i < RB; ++i) {
+    double w = 0.0;
+    if (i >= c) {
+      double acc = (i == c) ? 1.0 : 0.0;
+      for (int k = c; k < i; ++k) acc -= (double)Ls[k * (RB + 1) + i] * W[c * (RB + 1) + k];
+      w = acc / (double)Ls[i * (RB + 1) + i];
+    }
+    W[c * (RB + 1) + i] = w;
+  }
+  __syncthreads();
+  float* out = winv + (size_t)I * RB * RB;
+  for (int e = c; e < RB * RB; e += RB) {
+    const int col = e / RB, row = e % RB;
+    out[e] = (float)W[col * (RB + 1) + row];
+  }
+}
+
+// Super-block inverse storage: for super-block S, an RS x RS column-major FP32
+// matrix at wsup + S*RS*RS (upper triangle zero).  Diagonal 128-tiles are the
+// 128-block inverses; everything else starts at zero.
+__global__ void superinv_init_kernel(const float* __restrict__ winv, float* __restrict__ wsup,
+                                     int nblk128) {
+  const int S = blockIdx.y;
+  float* W = wsup + (size_t)S * RS * RS;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)RS * RS;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int col = (int)(e / RS), row = (int)(e % RS);
+    const int ti = row / RB, tj = col / RB;
+    float v = 0.0f;
+    const int g = S * (RS / RB) + ti;
+    if (ti == tj && g < nblk128) v = winv[(size_t)g * RB * RB + (col % RB) * RB + (row % RB)];
+    else if (ti == tj && row == col) v = 1.0f;
+    W[e] = v;
+  }
+}
+
+// C(128x128) = A(128 x K) * B(K x 128), A and B column-major, FP32 FMA.
+// 256 threads, 8 x 8 outputs each (rows tx*4+{0..3}, 64+tx*4+{0..3}).
+__device__ void gemm128(const float* A, int lda, int a_rows_valid, const float* B, int ldb, int K,
+                        float (&acc)[8][8], float* As, float* Bs) {
+  const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
+  for (int k0 = 0; k0 < K; k0 += 8) {
+    for (int e = tid; e < 8 * RB; e += NTH) {
+      const int kk = e / RB, r = e % RB;
+      As[kk * RB + r] = (r < a_rows_valid) ? A[(size_t)(k0 + kk) * lda + r] : 0.0f;
+      const int c = e / 8, k = e % 8;
+      Bs[k * RB + c] = B[(size_t)c * ldb + k0 + k];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < 8; ++kk) {
+      const float4 a0 = *reinterpret_cast<const float4*>(&As[kk * RB + tx * 4]);
+      const float4 a1 = *reinterpret_cast<const float4*>(&As[kk * RB + 64 + tx * 4]);
+      const float4 b0 = *reinterpret_cast<const float4*>(&Bs[kk * RB + ty * 4]);
+      const float4 b1 = *reinterpret_cast<const float4*>(&Bs[kk * RB + 64 + ty * 4]);
+      const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+      const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+      for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int b = 0; b < 8; ++b) acc[a][b] = fmaf(av[a], bv[b], acc[a][b]);
+    }
+    __syncthreads();
+  }
+}
+
+__device__ __forceinline__ int acc_row(int a) { return a < 4 ? (threadIdx.x % 16) * 4 + a : 64 + (threadIdx.x % 16) * 4 + (a - 4); }
+__device__ __forceinline__ int acc_col(int b) { return b < 4 ? (threadIdx.x / 16) * 4 + b : 64 + (threadIdx.x / 16) * 4 + (b - 4); }
+
+// One level d of the super-block inverse: tile (i = j + d, j) of every
+// super-block:  W_ij = -W_ii * sum_{k=j}^{i-1} L_ik W_kj.
+__global__ void __launch_bounds__(NTH)
+superinv_level_kernel(const float* __restrict__ L, int ldl, int n, float* __restrict__ wsup, int d) {
+  __shared__ __align__(16) float As[8 * RB];
+  __shared__ __align__(16) float Bs[8 * RB];
+  const int S = blockIdx.y, j = blockIdx.x, i = j + d;
+  const int s0 = S * RS;
+  const int rs = min(RS, n - s0);
+  const int nsub = (rs + RB - 1) / RB;
+  if (i >= nsub) return;
+  float* W = wsup + (size_t)S * RS * RS;
+  const int rows_valid = min(RB, rs - i * RB);
+  float acc[8][8] = {};
+  // T = L(i-block rows, cols j..i-1 blocks) * W(rows j..i-1 blocks, cols j-block)
+  gemm128(L + (size_t)(s0 + j * RB) * ldl + s0 + i * RB, ldl, rows_valid,
+          W + (size_t)(j * RB) * RS + j * RB, RS, d * RB, acc, As, Bs);
+  float* Wij = W + (size_t)(j * RB) * RS + i * RB;
+#pragma unroll
+  for (int a = 0; a < 8; ++a)
+#pragma unroll
+    for (int b = 0; b < 8; ++b) Wij[(size_t)acc_col(b) * RS + acc_row(a)] = acc[a][b];
+  __syncthreads();
+  __threadfence_block();
+  float acc2[8][8] = {};
+  gemm128(W + (size_t)(i * RB) * RS + i * RB, RS, RB, Wij, RS, RB, acc2, As, Bs);
+  __syncthreads();
+#pragma unroll
+  for (int a = 0; a < 8; ++a)
+#pragma unroll
+    for (int b = 0; b < 8; ++b) Wij[(size_t)acc_col(b) * RS + acc_row(a)] = -acc2[a][b];
+}
+
+// ---- y_S += W_S w_S (TRANS: z_S += W_S^T w_S) over the super-block's lower tiles
+template <int NR, bool TRANS>
+__global__ void __launch_bounds__(NTH)
+trmv_super_kernel(const float* __restrict__ W, int n, int s0, int rs, const double* __restrict__ in,
+                  double* __restrict__ out, const int* skip) {
+  if (skip != nullptr && *skip) return;
+  __shared__ double s_v[RB * NR];
+  __shared__ double s_col[RB * NR];
+  extern __shared__ double s_red[];
+  int i, j;
+  tri_of(blockIdx.x, i, j);
+  const int ri0 = s0 + i * RB, rj0 = s0 + j * RB;
+  const int ni = min(RB, s0 + rs - ri0), nj = min(RB, s0 + rs - rj0);
+  if (!TRANS) load_vec<NR>(in, n, rj0, nj, s_v);
+  else load_vec<NR>(in, n, ri0, ni, s_v);
+  __syncthreads();
+  double acc[4][NR] = {};
+  const float* T = W + (size_t)(j * RB) * RS + i * RB;
+  tile_pass<float, NR, 16>(T, RS, ni, nj, s_v, s_v, acc, s_col, 0, 0, !TRANS, TRANS);
+  __syncthreads();
+  if (!TRANS) {
+    flush_rows<NR>(acc, s_red, out, n, ri0, ni, 1.0);
+  } else {
+    for (int e = threadIdx.x; e < RB * NR; e += NTH) {
+      const int c = e / NR, k = e % NR;
+      if (c < nj) atomicAdd(&out[(size_t)k * n + rj0 + c], s_col[e]);
+    }
+  }
+}
+
+// ---- panel updates ---------------------------------------------------------
+// forward: w[rows below the super-block] -= L(rows, super-block cols) y_S
+// backward: w[cols left of the super-block] -= L(super-block rows, cols)^T z_S
+template <int NR, bool TRANS>
+__global__ void __launch_bounds__(NTH)
+panel_kernel(const float* __restrict__ L, int ldl, int n, int s0, int rs,
+             const double* __restrict__ v, double* __restrict__ w, const int* skip) {
+  if (skip != nullptr && *skip) return;
+  __shared__ double s_v[RB * NR];
+  __shared__ double s_col[RB * NR];
+  extern __shared__ double s_red[];
+  int r0, c0, nr_, nc_;
+  if (!TRANS) {
+    r0 = s0 + rs + blockIdx.x * RB;  c0 = s0 + blockIdx.y * RB;
+    nr_ = min(RB, n - r0);           nc_ = min(RB, s0 + rs - c0);
+    load_vec<NR>(v, n, c0, nc_, s_v);
+  } else {
+    r0 = s0 + blockIdx.y * RB;       c0 = blockIdx.x * RB;
+    nr_ = min(RB, s0 + rs - r0);     nc_ = min(RB, s0 - c0);
+    load_vec<NR>(v, n, r0, nr_, s_v);
+  }
+  __syncthreads();
+  double acc[4][NR] = {};
+  tile_pass<float, NR, 16>(L + (size_t)c0 * ldl + r0, ldl, nr_, nc_, s_v, s_v, acc, s_col, 0, 0,
+                           !TRANS, TRANS);
+  __syncthreads();
+  if (!TRANS) {
+    flush_rows<NR>(acc, s_red, w, n, r0, nr_, -1.0);
+  } else {
+    for (int e = threadIdx.x; e < RB * NR; e += NTH) {
+      const int c = e / NR, k = e % NR;
+      if (c < nc_) atomicAdd(&w[(size_t)k * n + c0 + c], -s_col[e]);
+    }
+  }
+}
+
+template <int NR>
+__global__ void copy_vec_kernel(const double* __restrict__ a, double* __restrict__ b, long long count,
+                                const int* skip) {
+  if (skip != nullptr && *skip) return;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
+       i += (long long)gridDim.x * blockDim.x)
+    b[i] = a[i];
+}
+
+__global__ void zero_vec_kernel(double* __restrict__ a, long long count, const int* skip) {
+  if (skip != nullptr && *skip) return;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
+       i += (long long)gridDim.x * blockDim.x)
+    a[i] = 0.0;
+}
+
+size_t red_bytes(int nr) { return (size_t)(NTH / 32) * RB * nr * sizeof(double); }
+
+template <typename K>
+cudaError_t set_dyn(K kernel, size_t bytes) {
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+}  // namespace
+
+#define NR_SWITCH(nrhs, CALL)                                 \
+  switch (nrhs) {                                             \
+    case 1: { constexpr int NRC = 1; CALL; } break;           \
+    case 2: { constexpr int NRC = 2; CALL; } break;           \
+    case 4: { constexpr int NRC = 4; CALL; } break;           \
+    case 8: { constexpr int NRC = 8; CALL; } break;           \
+    default: return cudaErrorInvalidValue;                    \
+  }
+
+int solve_super_rows() { return RS; }
+size_t solve_wsup_elems(int n) {
+  const int nbs = (n + RS - 1) / RS;
+  return (size_t)nbs * RS * RS;
+}
+size_t solve_winv_elems(int n) { return (size_t)((n + RB - 1) / RB) * RB * RB; }
+
+cudaError_t solve_init_attributes() {
+  cudaError_t e;
+  const size_t inv = (size_t)RB * (RB + 1) * (sizeof(double) + sizeof(float));
+  if ((e = set_dyn(block_inverse_kernel, inv)) != cudaSuccess) return e;
+#define SET_NR(NRC)                                                                         \
+  if ((e = set_dyn(symv_kernel<float, NRC>, red_bytes(NRC))) != cudaSuccess) return e;      \
+  if ((e = set_dyn(symv_kernel<double, NRC>, red_bytes(NRC))) != cudaSuccess) return e;     \
+  if ((e = set_dyn(trmv_super_kernel<NRC, false>, red_bytes(NRC))) != cudaSuccess) return e; \
+  if ((e = set_dyn(trmv_super_kernel<NRC, true>, red_bytes(NRC))) != cudaSuccess) return e;  \
+  if ((e = set_dyn(panel_kernel<NRC, false>, red_bytes(NRC))) != cudaSuccess) return e;      \
+  if ((e = set_dyn(panel_kernel<NRC, true>, red_bytes(NRC))) != cudaSuccess) return e;
+  SET_NR(1) SET_NR(2) SET_NR(4) SET_NR(8)
+#undef SET_NR
+  return cudaSuccess;
+}
+
+template <typename TA>
+cudaError_t launch_symv_skip(const TA* A, int lda, int n, const double* x, double* y, int nrhs,
+                             const int* skip, cudaStream_t stream) {
+  const long long cnt = (long long)n * nrhs;
+  zero_vec_kernel<<<148, 256, 0, stream>>>(y, cnt, skip);
+  const int T = ceil_div(n, RB);
+  NR_SWITCH(nrhs, (symv_kernel<TA, NRC><<<T * (T + 1) / 2, NTH, red_bytes(NRC), stream>>>(A, lda, n, x, y, skip)));
+  return cudaGetLastError();
+}
+template cudaError_t launch_symv_skip<float>(const float*, int, int, const double*, double*, int, const int*, cudaStream_t);
+template cudaError_t launch_symv_skip<double>(const double*, int, int, const double*, double*, int, const int*, cudaStream_t);
+
+cudaError_t launch_solve_setup(const float* L, int ldl, int n, float* winv, float* wsup,
+                               cudaStream_t stream) {
+  const size_t inv = (size_t)RB * (RB + 1) * (sizeof(double) + sizeof(float));
+  const int nb = ceil_div(n, RB);
+  block_inverse_kernel<<<nb, RB, inv, stream>>>(L, ldl, n, winv);
+  const int nbs = ceil_div(n, RS);
+  superinv_init_kernel<<<dim3(256, nbs), 256, 0, stream>>>(winv, wsup, nb);
+  for (int d = 1; d < RS / RB; ++d)
+    superinv_level_kernel<<<dim3(RS / RB - d, nbs), NTH, 0, stream>>>(L, ldl, n, wsup, d);
+  return cudaGetLastError();
+}
+
+int solve_setup_launches(int n) { (void)n; return 2 + RS / RB - 1; }
+
+// out = L^-1 in (forward) or L^-T in (backward); work is an n x nrhs scratch.
+cudaError_t launch_trsv_super(bool backward, const float* L, int ldl, int n, const float* wsup,
+                              const double* in, double* out, double* work, int nrhs,
+                              const int* skip, cudaStream_t stream, int* launches) {
+  const long long cnt = (long long)n * nrhs;
+  copy_vec_kernel<1><<<148, 256, 0, stream>>>(in, work, cnt, skip);
+  zero_vec_kernel<<<148, 256, 0, stream>>>(out, cnt, skip);
+  int nl = 2;
+  const int nbs = ceil_div(n, RS);
+  for (int t = 0; t < nbs; ++t) {
+    const int S = backward ? nbs - 1 - t : t;
+    const int s0 = S * RS;
+    const int rs = min(RS, n - s0);
+    const int nsub = ceil_div(rs, RB);
+    const float* W = wsup + (size_t)S * RS * RS;
+    if (!backward) {
+      NR_SWITCH(nrhs, (trmv_super_kernel<NRC, false><<<nsub * (nsub + 1) / 2, NTH, red_bytes(NRC), stream>>>(W, n, s0, rs, work, out, skip)));
+      ++nl;
+      const int below = n - s0 - rs;
+      if (below > 0) {
+        NR_SWITCH(nrhs, (panel_kernel<NRC, false><<<dim3(ceil_div(below, RB), nsub), NTH, red_bytes(NRC), stream>>>(L, ldl, n, s0, rs, out, work, skip)));
+        ++nl;
+      }
+    } else {
+      NR_SWITCH(nrhs, (trmv_super_kernel<NRC, true><<<nsub * (nsub + 1) / 2, NTH, red_bytes(NRC), stream>>>(W, n, s0, rs, work, out, skip)));
+      ++nl;
+      if (s0 > 0) {
+        NR_SWITCH(nrhs, (panel_kernel<NRC, true><<<dim3(ceil_div(s0, RB), nsub), NTH, red_bytes(NRC), stream>>>(L, ldl, n, s0, rs, out, work, skip)));
+        ++nl;
+      }
+    }
+  }
+  if (launches) *launches = nl;
+  return cudaGetLastError();
+}
+
+}  // namespace mpchol

@@ -92,7 +92,17 @@ def test_apply_precond_matches_oracle_potrs(cuda):
     R = np.random.default_rng(0).standard_normal((n, 3))
     Z = f.apply_precond(torch.from_numpy(R).cuda()).cpu().numpy()
     want = O.potrs(L, R)
-    assert np.abs(Z - want).max() / np.abs(want).max() < 1e-9
+    # the solves apply FP32-rounded inverses of the 1024-row diagonal
+    # super-blocks (FP64 vectors and accumulation): agreement to ~1e-6
+    err = np.abs(Z - want).max() / np.abs(want).max()
+    print(f"apply_precond rel err {err:.2e}")
+    assert err < 1e-5
+    # and the applied operator is symmetric: u^T M^-1 v == v^T M^-1 u
+    u = np.random.default_rng(1).standard_normal(n)
+    v = np.random.default_rng(2).standard_normal(n)
+    Mu = f.apply_precond(torch.from_numpy(u).cuda()).cpu().numpy()
+    Mv = f.apply_precond(torch.from_numpy(v).cuda()).cpu().numpy()
+    assert abs(v @ Mu - u @ Mv) <= 1e-10 * abs(v @ Mu)
 
 
 @pytest.mark.parametrize("n,b,prec,kappa,nrhs", [
