@@ -143,6 +143,7 @@ struct mpchol_factor {
   int* h_done = nullptr;      // pinned
   double* h_scal = nullptr;   // pinned
   PcgGraph graph;             // captured iteration pair (see run_pcg)
+  cudaStream_t capture_stream = nullptr;   // private stream used only to capture graphs
 };
 
 namespace {
@@ -185,6 +186,7 @@ void free_factor(mpchol_factor_t* f) {
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (f->graph.exec) cudaGraphExecDestroy(f->graph.exec);
+  if (f->capture_stream) cudaStreamDestroy(f->capture_stream);
   if (f->h_done) cudaFreeHost(f->h_done);
   if (f->h_scal) cudaFreeHost(f->h_scal);
   delete f;
@@ -356,16 +358,16 @@ mpchol_status run_pcg(mpchol_factor_t* f, const TA* dA, int lda, const double* d
     MPCHOL_CUDA_TRY(cudaMemsetAsync(f->done, 0, sizeof(int), stream));
     // One PCG iteration; rho[cur] is the current r^T z, rho[cur^1] receives
     // the next one.  Every kernel returns at once after *done is set.
-    auto iteration = [&](int cur) -> mpchol_status {
-      PHASE(MPCHOL_PH_SYMV, 2, stream, launch_symv_skip<TA>(dA, lda, n, p, Ap, nr, f->done, stream));
-      PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_dot(p, Ap, n, nr, part_pAp, f->done, stream));
-      PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_update_xr(x, r, p, Ap, n, nr, part_pAp, rho[cur], alpha, part_rr,
-                                       f->done, f->status, stream));
-      mpchol_status s2 = apply_precond(f, r, tmp, z, nr, f->done, stream);
+    auto iteration = [&](int cur, cudaStream_t s) -> mpchol_status {
+      PHASE(MPCHOL_PH_SYMV, 2, s, launch_symv_skip<TA>(dA, lda, n, p, Ap, nr, f->done, s));
+      PHASE(MPCHOL_PH_PCG_VEC, 1, s, launch_dot(p, Ap, n, nr, part_pAp, f->done, s));
+      PHASE(MPCHOL_PH_PCG_VEC, 1, s, launch_update_xr(x, r, p, Ap, n, nr, part_pAp, rho[cur], alpha, part_rr,
+                                  f->done, f->status, s));
+      mpchol_status s2 = apply_precond(f, r, tmp, z, nr, f->done, s);
       if (s2 != MPCHOL_OK) return s2;
-      PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_dot(r, z, n, nr, part_rz, f->done, stream));
-      PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_update_p(p, z, n, nr, part_rz, rho[cur], rho[cur ^ 1], part_rr,
-                                      bnorm2, tol2, f->done, f->done, f->done + 1, stream));
+      PHASE(MPCHOL_PH_PCG_VEC, 1, s, launch_dot(r, z, n, nr, part_rz, f->done, s));
+      PHASE(MPCHOL_PH_PCG_VEC, 1, s, launch_update_p(p, z, n, nr, part_rz, rho[cur], rho[cur ^ 1], part_rr,
+                                 bnorm2, tol2, f->done, f->done, f->done + 1, s));
       return MPCHOL_OK;
     };
     // Iteration pairs (which return the rho buffers to their starting roles)
@@ -380,10 +382,15 @@ mpchol_status run_pcg(mpchol_factor_t* f, const TA* dA, int lda, const double* d
         long long before[MPCHOL_NPHASES];
         launch_counts(before);
         cudaGraph_t graph = nullptr;
-        MPCHOL_CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-        mpchol_status s0 = iteration(0);
-        if (s0 == MPCHOL_OK) s0 = iteration(1);
-        cudaError_t ce = cudaStreamEndCapture(stream, &graph);
+        // capture on a private stream (the caller's may be the legacy default
+        // stream, which cannot be captured); the graph is launched into the
+        // caller's stream
+        if (f->capture_stream == nullptr)
+          MPCHOL_CUDA_TRY(cudaStreamCreateWithFlags(&f->capture_stream, cudaStreamNonBlocking));
+        MPCHOL_CUDA_TRY(cudaStreamBeginCapture(f->capture_stream, cudaStreamCaptureModeThreadLocal));
+        mpchol_status s0 = iteration(0, f->capture_stream);
+        if (s0 == MPCHOL_OK) s0 = iteration(1, f->capture_stream);
+        cudaError_t ce = cudaStreamEndCapture(f->capture_stream, &graph);
         if (s0 != MPCHOL_OK) return s0;
         MPCHOL_CUDA_TRY(ce);
         long long after[MPCHOL_NPHASES];
@@ -403,7 +410,7 @@ mpchol_status run_pcg(mpchol_factor_t* f, const TA* dA, int lda, const double* d
       int c = 0;
       if (use_graph) {
         if (cur == 1 && c < chunk) {
-          mpchol_status s3 = iteration(cur);
+          mpchol_status s3 = iteration(cur, stream);
           if (s3 != MPCHOL_OK) return s3;
           cur ^= 1;
           ++c;
@@ -414,7 +421,7 @@ mpchol_status run_pcg(mpchol_factor_t* f, const TA* dA, int lda, const double* d
         }
       }
       for (; c < chunk; ++c) {
-        mpchol_status s3 = iteration(cur);
+        mpchol_status s3 = iteration(cur, stream);
         if (s3 != MPCHOL_OK) return s3;
         cur ^= 1;
       }
