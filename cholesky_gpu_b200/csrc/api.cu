@@ -717,6 +717,7 @@ mpchol_status mpchol_symv(const float* dA, int lda, int n, const double* dX, dou
                           mpchol_stream_t stream) {
   if (dA == nullptr || dX == nullptr || dY == nullptr || n <= 0 || lda < n) return MPCHOL_ERR_BAD_ARG;
   if (nrhs != 1 && nrhs != 2 && nrhs != 4 && nrhs != 8) return MPCHOL_ERR_BAD_ARG;
+  MPCHOL_CUDA_TRY(solve_init_attributes());
   PHASE(MPCHOL_PH_SYMV, 1, reinterpret_cast<cudaStream_t>(stream), launch_symv_skip<float>(dA, lda, n, dX, dY, nrhs, nullptr,
                                           reinterpret_cast<cudaStream_t>(stream)));
   return MPCHOL_OK;

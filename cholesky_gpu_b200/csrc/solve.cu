@@ -17,10 +17,13 @@
 // symmetric positive definite whenever the W_S are nonsingular, so PCG stays
 // well defined; it equals (L L^T)^-1 up to the FP32 rounding of the W_S.
 // Partial sums are combined with FP64 atomics.
+#include <mutex>
+
 #include "common.cuh"
 #include "pcg.cuh"
 
 namespace mpchol {
+cudaError_t solve_set_attributes();
 namespace {
 
 constexpr int RB = 128;     // tile size
@@ -423,6 +426,20 @@ size_t solve_wsup_elems(int n) {
 size_t solve_winv_elems(int n) { return (size_t)((n + RB - 1) / RB) * RB * RB; }
 
 cudaError_t solve_init_attributes() {
+  // once per device (kernel attributes are per device)
+  static std::mutex mu;
+  static bool done[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(mu);
+  if (dev >= 0 && dev < 64 && done[dev]) return cudaSuccess;
+  e = solve_set_attributes();
+  if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev] = true;
+  return e;
+}
+
+cudaError_t solve_set_attributes() {
   cudaError_t e;
   const size_t inv = (size_t)RB * (RB + 1) * (sizeof(double) + sizeof(float));
   if ((e = set_dyn(block_inverse_kernel, inv)) != cudaSuccess) return e;
