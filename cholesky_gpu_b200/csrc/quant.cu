@@ -41,6 +41,7 @@ __device__ void quantize_tile(const float* __restrict__ P, int ldp, int m, int k
   const int row0 = blockIdx.x * QROWS;
   const int nr = min(QROWS, m - row0);
   // stage the rows (coalesced column reads), padded stride QROWS+1
+#pragma unroll 8
   for (int e = tid; e < k * QROWS; e += QTHR) {
     const int c = e / QROWS, r = e % QROWS;
     tile[c * (QROWS + 1) + r] = (r < nr) ? P[(size_t)c * ldp + row0 + r] : 0.0f;

@@ -40,6 +40,7 @@ syrk_f32_kernel(float* __restrict__ C, int ldc, int m, int k, const float* __res
     for (int b = 0; b < 8; ++b) acc[a][b] = 0.0f;
 
   for (int k0 = 0; k0 < k; k0 += BK) {
+#pragma unroll
     for (int e = tid; e < BK * BM; e += NTH) {
       const int kk = e / BM, r = e % BM;
       const int kc = k0 + kk;

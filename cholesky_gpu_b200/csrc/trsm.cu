@@ -40,7 +40,8 @@ trsm_panel_kernel(float* __restrict__ A, int lda, int n, int s, int bs, const fl
   const int nrows = min(TR, n - row0);
   if (nrows <= 0) return;
 
-  // load the CTA's rows of the panel
+  // load the CTA's rows of the panel (unrolled: many loads in flight)
+#pragma unroll 8
   for (int e = tid; e < bs * TR; e += NTHR) {
     const int c = e / TR, r = e % TR;
     Xs[e] = (r < nrows) ? A[(size_t)(s + c) * lda + row0 + r] : 0.0f;
@@ -50,10 +51,12 @@ trsm_panel_kernel(float* __restrict__ A, int lda, int n, int s, int bs, const fl
   for (int J = 0; J < NT; ++J) {
     // tile-row J of L11 (columns 0..32J+31) and the inverse of L_JJ
     const int kend = 32 * J;
+#pragma unroll 8
     for (int e = tid; e < (kend + 32) * 32; e += NTHR) {
       const int k = e / 32, c = e % 32;
       Ls[k * LLD + c] = A[(size_t)(s + k) * lda + s + 32 * J + c];
     }
+#pragma unroll
     for (int e = tid; e < 32 * 32; e += NTHR) {
       const int m = e / 32, c = e % 32;                // winv column-major: (L^-1)[c][m] at m*32+c
       Ws[m * LLD + c] = winv[J * 1024 + m * 32 + c];
@@ -99,6 +102,7 @@ trsm_panel_kernel(float* __restrict__ A, int lda, int n, int s, int bs, const fl
     __syncthreads();
   }
   // write back the solved rows
+#pragma unroll 8
   for (int e = tid; e < bs * TR; e += NTHR) {
     const int c = e / TR, r = e % TR;
     if (r < nrows) A[(size_t)(s + c) * lda + row0 + r] = Xs[e];
