@@ -6,13 +6,15 @@
 // (src/kernels_macros.cuh:191-211).
 //
 // X * L11^T = A21 for the m rows below the diagonal block.  Rows are
-// independent, so one CTA owns 64 rows for the whole solve (kept in shared
-// memory) and walks the 32-column tiles J: X_J -= X_{<J} L_{J,<J}^T (a small
-// register-tiled GEMM), then X_J = X_J L_JJ^-T with the tile inverse computed
-// by the POTRF kernel.  The epilogue writes X back, folds each row's sum of
+// independent, so one CTA owns 64 rows for the whole solve.  Everything it
+// needs is staged into shared memory once, with all loads in flight: its rows
+// of the panel, the strictly-lower 32 x 32 tiles of L11 and the inverses of
+// L11's diagonal tiles (written by the POTRF kernel).  It then walks the
+// 32-column tiles J: X_J -= X_{<J} L_{J,<J}^T (register-tiled), then
+// X_J = X_J L_JJ^-T.  The epilogue writes X back, folds each row's sum of
 // squares into the Schur-diagonal tracker dtilde and reduces the switching
-// statistics for the step (max d/dtilde, reference-literal choice) and the
-// near-indefinite flag of the next diagonal block.
+// statistics (max d/dtilde, reference-literal choice) and the near-indefinite
+// flag of the next diagonal block.
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -21,7 +23,16 @@ namespace {
 
 constexpr int TR = 64;       // rows per CTA
 constexpr int NTHR = 256;
-constexpr int LLD = 33;      // padded stride of the L tile-row in smem
+constexpr int TLD = 33;      // padded stride of a 32 x 32 tile
+constexpr int TSZ = 32 * TLD;
+constexpr int XLD = TR;      // X staged column-major, rows contiguous
+
+__device__ __forceinline__ int tl(int I, int M) { return I * (I - 1) / 2 + M; }  // I > M
+
+size_t trsm_smem_floats(int bs) {
+  const int NT = bs / 32;
+  return (size_t)bs * XLD + (size_t)(NT * (NT - 1) / 2) * TSZ + (size_t)NT * TSZ;
+}
 
 __global__ void __launch_bounds__(NTHR)
 trsm_panel_kernel(float* __restrict__ A, int lda, int n, int s, int bs, const float* __restrict__ winv,
@@ -29,9 +40,10 @@ trsm_panel_kernel(float* __restrict__ A, int lda, int n, int s, int bs, const fl
                   StepState* step, StepState* next, int next_bs, DecisionParams dp, DevStatus* st) {
   if (st->code != 0) return;
   extern __shared__ __align__(16) float sm[];
-  float* Xs = sm;                          // [bs][TR], column-major in smem
-  float* Ls = Xs + (size_t)bs * TR;        // [bs][LLD] tile-row of L11 (k-major)
-  float* Ws = Ls + (size_t)bs * LLD;       // [32][LLD] inverse of the diagonal tile
+  const int NT = bs / 32;
+  float* Xs = sm;                                   // [bs][XLD]
+  float* Lt = Xs + (size_t)bs * XLD;                // strictly-lower tiles of L11
+  float* Wt = Lt + (size_t)(NT * (NT - 1) / 2) * TSZ;   // inverses of the diagonal tiles
   __shared__ float red_max[NTHR / 32];
   __shared__ int red_lit[NTHR / 32];
 
@@ -40,37 +52,43 @@ trsm_panel_kernel(float* __restrict__ A, int lda, int n, int s, int bs, const fl
   const int nrows = min(TR, n - row0);
   if (nrows <= 0) return;
 
-  // load the CTA's rows of the panel (unrolled: many loads in flight)
+  // ---- stage everything (independent loads, unrolled) -------------------
 #pragma unroll 8
   for (int e = tid; e < bs * TR; e += NTHR) {
     const int c = e / TR, r = e % TR;
-    Xs[e] = (r < nrows) ? A[(size_t)(s + c) * lda + row0 + r] : 0.0f;
+    Xs[c * XLD + r] = (r < nrows) ? A[(size_t)(s + c) * lda + row0 + r] : 0.0f;
   }
-  const int tr = tid % 16, tc = tid / 16;   // 4 rows x 2 cols per thread
-  const int NT = bs / 32;
-  for (int J = 0; J < NT; ++J) {
-    // tile-row J of L11 (columns 0..32J+31) and the inverse of L_JJ
-    const int kend = 32 * J;
+  const int nlt = NT * (NT - 1) / 2;
 #pragma unroll 8
-    for (int e = tid; e < (kend + 32) * 32; e += NTHR) {
-      const int k = e / 32, c = e % 32;
-      Ls[k * LLD + c] = A[(size_t)(s + k) * lda + s + 32 * J + c];
-    }
-#pragma unroll
-    for (int e = tid; e < 32 * 32; e += NTHR) {
-      const int m = e / 32, c = e % 32;                // winv column-major: (L^-1)[c][m] at m*32+c
-      Ws[m * LLD + c] = winv[J * 1024 + m * 32 + c];
-    }
-    __syncthreads();
-    // X_J -= X_{<J} L_{J,<J}^T
+  for (int e = tid; e < nlt * 1024; e += NTHR) {
+    const int t = e >> 10, rc = e & 1023;
+    const int c = rc >> 5, r = rc & 31;
+    int I = 1;
+    while (tl(I + 1, 0) <= t) ++I;
+    const int M = t - tl(I, 0);
+    Lt[t * TSZ + c * TLD + r] = A[(size_t)(s + 32 * M + c) * lda + s + 32 * I + r];
+  }
+#pragma unroll 8
+  for (int e = tid; e < NT * 1024; e += NTHR) {
+    const int J = e >> 10, mc = e & 1023;        // winv column-major: (L^-1)[c][m] at m*32+c
+    const int m = mc >> 5, c = mc & 31;
+    Wt[J * TSZ + m * TLD + c] = winv[e];
+  }
+  __syncthreads();
+
+  const int tr = tid % 16, tc = tid / 16;   // 4 rows x 2 cols per thread
+  for (int J = 0; J < NT; ++J) {
+    const int kend = 32 * J;
     float acc[4][2];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int j = 0; j < 2; ++j) acc[i][j] = Xs[(kend + 2 * tc + j) * TR + 4 * tr + i];
+      for (int j = 0; j < 2; ++j) acc[i][j] = Xs[(kend + 2 * tc + j) * XLD + 4 * tr + i];
+    // X_J -= X_{<J} L_{J,<J}^T
     for (int k = 0; k < kend; ++k) {
-      const float4 xv = *reinterpret_cast<const float4*>(&Xs[k * TR + 4 * tr]);
-      const float l0 = Ls[k * LLD + 2 * tc], l1 = Ls[k * LLD + 2 * tc + 1];
+      const float4 xv = *reinterpret_cast<const float4*>(&Xs[k * XLD + 4 * tr]);
+      const float* lp = Lt + tl(J, k >> 5) * TSZ + (k & 31) * TLD + 2 * tc;
+      const float l0 = lp[0], l1 = lp[1];
       acc[0][0] -= xv.x * l0; acc[0][1] -= xv.x * l1;
       acc[1][0] -= xv.y * l0; acc[1][1] -= xv.y * l1;
       acc[2][0] -= xv.z * l0; acc[2][1] -= xv.z * l1;
@@ -80,15 +98,15 @@ trsm_panel_kernel(float* __restrict__ A, int lda, int n, int s, int bs, const fl
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int j = 0; j < 2; ++j) Xs[(kend + 2 * tc + j) * TR + 4 * tr + i] = acc[i][j];
+      for (int j = 0; j < 2; ++j) Xs[(kend + 2 * tc + j) * XLD + 4 * tr + i] = acc[i][j];
     __syncthreads();
     // X_J = X_J * L_JJ^-T :  x[r][c] = sum_{m<=c} a[r][m] * (L^-1)[c][m]
-    float out[4][2];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) { out[i][0] = 0.0f; out[i][1] = 0.0f; }
+    float out[4][2] = {};
+    const float* W = Wt + J * TSZ;
+#pragma unroll 4
     for (int m = 0; m < 32; ++m) {
-      const float4 av = *reinterpret_cast<const float4*>(&Xs[(kend + m) * TR + 4 * tr]);
-      const float w0 = Ws[m * LLD + 2 * tc], w1 = Ws[m * LLD + 2 * tc + 1];
+      const float4 av = *reinterpret_cast<const float4*>(&Xs[(kend + m) * XLD + 4 * tr]);
+      const float w0 = W[m * TLD + 2 * tc], w1 = W[m * TLD + 2 * tc + 1];
       out[0][0] += av.x * w0; out[0][1] += av.x * w1;
       out[1][0] += av.y * w0; out[1][1] += av.y * w1;
       out[2][0] += av.z * w0; out[2][1] += av.z * w1;
@@ -98,22 +116,22 @@ trsm_panel_kernel(float* __restrict__ A, int lda, int n, int s, int bs, const fl
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int j = 0; j < 2; ++j) Xs[(kend + 2 * tc + j) * TR + 4 * tr + i] = out[i][j];
+      for (int j = 0; j < 2; ++j) Xs[(kend + 2 * tc + j) * XLD + 4 * tr + i] = out[i][j];
     __syncthreads();
   }
-  // write back the solved rows
+  // ---- write back the solved rows -----------------------------------------
 #pragma unroll 8
   for (int e = tid; e < bs * TR; e += NTHR) {
     const int c = e / TR, r = e % TR;
-    if (r < nrows) A[(size_t)(s + c) * lda + row0 + r] = Xs[e];
+    if (r < nrows) A[(size_t)(s + c) * lda + row0 + r] = Xs[c * XLD + r];
   }
-  // fused epilogue: Schur diagonal tracker and switching statistics
+  // ---- fused epilogue: Schur diagonal tracker and switching statistics --
   float ratio = 0.0f;
   int lit = 0;   // 2 - (reference-literal choice index); max over rows
   if (tid < nrows) {
     const int gi = row0 + tid;
     float sq = 0.0f;
-    for (int c = 0; c < bs; ++c) { const float v = Xs[c * TR + tid]; sq += v * v; }
+    for (int c = 0; c < bs; ++c) { const float v = Xs[c * XLD + tid]; sq += v * v; }
     rowsq[gi] = sq;
     const float dt = dtilde[gi] - sq;
     dtilde[gi] = dt;
@@ -126,7 +144,9 @@ trsm_panel_kernel(float* __restrict__ A, int lda, int n, int s, int bs, const fl
     for (int p = 0; p < 3; ++p)
       if (ref_eps[p] * dt >= dp.eps_prime * di) { pick = p; break; }
     lit = 2 - pick;
-    if (next != nullptr && gi - (s + bs) < next_bs && dt <= dp.floor_ratio * di) next->fp64_diag = 1;
+    if (next != nullptr && dp.floor_ratio > 0.0f && gi - (s + bs) < next_bs &&
+        dt <= dp.floor_ratio * di)
+      next->fp64_diag = 1;
   }
   float wm = warp_max(ratio);
   int wl = lit;
@@ -150,9 +170,10 @@ cudaError_t launch_trsm_panel(float* A, int lda, int n, int s, int bs, const flo
                               DevStatus* st, cudaStream_t stream) {
   const int m = n - s - bs;
   if (m <= 0) return cudaSuccess;
-  const size_t smem = ((size_t)bs * TR + (size_t)bs * LLD + 32 * LLD) * sizeof(float);
+  const size_t smem = trsm_smem_floats(bs) * sizeof(float);
   cudaError_t e = cudaFuncSetAttribute(trsm_panel_kernel,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)(trsm_smem_floats(256) * sizeof(float)));
   if (e != cudaSuccess) return e;
   trsm_panel_kernel<<<ceil_div(m, TR), NTHR, smem, stream>>>(A, lda, n, s, bs, winv, d, dtilde,
                                                              rowsq, step, next, next_bs, dp, st);

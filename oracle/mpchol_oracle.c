@@ -438,7 +438,7 @@ int orc_blocked_chol(float* A, int n, int lda, const float* d, float* dt, float*
     {
       const int nb = m < b ? m : b;
       for (int i = 0; i < nb; ++i)
-        if (dtt[i] <= o->floor_ratio * d[s + bs + i]) next_fp64 = 1;
+        if (o->floor_ratio > 0.0f && dtt[i] <= o->floor_ratio * d[s + bs + i]) next_fp64 = 1;
     }
     /* rounding-shift estimate: u_p * sum_j L_ij^2 for low-precision steps */
     if (sh && p != ORC_FP32) {

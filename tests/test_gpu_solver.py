@@ -68,7 +68,9 @@ def test_switching_decisions_match_oracle_rule(cuda):
                         pert=1.0)
     assert list(r2["step_prec"][:-1]) == list(info.step_prec[:-1])
     d, dt = f.diags()
-    np.testing.assert_allclose(dt.cpu().numpy(), ref["dtilde"], rtol=1e-3, atol=1e-6)
+    # dtilde = d - sum L^2 loses digits to cancellation when it is small
+    # (d ~ 1 here): compare with an absolute floor
+    np.testing.assert_allclose(dt.cpu().numpy(), ref["dtilde"], rtol=1e-3, atol=2e-5)
 
 
 def test_not_spd_reports_failing_row(cuda):
