@@ -17,6 +17,7 @@
 #include "common.cuh"
 #include "kernels.cuh"
 #include "pcg.cuh"
+#include "tmap.cuh"
 
 using namespace mpchol;
 
@@ -144,6 +145,8 @@ struct mpchol_factor {
   double* h_scal = nullptr;   // pinned
   PcgGraph graph;             // captured iteration pair (see run_pcg)
   cudaStream_t capture_stream = nullptr;   // private stream used only to capture graphs
+  CUtensorMap tmap32;         // TMA map over A, 32 x 32 boxes
+  CUtensorMap tmapX;          // TMA map over A, 64 x b boxes (panel slabs)
 };
 
 namespace {
@@ -225,13 +228,14 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream) {
     const int s = k * b;
     const int bs = std::min(b, n - s);
     const int m = n - s - bs;
-    PHASE(MPCHOL_PH_POTRF, 1, stream, launch_potrf(f->A, ld, s, bs, f->d, f->sh, pp, &f->steps[k].fp64_diag,
-                                 f->scratch64, f->winv, f->status, o.floor > 0.0f, stream));
+    PHASE(MPCHOL_PH_POTRF, o.floor > 0.0f ? 2 : 1, stream,
+          launch_potrf(f->tmap32, f->A, ld, n, s, bs, f->d, f->sh, pp, &f->steps[k].fp64_diag,
+                       f->scratch64, f->winv, f->status, o.floor > 0.0f, stream));
     if (m <= 0) break;
     const int next_bs = std::min(b, m);
-    PHASE(MPCHOL_PH_TRSM, 1, stream, launch_trsm_panel(f->A, ld, n, s, bs, f->winv, f->d, f->dtilde, f->rowsq,
-                                      &f->steps[k], &f->steps[k + 1], next_bs, dp, f->status,
-                                      stream));
+    PHASE(MPCHOL_PH_TRSM, 1, stream,
+          launch_trsm_panel(f->tmapX, f->tmap32, n, s, bs, f->winv, f->d, f->dtilde, f->rowsq,
+                            &f->steps[k], &f->steps[k + 1], next_bs, dp, f->status, stream));
     float* P = f->A + (size_t)s * ld + s + bs;
     float* C = f->A + (size_t)(s + bs) * ld + s + bs;
     PHASE(MPCHOL_PH_QUANT, 1, stream, launch_quantize_panel(P, ld, m, bs, &f->steps[k], dp, f->q, bs, f->rowexp,
@@ -598,6 +602,15 @@ mpchol_status mpchol_factor_create(const mpchol_opts* opts, int n, mpchol_factor
     return MPCHOL_ERR_ALLOC;
   }
   if (solve_init_attributes() != cudaSuccess) {
+    free_factor(f);
+    return MPCHOL_ERR_CUDA;
+  }
+  // TMA maps over the factor's own storage (rows past n read as zeros and are
+  // never written)
+  if (!encode_tmap_2d(&f->tmap32, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, f->A, n, n, f->ld, 32, 32,
+                      CU_TENSOR_MAP_SWIZZLE_NONE) ||
+      !encode_tmap_2d(&f->tmapX, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, f->A, n, n, f->ld, 64,
+                      f->b, CU_TENSOR_MAP_SWIZZLE_NONE)) {
     free_factor(f);
     return MPCHOL_ERR_CUDA;
   }

@@ -1,5 +1,7 @@
 // Internal launch interfaces of the mpchol kernels (not part of the C ABI).
 #pragma once
+#include <cuda.h>
+
 #include "common.cuh"
 
 namespace mpchol {
@@ -32,19 +34,22 @@ size_t potrf_smem_bytes(int bs);
 size_t potrf_scratch64_elems(int bs);
 // Also writes the inverses of the 32x32 diagonal tiles of the factored block
 // to winv (ceil(bs/32) tiles, column-major 32x32 each) for the panel solve.
-cudaError_t launch_potrf(float* A, int lda, int s, int bs, const float* d, const float* sh,
-                         const PotrfParams& p, const int* fp64_flag, double* scratch64,
-                         float* winv, DevStatus* st, bool may_fp64, cudaStream_t stream);
+// tmap32: TMA map over A (FP32, n x n, column stride lda) with 32 x 32 boxes.
+cudaError_t launch_potrf(const CUtensorMap& tmap32, float* A, int lda, int n, int s, int bs,
+                         const float* d, const float* sh, const PotrfParams& p,
+                         const int* fp64_flag, double* scratch64, float* winv, DevStatus* st,
+                         bool may_fp64, cudaStream_t stream);
 
 // ---- panel TRSM + fused diagonal tracker / decision statistics ----------
 // Solves X * L11^T = A21 in place for rows [s+bs, n) of block column s,
 // subtracts each row's sum of squares from dtilde, stores it in rowsq, and
 // folds the switching statistics of the rows into step (and the FP64 flag of
-// the next diagonal block into next).
-cudaError_t launch_trsm_panel(float* A, int lda, int n, int s, int bs, const float* winv,
-                              const float* d, float* dtilde, float* rowsq, StepState* step,
-                              StepState* next, int next_bs, const DecisionParams& dp,
-                              DevStatus* st, cudaStream_t stream);
+// the next diagonal block into next).  tmapX: TMA map over A with 64 x bs
+// boxes; tmap32 as for launch_potrf.
+cudaError_t launch_trsm_panel(const CUtensorMap& tmapX, const CUtensorMap& tmap32, int n, int s,
+                              int bs, const float* winv, const float* d, float* dtilde,
+                              float* rowsq, StepState* step, StepState* next, int next_bs,
+                              const DecisionParams& dp, DevStatus* st, cudaStream_t stream);
 
 // ---- decision + panel quantization --------------------------------------
 // Resolves the step precision (from the policy or the statistics in step),

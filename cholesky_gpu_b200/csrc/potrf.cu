@@ -3,26 +3,27 @@
 // Replaces the reference's per-step cusolverDnSpotrf of the b x b diagonal
 // block (src/switching_chol.cuh:86-95) and its CPU micro_cholesky variant
 // (src/micro_chol.hpp:14-44, src/sChol.cuh:66-79).  One CTA factors a block of
-// up to 256 x 256 as a blocked right-looking Cholesky on 32 x 32 tiles held in
-// shared memory: one warp factors the diagonal tile (lane i owns row i), warps
-// solve the tiles below it, warps update the trailing tiles.  Blocks flagged
-// near-indefinite by the switching criterion are factored in FP64 in a global
-// scratch (L2-resident) by a separate kernel.
-//
-// The per-tile routines are rolled loops over shared memory: the same few
-// hundred instructions run for every step, so they stay in the instruction
-// cache (fully unrolled 32 x 32 code runs once per tile and is bound by
-// instruction fetch).
+// up to 256 x 256 as a blocked right-looking Cholesky on dense 32 x 32 tiles in
+// shared memory (column-major, lane i of a warp always owns row i, so every
+// shared access is either contiguous across lanes or a broadcast):
+//   * the lower tiles are staged by TMA (one thread issues the 2-D copies,
+//     an mbarrier counts the bytes) and written back by TMA stores;
+//   * one warp factors each diagonal tile; its rank-1 updates are done in
+//     register batches (all loads of a step issued before its stores);
+//   * warps solve the tiles below and update the trailing tiles;
+//   * the inverses of the diagonal tiles are formed for the panel solve.
+// Blocks flagged near-indefinite by the switching criterion are factored in
+// FP64 by a second kernel on a global (L2-resident) scratch.
 #include "common.cuh"
 #include "kernels.cuh"
+#include "tc_ptx.cuh"
 
 namespace mpchol {
 
 namespace {
 
-constexpr int TS = 32;        // tile size
-constexpr int TLD = 33;       // padded tile column stride (bank-conflict free)
-constexpr int TSZ = TS * TLD; // elements per tile
+constexpr int TS = 32;          // tile size
+constexpr int TSZ = TS * TS;    // elements per dense tile
 
 __device__ __forceinline__ int tidx(int I, int J) { return I * (I + 1) / 2 + J; }
 
@@ -33,9 +34,9 @@ __device__ __forceinline__ float dsqrt<float>(float x) { return sqrtf(x); }
 template <>
 __device__ __forceinline__ double dsqrt<double>(double x) { return sqrt(x); }
 
-// Factor the 32 x 32 tile t in place (lower triangle); lane i owns row i.
-// inv[k] receives 1 / L(k,k).  Returns false on a non-positive pivot when
-// pivot flooring is off (first failing local row in *fail_row).
+// Factor the 32 x 32 tile t in place (lower triangle).  inv[k] receives
+// 1 / L(k,k).  Returns false on a non-positive pivot when pivot flooring is
+// off (first failing local row in *fail_row).
 template <typename T>
 __device__ bool factor_diag_tile(T* t, T* inv, int lane, int nreal, const T* shift, const T* pmin,
                                  int diag_pert, int* nperturbed, int* fail_row) {
@@ -43,7 +44,7 @@ __device__ bool factor_diag_tile(T* t, T* inv, int lane, int nreal, const T* shi
   int npert = 0;
 #pragma unroll 1
   for (int k = 0; k < TS; ++k) {
-    T piv = t[k * TLD + k];
+    T piv = t[k * TS + k];
     if (k < nreal) {
       piv += shift[k];
       if (diag_pert) {
@@ -58,14 +59,23 @@ __device__ bool factor_diag_tile(T* t, T* inv, int lane, int nreal, const T* shi
     }
     const T lkk = dsqrt<T>(piv);
     const T rk = T(1) / lkk;
+    const T lik = (lane > k) ? t[k * TS + lane] * rk : T(0);
+    // batch: row `lane`, columns k+1..31 -- all loads before any store
+    T v[TS - 1];
+    T l[TS - 1];
+#pragma unroll
+    for (int q = 0; q < TS - 1; ++q) {
+      const int j = k + 1 + q;
+      l[q] = __shfl_sync(0xffffffffu, lik, j & (TS - 1));
+      v[q] = (j < TS) ? t[j * TS + lane] : T(0);
+    }
     __syncwarp();
-    if (lane == k) { t[k * TLD + k] = lkk; inv[k] = rk; }
-    else if (lane > k) t[k * TLD + lane] *= rk;
-    __syncwarp();
-    if (lane > k) {
-      const T lik = t[k * TLD + lane];
-#pragma unroll 4
-      for (int j = k + 1; j <= lane; ++j) t[j * TLD + lane] -= lik * t[k * TLD + j];
+    if (lane == k) { t[k * TS + k] = lkk; inv[k] = rk; }
+    else if (lane > k) t[k * TS + lane] = lik;
+#pragma unroll
+    for (int q = 0; q < TS - 1; ++q) {
+      const int j = k + 1 + q;
+      if (j < TS && j <= lane) t[j * TS + lane] = v[q] - lik * l[q];
     }
     __syncwarp();
   }
@@ -76,55 +86,60 @@ __device__ bool factor_diag_tile(T* t, T* inv, int lane, int nreal, const T* shi
 // X L^T = B for one tile (B in x, overwritten); lane i owns row i.
 template <typename T>
 __device__ void trsm_tile(T* x, const T* l, const T* inv, int lane) {
-#pragma unroll 1
+  T b[TS];
+#pragma unroll
+  for (int m = 0; m < TS; ++m) b[m] = x[m * TS + lane];
+#pragma unroll
   for (int j = 0; j < TS; ++j) {
-    T acc = x[j * TLD + lane];
-#pragma unroll 4
-    for (int m = 0; m < j; ++m) acc -= x[m * TLD + lane] * l[m * TLD + j];
-    x[j * TLD + lane] = acc * inv[j];
+    T acc = b[j];
+#pragma unroll
+    for (int m = 0; m < j; ++m) acc -= b[m] * l[m * TS + j];
+    b[j] = acc * inv[j];
   }
+#pragma unroll
+  for (int m = 0; m < TS; ++m) x[m * TS + lane] = b[m];
 }
 
-// C -= A B^T for 32 x 32 tiles; lane c owns column c of C.
+// C -= A B^T for 32 x 32 tiles; lane i owns row i of C and of A.
 template <typename T>
 __device__ void syrk_tile(T* c, const T* a, const T* b, int lane) {
-  T acc[TS];
+  T ar[TS];
 #pragma unroll
-  for (int r = 0; r < TS; ++r) acc[r] = c[lane * TLD + r];
-#pragma unroll 2
-  for (int m = 0; m < TS; ++m) {
-    const T bv = b[m * TLD + lane];
+  for (int m = 0; m < TS; ++m) ar[m] = a[m * TS + lane];
+#pragma unroll 1
+  for (int c0 = 0; c0 < TS; c0 += 4) {
+    T acc[4];
 #pragma unroll
-    for (int r = 0; r < TS; ++r) acc[r] -= a[m * TLD + r] * bv;
+    for (int u = 0; u < 4; ++u) acc[u] = c[(c0 + u) * TS + lane];
+#pragma unroll
+    for (int m = 0; m < TS; ++m)
+#pragma unroll
+      for (int u = 0; u < 4; ++u) acc[u] -= ar[m] * b[m * TS + c0 + u];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) c[(c0 + u) * TS + lane] = acc[u];
   }
-#pragma unroll
-  for (int r = 0; r < TS; ++r) c[lane * TLD + r] = acc[r];
 }
 
-// Inverse of the lower-triangular tile l: lane c forms column c of L^-1 in the
-// scratch tile w (column-major, stride TLD) and stores it to out (32 x 32,
-// column-major, FP32).
+// Inverse of the lower-triangular tile l into out (32 x 32 column-major,
+// FP32).  Rows of W = L^-1 are formed in order (lane j owns column j);
+// w is a scratch tile holding W row-major.
 template <typename T>
 __device__ void invert_tile(const T* l, const T* inv, T* w, float* out, int lane) {
 #pragma unroll 1
   for (int i = 0; i < TS; ++i) {
-    T v = T(0);
-    if (i >= lane) {
-      T acc = (i == lane) ? T(1) : T(0);
-#pragma unroll 4
-      for (int k = lane; k < i; ++k) acc -= l[k * TLD + i] * w[lane * TLD + k];
-      v = acc * inv[i];
-    }
-    w[lane * TLD + i] = v;
+    T acc = (i == lane) ? T(1) : T(0);
+#pragma unroll 8
+    for (int k = 0; k < i; ++k) acc -= l[k * TS + i] * w[k * TS + lane];
+    const T v = (lane <= i) ? acc * inv[i] : T(0);
+    w[i * TS + lane] = v;
+    out[lane * TS + i] = (float)v;
   }
-  __syncwarp();
-#pragma unroll 1
-  for (int i = 0; i < TS; ++i) out[i * TS + lane] = (float)w[i * TLD + lane];
 }
 
-template <typename T>
-__device__ void potrf_block(T* tiles, float* A, int lda, int s, int bs, const float* d,
-                            const float* sh, const PotrfParams& p, float* winv, DevStatus* st) {
+template <typename T, bool TMA>
+__device__ void potrf_block(const CUtensorMap* tmap, T* tiles, float* A, int lda, int n, int s,
+                            int bs, const float* d, const float* sh, const PotrfParams& p,
+                            float* winv, DevStatus* st) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
   const int NT = (bs + TS - 1) / TS;
   const int ntiles = NT * (NT + 1) / 2;
@@ -132,8 +147,9 @@ __device__ void potrf_block(T* tiles, float* A, int lda, int s, int bs, const fl
   __shared__ T s_shift[256];
   __shared__ T s_pmin[256];
   __shared__ T s_inv[256];
-  __shared__ int s_fail, s_pert;
-  if (tid == 0) { s_fail = -1; s_pert = 0; }
+  __shared__ int s_fail, s_pert, s_ok;
+  __shared__ __align__(8) uint64_t bar;
+  if (tid == 0) { s_fail = -1; s_pert = 0; s_ok = 1; }
   for (int i = tid; i < NT * TS; i += blockDim.x) {
     T shv = T(0), pm = T(0);
     if (i < bs) {
@@ -143,16 +159,51 @@ __device__ void potrf_block(T* tiles, float* A, int lda, int s, int bs, const fl
     s_shift[i] = shv;
     s_pmin[i] = pm;
   }
-  // load the lower tiles column by column (coalesced); padding is identity
-  for (int c = warp; c < NT * TS; c += nwarps) {
-    const int J = c / TS, cc = c % TS;
-#pragma unroll 8
-    for (int r = J * TS + lane; r < NT * TS; r += TS) {
-      const int I = r / TS, rr = r % TS;
-      T v;
-      if (r < bs && c < bs) v = T(A[(size_t)(s + c) * lda + (s + r)]);
-      else v = (r == c) ? T(1) : T(0);
-      tiles[tidx(I, J) * TSZ + cc * TLD + rr] = v;
+  if (TMA) {
+    // stage the lower tiles with TMA; rows/columns past n arrive as zeros
+    if (tid == 0) {
+      tc::mbar_init(&bar, 1);
+      tc::fence_mbar_init();
+      tc::mbar_expect_tx(&bar, (uint32_t)(ntiles * TSZ * sizeof(float)));
+      for (int I = 0; I < NT; ++I)
+        for (int J = 0; J <= I; ++J)
+          tc::tma_load_2d(tiles + tidx(I, J) * TSZ, tmap, &bar, s + I * TS, s + J * TS);
+      if (!tc::mbar_wait(&bar, 0)) {
+        s_ok = 0;
+        set_status(st, MPCHOL_ERR_TIMEOUT, s);
+        tc::mbar_wait(&bar, 0);
+      }
+    }
+    __syncthreads();
+    if (!s_ok) return;
+    // identity padding past the block (only the last block can be partial)
+    for (int i = bs + tid; i < NT * TS; i += blockDim.x)
+      tiles[tidx(i / TS, i / TS) * TSZ + (i % TS) * TS + (i % TS)] = T(1);
+  } else {
+    // FP64 path: batched loads from the FP32 matrix
+    const int total = NT * NT * TSZ;
+    for (int base = 0; base < total; base += 8 * blockDim.x) {
+      float v[8];
+      int dst[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int e = base + q * blockDim.x + tid;
+        dst[q] = -1;
+        v[q] = 0.0f;
+        if (e < total) {
+          const int T2 = e / TSZ, rc = e % TSZ;
+          const int I = T2 % NT, J = T2 / NT, c = rc / TS, r = rc % TS;
+          if (I >= J) {
+            const int gr = I * TS + r, gc = J * TS + c;
+            dst[q] = tidx(I, J) * TSZ + c * TS + r;
+            if (gr < bs && gc < bs) v[q] = A[(size_t)(s + gc) * lda + (s + gr)];
+            else v[q] = (gr == gc) ? 1.0f : 0.0f;
+          }
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 8; ++q)
+        if (dst[q] >= 0) tiles[dst[q]] = T(v[q]);
     }
   }
   __syncthreads();
@@ -190,12 +241,25 @@ __device__ void potrf_block(T* tiles, float* A, int lda, int s, int bs, const fl
     if (tid == 0) set_status(st, MPCHOL_ERR_NOT_SPD, s + s_fail);
     return;
   }
-  // write back the lower triangle (rounded to FP32 for the FP64 path)
-  for (int c = warp; c < bs; c += nwarps) {
-    const int J = c / TS, cc = c % TS;
-    for (int r = c + lane; r < bs; r += TS) {
-      const int I = r / TS, rr = r % TS;
-      A[(size_t)(s + c) * lda + (s + r)] = (float)tiles[tidx(I, J) * TSZ + cc * TLD + rr];
+  // write back: TMA stores of the lower tiles (FP32 path), or a coalesced loop
+  // that rounds the FP64 tiles to FP32.  The strictly upper part of a
+  // diagonal tile still holds the matrix's own upper-triangle values.
+  if (TMA) {
+    tc::fence_proxy_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      for (int I = 0; I < NT; ++I)
+        for (int J = 0; J <= I; ++J)
+          tc::tma_store_2d(tmap, tiles + tidx(I, J) * TSZ, s + I * TS, s + J * TS);
+      tc::bulk_commit();
+    }
+  } else {
+    for (int c = warp; c < bs; c += nwarps) {
+      const int J = c / TS, cc = c % TS;
+      for (int r = c + lane; r < bs; r += TS) {
+        const int I = r / TS, rr = r % TS;
+        A[(size_t)(s + c) * lda + (s + r)] = (float)tiles[tidx(I, J) * TSZ + cc * TS + rr];
+      }
     }
   }
   // inverses of the diagonal tiles, used by the panel solve
@@ -203,26 +267,30 @@ __device__ void potrf_block(T* tiles, float* A, int lda, int s, int bs, const fl
     invert_tile<T>(tiles + tidx(J, J) * TSZ, s_inv + J * TS, scratch + J * TSZ,
                    winv + J * TS * TS, lane);
   if (tid == 0 && s_pert) atomicAdd(&st->perturbed, s_pert);
+  if (TMA && tid == 0) tc::bulk_wait_read();   // smem must outlive the stores' reads
+  (void)n;
 }
 
-// FP32 blocks: tiles in shared memory.  Separate kernels for the two
-// precisions keep the FP64 register footprint out of the FP32 path.
+// FP32 blocks: tiles in shared memory, staged by TMA.  Separate kernels for
+// the two precisions keep the FP64 register footprint out of the FP32 path.
 __global__ void __launch_bounds__(512, 1)
-potrf_f32_kernel(float* A, int lda, int s, int bs, const float* d, const float* sh, PotrfParams p,
-                 const int* fp64_flag, float* winv, DevStatus* st) {
+potrf_f32_kernel(const __grid_constant__ CUtensorMap tmap, float* A, int lda, int n, int s, int bs,
+                 const float* d, const float* sh, PotrfParams p, const int* fp64_flag, float* winv,
+                 DevStatus* st) {
   if (st->code != 0) return;
   if (fp64_flag != nullptr && *fp64_flag != 0) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  potrf_block<float>(reinterpret_cast<float*>(smem_raw), A, lda, s, bs, d, sh, p, winv, st);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  potrf_block<float, true>(&tmap, reinterpret_cast<float*>(smem_raw), A, lda, n, s, bs, d, sh, p,
+                           winv, st);
 }
 
 // FP64 blocks (flagged near-indefinite): tiles in a global scratch.
 __global__ void __launch_bounds__(256, 1)
-potrf_f64_kernel(float* A, int lda, int s, int bs, const float* d, const float* sh, PotrfParams p,
-                 const int* fp64_flag, double* scratch64, float* winv, DevStatus* st) {
+potrf_f64_kernel(float* A, int lda, int n, int s, int bs, const float* d, const float* sh,
+                 PotrfParams p, const int* fp64_flag, double* scratch64, float* winv, DevStatus* st) {
   if (st->code != 0) return;
   if (fp64_flag == nullptr || *fp64_flag == 0) return;
-  potrf_block<double>(scratch64, A, lda, s, bs, d, sh, p, winv, st);
+  potrf_block<double, false>(nullptr, scratch64, A, lda, n, s, bs, d, sh, p, winv, st);
 }
 
 }  // namespace
@@ -236,16 +304,18 @@ size_t potrf_scratch64_elems(int bs) {
   return ((size_t)NT * (NT + 1) / 2 + NT) * TSZ;
 }
 
-cudaError_t launch_potrf(float* A, int lda, int s, int bs, const float* d, const float* sh,
-                         const PotrfParams& p, const int* fp64_flag, double* scratch64,
-                         float* winv, DevStatus* st, bool may_fp64, cudaStream_t stream) {
+cudaError_t launch_potrf(const CUtensorMap& tmap32, float* A, int lda, int n, int s, int bs,
+                         const float* d, const float* sh, const PotrfParams& p,
+                         const int* fp64_flag, double* scratch64, float* winv, DevStatus* st,
+                         bool may_fp64, cudaStream_t stream) {
   const size_t smem = potrf_smem_bytes(256);
   cudaError_t e = cudaFuncSetAttribute(potrf_f32_kernel,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  potrf_f32_kernel<<<1, 512, smem, stream>>>(A, lda, s, bs, d, sh, p, fp64_flag, winv, st);
+  potrf_f32_kernel<<<1, 512, smem, stream>>>(tmap32, A, lda, n, s, bs, d, sh, p,
+                                             may_fp64 ? fp64_flag : nullptr, winv, st);
   if (may_fp64)
-    potrf_f64_kernel<<<1, 256, 0, stream>>>(A, lda, s, bs, d, sh, p, fp64_flag, scratch64, winv, st);
+    potrf_f64_kernel<<<1, 256, 0, stream>>>(A, lda, n, s, bs, d, sh, p, fp64_flag, scratch64, winv, st);
   return cudaGetLastError();
 }
 

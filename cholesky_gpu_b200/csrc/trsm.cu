@@ -6,25 +6,26 @@
 // (src/kernels_macros.cuh:191-211).
 //
 // X * L11^T = A21 for the m rows below the diagonal block.  Rows are
-// independent, so one CTA owns 64 rows for the whole solve.  Everything it
-// needs is staged into shared memory once, with all loads in flight: its rows
-// of the panel, the strictly-lower 32 x 32 tiles of L11 and the inverses of
-// L11's diagonal tiles (written by the POTRF kernel).  It then walks the
-// 32-column tiles J: X_J -= X_{<J} L_{J,<J}^T (register-tiled), then
-// X_J = X_J L_JJ^-T.  The epilogue writes X back, folds each row's sum of
+// independent, so one CTA owns 64 rows for the whole solve.  One thread stages
+// everything the CTA needs with TMA in a single round: its 64 x b slab of the
+// panel (one 2-D box), the strictly-lower 32 x 32 tiles of L11 (2-D boxes) and
+// the inverses of L11's diagonal tiles (a 1-D bulk copy of what the POTRF
+// kernel wrote).  The CTA then walks the 32-column tiles J:
+// X_J -= X_{<J} L_{J,<J}^T (register-tiled), X_J = X_J L_JJ^-T, writes the
+// slab back with one TMA store and, in the epilogue, folds each row's sum of
 // squares into the Schur-diagonal tracker dtilde and reduces the switching
 // statistics (max d/dtilde, reference-literal choice) and the near-indefinite
 // flag of the next diagonal block.
 #include "common.cuh"
 #include "kernels.cuh"
+#include "tc_ptx.cuh"
 
 namespace mpchol {
 namespace {
 
 constexpr int TR = 64;       // rows per CTA
 constexpr int NTHR = 256;
-constexpr int TLD = 33;      // padded stride of a 32 x 32 tile
-constexpr int TSZ = 32 * TLD;
+constexpr int TSZ = 32 * 32; // dense 32 x 32 tile
 constexpr int XLD = TR;      // X staged column-major, rows contiguous
 
 __device__ __forceinline__ int tl(int I, int M) { return I * (I - 1) / 2 + M; }  // I > M
@@ -35,95 +36,100 @@ size_t trsm_smem_floats(int bs) {
 }
 
 __global__ void __launch_bounds__(NTHR)
-trsm_panel_kernel(float* __restrict__ A, int lda, int n, int s, int bs, const float* __restrict__ winv,
+trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_constant__ CUtensorMap tmap32,
+                  int n, int s, int bs, const float* __restrict__ winv,
                   const float* __restrict__ d, float* __restrict__ dtilde, float* __restrict__ rowsq,
                   StepState* step, StepState* next, int next_bs, DecisionParams dp, DevStatus* st) {
   if (st->code != 0) return;
-  extern __shared__ __align__(16) float sm[];
+  extern __shared__ __align__(128) float sm[];
   const int NT = bs / 32;
-  float* Xs = sm;                                   // [bs][XLD]
-  float* Lt = Xs + (size_t)bs * XLD;                // strictly-lower tiles of L11
-  float* Wt = Lt + (size_t)(NT * (NT - 1) / 2) * TSZ;   // inverses of the diagonal tiles
+  float* Xs = sm;                                        // [bs][XLD]
+  float* Lt = Xs + (size_t)bs * XLD;                     // strictly-lower tiles of L11
+  float* Wt = Lt + (size_t)(NT * (NT - 1) / 2) * TSZ;    // inverses of the diagonal tiles
   __shared__ float red_max[NTHR / 32];
   __shared__ int red_lit[NTHR / 32];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int s_ok;
 
   const int tid = threadIdx.x;
   const int row0 = s + bs + blockIdx.x * TR;   // first global row of this CTA
   const int nrows = min(TR, n - row0);
   if (nrows <= 0) return;
 
-  // ---- stage everything (independent loads, unrolled) -------------------
-#pragma unroll 8
-  for (int e = tid; e < bs * TR; e += NTHR) {
-    const int c = e / TR, r = e % TR;
-    Xs[c * XLD + r] = (r < nrows) ? A[(size_t)(s + c) * lda + row0 + r] : 0.0f;
-  }
-  const int nlt = NT * (NT - 1) / 2;
-#pragma unroll 8
-  for (int e = tid; e < nlt * 1024; e += NTHR) {
-    const int t = e >> 10, rc = e & 1023;
-    const int c = rc >> 5, r = rc & 31;
-    int I = 1;
-    while (tl(I + 1, 0) <= t) ++I;
-    const int M = t - tl(I, 0);
-    Lt[t * TSZ + c * TLD + r] = A[(size_t)(s + 32 * M + c) * lda + s + 32 * I + r];
-  }
-#pragma unroll 8
-  for (int e = tid; e < NT * 1024; e += NTHR) {
-    const int J = e >> 10, mc = e & 1023;        // winv column-major: (L^-1)[c][m] at m*32+c
-    const int m = mc >> 5, c = mc & 31;
-    Wt[J * TSZ + m * TLD + c] = winv[e];
+  // ---- stage with TMA (rows past n arrive as zeros) -----------------------
+  if (tid == 0) {
+    s_ok = 1;
+    const int nlt = NT * (NT - 1) / 2;
+    tc::mbar_init(&bar, 1);
+    tc::fence_mbar_init();
+    tc::mbar_expect_tx(&bar, (uint32_t)((bs * XLD + nlt * TSZ + NT * TSZ) * sizeof(float)));
+    tc::tma_load_2d(Xs, &tmapX, &bar, row0, s);
+    for (int I = 1; I < NT; ++I)
+      for (int M = 0; M < I; ++M)
+        tc::tma_load_2d(Lt + tl(I, M) * TSZ, &tmap32, &bar, s + 32 * I, s + 32 * M);
+    tc::bulk_load_1d(Wt, winv, (uint32_t)(NT * TSZ * sizeof(float)), &bar);
+    if (!tc::mbar_wait(&bar, 0)) {
+      s_ok = 0;
+      set_status(st, MPCHOL_ERR_TIMEOUT, row0);
+      tc::mbar_wait(&bar, 0);
+    }
   }
   __syncthreads();
+  if (!s_ok) return;
 
-  const int tr = tid % 16, tc = tid / 16;   // 4 rows x 2 cols per thread
+  const int tr = tid % 16, tc_ = tid / 16;   // 4 rows x 2 cols per thread
   for (int J = 0; J < NT; ++J) {
     const int kend = 32 * J;
     float acc[4][2];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int j = 0; j < 2; ++j) acc[i][j] = Xs[(kend + 2 * tc + j) * XLD + 4 * tr + i];
+      for (int j = 0; j < 2; ++j) acc[i][j] = Xs[(kend + 2 * tc_ + j) * XLD + 4 * tr + i];
     // X_J -= X_{<J} L_{J,<J}^T
-    for (int k = 0; k < kend; ++k) {
-      const float4 xv = *reinterpret_cast<const float4*>(&Xs[k * XLD + 4 * tr]);
-      const float* lp = Lt + tl(J, k >> 5) * TSZ + (k & 31) * TLD + 2 * tc;
-      const float l0 = lp[0], l1 = lp[1];
-      acc[0][0] -= xv.x * l0; acc[0][1] -= xv.x * l1;
-      acc[1][0] -= xv.y * l0; acc[1][1] -= xv.y * l1;
-      acc[2][0] -= xv.z * l0; acc[2][1] -= xv.z * l1;
-      acc[3][0] -= xv.w * l0; acc[3][1] -= xv.w * l1;
+    for (int kt = 0; kt < J; ++kt) {
+      const float* lt = Lt + tl(J, kt) * TSZ + 2 * tc_;
+      const float* xt = Xs + (32 * kt) * XLD + 4 * tr;
+#pragma unroll 8
+      for (int kk = 0; kk < 32; ++kk) {
+        const float4 xv = *reinterpret_cast<const float4*>(xt + kk * XLD);
+        const float2 lv = *reinterpret_cast<const float2*>(lt + kk * 32);
+        acc[0][0] -= xv.x * lv.x; acc[0][1] -= xv.x * lv.y;
+        acc[1][0] -= xv.y * lv.x; acc[1][1] -= xv.y * lv.y;
+        acc[2][0] -= xv.z * lv.x; acc[2][1] -= xv.z * lv.y;
+        acc[3][0] -= xv.w * lv.x; acc[3][1] -= xv.w * lv.y;
+      }
     }
     __syncthreads();
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int j = 0; j < 2; ++j) Xs[(kend + 2 * tc + j) * XLD + 4 * tr + i] = acc[i][j];
+      for (int j = 0; j < 2; ++j) Xs[(kend + 2 * tc_ + j) * XLD + 4 * tr + i] = acc[i][j];
     __syncthreads();
     // X_J = X_J * L_JJ^-T :  x[r][c] = sum_{m<=c} a[r][m] * (L^-1)[c][m]
     float out[4][2] = {};
-    const float* W = Wt + J * TSZ;
-#pragma unroll 4
+    const float* W = Wt + J * TSZ + 2 * tc_;
+#pragma unroll 8
     for (int m = 0; m < 32; ++m) {
       const float4 av = *reinterpret_cast<const float4*>(&Xs[(kend + m) * XLD + 4 * tr]);
-      const float w0 = W[m * TLD + 2 * tc], w1 = W[m * TLD + 2 * tc + 1];
-      out[0][0] += av.x * w0; out[0][1] += av.x * w1;
-      out[1][0] += av.y * w0; out[1][1] += av.y * w1;
-      out[2][0] += av.z * w0; out[2][1] += av.z * w1;
-      out[3][0] += av.w * w0; out[3][1] += av.w * w1;
+      const float2 wv = *reinterpret_cast<const float2*>(W + m * 32);
+      out[0][0] += av.x * wv.x; out[0][1] += av.x * wv.y;
+      out[1][0] += av.y * wv.x; out[1][1] += av.y * wv.y;
+      out[2][0] += av.z * wv.x; out[2][1] += av.z * wv.y;
+      out[3][0] += av.w * wv.x; out[3][1] += av.w * wv.y;
     }
     __syncthreads();
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int j = 0; j < 2; ++j) Xs[(kend + 2 * tc + j) * XLD + 4 * tr + i] = out[i][j];
+      for (int j = 0; j < 2; ++j) Xs[(kend + 2 * tc_ + j) * XLD + 4 * tr + i] = out[i][j];
     __syncthreads();
   }
-  // ---- write back the solved rows -----------------------------------------
-#pragma unroll 8
-  for (int e = tid; e < bs * TR; e += NTHR) {
-    const int c = e / TR, r = e % TR;
-    if (r < nrows) A[(size_t)(s + c) * lda + row0 + r] = Xs[c * XLD + r];
+  // ---- write the solved slab back (TMA store clips rows past n) -----------
+  tc::fence_proxy_async_smem();
+  __syncthreads();
+  if (tid == 0) {
+    tc::tma_store_2d(&tmapX, Xs, row0, s);
+    tc::bulk_commit();
   }
   // ---- fused epilogue: Schur diagonal tracker and switching statistics --
   float ratio = 0.0f;
@@ -159,15 +165,16 @@ trsm_panel_kernel(float* __restrict__ A, int lda, int n, int s, int bs, const fl
     for (int w = 0; w < NTHR / 32; ++w) { bm = fmaxf(bm, red_max[w]); bl = max(bl, red_lit[w]); }
     atomicMax(&step->max_ratio_bits, __float_as_uint(bm));
     atomicMax(&step->literal_code, bl);
+    tc::bulk_wait_read();
   }
 }
 
 }  // namespace
 
-cudaError_t launch_trsm_panel(float* A, int lda, int n, int s, int bs, const float* winv,
-                              const float* d, float* dtilde, float* rowsq, StepState* step,
-                              StepState* next, int next_bs, const DecisionParams& dp,
-                              DevStatus* st, cudaStream_t stream) {
+cudaError_t launch_trsm_panel(const CUtensorMap& tmapX, const CUtensorMap& tmap32, int n, int s,
+                              int bs, const float* winv, const float* d, float* dtilde,
+                              float* rowsq, StepState* step, StepState* next, int next_bs,
+                              const DecisionParams& dp, DevStatus* st, cudaStream_t stream) {
   const int m = n - s - bs;
   if (m <= 0) return cudaSuccess;
   const size_t smem = trsm_smem_floats(bs) * sizeof(float);
@@ -175,8 +182,9 @@ cudaError_t launch_trsm_panel(float* A, int lda, int n, int s, int bs, const flo
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)(trsm_smem_floats(256) * sizeof(float)));
   if (e != cudaSuccess) return e;
-  trsm_panel_kernel<<<ceil_div(m, TR), NTHR, smem, stream>>>(A, lda, n, s, bs, winv, d, dtilde,
-                                                             rowsq, step, next, next_bs, dp, st);
+  trsm_panel_kernel<<<ceil_div(m, TR), NTHR, smem, stream>>>(tmapX, tmap32, n, s, bs, winv, d,
+                                                             dtilde, rowsq, step, next, next_bs,
+                                                             dp, st);
   return cudaGetLastError();
 }
 
