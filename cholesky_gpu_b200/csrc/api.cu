@@ -154,7 +154,7 @@ namespace {
 mpchol_status validate_opts(const mpchol_opts* o, int n) {
   if (o == nullptr || n <= 0) return MPCHOL_ERR_BAD_ARG;
   if (o->block_size < 32 || o->block_size > 256 || o->block_size % 32 != 0) return MPCHOL_ERR_BAD_ARG;
-  if (o->precision < 0 || o->precision > MPCHOL_PREC_SWITCHING) return MPCHOL_ERR_BAD_ARG;
+  if (o->precision < 0 || o->precision > MPCHOL_PREC_FP16X2) return MPCHOL_ERR_BAD_ARG;
   if (o->left != 0) return MPCHOL_ERR_NOT_SUPPORTED;
   if (o->diag_pert && !(o->pivot_floor > 0.0f)) return MPCHOL_ERR_BAD_ARG;
   if (o->switch_mode != 0 && o->switch_mode != 1) return MPCHOL_ERR_BAD_ARG;
@@ -168,7 +168,7 @@ mpchol_status validate_opts(const mpchol_opts* o, int n) {
     } else {
       for (int i = 0; i < o->ladder_len; ++i) {
         const int p = o->ladder[i];
-        if (p < 0 || p > MPCHOL_PREC_MXFP8) return MPCHOL_ERR_BAD_ARG;
+        if (p < 0 || p > MPCHOL_PREC_FP16X2 || p == MPCHOL_PREC_SWITCHING) return MPCHOL_ERR_BAD_ARG;
         if (p == MPCHOL_PREC_MXFP8 || !tc_ok(p)) return MPCHOL_ERR_NOT_SUPPORTED;
       }
     }
@@ -584,7 +584,7 @@ mpchol_status mpchol_factor_create(const mpchol_opts* opts, int n, mpchol_factor
             dmalloc(&f->rowsq, n) == cudaSuccess && dmalloc(&f->sh, n) == cudaSuccess &&
             dmalloc(&f->winv, (size_t)8 * 32 * 32) == cudaSuccess &&
             dmalloc(&f->scratch64, potrf_scratch64_elems(256)) == cudaSuccess &&
-            dmalloc(reinterpret_cast<uint8_t**>(&f->q), (size_t)n * f->b * 2) == cudaSuccess &&
+            dmalloc(reinterpret_cast<uint8_t**>(&f->q), (size_t)n * f->b * 4) == cudaSuccess &&
             dmalloc(&f->rowexp, n) == cudaSuccess &&
             dmalloc(&f->mxexp, (size_t)n * (f->b / 32)) == cudaSuccess &&
             dmalloc(&f->steps, f->nsteps + 1) == cudaSuccess &&
@@ -667,7 +667,7 @@ mpchol_status mpchol_factor_info_get(const mpchol_factor_t* fc, mpchol_factor_in
     if (hStepPrec) hStepPrec[k] = p;
     if (hStepFp64) hStepFp64[k] = steps[k].fp64_diag;
     if (steps[k].fp64_diag) info->n_fp64_blocks++;
-    if (m > 0 && p >= 0 && p < 5) info->steps_by_prec[p]++;
+    if (m > 0 && p >= 0 && p < 7) info->steps_by_prec[p]++;
   }
   return MPCHOL_OK;
 }
@@ -819,7 +819,8 @@ mpchol_status mpchol_quantize_rows(const float* dP, int m, int k, int ldp, int f
                                    void* dScale, mpchol_stream_t stream) {
   if (dP == nullptr || dQ == nullptr || dScale == nullptr || m < 0 || ldp < m) return MPCHOL_ERR_BAD_ARG;
   if (k < 32 || k > 256 || k % 32 != 0) return MPCHOL_ERR_BAD_ARG;
-  if (fmt != FP16 && fmt != E4M3 && fmt != E5M2 && fmt != MXFP8) return MPCHOL_ERR_BAD_ARG;
+  if (fmt != FP16 && fmt != E4M3 && fmt != E5M2 && fmt != MXFP8 && fmt != FP16X2)
+    return MPCHOL_ERR_BAD_ARG;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   if (fmt == MXFP8)
     PHASE(MPCHOL_PH_QUANT, 1, s, launch_quantize_rows(dP, ldp, m, k, fmt, dQ, k, nullptr,

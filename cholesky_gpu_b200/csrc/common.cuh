@@ -10,7 +10,7 @@
 namespace mpchol {
 
 // Storage format ids match MPCHOL_PREC_*.
-enum Fmt : int { FP32 = 0, FP16 = 1, E4M3 = 2, E5M2 = 3, MXFP8 = 4, SWITCHING = 5 };
+enum Fmt : int { FP32 = 0, FP16 = 1, E4M3 = 2, E5M2 = 3, MXFP8 = 4, SWITCHING = 5, FP16X2 = 6 };
 
 // Device-side status block shared by every kernel of one factor/solve.  A
 // kernel that detects a failure (non-SPD pivot, exhausted bounded wait, bad
@@ -90,6 +90,7 @@ __host__ __device__ __forceinline__ float unit_roundoff(int fmt) {
     case E4M3: case MXFP8: return 0.0625f;
     case E5M2: return 0.125f;
     case FP16: return 4.8828125e-4f;
+    case FP16X2: return 2.3841858e-7f;   // hi + lo: 22 significant bits
     default: return 5.9604645e-8f;
   }
 }

@@ -78,6 +78,19 @@ __device__ void quantize_tile(const float* __restrict__ P, int ldp, int m, int k
 #pragma unroll
         for (int t = 0; t < 8; ++t)
           if (t < cpl) qr[t] = f32_to_f16(v[t] * inv);
+      } else if (fmt == FP16X2) {
+        // hi = fp16(x), lo = fp16(x - hi); x - hi is exact in FP32.  The lo
+        // panel follows the hi panel (m rows further on).
+        uint16_t* qh = reinterpret_cast<uint16_t*>(q) + (size_t)gi * ldq + lane * cpl;
+        uint16_t* ql = qh + (size_t)m * ldq;
+#pragma unroll
+        for (int t = 0; t < 8; ++t)
+          if (t < cpl) {
+            const float xs = v[t] * inv;
+            const __half h = __float2half_rn(xs);
+            qh[t] = __half_as_ushort(h);
+            ql[t] = f32_to_f16(xs - __half2float(h));
+          }
       } else {
         uint8_t* qr = reinterpret_cast<uint8_t*>(q) + (size_t)gi * ldq + lane * cpl;
 #pragma unroll

@@ -4,26 +4,37 @@
 // Replaces the reference's cuBLASLt trailing updates LtHSgemm_fp16in_fp32out
 // (src/switching_chol.cuh:170-197, src/fp8_utils.cuh:304-412), the per-tensor
 // scaled FP8 CUTLASS GEMM (src/fp8Chol.cuh:236-275) and the WMMA SYRK
-// (src/syrk_gemm.cuh:14-124).  C(m x m, lower tiles) -= s_i s_j (Q Q^T): Q is
-// the K-major quantized panel (FP16 / E4M3 / E5M2), s the per-row power-of-two
-// scales, accumulation in FP32 in tensor memory.  One CTA per 128 x 128 lower
-// tile: thread 0 stages both 128-row strips of Q with TMA (128-byte swizzle,
-// no multicast), issues the k/K_mma tcgen05.mma instructions into a 128-column
-// TMEM accumulator and commits to an mbarrier; four warps then read their 32
-// TMEM lanes and apply the scaled update to C in FP32 (coalesced along rows).
-// Diagonal tiles load one strip and use it for both operands.
-#include <cudaTypedefs.h>
-
+// (src/syrk_gemm.cuh:14-124).
+//
+// C(m x m, lower 128 x 128 tiles) -= s_i s_j (Q Q^T), Q the K-major quantized
+// panel with per-row power-of-two scales s, FP32 accumulation in tensor memory.
+// FP16X2 carries each panel value as hi + lo (two FP16 terms) and accumulates
+// hi hi^T + hi lo^T + lo hi^T, which is FP32-class accurate at FP16 tensor
+// speed.
+//
+// Persistent and warp-specialized, one CTA per SM (192 threads):
+//   warp 0  TMA producer: K chunks of 128 bytes per row (one 128-byte swizzle
+//           row) of the A strip (rows of tile I) and the B strip (rows of tile
+//           J; skipped on diagonal tiles) into a ring of NSTAGE stages;
+//   warp 1  allocates 2 x 128 TMEM columns; one thread issues tcgen05.mma and
+//           commits each stage back to the producer and each finished tile to
+//           the epilogue;
+//   warps 2-5 epilogue: tcgen05.ld of their 32 TMEM lanes, the scaled update
+//           applied to C with batched, coalesced loads and stores.
+// The two TMEM accumulators let the epilogue of one tile overlap the MMAs of
+// the next.  Every mbarrier wait is bounded.
 #include "common.cuh"
 #include "kernels.cuh"
 #include "tc_ptx.cuh"
+#include "tmap.cuh"
 
 namespace mpchol {
 namespace {
 
-constexpr int TM = 128;            // output tile (M = N = 128)
-constexpr int BOX_BYTES = 128;     // inner TMA box = one 128-byte swizzle row
-constexpr int STRIP_CHUNK = TM * BOX_BYTES;   // 16 KB per (strip, K chunk)
+constexpr int TM = 128;                    // output tile (M = N = 128)
+constexpr int CHUNK = 128;                 // bytes of K per row per stage
+constexpr int STRIP = TM * CHUNK;          // 16 KB: one operand strip chunk
+constexpr int NTHREADS = 192;
 
 __device__ __forceinline__ void tile_of(int t, int& I, int& J) {
   int i = (int)((sqrtf(8.0f * t + 1.0f) - 1.0f) * 0.5f);
@@ -33,101 +44,192 @@ __device__ __forceinline__ void tile_of(int t, int& I, int& J) {
   J = t - i * (i + 1) / 2;
 }
 
+template <int FMT> struct TcCfg;
+template <> struct TcCfg<FP16> {
+  static constexpr int ESIZE = 2, NSETS = 1, NSTAGE = 4;
+  static constexpr uint32_t IDESC = tc::make_idesc(0, 0, TM, TM);
+};
+template <> struct TcCfg<E4M3> {
+  static constexpr int ESIZE = 1, NSETS = 1, NSTAGE = 4;
+  static constexpr uint32_t IDESC = tc::make_idesc(0, 0, TM, TM);
+};
+template <> struct TcCfg<E5M2> {
+  static constexpr int ESIZE = 1, NSETS = 1, NSTAGE = 4;
+  static constexpr uint32_t IDESC = tc::make_idesc(1, 1, TM, TM);
+};
+template <> struct TcCfg<FP16X2> {
+  static constexpr int ESIZE = 2, NSETS = 2, NSTAGE = 3;
+  static constexpr uint32_t IDESC = tc::make_idesc(0, 0, TM, TM);
+};
+
+struct TcMaps {
+  CUtensorMap hi;   // main (or hi) panel: rows m, K-major
+  CUtensorMap lo;   // lo panel (FP16X2 only)
+};
+
 template <int FMT>
-__global__ void __launch_bounds__(128, 1)
-syrk_tc_kernel(const __grid_constant__ CUtensorMap tmap, float* __restrict__ C, int ldc, int m,
-               int k, const int8_t* __restrict__ rowexp, const int* prec_sel, DevStatus* st) {
+__global__ void __launch_bounds__(NTHREADS, 1)
+syrk_tc_kernel(const __grid_constant__ TcMaps maps, float* __restrict__ C, int ldc, int m, int k,
+               const int8_t* __restrict__ rowexp, const int* prec_sel, DevStatus* st) {
+  using Cfg = TcCfg<FMT>;
   if (st != nullptr && st->code != 0) return;
   if (prec_sel != nullptr && *prec_sel != FMT) return;
-  constexpr int ESIZE = (FMT == FP16) ? 2 : 1;
-  constexpr int ELEMS_PER_BOX = BOX_BYTES / ESIZE;
-  constexpr uint32_t IDESC = (FMT == FP16) ? tc::make_idesc(0, 0, TM, TM)
-                             : (FMT == E5M2) ? tc::make_idesc(1, 1, TM, TM)
-                                             : tc::make_idesc(0, 0, TM, TM);
-  constexpr int KSTEP_BYTES = 32;   // K per MMA: 16 x 2 B (f16) or 32 x 1 B (f8f6f4)
+  constexpr int NS = Cfg::NSTAGE;
+  constexpr int NSETS = Cfg::NSETS;
+  constexpr int STAGE_BYTES = 2 * NSETS * STRIP;       // A sets then B sets
+  constexpr int KSTEP = 32;                             // bytes of K per MMA
+  constexpr int ELEMS_PER_CHUNK = CHUNK / Cfg::ESIZE;
 
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  const int nbox = (k * ESIZE) / BOX_BYTES;
-  uint8_t* sA = smem;
-  uint8_t* sB = smem + (size_t)nbox * STRIP_CHUNK;
-  __shared__ __align__(8) uint64_t bar_tma;
-  __shared__ __align__(8) uint64_t bar_mma;
+  __shared__ __align__(8) uint64_t full_bar[NS];
+  __shared__ __align__(8) uint64_t empty_bar[NS];
+  __shared__ __align__(8) uint64_t accf_bar[2];
+  __shared__ __align__(8) uint64_t acce_bar[2];
   __shared__ uint32_t tmem_base_sh;
-  __shared__ int ok_sh;
-  __shared__ float s_scale_j[TM];
+  __shared__ volatile int abort_sh;
 
-  int I, J;
-  tile_of(blockIdx.x, I, J);
-  const bool diag = (I == J);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int T = (m + TM - 1) / TM;
+  const int ntiles = T * (T + 1) / 2;
+  const int nchunks = (k * Cfg::ESIZE) / CHUNK;
 
   if (threadIdx.x == 0) {
-    tc::prefetch_tmap(&tmap);
-    tc::mbar_init(&bar_tma, 1);
-    tc::mbar_init(&bar_mma, 1);
+    for (int s = 0; s < NS; ++s) { tc::mbar_init(&full_bar[s], 1); tc::mbar_init(&empty_bar[s], 1); }
+    for (int b = 0; b < 2; ++b) { tc::mbar_init(&accf_bar[b], 1); tc::mbar_init(&acce_bar[b], 4); }
     tc::fence_mbar_init();
-    ok_sh = 1;
+    tc::prefetch_tmap(&maps.hi);
+    if (NSETS == 2) tc::prefetch_tmap(&maps.lo);
+    abort_sh = 0;
   }
-  if (warp == 0) tc::tmem_alloc(&tmem_base_sh, TM);
-  {
-    const int j = J * TM + threadIdx.x;
-    s_scale_j[threadIdx.x] = (j < m) ? pow2f(rowexp[j]) : 0.0f;
-  }
+  if (warp == 1) tc::tmem_alloc(&tmem_base_sh, 2 * TM);
   tc::tc_fence_before();
   __syncthreads();
   tc::tc_fence_after();
   const uint32_t tmem = tmem_base_sh;
 
-  if (threadIdx.x == 0) {
-    const uint32_t bytes = (uint32_t)((diag ? 1 : 2) * nbox * STRIP_CHUNK);
-    tc::mbar_expect_tx(&bar_tma, bytes);
-    for (int b = 0; b < nbox; ++b) {
-      tc::tma_load_2d(sA + (size_t)b * STRIP_CHUNK, &tmap, &bar_tma, b * ELEMS_PER_BOX, I * TM);
-      if (!diag)
-        tc::tma_load_2d(sB + (size_t)b * STRIP_CHUNK, &tmap, &bar_tma, b * ELEMS_PER_BOX, J * TM);
-    }
-    if (tc::mbar_wait(&bar_tma, 0)) {
-      tc::tc_fence_after();
-      const uint8_t* sBop = diag ? sA : sB;
-      uint32_t accumulate = 0;
-      for (int b = 0; b < nbox; ++b) {
-        const uint32_t a0 = tc::smem_u32(sA + (size_t)b * STRIP_CHUNK);
-        const uint32_t b0 = tc::smem_u32(sBop + (size_t)b * STRIP_CHUNK);
-#pragma unroll
-        for (int kk = 0; kk < BOX_BYTES / KSTEP_BYTES; ++kk) {
-          const uint64_t ad = tc::make_desc_sw128(a0 + kk * KSTEP_BYTES);
-          const uint64_t bd = tc::make_desc_sw128(b0 + kk * KSTEP_BYTES);
-          if (FMT == FP16) tc::mma_f16(tmem, ad, bd, IDESC, accumulate);
-          else tc::mma_f8f6f4(tmem, ad, bd, IDESC, accumulate);
-          accumulate = 1;
+  if (warp == 0) {
+    // ---------------- TMA producer ----------------
+    if (lane == 0) {
+      int c = 0;   // global chunk counter
+      for (int t = blockIdx.x; t < ntiles && !abort_sh; t += gridDim.x) {
+        int I, J;
+        tile_of(t, I, J);
+        const bool diag = (I == J);
+        const uint32_t bytes = (uint32_t)((diag ? 1 : 2) * NSETS * STRIP);
+        for (int kc = 0; kc < nchunks; ++kc, ++c) {
+          const int s = c % NS;
+          const uint32_t pass = (uint32_t)(c / NS);
+          if (!tc::mbar_wait(&empty_bar[s], (pass & 1u) ^ 1u)) {
+            abort_sh = 1;
+            if (st != nullptr) set_status(st, MPCHOL_ERR_TIMEOUT, t);
+            break;
+          }
+          uint8_t* base = smem + (size_t)s * STAGE_BYTES;
+          tc::mbar_expect_tx(&full_bar[s], bytes);
+          const int x = kc * ELEMS_PER_CHUNK;
+          tc::tma_load_2d(base, &maps.hi, &full_bar[s], x, I * TM);
+          if (NSETS == 2) tc::tma_load_2d(base + STRIP, &maps.lo, &full_bar[s], x, I * TM);
+          if (!diag) {
+            tc::tma_load_2d(base + NSETS * STRIP, &maps.hi, &full_bar[s], x, J * TM);
+            if (NSETS == 2)
+              tc::tma_load_2d(base + (NSETS + 1) * STRIP, &maps.lo, &full_bar[s], x, J * TM);
+          }
         }
       }
-      tc::mma_commit(&bar_mma);
-    } else {
-      ok_sh = 0;
-      if (st != nullptr) set_status(st, MPCHOL_ERR_TIMEOUT, blockIdx.x);
-      tc::mbar_wait(&bar_tma, 0);   // give in-flight copies one more bounded chance to land
     }
-  }
-  __syncthreads();
-  if (ok_sh) {
-    if (!tc::mbar_wait(&bar_mma, 0)) {
-      if (st != nullptr) set_status(st, MPCHOL_ERR_TIMEOUT, blockIdx.x);
-    } else {
+  } else if (warp == 1) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0) {
+      int c = 0, tcount = 0;
+      for (int t = blockIdx.x; t < ntiles && !abort_sh; t += gridDim.x, ++tcount) {
+        int I, J;
+        tile_of(t, I, J);
+        const bool diag = (I == J);
+        const int buf = tcount & 1;
+        const uint32_t use = (uint32_t)(tcount >> 1);
+        if (!tc::mbar_wait(&acce_bar[buf], (use & 1u) ^ 1u)) {
+          abort_sh = 1;
+          if (st != nullptr) set_status(st, MPCHOL_ERR_TIMEOUT, t);
+          break;
+        }
+        tc::tc_fence_after();
+        const uint32_t dacc = tmem + (uint32_t)(buf * TM);
+        uint32_t accumulate = 0;
+        bool ok = true;
+        for (int kc = 0; kc < nchunks; ++kc, ++c) {
+          const int s = c % NS;
+          const uint32_t pass = (uint32_t)(c / NS);
+          if (!tc::mbar_wait(&full_bar[s], pass & 1u)) {
+            abort_sh = 1;
+            if (st != nullptr) set_status(st, MPCHOL_ERR_TIMEOUT, t);
+            ok = false;
+            break;
+          }
+          tc::tc_fence_after();
+          const uint32_t a_hi = tc::smem_u32(smem + (size_t)s * STAGE_BYTES);
+          const uint32_t a_lo = a_hi + STRIP;
+          const uint32_t b_hi = diag ? a_hi : a_hi + NSETS * STRIP;
+          const uint32_t b_lo = diag ? a_lo : a_hi + (NSETS + 1) * STRIP;
+#pragma unroll
+          for (int kk = 0; kk < CHUNK / KSTEP; ++kk) {
+            const uint32_t off = kk * KSTEP;
+            const uint64_t ad = tc::make_desc_sw128(a_hi + off);
+            const uint64_t bd = tc::make_desc_sw128(b_hi + off);
+            if (FMT == FP16 || FMT == FP16X2) tc::mma_f16(dacc, ad, bd, Cfg::IDESC, accumulate);
+            else tc::mma_f8f6f4(dacc, ad, bd, Cfg::IDESC, accumulate);
+            accumulate = 1;
+            if (NSETS == 2) {
+              tc::mma_f16(dacc, ad, tc::make_desc_sw128(b_lo + off), Cfg::IDESC, 1);
+              tc::mma_f16(dacc, tc::make_desc_sw128(a_lo + off), bd, Cfg::IDESC, 1);
+            }
+          }
+          tc::mma_commit(&empty_bar[s]);     // stage free once these MMAs finish
+        }
+        if (!ok) break;
+        tc::mma_commit(&accf_bar[buf]);      // tile accumulated
+      }
+    }
+  } else {
+    // ---------------- epilogue (warps 2..5) ----------------
+    const int q = warp & 3;                  // TMEM lane quarter this warp may access
+    int tcount = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++tcount) {
+      int I, J;
+      tile_of(t, I, J);
+      const int buf = tcount & 1;
+      const uint32_t use = (uint32_t)(tcount >> 1);
+      if (!tc::mbar_wait(&accf_bar[buf], use & 1u)) {
+        if (lane == 0) { abort_sh = 1; if (st != nullptr) set_status(st, MPCHOL_ERR_TIMEOUT, t); }
+        break;
+      }
       tc::tc_fence_after();
-      const int i = I * TM + warp * 32 + lane;
+      const int i = I * TM + q * 32 + lane;
       const float si = (i < m) ? pow2f(rowexp[i]) : 0.0f;
+      const uint32_t taddr = tmem + (uint32_t)(buf * TM) + ((uint32_t)(q * 32) << 16);
 #pragma unroll 1
       for (int c0 = 0; c0 < TM; c0 += 32) {
         float v[32];
-        tc::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+        tc::tmem_ld32(taddr + (uint32_t)c0, v);
+        if (c0 + 32 >= TM) {
+          // last read of this accumulator: hand it back to the MMA warp
+          tc::tc_fence_before();
+          __syncwarp();
+          if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tc::smem_u32(&acce_bar[buf])) : "memory");
+        }
+        const int j0 = J * TM + c0;
         if (i < m) {
+          float cv[32];
 #pragma unroll
-          for (int t = 0; t < 32; ++t) {
-            const int j = J * TM + c0 + t;
-            if (j < m && i >= j) C[(size_t)j * ldc + i] -= (v[t] * si) * s_scale_j[c0 + t];
+          for (int u = 0; u < 32; ++u) {
+            const int j = j0 + u;
+            cv[u] = (j < m && i >= j) ? C[(size_t)j * ldc + i] : 0.0f;
+          }
+#pragma unroll
+          for (int u = 0; u < 32; ++u) {
+            const int j = j0 + u;
+            if (j < m && i >= j) C[(size_t)j * ldc + i] = cv[u] - (v[u] * si) * pow2f(rowexp[j]);
           }
         }
       }
@@ -135,30 +237,40 @@ syrk_tc_kernel(const __grid_constant__ CUtensorMap tmap, float* __restrict__ C, 
   }
   tc::tc_fence_before();
   __syncthreads();
-  if (warp == 0) {
+  if (warp == 1) {
     tc::tc_fence_after();
-    tc::tmem_dealloc(tmem, TM);
+    tc::tmem_dealloc(tmem, 2 * TM);
   }
 }
 
-PFN_cuTensorMapEncodeTiled_v12000 get_encode_fn() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  if (fn == nullptr) {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
-            cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-  }
-  return fn;
+template <int FMT>
+size_t tc_smem() {
+  return (size_t)TcCfg<FMT>::NSTAGE * 2 * TcCfg<FMT>::NSETS * STRIP + 1024;
+}
+
+template <int FMT>
+cudaError_t launch_fmt(const TcMaps& maps, float* C, int ldc, int m, int k, const int8_t* rowexp,
+                       const int* prec_sel, DevStatus* st, cudaStream_t stream) {
+  const size_t smem = tc_smem<FMT>();
+  cudaError_t e = cudaFuncSetAttribute(syrk_tc_kernel<FMT>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int nsm = 148;
+  int dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess)
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const int T = ceil_div(m, TM);
+  const int ntiles = T * (T + 1) / 2;
+  const int grid = ntiles < nsm ? ntiles : nsm;
+  syrk_tc_kernel<FMT><<<grid, NTHREADS, smem, stream>>>(maps, C, ldc, m, k, rowexp, prec_sel, st);
+  return cudaGetLastError();
 }
 
 }  // namespace
 
 bool syrk_tc_supported(int fmt, int k) {
-  if (fmt == FP16) return k > 0 && (k * 2) % BOX_BYTES == 0 && k <= 256;
-  if (fmt == E4M3 || fmt == E5M2) return k > 0 && k % BOX_BYTES == 0 && k <= 256;
+  if (fmt == FP16 || fmt == FP16X2) return k > 0 && (k * 2) % CHUNK == 0 && k <= 256;
+  if (fmt == E4M3 || fmt == E5M2) return k > 0 && k % CHUNK == 0 && k <= 256;
   return false;
 }
 
@@ -168,44 +280,26 @@ cudaError_t launch_syrk_tc(float* C, int ldc, int m, int k, int fmt, const void*
   (void)mxexp; (void)ldmx;
   if (m <= 0) return cudaSuccess;
   if (!syrk_tc_supported(fmt, k)) return cudaErrorInvalidValue;
-  auto encode = get_encode_fn();
-  if (encode == nullptr) return cudaErrorNotSupported;
-  const int esize = (fmt == FP16) ? 2 : 1;
-  CUtensorMap map;
-  cuuint64_t dims[2] = {(cuuint64_t)k, (cuuint64_t)m};
-  cuuint64_t strides[1] = {(cuuint64_t)ldq * esize};
-  cuuint32_t box[2] = {(cuuint32_t)(BOX_BYTES / esize), (cuuint32_t)TM};
-  cuuint32_t estr[2] = {1, 1};
-  CUresult r = encode(&map, esize == 2 ? CU_TENSOR_MAP_DATA_TYPE_UINT16 : CU_TENSOR_MAP_DATA_TYPE_UINT8,
-                      2, const_cast<void*>(q), dims, strides, box, estr,
-                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
-  const int nbox = (k * esize) / BOX_BYTES;
-  const size_t smem = (size_t)2 * nbox * STRIP_CHUNK + 1024;
-  const int T = ceil_div(m, TM);
-  const int grid = T * (T + 1) / 2;
-  cudaError_t e;
-  switch (fmt) {
-    case FP16:
-      e = cudaFuncSetAttribute(syrk_tc_kernel<FP16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess) return e;
-      syrk_tc_kernel<FP16><<<grid, 128, smem, stream>>>(map, C, ldc, m, k, rowexp, prec_sel, st);
-      break;
-    case E4M3:
-      e = cudaFuncSetAttribute(syrk_tc_kernel<E4M3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess) return e;
-      syrk_tc_kernel<E4M3><<<grid, 128, smem, stream>>>(map, C, ldc, m, k, rowexp, prec_sel, st);
-      break;
-    case E5M2:
-      e = cudaFuncSetAttribute(syrk_tc_kernel<E5M2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess) return e;
-      syrk_tc_kernel<E5M2><<<grid, 128, smem, stream>>>(map, C, ldc, m, k, rowexp, prec_sel, st);
-      break;
-    default:
+  const int esize = (fmt == FP16 || fmt == FP16X2) ? 2 : 1;
+  const CUtensorMapDataType dt = esize == 2 ? CU_TENSOR_MAP_DATA_TYPE_UINT16 : CU_TENSOR_MAP_DATA_TYPE_UINT8;
+  TcMaps maps;
+  if (!encode_tmap_2d(&maps.hi, dt, esize, q, (uint64_t)k, (uint64_t)m, (uint64_t)ldq,
+                      CHUNK / esize, TM, CU_TENSOR_MAP_SWIZZLE_128B))
+    return cudaErrorInvalidValue;
+  maps.lo = maps.hi;
+  if (fmt == FP16X2) {
+    const uint16_t* lo = reinterpret_cast<const uint16_t*>(q) + (size_t)m * ldq;
+    if (!encode_tmap_2d(&maps.lo, dt, esize, lo, (uint64_t)k, (uint64_t)m, (uint64_t)ldq,
+                        CHUNK / esize, TM, CU_TENSOR_MAP_SWIZZLE_128B))
       return cudaErrorInvalidValue;
   }
-  return cudaGetLastError();
+  switch (fmt) {
+    case FP16: return launch_fmt<FP16>(maps, C, ldc, m, k, rowexp, prec_sel, st, stream);
+    case E4M3: return launch_fmt<E4M3>(maps, C, ldc, m, k, rowexp, prec_sel, st, stream);
+    case E5M2: return launch_fmt<E5M2>(maps, C, ldc, m, k, rowexp, prec_sel, st, stream);
+    case FP16X2: return launch_fmt<FP16X2>(maps, C, ldc, m, k, rowexp, prec_sel, st, stream);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 }  // namespace mpchol

@@ -58,7 +58,9 @@ typedef enum {
   MPCHOL_PREC_E4M3 = 2,   /* per-row power-of-two scaled E4M3 (RNE, satfinite) */
   MPCHOL_PREC_E5M2 = 3,   /* per-row power-of-two scaled E5M2 */
   MPCHOL_PREC_MXFP8 = 4,  /* OCP MX: E4M3 + E8M0 scale per 32 elements along K */
-  MPCHOL_PREC_SWITCHING = 5 /* per-step choice by the switching criterion */
+  MPCHOL_PREC_SWITCHING = 5, /* per-step choice by the switching criterion */
+  MPCHOL_PREC_FP16X2 = 6     /* two-term FP16 split (hi + lo, per-row scaled): FP32-class
+                                accuracy on FP16 tensor cores */
 } mpchol_precision;
 
 /* Factorization options.  Field names follow the reference's settings.json
@@ -85,7 +87,7 @@ typedef struct {
   int n_perturbed;     /* pivots raised by diag_pert */
   int nsteps;          /* ceil(n / b) */
   int n_fp64_blocks;   /* diagonal blocks factored in FP64 */
-  int steps_by_prec[5];/* number of trailing updates done in each mpchol_precision */
+  int steps_by_prec[7];/* number of trailing updates done in each mpchol_precision */
 } mpchol_factor_info;
 
 typedef struct {
@@ -213,7 +215,8 @@ MPCHOL_API int mpchol_switching_chol(float* dA, int n, int b, float* d_diagVals,
 MPCHOL_API mpchol_status mpchol_quantize(const float* dX, void* dQ, long long count, int fmt,
                               mpchol_stream_t stream);
 /* Panel quantization as done inside the factor: dP is m x k column-major
- * (ld = ldp); dQ receives a row-major (K-major) m x k copy in fmt; dScale
+ * (ld = ldp); dQ receives a row-major (K-major) m x k copy in fmt (FP16X2:
+ * the m x k hi panel followed by the m x k lo panel); dScale
  * receives per-row int8 exponents (E4M3/E5M2/FP16, scale = 2^e, m bytes) or
  * per-32-block E8M0 codes (MXFP8, m x ceil(k/32) bytes, row-major). */
 MPCHOL_API mpchol_status mpchol_quantize_rows(const float* dP, int m, int k, int ldp, int fmt, void* dQ,

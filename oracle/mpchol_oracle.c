@@ -30,7 +30,8 @@
 #endif
 
 /* Format ids shared with include/mpchol.h (MPCHOL_PREC_*). */
-enum { ORC_FP32 = 0, ORC_FP16 = 1, ORC_E4M3 = 2, ORC_E5M2 = 3, ORC_MXFP8 = 4, ORC_SWITCHING = 5 };
+enum { ORC_FP32 = 0, ORC_FP16 = 1, ORC_E4M3 = 2, ORC_E5M2 = 3, ORC_MXFP8 = 4, ORC_SWITCHING = 5,
+       ORC_FP16X2 = 6 };
 
 static inline uint32_t f2u(float x) { uint32_t u; memcpy(&u, &x, 4); return u; }
 static inline float u2f(uint32_t u) { float x; memcpy(&x, &u, 4); return x; }
@@ -140,7 +141,7 @@ int orc_row_scale_exp(float amax, int fmt) {
   switch (fmt) {
     case ORC_E4M3: emax = 8; mmax_bits = 0x600000u; break;    /* 1.75 * 2^8  = 448   */
     case ORC_E5M2: emax = 15; mmax_bits = 0x600000u; break;   /* 1.75 * 2^15 = 57344 */
-    case ORC_FP16: emax = 15; mmax_bits = 0x7fe000u; break;   /* 65504 */
+    case ORC_FP16: case ORC_FP16X2: emax = 15; mmax_bits = 0x7fe000u; break;   /* 65504 */
     default: return 0;
   }
   const int E = ilog2f(amax);
@@ -250,6 +251,7 @@ float orc_unit_roundoff(int fmt) {
     case ORC_E4M3: case ORC_MXFP8: return 0.0625f;    /* 2^-4 */
     case ORC_E5M2: return 0.125f;                     /* 2^-3 */
     case ORC_FP16: return 4.8828125e-4f;               /* 2^-11 */
+    case ORC_FP16X2: return 2.3841858e-7f;             /* 2^-22: hi + lo */
     default: return 5.9604645e-8f;                    /* 2^-24 */
   }
 }
@@ -356,6 +358,15 @@ static void quant_row(const float* row, int ld, int bs, int p, float* out) {
     float q;
     if (p == ORC_E4M3) q = orc_e4m3_to_f32(orc_f32_to_e4m3(v, 1));
     else if (p == ORC_E5M2) q = orc_e5m2_to_f32(orc_f32_to_e5m2(v, 1));
+    else if (p == ORC_FP16X2) {
+      /* two-term split: hi = fp16(v), lo = fp16(v - hi); the update uses
+       * hi hi^T + hi lo^T + lo hi^T, i.e. (hi+lo)(hi+lo)^T - lo lo^T; the
+       * dropped lo lo^T term is below the FP32 accumulation error, so the
+       * oracle uses hi + lo */
+      const float hi = orc_f16_to_f32(orc_f32_to_f16(v));
+      const float lo = orc_f16_to_f32(orc_f32_to_f16(v - hi));
+      q = hi + lo;
+    }
     else q = orc_f16_to_f32(orc_f32_to_f16(v));
     out[k] = q * sc;
   }

@@ -29,7 +29,7 @@ LIB = HERE / "_build" / "liboracle.so"
 REF_LOFLOAT = HERE / "_ref" / "libref_lofloat.so"
 REF_MICRO = HERE / "_ref" / "libref_micro.so"
 
-FP32, FP16, E4M3, E5M2, MXFP8, SWITCHING = range(6)
+FP32, FP16, E4M3, E5M2, MXFP8, SWITCHING, FP16X2 = range(7)
 
 _lib = None
 
@@ -164,7 +164,12 @@ def quantize_rows(P: np.ndarray, fmt: int) -> tuple[np.ndarray, np.ndarray]:
     amax = np.abs(P).max(axis=1) if k else np.zeros(m, np.float32)
     ex = np.array([row_scale_exp(a, fmt) for a in amax], dtype=np.int32)
     inv = np.ldexp(np.float32(1.0), -ex).astype(np.float32)[:, None]
-    codes = quantize((P * inv).astype(np.float32), fmt).reshape(m, k)
+    xs = (P * inv).astype(np.float32)
+    if fmt == FP16X2:
+        hi = quantize(xs, FP16).reshape(m, k)
+        lo = quantize((xs - decode(hi, FP16)).astype(np.float32), FP16).reshape(m, k)
+        return np.concatenate([hi, lo], axis=0), ex.astype(np.int8)
+    codes = quantize(xs, fmt).reshape(m, k)
     return codes, ex.astype(np.int8)
 
 

@@ -69,12 +69,14 @@ def gpu_quantize_rows(P: np.ndarray, fmt: int):
     lib = _lib.load()
     m, k = P.shape
     Pd = torch.from_numpy(np.asfortranarray(P).T.copy()).cuda()   # column-major storage
-    q = torch.zeros(m * k, dtype=torch.int16 if fmt == O.FP16 else torch.uint8, device="cuda")
+    half = fmt in (O.FP16, O.FP16X2)
+    q = torch.zeros(m * k * (2 if fmt == O.FP16X2 else 1), dtype=torch.int16 if half else torch.uint8,
+                    device="cuda")
     sc = torch.zeros(m * (k // 32 if fmt == O.MXFP8 else 1), dtype=torch.uint8, device="cuda")
     _lib.check(lib.mpchol_quantize_rows(Pd.data_ptr(), m, k, m, fmt, q.data_ptr(), sc.data_ptr(),
                                         stream()))
-    codes = q.cpu().numpy().reshape(m, k)
-    if fmt == O.FP16:
+    codes = q.cpu().numpy().reshape(-1, k)
+    if half:
         codes = codes.view(np.uint16)
     s = sc.cpu().numpy()
     s = s.reshape(m, k // 32) if fmt == O.MXFP8 else s.view(np.int8)
@@ -90,7 +92,7 @@ def panel(m, k, seed):
     return P
 
 
-@pytest.mark.parametrize("fmt", [O.E4M3, O.E5M2, O.FP16, O.MXFP8])
+@pytest.mark.parametrize("fmt", [O.E4M3, O.E5M2, O.FP16, O.MXFP8, O.FP16X2])
 @pytest.mark.parametrize("m,k", [(300, 256), (129, 128), (64, 64)])
 def test_quantize_rows_matches_oracle(cuda, fmt, m, k):
     P = panel(m, k, 7 + k)
@@ -104,6 +106,11 @@ def syrk_ref(C, Q, s, fmt, m, k):
     if fmt == O.MXFP8:
         vals = O.decode(Q, O.E4M3).astype(np.float64) * np.repeat(2.0 ** (s.astype(np.int64) - 127), 32, 1)
         prod = vals @ vals.T
+    elif fmt == O.FP16X2:
+        hi = O.decode(Q[:m], O.FP16).astype(np.float64)
+        lo = O.decode(Q[m:], O.FP16).astype(np.float64)
+        sc = 2.0 ** s.astype(np.float64)
+        prod = (hi @ hi.T + hi @ lo.T + lo @ hi.T) * sc[:, None] * sc[None, :]
     else:
         vals = O.decode(Q, fmt).astype(np.float64)
         sc = 2.0 ** s.astype(np.float64)
@@ -114,8 +121,8 @@ def syrk_ref(C, Q, s, fmt, m, k):
     return out
 
 
-@pytest.mark.parametrize("fmt", [O.E4M3, O.E5M2, O.FP16])
-@pytest.mark.parametrize("m,k", [(640, 256), (300, 128), (1000, 256)])
+@pytest.mark.parametrize("fmt", [O.E4M3, O.E5M2, O.FP16, O.FP16X2])
+@pytest.mark.parametrize("m,k", [(640, 256), (300, 128), (1000, 256), (2500, 256)])
 def test_tensor_core_syrk_matches_oracle(cuda, fmt, m, k):
     lib = _lib.load()
     P = panel(m, k, 3)
@@ -124,7 +131,7 @@ def test_tensor_core_syrk_matches_oracle(cuda, fmt, m, k):
     g = np.random.default_rng(4)
     C = g.standard_normal((m, m)).astype(np.float32)
     Cd = torch.from_numpy(C.T.copy()).cuda()    # column-major
-    Qd = torch.from_numpy(codes.view(np.int16) if fmt == O.FP16 else codes).cuda()
+    Qd = torch.from_numpy(codes.view(np.int16) if fmt in (O.FP16, O.FP16X2) else codes).cuda()
     Sd = torch.from_numpy(s.view(np.uint8)).cuda()
     _lib.check(lib.mpchol_syrk_update(Cd.data_ptr(), m, m, k, fmt, Qd.data_ptr(), Sd.data_ptr(),
                                       None, 0, stream()))
@@ -136,7 +143,7 @@ def test_tensor_core_syrk_matches_oracle(cuda, fmt, m, k):
     print(f"tc syrk fmt={fmt} m={m} k={k} max rel err {err:.3e}")
     # FP32 accumulation in TMEM; the FP8 MMA accumulates with reduced internal
     # precision, so its bar is looser.
-    assert err < (2e-6 if fmt == O.FP16 else 1e-4), err
+    assert err < (2e-6 if fmt in (O.FP16, O.FP16X2) else 1e-4), err
     # upper triangle untouched
     assert np.array_equal(got[~low], C[~low])
 

@@ -17,7 +17,8 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 # relative Frobenius bar of ||L_gpu - L_oracle|| / ||L_oracle|| per step precision
-FACTOR_TOL = {O.FP32: 1e-5, O.FP16: 1e-3, O.E4M3: 5e-2, O.E5M2: 5e-2, O.MXFP8: 5e-2}
+FACTOR_TOL = {O.FP32: 1e-5, O.FP16: 1e-3, O.E4M3: 5e-2, O.E5M2: 5e-2, O.MXFP8: 5e-2,
+              O.FP16X2: 1e-5}
 
 
 def factor_parity(A: np.ndarray, **opts):
@@ -41,6 +42,7 @@ def factor_parity(A: np.ndarray, **opts):
     (512, 256, "fp32"),
     (768, 256, "e4m3"),
     (640, 128, "e5m2"),
+    (1024, 256, "fp16x2"),  # split FP16: FP32-class factor on tensor cores
     (96, 256, "fp32"),      # n < b: a single diagonal block
 ])
 def test_factor_matches_oracle(cuda, n, b, prec):
@@ -116,6 +118,7 @@ def test_apply_precond_matches_oracle_potrs(cuda):
     (1024, 128, "fp16", 1e4, 1),     # plain-method workload
     (1024, 128, "fp32", 1e4, 2),
     (2048, 256, "switching", 1e6, 1),
+    (2048, 256, "fp16x2", 1e6, 1),
     (1000, 128, "fp32", 1e3, 8),
 ])
 def test_pcg_reaches_1e10_and_matches_dense_solve(cuda, n, b, prec, kappa, nrhs):
