@@ -50,6 +50,10 @@ def parse():
     ap.add_argument("--kappa", type=float, default=1e6)
     ap.add_argument("--block", type=int, default=256)
     ap.add_argument("--eps-prime", type=float, default=0.05)
+    ap.add_argument("--precision", default="switching",
+                    help="policy of the mixed arm: switching, e4m3, e5m2, fp16, fp16x2")
+    ap.add_argument("--ladder", default="e4m3,fp16,fp16x2",
+                    help="switching ladder, lowest precision first (FP32 is the fallback)")
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--max-it", type=int, default=400)
     ap.add_argument("--check-every", type=int, default=4)
@@ -159,8 +163,12 @@ def run_gpu(args, world, rank, local):
         return f, X, rep
 
     # factor objects are created outside the timed region (allocation is setup)
-    fobj = {p: mp.Factor(n, block_size=b, precision=p, eps_prime=args.eps_prime)
-            for p in ("switching", "fp32")}
+    # "switching" is the mixed-precision arm (its policy from --precision /
+    # --ladder), "fp32" the plain FP32-factor comparator
+    ladder = [x.strip() for x in args.ladder.split(",") if x.strip()]
+    fobj = {"switching": mp.Factor(n, block_size=b, precision=args.precision,
+                                   eps_prime=args.eps_prime, ladder=ladder),
+            "fp32": mp.Factor(n, block_size=b, precision="fp32")}
 
     def step(precision):
         f = fobj[precision]
@@ -271,7 +279,8 @@ def run_gpu(args, world, rank, local):
         "vs_baseline": None,
         "dtype": "e4m3/fp16/fp32 factor, fp64 pcg",
         "data": "synthetic (seeded Q diag(sigma) Q^T, geometric spectrum)",
-        "config": {"workload": f"spd n={n} kappa={args.kappa:g} block={b} switching eps'={args.eps_prime}",
+        "config": {"workload": (f"spd n={n} kappa={args.kappa:g} block={b} {args.precision}"
+                                f" ladder={args.ladder} eps'={args.eps_prime}"),
                    "n": n, "kappa": args.kappa, "block": b, "rhs": 1, "tol": args.tol,
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (A = %d MiB)" % (n * n * 4 // (1 << 20))},
@@ -280,8 +289,9 @@ def run_gpu(args, world, rank, local):
         "iterations": {"switching": r_sw[-1].iterations, "fp32": r_32[-1].iterations},
         "rel_residual": {"switching": r_sw[-1].rel_residual, "fp32": r_32[-1].rel_residual},
         "backward_error": {"switching": r_sw[-1].backward_error, "fp32": r_32[-1].backward_error},
-        "step_precisions": {"fp32": info_sw.steps_by_prec[0], "fp16": info_sw.steps_by_prec[1],
-                            "e4m3": info_sw.steps_by_prec[2], "e5m2": info_sw.steps_by_prec[3]},
+        "step_precisions": {nm: info_sw.steps_by_prec[i]
+                            for i, nm in ((0, "fp32"), (1, "fp16"), (2, "e4m3"), (3, "e5m2"),
+                                          (4, "mxfp8"), (6, "fp16x2"))},
         "phase_ms_switching_step": phases,
         "phase_calls_switching_step": calls,
         "e2e": {"value": round(e2e_ms, 3), "unit": "ms",
