@@ -49,7 +49,7 @@ def parse():
     ap.add_argument("--n", type=int, default=8192)
     ap.add_argument("--kappa", type=float, default=1e6)
     ap.add_argument("--block", type=int, default=256)
-    ap.add_argument("--eps-prime", type=float, default=0.05)
+    ap.add_argument("--eps-prime", type=float, default=1e-5)
     ap.add_argument("--precision", default="switching",
                     help="policy of the mixed arm: switching, e4m3, e5m2, fp16, fp16x2")
     ap.add_argument("--ladder", default="e4m3,fp16,fp16x2",

@@ -48,7 +48,13 @@ __device__ bool factor_diag_tile(T* t, T* inv, int lane, int nreal, const T* shi
     if (k < nreal) {
       piv += shift[k];
       if (diag_pert) {
-        if (!(piv > pmin[k])) { piv = pmin[k]; ++npert; }
+        // repair: max(|pivot|, floor), the reference's fixDiag rule
+        // (src/kernels_macros.cuh:90-99); a NaN pivot takes the floor
+        if (!(piv > pmin[k])) {
+          const T ap = piv < T(0) ? -piv : piv;
+          piv = (ap > pmin[k]) ? ap : pmin[k];
+          ++npert;
+        }
       } else if (!(piv > T(0))) {
         if (ok) *fail_row = k;
         ok = false;

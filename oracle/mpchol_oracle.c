@@ -309,7 +309,11 @@ int orc_choose_precision(const float* d, const float* dt, int m, const orc_chol_
       T piv = a[k + (size_t)k * ld];                                                  \
       if (shift) piv += shift[k];                                                     \
       if (pivmin) {                                                                   \
-        if (!(piv > pivmin[k])) { piv = pivmin[k]; ++*nperturbed; }                   \
+        if (!(piv > pivmin[k])) { /* max(|piv|, floor): fixDiag, src/kernels_macros.cuh:90-99 */ \
+          const T ap = piv < 0 ? -piv : piv;                                          \
+          piv = (ap > pivmin[k]) ? ap : pivmin[k];                                    \
+          ++*nperturbed;                                                              \
+        }                                                                             \
       } else if (!(piv > 0)) {                                                        \
         return k;                                                                     \
       }                                                                               \

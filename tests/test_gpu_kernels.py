@@ -143,7 +143,8 @@ def test_tensor_core_syrk_matches_oracle(cuda, fmt, m, k):
     print(f"tc syrk fmt={fmt} m={m} k={k} max rel err {err:.3e}")
     # FP32 accumulation in TMEM; the FP8 MMA accumulates with reduced internal
     # precision, so its bar is looser.
-    assert err < (2e-6 if fmt in (O.FP16, O.FP16X2) else 1e-4), err
+    # (FP16X2 accumulates three products per K step: slightly more rounding)
+    assert err < {O.FP16: 2e-6, O.FP16X2: 5e-6}.get(fmt, 1e-4), err
     # upper triangle untouched
     assert np.array_equal(got[~low], C[~low])
 

@@ -18,7 +18,7 @@ pytestmark = pytest.mark.gpu
 
 # relative Frobenius bar of ||L_gpu - L_oracle|| / ||L_oracle|| per step precision
 FACTOR_TOL = {O.FP32: 1e-5, O.FP16: 1e-3, O.E4M3: 5e-2, O.E5M2: 5e-2, O.MXFP8: 5e-2,
-              O.FP16X2: 1e-5}
+              O.FP16X2: 3e-5}
 
 
 def factor_parity(A: np.ndarray, **opts):
