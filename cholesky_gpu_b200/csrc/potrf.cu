@@ -28,11 +28,11 @@ constexpr int TSZ = TS * TS;    // elements per dense tile
 __device__ __forceinline__ int tidx(int I, int J) { return I * (I + 1) / 2 + J; }
 
 template <typename T>
-__device__ __forceinline__ T dsqrt(T x);
+__device__ __forceinline__ T drsqrt(T x);
 template <>
-__device__ __forceinline__ float dsqrt<float>(float x) { return sqrtf(x); }
+__device__ __forceinline__ float drsqrt<float>(float x) { return rsqrtf(x); }
 template <>
-__device__ __forceinline__ double dsqrt<double>(double x) { return sqrt(x); }
+__device__ __forceinline__ double drsqrt<double>(double x) { return rsqrt(x); }
 
 // Factor the 32 x 32 tile t in place (lower triangle).  inv[k] receives
 // 1 / L(k,k).  Returns false on a non-positive pivot when pivot flooring is
@@ -63,8 +63,10 @@ __device__ bool factor_diag_tile(T* t, T* inv, int lane, int nreal, const T* shi
     } else {
       piv = T(1);     // identity padding beyond the real block
     }
-    const T lkk = dsqrt<T>(piv);
-    const T rk = T(1) / lkk;
+    // one SFU reciprocal square root on the dependency chain: rk = 1/sqrt(piv),
+    // L(k,k) = piv * rk
+    const T rk = drsqrt<T>(piv);
+    const T lkk = piv * rk;
     const T lik = (lane > k) ? t[k * TS + lane] * rk : T(0);
     // batch: row `lane`, columns k+1..31 -- all loads before any store
     T v[TS - 1];
@@ -127,19 +129,22 @@ __device__ void syrk_tile(T* c, const T* a, const T* b, int lane) {
 }
 
 // Inverse of the lower-triangular tile l into out (32 x 32 column-major,
-// FP32).  Rows of W = L^-1 are formed in order (lane j owns column j);
-// w is a scratch tile holding W row-major.
+// FP32).  Rows of W = L^-1 are formed in order (lane j owns column j) in the
+// scratch tile w (row-major, row stride TS+1 so the transposing read below is
+// conflict-free), then written out with coalesced stores.
 template <typename T>
 __device__ void invert_tile(const T* l, const T* inv, T* w, float* out, int lane) {
+  constexpr int WLD = TS + 1;
 #pragma unroll 1
   for (int i = 0; i < TS; ++i) {
     T acc = (i == lane) ? T(1) : T(0);
 #pragma unroll 8
-    for (int k = 0; k < i; ++k) acc -= l[k * TS + i] * w[k * TS + lane];
-    const T v = (lane <= i) ? acc * inv[i] : T(0);
-    w[i * TS + lane] = v;
-    out[lane * TS + i] = (float)v;
+    for (int k = 0; k < i; ++k) acc -= l[k * TS + i] * w[k * WLD + lane];
+    w[i * WLD + lane] = (lane <= i) ? acc * inv[i] : T(0);
   }
+  __syncwarp();
+#pragma unroll 4
+  for (int c = 0; c < TS; ++c) out[c * TS + lane] = (float)w[lane * WLD + c];
 }
 
 template <typename T, bool TMA>
@@ -270,7 +275,7 @@ __device__ void potrf_block(const CUtensorMap* tmap, T* tiles, float* A, int lda
   }
   // inverses of the diagonal tiles, used by the panel solve
   for (int J = warp; J < NT; J += nwarps)
-    invert_tile<T>(tiles + tidx(J, J) * TSZ, s_inv + J * TS, scratch + J * TSZ,
+    invert_tile<T>(tiles + tidx(J, J) * TSZ, s_inv + J * TS, scratch + J * (TS * (TS + 1)),
                    winv + J * TS * TS, lane);
   if (tid == 0 && s_pert) atomicAdd(&st->perturbed, s_pert);
   if (TMA && tid == 0) tc::bulk_wait_read();   // smem must outlive the stores' reads
@@ -301,14 +306,12 @@ potrf_f64_kernel(float* A, int lda, int n, int s, int bs, const float* d, const 
 
 }  // namespace
 
-size_t potrf_smem_bytes(int bs) {
-  const int NT = (bs + TS - 1) / TS;
-  return ((size_t)NT * (NT + 1) / 2 + NT) * TSZ * sizeof(float);
-}
+// lower tiles + one padded (32 x 33) scratch tile per diagonal tile
 size_t potrf_scratch64_elems(int bs) {
   const int NT = (bs + TS - 1) / TS;
-  return ((size_t)NT * (NT + 1) / 2 + NT) * TSZ;
+  return (size_t)NT * (NT + 1) / 2 * TSZ + (size_t)NT * TS * (TS + 1);
 }
+size_t potrf_smem_bytes(int bs) { return potrf_scratch64_elems(bs) * sizeof(float); }
 
 cudaError_t launch_potrf(const CUtensorMap& tmap32, float* A, int lda, int n, int s, int bs,
                          const float* d, const float* sh, const PotrfParams& p,
