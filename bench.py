@@ -53,7 +53,8 @@ def parse():
     ap.add_argument("--precision", default="switching",
                     help="policy of the mixed arm: switching, e4m3, e5m2, fp16, fp16x2")
     ap.add_argument("--ladder", default="e4m3,fp16,fp16x2",
-                    help="switching ladder, lowest precision first (FP32 is the fallback)")
+                    help="switching ladder, lowest precision first (its last entry is the "
+                         "fallback)")
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--max-it", type=int, default=400)
     ap.add_argument("--check-every", type=int, default=4)
@@ -70,18 +71,46 @@ def dist_init(args):
 
 # ---------------------------------------------------------------- clocks
 class ClockSampler:
-    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+    """SM clock and throttle-reason sampling during a region (NVML reads every
+    10 ms from a thread; nvidia-smi -lms 200 if NVML is not importable)."""
 
+    REASONS = {"hw_slowdown": "nvmlClocksEventReasonHwSlowdown",
+               "hw_thermal_slowdown": "nvmlClocksEventReasonHwThermalSlowdown",
+               "sw_thermal_slowdown": "nvmlClocksEventReasonSwThermalSlowdown",
+               "sw_power_cap": "nvmlClocksEventReasonSwPowerCap"}
+    FALLBACK_BITS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40,
+                     "sw_thermal_slowdown": 0x20, "sw_power_cap": 0x4}
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index: int):
+    def __init__(self, index: int, pci_bus_id: str | None = None):
         self.index = index
+        self.pci = pci_bus_id
         self.proc = None
-        self.lines = []
+        self.nvml = None
+        self.samples = []          # (sm_mhz, max_mhz, set of reasons)
+        self.stop = threading.Event()
 
     def __enter__(self):
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            h = None
+            if self.pci:
+                try:
+                    h = nv.nvmlDeviceGetHandleByPciBusId(self.pci)
+                except Exception:
+                    h = None
+            if h is None:
+                h = nv.nvmlDeviceGetHandleByIndex(self.index)
+            self.nvml, self.h = nv, h
+            self.bits = {k: getattr(nv, v, self.FALLBACK_BITS[k]) for k, v in self.REASONS.items()}
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+            return self
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
@@ -93,44 +122,77 @@ class ClockSampler:
             self.proc = None
         return self
 
+    def _poll(self):
+        nv, h = self.nvml, self.h
+        while not self.stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((float(sm), float(mx),
+                                     {k for k, bit in self.bits.items() if r & bit}))
+            except Exception:
+                return
+            time.sleep(0.01)
+
     def _read(self):
+        names = list(self.FALLBACK_BITS)
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            parts = [p.strip() for p in line.strip().split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                self.samples.append((float(parts[0]), float(parts[1]),
+                                     {nm for nm, v in zip(names, parts[4:8])
+                                      if v.lower() == "active"}))
+            except ValueError:
+                continue
 
     def __exit__(self, *exc):
+        self.stop.set()
         if self.proc is not None:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
+        elif self.nvml is not None:
+            self.t.join(timeout=1.0)
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 8:
-                continue
-            try:
-                sm.append(float(parts[0]))
-                mx = float(parts[1])
-            except ValueError:
-                continue
-            for nm, v in zip(names, parts[4:8]):
-                if v.lower() == "active":
-                    reasons.add(nm)
+        sm = [s[0] for s in self.samples]
+        mx = self.samples[-1][1] if self.samples else None
+        reasons = set().union(*[s[2] for s in self.samples]) if self.samples else set()
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm),
+                "source": "nvml" if self.nvml is not None else "nvidia-smi"}
 
 
 # ---------------------------------------------------------------- peaks
 def measured_peaks():
+    """(HBM GB/s, dense bf16 TFLOP/s burst, kind): the driver-measured copy
+    bandwidth and cuBLAS bf16 rate of this GPU type, else the pool fallback."""
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
         d = json.loads(p.read_text())
-        return d.get("hbm_gbs", 6650.0), "measured"
-    return 6650.0, "fallback"
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+def profiled_traffic(kernel: str, n: int):
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum)
+    recorded from an ncu capture in profiles/<kernel>_n<n>.txt as a line
+    'traffic_bytes_per_launch: <int>', or None."""
+    p = ROOT / "profiles" / f"{kernel}_n{n}.txt"
+    if not p.exists():
+        return None
+    for ln in p.read_text().splitlines():
+        if ln.startswith("traffic_bytes_per_launch:"):
+            try:
+                return int(ln.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
 
 
 # ---------------------------------------------------------------- GPU arm
@@ -196,7 +258,7 @@ def run_gpu(args, world, rank, local):
         step("switching")
         step("fp32")
     launches0 = lib.mpchol_kernel_launches()
-    with ClockSampler(local) as clk:
+    with ClockSampler(local, getattr(torch.cuda.get_device_properties(local), "pci_bus_id", None)) as clk:
         t_sw, r_sw = timed("switching", args.steps)
         launches_sw = lib.mpchol_kernel_launches() - launches0
         t_32, r_32 = timed("fp32", args.steps)
@@ -243,28 +305,55 @@ def run_gpu(args, world, rank, local):
     phases = {nm: round(prof.ms[i], 4) for i, nm in enumerate(_lib.PHASE_NAMES) if prof.calls[i]}
     calls = {nm: int(prof.calls[i]) for i, nm in enumerate(_lib.PHASE_NAMES) if prof.calls[i]}
 
-    # roofline of the dominant kernel group (PCG preconditioner solves or SYRK)
-    hbm, peak_kind = measured_peaks()
-    it = rep_p.iterations
-    dom = max(phases, key=phases.get)
-    nb128 = (n + 127) // 128
-    if dom == "trsv":
-        # one triangular solve reads the lower triangle of L (FP32) + the 128x128
-        # FP32 diagonal-block inverses, and reads/writes the n-vectors (FP64)
-        per_launch = (n * (n + 1) / 2) * 4 + nb128 * 128 * 128 * 4 + 3 * n * 8
-        achieved = per_launch / (phases[dom] / calls[dom] * 1e-3) / 1e9
-        bound, unit, peak = "hbm", "GB/s", hbm
-    elif dom == "symv":
-        per_launch = (n * (n + 1) / 2) * 4 + 2 * n * 8
-        achieved = per_launch / (phases[dom] / calls[dom] * 1e-3) / 1e9
-        bound, unit, peak = "hbm", "GB/s", hbm
+    # rooflines of the bandwidth- and tensor-bound phases of the profiled step;
+    # the headline one is the phase with the largest device time
+    hbm, bf16, peak_kind = measured_peaks()
+    info_p = fobj["switching"].info()
+    tc_flops, tc_exec, tc_fmts = 0.0, 0, {}
+    for k, pr in enumerate(info_p.step_prec):
+        s0 = k * b
+        bs = min(b, n - s0)
+        m = n - s0 - bs
+        if m <= 0:
+            break
+        if pr != _lib.PREC_FP32:
+            tc_flops += float(m) * (m + 1) * bs       # lower triangle, algorithmic
+            tc_exec += 1
+            tc_fmts[pr] = tc_fmts.get(pr, 0) + 1
+    by_phase = {}
+
+    def add(name, bound, unit, peak, work, launches, note):
+        if name not in phases or launches <= 0:
+            return
+        sec = phases[name] * 1e-3
+        scale = 1e9 if unit == "GB/s" else 1e12
+        achieved = work * launches / sec / scale
+        by_phase[name] = {"bound": bound, "unit": unit, "achieved": round(achieved, 1),
+                          "peak": peak, "frac": round(achieved / peak, 4),
+                          "work_per_launch": work, "launches": launches,
+                          "ms": phases[name], "note": note}
+
+    tri = n * (n + 1) / 2 * 4 + 3 * n * 8
+    add("trsv", "hbm", "GB/s", hbm, tri, calls.get("trsv", 0),
+        "one triangular solve: lower triangle of L in FP32 + FP64 vectors")
+    add("symv", "hbm", "GB/s", hbm, n * (n + 1) / 2 * 4 + 2 * n * 8, calls.get("symv", 0),
+        "A x from the lower triangle of A in FP32, FP64 vectors")
+    if tc_exec:
+        fp8 = sum(v for k_, v in tc_fmts.items() if k_ in (_lib.PREC_E4M3, _lib.PREC_E5M2))
+        tpeak = 2 * bf16 if fp8 * 2 > tc_exec else bf16
+        add("syrk_tc", "tensor", "TFLOP/s", tpeak, tc_flops / tc_exec, tc_exec,
+            "trailing update m(m+1)b useful flops per executing launch; FP16X2 issues 3x; "
+            "peak: measured bf16 rate" + (" x2 (FP8 steps)" if tpeak != bf16 else ""))
+    dom = max(by_phase, key=lambda k_: by_phase[k_]["ms"]) if by_phase else None
+    if dom:
+        r = by_phase[dom]
+        roof = {"kernel": dom, "bound": r["bound"], "achieved": r["achieved"], "peak": r["peak"],
+                "peak_kind": peak_kind, "unit": r["unit"], "frac": r["frac"],
+                "algorithmic_per_launch": r["work_per_launch"],
+                "traffic": profiled_traffic(dom, n), "by_phase": by_phase}
     else:
-        per_launch = None
-        achieved, bound, unit, peak = None, "hbm", "GB/s", hbm
-    roof = {"kernel": dom, "bound": bound, "achieved": achieved and round(achieved, 1),
-            "peak": peak, "peak_kind": peak_kind, "unit": unit,
-            "frac": achieved and round(achieved / peak, 4),
-            "algorithmic_bytes_per_launch": per_launch, "traffic": None}
+        roof = {"kernel": None, "bound": "hbm", "achieved": None, "peak": hbm,
+                "peak_kind": peak_kind, "unit": "GB/s", "frac": None, "traffic": None}
 
     result = {
         "metric": METRIC,
@@ -277,7 +366,9 @@ def run_gpu(args, world, rank, local):
         "higher_is_better": False,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "e4m3/fp16/fp32 factor, fp64 pcg",
+        "dtype": "%s factor, fp64 pcg" % "/".join(
+            nm for i, nm in ((2, "e4m3"), (3, "e5m2"), (1, "fp16"), (6, "fp16x2"), (0, "fp32"))
+            if info_sw.steps_by_prec[i]),
         "data": "synthetic (seeded Q diag(sigma) Q^T, geometric spectrum)",
         "config": {"workload": (f"spd n={n} kappa={args.kappa:g} block={b} {args.precision}"
                                 f" ladder={args.ladder} eps'={args.eps_prime}"),

@@ -218,11 +218,14 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream) {
   PHASE(MPCHOL_PH_SETUP, 1, stream, launch_extract_diag(f->A, ld, n, f->d, f->dtilde, stream));
   const bool fixed = o.precision != MPCHOL_PREC_SWITCHING;
   std::vector<int> tc_fmts;
+  bool f32_possible = fixed || o.switch_mode == 1 || o.ladder_len == 0;
   if (!fixed) {
     if (o.switch_mode == 1) tc_fmts = {FP16, E4M3};
     else
-      for (int i = 0; i < o.ladder_len; ++i)
+      for (int i = 0; i < o.ladder_len; ++i) {
         if (o.ladder[i] != FP32) tc_fmts.push_back(o.ladder[i]);
+        else f32_possible = true;
+      }
   }
   for (int k = 0; k < f->nsteps; ++k) {
     const int s = k * b;
@@ -250,7 +253,8 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream) {
                                        bs / 32, nullptr, f->status, stream));
     } else {
       const int* sel = &f->steps[k].prec;
-      PHASE(MPCHOL_PH_SYRK_F32, 1, stream, launch_syrk_f32(C, ld, m, bs, P, ld, sel, f->status, stream));
+      if (f32_possible)
+        PHASE(MPCHOL_PH_SYRK_F32, 1, stream, launch_syrk_f32(C, ld, m, bs, P, ld, sel, f->status, stream));
       for (int fmt : tc_fmts)
         PHASE(MPCHOL_PH_SYRK_TC, 1, stream, launch_syrk_tc(C, ld, m, bs, fmt, f->q, bs, f->rowexp, f->mxexp, bs / 32,
                                        sel, f->status, stream));

@@ -37,58 +37,66 @@ __device__ __forceinline__ double drsqrt<double>(double x) { return rsqrt(x); }
 // Factor the 32 x 32 tile t in place (lower triangle).  inv[k] receives
 // 1 / L(k,k).  Returns false on a non-positive pivot when pivot flooring is
 // off (first failing local row in *fail_row).
+//
+// Lane i holds row i of the tile in registers for the whole factorization (the
+// column loop is unrolled so every register index is a constant): per column
+// lane k forms and repairs the pivot, one shuffle broadcasts 1/sqrt(pivot),
+// and the rank-1 update takes the column's multipliers by shuffles.  Shared
+// memory is read once and the lower triangle written once.
 template <typename T>
 __device__ bool factor_diag_tile(T* t, T* inv, int lane, int nreal, const T* shift, const T* pmin,
                                  int diag_pert, int* nperturbed, int* fail_row) {
-  bool ok = true;
-  int npert = 0;
-#pragma unroll 1
+  T a[TS];
+#pragma unroll
+  for (int j = 0; j < TS; ++j) a[j] = t[j * TS + lane];
+  const T my_shift = (lane < nreal) ? shift[lane] : T(0);
+  const T my_pmin = pmin[lane];
+  bool failed = false, perturbed = false;
+  T my_inv = T(1);
+#pragma unroll
   for (int k = 0; k < TS; ++k) {
-    T piv = t[k * TS + k];
-    if (k < nreal) {
-      piv += shift[k];
-      if (diag_pert) {
-        // repair: max(|pivot|, floor), the reference's fixDiag rule
-        // (src/kernels_macros.cuh:90-99); a NaN pivot takes the floor
-        if (!(piv > pmin[k])) {
-          const T ap = piv < T(0) ? -piv : piv;
-          piv = (ap > pmin[k]) ? ap : pmin[k];
-          ++npert;
+    T rk = T(1);
+    if (lane == k) {
+      T piv = a[k];
+      if (k < nreal) {
+        piv += my_shift;
+        if (diag_pert) {
+          // repair: max(|pivot|, floor), the reference's fixDiag rule
+          // (src/kernels_macros.cuh:90-99); a NaN pivot takes the floor
+          if (!(piv > my_pmin)) {
+            const T ap = piv < T(0) ? -piv : piv;
+            piv = (ap > my_pmin) ? ap : my_pmin;
+            perturbed = true;
+          }
+        } else if (!(piv > T(0))) {
+          failed = true;
+          piv = T(1);   // keep the arithmetic finite; the caller discards the result
         }
-      } else if (!(piv > T(0))) {
-        if (ok) *fail_row = k;
-        ok = false;
-        piv = T(1);   // keep the arithmetic finite; the caller discards the result
+      } else {
+        piv = T(1);     // identity padding beyond the real block
       }
-    } else {
-      piv = T(1);     // identity padding beyond the real block
+      // one SFU reciprocal square root on the dependency chain:
+      // rk = 1/sqrt(piv), L(k,k) = piv * rk
+      rk = drsqrt<T>(piv);
+      a[k] = piv * rk;
+      my_inv = rk;
     }
-    // one SFU reciprocal square root on the dependency chain: rk = 1/sqrt(piv),
-    // L(k,k) = piv * rk
-    const T rk = drsqrt<T>(piv);
-    const T lkk = piv * rk;
-    const T lik = (lane > k) ? t[k * TS + lane] * rk : T(0);
-    // batch: row `lane`, columns k+1..31 -- all loads before any store
-    T v[TS - 1];
-    T l[TS - 1];
+    rk = __shfl_sync(0xffffffffu, rk, k);
+    const T lik = (lane > k) ? a[k] * rk : T(0);
+    if (lane > k) a[k] = lik;
 #pragma unroll
-    for (int q = 0; q < TS - 1; ++q) {
-      const int j = k + 1 + q;
-      l[q] = __shfl_sync(0xffffffffu, lik, j & (TS - 1));
-      v[q] = (j < TS) ? t[j * TS + lane] : T(0);
-    }
-    __syncwarp();
-    if (lane == k) { t[k * TS + k] = lkk; inv[k] = rk; }
-    else if (lane > k) t[k * TS + lane] = lik;
-#pragma unroll
-    for (int q = 0; q < TS - 1; ++q) {
-      const int j = k + 1 + q;
-      if (j < TS && j <= lane) t[j * TS + lane] = v[q] - lik * l[q];
-    }
-    __syncwarp();
+    for (int j = k + 1; j < TS; ++j) a[j] -= lik * __shfl_sync(0xffffffffu, lik, j);
   }
-  if (lane == 0) *nperturbed += npert;
-  return ok;
+#pragma unroll
+  for (int j = 0; j < TS; ++j)
+    if (j <= lane) t[j * TS + lane] = a[j];
+  inv[lane] = my_inv;
+  const unsigned fm = __ballot_sync(0xffffffffu, failed);
+  const unsigned pm = __ballot_sync(0xffffffffu, perturbed);
+  if (fm) *fail_row = __ffs(fm) - 1;
+  if (lane == 0) *nperturbed += __popc(pm);
+  __syncwarp();
+  return fm == 0;
 }
 
 // X L^T = B for one tile (B in x, overwritten); lane i owns row i.
@@ -129,22 +137,24 @@ __device__ void syrk_tile(T* c, const T* a, const T* b, int lane) {
 }
 
 // Inverse of the lower-triangular tile l into out (32 x 32 column-major,
-// FP32).  Rows of W = L^-1 are formed in order (lane j owns column j) in the
-// scratch tile w (row-major, row stride TS+1 so the transposing read below is
-// conflict-free), then written out with coalesced stores.
+// FP32).  Lane j solves L w = e_j for column j of L^-1, right-looking with the
+// column held in registers; the column of L used at each step is a shared
+// broadcast.  Each lane then stores its column as 16-byte vectors.
 template <typename T>
-__device__ void invert_tile(const T* l, const T* inv, T* w, float* out, int lane) {
-  constexpr int WLD = TS + 1;
-#pragma unroll 1
-  for (int i = 0; i < TS; ++i) {
-    T acc = (i == lane) ? T(1) : T(0);
-#pragma unroll 8
-    for (int k = 0; k < i; ++k) acc -= l[k * TS + i] * w[k * WLD + lane];
-    w[i * WLD + lane] = (lane <= i) ? acc * inv[i] : T(0);
+__device__ void invert_tile(const T* l, const T* inv, float* out, int lane) {
+  T w[TS];
+#pragma unroll
+  for (int i = 0; i < TS; ++i) w[i] = (i == lane) ? T(1) : T(0);
+#pragma unroll
+  for (int k = 0; k < TS; ++k) {
+    w[k] *= inv[k];
+#pragma unroll
+    for (int i = k + 1; i < TS; ++i) w[i] -= l[k * TS + i] * w[k];
   }
-  __syncwarp();
-#pragma unroll 4
-  for (int c = 0; c < TS; ++c) out[c * TS + lane] = (float)w[lane * WLD + c];
+  float4* o = reinterpret_cast<float4*>(out + lane * TS);
+#pragma unroll
+  for (int q = 0; q < TS / 4; ++q)
+    o[q] = make_float4((float)w[4 * q], (float)w[4 * q + 1], (float)w[4 * q + 2], (float)w[4 * q + 3]);
 }
 
 template <typename T, bool TMA>
@@ -154,7 +164,6 @@ __device__ void potrf_block(const CUtensorMap* tmap, T* tiles, float* A, int lda
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
   const int NT = (bs + TS - 1) / TS;
   const int ntiles = NT * (NT + 1) / 2;
-  T* scratch = tiles + ntiles * TSZ;       // NT tiles for the inverses
   __shared__ T s_shift[256];
   __shared__ T s_pmin[256];
   __shared__ T s_inv[256];
@@ -275,8 +284,7 @@ __device__ void potrf_block(const CUtensorMap* tmap, T* tiles, float* A, int lda
   }
   // inverses of the diagonal tiles, used by the panel solve
   for (int J = warp; J < NT; J += nwarps)
-    invert_tile<T>(tiles + tidx(J, J) * TSZ, s_inv + J * TS, scratch + J * (TS * (TS + 1)),
-                   winv + J * TS * TS, lane);
+    invert_tile<T>(tiles + tidx(J, J) * TSZ, s_inv + J * TS, winv + J * TS * TS, lane);
   if (tid == 0 && s_pert) atomicAdd(&st->perturbed, s_pert);
   if (TMA && tid == 0) tc::bulk_wait_read();   // smem must outlive the stores' reads
   (void)n;
@@ -306,10 +314,10 @@ potrf_f64_kernel(float* A, int lda, int n, int s, int bs, const float* d, const 
 
 }  // namespace
 
-// lower tiles + one padded (32 x 33) scratch tile per diagonal tile
+// the lower tiles of the block
 size_t potrf_scratch64_elems(int bs) {
   const int NT = (bs + TS - 1) / TS;
-  return (size_t)NT * (NT + 1) / 2 * TSZ + (size_t)NT * TS * (TS + 1);
+  return (size_t)NT * (NT + 1) / 2 * TSZ;
 }
 size_t potrf_smem_bytes(int bs) { return potrf_scratch64_elems(bs) * sizeof(float); }
 

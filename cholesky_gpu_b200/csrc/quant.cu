@@ -29,7 +29,8 @@ __device__ __forceinline__ int resolve_precision(const StepState* step, const De
     const int p = dp.ladder[k];
     if (unit_roundoff(p) * ratio <= dp.eps_prime) return p;
   }
-  return FP32;
+  // no entry meets the bound: the ladder's most precise (last) entry
+  return dp.ladder_len > 0 ? dp.ladder[dp.ladder_len - 1] : FP32;
 }
 
 // Quantize one CTA tile of QROWS rows x k columns.  Lane l of a warp owns the

@@ -75,7 +75,8 @@ typedef struct {
   float pivot_floor;   /* diag_pert: pivots <= pivot_floor * d_i are raised to pivot_floor * d_i */
   int switch_mode;     /* 0: build criterion (lowest ladder precision with u_p*max(d/dtilde) <= eps');
                           1: reference-literal can_switch comparison (src/kernels_macros.cuh:191-211) */
-  int ladder_len;      /* switching ladder, lowest precision first (default {E4M3, FP16, FP32}) */
+  int ladder_len;      /* switching ladder, lowest precision first (default {E4M3, FP16, FP32});
+                          a step no entry qualifies for takes the last (most precise) entry */
   int ladder[4];
   int left;            /* 0: right-looking (only value built); settings.json "left" */
 } mpchol_opts;

@@ -268,7 +268,7 @@ static float ref_mach_eps(int fmt) {
 /*
  * Step precision choice.  mode 0 (build criterion): the first ladder entry p
  * (lowest precision first) with u_p * max_i d_i / dtilde_i <= eps_prime over
- * the trailing rows; FP32 if none.  mode 1 (reference-literal): per row, the
+ * the trailing rows; the last (most precise) entry if none.  mode 1 (reference-literal): per row, the
  * first entry of the reference list {FP32, FP16, E4M3} with
  * mach_eps_p * dtilde_i >= eps_prime * d_i (src/kernels_macros.cuh:191-211);
  * rows with no match choose FP32; the step takes the most precise row choice.
@@ -296,7 +296,7 @@ int orc_choose_precision(const float* d, const float* dt, int m, const orc_chol_
     const int p = o->ladder[k];
     if (orc_unit_roundoff(p) * ratio <= o->eps_prime) return p;
   }
-  return ORC_FP32;
+  return o->ladder_len > 0 ? o->ladder[o->ladder_len - 1] : ORC_FP32;
 }
 
 /* Unblocked right-looking POTRF of an nb x nb column-major block (lower),

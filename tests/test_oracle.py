@@ -144,6 +144,12 @@ def test_switching_rule_picks_lowest_admissible_precision():
     assert O.choose_precision(d, dt, eps_prime=1e-5) == O.FP32
     dt[3] = 0.0   # exhausted pivot forbids everything but FP32
     assert O.choose_precision(d, dt, eps_prime=100.0) == O.FP32
+    # a ladder without FP32 falls back to its own most precise (last) entry
+    dt[3] = 0.5
+    lad = (O.E4M3, O.FP16, O.FP16X2)
+    assert O.choose_precision(d, dt, eps_prime=1e-9, ladder=lad) == O.FP16X2
+    assert O.choose_precision(d, dt, eps_prime=1e-6, ladder=lad) == O.FP16X2
+    assert O.choose_precision(d, dt, eps_prime=0.2, ladder=lad) == O.E4M3
 
 
 def test_reference_literal_rule():
