@@ -97,9 +97,9 @@ class ClockSampler:
             import pynvml as nv
             nv.nvmlInit()
             h = None
-            if self.pci:
+            if isinstance(self.pci, str):
                 try:
-                    h = nv.nvmlDeviceGetHandleByPciBusId(self.pci)
+                    h = nv.nvmlDeviceGetHandleByPciBusId(self.pci.encode())
                 except Exception:
                     h = None
             if h is None:
@@ -166,6 +166,15 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
                 "reasons": sorted(reasons), "samples": len(sm),
                 "source": "nvml" if self.nvml is not None else "nvidia-smi"}
+
+
+def pci_bus_id(torch, index: int):
+    """NVML-style PCI bus id string ("DDDDDDDD:BB:DD.0") of a CUDA device."""
+    p = torch.cuda.get_device_properties(index)
+    ids = [getattr(p, k, None) for k in ("pci_domain_id", "pci_bus_id", "pci_device_id")]
+    if not all(isinstance(v, int) for v in ids):
+        return None
+    return "%08X:%02X:%02X.0" % tuple(ids)
 
 
 # ---------------------------------------------------------------- peaks
@@ -258,7 +267,7 @@ def run_gpu(args, world, rank, local):
         step("switching")
         step("fp32")
     launches0 = lib.mpchol_kernel_launches()
-    with ClockSampler(local, getattr(torch.cuda.get_device_properties(local), "pci_bus_id", None)) as clk:
+    with ClockSampler(local, pci_bus_id(torch, local)) as clk:
         t_sw, r_sw = timed("switching", args.steps)
         launches_sw = lib.mpchol_kernel_launches() - launches0
         t_32, r_32 = timed("fp32", args.steps)

@@ -133,7 +133,6 @@ struct mpchol_factor {
   StepState* steps = nullptr;
   DevStatus* status = nullptr;
   // solve side
-  float* blkinv = nullptr;    // inverses of the 128-row diagonal blocks
   float* wsup = nullptr;      // inverses of the 1024-row diagonal super-blocks
   bool solve_ready = false;
   // PCG workspace (sized for 8 rhs)
@@ -184,7 +183,7 @@ cudaError_t dmalloc(T** p, size_t count) {
 void free_factor(mpchol_factor_t* f) {
   if (f == nullptr) return;
   void* ptrs[] = {f->A, f->d, f->dtilde, f->rowsq, f->sh, f->winv, f->scratch64, f->q,
-                  f->rowexp, f->mxexp, f->steps, f->status, f->blkinv, f->wsup,
+                  f->rowexp, f->mxexp, f->steps, f->status, f->wsup,
                   f->vec, f->partials, f->scal, f->done};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -267,7 +266,7 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream) {
 mpchol_status ensure_solve(mpchol_factor_t* f, cudaStream_t stream) {
   if (f->solve_ready) return MPCHOL_OK;
   PHASE(MPCHOL_PH_SETUP, solve_setup_launches(f->n), stream,
-        launch_solve_setup(f->A, f->ld, f->n, f->blkinv, f->wsup, stream));
+        launch_solve_setup(f->A, f->ld, f->n, f->wsup, stream));
   f->solve_ready = true;
   return MPCHOL_OK;
 }
@@ -593,7 +592,6 @@ mpchol_status mpchol_factor_create(const mpchol_opts* opts, int n, mpchol_factor
             dmalloc(&f->mxexp, (size_t)n * (f->b / 32)) == cudaSuccess &&
             dmalloc(&f->steps, f->nsteps + 1) == cudaSuccess &&
             dmalloc(&f->status, 1) == cudaSuccess &&
-            dmalloc(&f->blkinv, solve_winv_elems(n)) == cudaSuccess &&
             dmalloc(&f->wsup, solve_wsup_elems(n)) == cudaSuccess &&
             dmalloc(&f->vec, 8 * nv) == cudaSuccess &&
             dmalloc(&f->partials, (size_t)4 * pcg_vgrid() * 8) == cudaSuccess &&

@@ -11,14 +11,12 @@ int pcg_vgrid();                 // CTAs of the reduction kernels (partials per 
 cudaError_t solve_init_attributes();
 int solve_super_rows();
 size_t solve_wsup_elems(int n);
-size_t solve_winv_elems(int n);
 int solve_setup_launches(int n);
 template <typename TA>
 cudaError_t launch_symv_skip(const TA* A, int lda, int n, const double* x, double* y, int nrhs,
                              const int* skip, cudaStream_t stream);
 // 128-block inverses into winv, then the super-block inverses into wsup.
-cudaError_t launch_solve_setup(const float* L, int ldl, int n, float* winv, float* wsup,
-                               cudaStream_t stream);
+cudaError_t launch_solve_setup(const float* L, int ldl, int n, float* wsup, cudaStream_t stream);
 // out = L^-1 in (forward) or L^-T in (backward); work is an n x nrhs scratch.
 // *launches receives the number of kernels launched.
 cudaError_t launch_trsv_super(bool backward, const float* L, int ldl, int n, const float* wsup,

@@ -8,7 +8,8 @@
 // Triangular solves.  A row-by-row (or 128-block-by-block) substitution is a
 // chain of n/128 dependent steps and runs at a few GB/s on one B200.  Instead,
 // once per factor, the inverses W_S of the 1024-row diagonal super-blocks
-// L_SS are formed (FP32, from FP64 128-block inverses and FP32 GEMMs).  A
+// L_SS are formed by recursive doubling (FP64 128-block inverses, FP32 GEMM
+// tiles above that).  A
 // forward solve is then n/1024 steps of two fully parallel kernels:
 //     y_S  = W_S w_S                      (TRMV over the super-block's lower tiles)
 //     w_T -= L_TS y_S   for T > S         (GEMV over the panel below)
@@ -198,57 +199,111 @@ symv_kernel(const TA* __restrict__ A, int lda, int n, const double* __restrict__
   flush_rows<NR>(acc, s_red, y, n, i0, ni, 1.0);
 }
 
-// ---- setup: 128-block inverses (FP64 arithmetic, FP32 result) ------------
-// winv + I*RB*RB = inv(L_II), column-major, padded with identity past n.
-__global__ void __launch_bounds__(RB)
-block_inverse_kernel(const float* __restrict__ L, int ldl, int n, float* __restrict__ winv) {
+// ---- setup: super-block inverses by recursive doubling ---------------------
+// For a lower-triangular [A 0; B C], inv = [A^-1 0; X C^-1] with
+// X = -C^-1 (B A^-1).  The inverses W_S of the RS-row diagonal super-blocks
+// are built bottom-up: the 128-row diagonal blocks in FP64 inside one CTA each
+// (32-row tiles, then the 32 -> 64 -> 128 doublings), then the 128 -> 1024
+// doublings as 128 x 128 FP32 GEMM tiles over all super-blocks at once.
+// Storage: W_S is RS x RS column-major at wsup + S*RS*RS.  Its lower 128-tiles
+// hold the inverse (diagonal tiles with a zero upper part); the strictly
+// upper 128-tiles are scratch for the doubling products T = B A^-1 and are
+// never read by the solves.
+
+constexpr int BLD = RB + 1;     // padded column stride of the shared tiles
+
+// One 128-row diagonal block per CTA (256 threads), FP64 in shared memory;
+// the FP32 result goes to its diagonal tile of W_S.  Rows and columns past n
+// are identity.
+__global__ void __launch_bounds__(NTH)
+block_inverse_kernel(const float* __restrict__ L, int ldl, int n, float* __restrict__ wsup) {
   extern __shared__ __align__(16) unsigned char sm_raw[];
-  double* W = reinterpret_cast<double*>(sm_raw);            // [RB][RB+1]
-  float* Ls = reinterpret_cast<float*>(W + RB * (RB + 1));  // [RB][RB+1]
-  const int I = blockIdx.x, c = threadIdx.x;
-  const int i0 = I * RB;
+  double* W = reinterpret_cast<double*>(sm_raw);            // [RB][BLD], column-major
+  float* Ls = reinterpret_cast<float*>(W + RB * BLD);        // [RB][BLD], column-major
+  const int g = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int i0 = g * RB;
   const int nb = min(RB, n - i0);
-  for (int e = c; e < RB * RB; e += RB) {
+  for (int e = tid; e < RB * RB; e += NTH) {
     const int col = e / RB, row = e % RB;
     float v;
-    if (row < nb && col < nb) v = L[(size_t)(i0 + col) * ldl + i0 + row];
+    if (row < nb && col < nb) v = (row >= col) ? L[(size_t)(i0 + col) * ldl + i0 + row] : 0.0f;
     else v = (row == col) ? 1.0f : 0.0f;
-    Ls[col * (RB + 1) + row] = v;
+    Ls[col * BLD + row] = v;
+    W[col * BLD + row] = 0.0;
   }
   __syncthreads();
-  for (int i = 0; i < RB; ++i) {
-    double w = 0.0;
-    if (i >= c) {
-      double acc = (i == c) ? 1.0 : 0.0;
-      for (int k = c; k < i; ++k) acc -= (double)Ls[k * (RB + 1) + i] * W[c * (RB + 1) + k];
-      w = acc / (double)Ls[i * (RB + 1) + i];
+  // 32-row diagonal tiles: warp t, lane j solves L_tt w = e_j (right-looking,
+  // the column held in registers)
+  if (warp < RB / 32) {
+    const int t0 = warp * 32;
+    double w[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) w[i] = (i == lane) ? 1.0 : 0.0;
+#pragma unroll
+    for (int k = 0; k < 32; ++k) {
+      w[k] = w[k] / (double)Ls[(t0 + k) * BLD + t0 + k];
+#pragma unroll
+      for (int i = k + 1; i < 32; ++i) w[i] -= (double)Ls[(t0 + k) * BLD + t0 + i] * w[k];
     }
-    W[c * (RB + 1) + i] = w;
+#pragma unroll
+    for (int i = 0; i < 32; ++i) W[(t0 + lane) * BLD + t0 + i] = w[i];
   }
   __syncthreads();
-  float* out = winv + (size_t)I * RB * RB;
-  for (int e = c; e < RB * RB; e += RB) {
-    const int col = e / RB, row = e % RB;
-    out[e] = (float)W[col * (RB + 1) + row];
+  // doublings h = 32 (two pairs) and h = 64 (one pair) inside the block;
+  // output e of a level: row r = e % h, column c = (e / h) % h of pair e / h^2
+  for (int h = 32; h < RB; h *= 2) {
+    const int per = (RB / (2 * h)) * h * h / NTH;    // outputs per thread: 8 or 16
+    double acc[16];
+    // T = B A^-1 -> the pair's upper-right block (scratch)
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      acc[q] = 0.0;
+      if (q < per) {
+        const int e = tid + NTH * q;
+        const int r = e % h, c = (e / h) % h, a0 = (e / (h * h)) * 2 * h;
+        double sacc = 0.0;
+        for (int k = c; k < h; ++k)
+          sacc += (double)Ls[(a0 + k) * BLD + a0 + h + r] * W[(a0 + c) * BLD + a0 + k];
+        acc[q] = sacc;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 16; ++q)
+      if (q < per) {
+        const int e = tid + NTH * q;
+        const int r = e % h, c = (e / h) % h, a0 = (e / (h * h)) * 2 * h;
+        W[(a0 + h + c) * BLD + a0 + r] = acc[q];
+      }
+    __syncthreads();
+    // X = -C^-1 T -> the pair's lower-left block; the scratch is cleared
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      if (q < per) {
+        const int e = tid + NTH * q;
+        const int r = e % h, c = (e / h) % h, a0 = (e / (h * h)) * 2 * h;
+        double sacc = 0.0;
+        for (int k = 0; k <= r; ++k)
+          sacc += W[(a0 + h + k) * BLD + a0 + h + r] * W[(a0 + h + c) * BLD + a0 + k];
+        acc[q] = -sacc;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 16; ++q)
+      if (q < per) {
+        const int e = tid + NTH * q;
+        const int r = e % h, c = (e / h) % h, a0 = (e / (h * h)) * 2 * h;
+        W[(a0 + c) * BLD + a0 + h + r] = acc[q];
+        W[(a0 + h + c) * BLD + a0 + r] = 0.0;
+      }
+    __syncthreads();
   }
-}
-
-// Super-block inverse storage: for super-block S, an RS x RS column-major FP32
-// matrix at wsup + S*RS*RS (upper triangle zero).  Diagonal 128-tiles are the
-// 128-block inverses; everything else starts at zero.
-__global__ void superinv_init_kernel(const float* __restrict__ winv, float* __restrict__ wsup,
-                                     int nblk128) {
-  const int S = blockIdx.y;
-  float* W = wsup + (size_t)S * RS * RS;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)RS * RS;
-       e += (long long)gridDim.x * blockDim.x) {
-    const int col = (int)(e / RS), row = (int)(e % RS);
-    const int ti = row / RB, tj = col / RB;
-    float v = 0.0f;
-    const int g = S * (RS / RB) + ti;
-    if (ti == tj && g < nblk128) v = winv[(size_t)g * RB * RB + (col % RB) * RB + (row % RB)];
-    else if (ti == tj && row == col) v = 1.0f;
-    W[e] = v;
+  const int S = i0 / RS, t = (i0 % RS) / RB;
+  float* out = wsup + (size_t)S * RS * RS + (size_t)(t * RB) * RS + t * RB;
+  for (int e = tid; e < RB * RB; e += NTH) {
+    const int col = e / RB, row = e % RB;
+    out[(size_t)col * RS + row] = (float)W[col * BLD + row];
   }
 }
 
@@ -285,37 +340,41 @@ __device__ void gemm128(const float* A, int lda, int a_rows_valid, const float* 
 __device__ __forceinline__ int acc_row(int a) { return a < 4 ? (threadIdx.x % 16) * 4 + a : 64 + (threadIdx.x % 16) * 4 + (a - 4); }
 __device__ __forceinline__ int acc_col(int b) { return b < 4 ? (threadIdx.x / 16) * 4 + b : 64 + (threadIdx.x / 16) * 4 + (b - 4); }
 
-// One level d of the super-block inverse: tile (i = j + d, j) of every
-// super-block:  W_ij = -W_ii * sum_{k=j}^{i-1} L_ik W_kj.
+// One doubling level of half-size h (a multiple of RB) for pair blockIdx.y of
+// super-block blockIdx.z; blockIdx.x enumerates the (h/RB)^2 output tiles.
+//   PHASE 0:  T(ti,tj) = sum_{kt >= tj} L(h + ti, kt) A^-1(kt, tj)  -> upper-right scratch
+//   PHASE 1:  X(ti,tj) = -sum_{kt <= ti} C^-1(ti, kt) T(kt, tj)     -> lower-left block
+// (128-tile indices relative to the pair's origin a0 = 2 h * pair).  Tiles
+// whose rows start at or past n are skipped: the solves never read them.
+template <int PHASE>
 __global__ void __launch_bounds__(NTH)
-superinv_level_kernel(const float* __restrict__ L, int ldl, int n, float* __restrict__ wsup, int d) {
+superinv_gemm_kernel(const float* __restrict__ L, int ldl, int n, float* __restrict__ wsup, int h) {
   __shared__ __align__(16) float As[8 * RB];
   __shared__ __align__(16) float Bs[8 * RB];
-  const int S = blockIdx.y, j = blockIdx.x, i = j + d;
-  const int s0 = S * RS;
-  const int rs = min(RS, n - s0);
-  const int nsub = (rs + RB - 1) / RB;
-  if (i >= nsub) return;
+  const int tpr = h / RB;
+  const int ti = blockIdx.x / tpr, tj = blockIdx.x % tpr;
+  const int S = blockIdx.z, s0 = S * RS, a0 = blockIdx.y * 2 * h;
+  const int grow = s0 + a0 + h + ti * RB;          // first global row of the output tile
+  if (grow >= n) return;
   float* W = wsup + (size_t)S * RS * RS;
-  const int rows_valid = min(RB, rs - i * RB);
   float acc[8][8] = {};
-  // T = L(i-block rows, cols j..i-1 blocks) * W(rows j..i-1 blocks, cols j-block)
-  gemm128(L + (size_t)(s0 + j * RB) * ldl + s0 + i * RB, ldl, rows_valid,
-          W + (size_t)(j * RB) * RS + j * RB, RS, d * RB, acc, As, Bs);
-  float* Wij = W + (size_t)(j * RB) * RS + i * RB;
+  if (PHASE == 0) {
+    gemm128(L + (size_t)(s0 + a0 + tj * RB) * ldl + grow, ldl, min(RB, n - grow),
+            W + (size_t)(a0 + tj * RB) * RS + a0 + tj * RB, RS, h - tj * RB, acc, As, Bs);
+    float* T = W + (size_t)(a0 + h + tj * RB) * RS + a0 + ti * RB;
 #pragma unroll
-  for (int a = 0; a < 8; ++a)
+    for (int a = 0; a < 8; ++a)
 #pragma unroll
-    for (int b = 0; b < 8; ++b) Wij[(size_t)acc_col(b) * RS + acc_row(a)] = acc[a][b];
-  __syncthreads();
-  __threadfence_block();
-  float acc2[8][8] = {};
-  gemm128(W + (size_t)(i * RB) * RS + i * RB, RS, RB, Wij, RS, RB, acc2, As, Bs);
-  __syncthreads();
+      for (int b = 0; b < 8; ++b) T[(size_t)acc_col(b) * RS + acc_row(a)] = acc[a][b];
+  } else {
+    gemm128(W + (size_t)(a0 + h) * RS + a0 + h + ti * RB, RS, RB,
+            W + (size_t)(a0 + h + tj * RB) * RS + a0, RS, (ti + 1) * RB, acc, As, Bs);
+    float* X = W + (size_t)(a0 + tj * RB) * RS + a0 + h + ti * RB;
 #pragma unroll
-  for (int a = 0; a < 8; ++a)
+    for (int a = 0; a < 8; ++a)
 #pragma unroll
-    for (int b = 0; b < 8; ++b) Wij[(size_t)acc_col(b) * RS + acc_row(a)] = -acc2[a][b];
+      for (int b = 0; b < 8; ++b) X[(size_t)acc_col(b) * RS + acc_row(a)] = -acc[a][b];
+  }
 }
 
 // ---- y_S += W_S w_S (TRANS: z_S += W_S^T w_S) over the super-block's lower tiles
@@ -423,7 +482,6 @@ size_t solve_wsup_elems(int n) {
   const int nbs = (n + RS - 1) / RS;
   return (size_t)nbs * RS * RS;
 }
-size_t solve_winv_elems(int n) { return (size_t)((n + RB - 1) / RB) * RB * RB; }
 
 cudaError_t solve_init_attributes() {
   // once per device (kernel attributes are per device)
@@ -441,7 +499,7 @@ cudaError_t solve_init_attributes() {
 
 cudaError_t solve_set_attributes() {
   cudaError_t e;
-  const size_t inv = (size_t)RB * (RB + 1) * (sizeof(double) + sizeof(float));
+  const size_t inv = (size_t)RB * BLD * (sizeof(double) + sizeof(float));
   if ((e = set_dyn(block_inverse_kernel, inv)) != cudaSuccess) return e;
 #define SET_NR(NRC)                                                                         \
   if ((e = set_dyn(symv_kernel<float, NRC>, red_bytes(NRC))) != cudaSuccess) return e;      \
@@ -467,19 +525,24 @@ cudaError_t launch_symv_skip(const TA* A, int lda, int n, const double* x, doubl
 template cudaError_t launch_symv_skip<float>(const float*, int, int, const double*, double*, int, const int*, cudaStream_t);
 template cudaError_t launch_symv_skip<double>(const double*, int, int, const double*, double*, int, const int*, cudaStream_t);
 
-cudaError_t launch_solve_setup(const float* L, int ldl, int n, float* winv, float* wsup,
-                               cudaStream_t stream) {
-  const size_t inv = (size_t)RB * (RB + 1) * (sizeof(double) + sizeof(float));
-  const int nb = ceil_div(n, RB);
-  block_inverse_kernel<<<nb, RB, inv, stream>>>(L, ldl, n, winv);
+cudaError_t launch_solve_setup(const float* L, int ldl, int n, float* wsup, cudaStream_t stream) {
+  const size_t inv = (size_t)RB * BLD * (sizeof(double) + sizeof(float));
+  block_inverse_kernel<<<ceil_div(n, RB), NTH, inv, stream>>>(L, ldl, n, wsup);
   const int nbs = ceil_div(n, RS);
-  superinv_init_kernel<<<dim3(256, nbs), 256, 0, stream>>>(winv, wsup, nb);
-  for (int d = 1; d < RS / RB; ++d)
-    superinv_level_kernel<<<dim3(RS / RB - d, nbs), NTH, 0, stream>>>(L, ldl, n, wsup, d);
+  for (int h = RB; h < RS; h *= 2) {
+    const dim3 grid((h / RB) * (h / RB), RS / (2 * h), nbs);
+    superinv_gemm_kernel<0><<<grid, NTH, 0, stream>>>(L, ldl, n, wsup, h);
+    superinv_gemm_kernel<1><<<grid, NTH, 0, stream>>>(L, ldl, n, wsup, h);
+  }
   return cudaGetLastError();
 }
 
-int solve_setup_launches(int n) { (void)n; return 2 + RS / RB - 1; }
+int solve_setup_launches(int n) {
+  (void)n;
+  int k = 1;
+  for (int h = RB; h < RS; h *= 2) k += 2;
+  return k;
+}
 
 // out = L^-1 in (forward) or L^-T in (backward); work is an n x nrhs scratch.
 cudaError_t launch_trsv_super(bool backward, const float* L, int ldl, int n, const float* wsup,
