@@ -128,6 +128,7 @@ SIGNATURES = {
     "mpchol_quantize_rows": (_i, [_vp, _i, _i, _i, _i, _vp, _vp, _vp]),
     "mpchol_quantize_hash": (_i, [_ull, _ull, _ull, _i, _vp, _vp]),
     "mpchol_syrk_update": (_i, [_vp, _i, _i, _i, _i, _vp, _vp, _vp, _i, _vp]),
+    "mpchol_potrf_static": (_i, [_vp, _i, _i, ctypes.c_float, _vp, _vp]),
 }
 
 _LIB = None

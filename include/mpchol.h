@@ -237,6 +237,29 @@ MPCHOL_API mpchol_status mpchol_syrk_update(float* dC, int ldc, int m, int k, in
                                  const void* dScale, const float* dP, int ldp,
                                  mpchol_stream_t stream);
 
+/* ---- allocation-free diagonal-block POTRF ------------------------------- */
+/* No counterpart in the reference (its diagonal factor is cusolverDnSpotrf on
+ * a workspace the caller allocates, src/switching_chol.cuh:86-95).
+ * Factors the n x n block dA (column-major, ld = lda, lower triangle, FP32)
+ * in place with the factorization's diagonal-block kernel and allocates
+ * nothing: no cudaMalloc/cudaFree, no allocating library call.  For callers
+ * that cannot allocate at the point of the call: cudaMalloc/cudaFree
+ * synchronize the device (stalling every other stream), and a process whose
+ * device memory is held by a caching allocator may have none to give.
+ *   n <= MPCHOL_POTRF_STATIC_MAX (larger n: MPCHOL_ERR_BAD_ARG, nothing runs);
+ *   dA 16-byte aligned and lda a multiple of 4 (TMA); lda >= n.
+ *   pivot_floor > 0: pivots <= pivot_floor * A(i,i) are raised to that value
+ *   (max(|pivot|, floor) repair); pivot_floor = 0: no repair.
+ *   dInfo (device int): 0 on success, i + 1 if pivot i was not positive
+ *   (pivot_floor = 0), -1 for another device-side error; written on `stream`.
+ * Scratch is one static device array per device: calls that overlap in time
+ * on one device race on it (order them on one stream).  The first call on
+ * each device does one-time setup (symbol lookup); make it before any stream
+ * capture. */
+#define MPCHOL_POTRF_STATIC_MAX 256
+MPCHOL_API mpchol_status mpchol_potrf_static(float* dA, int lda, int n, float pivot_floor,
+                                             int* dInfo, mpchol_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif
