@@ -159,7 +159,6 @@ mpchol_status validate_opts(const mpchol_opts* o, int n) {
   if (o->switch_mode != 0 && o->switch_mode != 1) return MPCHOL_ERR_BAD_ARG;
   if (o->ladder_len < 0 || o->ladder_len > 4) return MPCHOL_ERR_BAD_ARG;
   auto tc_ok = [&](int fmt) { return fmt == MPCHOL_PREC_FP32 || syrk_tc_supported(fmt, o->block_size); };
-  if (o->precision == MPCHOL_PREC_MXFP8) return MPCHOL_ERR_NOT_SUPPORTED;
   if (o->precision != MPCHOL_PREC_SWITCHING && !tc_ok(o->precision)) return MPCHOL_ERR_NOT_SUPPORTED;
   if (o->precision == MPCHOL_PREC_SWITCHING) {
     if (o->switch_mode == 1) {
@@ -168,7 +167,7 @@ mpchol_status validate_opts(const mpchol_opts* o, int n) {
       for (int i = 0; i < o->ladder_len; ++i) {
         const int p = o->ladder[i];
         if (p < 0 || p > MPCHOL_PREC_FP16X2 || p == MPCHOL_PREC_SWITCHING) return MPCHOL_ERR_BAD_ARG;
-        if (p == MPCHOL_PREC_MXFP8 || !tc_ok(p)) return MPCHOL_ERR_NOT_SUPPORTED;
+        if (!tc_ok(p)) return MPCHOL_ERR_NOT_SUPPORTED;
       }
     }
   }
@@ -855,8 +854,14 @@ mpchol_status mpchol_syrk_update(float* dC, int ldc, int m, int k, int fmt, cons
   }
   if (!syrk_tc_supported(fmt, k)) return MPCHOL_ERR_NOT_SUPPORTED;
   if (dQ == nullptr || dScale == nullptr) return MPCHOL_ERR_BAD_ARG;
-  PHASE(MPCHOL_PH_SYRK_TC, 1, s, launch_syrk_tc(dC, ldc, m, k, fmt, dQ, k, reinterpret_cast<const int8_t*>(dScale),
-                                 nullptr, 0, nullptr, nullptr, s));
+  if (fmt == MXFP8)
+    PHASE(MPCHOL_PH_SYRK_TC, 1, s, launch_syrk_tc(dC, ldc, m, k, fmt, dQ, k, nullptr,
+                                   reinterpret_cast<const uint8_t*>(dScale), k / 32, nullptr,
+                                   nullptr, s));
+  else
+    PHASE(MPCHOL_PH_SYRK_TC, 1, s, launch_syrk_tc(dC, ldc, m, k, fmt, dQ, k,
+                                   reinterpret_cast<const int8_t*>(dScale), nullptr, 0, nullptr,
+                                   nullptr, s));
   return MPCHOL_OK;
 }
 

@@ -37,14 +37,31 @@ __device__ __forceinline__ void block_reduce_store(double (&v)[NR], double* part
   }
 }
 
+// Sum of the VG partials of each rhs, formed by the whole block with a fixed
+// tree (two loads per thread, warp shuffles, then the eight warp sums in
+// order), so every block -- and every launch -- gets the same bits.  Every
+// thread of the block must call it; all receive the sums.
 template <int NR>
 __device__ __forceinline__ void sum_partials(const double* partials, double (&out)[NR]) {
-  // every thread sums the VG partials in the same fixed order
+  static_assert(VG <= 2 * NTH, "two partials per thread");
+  __shared__ double s_w[NTH / 32][NR];
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
 #pragma unroll
-  for (int k = 0; k < NR; ++k) out[k] = 0.0;
-  for (int b = 0; b < VG; ++b)
+  for (int k = 0; k < NR; ++k) {
+    double v = (t < VG) ? partials[t * NR + k] : 0.0;
+    if (t + NTH < VG) v += partials[(t + NTH) * NR + k];
+    v = warp_sum(v);
+    if (lane == 0) s_w[warp][k] = v;
+  }
+  __syncthreads();
 #pragma unroll
-    for (int k = 0; k < NR; ++k) out[k] += partials[b * NR + k];
+  for (int k = 0; k < NR; ++k) {
+    double s = 0.0;
+#pragma unroll
+    for (int w = 0; w < NTH / 32; ++w) s += s_w[w][k];
+    out[k] = s;
+  }
+  __syncthreads();
 }
 
 template <int NR>
@@ -113,9 +130,9 @@ update_p_kernel(double* __restrict__ p, const double* __restrict__ z, int n,
     const double b = rz[k] / rho_old[k];
     be[k] = (rho_old[k] != 0.0 && isfinite(b)) ? b : 0.0;
   }
+  double rr[NR];
+  sum_partials<NR>(rr_partials, rr);
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    double rr[NR];
-    sum_partials<NR>(rr_partials, rr);
     int all = 1;
 #pragma unroll
     for (int k = 0; k < NR; ++k) {
@@ -136,13 +153,12 @@ update_p_kernel(double* __restrict__ p, const double* __restrict__ z, int n,
 // out = sum of partials (fixed order) for the first NR slots; used to form
 // rho_0 = r_0^T z_0 and ||b||^2 on the device.
 template <int NR>
-__global__ void reduce_partials_kernel(const double* partials, double* out) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) {
-    double s[NR];
-    sum_partials<NR>(partials, s);
+__global__ void __launch_bounds__(NTH) reduce_partials_kernel(const double* partials, double* out) {
+  double s[NR];
+  sum_partials<NR>(partials, s);
+  if (threadIdx.x == 0)
 #pragma unroll
     for (int k = 0; k < NR; ++k) out[k] = s[k];
-  }
 }
 
 // r = b - y (y = A x), partial ||r||^2
@@ -210,7 +226,7 @@ cudaError_t launch_update_p(double* p, const double* z, int n, int nrhs, const d
 
 cudaError_t launch_reduce_partials(const double* partials, double* out, int nrhs,
                                    cudaStream_t stream) {
-  NR_DISPATCH(nrhs, (reduce_partials_kernel<NRC><<<1, 32, 0, stream>>>(partials, out)));
+  NR_DISPATCH(nrhs, (reduce_partials_kernel<NRC><<<1, NTH, 0, stream>>>(partials, out)));
   return cudaGetLastError();
 }
 

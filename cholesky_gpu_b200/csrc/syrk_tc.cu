@@ -47,20 +47,50 @@ __device__ __forceinline__ void tile_of(int t, int& I, int& J) {
 template <int FMT> struct TcCfg;
 template <> struct TcCfg<FP16> {
   static constexpr int ESIZE = 2, NSETS = 1, NSTAGE = 4;
+  static constexpr bool MX = false;
   static constexpr uint32_t IDESC = tc::make_idesc(0, 0, TM, TM);
 };
 template <> struct TcCfg<E4M3> {
   static constexpr int ESIZE = 1, NSETS = 1, NSTAGE = 4;
+  static constexpr bool MX = false;
   static constexpr uint32_t IDESC = tc::make_idesc(0, 0, TM, TM);
 };
 template <> struct TcCfg<E5M2> {
   static constexpr int ESIZE = 1, NSETS = 1, NSTAGE = 4;
+  static constexpr bool MX = false;
   static constexpr uint32_t IDESC = tc::make_idesc(1, 1, TM, TM);
 };
 template <> struct TcCfg<FP16X2> {
   static constexpr int ESIZE = 2, NSETS = 2, NSTAGE = 3;
+  static constexpr bool MX = false;
   static constexpr uint32_t IDESC = tc::make_idesc(0, 0, TM, TM);
 };
+// MXFP8: E4M3 codes with one E8M0 scale per 32 K-elements, applied by the
+// block-scaled MMA (kind::mxf8f6f4) from scales staged in tensor memory.
+template <> struct TcCfg<MXFP8> {
+  static constexpr int ESIZE = 1, NSETS = 1, NSTAGE = 4;
+  static constexpr bool MX = true;
+  static constexpr uint32_t IDESC = tc::make_idesc_mx(0, 0, TM, TM);
+};
+
+// Scales of one stage (a 128-element K chunk = four 32-element blocks) for
+// 128 rows, in the layout the 32x128b tensor-memory copy reads: 32 lines of
+// 16 bytes; line l holds, in 32-bit word w, the four block scales of row
+// 32 w + l (byte b = block b of the chunk).
+constexpr int SF_BYTES = 512;
+
+__device__ __forceinline__ void stage_scales(uint8_t* sf, const uint8_t* __restrict__ mxexp,
+                                             int ldmx, int row0, int m, int kc, int lane) {
+  uint32_t w[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int row = row0 + 32 * q + lane;
+    // rows past m multiply zero codes: give them a unit scale (code 127)
+    w[q] = (row < m) ? *reinterpret_cast<const uint32_t*>(mxexp + (size_t)row * ldmx + 4 * kc)
+                     : 0x7F7F7F7Fu;
+  }
+  *reinterpret_cast<uint4*>(sf + 16 * lane) = make_uint4(w[0], w[1], w[2], w[3]);
+}
 
 struct TcMaps {
   CUtensorMap hi;   // main (or hi) panel: rows m, K-major
@@ -70,13 +100,17 @@ struct TcMaps {
 template <int FMT>
 __global__ void __launch_bounds__(NTHREADS, 1)
 syrk_tc_kernel(const __grid_constant__ TcMaps maps, float* __restrict__ C, int ldc, int m, int k,
-               const int8_t* __restrict__ rowexp, const int* prec_sel, DevStatus* st) {
+               const int8_t* __restrict__ rowexp, const uint8_t* __restrict__ mxexp, int ldmx,
+               const int* prec_sel, DevStatus* st) {
   using Cfg = TcCfg<FMT>;
   if (st != nullptr && st->code != 0) return;
   if (prec_sel != nullptr && *prec_sel != FMT) return;
   constexpr int NS = Cfg::NSTAGE;
   constexpr int NSETS = Cfg::NSETS;
-  constexpr int STAGE_BYTES = 2 * NSETS * STRIP;       // A sets then B sets
+  constexpr bool MX = Cfg::MX;
+  // A sets, B sets, then (MXFP8) the A and B scales of the chunk
+  constexpr int STAGE_BYTES = 2 * NSETS * STRIP + (MX ? 2 * SF_BYTES : 0);
+  constexpr uint32_t TMEM_COLS = MX ? 4 * TM : 2 * TM;  // accumulators (+ scales)
   constexpr int KSTEP = 32;                             // bytes of K per MMA
   constexpr int ELEMS_PER_CHUNK = CHUNK / Cfg::ESIZE;
 
@@ -103,7 +137,7 @@ syrk_tc_kernel(const __grid_constant__ TcMaps maps, float* __restrict__ C, int l
     if (NSETS == 2) tc::prefetch_tmap(&maps.lo);
     abort_sh = 0;
   }
-  if (warp == 1) tc::tmem_alloc(&tmem_base_sh, 2 * TM);
+  if (warp == 1) tc::tmem_alloc(&tmem_base_sh, TMEM_COLS);
   tc::tc_fence_before();
   __syncthreads();
   tc::tc_fence_after();
@@ -111,22 +145,38 @@ syrk_tc_kernel(const __grid_constant__ TcMaps maps, float* __restrict__ C, int l
 
   if (warp == 0) {
     // ---------------- TMA producer ----------------
-    if (lane == 0) {
-      int c = 0;   // global chunk counter
-      for (int t = blockIdx.x; t < ntiles && !abort_sh; t += gridDim.x) {
-        int I, J;
-        tile_of(t, I, J);
-        const bool diag = (I == J);
-        const uint32_t bytes = (uint32_t)((diag ? 1 : 2) * NSETS * STRIP);
-        for (int kc = 0; kc < nchunks; ++kc, ++c) {
-          const int s = c % NS;
-          const uint32_t pass = (uint32_t)(c / NS);
-          if (!tc::mbar_wait(&empty_bar[s], (pass & 1u) ^ 1u)) {
+    // lane 0 waits and issues the copies; for MXFP8 the whole warp stages the
+    // chunk's scales into the stage first
+    int c = 0;   // global chunk counter
+    bool failed = false;
+    for (int t = blockIdx.x; t < ntiles && !failed; t += gridDim.x) {
+      int I, J;
+      tile_of(t, I, J);
+      const bool diag = (I == J);
+      const uint32_t bytes = (uint32_t)((diag ? 1 : 2) * NSETS * STRIP);
+      for (int kc = 0; kc < nchunks; ++kc, ++c) {
+        const int s = c % NS;
+        const uint32_t pass = (uint32_t)(c / NS);
+        int ok = 1;
+        if (lane == 0) ok = (!abort_sh && tc::mbar_wait(&empty_bar[s], (pass & 1u) ^ 1u)) ? 1 : 0;
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (!ok) {
+          if (lane == 0) {
             abort_sh = 1;
             if (st != nullptr) set_status(st, MPCHOL_ERR_TIMEOUT, t);
-            break;
           }
-          uint8_t* base = smem + (size_t)s * STAGE_BYTES;
+          failed = true;
+          break;
+        }
+        uint8_t* base = smem + (size_t)s * STAGE_BYTES;
+        if (MX) {
+          uint8_t* sf = base + 2 * NSETS * STRIP;
+          stage_scales(sf, mxexp, ldmx, I * TM, m, kc, lane);
+          if (!diag) stage_scales(sf + SF_BYTES, mxexp, ldmx, J * TM, m, kc, lane);
+          tc::fence_proxy_async_smem();    // generic writes -> async-proxy reader
+          __syncwarp();
+        }
+        if (lane == 0) {
           tc::mbar_expect_tx(&full_bar[s], bytes);
           const int x = kc * ELEMS_PER_CHUNK;
           tc::tma_load_2d(base, &maps.hi, &full_bar[s], x, I * TM);
@@ -172,12 +222,27 @@ syrk_tc_kernel(const __grid_constant__ TcMaps maps, float* __restrict__ C, int l
           const uint32_t a_lo = a_hi + STRIP;
           const uint32_t b_hi = diag ? a_hi : a_hi + NSETS * STRIP;
           const uint32_t b_lo = diag ? a_lo : a_hi + (NSETS + 1) * STRIP;
+          // MXFP8: this chunk's scales -> TMEM columns 2*TM + buf*16 + kc*8
+          // (A at +0, B at +4); chunks and accumulator buffers use separate
+          // columns, so no copy overwrites scales an unfinished MMA reads
+          uint32_t sfa_t = 0, sfb_t = 0;
+          if (MX) {
+            const uint32_t sfa_s = a_hi + 2 * NSETS * STRIP;
+            const uint32_t sfb_s = diag ? sfa_s : sfa_s + SF_BYTES;
+            sfa_t = tmem + (uint32_t)(2 * TM + buf * 16 + kc * 8);
+            sfb_t = sfa_t + 4;
+            tc::utccp_32x128b_warpx4(sfa_t, tc::make_desc_plain(sfa_s, 128));
+            tc::utccp_32x128b_warpx4(sfb_t, tc::make_desc_plain(sfb_s, 128));
+          }
 #pragma unroll
           for (int kk = 0; kk < CHUNK / KSTEP; ++kk) {
             const uint32_t off = kk * KSTEP;
             const uint64_t ad = tc::make_desc_sw128(a_hi + off);
             const uint64_t bd = tc::make_desc_sw128(b_hi + off);
-            if (FMT == FP16 || FMT == FP16X2) tc::mma_f16(dacc, ad, bd, Cfg::IDESC, accumulate);
+            if (MX)
+              tc::mma_mxf8f6f4(dacc, ad, bd, tc::idesc_sf_ids(Cfg::IDESC, kk, kk), accumulate,
+                               sfa_t | ((uint32_t)kk << 30), sfb_t | ((uint32_t)kk << 30));
+            else if (FMT == FP16 || FMT == FP16X2) tc::mma_f16(dacc, ad, bd, Cfg::IDESC, accumulate);
             else tc::mma_f8f6f4(dacc, ad, bd, Cfg::IDESC, accumulate);
             accumulate = 1;
             if (NSETS == 2) {
@@ -206,7 +271,7 @@ syrk_tc_kernel(const __grid_constant__ TcMaps maps, float* __restrict__ C, int l
       }
       tc::tc_fence_after();
       const int i = I * TM + q * 32 + lane;
-      const float si = (i < m) ? pow2f(rowexp[i]) : 0.0f;
+      const float si = (i < m) ? (MX ? 1.0f : pow2f(rowexp[i])) : 0.0f;
       const uint32_t taddr = tmem + (uint32_t)(buf * TM) + ((uint32_t)(q * 32) << 16);
 #pragma unroll 1
       for (int c0 = 0; c0 < TM; c0 += 32) {
@@ -229,7 +294,8 @@ syrk_tc_kernel(const __grid_constant__ TcMaps maps, float* __restrict__ C, int l
 #pragma unroll
           for (int u = 0; u < 32; ++u) {
             const int j = j0 + u;
-            if (j < m && i >= j) C[(size_t)j * ldc + i] = cv[u] - (v[u] * si) * pow2f(rowexp[j]);
+            if (j < m && i >= j)
+              C[(size_t)j * ldc + i] = cv[u] - (v[u] * si) * (MX ? 1.0f : pow2f(rowexp[j]));
           }
         }
       }
@@ -239,18 +305,20 @@ syrk_tc_kernel(const __grid_constant__ TcMaps maps, float* __restrict__ C, int l
   __syncthreads();
   if (warp == 1) {
     tc::tc_fence_after();
-    tc::tmem_dealloc(tmem, 2 * TM);
+    tc::tmem_dealloc(tmem, TMEM_COLS);
   }
 }
 
 template <int FMT>
 size_t tc_smem() {
-  return (size_t)TcCfg<FMT>::NSTAGE * 2 * TcCfg<FMT>::NSETS * STRIP + 1024;
+  using Cfg = TcCfg<FMT>;
+  return (size_t)Cfg::NSTAGE * (2 * Cfg::NSETS * STRIP + (Cfg::MX ? 2 * SF_BYTES : 0)) + 1024;
 }
 
 template <int FMT>
 cudaError_t launch_fmt(const TcMaps& maps, float* C, int ldc, int m, int k, const int8_t* rowexp,
-                       const int* prec_sel, DevStatus* st, cudaStream_t stream) {
+                       const uint8_t* mxexp, int ldmx, const int* prec_sel, DevStatus* st,
+                       cudaStream_t stream) {
   const size_t smem = tc_smem<FMT>();
   cudaError_t e = cudaFuncSetAttribute(syrk_tc_kernel<FMT>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -262,7 +330,8 @@ cudaError_t launch_fmt(const TcMaps& maps, float* C, int ldc, int m, int k, cons
   const int T = ceil_div(m, TM);
   const int ntiles = T * (T + 1) / 2;
   const int grid = ntiles < nsm ? ntiles : nsm;
-  syrk_tc_kernel<FMT><<<grid, NTHREADS, smem, stream>>>(maps, C, ldc, m, k, rowexp, prec_sel, st);
+  syrk_tc_kernel<FMT><<<grid, NTHREADS, smem, stream>>>(maps, C, ldc, m, k, rowexp, mxexp, ldmx,
+                                                        prec_sel, st);
   return cudaGetLastError();
 }
 
@@ -270,15 +339,17 @@ cudaError_t launch_fmt(const TcMaps& maps, float* C, int ldc, int m, int k, cons
 
 bool syrk_tc_supported(int fmt, int k) {
   if (fmt == FP16 || fmt == FP16X2) return k > 0 && (k * 2) % CHUNK == 0 && k <= 256;
-  if (fmt == E4M3 || fmt == E5M2) return k > 0 && k % CHUNK == 0 && k <= 256;
+  if (fmt == E4M3 || fmt == E5M2 || fmt == MXFP8) return k > 0 && k % CHUNK == 0 && k <= 256;
   return false;
 }
 
 cudaError_t launch_syrk_tc(float* C, int ldc, int m, int k, int fmt, const void* q, int ldq,
                            const int8_t* rowexp, const uint8_t* mxexp, int ldmx,
                            const int* prec_sel, DevStatus* st, cudaStream_t stream) {
-  (void)mxexp; (void)ldmx;
   if (m <= 0) return cudaSuccess;
+  if (fmt == MXFP8 && (mxexp == nullptr || ldmx < k / 32 ||
+                       (reinterpret_cast<uintptr_t>(mxexp) & 3) != 0 || (ldmx & 3) != 0))
+    return cudaErrorInvalidValue;
   if (!syrk_tc_supported(fmt, k)) return cudaErrorInvalidValue;
   const int esize = (fmt == FP16 || fmt == FP16X2) ? 2 : 1;
   const CUtensorMapDataType dt = esize == 2 ? CU_TENSOR_MAP_DATA_TYPE_UINT16 : CU_TENSOR_MAP_DATA_TYPE_UINT8;
@@ -294,10 +365,11 @@ cudaError_t launch_syrk_tc(float* C, int ldc, int m, int k, int fmt, const void*
       return cudaErrorInvalidValue;
   }
   switch (fmt) {
-    case FP16: return launch_fmt<FP16>(maps, C, ldc, m, k, rowexp, prec_sel, st, stream);
-    case E4M3: return launch_fmt<E4M3>(maps, C, ldc, m, k, rowexp, prec_sel, st, stream);
-    case E5M2: return launch_fmt<E5M2>(maps, C, ldc, m, k, rowexp, prec_sel, st, stream);
-    case FP16X2: return launch_fmt<FP16X2>(maps, C, ldc, m, k, rowexp, prec_sel, st, stream);
+    case FP16: return launch_fmt<FP16>(maps, C, ldc, m, k, rowexp, mxexp, ldmx, prec_sel, st, stream);
+    case E4M3: return launch_fmt<E4M3>(maps, C, ldc, m, k, rowexp, mxexp, ldmx, prec_sel, st, stream);
+    case E5M2: return launch_fmt<E5M2>(maps, C, ldc, m, k, rowexp, mxexp, ldmx, prec_sel, st, stream);
+    case FP16X2: return launch_fmt<FP16X2>(maps, C, ldc, m, k, rowexp, mxexp, ldmx, prec_sel, st, stream);
+    case MXFP8: return launch_fmt<MXFP8>(maps, C, ldc, m, k, rowexp, mxexp, ldmx, prec_sel, st, stream);
     default: return cudaErrorInvalidValue;
   }
 }

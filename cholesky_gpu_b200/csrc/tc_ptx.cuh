@@ -115,6 +115,27 @@ __device__ __forceinline__ uint64_t make_desc_sw128(uint32_t smem_addr) {
   return d;
 }
 
+// Shared-memory descriptor, no swizzle, K-major: 8-row x 16-byte core
+// matrices, `sbo` bytes between consecutive groups of 8 rows.
+__device__ __forceinline__ uint64_t make_desc_plain(uint32_t smem_addr, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((smem_addr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 16;   // LBO (one core matrix along K: unused)
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;   // SBO
+  d |= (uint64_t)1u << 46;                       // version
+  return d;                                      // layout type 0: no swizzle
+}
+
+// Instruction descriptor of kind::mxf8f6f4 with E8M0 scales: A/B formats
+// (0 E4M3, 1 E5M2), K-major, M = m, N = n; scale-id fields left zero.
+__host__ __device__ constexpr uint32_t make_idesc_mx(int a_fmt, int b_fmt, int m, int n) {
+  return ((uint32_t)a_fmt << 7) | ((uint32_t)b_fmt << 10) | ((uint32_t)(n >> 3) << 17) |
+         (1u << 23) | ((uint32_t)(m >> 4) << 24);
+}
+__host__ __device__ constexpr uint32_t idesc_sf_ids(uint32_t idesc, uint32_t a_id, uint32_t b_id) {
+  return idesc | (a_id << 29) | (b_id << 4);
+}
+
 // Instruction descriptor: dense, D = F32, A/B K-major, M = 128, N = n.
 // a_fmt/b_fmt: kind::f16 -> 0 F16, 1 BF16; kind::f8f6f4 -> 0 E4M3, 1 E5M2.
 __host__ __device__ constexpr uint32_t make_idesc(int a_fmt, int b_fmt, int m, int n) {
@@ -139,6 +160,26 @@ __device__ __forceinline__ void mma_f8f6f4(uint32_t tmem_d, uint64_t adesc, uint
       "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
       "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
 }
+// Block-scaled MMA (kind::mxf8f6f4, one E8M0 scale per 32 K-elements of each
+// row of A and of B).  The scale operands are TMEM addresses whose two top
+// bits select the byte (the 32-element K block) inside each 32-bit scale word;
+// the same byte index goes into the instruction descriptor's scale-id fields.
+__device__ __forceinline__ void mma_mxf8f6f4(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                             uint32_t idesc, uint32_t accumulate,
+                                             uint32_t tmem_sfa, uint32_t tmem_sfb) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::mxf8f6f4.block_scale [%0], %1, %2, %3, [%5], [%6], p;\n\t}" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(tmem_sfa), "r"(tmem_sfb));
+}
+
+// Shared -> tensor memory copy of a 32-row x 16-byte matrix, broadcast to the
+// four 32-lane quarters of TMEM (4 columns of 32 bits per lane).
+__device__ __forceinline__ void utccp_32x128b_warpx4(uint32_t taddr, uint64_t sdesc) {
+  asm volatile("tcgen05.cp.cta_group::1.32x128b.warpx4 [%0], %1;" ::"r"(taddr), "l"(sdesc) : "memory");
+}
+
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                    smem_u32(bar))

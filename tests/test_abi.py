@@ -58,6 +58,7 @@ def test_default_options():
     (dict(diag_pert=1, pivot_floor=0.0), _lib.ERR_BAD_ARG),
     (dict(switch_mode=3), _lib.ERR_BAD_ARG),
     (dict(precision="e4m3", block_size=64), _lib.ERR_NOT_SUPPORTED),
+    (dict(precision="mxfp8", block_size=96), _lib.ERR_NOT_SUPPORTED),
 ])
 def test_option_validation_without_gpu(kw, status):
     lib = _lib.load()

@@ -121,7 +121,7 @@ def syrk_ref(C, Q, s, fmt, m, k):
     return out
 
 
-@pytest.mark.parametrize("fmt", [O.E4M3, O.E5M2, O.FP16, O.FP16X2])
+@pytest.mark.parametrize("fmt", [O.E4M3, O.E5M2, O.FP16, O.FP16X2, O.MXFP8])
 @pytest.mark.parametrize("m,k", [(640, 256), (300, 128), (1000, 256), (2500, 256)])
 def test_tensor_core_syrk_matches_oracle(cuda, fmt, m, k):
     lib = _lib.load()
@@ -141,8 +141,8 @@ def test_tensor_core_syrk_matches_oracle(cuda, fmt, m, k):
     scale = np.abs(want[low]).max()
     err = np.abs(got[low] - want[low]).max() / scale
     print(f"tc syrk fmt={fmt} m={m} k={k} max rel err {err:.3e}")
-    # FP32 accumulation in TMEM; the FP8 MMA accumulates with reduced internal
-    # precision, so its bar is looser.
+    # FP32 accumulation in TMEM; the FP8 MMA (plain and block-scaled MX)
+    # accumulates with reduced internal precision, so its bar is looser.
     # (FP16X2 accumulates three products per K step: slightly more rounding)
     assert err < {O.FP16: 2e-6, O.FP16X2: 5e-6}.get(fmt, 1e-4), err
     # upper triangle untouched

@@ -42,11 +42,13 @@ def factor_parity(A: np.ndarray, **opts):
     (512, 256, "fp32"),
     (768, 256, "e4m3"),
     (640, 128, "e5m2"),
+    (768, 256, "mxfp8"),    # block-scaled MX trailing updates (kind::mxf8f6f4)
+    (1000, 128, "mxfp8"),   # ragged, K = 128
     (1024, 256, "fp16x2"),  # split FP16: FP32-class factor on tensor cores
     (96, 256, "fp32"),      # n < b: a single diagonal block
 ])
 def test_factor_matches_oracle(cuda, n, b, prec):
-    A = matgen.spd_matrix(n, 1e2 if prec in ("e4m3", "e5m2") else 1e4, 1).numpy()
+    A = matgen.spd_matrix(n, 1e2 if prec in ("e4m3", "e5m2", "mxfp8") else 1e4, 1).numpy()
     f, info, ref, err = factor_parity(A, block_size=b, precision=prec)
     assert info.status == 0 and ref["status"] == 0
     worst = max([O.FP32] + [p for p in info.step_prec[:-1]], key=lambda p: FACTOR_TOL[p])
@@ -120,6 +122,7 @@ def test_apply_precond_matches_oracle_potrs(cuda):
     (2048, 256, "switching", 1e6, 1),
     (2048, 256, "fp16x2", 1e6, 1),
     (1000, 128, "fp32", 1e3, 8),
+    (1024, 128, "mxfp8", 1e3, 2),
 ])
 def test_pcg_reaches_1e10_and_matches_dense_solve(cuda, n, b, prec, kappa, nrhs):
     A = matgen.spd_matrix(n, kappa, 1).numpy()
