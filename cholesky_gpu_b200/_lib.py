@@ -129,6 +129,10 @@ SIGNATURES = {
     "mpchol_quantize_hash": (_i, [_ull, _ull, _ull, _i, _vp, _vp]),
     "mpchol_syrk_update": (_i, [_vp, _i, _i, _i, _i, _vp, _vp, _vp, _i, _vp]),
     "mpchol_potrf_static": (_i, [_vp, _i, _i, ctypes.c_float, _vp, _vp]),
+    "mpchol_rbf_build": (_i, [_vp, _i, _i, _i, ctypes.c_double, ctypes.c_double, _vp, _vp, _i, _i,
+                              _vp]),
+    "mpchol_rbf_grad_work_elems": (_i, [_i]),
+    "mpchol_rbf_grad": (_i, [_vp, _i, _i, _i, ctypes.c_double, _vp, _vp, _vp, _vp, _vp, _vp]),
 }
 
 _LIB = None

@@ -865,4 +865,31 @@ mpchol_status mpchol_syrk_update(float* dC, int ldc, int m, int k, int fmt, cons
   return MPCHOL_OK;
 }
 
+mpchol_status mpchol_rbf_build(const float* dX, int n, int d, int ldx, double lengthscale,
+                               double nugget, double* dK64, float* dK32, int ldk, int lower_only,
+                               mpchol_stream_t stream) {
+  if (dX == nullptr || (dK64 == nullptr && dK32 == nullptr)) return MPCHOL_ERR_BAD_ARG;
+  if (n < 1 || d < 1 || ldx < d || ldk < n || !(lengthscale > 0.0) || !(nugget >= 0.0))
+    return MPCHOL_ERR_BAD_ARG;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  PHASE(MPCHOL_PH_SETUP, 1, s, launch_rbf_build(dX, n, d, ldx, lengthscale, nugget, dK64, dK32, ldk,
+                                                lower_only, s));
+  return MPCHOL_OK;
+}
+
+int mpchol_rbf_grad_work_elems(int n) { return n > 0 ? rbf_grad_work_elems(n) : 0; }
+
+mpchol_status mpchol_rbf_grad(const float* dX, int n, int d, int ldx, double lengthscale,
+                              const double* dA, const double* dB, double* dP, double* dS,
+                              double* dWork, mpchol_stream_t stream) {
+  if (dX == nullptr || dA == nullptr || dB == nullptr || dP == nullptr || dS == nullptr ||
+      dWork == nullptr)
+    return MPCHOL_ERR_BAD_ARG;
+  if (n < 1 || d < 1 || ldx < d || !(lengthscale > 0.0)) return MPCHOL_ERR_BAD_ARG;
+  if (d > rbf_grad_max_features()) return MPCHOL_ERR_NOT_SUPPORTED;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  PHASE(MPCHOL_PH_SETUP, 2, s, launch_rbf_grad(dX, n, d, ldx, lengthscale, dA, dB, dP, dS, dWork, s));
+  return MPCHOL_OK;
+}
+
 }  // extern "C"

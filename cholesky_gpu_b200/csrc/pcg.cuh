@@ -48,4 +48,14 @@ cudaError_t launch_frob_lower(const TA* A, int lda, int n, double* partials, cud
 cudaError_t launch_pad_columns(const double* src, int n, int ncols, double* dst, int ncols_pad,
                                cudaStream_t stream);
 
+// RBF kernel matrix (FP64 arithmetic) and its gradient contraction.
+int rbf_grad_max_features();
+int rbf_grad_work_elems(int n);
+cudaError_t launch_rbf_build(const float* X, int n, int d, int ldx, double lengthscale,
+                             double nugget, double* K64, float* K32, int ldk, int lower_only,
+                             cudaStream_t stream);
+cudaError_t launch_rbf_grad(const float* X, int n, int d, int ldx, double lengthscale,
+                            const double* a, const double* b, double* P, double* s, double* work,
+                            cudaStream_t stream);
+
 }  // namespace mpchol

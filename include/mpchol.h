@@ -237,6 +237,28 @@ MPCHOL_API mpchol_status mpchol_syrk_update(float* dC, int ldc, int m, int k, in
                                  const void* dScale, const float* dP, int ldp,
                                  mpchol_stream_t stream);
 
+/* ---- Gaussian RBF kernel matrices (no reference arithmetic: src/RBF.cu is a stub)
+ * dX: n points x d features, row-major FP32 (ld = ldx).  Writes
+ *   K_ij = exp(-||x_i - x_j||^2 / (2 lengthscale^2)) + nugget * delta_ij
+ * computed in FP64 from coordinate differences, column-major (ld = ldk) into
+ * dK64 (FP64) and/or dK32 (FP32); either may be NULL.  lower_only = 1 writes
+ * the lower triangle only (all the factor and the PCG operator read). */
+MPCHOL_API mpchol_status mpchol_rbf_build(const float* dX, int n, int d, int ldx, double lengthscale,
+                                          double nugget, double* dK64, float* dK32, int ldk,
+                                          int lower_only, mpchol_stream_t stream);
+/* Gradient contraction for a solve x = K^-1 y with adjoint a = K^-1 (dL/dx):
+ * recomputes the K tiles from dX (FP64) and writes
+ *   dP (n x (2 + 2d), column-major, ld = n) = K_rbf [a, b, a*X, b*X]
+ *   dS (1 double) = sum_ij a_i b_j K_ij ||x_i - x_j||^2
+ * (K_rbf without the nugget; b = x).  d <= 128.  dWork: at least
+ * mpchol_rbf_grad_work_elems(n) doubles of caller scratch.  The gradients
+ * follow: dL/dnugget = -a.b, dL/dlengthscale = -S / l^3, dL/dy = a,
+ * dL/dX_i = (X_i (a_i P_i1 + b_i P_i0) - a_i P_i(b*X) - b_i P_i(a*X)) / l^2. */
+MPCHOL_API int mpchol_rbf_grad_work_elems(int n);
+MPCHOL_API mpchol_status mpchol_rbf_grad(const float* dX, int n, int d, int ldx, double lengthscale,
+                                         const double* dA, const double* dB, double* dP, double* dS,
+                                         double* dWork, mpchol_stream_t stream);
+
 /* ---- allocation-free diagonal-block POTRF ------------------------------- */
 /* No counterpart in the reference (its diagonal factor is cusolverDnSpotrf on
  * a workspace the caller allocates, src/switching_chol.cuh:86-95).

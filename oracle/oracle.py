@@ -315,3 +315,44 @@ def dense_solve(A: np.ndarray, b: np.ndarray) -> np.ndarray:
     from scipy.linalg import cho_factor, cho_solve
     c = cho_factor(np.asarray(A, dtype=np.float64), lower=True, check_finite=False)
     return cho_solve(c, np.asarray(b, dtype=np.float64), check_finite=False)
+
+
+# ---- RBF kernel solve (FP64 dense oracle for the differentiable solve) -------
+
+def rbf_kernel_f64(X: np.ndarray, ell: float, lam: float) -> tuple[np.ndarray, np.ndarray]:
+    """(K, r2): K_ij = exp(-r2_ij / (2 ell^2)) + lam delta_ij in FP64, r2 from
+    coordinate differences."""
+    Xd = np.asarray(X, dtype=np.float64)
+    r2 = ((Xd[:, None, :] - Xd[None, :, :]) ** 2).sum(-1)
+    K = np.exp(-r2 / (2.0 * ell * ell))
+    K[np.diag_indices_from(K)] += lam
+    return K, r2
+
+
+def rbf_loss_f64(X: np.ndarray, ell: float, lam: float, y: np.ndarray) -> float:
+    """L = 1/2 y^T K^-1 y by FP64 dense Cholesky."""
+    import scipy.linalg as sl
+    K, _ = rbf_kernel_f64(X, ell, lam)
+    c = sl.cho_factor(K, lower=True)
+    yd = np.asarray(y, dtype=np.float64)
+    return 0.5 * float(np.sum(yd * sl.cho_solve(c, yd)))
+
+
+def rbf_loss_grads_f64(X: np.ndarray, ell: float, lam: float, y: np.ndarray):
+    """Gradients of L = 1/2 y^T K^-1 y w.r.t. (X, ell, lam, y), FP64 dense:
+    x = K^-1 y, G_K = -x x^T / 2; dL/dlam = tr G_K; dL/dell = sum G_K K r2 / ell^3;
+    dL/dX_i = sum_j 2 G_K,ij K_ij (X_j - X_i) / ell^2; dL/dy = x."""
+    import scipy.linalg as sl
+    Xd = np.asarray(X, dtype=np.float64)
+    K, r2 = rbf_kernel_f64(Xd, ell, lam)
+    Kr = K - lam * np.eye(K.shape[0])
+    c = sl.cho_factor(K, lower=True)
+    yd = np.asarray(y, dtype=np.float64)
+    x = sl.cho_solve(c, yd)
+    x2 = x.reshape(x.shape[0], -1)
+    G = -0.5 * x2 @ x2.T
+    d_lam = float(np.trace(G))
+    d_ell = float(np.sum(G * Kr * r2) / ell ** 3)
+    W = 2.0 * G * Kr
+    dX = (W @ Xd - W.sum(1)[:, None] * Xd) / (ell * ell)
+    return dX, d_ell, d_lam, x

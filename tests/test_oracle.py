@@ -159,3 +159,21 @@ def test_reference_literal_rule():
     assert O.choose_precision(d, dt, eps_prime=5e-4, switch_mode=1) == O.FP16
     assert O.choose_precision(d, dt, eps_prime=1e-2, switch_mode=1) == O.E4M3
     assert O.choose_precision(d, dt, eps_prime=1e-9, switch_mode=1) == O.FP32
+
+
+def test_rbf_oracle_gradients_match_central_differences():
+    """Pins the FP64 gradient formulas of the RBF solve oracle (loss
+    1/2 y^T K^-1 y) against FP64 central differences, h = 1e-5."""
+    g = np.random.default_rng(0)
+    n, d, ell, lam, h = 40, 3, 1.3, 0.1, 1e-5
+    X = g.standard_normal((n, d))
+    y = g.standard_normal(n)
+    dX, d_ell, d_lam, x = O.rbf_loss_grads_f64(X, ell, lam, y)
+    L = lambda X_, e_, l_: O.rbf_loss_f64(X_, e_, l_, y)  # noqa: E731
+    assert abs((L(X, ell + h, lam) - L(X, ell - h, lam)) / (2 * h) - d_ell) <= 1e-7 * abs(d_ell)
+    assert abs((L(X, ell, lam + h) - L(X, ell, lam - h)) / (2 * h) - d_lam) <= 1e-7 * abs(d_lam)
+    for (i, k) in ((5, 1), (0, 0), (39, 2)):
+        E = np.zeros_like(X)
+        E[i, k] = h
+        fd = (L(X + E, ell, lam) - L(X - E, ell, lam)) / (2 * h)
+        assert abs(fd - dX[i, k]) <= 1e-6 * max(abs(dX[i, k]), 1e-3)
