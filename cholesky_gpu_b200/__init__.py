@@ -9,7 +9,8 @@ from ._lib import (  # noqa: F401
     PREC_E4M3, PREC_E5M2, PREC_FP16, PREC_FP32, PREC_MXFP8, PREC_SWITCHING, PREC_NAMES,
     MpcholError, load,
 )
-from .api import Factor, FactorInfo, Report, factor, precond_CG, solve, switching_chol  # noqa: F401
+from .api import Batch, Factor, FactorInfo, Report, factor, precond_CG, solve, switching_chol  # noqa: F401
+from .autograd import RBFSolve, rbf_build, rbf_solve  # noqa: F401
 
 __all__ = ["Factor", "FactorInfo", "Report", "factor", "solve", "precond_CG", "switching_chol",
            "load", "MpcholError"]

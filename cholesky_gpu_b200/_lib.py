@@ -132,6 +132,12 @@ SIGNATURES = {
     "mpchol_rbf_build": (_i, [_vp, _i, _i, _i, ctypes.c_double, ctypes.c_double, _vp, _vp, _i, _i,
                               _vp]),
     "mpchol_rbf_grad_work_elems": (_i, [_i]),
+    "mpchol_batch_create": (_i, [ctypes.POINTER(Opts), _i, _vp, _i, _vp]),
+    "mpchol_batch_factor": (_i, [_vp, _vp, _vp, _vp]),
+    "mpchol_batch_info": (_i, [_vp, _vp, _vp, _vp, _vp]),
+    "mpchol_batch_lower": (_i, [_vp, _i, _vp, _vp, _vp]),
+    "mpchol_batch_pcg": (_i, [_vp, _vp, _vp, _vp, _vp, ctypes.POINTER(PcgOpts), _vp, _vp]),
+    "mpchol_batch_destroy": (_i, [_vp]),
     "mpchol_rbf_grad": (_i, [_vp, _i, _i, _i, ctypes.c_double, _vp, _vp, _vp, _vp, _vp, _vp]),
 }
 

@@ -239,3 +239,99 @@ def switching_chol(d_A: torch.Tensor, n: int, b: int, d_diagVals: torch.Tensor,
     return load().mpchol_switching_chol(d_A.data_ptr(), n, b, _ptr(d_diagVals),
                                         _ptr(updated_diag), eps_prime, int(perturb_diag),
                                         microscal_size, _stream_handle(), _ptr(scales))
+
+
+class Batch:
+    """Many independent SPD systems of uneven size, factored and solved with
+    batched launches (every kernel serves all systems; the factorization is
+    one CUDA graph launch, PCG runs the systems in lockstep)."""
+
+    def __init__(self, ns, nrhs: int = 1, **opts):
+        self.lib = load()
+        self.ns = [int(v) for v in ns]
+        self.count = len(self.ns)
+        self.nrhs = nrhs
+        self.opts = _lib.default_opts(**opts)
+        arr = (ctypes.c_int * self.count)(*self.ns)
+        h = ctypes.c_void_p()
+        check(self.lib.mpchol_batch_create(ctypes.byref(self.opts), self.count, arr, nrhs,
+                                           ctypes.byref(h)), "mpchol_batch_create")
+        self.handle = h
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            self.lib.mpchol_batch_destroy(h)
+            self.handle = None
+
+    def _mats(self, As, dtype=torch.float32):
+        ptrs = (ctypes.c_void_p * self.count)()
+        lds = (ctypes.c_int * self.count)()
+        keep = []
+        for i, A in enumerate(As):
+            _require_cuda(A, dtype, f"A[{i}]")
+            if A.shape[0] != self.ns[i]:
+                raise ValueError(f"A[{i}] has order {A.shape[0]}, expected {self.ns[i]}")
+            Ac, lda = _col_major(A)
+            keep.append(Ac)
+            ptrs[i] = Ac.data_ptr()
+            lds[i] = lda
+        return ptrs, lds, keep
+
+    def factor(self, As) -> "Batch":
+        ptrs, lds, keep = self._mats(As)
+        check(self.lib.mpchol_batch_factor(self.handle, ptrs, lds, _stream_handle()),
+              "mpchol_batch_factor")
+        self._keep = keep
+        return self
+
+    def info(self):
+        st = (ctypes.c_int * self.count)()
+        row = (ctypes.c_int * self.count)()
+        npert = (ctypes.c_int * self.count)()
+        check(self.lib.mpchol_batch_info(self.handle, st, row, npert, _stream_handle()),
+              "mpchol_batch_info")
+        return list(st), list(row), list(npert)
+
+    def lower(self, i: int) -> torch.Tensor:
+        p = ctypes.c_void_p()
+        ld = ctypes.c_int()
+        n = ctypes.c_int()
+        check(self.lib.mpchol_batch_lower(self.handle, i, ctypes.byref(p), ctypes.byref(ld),
+                                          ctypes.byref(n)), "mpchol_batch_lower")
+        torch.cuda.current_stream().synchronize()
+        src = _wrap_device(p.value, (n.value, ld.value), torch.float32)
+        return src.clone()[:, : n.value].t().tril()
+
+    def pcg(self, As, Bs, rel_tol: float = 1e-10, max_it: int = 200, x0_precond: bool = True,
+            check_every: int = 4):
+        """Solve A_i X_i = B_i for every system; B_i: n_i x nrhs (or n_i) FP64."""
+        ptrs, lds, keep = self._mats(As)
+        bp = (ctypes.c_void_p * self.count)()
+        xp = (ctypes.c_void_p * self.count)()
+        Xs, Bc = [], []
+        for i, B in enumerate(Bs):
+            _require_cuda(B, torch.float64, f"B[{i}]")
+            B2 = B.reshape(self.ns[i], -1)
+            if B2.shape[1] != self.nrhs:
+                raise ValueError(f"B[{i}] has {B2.shape[1]} columns, expected {self.nrhs}")
+            Bt = B2.t().contiguous()            # column-major n x nrhs
+            X = torch.empty_like(Bt)
+            Bc.append(Bt)
+            Xs.append(X)
+            bp[i] = Bt.data_ptr()
+            xp[i] = X.data_ptr()
+        po = _lib.default_pcg_opts(rel_tol=rel_tol, max_it=max_it, x0_precond=int(x0_precond),
+                                   check_every=check_every)
+        reps = (_lib.Report * self.count)()
+        st = self.lib.mpchol_batch_pcg(self.handle, ptrs, lds, bp, xp, ctypes.byref(po), reps,
+                                       _stream_handle())
+        if st not in (_lib.OK, _lib.PCG_MAXIT):
+            check(st, "mpchol_batch_pcg")
+        out = []
+        for i, X in enumerate(Xs):
+            Xo = X.t()
+            out.append(Xo.reshape(Bs[i].shape) if Bs[i].dim() == 1 else Xo)
+        reports = [Report(r.iterations, bool(r.converged), r.rel_residual, r.backward_error,
+                          r.precond_residual, st) for r in reps]
+        return out, reports, st

@@ -111,7 +111,7 @@ __device__ __forceinline__ float warp_max(float v) {
   return v;
 }
 
-inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+__host__ __device__ inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
 
 }  // namespace mpchol
 

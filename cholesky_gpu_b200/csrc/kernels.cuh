@@ -82,6 +82,48 @@ cudaError_t launch_syrk_tc(float* C, int ldc, int m, int k, int fmt, const void*
                            const int8_t* rowexp, const uint8_t* mxexp, int ldmx,
                            const int* prec_sel, DevStatus* st, cudaStream_t stream);
 
+// ---- batched factorization and solve of many independent systems --------
+// Systems are ordered by decreasing n, so the systems still active at a
+// factor step are a prefix of the array.
+struct BatchSys {
+  float* A;            // factor storage (copy of the input), column-major, ld
+  int ld;
+  int n;
+  float* d;            // original diagonal (pivot floors)
+  float* dtilde;       // diagonal tracker (not used for decisions in batch mode)
+  float* rowsq;        // per-row sum of squares of the latest panel
+  float* sh;           // rounding-shift accumulator
+  float* winv;         // inverses of the current diagonal block's 32-tiles
+  float* wsup;         // super-block inverses for the solves
+  DevStatus* st;
+  // solve side
+  const float* op;     // PCG operator (FP32, column-major, lda = op_ld)
+  int op_ld;
+  double* vec;         // 8 vector slots of n x nr (column-major), slot s at vec + s*n*nr
+  double* part;        // partial sums: 4 groups x BATCH_VB x 8
+  double* scal;        // 64 scalars (rho[2], alpha, bnorm2, misc)
+  int* done;           // [0] converged (recursive residual), [1] iterations
+};
+// Per system and factor step.
+struct BatchStep {
+  int m;               // trailing rows after this step's diagonal block (<= 0: none)
+  int q_row0;          // first row of the system's panel in the panel arena (multiple of 128)
+  int tile0;           // first tile of the system in this step's SYRK tile numbering
+};
+constexpr int BATCH_VB = 4;   // partial-sum blocks per system in the batched PCG reductions
+
+cudaError_t launch_potrf_batched(BatchSys* sys, int nact, int s, int b, const PotrfParams& p,
+                                 cudaStream_t stream);
+cudaError_t launch_trsm_batched(BatchSys* sys, int nact, int s, int b, int max_m,
+                                cudaStream_t stream);
+cudaError_t launch_quantize_batched(BatchSys* sys, const BatchStep* steps, int nact, int s, int b,
+                                    int max_m, int fmt, void* q, int qrows, int8_t* rowexp,
+                                    uint8_t* mxexp, int diag_pert, cudaStream_t stream);
+cudaError_t launch_syrk_tc_batched(BatchSys* sys, const BatchStep* steps, int nact, int ntiles,
+                                   int s, int b, int fmt, const void* q, int qrows,
+                                   const int8_t* rowexp, const uint8_t* mxexp,
+                                   cudaStream_t stream);
+
 // ---- PCG building blocks ------------------------------------------------
 template <typename TA>
 cudaError_t launch_symv(const TA* A, int lda, int n, const double* x, double* y, int nrhs,

@@ -58,4 +58,34 @@ cudaError_t launch_rbf_grad(const float* X, int n, int d, int ldx, double length
                             const double* a, const double* b, double* P, double* s, double* work,
                             cudaStream_t stream);
 
+// ---- batched solve side (solve.cu, pcg.cu): every launch serves all systems
+struct BatchSys;
+cudaError_t launch_vec_slot_batched(const BatchSys* sys, int nsys, int src, int dst, int nr,
+                                    int use_skip, cudaStream_t stream);
+cudaError_t launch_symv_batched(const BatchSys* sys, int nsys, int max_n, int xslot, int yslot,
+                                int nr, int use_skip, cudaStream_t stream);
+cudaError_t launch_solve_setup_batched(const BatchSys* sys, int nsys, int max_n,
+                                       cudaStream_t stream);
+cudaError_t launch_trsv_batched(bool backward, const BatchSys* sys, int nsys, int max_n,
+                                int in_slot, int out_slot, int work_slot, int nr, int use_skip,
+                                cudaStream_t stream);
+
+cudaError_t launch_dot_batched(const BatchSys* sys, int nsys, int aslot, int bslot, int group,
+                               int nr, int use_skip, cudaStream_t stream);
+cudaError_t launch_update_xr_batched(const BatchSys* sys, int nsys, int cur, int nr,
+                                     cudaStream_t stream);
+cudaError_t launch_update_p_batched(const BatchSys* sys, int nsys, int cur, int nrhs, int nr,
+                                    double tol2, cudaStream_t stream);
+cudaError_t launch_reduce_batched(const BatchSys* sys, int nsys, int group, int off, int nr,
+                                  int use_skip, cudaStream_t stream);
+cudaError_t launch_residual_batched(const BatchSys* sys, int nsys, int nr, cudaStream_t stream);
+cudaError_t launch_check_true_batched(const BatchSys* sys, int nsys, int nrhs, double tol2,
+                                      cudaStream_t stream);
+cudaError_t launch_count_open(const BatchSys* sys, int nsys, int* out, cudaStream_t stream);
+cudaError_t launch_load_rhs_batched(const BatchSys* sys, int nsys, const double* const* B, int nrhs,
+                                    int nr, cudaStream_t stream);
+cudaError_t launch_store_x_batched(const BatchSys* sys, int nsys, double* const* X, int nrhs,
+                                   int nr, cudaStream_t stream);
+cudaError_t launch_frob_batched(const BatchSys* sys, int nsys, cudaStream_t stream);
+
 }  // namespace mpchol

@@ -303,6 +303,19 @@ potrf_f32_kernel(const __grid_constant__ CUtensorMap tmap, float* A, int lda, in
                            winv, st);
 }
 
+// Batched: CTA i factors the current diagonal block of system i (tiles in
+// shared memory, staged with plain coalesced loads: one tensor map per
+// system would not fit the launch).
+__global__ void __launch_bounds__(512, 1)
+potrf_batched_kernel(BatchSys* __restrict__ sys, int s, int b, PotrfParams p) {
+  const BatchSys& S = sys[blockIdx.x];
+  const int bs = min(b, S.n - s);
+  if (bs <= 0 || S.st->code != 0) return;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  potrf_block<float, false>(nullptr, reinterpret_cast<float*>(smem_raw), S.A, S.ld, S.n, s, bs,
+                            S.d, S.sh, p, S.winv, S.st);
+}
+
 // FP64 blocks (flagged near-indefinite): tiles in a global scratch.
 __global__ void __launch_bounds__(256, 1)
 potrf_f64_kernel(float* A, int lda, int n, int s, int bs, const float* d, const float* sh,
@@ -333,6 +346,17 @@ cudaError_t launch_potrf(const CUtensorMap& tmap32, float* A, int lda, int n, in
                                              may_fp64 ? fp64_flag : nullptr, winv, st);
   if (may_fp64)
     potrf_f64_kernel<<<1, 256, 0, stream>>>(A, lda, n, s, bs, d, sh, p, fp64_flag, scratch64, winv, st);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_potrf_batched(BatchSys* sys, int nact, int s, int b, const PotrfParams& p,
+                                 cudaStream_t stream) {
+  if (nact <= 0) return cudaSuccess;
+  const size_t smem = potrf_smem_bytes(b);
+  cudaError_t e = cudaFuncSetAttribute(potrf_batched_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  potrf_batched_kernel<<<nact, 512, smem, stream>>>(sys, s, b, p);
   return cudaGetLastError();
 }
 

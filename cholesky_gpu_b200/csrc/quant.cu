@@ -35,9 +35,11 @@ __device__ __forceinline__ int resolve_precision(const StepState* step, const De
 
 // Quantize one CTA tile of QROWS rows x k columns.  Lane l of a warp owns the
 // contiguous columns [l*c, (l+1)*c), c = k/32 (k is a multiple of 32, <= 256).
+// lo_rows: rows from a row of the FP16X2 hi panel to the same row of the lo
+// panel (m for a single panel; the arena height for batched panels).
 __device__ void quantize_tile(const float* __restrict__ P, int ldp, int m, int k, int fmt,
                               void* q, int ldq, int8_t* rowexp, uint8_t* mxexp, int ldmx,
-                              float* tile) {
+                              float* tile, int lo_rows) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int row0 = blockIdx.x * QROWS;
   const int nr = min(QROWS, m - row0);
@@ -81,9 +83,9 @@ __device__ void quantize_tile(const float* __restrict__ P, int ldp, int m, int k
           if (t < cpl) qr[t] = f32_to_f16(v[t] * inv);
       } else if (fmt == FP16X2) {
         // hi = fp16(x), lo = fp16(x - hi); x - hi is exact in FP32.  The lo
-        // panel follows the hi panel (m rows further on).
+        // panel follows the hi panel (lo_rows rows further on).
         uint16_t* qh = reinterpret_cast<uint16_t*>(q) + (size_t)gi * ldq + lane * cpl;
-        uint16_t* ql = qh + (size_t)m * ldq;
+        uint16_t* ql = qh + (size_t)lo_rows * ldq;
 #pragma unroll
         for (int t = 0; t < 8; ++t)
           if (t < cpl) {
@@ -119,14 +121,40 @@ quantize_panel_kernel(const float* __restrict__ P, int ldp, int m, int k, StepSt
       if (gi < m) sh[gi] += u * rowsq[gi];
     }
   }
-  quantize_tile(P, ldp, m, k, p, q, ldq, rowexp, mxexp, ldmx, qtile);
+  quantize_tile(P, ldp, m, k, p, q, ldq, rowexp, mxexp, ldmx, qtile, m);
 }
 
 __global__ void __launch_bounds__(QTHR)
 quantize_rows_kernel(const float* __restrict__ P, int ldp, int m, int k, int fmt, void* q, int ldq,
                      int8_t* rowexp, uint8_t* mxexp, int ldmx) {
   extern __shared__ __align__(16) float qtile[];
-  quantize_tile(P, ldp, m, k, fmt, q, ldq, rowexp, mxexp, ldmx, qtile);
+  quantize_tile(P, ldp, m, k, fmt, q, ldq, rowexp, mxexp, ldmx, qtile, m);
+}
+
+// Batched: blockIdx.y = system; its panel goes to rows q_row0.. of the
+// panel arena (qrows rows per FP16X2 half), scales alongside.
+__global__ void __launch_bounds__(QTHR)
+quantize_batched_kernel(BatchSys* __restrict__ sys, const BatchStep* __restrict__ steps, int s,
+                        int b, int fmt, void* q, int qrows, int8_t* rowexp, uint8_t* mxexp,
+                        int diag_pert) {
+  const BatchSys& S = sys[blockIdx.y];
+  const BatchStep& T = steps[blockIdx.y];
+  const int m = T.m;
+  if (m <= 0 || (int)blockIdx.x * QROWS >= m || S.st->code != 0) return;
+  extern __shared__ __align__(16) float qtile[];
+  const int bs = b;                       // a step with rows below is a full block
+  const float* P = S.A + (size_t)s * S.ld + s + bs;
+  if (diag_pert) {
+    const float u = unit_roundoff(fmt);
+    for (int r = threadIdx.x; r < QROWS; r += QTHR) {
+      const int gi = blockIdx.x * QROWS + r;
+      if (gi < m) S.sh[s + bs + gi] += u * S.rowsq[s + bs + gi];
+    }
+  }
+  const size_t esz = (fmt == FP16 || fmt == FP16X2) ? 2 : 1;
+  void* qs = reinterpret_cast<uint8_t*>(q) + (size_t)T.q_row0 * bs * esz;
+  quantize_tile(P, S.ld, m, bs, fmt, qs, bs, rowexp + T.q_row0,
+                mxexp ? mxexp + (size_t)T.q_row0 * (bs / 32) : nullptr, bs / 32, qtile, qrows);
 }
 
 __global__ void quantize_elems_kernel(const float* __restrict__ x, void* q, long long count, int fmt) {
@@ -224,6 +252,19 @@ cudaError_t launch_quantize_hash(unsigned long long first, unsigned long long co
   long long blocks = (nch * 32 + 255) / 256;
   if (blocks > 148 * 16) blocks = 148 * 16;
   quantize_hash_kernel<<<(int)blocks, 256, 0, stream>>>(first, count, chunk, fmt, hashes);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_quantize_batched(BatchSys* sys, const BatchStep* steps, int nact, int s, int b,
+                                    int max_m, int fmt, void* q, int qrows, int8_t* rowexp,
+                                    uint8_t* mxexp, int diag_pert, cudaStream_t stream) {
+  if (nact <= 0 || max_m <= 0) return cudaSuccess;
+  const size_t smem = qtile_smem(b);
+  cudaError_t e = cudaFuncSetAttribute(quantize_batched_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  quantize_batched_kernel<<<dim3(ceil_div(max_m, QROWS), nact), QTHR, smem, stream>>>(
+      sys, steps, s, b, fmt, q, qrows, rowexp, mxexp, diag_pert);
   return cudaGetLastError();
 }
 

@@ -21,6 +21,7 @@
 #include <mutex>
 
 #include "common.cuh"
+#include "kernels.cuh"
 #include "pcg.cuh"
 
 namespace mpchol {
@@ -171,16 +172,16 @@ template <> struct ChunkOf<double> { static constexpr int value = 8; };
 
 // ---- y += A x, symmetric A, lower triangle only (one CTA per lower tile) ----
 template <typename TA, int NR>
-__global__ void __launch_bounds__(NTH)
-symv_kernel(const TA* __restrict__ A, int lda, int n, const double* __restrict__ x,
-            double* __restrict__ y, const int* skip) {
+__device__ __forceinline__ void
+symv_body(const TA* __restrict__ A, int lda, int n, const double* __restrict__ x,
+            double* __restrict__ y, const int* skip, uint3 bid) {
   if (skip != nullptr && *skip) return;
   __shared__ double s_xJ[RB * NR];
   __shared__ double s_xI[RB * NR];
   __shared__ double s_col[RB * NR];
   extern __shared__ double s_red[];
   int I, J;
-  tri_of(blockIdx.x, I, J);
+  tri_of(bid.x, I, J);
   const int i0 = I * RB, j0 = J * RB;
   const int ni = min(RB, n - i0), nj = min(RB, n - j0);
   load_vec<NR>(x, n, j0, nj, s_xJ);
@@ -199,6 +200,13 @@ symv_kernel(const TA* __restrict__ A, int lda, int n, const double* __restrict__
   flush_rows<NR>(acc, s_red, y, n, i0, ni, 1.0);
 }
 
+template <typename TA, int NR>
+__global__ void __launch_bounds__(NTH)
+symv_kernel(const TA* __restrict__ A, int lda, int n, const double* __restrict__ x,
+            double* __restrict__ y, const int* skip) {
+  symv_body<TA, NR>(A, lda, n, x, y, skip, blockIdx);
+}
+
 // ---- setup: super-block inverses by recursive doubling ---------------------
 // For a lower-triangular [A 0; B C], inv = [A^-1 0; X C^-1] with
 // X = -C^-1 (B A^-1).  The inverses W_S of the RS-row diagonal super-blocks
@@ -215,12 +223,12 @@ constexpr int BLD = RB + 1;     // padded column stride of the shared tiles
 // One 128-row diagonal block per CTA (256 threads), FP64 in shared memory;
 // the FP32 result goes to its diagonal tile of W_S.  Rows and columns past n
 // are identity.
-__global__ void __launch_bounds__(NTH)
-block_inverse_kernel(const float* __restrict__ L, int ldl, int n, float* __restrict__ wsup) {
+__device__ __forceinline__ void
+block_inverse_body(const float* __restrict__ L, int ldl, int n, float* __restrict__ wsup, uint3 bid) {
   extern __shared__ __align__(16) unsigned char sm_raw[];
   double* W = reinterpret_cast<double*>(sm_raw);            // [RB][BLD], column-major
   float* Ls = reinterpret_cast<float*>(W + RB * BLD);        // [RB][BLD], column-major
-  const int g = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = bid.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int i0 = g * RB;
   const int nb = min(RB, n - i0);
   for (int e = tid; e < RB * RB; e += NTH) {
@@ -307,6 +315,11 @@ block_inverse_kernel(const float* __restrict__ L, int ldl, int n, float* __restr
   }
 }
 
+__global__ void __launch_bounds__(NTH)
+block_inverse_kernel(const float* __restrict__ L, int ldl, int n, float* __restrict__ wsup) {
+  block_inverse_body(L, ldl, n, wsup, blockIdx);
+}
+
 // C(128x128) = A(128 x K) * B(K x 128), A and B column-major, FP32 FMA.
 // 256 threads, 8 x 8 outputs each (rows tx*4+{0..3}, 64+tx*4+{0..3}).
 __device__ void gemm128(const float* A, int lda, int a_rows_valid, const float* B, int ldb, int K,
@@ -347,13 +360,13 @@ __device__ __forceinline__ int acc_col(int b) { return b < 4 ? (threadIdx.x / 16
 // (128-tile indices relative to the pair's origin a0 = 2 h * pair).  Tiles
 // whose rows start at or past n are skipped: the solves never read them.
 template <int PHASE>
-__global__ void __launch_bounds__(NTH)
-superinv_gemm_kernel(const float* __restrict__ L, int ldl, int n, float* __restrict__ wsup, int h) {
+__device__ __forceinline__ void
+superinv_gemm_body(const float* __restrict__ L, int ldl, int n, float* __restrict__ wsup, int h, uint3 bid) {
   __shared__ __align__(16) float As[8 * RB];
   __shared__ __align__(16) float Bs[8 * RB];
   const int tpr = h / RB;
-  const int ti = blockIdx.x / tpr, tj = blockIdx.x % tpr;
-  const int S = blockIdx.z, s0 = S * RS, a0 = blockIdx.y * 2 * h;
+  const int ti = bid.x / tpr, tj = bid.x % tpr;
+  const int S = bid.z, s0 = S * RS, a0 = bid.y * 2 * h;
   const int grow = s0 + a0 + h + ti * RB;          // first global row of the output tile
   if (grow >= n) return;
   float* W = wsup + (size_t)S * RS * RS;
@@ -377,17 +390,23 @@ superinv_gemm_kernel(const float* __restrict__ L, int ldl, int n, float* __restr
   }
 }
 
+template <int PHASE>
+__global__ void __launch_bounds__(NTH)
+superinv_gemm_kernel(const float* __restrict__ L, int ldl, int n, float* __restrict__ wsup, int h) {
+  superinv_gemm_body<PHASE>(L, ldl, n, wsup, h, blockIdx);
+}
+
 // ---- y_S += W_S w_S (TRANS: z_S += W_S^T w_S) over the super-block's lower tiles
 template <int NR, bool TRANS>
-__global__ void __launch_bounds__(NTH)
-trmv_super_kernel(const float* __restrict__ W, int n, int s0, int rs, const double* __restrict__ in,
-                  double* __restrict__ out, const int* skip) {
+__device__ __forceinline__ void
+trmv_super_body(const float* __restrict__ W, int n, int s0, int rs, const double* __restrict__ in,
+                  double* __restrict__ out, const int* skip, uint3 bid) {
   if (skip != nullptr && *skip) return;
   __shared__ double s_v[RB * NR];
   __shared__ double s_col[RB * NR];
   extern __shared__ double s_red[];
   int i, j;
-  tri_of(blockIdx.x, i, j);
+  tri_of(bid.x, i, j);
   const int ri0 = s0 + i * RB, rj0 = s0 + j * RB;
   const int ni = min(RB, s0 + rs - ri0), nj = min(RB, s0 + rs - rj0);
   if (!TRANS) load_vec<NR>(in, n, rj0, nj, s_v);
@@ -407,24 +426,31 @@ trmv_super_kernel(const float* __restrict__ W, int n, int s0, int rs, const doub
   }
 }
 
+template <int NR, bool TRANS>
+__global__ void __launch_bounds__(NTH)
+trmv_super_kernel(const float* __restrict__ W, int n, int s0, int rs, const double* __restrict__ in,
+                  double* __restrict__ out, const int* skip) {
+  trmv_super_body<NR, TRANS>(W, n, s0, rs, in, out, skip, blockIdx);
+}
+
 // ---- panel updates ---------------------------------------------------------
 // forward: w[rows below the super-block] -= L(rows, super-block cols) y_S
 // backward: w[cols left of the super-block] -= L(super-block rows, cols)^T z_S
 template <int NR, bool TRANS>
-__global__ void __launch_bounds__(NTH)
-panel_kernel(const float* __restrict__ L, int ldl, int n, int s0, int rs,
-             const double* __restrict__ v, double* __restrict__ w, const int* skip) {
+__device__ __forceinline__ void
+panel_body(const float* __restrict__ L, int ldl, int n, int s0, int rs,
+             const double* __restrict__ v, double* __restrict__ w, const int* skip, uint3 bid) {
   if (skip != nullptr && *skip) return;
   __shared__ double s_v[RB * NR];
   __shared__ double s_col[RB * NR];
   extern __shared__ double s_red[];
   int r0, c0, nr_, nc_;
   if (!TRANS) {
-    r0 = s0 + rs + blockIdx.x * RB;  c0 = s0 + blockIdx.y * RB;
+    r0 = s0 + rs + bid.x * RB;  c0 = s0 + bid.y * RB;
     nr_ = min(RB, n - r0);           nc_ = min(RB, s0 + rs - c0);
     load_vec<NR>(v, n, c0, nc_, s_v);
   } else {
-    r0 = s0 + blockIdx.y * RB;       c0 = blockIdx.x * RB;
+    r0 = s0 + bid.y * RB;       c0 = bid.x * RB;
     nr_ = min(RB, s0 + rs - r0);     nc_ = min(RB, s0 - c0);
     load_vec<NR>(v, n, r0, nr_, s_v);
   }
@@ -441,6 +467,89 @@ panel_kernel(const float* __restrict__ L, int ldl, int n, int s0, int rs,
       if (c < nc_) atomicAdd(&w[(size_t)k * n + c0 + c], -s_col[e]);
     }
   }
+}
+
+template <int NR, bool TRANS>
+__global__ void __launch_bounds__(NTH)
+panel_kernel(const float* __restrict__ L, int ldl, int n, int s0, int rs,
+             const double* __restrict__ v, double* __restrict__ w, const int* skip) {
+  panel_body<NR, TRANS>(L, ldl, n, s0, rs, v, w, skip, blockIdx);
+}
+
+// ---- batched variants: one launch serves every system of a batch --------
+// blockIdx.y (or .z) selects the system; CTAs past a system's own extent
+// return at once.  Vectors live in the system's slots (n x NR column-major).
+__device__ __forceinline__ double* bslot(const BatchSys& S, int slot, int nr) {
+  return S.vec + (size_t)slot * S.n * nr;
+}
+
+template <int NR>
+__global__ void __launch_bounds__(NTH)
+symv_batched_kernel(const BatchSys* __restrict__ sys, int xslot, int yslot, int use_skip) {
+  const BatchSys& S = sys[blockIdx.y];
+  const int T = ceil_div(S.n, RB);
+  if ((int)blockIdx.x >= T * (T + 1) / 2) return;
+  symv_body<float, NR>(S.op, S.op_ld, S.n, bslot(S, xslot, NR), bslot(S, yslot, NR),
+                       use_skip ? S.done : nullptr, make_uint3(blockIdx.x, 0, 0));
+}
+
+// dst slot = 0 (src < 0) or a copy of the src slot
+__global__ void vec_slot_batched_kernel(const BatchSys* __restrict__ sys, int src, int dst, int nr,
+                                        int use_skip) {
+  const BatchSys& S = sys[blockIdx.y];
+  if (use_skip && S.done[0]) return;
+  const long long cnt = (long long)S.n * nr;
+  double* d = bslot(S, dst, nr);
+  const double* a = src >= 0 ? bslot(S, src, nr) : nullptr;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < cnt;
+       i += (long long)gridDim.x * blockDim.x)
+    d[i] = a ? a[i] : 0.0;
+}
+
+__global__ void __launch_bounds__(NTH)
+block_inverse_batched_kernel(const BatchSys* __restrict__ sys) {
+  const BatchSys& S = sys[blockIdx.y];
+  if ((int)blockIdx.x * RB >= S.n) return;
+  block_inverse_body(S.A, S.ld, S.n, S.wsup, make_uint3(blockIdx.x, 0, 0));
+}
+
+template <int PHASE>
+__global__ void __launch_bounds__(NTH)
+superinv_gemm_batched_kernel(const BatchSys* __restrict__ sys, int h, int max_super) {
+  const BatchSys& S = sys[blockIdx.z / max_super];
+  const int sup = blockIdx.z % max_super;
+  if (sup * RS >= S.n) return;
+  superinv_gemm_body<PHASE>(S.A, S.ld, S.n, S.wsup, h, make_uint3(blockIdx.x, blockIdx.y, sup));
+}
+
+template <int NR, bool TRANS>
+__global__ void __launch_bounds__(NTH)
+trmv_super_batched_kernel(const BatchSys* __restrict__ sys, int sup, int in_slot, int out_slot,
+                          int use_skip) {
+  const BatchSys& S = sys[blockIdx.y];
+  const int s0 = sup * RS;
+  if (s0 >= S.n) return;
+  const int rs = min(RS, S.n - s0);
+  const int nsub = ceil_div(rs, RB);
+  if ((int)blockIdx.x >= nsub * (nsub + 1) / 2) return;
+  trmv_super_body<NR, TRANS>(S.wsup + (size_t)sup * RS * RS, S.n, s0, rs, bslot(S, in_slot, NR),
+                             bslot(S, out_slot, NR), use_skip ? S.done : nullptr,
+                             make_uint3(blockIdx.x, 0, 0));
+}
+
+template <int NR, bool TRANS>
+__global__ void __launch_bounds__(NTH)
+panel_batched_kernel(const BatchSys* __restrict__ sys, int sup, int v_slot, int w_slot,
+                     int use_skip) {
+  const BatchSys& S = sys[blockIdx.z];
+  const int s0 = sup * RS;
+  if (s0 >= S.n) return;
+  const int rs = min(RS, S.n - s0);
+  const int nsub = ceil_div(rs, RB);
+  const int span = TRANS ? s0 : S.n - s0 - rs;      // rows below (forward) / columns left (backward)
+  if (span <= 0 || (int)blockIdx.x >= ceil_div(span, RB) || (int)blockIdx.y >= nsub) return;
+  panel_body<NR, TRANS>(S.A, S.ld, S.n, s0, rs, bslot(S, v_slot, NR), bslot(S, w_slot, NR),
+                        use_skip ? S.done : nullptr, make_uint3(blockIdx.x, blockIdx.y, 0));
 }
 
 template <int NR>
@@ -510,6 +619,15 @@ cudaError_t solve_set_attributes() {
   if ((e = set_dyn(panel_kernel<NRC, true>, red_bytes(NRC))) != cudaSuccess) return e;
   SET_NR(1) SET_NR(2) SET_NR(4) SET_NR(8)
 #undef SET_NR
+  if ((e = set_dyn(block_inverse_batched_kernel, inv)) != cudaSuccess) return e;
+#define SET_NRB(NRC)                                                                              \
+  if ((e = set_dyn(symv_batched_kernel<NRC>, red_bytes(NRC))) != cudaSuccess) return e;           \
+  if ((e = set_dyn(trmv_super_batched_kernel<NRC, false>, red_bytes(NRC))) != cudaSuccess) return e; \
+  if ((e = set_dyn(trmv_super_batched_kernel<NRC, true>, red_bytes(NRC))) != cudaSuccess) return e;  \
+  if ((e = set_dyn(panel_batched_kernel<NRC, false>, red_bytes(NRC))) != cudaSuccess) return e;      \
+  if ((e = set_dyn(panel_batched_kernel<NRC, true>, red_bytes(NRC))) != cudaSuccess) return e;
+  SET_NRB(1) SET_NRB(2) SET_NRB(4) SET_NRB(8)
+#undef SET_NRB
   return cudaSuccess;
 }
 
@@ -542,6 +660,58 @@ int solve_setup_launches(int n) {
   int k = 1;
   for (int h = RB; h < RS; h *= 2) k += 2;
   return k;
+}
+
+cudaError_t launch_vec_slot_batched(const BatchSys* sys, int nsys, int src, int dst, int nr,
+                                    int use_skip, cudaStream_t stream) {
+  vec_slot_batched_kernel<<<dim3(8, nsys), NTH, 0, stream>>>(sys, src, dst, nr, use_skip);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_symv_batched(const BatchSys* sys, int nsys, int max_n, int xslot, int yslot,
+                                int nr, int use_skip, cudaStream_t stream) {
+  cudaError_t e = launch_vec_slot_batched(sys, nsys, -1, yslot, nr, use_skip, stream);
+  if (e != cudaSuccess) return e;
+  const int T = ceil_div(max_n, RB);
+  NR_SWITCH(nr, (symv_batched_kernel<NRC><<<dim3(T * (T + 1) / 2, nsys), NTH, red_bytes(NRC), stream>>>(sys, xslot, yslot, use_skip)));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_solve_setup_batched(const BatchSys* sys, int nsys, int max_n,
+                                       cudaStream_t stream) {
+  const size_t inv = (size_t)RB * BLD * (sizeof(double) + sizeof(float));
+  block_inverse_batched_kernel<<<dim3(ceil_div(max_n, RB), nsys), NTH, inv, stream>>>(sys);
+  const int max_super = ceil_div(max_n, RS);
+  for (int h = RB; h < RS; h *= 2) {
+    const dim3 grid((h / RB) * (h / RB), RS / (2 * h), nsys * max_super);
+    superinv_gemm_batched_kernel<0><<<grid, NTH, 0, stream>>>(sys, h, max_super);
+    superinv_gemm_batched_kernel<1><<<grid, NTH, 0, stream>>>(sys, h, max_super);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_trsv_batched(bool backward, const BatchSys* sys, int nsys, int max_n,
+                                int in_slot, int out_slot, int work_slot, int nr, int use_skip,
+                                cudaStream_t stream) {
+  cudaError_t e = launch_vec_slot_batched(sys, nsys, in_slot, work_slot, nr, use_skip, stream);
+  if (e == cudaSuccess) e = launch_vec_slot_batched(sys, nsys, -1, out_slot, nr, use_skip, stream);
+  if (e != cudaSuccess) return e;
+  const int max_super = ceil_div(max_n, RS);
+  const int nsub_max = ceil_div(min(max_n, RS), RB);
+  const int span_tiles = ceil_div(max_n, RB);
+  for (int t = 0; t < max_super; ++t) {
+    const int sup = backward ? max_super - 1 - t : t;
+    const dim3 gt(nsub_max * (nsub_max + 1) / 2, nsys);
+    const dim3 gp(span_tiles, nsub_max, nsys);
+    if (!backward) {
+      NR_SWITCH(nr, (trmv_super_batched_kernel<NRC, false><<<gt, NTH, red_bytes(NRC), stream>>>(sys, sup, work_slot, out_slot, use_skip)));
+      NR_SWITCH(nr, (panel_batched_kernel<NRC, false><<<gp, NTH, red_bytes(NRC), stream>>>(sys, sup, out_slot, work_slot, use_skip)));
+    } else {
+      NR_SWITCH(nr, (trmv_super_batched_kernel<NRC, true><<<gt, NTH, red_bytes(NRC), stream>>>(sys, sup, work_slot, out_slot, use_skip)));
+      NR_SWITCH(nr, (panel_batched_kernel<NRC, true><<<gp, NTH, red_bytes(NRC), stream>>>(sys, sup, out_slot, work_slot, use_skip)));
+    }
+  }
+  return cudaGetLastError();
 }
 
 // out = L^-1 in (forward) or L^-T in (backward); work is an n x nrhs scratch.

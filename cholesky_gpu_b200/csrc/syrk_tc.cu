@@ -97,11 +97,55 @@ struct TcMaps {
   CUtensorMap lo;   // lo panel (FP16X2 only)
 };
 
-template <int FMT>
+// Batched launches: the tiles of all active systems are numbered in one
+// sequence (system i owns [steps[i].tile0, steps[i+1].tile0)); each system's
+// panel sits at rows steps[i].q_row0.. of the shared panel arena.
+struct TcBatch {
+  BatchSys* sys;
+  const BatchStep* steps;
+  int nact;
+  int s;
+  int b;
+};
+
+// Where tile t of the launch writes: C (ld ldc, m x m lower), its tile
+// coordinates and the first row of its panel in the panel arena.
+struct TileCtx {
+  int I, J;
+  float* C;
+  int ldc;
+  int m;
+  int row0;
+};
+
+template <bool BATCH>
+__device__ __forceinline__ TileCtx tile_ctx(int t, const TcBatch& bt, float* C, int ldc, int m) {
+  TileCtx c;
+  if (!BATCH) {
+    tile_of(t, c.I, c.J);
+    c.C = C; c.ldc = ldc; c.m = m; c.row0 = 0;
+    return c;
+  }
+  int lo = 0, hi = bt.nact - 1;           // last system with tile0 <= t
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (bt.steps[mid].tile0 <= t) lo = mid; else hi = mid - 1;
+  }
+  const BatchSys& S = bt.sys[lo];
+  const BatchStep& T = bt.steps[lo];
+  tile_of(t - T.tile0, c.I, c.J);
+  c.C = S.A + (size_t)(bt.s + bt.b) * S.ld + bt.s + bt.b;
+  c.ldc = S.ld;
+  c.m = T.m;
+  c.row0 = T.q_row0;
+  return c;
+}
+
+template <int FMT, bool BATCH>
 __global__ void __launch_bounds__(NTHREADS, 1)
 syrk_tc_kernel(const __grid_constant__ TcMaps maps, float* __restrict__ C, int ldc, int m, int k,
                const int8_t* __restrict__ rowexp, const uint8_t* __restrict__ mxexp, int ldmx,
-               const int* prec_sel, DevStatus* st) {
+               const int* prec_sel, DevStatus* st, TcBatch bt, int ntiles_b) {
   using Cfg = TcCfg<FMT>;
   if (st != nullptr && st->code != 0) return;
   if (prec_sel != nullptr && *prec_sel != FMT) return;
@@ -126,7 +170,7 @@ syrk_tc_kernel(const __grid_constant__ TcMaps maps, float* __restrict__ C, int l
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int T = (m + TM - 1) / TM;
-  const int ntiles = T * (T + 1) / 2;
+  const int ntiles = BATCH ? ntiles_b : T * (T + 1) / 2;
   const int nchunks = (k * Cfg::ESIZE) / CHUNK;
 
   if (threadIdx.x == 0) {
@@ -150,8 +194,8 @@ syrk_tc_kernel(const __grid_constant__ TcMaps maps, float* __restrict__ C, int l
     int c = 0;   // global chunk counter
     bool failed = false;
     for (int t = blockIdx.x; t < ntiles && !failed; t += gridDim.x) {
-      int I, J;
-      tile_of(t, I, J);
+      const TileCtx tc_ = tile_ctx<BATCH>(t, bt, C, ldc, m);
+      const int I = tc_.I, J = tc_.J;
       const bool diag = (I == J);
       const uint32_t bytes = (uint32_t)((diag ? 1 : 2) * NSETS * STRIP);
       for (int kc = 0; kc < nchunks; ++kc, ++c) {
@@ -171,20 +215,22 @@ syrk_tc_kernel(const __grid_constant__ TcMaps maps, float* __restrict__ C, int l
         uint8_t* base = smem + (size_t)s * STAGE_BYTES;
         if (MX) {
           uint8_t* sf = base + 2 * NSETS * STRIP;
-          stage_scales(sf, mxexp, ldmx, I * TM, m, kc, lane);
-          if (!diag) stage_scales(sf + SF_BYTES, mxexp, ldmx, J * TM, m, kc, lane);
+          const uint8_t* mx = mxexp + (size_t)tc_.row0 * ldmx;
+          stage_scales(sf, mx, ldmx, I * TM, tc_.m, kc, lane);
+          if (!diag) stage_scales(sf + SF_BYTES, mx, ldmx, J * TM, tc_.m, kc, lane);
           tc::fence_proxy_async_smem();    // generic writes -> async-proxy reader
           __syncwarp();
         }
         if (lane == 0) {
           tc::mbar_expect_tx(&full_bar[s], bytes);
           const int x = kc * ELEMS_PER_CHUNK;
-          tc::tma_load_2d(base, &maps.hi, &full_bar[s], x, I * TM);
-          if (NSETS == 2) tc::tma_load_2d(base + STRIP, &maps.lo, &full_bar[s], x, I * TM);
+          const int yi = tc_.row0 + I * TM, yj = tc_.row0 + J * TM;
+          tc::tma_load_2d(base, &maps.hi, &full_bar[s], x, yi);
+          if (NSETS == 2) tc::tma_load_2d(base + STRIP, &maps.lo, &full_bar[s], x, yi);
           if (!diag) {
-            tc::tma_load_2d(base + NSETS * STRIP, &maps.hi, &full_bar[s], x, J * TM);
+            tc::tma_load_2d(base + NSETS * STRIP, &maps.hi, &full_bar[s], x, yj);
             if (NSETS == 2)
-              tc::tma_load_2d(base + (NSETS + 1) * STRIP, &maps.lo, &full_bar[s], x, J * TM);
+              tc::tma_load_2d(base + (NSETS + 1) * STRIP, &maps.lo, &full_bar[s], x, yj);
           }
         }
       }
@@ -194,9 +240,8 @@ syrk_tc_kernel(const __grid_constant__ TcMaps maps, float* __restrict__ C, int l
     if (lane == 0) {
       int c = 0, tcount = 0;
       for (int t = blockIdx.x; t < ntiles && !abort_sh; t += gridDim.x, ++tcount) {
-        int I, J;
-        tile_of(t, I, J);
-        const bool diag = (I == J);
+        const TileCtx tc_ = tile_ctx<BATCH>(t, bt, C, ldc, m);
+        const bool diag = (tc_.I == tc_.J);
         const int buf = tcount & 1;
         const uint32_t use = (uint32_t)(tcount >> 1);
         if (!tc::mbar_wait(&acce_bar[buf], (use & 1u) ^ 1u)) {
@@ -261,8 +306,11 @@ syrk_tc_kernel(const __grid_constant__ TcMaps maps, float* __restrict__ C, int l
     const int q = warp & 3;                  // TMEM lane quarter this warp may access
     int tcount = 0;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++tcount) {
-      int I, J;
-      tile_of(t, I, J);
+      const TileCtx tc_ = tile_ctx<BATCH>(t, bt, C, ldc, m);
+      const int I = tc_.I, J = tc_.J;
+      float* Ct = tc_.C;
+      const int ldct = tc_.ldc, mt = tc_.m;
+      const int8_t* rexp = rowexp + tc_.row0;
       const int buf = tcount & 1;
       const uint32_t use = (uint32_t)(tcount >> 1);
       if (!tc::mbar_wait(&accf_bar[buf], use & 1u)) {
@@ -271,7 +319,7 @@ syrk_tc_kernel(const __grid_constant__ TcMaps maps, float* __restrict__ C, int l
       }
       tc::tc_fence_after();
       const int i = I * TM + q * 32 + lane;
-      const float si = (i < m) ? (MX ? 1.0f : pow2f(rowexp[i])) : 0.0f;
+      const float si = (i < mt) ? (MX ? 1.0f : pow2f(rexp[i])) : 0.0f;
       const uint32_t taddr = tmem + (uint32_t)(buf * TM) + ((uint32_t)(q * 32) << 16);
 #pragma unroll 1
       for (int c0 = 0; c0 < TM; c0 += 32) {
@@ -284,18 +332,18 @@ syrk_tc_kernel(const __grid_constant__ TcMaps maps, float* __restrict__ C, int l
           if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tc::smem_u32(&acce_bar[buf])) : "memory");
         }
         const int j0 = J * TM + c0;
-        if (i < m) {
+        if (i < mt) {
           float cv[32];
 #pragma unroll
           for (int u = 0; u < 32; ++u) {
             const int j = j0 + u;
-            cv[u] = (j < m && i >= j) ? C[(size_t)j * ldc + i] : 0.0f;
+            cv[u] = (j < mt && i >= j) ? Ct[(size_t)j * ldct + i] : 0.0f;
           }
 #pragma unroll
           for (int u = 0; u < 32; ++u) {
             const int j = j0 + u;
-            if (j < m && i >= j)
-              C[(size_t)j * ldc + i] = cv[u] - (v[u] * si) * (MX ? 1.0f : pow2f(rowexp[j]));
+            if (j < mt && i >= j)
+              Ct[(size_t)j * ldct + i] = cv[u] - (v[u] * si) * (MX ? 1.0f : pow2f(rexp[j]));
           }
         }
       }
@@ -315,12 +363,12 @@ size_t tc_smem() {
   return (size_t)Cfg::NSTAGE * (2 * Cfg::NSETS * STRIP + (Cfg::MX ? 2 * SF_BYTES : 0)) + 1024;
 }
 
-template <int FMT>
+template <int FMT, bool BATCH>
 cudaError_t launch_fmt(const TcMaps& maps, float* C, int ldc, int m, int k, const int8_t* rowexp,
                        const uint8_t* mxexp, int ldmx, const int* prec_sel, DevStatus* st,
-                       cudaStream_t stream) {
+                       const TcBatch& bt, int ntiles_b, cudaStream_t stream) {
   const size_t smem = tc_smem<FMT>();
-  cudaError_t e = cudaFuncSetAttribute(syrk_tc_kernel<FMT>,
+  cudaError_t e = cudaFuncSetAttribute(syrk_tc_kernel<FMT, BATCH>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int nsm = 148;
@@ -328,10 +376,10 @@ cudaError_t launch_fmt(const TcMaps& maps, float* C, int ldc, int m, int k, cons
   if (cudaGetDevice(&dev) == cudaSuccess)
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   const int T = ceil_div(m, TM);
-  const int ntiles = T * (T + 1) / 2;
+  const int ntiles = BATCH ? ntiles_b : T * (T + 1) / 2;
   const int grid = ntiles < nsm ? ntiles : nsm;
-  syrk_tc_kernel<FMT><<<grid, NTHREADS, smem, stream>>>(maps, C, ldc, m, k, rowexp, mxexp, ldmx,
-                                                        prec_sel, st);
+  syrk_tc_kernel<FMT, BATCH><<<grid, NTHREADS, smem, stream>>>(maps, C, ldc, m, k, rowexp, mxexp,
+                                                               ldmx, prec_sel, st, bt, ntiles_b);
   return cudaGetLastError();
 }
 
@@ -365,11 +413,42 @@ cudaError_t launch_syrk_tc(float* C, int ldc, int m, int k, int fmt, const void*
       return cudaErrorInvalidValue;
   }
   switch (fmt) {
-    case FP16: return launch_fmt<FP16>(maps, C, ldc, m, k, rowexp, mxexp, ldmx, prec_sel, st, stream);
-    case E4M3: return launch_fmt<E4M3>(maps, C, ldc, m, k, rowexp, mxexp, ldmx, prec_sel, st, stream);
-    case E5M2: return launch_fmt<E5M2>(maps, C, ldc, m, k, rowexp, mxexp, ldmx, prec_sel, st, stream);
-    case FP16X2: return launch_fmt<FP16X2>(maps, C, ldc, m, k, rowexp, mxexp, ldmx, prec_sel, st, stream);
-    case MXFP8: return launch_fmt<MXFP8>(maps, C, ldc, m, k, rowexp, mxexp, ldmx, prec_sel, st, stream);
+    case FP16: return launch_fmt<FP16, false>(maps, C, ldc, m, k, rowexp, mxexp, ldmx, prec_sel, st, TcBatch{}, 0, stream);
+    case E4M3: return launch_fmt<E4M3, false>(maps, C, ldc, m, k, rowexp, mxexp, ldmx, prec_sel, st, TcBatch{}, 0, stream);
+    case E5M2: return launch_fmt<E5M2, false>(maps, C, ldc, m, k, rowexp, mxexp, ldmx, prec_sel, st, TcBatch{}, 0, stream);
+    case FP16X2: return launch_fmt<FP16X2, false>(maps, C, ldc, m, k, rowexp, mxexp, ldmx, prec_sel, st, TcBatch{}, 0, stream);
+    case MXFP8: return launch_fmt<MXFP8, false>(maps, C, ldc, m, k, rowexp, mxexp, ldmx, prec_sel, st, TcBatch{}, 0, stream);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_syrk_tc_batched(BatchSys* sys, const BatchStep* steps, int nact, int ntiles,
+                                   int s, int b, int fmt, const void* q, int qrows,
+                                   const int8_t* rowexp, const uint8_t* mxexp,
+                                   cudaStream_t stream) {
+  if (nact <= 0 || ntiles <= 0) return cudaSuccess;
+  if (!syrk_tc_supported(fmt, b)) return cudaErrorInvalidValue;
+  const int esize = (fmt == FP16 || fmt == FP16X2) ? 2 : 1;
+  const CUtensorMapDataType dt = esize == 2 ? CU_TENSOR_MAP_DATA_TYPE_UINT16 : CU_TENSOR_MAP_DATA_TYPE_UINT8;
+  TcMaps maps;
+  if (!encode_tmap_2d(&maps.hi, dt, esize, q, (uint64_t)b, (uint64_t)qrows, (uint64_t)b,
+                      CHUNK / esize, TM, CU_TENSOR_MAP_SWIZZLE_128B))
+    return cudaErrorInvalidValue;
+  maps.lo = maps.hi;
+  if (fmt == FP16X2) {
+    const uint16_t* lo = reinterpret_cast<const uint16_t*>(q) + (size_t)qrows * b;
+    if (!encode_tmap_2d(&maps.lo, dt, esize, lo, (uint64_t)b, (uint64_t)qrows, (uint64_t)b,
+                        CHUNK / esize, TM, CU_TENSOR_MAP_SWIZZLE_128B))
+      return cudaErrorInvalidValue;
+  }
+  const TcBatch bt{sys, steps, nact, s, b};
+  const int ldmx = b / 32;
+  switch (fmt) {
+    case FP16: return launch_fmt<FP16, true>(maps, nullptr, 0, 0, b, rowexp, mxexp, ldmx, nullptr, nullptr, bt, ntiles, stream);
+    case E4M3: return launch_fmt<E4M3, true>(maps, nullptr, 0, 0, b, rowexp, mxexp, ldmx, nullptr, nullptr, bt, ntiles, stream);
+    case E5M2: return launch_fmt<E5M2, true>(maps, nullptr, 0, 0, b, rowexp, mxexp, ldmx, nullptr, nullptr, bt, ntiles, stream);
+    case FP16X2: return launch_fmt<FP16X2, true>(maps, nullptr, 0, 0, b, rowexp, mxexp, ldmx, nullptr, nullptr, bt, ntiles, stream);
+    case MXFP8: return launch_fmt<MXFP8, true>(maps, nullptr, 0, 0, b, rowexp, mxexp, ldmx, nullptr, nullptr, bt, ntiles, stream);
     default: return cudaErrorInvalidValue;
   }
 }

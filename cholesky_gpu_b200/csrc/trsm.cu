@@ -35,48 +35,9 @@ size_t trsm_smem_floats(int bs) {
   return (size_t)bs * XLD + (size_t)(NT * (NT - 1) / 2) * TSZ + (size_t)NT * TSZ;
 }
 
-__global__ void __launch_bounds__(NTHR)
-trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_constant__ CUtensorMap tmap32,
-                  int n, int s, int bs, const float* __restrict__ winv,
-                  const float* __restrict__ d, float* __restrict__ dtilde, float* __restrict__ rowsq,
-                  StepState* step, StepState* next, int next_bs, DecisionParams dp, DevStatus* st) {
-  if (st->code != 0) return;
-  extern __shared__ __align__(128) float sm[];
-  const int NT = bs / 32;
-  float* Xs = sm;                                        // [bs][XLD]
-  float* Lt = Xs + (size_t)bs * XLD;                     // strictly-lower tiles of L11
-  float* Wt = Lt + (size_t)(NT * (NT - 1) / 2) * TSZ;    // inverses of the diagonal tiles
-  __shared__ float red_max[NTHR / 32];
-  __shared__ int red_lit[NTHR / 32];
-  __shared__ __align__(8) uint64_t bar;
-  __shared__ int s_ok;
-
-  const int tid = threadIdx.x;
-  const int row0 = s + bs + blockIdx.x * TR;   // first global row of this CTA
-  const int nrows = min(TR, n - row0);
-  if (nrows <= 0) return;
-
-  // ---- stage with TMA (rows past n arrive as zeros) -----------------------
-  if (tid == 0) {
-    s_ok = 1;
-    const int nlt = NT * (NT - 1) / 2;
-    tc::mbar_init(&bar, 1);
-    tc::fence_mbar_init();
-    tc::mbar_expect_tx(&bar, (uint32_t)((bs * XLD + nlt * TSZ + NT * TSZ) * sizeof(float)));
-    tc::tma_load_2d(Xs, &tmapX, &bar, row0, s);
-    for (int I = 1; I < NT; ++I)
-      for (int M = 0; M < I; ++M)
-        tc::tma_load_2d(Lt + tl(I, M) * TSZ, &tmap32, &bar, s + 32 * I, s + 32 * M);
-    tc::bulk_load_1d(Wt, winv, (uint32_t)(NT * TSZ * sizeof(float)), &bar);
-    if (!tc::mbar_wait(&bar, 0)) {
-      s_ok = 0;
-      set_status(st, MPCHOL_ERR_TIMEOUT, row0);
-      tc::mbar_wait(&bar, 0);
-    }
-  }
-  __syncthreads();
-  if (!s_ok) return;
-
+// Solve the staged 64-row slab in place: for each 32-column tile J,
+// X_J -= X_{<J} L_{J,<J}^T (register-tiled), then X_J = X_J L_JJ^-T.
+__device__ void trsm_slab(float* Xs, const float* Lt, const float* Wt, int NT, int tid) {
   const int tr = tid % 16, tc_ = tid / 16;   // 4 rows x 2 cols per thread
   for (int J = 0; J < NT; ++J) {
     const int kend = 32 * J;
@@ -124,6 +85,51 @@ trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_consta
       for (int j = 0; j < 2; ++j) Xs[(kend + 2 * tc_ + j) * XLD + 4 * tr + i] = out[i][j];
     __syncthreads();
   }
+}
+
+__global__ void __launch_bounds__(NTHR)
+trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_constant__ CUtensorMap tmap32,
+                  int n, int s, int bs, const float* __restrict__ winv,
+                  const float* __restrict__ d, float* __restrict__ dtilde, float* __restrict__ rowsq,
+                  StepState* step, StepState* next, int next_bs, DecisionParams dp, DevStatus* st) {
+  if (st->code != 0) return;
+  extern __shared__ __align__(128) float sm[];
+  const int NT = bs / 32;
+  float* Xs = sm;                                        // [bs][XLD]
+  float* Lt = Xs + (size_t)bs * XLD;                     // strictly-lower tiles of L11
+  float* Wt = Lt + (size_t)(NT * (NT - 1) / 2) * TSZ;    // inverses of the diagonal tiles
+  __shared__ float red_max[NTHR / 32];
+  __shared__ int red_lit[NTHR / 32];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int s_ok;
+
+  const int tid = threadIdx.x;
+  const int row0 = s + bs + blockIdx.x * TR;   // first global row of this CTA
+  const int nrows = min(TR, n - row0);
+  if (nrows <= 0) return;
+
+  // ---- stage with TMA (rows past n arrive as zeros) -----------------------
+  if (tid == 0) {
+    s_ok = 1;
+    const int nlt = NT * (NT - 1) / 2;
+    tc::mbar_init(&bar, 1);
+    tc::fence_mbar_init();
+    tc::mbar_expect_tx(&bar, (uint32_t)((bs * XLD + nlt * TSZ + NT * TSZ) * sizeof(float)));
+    tc::tma_load_2d(Xs, &tmapX, &bar, row0, s);
+    for (int I = 1; I < NT; ++I)
+      for (int M = 0; M < I; ++M)
+        tc::tma_load_2d(Lt + tl(I, M) * TSZ, &tmap32, &bar, s + 32 * I, s + 32 * M);
+    tc::bulk_load_1d(Wt, winv, (uint32_t)(NT * TSZ * sizeof(float)), &bar);
+    if (!tc::mbar_wait(&bar, 0)) {
+      s_ok = 0;
+      set_status(st, MPCHOL_ERR_TIMEOUT, row0);
+      tc::mbar_wait(&bar, 0);
+    }
+  }
+  __syncthreads();
+  if (!s_ok) return;
+
+  trsm_slab(Xs, Lt, Wt, NT, tid);
   // ---- write the solved slab back (TMA store clips rows past n) -----------
   tc::fence_proxy_async_smem();
   __syncthreads();
@@ -169,6 +175,51 @@ trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_consta
   }
 }
 
+// Batched: blockIdx.y = system, blockIdx.x = 64-row slab.  Staging by
+// plain coalesced loads (no per-system tensor maps); the epilogue keeps the
+// row sums of squares (rounding-shift estimate) and the diagonal tracker.
+__global__ void __launch_bounds__(NTHR)
+trsm_batched_kernel(BatchSys* __restrict__ sys, int s, int b) {
+  const BatchSys& S = sys[blockIdx.y];
+  const int n = S.n;
+  const int bs = min(b, n - s);
+  const int row0 = s + bs + blockIdx.x * TR;
+  const int nrows = min(TR, n - row0);
+  if (bs <= 0 || nrows <= 0 || S.st->code != 0) return;
+  extern __shared__ __align__(128) float sm[];
+  const int NT = bs / 32;                     // bs == b: only the last block can be partial
+  float* Xs = sm;
+  float* Lt = Xs + (size_t)bs * XLD;
+  float* Wt = Lt + (size_t)(NT * (NT - 1) / 2) * TSZ;
+  const int tid = threadIdx.x;
+  const float* A = S.A;
+  const int ld = S.ld;
+  for (int e = tid; e < bs * TR; e += NTHR) {
+    const int c = e / TR, r = e % TR;
+    Xs[c * XLD + r] = (r < nrows) ? A[(size_t)(s + c) * ld + row0 + r] : 0.0f;
+  }
+  for (int I = 1; I < NT; ++I)
+    for (int M = 0; M < I; ++M)
+      for (int e = tid; e < TSZ; e += NTHR) {
+        const int c = e / 32, r = e % 32;
+        Lt[tl(I, M) * TSZ + e] = A[(size_t)(s + 32 * M + c) * ld + s + 32 * I + r];
+      }
+  for (int e = tid; e < NT * TSZ; e += NTHR) Wt[e] = S.winv[e];
+  __syncthreads();
+  trsm_slab(Xs, Lt, Wt, NT, tid);
+  for (int e = tid; e < bs * TR; e += NTHR) {
+    const int c = e / TR, r = e % TR;
+    if (r < nrows) S.A[(size_t)(s + c) * ld + row0 + r] = Xs[c * XLD + r];
+  }
+  if (tid < nrows) {
+    const int gi = row0 + tid;
+    float sq = 0.0f;
+    for (int c = 0; c < bs; ++c) { const float v = Xs[c * XLD + tid]; sq += v * v; }
+    S.rowsq[gi] = sq;
+    S.dtilde[gi] -= sq;
+  }
+}
+
 }  // namespace
 
 cudaError_t launch_trsm_panel(const CUtensorMap& tmapX, const CUtensorMap& tmap32, int n, int s,
@@ -185,6 +236,17 @@ cudaError_t launch_trsm_panel(const CUtensorMap& tmapX, const CUtensorMap& tmap3
   trsm_panel_kernel<<<ceil_div(m, TR), NTHR, smem, stream>>>(tmapX, tmap32, n, s, bs, winv, d,
                                                              dtilde, rowsq, step, next, next_bs,
                                                              dp, st);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_trsm_batched(BatchSys* sys, int nact, int s, int b, int max_m,
+                                cudaStream_t stream) {
+  if (nact <= 0 || max_m <= 0) return cudaSuccess;
+  const size_t smem = trsm_smem_floats(b) * sizeof(float);
+  cudaError_t e = cudaFuncSetAttribute(trsm_batched_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  trsm_batched_kernel<<<dim3(ceil_div(max_m, TR), nact), NTHR, smem, stream>>>(sys, s, b);
   return cudaGetLastError();
 }
 

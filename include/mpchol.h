@@ -237,6 +237,37 @@ MPCHOL_API mpchol_status mpchol_syrk_update(float* dC, int ldc, int m, int k, in
                                  const void* dScale, const float* dP, int ldp,
                                  mpchol_stream_t stream);
 
+/* ---- batches of independent systems of uneven size --------------------- */
+/* No counterpart in the reference (one system per precond_CG call).  All
+ * systems share the options (a fixed tensor-core precision: FP16, E4M3,
+ * E5M2, MXFP8 or FP16X2; not FP32 or SWITCHING) and the rhs count; every
+ * kernel launch serves all of them.  ns[i] is the order of system i; arrays
+ * passed to the calls below are indexed in that same (caller) order and hold
+ * device pointers.  Matrices are FP32 column-major (ld lda[i]) with the lower
+ * triangle read; B and X are n_i x nrhs FP64 column-major (ld n_i).
+ *   mpchol_batch_factor: one CUDA graph launch factors every system (and
+ *     forms the solve data); blocks the host until it has read the pointer
+ *     tables.
+ *   mpchol_batch_pcg: PCG of every system in lockstep (converged ones skip),
+ *     FP64 true residual per system; reports[i] per system (may be NULL).
+ *     Returns OK if every system converged, PCG_MAXIT otherwise. */
+typedef struct mpchol_batch mpchol_batch_t;
+MPCHOL_API mpchol_status mpchol_batch_create(const mpchol_opts* opts, int count, const int* ns,
+                                             int nrhs, mpchol_batch_t** out);
+MPCHOL_API mpchol_status mpchol_batch_factor(mpchol_batch_t* b, const float* const* dA,
+                                             const int* lda, mpchol_stream_t stream);
+/* the factor of system `index` (caller order): device pointer, ld, n */
+MPCHOL_API mpchol_status mpchol_batch_lower(const mpchol_batch_t* b, int index, const float** dL,
+                                            int* ldl, int* n);
+/* per-system factor status (mpchol_status), failing row and floored-pivot count */
+MPCHOL_API mpchol_status mpchol_batch_info(mpchol_batch_t* b, int* status, int* fail_row,
+                                           int* n_perturbed, mpchol_stream_t stream);
+MPCHOL_API mpchol_status mpchol_batch_pcg(mpchol_batch_t* b, const float* const* dA,
+                                          const int* lda, const double* const* dB,
+                                          double* const* dX, const mpchol_pcg_opts* opts,
+                                          mpchol_report* reports, mpchol_stream_t stream);
+MPCHOL_API mpchol_status mpchol_batch_destroy(mpchol_batch_t* b);
+
 /* ---- Gaussian RBF kernel matrices (no reference arithmetic: src/RBF.cu is a stub)
  * dX: n points x d features, row-major FP32 (ld = ldx).  Writes
  *   K_ij = exp(-||x_i - x_j||^2 / (2 lengthscale^2)) + nugget * delta_ij
