@@ -59,6 +59,11 @@ def parse():
     ap.add_argument("--max-it", type=int, default=400)
     ap.add_argument("--check-every", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="spd", choices=["spd", "rbf", "rbf-grad", "batch"],
+                    help="spd: the dense SPD time-to-solution workload (default); rbf: Gaussian "
+                         "RBF kernel matrix, n=16384 points in [0,1]^784, 8 rhs; rbf-grad: "
+                         "forward + adjoint gradients of 1/2 y^T K^-1 y, n=8192, d=64; batch: "
+                         "512 SPD systems of order U[64, 2048]")
     return ap.parse_args()
 
 
@@ -475,11 +480,185 @@ def run_reference(args, world, rank):
     }
 
 
+# ---------------------------------------------------------------- other workloads
+def _timed(fn, steps, warmup, stream):
+    import torch
+    for _ in range(warmup):
+        fn()
+    times, last = [], None
+    for _ in range(steps):
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        last = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    return statistics.median(times), last
+
+
+def _base(args, world, value, unit, dtype, data, config, extra):
+    out = {"metric": METRIC, "value": round(value, 3), "unit": unit, "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(value, 3),
+           "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
+           "data": data, "config": config}
+    out.update(extra)
+    return out
+
+
+def run_rbf(args, world, rank, local):
+    """Gaussian RBF kernel matrix: n = 16384 points, 80 % zero coordinates,
+    the rest U(0,1) in [0,1]^784 (seeded stand-in for image data);
+    l = exact median pairwise distance; nugget 1e-3; 8 rhs.  One step =
+    factor + PCG to the tolerance (the kernel-matrix build is timed apart)."""
+    import torch
+    import cholesky_gpu_b200 as mp
+    from cholesky_gpu_b200 import autograd as AG, matgen
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n = args.n if args.n != 8192 else 16384
+    X = torch.from_numpy(matgen.mnist_like_points(n, 784, 4 + rank)).to(dev)
+    ell = matgen.median_pairwise_distance(X)
+    stream = torch.cuda.current_stream(dev)
+    t_build, (_, K32) = _timed(lambda: AG.rbf_build(X, ell, 1e-3, fp64=False), 1, 1, stream)
+    B = matgen.rhs(n, 8, 5 + rank, device=dev)
+    prec = args.precision
+    mixed = dict(block_size=args.block, precision=prec)
+    if prec == "switching":
+        # MXFP8 first: the criterion keeps it only where the Schur diagonal allows
+        mixed.update(eps_prime=args.eps_prime, ladder=["mxfp8", "fp16", "fp16x2"])
+    arms = {prec: mp.Factor(n, **mixed),
+            "fp32": mp.Factor(n, block_size=args.block, precision="fp32")}
+    res = {}
+    for name, f in arms.items():
+        def step(f=f):
+            f.compute(K32)
+            return f.pcg(K32, B, rel_tol=args.tol, max_it=args.max_it, check_every=args.check_every)
+        ms, (X_, rep) = _timed(step, args.steps, args.warmup, stream)
+        res[name] = (ms, rep)
+    ms, rep = res[prec]
+    info = arms[prec].info()
+    steps_used = {nm: info.steps_by_prec[i] for i, nm in
+                  ((0, "fp32"), (1, "fp16"), (2, "e4m3"), (3, "e5m2"), (4, "mxfp8"), (6, "fp16x2"))
+                  if info.steps_by_prec[i]}
+    return _base(args, world, ms, "ms", f"{'/'.join(steps_used) or prec} factor, fp64 pcg",
+                 "synthetic (seeded sparse points in [0,1]^784, RBF kernel)",
+                 {"workload": f"rbf n={n} d=784 l=median({ell:.3f}) nugget=1e-3 rhs=8 {prec}",
+                  "n": n, "block": args.block, "rhs": 8, "tol": args.tol},
+                 {"comparator_fp32_factor_ms": round(res["fp32"][0], 3),
+                  "speedup_vs_fp32_factor": round(res["fp32"][0] / ms, 3),
+                  "iterations": {k: v[1].iterations for k, v in res.items()},
+                  "converged": {k: v[1].converged for k, v in res.items()},
+                  "rel_residual": {k: v[1].rel_residual for k, v in res.items()},
+                  "kernel_build_ms": round(t_build, 3), "step_precisions": steps_used})
+
+
+def run_rbf_grad(args, world, rank, local):
+    """Differentiation workload: RBF kernel, n = 8192 points x ~ N(0, I_64),
+    l = 4, nugget 1e-2, y ~ N(0,1); one step = forward solve + backward
+    (adjoint PCG reusing the factor, fused gradient contraction)."""
+    import torch
+    from cholesky_gpu_b200 import autograd as AG, matgen
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n = args.n if args.n != 8192 else 8192
+    X0 = torch.from_numpy(matgen.gaussian_points(n, 64, 6 + rank)).to(dev)
+    y = torch.from_numpy(np.random.default_rng(7 + rank).standard_normal(n)).to(dev)
+    stream = torch.cuda.current_stream(dev)
+    prec = args.precision
+    res = {}
+    for name in (prec, "fp32"):
+        fopts = dict(block_size=args.block, precision=name)
+        if name == "switching":
+            fopts.update(eps_prime=args.eps_prime, ladder=["e4m3", "fp16", "fp16x2"])
+
+        def step(fopts=fopts):
+            Xt = X0.clone().requires_grad_(True)
+            ell = torch.tensor(4.0, dtype=torch.float64, requires_grad=True)
+            lam = torch.tensor(1e-2, dtype=torch.float64, requires_grad=True)
+            x = AG.rbf_solve(Xt, ell, lam, y, rel_tol=1e-12, max_it=args.max_it, **fopts)
+            loss = 0.5 * (y * x).sum()
+            loss.backward()
+            return loss.item(), ell.grad.item(), lam.grad.item()
+        res[name] = _timed(step, args.steps, args.warmup, stream)
+    ms, (loss, gl, gn) = res[prec]
+    return _base(args, world, ms, "ms", f"{prec} factor, fp64 pcg + fp64 gradients",
+                 "synthetic (seeded x ~ N(0, I_64))",
+                 {"workload": f"rbf-grad n={n} d=64 l=4 nugget=1e-2 {prec}", "n": n,
+                  "block": args.block, "tol": 1e-12},
+                 {"comparator_fp32_factor_ms": round(res["fp32"][0], 3),
+                  "speedup_vs_fp32_factor": round(res["fp32"][0] / ms, 3),
+                  "loss": loss, "dL_dl": gl, "dL_dnugget": gn})
+
+
+def run_batch(args, world, rank, local):
+    """512 SPD systems, n_i ~ U[64, 2048], kappa_i log-uniform in [1e2, 1e6]
+    (seeded), 4 rhs each; one step = batched factor + lockstep PCG of all."""
+    import torch
+    import cholesky_gpu_b200 as mp
+    from cholesky_gpu_b200 import matgen
+    from cholesky_gpu_b200.shard import gather_by_system, max_over_ranks, partition_systems
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    count = 512
+    # the same 512 systems for every world size; each rank owns a shard (no
+    # data-path collective: systems are independent)
+    ns_all = [int(v) for v in matgen.batch_sizes(count, 64, 2048, 8)]
+    ks = matgen.batch_kappas(count, 1e2, 1e6, 9)
+    mine = partition_systems(ns_all, world)[rank]
+    ns = [ns_all[i] for i in mine]
+    As = [matgen.spd_matrix(ns_all[i], float(ks[i]), i, device=dev) for i in mine]
+    Bs = [matgen.rhs(ns_all[i], 4, 7000 + i, device=dev) for i in mine]
+    stream = torch.cuda.current_stream(dev)
+    prec = args.precision if args.precision != "switching" else "fp16x2"
+    bt = mp.Batch(ns, nrhs=4, block_size=128, precision=prec)
+
+    def step():
+        if dist is not None:
+            dist.barrier()
+        bt.factor(As)
+        return bt.pcg(As, Bs, rel_tol=args.tol, max_it=args.max_it, check_every=args.check_every)
+    ms, (Xs, reps, st) = _timed(step, args.steps, args.warmup, stream)
+    ms = max_over_ranks(ms, dist)
+    allrep = gather_by_system({i: (r.iterations, r.converged) for i, r in zip(mine, reps)},
+                              count, dist)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return None
+    its = [r[0] for r in allrep]
+    flops = sum(n ** 3 / 3.0 for n in ns_all)
+    return _base(args, world, ms, "ms", f"{prec} factor, fp64 pcg",
+                 "synthetic (seeded Q diag(sigma) Q^T per system)",
+                 {"workload": f"batch 512 systems n~U[64,2048] kappa~logU[1e2,1e6] rhs=4 {prec}",
+                  "systems": count, "block": 128, "rhs": 4, "tol": args.tol,
+                  "parallelism": f"systems sharded over {world} GPUs" if world > 1 else "single GPU"},
+                 {"scaling": "strong",
+                  "solves_per_s": round(count / (ms * 1e-3), 1),
+                  "ms_per_system": round(ms / count, 4),
+                  "all_converged": all(r[1] for r in allrep),
+                  "iterations": {"max": max(its), "median": statistics.median(its)},
+                  "factor_tflops_equiv": round(flops / (ms * 1e-3) / 1e12, 2)})
+
+
 def main():
     args = parse()
     world, rank, local = dist_init(args)
     if args.impl == "reference":
         out = run_reference(args, world, rank)
+    elif args.workload == "rbf":
+        out = run_rbf(args, world, rank, local)
+    elif args.workload == "rbf-grad":
+        out = run_rbf_grad(args, world, rank, local)
+    elif args.workload == "batch":
+        out = run_batch(args, world, rank, local)
     else:
         out = run_gpu(args, world, rank, local)
     if out is not None:
