@@ -12,15 +12,19 @@
 // hi hi^T + hi lo^T + lo hi^T, which is FP32-class accurate at FP16 tensor
 // speed.
 //
-// Persistent and warp-specialized, one CTA per SM (192 threads):
+// Persistent and warp-specialized, one CTA per SM (320 threads):
 //   warp 0  TMA producer: K chunks of 128 bytes per row (one 128-byte swizzle
 //           row) of the A strip (rows of tile I) and the B strip (rows of tile
 //           J; skipped on diagonal tiles) into a ring of NSTAGE stages;
-//   warp 1  allocates 2 x 128 TMEM columns; one thread issues tcgen05.mma and
+//   warp 1  allocates the TMEM columns; one thread issues tcgen05.mma and
 //           commits each stage back to the producer and each finished tile to
 //           the epilogue;
-//   warps 2-5 epilogue: tcgen05.ld of their 32 TMEM lanes, the scaled update
-//           applied to C with batched, coalesced loads and stores.
+//   warps 2-9 epilogue, two per 32-lane TMEM quarter (64 columns each):
+//           tcgen05.ld of the accumulator, the scaled update staged as 32 x 32
+//           boxes in shared memory and added into C by TMA reduce-adds, so the
+//           read-modify-write of C happens in L2 instead of through the SM
+//           (batched launches, whose C differs per system, read and write C
+//           with coalesced loads and stores instead).
 // The two TMEM accumulators let the epilogue of one tile overlap the MMAs of
 // the next.  Every mbarrier wait is bounded.
 #include "common.cuh"
@@ -34,7 +38,8 @@ namespace {
 constexpr int TM = 128;                    // output tile (M = N = 128)
 constexpr int CHUNK = 128;                 // bytes of K per row per stage
 constexpr int STRIP = TM * CHUNK;          // 16 KB: one operand strip chunk
-constexpr int NTHREADS = 192;
+constexpr int EPI_WARPS = 8;               // two per TMEM lane quarter, half the columns each
+constexpr int NTHREADS = 64 + 32 * EPI_WARPS;
 
 __device__ __forceinline__ void tile_of(int t, int& I, int& J) {
   int i = (int)((sqrtf(8.0f * t + 1.0f) - 1.0f) * 0.5f);
@@ -95,7 +100,9 @@ __device__ __forceinline__ void stage_scales(uint8_t* sf, const uint8_t* __restr
 struct TcMaps {
   CUtensorMap hi;   // main (or hi) panel: rows m, K-major
   CUtensorMap lo;   // lo panel (FP16X2 only)
+  CUtensorMap c;    // the trailing block C (FP32, m x m, 32 x 32 boxes): TMA reduce-add target
 };
+constexpr int STAGE_C = 32 * 32 * 4;        // one epilogue warp's 32 x 32 FP32 staging box
 
 // Batched launches: the tiles of all active systems are numbered in one
 // sequence (system i owns [steps[i].tile0, steps[i+1].tile0)); each system's
@@ -155,6 +162,9 @@ syrk_tc_kernel(const __grid_constant__ TcMaps maps, float* __restrict__ C, int l
   // A sets, B sets, then (MXFP8) the A and B scales of the chunk
   constexpr int STAGE_BYTES = 2 * NSETS * STRIP + (MX ? 2 * SF_BYTES : 0);
   constexpr uint32_t TMEM_COLS = MX ? 4 * TM : 2 * TM;  // accumulators (+ scales)
+  // single-matrix launches hand the update to the L2 with TMA reduce-adds
+  // (no C traffic through the SM); batched launches read-modify-write C
+  constexpr bool RED = !BATCH;
   constexpr int KSTEP = 32;                             // bytes of K per MMA
   constexpr int ELEMS_PER_CHUNK = CHUNK / Cfg::ESIZE;
 
@@ -175,7 +185,7 @@ syrk_tc_kernel(const __grid_constant__ TcMaps maps, float* __restrict__ C, int l
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < NS; ++s) { tc::mbar_init(&full_bar[s], 1); tc::mbar_init(&empty_bar[s], 1); }
-    for (int b = 0; b < 2; ++b) { tc::mbar_init(&accf_bar[b], 1); tc::mbar_init(&acce_bar[b], 4); }
+    for (int b = 0; b < 2; ++b) { tc::mbar_init(&accf_bar[b], 1); tc::mbar_init(&acce_bar[b], EPI_WARPS); }
     tc::fence_mbar_init();
     tc::prefetch_tmap(&maps.hi);
     if (NSETS == 2) tc::prefetch_tmap(&maps.lo);
@@ -304,6 +314,8 @@ syrk_tc_kernel(const __grid_constant__ TcMaps maps, float* __restrict__ C, int l
   } else {
     // ---------------- epilogue (warps 2..5) ----------------
     const int q = warp & 3;                  // TMEM lane quarter this warp may access
+    const int half = (warp - 2) >> 2;        // which 64 columns of the tile
+    float* stg = reinterpret_cast<float*>(smem + (size_t)NS * STAGE_BYTES + (size_t)(warp - 2) * STAGE_C);
     int tcount = 0;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++tcount) {
       const TileCtx tc_ = tile_ctx<BATCH>(t, bt, C, ldc, m);
@@ -322,17 +334,38 @@ syrk_tc_kernel(const __grid_constant__ TcMaps maps, float* __restrict__ C, int l
       const float si = (i < mt) ? (MX ? 1.0f : pow2f(rexp[i])) : 0.0f;
       const uint32_t taddr = tmem + (uint32_t)(buf * TM) + ((uint32_t)(q * 32) << 16);
 #pragma unroll 1
-      for (int c0 = 0; c0 < TM; c0 += 32) {
+      for (int c0 = half * (TM / 2); c0 < (half + 1) * (TM / 2); c0 += 32) {
         float v[32];
         tc::tmem_ld32(taddr + (uint32_t)c0, v);
-        if (c0 + 32 >= TM) {
+        if (c0 + 32 >= (half + 1) * (TM / 2)) {
           // last read of this accumulator: hand it back to the MMA warp
           tc::tc_fence_before();
           __syncwarp();
           if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tc::smem_u32(&acce_bar[buf])) : "memory");
         }
         const int j0 = J * TM + c0;
-        if (i < mt) {
+        if (RED) {
+          // C(rows i0.., cols j0..) += -(s_i s_j acc) as one 32 x 32 TMA
+          // reduce-add; boxes wholly above the diagonal or past m are skipped,
+          // and entries above the diagonal add -0.0, which leaves every value
+          // (signed zeros included) as it was
+          const int i0 = I * TM + q * 32;
+          if (i0 < mt && j0 < mt && !(I == J && j0 >= i0 + 32)) {
+            if (lane == 0) tc::bulk_wait_read();     // this warp's previous box has been read
+            __syncwarp();
+#pragma unroll
+            for (int u = 0; u < 32; ++u)
+              stg[u * 32 + lane] = (I == J && j0 + u > i)
+                                       ? -0.0f
+                                       : -((v[u] * si) * (MX ? 1.0f : pow2f(rexp[j0 + u])));
+            tc::fence_proxy_async_smem();
+            __syncwarp();
+            if (lane == 0) {
+              tc::tma_reduce_add_2d(&maps.c, stg, i0, j0);
+              tc::bulk_commit();
+            }
+          }
+        } else if (i < mt) {
           float cv[32];
 #pragma unroll
           for (int u = 0; u < 32; ++u) {
@@ -349,6 +382,7 @@ syrk_tc_kernel(const __grid_constant__ TcMaps maps, float* __restrict__ C, int l
       }
     }
   }
+  if (RED && warp >= 2 && lane == 0) tc::bulk_wait_read();   // staging read before exit
   tc::tc_fence_before();
   __syncthreads();
   if (warp == 1) {
@@ -357,17 +391,18 @@ syrk_tc_kernel(const __grid_constant__ TcMaps maps, float* __restrict__ C, int l
   }
 }
 
-template <int FMT>
+template <int FMT, bool BATCH>
 size_t tc_smem() {
   using Cfg = TcCfg<FMT>;
-  return (size_t)Cfg::NSTAGE * (2 * Cfg::NSETS * STRIP + (Cfg::MX ? 2 * SF_BYTES : 0)) + 1024;
+  return (size_t)Cfg::NSTAGE * (2 * Cfg::NSETS * STRIP + (Cfg::MX ? 2 * SF_BYTES : 0)) +
+         (BATCH ? 0 : (size_t)EPI_WARPS * STAGE_C) + 1024;
 }
 
 template <int FMT, bool BATCH>
 cudaError_t launch_fmt(const TcMaps& maps, float* C, int ldc, int m, int k, const int8_t* rowexp,
                        const uint8_t* mxexp, int ldmx, const int* prec_sel, DevStatus* st,
                        const TcBatch& bt, int ntiles_b, cudaStream_t stream) {
-  const size_t smem = tc_smem<FMT>();
+  const size_t smem = tc_smem<FMT, BATCH>();
   cudaError_t e = cudaFuncSetAttribute(syrk_tc_kernel<FMT, BATCH>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -406,6 +441,9 @@ cudaError_t launch_syrk_tc(float* C, int ldc, int m, int k, int fmt, const void*
                       CHUNK / esize, TM, CU_TENSOR_MAP_SWIZZLE_128B))
     return cudaErrorInvalidValue;
   maps.lo = maps.hi;
+  if (!encode_tmap_2d(&maps.c, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, C, (uint64_t)m, (uint64_t)m,
+                      (uint64_t)ldc, 32, 32, CU_TENSOR_MAP_SWIZZLE_NONE))
+    return cudaErrorInvalidValue;
   if (fmt == FP16X2) {
     const uint16_t* lo = reinterpret_cast<const uint16_t*>(q) + (size_t)m * ldq;
     if (!encode_tmap_2d(&maps.lo, dt, esize, lo, (uint64_t)k, (uint64_t)m, (uint64_t)ldq,
@@ -435,6 +473,7 @@ cudaError_t launch_syrk_tc_batched(BatchSys* sys, const BatchStep* steps, int na
                       CHUNK / esize, TM, CU_TENSOR_MAP_SWIZZLE_128B))
     return cudaErrorInvalidValue;
   maps.lo = maps.hi;
+  maps.c = maps.hi;            // unused: batched launches update C in place
   if (fmt == FP16X2) {
     const uint16_t* lo = reinterpret_cast<const uint16_t*>(q) + (size_t)qrows * b;
     if (!encode_tmap_2d(&maps.lo, dt, esize, lo, (uint64_t)b, (uint64_t)qrows, (uint64_t)b,
