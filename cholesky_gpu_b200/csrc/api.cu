@@ -134,6 +134,7 @@ struct mpchol_factor {
   DevStatus* status = nullptr;
   // solve side
   float* wsup = nullptr;      // inverses of the 1024-row diagonal super-blocks
+  int* trsv_ctr = nullptr;    // dependency counters of the persistent triangular solve
   bool solve_ready = false;
   // PCG workspace (sized for 8 rhs)
   double* vec = nullptr;      // x, r, z, p, Ap, b, tmp, work : 8 * n * 8
@@ -182,7 +183,7 @@ cudaError_t dmalloc(T** p, size_t count) {
 void free_factor(mpchol_factor_t* f) {
   if (f == nullptr) return;
   void* ptrs[] = {f->A, f->d, f->dtilde, f->rowsq, f->sh, f->winv, f->scratch64, f->q,
-                  f->rowexp, f->mxexp, f->steps, f->status, f->wsup,
+                  f->rowexp, f->mxexp, f->steps, f->status, f->wsup, f->trsv_ctr,
                   f->vec, f->partials, f->scal, f->done};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -270,9 +271,10 @@ mpchol_status ensure_solve(mpchol_factor_t* f, cudaStream_t stream) {
   return MPCHOL_OK;
 }
 
+// kernels per triangular solve: copy, zero, the persistent solve
 int trsv_launch_count(int n) {
-  const int nbs = (n + solve_super_rows() - 1) / solve_super_rows();
-  return 2 + 2 * nbs - 1;
+  (void)n;
+  return 3;
 }
 
 // z = M^-1 r for NR-padded vectors (tmp, work: n x nr scratch)
@@ -281,9 +283,11 @@ mpchol_status apply_precond(mpchol_factor_t* f, const double* r, double* tmp, do
   double* work = f->vec + 7 * (size_t)f->n * 8;
   const int nk = trsv_launch_count(f->n);
   PHASE(MPCHOL_PH_TRSV, nk, stream,
-        launch_trsv_super(false, f->A, f->ld, f->n, f->wsup, r, tmp, work, nr, skip, stream, nullptr));
+        launch_trsv_persistent(false, f->A, f->ld, f->n, f->wsup, r, tmp, work, nr, f->trsv_ctr,
+                               skip, f->status, stream));
   PHASE(MPCHOL_PH_TRSV, nk, stream,
-        launch_trsv_super(true, f->A, f->ld, f->n, f->wsup, tmp, z, work, nr, skip, stream, nullptr));
+        launch_trsv_persistent(true, f->A, f->ld, f->n, f->wsup, tmp, z, work, nr, f->trsv_ctr,
+                               skip, f->status, stream));
   return MPCHOL_OK;
 }
 
@@ -592,6 +596,7 @@ mpchol_status mpchol_factor_create(const mpchol_opts* opts, int n, mpchol_factor
             dmalloc(&f->steps, f->nsteps + 1) == cudaSuccess &&
             dmalloc(&f->status, 1) == cudaSuccess &&
             dmalloc(&f->wsup, solve_wsup_elems(n)) == cudaSuccess &&
+            dmalloc(&f->trsv_ctr, trsv_counter_ints(n)) == cudaSuccess &&
             dmalloc(&f->vec, 8 * nv) == cudaSuccess &&
             dmalloc(&f->partials, (size_t)4 * pcg_vgrid() * 8) == cudaSuccess &&
             dmalloc(&f->scal, 64) == cudaSuccess && dmalloc(&f->done, 2) == cudaSuccess &&

@@ -19,6 +19,13 @@ cudaError_t launch_symv_skip(const TA* A, int lda, int n, const double* x, doubl
 cudaError_t launch_solve_setup(const float* L, int ldl, int n, float* wsup, cudaStream_t stream);
 // out = L^-1 in (forward) or L^-T in (backward); work is an n x nrhs scratch.
 // *launches receives the number of kernels launched.
+// The same solve as one persistent cooperative launch (plus counter reset and
+// two vector kernels); counters: trsv_counter_ints(n) ints of scratch.
+size_t trsv_counter_ints(int n);
+cudaError_t launch_trsv_persistent(bool backward, const float* L, int ldl, int n,
+                                   const float* wsup, const double* in, double* out,
+                                   double* work, int nrhs, int* counters, const int* skip,
+                                   DevStatus* st, cudaStream_t stream);
 cudaError_t launch_trsv_super(bool backward, const float* L, int ldl, int n, const float* wsup,
                               const double* in, double* out, double* work, int nrhs,
                               const int* skip, cudaStream_t stream, int* launches);

@@ -18,6 +18,7 @@
 // symmetric positive definite whenever the W_S are nonsingular, so PCG stays
 // well defined; it equals (L L^T)^-1 up to the FP32 rounding of the W_S.
 // Partial sums are combined with FP64 atomics.
+#include <algorithm>
 #include <mutex>
 
 #include "common.cuh"
@@ -151,11 +152,14 @@ __device__ __forceinline__ void flush_rows(double (&acc)[4][NR], double* red, do
   }
 }
 
+// Vector segments are read from L2 (ld.global.cg): inside the persistent
+// solve other CTAs produce them with atomics while this SM may hold older
+// lines of the same arrays in L1.
 template <int NR>
 __device__ __forceinline__ void load_vec(const double* x, int n, int row0, int nvalid, double* s) {
   for (int e = threadIdx.x; e < RB * NR; e += NTH) {
     const int r = e / NR, k = e % NR;
-    s[e] = (r < nvalid) ? x[(size_t)k * n + row0 + r] : 0.0;
+    s[e] = (r < nvalid) ? __ldcg(x + (size_t)k * n + row0 + r) : 0.0;
   }
 }
 
@@ -476,6 +480,111 @@ panel_kernel(const float* __restrict__ L, int ldl, int n, int s0, int rs,
   panel_body<NR, TRANS>(L, ldl, n, s0, rs, v, w, skip, blockIdx);
 }
 
+// ---- persistent triangular solve -------------------------------------------
+// One launch per solve.  The tiles of a solve form a dependency DAG: for
+// super-step S the TRMV tiles of W_S (which need every panel contribution to
+// their input segment) and then the panel tiles below (forward) or left of
+// (backward) S (which need their segment of y_S / z_S complete).  Units are
+// handed out in that topological order by an atomic counter, so a unit only
+// ever waits on units already taken by running CTAs; the launch is
+// cooperative, so all CTAs are resident and every wait ends.  Completion is
+// counted per 128-row segment:
+//   seg_in[g]   panel contributions received by segment g (global 128-tile g)
+//   seg_out[g]  TRMV tiles finished that write segment g of the result
+// Waits are bounded; a wait that runs out records MPCHOL_ERR_TIMEOUT and the
+// unit proceeds (the result is then wrong, but no CTA waits forever).
+constexpr int SEGS = RS / RB;                 // 128-row segments per super-block
+constexpr long long kTrsvMaxPolls = 1ll << 24;
+
+__device__ __forceinline__ void wait_count(const int* ctr, int need, DevStatus* st, int unit) {
+  if (threadIdx.x == 0) {
+    long long it = 0;
+    while (*reinterpret_cast<const volatile int*>(ctr) < need) {
+      if (++it > kTrsvMaxPolls) {
+        if (st != nullptr) set_status(st, MPCHOL_ERR_TIMEOUT, unit);
+        break;
+      }
+      __nanosleep(64);
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ void signal_count(int* ctr) {
+  __threadfence();                            // this thread's atomics visible device-wide
+  __syncthreads();                            // ... for every thread of the unit
+  if (threadIdx.x == 0) atomicAdd(ctr, 1);
+}
+
+template <int NR, bool TRANS>
+__global__ void __launch_bounds__(NTH)
+trsv_persistent_kernel(const float* __restrict__ L, int ldl, int n, const float* __restrict__ wsup,
+                       double* __restrict__ work, double* __restrict__ out, int* ctr,
+                       const int* skip, DevStatus* st) {
+  if (skip != nullptr && *skip) return;
+  __shared__ int s_unit;
+  int* next = ctr;
+  int* seg_in = ctr + 1;
+  const int ntiles = ceil_div(n, RB);
+  int* seg_out = seg_in + ntiles;
+  const int NS = ceil_div(n, RS);
+  for (;;) {
+    if (threadIdx.x == 0) s_unit = atomicAdd(next, 1);
+    __syncthreads();
+    int u = s_unit;
+    __syncthreads();
+    bool found = false;
+    for (int t = 0; t < NS && !found; ++t) {
+      const int S = TRANS ? NS - 1 - t : t;
+      const int s0 = S * RS;
+      const int rs = min(RS, n - s0);
+      const int nsub = ceil_div(rs, RB);
+      const int g0 = s0 / RB;                 // first global segment of S
+      const int ntr = nsub * (nsub + 1) / 2;
+      const int span = TRANS ? g0 : ceil_div(n - s0 - rs, RB);
+      const int npan = span * nsub;
+      const float* W = wsup + (size_t)S * RS * RS;
+      if (u < ntr) {
+        found = true;
+        int i, j;
+        tri_of(u, i, j);
+        if (!TRANS) {
+          // y_S(i) += W(i,j) w_S(j): w_S(j) has all g0 panel contributions
+          wait_count(seg_in + g0 + j, g0, st, u);
+          trmv_super_body<NR, false>(W, n, s0, rs, work, out, nullptr, make_uint3(u, 0, 0));
+          signal_count(seg_out + g0 + i);
+        } else {
+          // z_S(j) += W(i,j)^T w_S(i): w_S(i) has the contributions of every
+          // segment below S
+          wait_count(seg_in + g0 + i, ntiles - g0 - nsub, st, u);
+          trmv_super_body<NR, true>(W, n, s0, rs, work, out, nullptr, make_uint3(u, 0, 0));
+          signal_count(seg_out + g0 + j);
+        }
+      } else if (u < ntr + npan) {
+        found = true;
+        const int p = u - ntr;
+        if (!TRANS) {
+          // w(row segment r below S) -= L(r, S col c) y_S(c); rows nearest S first
+          const int r = p / nsub, c = p % nsub;
+          wait_count(seg_out + g0 + c, c + 1, st, u);
+          panel_body<NR, false>(L, ldl, n, s0, rs, out, work, nullptr, make_uint3(r, c, 0));
+          signal_count(seg_in + g0 + nsub + r);
+        } else {
+          // w(col segment c left of S) -= L(S row rt, c)^T z_S(rt); columns nearest S first
+          const int c = span - 1 - p / nsub, rt = p % nsub;
+          wait_count(seg_out + g0 + rt, nsub - rt, st, u);
+          panel_body<NR, true>(L, ldl, n, s0, rs, out, work, nullptr, make_uint3(c, rt, 0));
+          signal_count(seg_in + c);
+        }
+      } else {
+        u -= ntr + npan;
+      }
+    }
+    if (!found) return;                         // past the last unit
+  }
+}
+
 // ---- batched variants: one launch serves every system of a batch --------
 // blockIdx.y (or .z) selects the system; CTAs past a system's own extent
 // return at once.  Vectors live in the system's slots (n x NR column-major).
@@ -619,6 +728,11 @@ cudaError_t solve_set_attributes() {
   if ((e = set_dyn(panel_kernel<NRC, true>, red_bytes(NRC))) != cudaSuccess) return e;
   SET_NR(1) SET_NR(2) SET_NR(4) SET_NR(8)
 #undef SET_NR
+#define SET_NRP(NRC)                                                                              \
+  if ((e = set_dyn(trsv_persistent_kernel<NRC, false>, red_bytes(NRC))) != cudaSuccess) return e; \
+  if ((e = set_dyn(trsv_persistent_kernel<NRC, true>, red_bytes(NRC))) != cudaSuccess) return e;
+  SET_NRP(1) SET_NRP(2) SET_NRP(4) SET_NRP(8)
+#undef SET_NRP
   if ((e = set_dyn(block_inverse_batched_kernel, inv)) != cudaSuccess) return e;
 #define SET_NRB(NRC)                                                                              \
   if ((e = set_dyn(symv_batched_kernel<NRC>, red_bytes(NRC))) != cudaSuccess) return e;           \
@@ -711,6 +825,54 @@ cudaError_t launch_trsv_batched(bool backward, const BatchSys* sys, int nsys, in
       NR_SWITCH(nr, (panel_batched_kernel<NRC, true><<<gp, NTH, red_bytes(NRC), stream>>>(sys, sup, out_slot, work_slot, use_skip)));
     }
   }
+  return cudaGetLastError();
+}
+
+size_t trsv_counter_ints(int n) { return 1 + 2 * (size_t)ceil_div(n, RB); }
+
+// The persistent solve: counters (trsv_counter_ints(n) ints) are cleared,
+// work <- in, out <- 0, then one cooperative launch over every resident CTA.
+cudaError_t launch_trsv_persistent(bool backward, const float* L, int ldl, int n,
+                                   const float* wsup, const double* in, double* out,
+                                   double* work, int nrhs, int* counters, const int* skip,
+                                   DevStatus* st, cudaStream_t stream) {
+  const long long cnt = (long long)n * nrhs;
+  cudaError_t e = cudaMemsetAsync(counters, 0, sizeof(int) * trsv_counter_ints(n), stream);
+  if (e != cudaSuccess) return e;
+  copy_vec_kernel<1><<<148, 256, 0, stream>>>(in, work, cnt, skip);
+  zero_vec_kernel<<<148, 256, 0, stream>>>(out, cnt, skip);
+  static int grid_cache[64][2][4] = {};
+  int dev = 0;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  const int nri = nrhs == 1 ? 0 : nrhs == 2 ? 1 : nrhs == 4 ? 2 : 3;
+  int& grid = grid_cache[dev & 63][backward ? 1 : 0][nri];
+  auto launch = [&](auto kernel) -> cudaError_t {
+    if (grid == 0) {
+      int per_sm = 0, nsm = 0;
+      cudaError_t ee = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, NTH,
+                                                                     red_bytes(nrhs));
+      if (ee == cudaSuccess) ee = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+      if (ee != cudaSuccess) return ee;
+      grid = std::max(1, per_sm) * nsm;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(NTH);
+    cfg.dynamicSmemBytes = red_bytes(nrhs);
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, L, ldl, n, wsup, work, out, counters, skip, st);
+  };
+  if (!backward) {
+    NR_SWITCH(nrhs, (e = launch(trsv_persistent_kernel<NRC, false>)));
+  } else {
+    NR_SWITCH(nrhs, (e = launch(trsv_persistent_kernel<NRC, true>)));
+  }
+  if (e != cudaSuccess) return e;
   return cudaGetLastError();
 }
 
