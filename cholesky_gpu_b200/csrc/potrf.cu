@@ -8,8 +8,8 @@
 // shared access is either contiguous across lanes or a broadcast):
 //   * the lower tiles are staged by TMA (one thread issues the 2-D copies,
 //     an mbarrier counts the bytes) and written back by TMA stores;
-//   * one warp factors each diagonal tile; its rank-1 updates are done in
-//     register batches (all loads of a step issued before its stores);
+//   * one warp factors each diagonal tile with the tile's rows held in
+//     registers, one tile ahead of the trailing update of the other warps;
 //   * warps solve the tiles below and update the trailing tiles;
 //   * the inverses of the diagonal tiles are formed for the panel solve.
 // Blocks flagged near-indefinite by the switching criterion are factored in
@@ -41,11 +41,12 @@ __device__ __forceinline__ double drsqrt<double>(double x) { return rsqrt(x); }
 // Lane i holds row i of the tile in registers for the whole factorization (the
 // column loop is unrolled so every register index is a constant): per column
 // lane k forms and repairs the pivot, one shuffle broadcasts 1/sqrt(pivot),
-// and the rank-1 update takes the column's multipliers by shuffles.  Shared
-// memory is read once and the lower triangle written once.
+// and the rank-1 update reads the column's multipliers from the 32-entry
+// shared buffer col as 16-byte broadcasts.  The tile itself is read once and
+// its lower triangle written once.
 template <typename T>
 __device__ bool factor_diag_tile(T* t, T* inv, int lane, int nreal, const T* shift, const T* pmin,
-                                 int diag_pert, int* nperturbed, int* fail_row) {
+                                 int diag_pert, int* nperturbed, int* fail_row, T* col) {
   T a[TS];
 #pragma unroll
   for (int j = 0; j < TS; ++j) a[j] = t[j * TS + lane];
@@ -53,11 +54,15 @@ __device__ bool factor_diag_tile(T* t, T* inv, int lane, int nreal, const T* shi
   const T my_pmin = pmin[lane];
   bool failed = false, perturbed = false;
   T my_inv = T(1);
+  // dnext: the next pivot candidate, formed by lane k+1 from its own
+  // multiplier (the same fma the rank-1 update applies to a[k+1]), so the
+  // pivot chain does not wait on the update's shared-memory round trip
+  T dnext = a[0];
 #pragma unroll
   for (int k = 0; k < TS; ++k) {
     T rk = T(1);
     if (lane == k) {
-      T piv = a[k];
+      T piv = dnext;
       if (k < nreal) {
         piv += my_shift;
         if (diag_pert) {
@@ -84,8 +89,28 @@ __device__ bool factor_diag_tile(T* t, T* inv, int lane, int nreal, const T* shi
     rk = __shfl_sync(0xffffffffu, rk, k);
     const T lik = (lane > k) ? a[k] * rk : T(0);
     if (lane > k) a[k] = lik;
+    if (k + 1 < TS) dnext = fma(-lik, lik, a[k + 1]);
+    col[lane] = lik;
+    __syncwarp();
+    constexpr int V = 16 / sizeof(T);
 #pragma unroll
-    for (int j = k + 1; j < TS; ++j) a[j] -= lik * __shfl_sync(0xffffffffu, lik, j);
+    for (int q = 0; q < TS / V; ++q) {
+      if (V * q + V - 1 <= k) continue;
+      T l[V];
+      if (V == 4) {
+        const float4 w = *reinterpret_cast<const float4*>(col + V * q);
+        l[0] = w.x; l[1] = w.y; l[2 % V] = w.z; l[3 % V] = w.w;
+      } else {
+        const double2 w = *reinterpret_cast<const double2*>(col + V * q);
+        l[0] = w.x; l[1 % V] = w.y;
+      }
+#pragma unroll
+      for (int e = 0; e < V; ++e) {
+        const int j = V * q + e;
+        if (j > k) a[j] = fma(-lik, l[e], a[j]);
+      }
+    }
+    __syncwarp();
   }
 #pragma unroll
   for (int j = 0; j < TS; ++j)
@@ -123,16 +148,16 @@ __device__ void syrk_tile(T* c, const T* a, const T* b, int lane) {
 #pragma unroll
   for (int m = 0; m < TS; ++m) ar[m] = a[m * TS + lane];
 #pragma unroll 1
-  for (int c0 = 0; c0 < TS; c0 += 4) {
-    T acc[4];
+  for (int c0 = 0; c0 < TS; c0 += 8) {
+    T acc[8];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) acc[u] = c[(c0 + u) * TS + lane];
+    for (int u = 0; u < 8; ++u) acc[u] = c[(c0 + u) * TS + lane];
 #pragma unroll
     for (int m = 0; m < TS; ++m)
 #pragma unroll
-      for (int u = 0; u < 4; ++u) acc[u] -= ar[m] * b[m * TS + c0 + u];
+      for (int u = 0; u < 8; ++u) acc[u] -= ar[m] * b[m * TS + c0 + u];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) c[(c0 + u) * TS + lane] = acc[u];
+    for (int u = 0; u < 8; ++u) c[(c0 + u) * TS + lane] = acc[u];
   }
 }
 
@@ -167,6 +192,7 @@ __device__ void potrf_block(const CUtensorMap* tmap, T* tiles, float* A, int lda
   __shared__ T s_shift[256];
   __shared__ T s_pmin[256];
   __shared__ T s_inv[256];
+  __shared__ __align__(16) T s_col[TS];
   __shared__ int s_fail, s_pert, s_ok;
   __shared__ __align__(8) uint64_t bar;
   if (tid == 0) { s_fail = -1; s_pert = 0; s_ok = 1; }
@@ -227,33 +253,48 @@ __device__ void potrf_block(const CUtensorMap* tmap, T* tiles, float* A, int lda
     }
   }
   __syncthreads();
-  for (int J = 0; J < NT; ++J) {
-    if (warp == 0) {
-      int nreal = bs - J * TS;
-      nreal = nreal > TS ? TS : nreal;
-      int fail = -1, npert = 0;
-      bool ok = factor_diag_tile<T>(tiles + tidx(J, J) * TSZ, s_inv + J * TS, lane, nreal,
-                                    s_shift + J * TS, s_pmin + J * TS, p.diag_pert, &npert, &fail);
-      if (lane == 0) {
-        if (!ok) s_fail = J * TS + fail;
-        s_pert += npert;
-      }
+  // Look-ahead: warp 0 owns the diagonal tiles.  At step J it applies column
+  // J to tile (J+1, J+1) -- its last update -- and factors it at once, while
+  // the other warps update the rest of the trailing tiles; so the factor of
+  // the next diagonal tile overlaps the trailing update.
+  auto factor_tile = [&](int J) {
+    int nreal = bs - J * TS;
+    nreal = nreal > TS ? TS : nreal;
+    int fail = -1, npert = 0;
+    const bool ok = factor_diag_tile<T>(tiles + tidx(J, J) * TSZ, s_inv + J * TS, lane, nreal,
+                                        s_shift + J * TS, s_pmin + J * TS, p.diag_pert, &npert,
+                                        &fail, s_col);
+    if (lane == 0) {
+      if (!ok) s_fail = J * TS + fail;
+      s_pert += npert;
     }
-    __syncthreads();
+  };
+  if (warp == 0) factor_tile(0);
+  __syncthreads();
+  for (int J = 0; J < NT; ++J) {
     if (s_fail >= 0) break;
     for (int I = J + 1 + warp; I < NT; I += nwarps)
       trsm_tile<T>(tiles + tidx(I, J) * TSZ, tiles + tidx(J, J) * TSZ, s_inv + J * TS, lane);
     __syncthreads();
-    // trailing tiles (I, K), J < K <= I < NT
-    const int T_ = NT - J - 1;
-    const int nupd = T_ * (T_ + 1) / 2;
-    for (int u = warp; u < nupd; u += nwarps) {
-      int i = 0;
-      while ((i + 1) * (i + 2) / 2 <= u) ++i;
-      const int k = u - i * (i + 1) / 2;
-      const int I = J + 1 + i, K = J + 1 + k;
-      syrk_tile<T>(tiles + tidx(I, K) * TSZ, tiles + tidx(I, J) * TSZ, tiles + tidx(K, J) * TSZ,
-                   lane);
+    if (J + 1 < NT) {
+      if (warp == 0) {
+        syrk_tile<T>(tiles + tidx(J + 1, J + 1) * TSZ, tiles + tidx(J + 1, J) * TSZ,
+                     tiles + tidx(J + 1, J) * TSZ, lane);
+        __syncwarp();
+        factor_tile(J + 1);
+      } else {
+        // trailing tiles (I, K), J < K <= I < NT, except (J+1, J+1)
+        const int T_ = NT - J - 1;
+        const int nupd = T_ * (T_ + 1) / 2;
+        for (int u = warp; u < nupd; u += nwarps - 1) {
+          int i = 0;
+          while ((i + 1) * (i + 2) / 2 <= u) ++i;
+          const int k = u - i * (i + 1) / 2;
+          const int I = J + 1 + i, K = J + 1 + k;
+          syrk_tile<T>(tiles + tidx(I, K) * TSZ, tiles + tidx(I, J) * TSZ,
+                       tiles + tidx(K, J) * TSZ, lane);
+        }
+      }
     }
     __syncthreads();
   }
