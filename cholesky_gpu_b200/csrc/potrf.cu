@@ -40,7 +40,7 @@ __device__ __forceinline__ double drsqrt<double>(double x) { return rsqrt(x); }
 //
 // Lane i holds row i of the tile in registers for the whole factorization (the
 // column loop is unrolled so every register index is a constant): per column
-// lane k forms and repairs the pivot, one shuffle broadcasts 1/sqrt(pivot),
+// lane k's pivot is repaired, one shuffle broadcasts 1/sqrt(pivot),
 // and the rank-1 update reads the column's multipliers from the 32-entry
 // shared buffer col as 16-byte broadcasts.  The tile itself is read once and
 // its lower triangle written once.
@@ -60,35 +60,31 @@ __device__ bool factor_diag_tile(T* t, T* inv, int lane, int nreal, const T* shi
   T dnext = a[0];
 #pragma unroll
   for (int k = 0; k < TS; ++k) {
-    T rk = T(1);
-    if (lane == k) {
-      T piv = dnext;
-      if (k < nreal) {
-        piv += my_shift;
-        if (diag_pert) {
-          // repair: max(|pivot|, floor), the reference's fixDiag rule
-          // (src/kernels_macros.cuh:90-99); a NaN pivot takes the floor
-          if (!(piv > my_pmin)) {
-            const T ap = piv < T(0) ? -piv : piv;
-            piv = (ap > my_pmin) ? ap : my_pmin;
-            perturbed = true;
-          }
-        } else if (!(piv > T(0))) {
-          failed = true;
-          piv = T(1);   // keep the arithmetic finite; the caller discards the result
-        }
-      } else {
-        piv = T(1);     // identity padding beyond the real block
-      }
-      // one SFU reciprocal square root on the dependency chain:
-      // rk = 1/sqrt(piv), L(k,k) = piv * rk
-      rk = drsqrt<T>(piv);
-      a[k] = piv * rk;
-      my_inv = rk;
+    // every lane evaluates the pivot rule on its own candidate (no divergent
+    // branch on the chain); lane k's value is the pivot, broadcast as 1/sqrt
+    const bool real = k < nreal;   // identity padding beyond the real block
+    T piv = real ? dnext + my_shift : T(1);
+    bool pert = false, bad = false;
+    if (diag_pert) {
+      // repair: max(|pivot|, floor), the reference's fixDiag rule
+      // (src/kernels_macros.cuh:90-99); a NaN pivot takes the floor
+      pert = real && !(piv > my_pmin);
+      const T ap = piv < T(0) ? -piv : piv;
+      piv = pert ? (ap > my_pmin ? ap : my_pmin) : piv;
+    } else {
+      bad = real && !(piv > T(0));
+      piv = bad ? T(1) : piv;   // keep the arithmetic finite; the caller discards the result
     }
-    rk = __shfl_sync(0xffffffffu, rk, k);
+    // one SFU reciprocal square root on the dependency chain:
+    // r = 1/sqrt(piv), L(k,k) = piv * r
+    const T r = drsqrt<T>(piv);
+    const T rk = __shfl_sync(0xffffffffu, r, k);
+    const bool mine = lane == k;
+    perturbed = perturbed || (mine && pert);
+    failed = failed || (mine && bad);
+    my_inv = mine ? r : my_inv;
     const T lik = (lane > k) ? a[k] * rk : T(0);
-    if (lane > k) a[k] = lik;
+    a[k] = mine ? piv * r : ((lane > k) ? lik : a[k]);
     if (k + 1 < TS) dnext = fma(-lik, lik, a[k + 1]);
     col[lane] = lik;
     __syncwarp();
