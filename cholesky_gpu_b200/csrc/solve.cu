@@ -325,26 +325,52 @@ block_inverse_kernel(const float* __restrict__ L, int ldl, int n, float* __restr
 }
 
 // C(128x128) = A(128 x K) * B(K x 128), A and B column-major, FP32 FMA.
-// 256 threads, 8 x 8 outputs each (rows tx*4+{0..3}, 64+tx*4+{0..3}).
+// 256 threads, 8 x 8 outputs each (rows tx*4+{0..3}, 64+tx*4+{0..3}).  K
+// advances in chunks of GK (a multiple of GK): the next chunk is loaded into
+// registers (coalesced: 128 consecutive rows of A, GK consecutive k of each B
+// column) while the current one is multiplied from shared memory.
+constexpr int GK = 32;
+constexpr int GPT = GK * RB / NTH;   // elements of A (and of B) per thread per chunk
+constexpr int BLDK = GK + 1;         // padded column stride of the staged B chunk
+
+__device__ __forceinline__ int acc_col_of(int ty, int b) { return b < 4 ? ty * 4 + b : 64 + ty * 4 + (b - 4); }
+
+__device__ __forceinline__ void gemm128_load(const float* A, int lda, int a_rows_valid,
+                                             const float* B, int ldb, int k0, float (&ra)[GPT],
+                                             float (&rb)[GPT]) {
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int q = 0; q < GPT; ++q) {
+    const int e = tid + NTH * q;
+    const int r = e % RB, kk = e / RB;          // A: rows fastest
+    ra[q] = (r < a_rows_valid) ? A[(size_t)(k0 + kk) * lda + r] : 0.0f;
+    const int k = e % GK, c = e / GK;           // B: k fastest within a column
+    rb[q] = B[(size_t)c * ldb + k0 + k];
+  }
+}
+
 __device__ void gemm128(const float* A, int lda, int a_rows_valid, const float* B, int ldb, int K,
                         float (&acc)[8][8], float* As, float* Bs) {
   const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
-  for (int k0 = 0; k0 < K; k0 += 8) {
-    for (int e = tid; e < 8 * RB; e += NTH) {
-      const int kk = e / RB, r = e % RB;
-      As[kk * RB + r] = (r < a_rows_valid) ? A[(size_t)(k0 + kk) * lda + r] : 0.0f;
-      const int c = e / 8, k = e % 8;
-      Bs[k * RB + c] = B[(size_t)c * ldb + k0 + k];
+  float ra[GPT], rb[GPT];
+  gemm128_load(A, lda, a_rows_valid, B, ldb, 0, ra, rb);
+  for (int k0 = 0; k0 < K; k0 += GK) {
+#pragma unroll
+    for (int q = 0; q < GPT; ++q) {
+      const int e = tid + NTH * q;
+      As[(e / RB) * RB + e % RB] = ra[q];
+      Bs[(e / GK) * BLDK + e % GK] = rb[q];      // B column-major in shared memory too
     }
     __syncthreads();
-#pragma unroll
-    for (int kk = 0; kk < 8; ++kk) {
+    if (k0 + GK < K) gemm128_load(A, lda, a_rows_valid, B, ldb, k0 + GK, ra, rb);
+#pragma unroll 4
+    for (int kk = 0; kk < GK; ++kk) {
       const float4 a0 = *reinterpret_cast<const float4*>(&As[kk * RB + tx * 4]);
       const float4 a1 = *reinterpret_cast<const float4*>(&As[kk * RB + 64 + tx * 4]);
-      const float4 b0 = *reinterpret_cast<const float4*>(&Bs[kk * RB + ty * 4]);
-      const float4 b1 = *reinterpret_cast<const float4*>(&Bs[kk * RB + 64 + ty * 4]);
       const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-      const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+      float bv[8];
+#pragma unroll
+      for (int b = 0; b < 8; ++b) bv[b] = Bs[acc_col_of(ty, b) * BLDK + kk];
 #pragma unroll
       for (int a = 0; a < 8; ++a)
 #pragma unroll
@@ -366,8 +392,8 @@ __device__ __forceinline__ int acc_col(int b) { return b < 4 ? (threadIdx.x / 16
 template <int PHASE>
 __device__ __forceinline__ void
 superinv_gemm_body(const float* __restrict__ L, int ldl, int n, float* __restrict__ wsup, int h, uint3 bid) {
-  __shared__ __align__(16) float As[8 * RB];
-  __shared__ __align__(16) float Bs[8 * RB];
+  __shared__ __align__(16) float As[GK * RB];
+  __shared__ __align__(16) float Bs[RB * BLDK];
   const int tpr = h / RB;
   const int ti = bid.x / tpr, tj = bid.x % tpr;
   const int S = bid.z, s0 = S * RS, a0 = bid.y * 2 * h;

@@ -30,15 +30,16 @@ __global__ void f64_to_f32_kernel(const double* __restrict__ src, int lds, float
   }
 }
 
+// ||A||_F^2 of a symmetric matrix from its lower triangle.  Block b takes
+// the columns b, b + gridDim.x, ...; its threads stride down each column from
+// the diagonal (coalesced, no index division).  One partial per block.
 template <typename TA>
 __global__ void frob_lower_kernel(const TA* __restrict__ A, int lda, int n, double* partials) {
   double s = 0.0;
-  const long long total = (long long)n * n;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
-       e += (long long)gridDim.x * blockDim.x) {
-    const int c = (int)(e / n), r = (int)(e % n);
-    if (r >= c) {
-      const double v = (double)A[(size_t)c * lda + r];
+  for (int c = blockIdx.x; c < n; c += gridDim.x) {
+    const TA* col = A + (size_t)c * lda;
+    for (int r = c + threadIdx.x; r < n; r += blockDim.x) {
+      const double v = (double)col[r];
       s += (r == c ? 1.0 : 2.0) * v * v;
     }
   }
