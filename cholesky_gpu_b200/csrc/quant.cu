@@ -43,11 +43,22 @@ __device__ void quantize_tile(const float* __restrict__ P, int ldp, int m, int k
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int row0 = blockIdx.x * QROWS;
   const int nr = min(QROWS, m - row0);
-  // stage the rows (coalesced column reads), padded stride QROWS+1
-#pragma unroll 8
-  for (int e = tid; e < k * QROWS; e += QTHR) {
-    const int c = e / QROWS, r = e % QROWS;
-    tile[c * (QROWS + 1) + r] = (r < nr) ? P[(size_t)c * ldp + row0 + r] : 0.0f;
+  // stage the rows (coalesced column reads, 16 loads in flight per thread
+  // before their shared-memory stores), padded stride QROWS+1
+  constexpr int B = 16;
+  for (int e0 = tid; e0 < k * QROWS; e0 += B * QTHR) {
+    float vv[B];
+#pragma unroll
+    for (int u = 0; u < B; ++u) {
+      const int e = e0 + u * QTHR;
+      const int c = e / QROWS, r = e % QROWS;
+      vv[u] = (e < k * QROWS && r < nr) ? P[(size_t)c * ldp + row0 + r] : 0.0f;
+    }
+#pragma unroll
+    for (int u = 0; u < B; ++u) {
+      const int e = e0 + u * QTHR;
+      if (e < k * QROWS) tile[(e / QROWS) * (QROWS + 1) + e % QROWS] = vv[u];
+    }
   }
   __syncthreads();
   const int cpl = k / 32;                   // columns per lane

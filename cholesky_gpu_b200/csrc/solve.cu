@@ -84,9 +84,31 @@ __device__ __forceinline__ void load_cols(const double* T, int ld, int rloc, int
   }
 }
 
+// Sum each of the 16 per-lane values w[i] over the 32 lanes of the warp with
+// 16 shuffles (a butterfly that halves the values kept per lane at each
+// step).  Returns the sum of column col_of_lane(lane); lanes l and l^1 hold
+// the same one.
+__device__ __forceinline__ int col_of_lane(int lane) {
+  return ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
+}
+__device__ __forceinline__ double butterfly16(double (&w)[16], int lane) {
+#pragma unroll
+  for (int h = 8, off = 16; h >= 1; h >>= 1, off >>= 1) {
+    const bool upper = (lane & off) != 0;
+#pragma unroll
+    for (int i = 0; i < h; ++i) {
+      const double send = upper ? w[i] : w[i + h];
+      const double keep = upper ? w[i + h] : w[i];
+      w[i] = keep + __shfl_xor_sync(0xffffffffu, send, off);
+    }
+  }
+  return w[0] + __shfl_xor_sync(0xffffffffu, w[0], 1);
+}
+
 // Accumulate a 128 x 128 tile times a vector segment.
 //   NOTRANS: part[r][k] += T[r][c] * vin[c][k]   (per-thread rows, summed over the warp's columns)
-//   TRANS  : colsum[c][k] = sum_r T[r][c] * vin[r][k], reduced over the warp -> lane 0
+//   TRANS  : colsum[c][k] = sum_r T[r][c] * vin[r][k], reduced over the warp (butterfly
+//            for NR <= 2, one shuffle tree per column otherwise)
 // `mask`: 0 none, 1 keep r >= c (lower incl. diagonal), 2 keep r > c.
 template <typename TA, int NR, int CH>
 __device__ __forceinline__ void tile_pass(const TA* T, int ld, int rows_valid, int cols_valid,
@@ -95,7 +117,9 @@ __device__ __forceinline__ void tile_pass(const TA* T, int ld, int rows_valid, i
                                           int mask_t, bool do_nt, bool do_t) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int rloc = 4 * lane;
-#pragma unroll 1
+  constexpr bool BFLY = NR <= 2;
+  double pc[BFLY ? 16 : 1][NR];   // per-lane column partials (butterfly path)
+#pragma unroll
   for (int cb = 0; cb < 16; cb += CH) {
     double v[CH][4];
     load_cols<CH>(T, ld, rloc, rows_valid, warp * 16 + cb, cols_valid, v);
@@ -122,10 +146,24 @@ __device__ __forceinline__ void tile_pass(const TA* T, int ld, int rows_valid, i
             const bool keep = mask_t == 0 || (mask_t == 1 ? (rloc + r >= c) : (rloc + r > c));
             if (keep) s = fma(v[cc][r], vin_rows[(rloc + r) * NR + k], s);
           }
-          s = warp_sum(s);
-          if (lane == 0) colsum_smem[c * NR + k] = s;
+          if (BFLY) {
+            pc[BFLY ? cb + cc : 0][k] = s;
+          } else {
+            s = warp_sum(s);
+            if (lane == 0) colsum_smem[c * NR + k] = s;
+          }
         }
       }
+    }
+  }
+  if (BFLY && do_t) {
+#pragma unroll
+    for (int k = 0; k < NR; ++k) {
+      double w[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) w[i] = pc[BFLY ? i : 0][k];
+      const double sum = butterfly16(w, lane);
+      if ((lane & 1) == 0) colsum_smem[(warp * 16 + col_of_lane(lane)) * NR + k] = sum;
     }
   }
 }

@@ -24,7 +24,8 @@ namespace mpchol {
 namespace {
 
 constexpr int TR = 64;       // rows per CTA
-constexpr int NTHR = 256;
+constexpr int NTHR = 256;    // 8 warps: 4 rows x 2 columns of each tile per thread
+constexpr int CPT = 32 / (NTHR / 16);   // tile columns per thread
 constexpr int TSZ = 32 * 32; // dense 32 x 32 tile
 constexpr int XLD = TR;      // X staged column-major, rows contiguous
 
@@ -38,51 +39,55 @@ size_t trsm_smem_floats(int bs) {
 // Solve the staged 64-row slab in place: for each 32-column tile J,
 // X_J -= X_{<J} L_{J,<J}^T (register-tiled), then X_J = X_J L_JJ^-T.
 __device__ void trsm_slab(float* Xs, const float* Lt, const float* Wt, int NT, int tid) {
-  const int tr = tid % 16, tc_ = tid / 16;   // 4 rows x 2 cols per thread
+  const int tr = tid % 16, tc_ = tid / 16;   // rows 4*tr..4*tr+3, columns CPT*tc_..
   for (int J = 0; J < NT; ++J) {
     const int kend = 32 * J;
-    float acc[4][2];
+    float acc[4][CPT];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int j = 0; j < 2; ++j) acc[i][j] = Xs[(kend + 2 * tc_ + j) * XLD + 4 * tr + i];
+      for (int j = 0; j < CPT; ++j) acc[i][j] = Xs[(kend + CPT * tc_ + j) * XLD + 4 * tr + i];
     // X_J -= X_{<J} L_{J,<J}^T
     for (int kt = 0; kt < J; ++kt) {
-      const float* lt = Lt + tl(J, kt) * TSZ + 2 * tc_;
+      const float* lt = Lt + tl(J, kt) * TSZ + CPT * tc_;
       const float* xt = Xs + (32 * kt) * XLD + 4 * tr;
 #pragma unroll 8
       for (int kk = 0; kk < 32; ++kk) {
         const float4 xv = *reinterpret_cast<const float4*>(xt + kk * XLD);
-        const float2 lv = *reinterpret_cast<const float2*>(lt + kk * 32);
-        acc[0][0] -= xv.x * lv.x; acc[0][1] -= xv.x * lv.y;
-        acc[1][0] -= xv.y * lv.x; acc[1][1] -= xv.y * lv.y;
-        acc[2][0] -= xv.z * lv.x; acc[2][1] -= xv.z * lv.y;
-        acc[3][0] -= xv.w * lv.x; acc[3][1] -= xv.w * lv.y;
+        const float xr[4] = {xv.x, xv.y, xv.z, xv.w};
+#pragma unroll
+        for (int j = 0; j < CPT; ++j) {
+          const float lv = lt[kk * 32 + j];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) acc[i][j] -= xr[i] * lv;
+        }
       }
     }
     __syncthreads();
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int j = 0; j < 2; ++j) Xs[(kend + 2 * tc_ + j) * XLD + 4 * tr + i] = acc[i][j];
+      for (int j = 0; j < CPT; ++j) Xs[(kend + CPT * tc_ + j) * XLD + 4 * tr + i] = acc[i][j];
     __syncthreads();
     // X_J = X_J * L_JJ^-T :  x[r][c] = sum_{m<=c} a[r][m] * (L^-1)[c][m]
-    float out[4][2] = {};
-    const float* W = Wt + J * TSZ + 2 * tc_;
+    float out[4][CPT] = {};
+    const float* W = Wt + J * TSZ + CPT * tc_;
 #pragma unroll 8
     for (int m = 0; m < 32; ++m) {
       const float4 av = *reinterpret_cast<const float4*>(&Xs[(kend + m) * XLD + 4 * tr]);
-      const float2 wv = *reinterpret_cast<const float2*>(W + m * 32);
-      out[0][0] += av.x * wv.x; out[0][1] += av.x * wv.y;
-      out[1][0] += av.y * wv.x; out[1][1] += av.y * wv.y;
-      out[2][0] += av.z * wv.x; out[2][1] += av.z * wv.y;
-      out[3][0] += av.w * wv.x; out[3][1] += av.w * wv.y;
+      const float ar[4] = {av.x, av.y, av.z, av.w};
+#pragma unroll
+      for (int j = 0; j < CPT; ++j) {
+        const float wv = W[m * 32 + j];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) out[i][j] += ar[i] * wv;
+      }
     }
     __syncthreads();
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int j = 0; j < 2; ++j) Xs[(kend + 2 * tc_ + j) * XLD + 4 * tr + i] = out[i][j];
+      for (int j = 0; j < CPT; ++j) Xs[(kend + CPT * tc_ + j) * XLD + 4 * tr + i] = out[i][j];
     __syncthreads();
   }
 }
