@@ -35,14 +35,27 @@ __global__ void f64_to_f32_kernel(const double* __restrict__ src, int lds, float
 // the diagonal (coalesced, no index division).  One partial per block.
 template <typename TA>
 __global__ void frob_lower_kernel(const TA* __restrict__ A, int lda, int n, double* partials) {
-  double s = 0.0;
+  double s = 0.0, s4[4] = {0.0, 0.0, 0.0, 0.0};
   for (int c = blockIdx.x; c < n; c += gridDim.x) {
     const TA* col = A + (size_t)c * lda;
-    for (int r = c + threadIdx.x; r < n; r += blockDim.x) {
+    if (threadIdx.x == 0) {
+      const double v = (double)col[c];
+      s += v * v;
+    }
+    // off-diagonal part of the column: four independent loads in flight
+    int r = c + 1 + threadIdx.x;
+    for (; r + 3 * (int)blockDim.x < n; r += 4 * blockDim.x)
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const double v = (double)col[r + u * blockDim.x];
+        s4[u] = fma(v, v, s4[u]);
+      }
+    for (; r < n; r += blockDim.x) {
       const double v = (double)col[r];
-      s += (r == c ? 1.0 : 2.0) * v * v;
+      s4[0] = fma(v, v, s4[0]);
     }
   }
+  s += 2.0 * ((s4[0] + s4[1]) + (s4[2] + s4[3]));
   __shared__ double red[8];
   s = warp_sum(s);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
