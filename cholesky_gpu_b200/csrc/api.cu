@@ -235,15 +235,14 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream) {
                        f->scratch64, f->winv, f->status, o.floor > 0.0f, stream));
     if (m <= 0) break;
     const int next_bs = std::min(b, m);
+    // panel solve, step decision and panel quantization in one launch
+    const QuantOut qo{f->q, bs, f->rowexp, f->mxexp, bs / 32, o.diag_pert ? f->sh + s + bs : nullptr};
     PHASE(MPCHOL_PH_TRSM, 1, stream,
-          launch_trsm_panel(f->tmapX, f->tmap32, n, s, bs, f->winv, f->d, f->dtilde, f->rowsq,
-                            &f->steps[k], &f->steps[k + 1], next_bs, dp, f->status, stream));
+          launch_trsm_panel(f->tmapX, f->tmap32, f->A, ld, n, s, bs, f->winv, f->d, f->dtilde,
+                            f->rowsq, &f->steps[k], &f->steps[k + 1], next_bs, dp, qo, f->status,
+                            stream));
     float* P = f->A + (size_t)s * ld + s + bs;
     float* C = f->A + (size_t)(s + bs) * ld + s + bs;
-    PHASE(MPCHOL_PH_QUANT, 1, stream, launch_quantize_panel(P, ld, m, bs, &f->steps[k], dp, f->q, bs, f->rowexp,
-                                          f->mxexp, bs / 32, f->rowsq + s + bs,
-                                          o.diag_pert ? f->sh + s + bs : nullptr, f->status,
-                                          stream));
     if (fixed) {
       if (o.precision == FP32)
         PHASE(MPCHOL_PH_SYRK_F32, 1, stream, launch_syrk_f32(C, ld, m, bs, P, ld, nullptr, f->status, stream));

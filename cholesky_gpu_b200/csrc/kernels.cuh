@@ -18,6 +18,7 @@ struct StepState {
   int literal_code;             // reference-literal: max over rows of (2 - choice index); choice index 0 FP32, 1 FP16, 2 E4M3
   int prec;                     // chosen trailing-update precision (Fmt)
   int fp64_diag;                // 1: factor this step's diagonal block in FP64
+  int grid_bar;                 // arrivals at the panel solve's grid barrier
 };
 
 struct DecisionParams {
@@ -40,26 +41,31 @@ cudaError_t launch_potrf(const CUtensorMap& tmap32, float* A, int lda, int n, in
                          const int* fp64_flag, double* scratch64, float* winv, DevStatus* st,
                          bool may_fp64, cudaStream_t stream);
 
-// ---- panel TRSM + fused diagonal tracker / decision statistics ----------
+// ---- panel TRSM + fused diagonal tracker, decision and quantization ------
+// Where the fused panel solve writes the quantized panel: K-major codes q
+// (row stride ldq elements), per-row exponents or per-32 E8M0 scales, and
+// the rounding-shift accumulator of the trailing rows (nullable).
+struct QuantOut {
+  void* q;
+  int ldq;
+  int8_t* rowexp;
+  uint8_t* mxexp;
+  int ldmx;
+  float* sh;
+};
 // Solves X * L11^T = A21 in place for rows [s+bs, n) of block column s,
-// subtracts each row's sum of squares from dtilde, stores it in rowsq, and
-// folds the switching statistics of the rows into step (and the FP64 flag of
-// the next diagonal block into next).  tmapX: TMA map over A with 64 x bs
-// boxes; tmap32 as for launch_potrf.
-cudaError_t launch_trsm_panel(const CUtensorMap& tmapX, const CUtensorMap& tmap32, int n, int s,
-                              int bs, const float* winv, const float* d, float* dtilde,
-                              float* rowsq, StepState* step, StepState* next, int next_bs,
-                              const DecisionParams& dp, DevStatus* st, cudaStream_t stream);
+// subtracts each row's sum of squares from dtilde, stores it in rowsq, folds
+// the switching statistics into step (and the FP64 flag of the next diagonal
+// block into next), then resolves the step precision (step->prec) and writes
+// the quantized panel.  tmapX: TMA map over A with 64 x bs boxes; tmap32 as
+// for launch_potrf.  Cooperative launch (grid barrier inside).
+cudaError_t launch_trsm_panel(const CUtensorMap& tmapX, const CUtensorMap& tmap32, float* A,
+                              int lda, int n, int s, int bs, const float* winv, const float* d,
+                              float* dtilde, float* rowsq, StepState* step, StepState* next,
+                              int next_bs, const DecisionParams& dp, const QuantOut& qo,
+                              DevStatus* st, cudaStream_t stream);
 
-// ---- decision + panel quantization --------------------------------------
-// Resolves the step precision (from the policy or the statistics in step),
-// then writes the K-major quantized panel q (row stride ldq bytes-or-halfs,
-// see quant.cu) with per-row or per-32-block scales, and accumulates the
-// rounding-shift estimate sh[i] += u_p * rowsq[i] for low-precision steps.
-cudaError_t launch_quantize_panel(const float* P, int ldp, int m, int k, StepState* step,
-                                  const DecisionParams& dp, void* q, int ldq, int8_t* rowexp,
-                                  uint8_t* mxexp, int ldmx, const float* rowsq, float* sh,
-                                  DevStatus* st, cudaStream_t stream);
+// ---- panel quantization ---------------------------------------------------
 // Fixed-format variant (test entry point): no decision, no shift.
 cudaError_t launch_quantize_rows(const float* P, int ldp, int m, int k, int fmt, void* q, int ldq,
                                  int8_t* rowexp, uint8_t* mxexp, int ldmx, cudaStream_t stream);

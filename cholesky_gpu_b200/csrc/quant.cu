@@ -4,142 +4,23 @@
 // (src/kernels_macros.cuh:191-211, src/switching_chol.cuh:117-124) and its
 // panel conversions convert_fp32_to_mxe4m3 / convert_transpose_fp32_to_mxe4m3
 // (src/fp8_utils.cuh:27-130) and convertFloatToHalf (src/kernels_macros.cuh:115-124).
-// The decision never leaves the device: every CTA resolves the same precision
-// from the statistics the panel solve reduced, CTA 0 records it, and the
-// trailing-update kernels read it.  The quantized panel is written K-major
+// The decision never leaves the device: the fused panel solve (trsm.cu)
+// resolves it from its own statistics after a grid barrier and quantizes the
+// panel with the tile routine of quant.cuh; this file keeps the stand-alone
+// and batched quantizers.  The quantized panel is written K-major
 // (row-major m x k) so TMA can stage it for the tensor-core update.
 #include "common.cuh"
 #include "kernels.cuh"
+#include "quant.cuh"
 
 namespace mpchol {
 namespace {
-
-constexpr int QROWS = 32;    // rows per CTA
-constexpr int QTHR = 256;
-
-__device__ __forceinline__ int resolve_precision(const StepState* step, const DecisionParams& dp) {
-  if (dp.policy != SWITCHING) return dp.policy;
-  if (dp.switch_mode == 1) {
-    const int code = step->literal_code;            // 2 - min choice index
-    const int choice = 2 - code;
-    return choice == 0 ? FP32 : (choice == 1 ? FP16 : E4M3);
-  }
-  const float ratio = __uint_as_float(step->max_ratio_bits);
-  for (int k = 0; k < dp.ladder_len; ++k) {
-    const int p = dp.ladder[k];
-    if (unit_roundoff(p) * ratio <= dp.eps_prime) return p;
-  }
-  // no entry meets the bound: the ladder's most precise (last) entry
-  return dp.ladder_len > 0 ? dp.ladder[dp.ladder_len - 1] : FP32;
-}
-
-// Quantize one CTA tile of QROWS rows x k columns.  Lane l of a warp owns the
-// contiguous columns [l*c, (l+1)*c), c = k/32 (k is a multiple of 32, <= 256).
-// lo_rows: rows from a row of the FP16X2 hi panel to the same row of the lo
-// panel (m for a single panel; the arena height for batched panels).
-__device__ void quantize_tile(const float* __restrict__ P, int ldp, int m, int k, int fmt,
-                              void* q, int ldq, int8_t* rowexp, uint8_t* mxexp, int ldmx,
-                              float* tile, int lo_rows) {
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int row0 = blockIdx.x * QROWS;
-  const int nr = min(QROWS, m - row0);
-  // stage the rows (coalesced column reads, 16 loads in flight per thread
-  // before their shared-memory stores), padded stride QROWS+1
-  constexpr int B = 16;
-  for (int e0 = tid; e0 < k * QROWS; e0 += B * QTHR) {
-    float vv[B];
-#pragma unroll
-    for (int u = 0; u < B; ++u) {
-      const int e = e0 + u * QTHR;
-      const int c = e / QROWS, r = e % QROWS;
-      vv[u] = (e < k * QROWS && r < nr) ? P[(size_t)c * ldp + row0 + r] : 0.0f;
-    }
-#pragma unroll
-    for (int u = 0; u < B; ++u) {
-      const int e = e0 + u * QTHR;
-      if (e < k * QROWS) tile[(e / QROWS) * (QROWS + 1) + e % QROWS] = vv[u];
-    }
-  }
-  __syncthreads();
-  const int cpl = k / 32;                   // columns per lane
-  for (int r = warp; r < nr; r += QTHR / 32) {
-    const int gi = row0 + r;
-    float v[8];
-    float amax = 0.0f;
-#pragma unroll
-    for (int t = 0; t < 8; ++t) {
-      v[t] = (t < cpl) ? tile[(lane * cpl + t) * (QROWS + 1) + r] : 0.0f;
-      amax = fmaxf(amax, fabsf(v[t]));
-    }
-    if (fmt == MXFP8) {
-      // one E8M0 scale per 32 consecutive columns = 32/cpl lanes
-      const int lpb = 32 / cpl;
-      float bmax = amax;
-      for (int o = 1; o < lpb; o <<= 1) bmax = fmaxf(bmax, __shfl_xor_sync(0xffffffffu, bmax, o));
-      const int e = mx_scale_exp(bmax);
-      const float inv = pow2f(-e);
-      uint8_t* qr = reinterpret_cast<uint8_t*>(q) + (size_t)gi * ldq + lane * cpl;
-#pragma unroll
-      for (int t = 0; t < 8; ++t)
-        if (t < cpl) qr[t] = f32_to_e4m3(v[t] * inv);
-      if ((lane % lpb) == 0) mxexp[(size_t)gi * ldmx + lane / lpb] = (uint8_t)(e + 127);
-    } else {
-      const float rmax = warp_max(amax);
-      const int e = row_scale_exp(rmax, fmt);
-      const float inv = pow2f(-e);
-      if (fmt == FP16) {
-        uint16_t* qr = reinterpret_cast<uint16_t*>(q) + (size_t)gi * ldq + lane * cpl;
-#pragma unroll
-        for (int t = 0; t < 8; ++t)
-          if (t < cpl) qr[t] = f32_to_f16(v[t] * inv);
-      } else if (fmt == FP16X2) {
-        // hi = fp16(x), lo = fp16(x - hi); x - hi is exact in FP32.  The lo
-        // panel follows the hi panel (lo_rows rows further on).
-        uint16_t* qh = reinterpret_cast<uint16_t*>(q) + (size_t)gi * ldq + lane * cpl;
-        uint16_t* ql = qh + (size_t)lo_rows * ldq;
-#pragma unroll
-        for (int t = 0; t < 8; ++t)
-          if (t < cpl) {
-            const float xs = v[t] * inv;
-            const __half h = __float2half_rn(xs);
-            qh[t] = __half_as_ushort(h);
-            ql[t] = f32_to_f16(xs - __half2float(h));
-          }
-      } else {
-        uint8_t* qr = reinterpret_cast<uint8_t*>(q) + (size_t)gi * ldq + lane * cpl;
-#pragma unroll
-        for (int t = 0; t < 8; ++t)
-          if (t < cpl) qr[t] = (fmt == E4M3) ? f32_to_e4m3(v[t] * inv) : f32_to_e5m2(v[t] * inv);
-      }
-      if (lane == 0) rowexp[gi] = (int8_t)e;
-    }
-  }
-}
-
-__global__ void __launch_bounds__(QTHR)
-quantize_panel_kernel(const float* __restrict__ P, int ldp, int m, int k, StepState* step,
-                      DecisionParams dp, void* q, int ldq, int8_t* rowexp, uint8_t* mxexp, int ldmx,
-                      const float* __restrict__ rowsq, float* sh, DevStatus* st) {
-  if (st->code != 0) return;
-  extern __shared__ __align__(16) float qtile[];
-  const int p = resolve_precision(step, dp);
-  if (blockIdx.x == 0 && threadIdx.x == 0) step->prec = p;
-  if (p == FP32) return;
-  if (sh != nullptr) {
-    const float u = unit_roundoff(p);
-    for (int r = threadIdx.x; r < QROWS; r += QTHR) {
-      const int gi = blockIdx.x * QROWS + r;
-      if (gi < m) sh[gi] += u * rowsq[gi];
-    }
-  }
-  quantize_tile(P, ldp, m, k, p, q, ldq, rowexp, mxexp, ldmx, qtile, m);
-}
 
 __global__ void __launch_bounds__(QTHR)
 quantize_rows_kernel(const float* __restrict__ P, int ldp, int m, int k, int fmt, void* q, int ldq,
                      int8_t* rowexp, uint8_t* mxexp, int ldmx) {
   extern __shared__ __align__(16) float qtile[];
-  quantize_tile(P, ldp, m, k, fmt, q, ldq, rowexp, mxexp, ldmx, qtile, m);
+  quantize_tile(P, ldp, m, k, fmt, q, ldq, rowexp, mxexp, ldmx, qtile, m, blockIdx.x * QROWS);
 }
 
 // Batched: blockIdx.y = system; its panel goes to rows q_row0.. of the
@@ -165,7 +46,7 @@ quantize_batched_kernel(BatchSys* __restrict__ sys, const BatchStep* __restrict_
   const size_t esz = (fmt == FP16 || fmt == FP16X2) ? 2 : 1;
   void* qs = reinterpret_cast<uint8_t*>(q) + (size_t)T.q_row0 * bs * esz;
   quantize_tile(P, S.ld, m, bs, fmt, qs, bs, rowexp + T.q_row0,
-                mxexp ? mxexp + (size_t)T.q_row0 * (bs / 32) : nullptr, bs / 32, qtile, qrows);
+                mxexp ? mxexp + (size_t)T.q_row0 * (bs / 32) : nullptr, bs / 32, qtile, qrows, blockIdx.x * QROWS);
 }
 
 __global__ void quantize_elems_kernel(const float* __restrict__ x, void* q, long long count, int fmt) {
@@ -219,20 +100,6 @@ __global__ void quantize_hash_kernel(unsigned long long first, unsigned long lon
 size_t qtile_smem(int k) { return (size_t)k * (QROWS + 1) * sizeof(float); }
 
 }  // namespace
-
-cudaError_t launch_quantize_panel(const float* P, int ldp, int m, int k, StepState* step,
-                                  const DecisionParams& dp, void* q, int ldq, int8_t* rowexp,
-                                  uint8_t* mxexp, int ldmx, const float* rowsq, float* sh,
-                                  DevStatus* st, cudaStream_t stream) {
-  if (m <= 0) return cudaSuccess;
-  const size_t smem = qtile_smem(k);
-  cudaError_t e = cudaFuncSetAttribute(quantize_panel_kernel,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  quantize_panel_kernel<<<ceil_div(m, QROWS), QTHR, smem, stream>>>(P, ldp, m, k, step, dp, q, ldq,
-                                                                    rowexp, mxexp, ldmx, rowsq, sh, st);
-  return cudaGetLastError();
-}
 
 cudaError_t launch_quantize_rows(const float* P, int ldp, int m, int k, int fmt, void* q, int ldq,
                                  int8_t* rowexp, uint8_t* mxexp, int ldmx, cudaStream_t stream) {

@@ -16,8 +16,11 @@
 // squares into the Schur-diagonal tracker dtilde and reduces the switching
 // statistics (max d/dtilde, reference-literal choice) and the near-indefinite
 // flag of the next diagonal block.
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.cuh"
+#include "quant.cuh"
 #include "tc_ptx.cuh"
 
 namespace mpchol {
@@ -92,12 +95,25 @@ __device__ void trsm_slab(float* Xs, const float* Lt, const float* Wt, int NT, i
   }
 }
 
-__global__ void __launch_bounds__(NTHR)
+constexpr long long kGridBarPolls = 1ll << 24;
+static_assert(NTHR == QTHR, "the fused quantizer runs with the panel solve's threads");
+
+// Persistent panel solve with the quantization of the panel fused in.
+// Phase 1: CTA c solves the 64-row slabs c, c + grid, ... (L11's tiles and
+// tile inverses are staged once per CTA by TMA, each slab by one 2-D box),
+// writes them back, and folds their rows into the diagonal tracker and the
+// switching statistics.  A grid barrier (the launch is cooperative, so all
+// CTAs are resident; the wait is bounded) then makes the statistics and the
+// solved panel complete.  Phase 2: every CTA resolves the same step
+// precision and quantizes 32-row tiles of the panel (read back from L2) into
+// the K-major codes the trailing update reads, adding the step's rounding
+// shift u_p * sum_j L_ij^2 to sh.
+__global__ void __launch_bounds__(NTHR, 1)
 trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_constant__ CUtensorMap tmap32,
-                  int n, int s, int bs, const float* __restrict__ winv,
+                  float* __restrict__ A, int lda, int n, int s, int bs, const float* __restrict__ winv,
                   const float* __restrict__ d, float* __restrict__ dtilde, float* __restrict__ rowsq,
-                  StepState* step, StepState* next, int next_bs, DecisionParams dp, DevStatus* st) {
-  if (st->code != 0) return;
+                  StepState* step, StepState* next, int next_bs, DecisionParams dp, DevStatus* st,
+                  QuantOut qo) {
   extern __shared__ __align__(128) float sm[];
   const int NT = bs / 32;
   float* Xs = sm;                                        // [bs][XLD]
@@ -109,74 +125,115 @@ trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_consta
   __shared__ int s_ok;
 
   const int tid = threadIdx.x;
-  const int row0 = s + bs + blockIdx.x * TR;   // first global row of this CTA
-  const int nrows = min(TR, n - row0);
-  if (nrows <= 0) return;
-
-  // ---- stage with TMA (rows past n arrive as zeros) -----------------------
+  const int m = n - s - bs;
+  const int nslab = ceil_div(m, TR);
   if (tid == 0) {
-    s_ok = 1;
-    const int nlt = NT * (NT - 1) / 2;
+    s_ok = st->code == 0;
     tc::mbar_init(&bar, 1);
     tc::fence_mbar_init();
-    tc::mbar_expect_tx(&bar, (uint32_t)((bs * XLD + nlt * TSZ + NT * TSZ) * sizeof(float)));
-    tc::tma_load_2d(Xs, &tmapX, &bar, row0, s);
-    for (int I = 1; I < NT; ++I)
-      for (int M = 0; M < I; ++M)
-        tc::tma_load_2d(Lt + tl(I, M) * TSZ, &tmap32, &bar, s + 32 * I, s + 32 * M);
-    tc::bulk_load_1d(Wt, winv, (uint32_t)(NT * TSZ * sizeof(float)), &bar);
-    if (!tc::mbar_wait(&bar, 0)) {
-      s_ok = 0;
-      set_status(st, MPCHOL_ERR_TIMEOUT, row0);
-      tc::mbar_wait(&bar, 0);
+  }
+  __syncthreads();
+  uint32_t phase = 0;
+  float bm = 0.0f;   // this CTA's max d/dtilde and literal code over its slabs
+  int bl = 0;
+  for (int slab = blockIdx.x; slab < nslab && s_ok; slab += gridDim.x, phase ^= 1u) {
+    const int row0 = s + bs + slab * TR;                 // first global row of the slab
+    const int nrows = min(TR, n - row0);
+    // ---- stage with TMA (rows past n arrive as zeros) ---------------------
+    if (tid == 0) {
+      const bool first = slab == (int)blockIdx.x;
+      const int nlt = NT * (NT - 1) / 2;
+      uint32_t bytes = (uint32_t)(bs * XLD * sizeof(float));
+      if (first) bytes += (uint32_t)((nlt * TSZ + NT * TSZ) * sizeof(float));
+      tc::mbar_expect_tx(&bar, bytes);
+      tc::tma_load_2d(Xs, &tmapX, &bar, row0, s);
+      if (first) {
+        for (int I = 1; I < NT; ++I)
+          for (int M = 0; M < I; ++M)
+            tc::tma_load_2d(Lt + tl(I, M) * TSZ, &tmap32, &bar, s + 32 * I, s + 32 * M);
+        tc::bulk_load_1d(Wt, winv, (uint32_t)(NT * TSZ * sizeof(float)), &bar);
+      }
+      if (!tc::mbar_wait(&bar, phase)) {
+        s_ok = 0;
+        set_status(st, MPCHOL_ERR_TIMEOUT, row0);
+        tc::mbar_wait(&bar, phase);
+      }
     }
+    __syncthreads();
+    if (!s_ok) break;
+    trsm_slab(Xs, Lt, Wt, NT, tid);
+    // ---- write the solved slab back (coalesced; rows past n skipped) -----
+    for (int e = tid; e < bs * TR; e += NTHR) {
+      const int c = e / TR, r = e % TR;
+      if (r < nrows) A[(size_t)(s + c) * lda + row0 + r] = Xs[c * XLD + r];
+    }
+    // ---- Schur diagonal tracker and switching statistics of the slab -----
+    if (tid < nrows) {
+      const int gi = row0 + tid;
+      float sq = 0.0f;
+      for (int c = 0; c < bs; ++c) { const float v = Xs[c * XLD + tid]; sq += v * v; }
+      rowsq[gi] = sq;
+      const float dt = dtilde[gi] - sq;
+      dtilde[gi] = dt;
+      const float di = d[gi];
+      float ratio = dt > 0.0f ? di / dt : INFINITY;
+      if (isnan(ratio)) ratio = INFINITY;
+      bm = fmaxf(bm, ratio);
+      // reference list {FP32, FP16, E4M3} with the reference's machine epsilons
+      const float ref_eps[3] = {1.1920929e-7f, 0.0009765625f, 0.125f};
+      int pick = 0;
+      for (int p = 0; p < 3; ++p)
+        if (ref_eps[p] * dt >= dp.eps_prime * di) { pick = p; break; }
+      bl = max(bl, 2 - pick);
+      if (next != nullptr && dp.floor_ratio > 0.0f && gi - (s + bs) < next_bs &&
+          dt <= dp.floor_ratio * di)
+        next->fp64_diag = 1;
+    }
+    __syncthreads();                                     // Xs is restaged next
   }
-  __syncthreads();
-  if (!s_ok) return;
-
-  trsm_slab(Xs, Lt, Wt, NT, tid);
-  // ---- write the solved slab back (TMA store clips rows past n) -----------
-  tc::fence_proxy_async_smem();
-  __syncthreads();
-  if (tid == 0) {
-    tc::tma_store_2d(&tmapX, Xs, row0, s);
-    tc::bulk_commit();
-  }
-  // ---- fused epilogue: Schur diagonal tracker and switching statistics --
-  float ratio = 0.0f;
-  int lit = 0;   // 2 - (reference-literal choice index); max over rows
-  if (tid < nrows) {
-    const int gi = row0 + tid;
-    float sq = 0.0f;
-    for (int c = 0; c < bs; ++c) { const float v = Xs[c * XLD + tid]; sq += v * v; }
-    rowsq[gi] = sq;
-    const float dt = dtilde[gi] - sq;
-    dtilde[gi] = dt;
-    const float di = d[gi];
-    ratio = dt > 0.0f ? di / dt : INFINITY;
-    if (isnan(ratio)) ratio = INFINITY;
-    // reference list {FP32, FP16, E4M3} with the reference's machine epsilons
-    const float ref_eps[3] = {1.1920929e-7f, 0.0009765625f, 0.125f};
-    int pick = 0;
-    for (int p = 0; p < 3; ++p)
-      if (ref_eps[p] * dt >= dp.eps_prime * di) { pick = p; break; }
-    lit = 2 - pick;
-    if (next != nullptr && dp.floor_ratio > 0.0f && gi - (s + bs) < next_bs &&
-        dt <= dp.floor_ratio * di)
-      next->fp64_diag = 1;
-  }
-  float wm = warp_max(ratio);
-  int wl = lit;
+  // ---- statistics of the CTA, then the grid barrier ----------------------
+  bm = warp_max(bm);
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) wl = max(wl, __shfl_xor_sync(0xffffffffu, wl, o));
-  if ((tid & 31) == 0) { red_max[tid >> 5] = wm; red_lit[tid >> 5] = wl; }
+  for (int o = 16; o > 0; o >>= 1) bl = max(bl, __shfl_xor_sync(0xffffffffu, bl, o));
+  if ((tid & 31) == 0) { red_max[tid >> 5] = bm; red_lit[tid >> 5] = bl; }
+  __threadfence();                                       // this thread's panel writes
   __syncthreads();
   if (tid == 0) {
-    float bm = 0.0f; int bl = 0;
-    for (int w = 0; w < NTHR / 32; ++w) { bm = fmaxf(bm, red_max[w]); bl = max(bl, red_lit[w]); }
-    atomicMax(&step->max_ratio_bits, __float_as_uint(bm));
-    atomicMax(&step->literal_code, bl);
-    tc::bulk_wait_read();
+    float cm = 0.0f; int cl = 0;
+    for (int w = 0; w < NTHR / 32; ++w) { cm = fmaxf(cm, red_max[w]); cl = max(cl, red_lit[w]); }
+    atomicMax(&step->max_ratio_bits, __float_as_uint(cm));
+    atomicMax(&step->literal_code, cl);
+    __threadfence();
+    atomicAdd(&step->grid_bar, 1);
+    long long it = 0;
+    while (*reinterpret_cast<volatile int*>(&step->grid_bar) < (int)gridDim.x) {
+      if (++it > kGridBarPolls) {
+        set_status(st, MPCHOL_ERR_TIMEOUT, s);
+        break;
+      }
+      __nanosleep(32);
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  if (*reinterpret_cast<volatile int*>(&st->code) != 0) return;
+  // ---- phase 2: the step precision and the quantized panel ----------------
+  StepState ss;
+  ss.max_ratio_bits = *reinterpret_cast<volatile unsigned int*>(&step->max_ratio_bits);
+  ss.literal_code = *reinterpret_cast<volatile int*>(&step->literal_code);
+  const int p = resolve_precision(&ss, dp);
+  if (blockIdx.x == 0 && tid == 0) step->prec = p;
+  if (p == FP32) return;
+  const float* P = A + (size_t)s * lda + s + bs;
+  const float u = unit_roundoff(p);
+  for (int t = blockIdx.x; t * QROWS < m; t += gridDim.x) {
+    if (qo.sh != nullptr)
+      for (int r = tid; r < QROWS; r += NTHR) {
+        const int gi = t * QROWS + r;
+        if (gi < m) qo.sh[gi] += u * rowsq[s + bs + gi];
+      }
+    quantize_tile(P, lda, m, bs, p, qo.q, qo.ldq, qo.rowexp, qo.mxexp, qo.ldmx, Xs, m, t * QROWS);
+    __syncthreads();                                     // the staging tile is reused
   }
 }
 
@@ -227,10 +284,11 @@ trsm_batched_kernel(BatchSys* __restrict__ sys, int s, int b) {
 
 }  // namespace
 
-cudaError_t launch_trsm_panel(const CUtensorMap& tmapX, const CUtensorMap& tmap32, int n, int s,
-                              int bs, const float* winv, const float* d, float* dtilde,
-                              float* rowsq, StepState* step, StepState* next, int next_bs,
-                              const DecisionParams& dp, DevStatus* st, cudaStream_t stream) {
+cudaError_t launch_trsm_panel(const CUtensorMap& tmapX, const CUtensorMap& tmap32, float* A,
+                              int lda, int n, int s, int bs, const float* winv, const float* d,
+                              float* dtilde, float* rowsq, StepState* step, StepState* next,
+                              int next_bs, const DecisionParams& dp, const QuantOut& qo,
+                              DevStatus* st, cudaStream_t stream) {
   const int m = n - s - bs;
   if (m <= 0) return cudaSuccess;
   const size_t smem = trsm_smem_floats(bs) * sizeof(float);
@@ -238,9 +296,34 @@ cudaError_t launch_trsm_panel(const CUtensorMap& tmapX, const CUtensorMap& tmap3
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)(trsm_smem_floats(256) * sizeof(float)));
   if (e != cudaSuccess) return e;
-  trsm_panel_kernel<<<ceil_div(m, TR), NTHR, smem, stream>>>(tmapX, tmap32, n, s, bs, winv, d,
-                                                             dtilde, rowsq, step, next, next_bs,
-                                                             dp, st);
+  // one CTA per SM at most (shared memory), all resident: the launch is
+  // cooperative because the CTAs meet at a grid barrier
+  static int nsm_cache[64] = {};
+  int dev = 0;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  int& nsm = nsm_cache[dev & 63];
+  if (nsm == 0) {
+    int per_sm = 0, sms = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+             &per_sm, trsm_panel_kernel, NTHR, trsm_smem_floats(256) * sizeof(float))) != cudaSuccess)
+      return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+      return e;
+    nsm = std::max(1, per_sm) * sms;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(std::min(ceil_div(m, TR), nsm));
+  cfg.blockDim = dim3(NTHR);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  e = cudaLaunchKernelEx(&cfg, trsm_panel_kernel, tmapX, tmap32, A, lda, n, s, bs, winv, d, dtilde,
+                         rowsq, step, next, next_bs, dp, st, qo);
+  if (e != cudaSuccess) return e;
   return cudaGetLastError();
 }
 
