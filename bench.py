@@ -511,6 +511,22 @@ def _timed(fn, steps, warmup, stream):
     return statistics.median(times), last
 
 
+def _phases(fn):
+    """Per-phase device times (library CUDA events) of one call of fn."""
+    import torch
+    from cholesky_gpu_b200 import _lib
+    lib = _lib.load()
+    lib.mpchol_profile_enable(1)
+    p0 = _lib.Profile()
+    lib.mpchol_profile_read(p0, 1)
+    fn()
+    torch.cuda.synchronize()
+    p = _lib.Profile()
+    lib.mpchol_profile_read(p, 1)
+    lib.mpchol_profile_enable(0)
+    return {nm: round(p.ms[i], 4) for i, nm in enumerate(_lib.PHASE_NAMES) if p.calls[i]}
+
+
 def _base(args, world, value, unit, dtype, data, config, extra):
     out = {"metric": METRIC, "value": round(value, 3), "unit": unit, "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(value, 3),
@@ -549,8 +565,8 @@ def run_rbf(args, world, rank, local):
             f.compute(K32)
             return f.pcg(K32, B, rel_tol=args.tol, max_it=args.max_it, check_every=args.check_every)
         ms, (X_, rep) = _timed(step, args.steps, args.warmup, stream)
-        res[name] = (ms, rep)
-    ms, rep = res[prec]
+        res[name] = (ms, rep, _phases(step))
+    ms, rep, _ = res[prec]
     info = arms[prec].info()
     steps_used = {nm: info.steps_by_prec[i] for i, nm in
                   ((0, "fp32"), (1, "fp16"), (2, "e4m3"), (3, "e5m2"), (4, "mxfp8"), (6, "fp16x2"))
@@ -564,7 +580,8 @@ def run_rbf(args, world, rank, local):
                   "iterations": {k: v[1].iterations for k, v in res.items()},
                   "converged": {k: v[1].converged for k, v in res.items()},
                   "rel_residual": {k: v[1].rel_residual for k, v in res.items()},
-                  "kernel_build_ms": round(t_build, 3), "step_precisions": steps_used})
+                  "kernel_build_ms": round(t_build, 3), "step_precisions": steps_used,
+                  "phase_ms": {k: v[2] for k, v in res.items()}})
 
 
 def run_rbf_grad(args, world, rank, local):

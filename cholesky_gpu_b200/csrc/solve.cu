@@ -54,21 +54,18 @@ struct TileRegs {
   double v[CH][4];
 };
 
+// Tile values stay in the matrix's own type in registers (FP32 tiles take
+// half the registers of a widened copy); they are widened at each use.
 template <int CH>
 __device__ __forceinline__ void load_cols(const float* T, int ld, int rloc, int rows_valid,
-                                          int col0, int cols_valid, double (&v)[CH][4]) {
-  float f[CH][4];
+                                          int col0, int cols_valid, float (&v)[CH][4]) {
   const int nv = min(4, rows_valid - rloc);
 #pragma unroll
   for (int cc = 0; cc < CH; ++cc) {
     const int c = col0 + cc;
-    if (c < cols_valid && nv > 0) load4<float>(T + (size_t)c * ld + rloc, nv, f[cc]);
-    else f[cc][0] = f[cc][1] = f[cc][2] = f[cc][3] = 0.0f;
+    if (c < cols_valid && nv > 0) load4<float>(T + (size_t)c * ld + rloc, nv, v[cc]);
+    else v[cc][0] = v[cc][1] = v[cc][2] = v[cc][3] = 0.0f;
   }
-#pragma unroll
-  for (int cc = 0; cc < CH; ++cc)
-#pragma unroll
-    for (int r = 0; r < 4; ++r) v[cc][r] = f[cc][r];
 }
 
 template <int CH>
@@ -84,16 +81,23 @@ __device__ __forceinline__ void load_cols(const double* T, int ld, int rloc, int
   }
 }
 
-// Sum each of the 16 per-lane values w[i] over the 32 lanes of the warp with
-// 16 shuffles (a butterfly that halves the values kept per lane at each
-// step).  Returns the sum of column col_of_lane(lane); lanes l and l^1 hold
-// the same one.
+// Sum each of the W per-lane values w[i] (W = 8 or 16) over the 32 lanes of
+// the warp: a butterfly that halves the values a lane keeps at each step
+// (W/2 + W/4 + ... shuffles), then plain xor steps for the remaining lane
+// bits.  Lane l ends with the sum of column col_of_lane<W>(l); the lanes
+// that differ only in the low 5 - log2(W) bits hold the same sum.
+template <int W>
 __device__ __forceinline__ int col_of_lane(int lane) {
-  return ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
-}
-__device__ __forceinline__ double butterfly16(double (&w)[16], int lane) {
+  int c = 0;
 #pragma unroll
-  for (int h = 8, off = 16; h >= 1; h >>= 1, off >>= 1) {
+  for (int off = 16, h = W / 2; h >= 1; off >>= 1, h >>= 1) c += ((lane & off) ? h : 0);
+  return c;
+}
+template <int W>
+__device__ __forceinline__ double butterfly(double (&w)[W], int lane) {
+  int off = 16;
+#pragma unroll
+  for (int h = W / 2; h >= 1; h >>= 1, off >>= 1) {
     const bool upper = (lane & off) != 0;
 #pragma unroll
     for (int i = 0; i < h; ++i) {
@@ -102,13 +106,16 @@ __device__ __forceinline__ double butterfly16(double (&w)[16], int lane) {
       w[i] = keep + __shfl_xor_sync(0xffffffffu, send, off);
     }
   }
-  return w[0] + __shfl_xor_sync(0xffffffffu, w[0], 1);
+  double v = w[0];
+#pragma unroll
+  for (; off >= 1; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  return v;
 }
 
 // Accumulate a 128 x 128 tile times a vector segment.
 //   NOTRANS: part[r][k] += T[r][c] * vin[c][k]   (per-thread rows, summed over the warp's columns)
-//   TRANS  : colsum[c][k] = sum_r T[r][c] * vin[r][k], reduced over the warp (butterfly
-//            for NR <= 2, one shuffle tree per column otherwise)
+//   TRANS  : colsum[c][k] = sum_r T[r][c] * vin[r][k], the CH columns of a chunk reduced
+//            over the warp together by one butterfly per rhs
 // `mask`: 0 none, 1 keep r >= c (lower incl. diagonal), 2 keep r > c.
 template <typename TA, int NR, int CH>
 __device__ __forceinline__ void tile_pass(const TA* T, int ld, int rows_valid, int cols_valid,
@@ -117,53 +124,46 @@ __device__ __forceinline__ void tile_pass(const TA* T, int ld, int rows_valid, i
                                           int mask_t, bool do_nt, bool do_t) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int rloc = 4 * lane;
-  constexpr bool BFLY = NR <= 2;
-  double pc[BFLY ? 16 : 1][NR];   // per-lane column partials (butterfly path)
+  constexpr int LOWBITS = (CH == 16) ? 1 : 3;   // lanes holding the same column sum
 #pragma unroll
   for (int cb = 0; cb < 16; cb += CH) {
-    double v[CH][4];
+    TA v[CH][4];
     load_cols<CH>(T, ld, rloc, rows_valid, warp * 16 + cb, cols_valid, v);
+    if (do_nt) {
 #pragma unroll
-    for (int cc = 0; cc < CH; ++cc) {
-      const int c = warp * 16 + cb + cc;
-      if (do_nt) {
+      for (int cc = 0; cc < CH; ++cc) {
+        const int c = warp * 16 + cb + cc;
 #pragma unroll
         for (int k = 0; k < NR; ++k) {
           const double xc = vin_cols[c * NR + k];
 #pragma unroll
           for (int r = 0; r < 4; ++r) {
             const bool keep = mask_nt == 0 || (mask_nt == 1 ? (rloc + r >= c) : (rloc + r > c));
-            if (keep) acc[r][k] = fma(v[cc][r], xc, acc[r][k]);
-          }
-        }
-      }
-      if (do_t) {
-#pragma unroll
-        for (int k = 0; k < NR; ++k) {
-          double s = 0.0;
-#pragma unroll
-          for (int r = 0; r < 4; ++r) {
-            const bool keep = mask_t == 0 || (mask_t == 1 ? (rloc + r >= c) : (rloc + r > c));
-            if (keep) s = fma(v[cc][r], vin_rows[(rloc + r) * NR + k], s);
-          }
-          if (BFLY) {
-            pc[BFLY ? cb + cc : 0][k] = s;
-          } else {
-            s = warp_sum(s);
-            if (lane == 0) colsum_smem[c * NR + k] = s;
+            if (keep) acc[r][k] = fma((double)v[cc][r], xc, acc[r][k]);
           }
         }
       }
     }
-  }
-  if (BFLY && do_t) {
+    if (do_t) {
+      // one rhs at a time (bounded register pressure for NR > 2)
+#pragma unroll 1
+      for (int k = 0; k < NR; ++k) {
+        double w[CH];
 #pragma unroll
-    for (int k = 0; k < NR; ++k) {
-      double w[16];
+        for (int cc = 0; cc < CH; ++cc) {
+          const int c = warp * 16 + cb + cc;
+          double sacc = 0.0;
 #pragma unroll
-      for (int i = 0; i < 16; ++i) w[i] = pc[BFLY ? i : 0][k];
-      const double sum = butterfly16(w, lane);
-      if ((lane & 1) == 0) colsum_smem[(warp * 16 + col_of_lane(lane)) * NR + k] = sum;
+          for (int r = 0; r < 4; ++r) {
+            const bool keep = mask_t == 0 || (mask_t == 1 ? (rloc + r >= c) : (rloc + r > c));
+            if (keep) sacc = fma((double)v[cc][r], vin_rows[(rloc + r) * NR + k], sacc);
+          }
+          w[cc] = sacc;
+        }
+        const double sum = butterfly<CH>(w, lane);
+        if ((lane & LOWBITS) == 0)
+          colsum_smem[(warp * 16 + cb + col_of_lane<CH>(lane)) * NR + k] = sum;
+      }
     }
   }
 }
