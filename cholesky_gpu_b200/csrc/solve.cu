@@ -113,9 +113,10 @@ __device__ __forceinline__ double butterfly(double (&w)[W], int lane) {
 }
 
 // Accumulate a 128 x 128 tile times a vector segment.
-//   NOTRANS: part[r][k] += T[r][c] * vin[c][k]   (per-thread rows, summed over the warp's columns)
-//   TRANS  : colsum[c][k] = sum_r T[r][c] * vin[r][k], the CH columns of a chunk reduced
+//   NOTRANS: part[r][k] += T[r][c] * vin[k][c]   (per-thread rows, summed over the warp's columns)
+//   TRANS  : colsum[k][c] = sum_r T[r][c] * vin[k][r], the CH columns of a chunk reduced
 //            over the warp together by one butterfly per rhs
+// (staged vectors and column sums are k-major: [k * RB + index])
 // `mask`: 0 none, 1 keep r >= c (lower incl. diagonal), 2 keep r > c.
 template <typename TA, int NR, int CH>
 __device__ __forceinline__ void tile_pass(const TA* T, int ld, int rows_valid, int cols_valid,
@@ -135,7 +136,7 @@ __device__ __forceinline__ void tile_pass(const TA* T, int ld, int rows_valid, i
         const int c = warp * 16 + cb + cc;
 #pragma unroll
         for (int k = 0; k < NR; ++k) {
-          const double xc = vin_cols[c * NR + k];
+          const double xc = vin_cols[k * RB + c];
 #pragma unroll
           for (int r = 0; r < 4; ++r) {
             const bool keep = mask_nt == 0 || (mask_nt == 1 ? (rloc + r >= c) : (rloc + r > c));
@@ -148,6 +149,10 @@ __device__ __forceinline__ void tile_pass(const TA* T, int ld, int rows_valid, i
       // one rhs at a time (bounded register pressure for NR > 2)
 #pragma unroll 1
       for (int k = 0; k < NR; ++k) {
+        // this lane's four rows of the rhs, read once (two 16-byte loads)
+        const double2 x01 = *reinterpret_cast<const double2*>(vin_rows + k * RB + rloc);
+        const double2 x23 = *reinterpret_cast<const double2*>(vin_rows + k * RB + rloc + 2);
+        const double xr[4] = {x01.x, x01.y, x23.x, x23.y};
         double w[CH];
 #pragma unroll
         for (int cc = 0; cc < CH; ++cc) {
@@ -156,13 +161,13 @@ __device__ __forceinline__ void tile_pass(const TA* T, int ld, int rows_valid, i
 #pragma unroll
           for (int r = 0; r < 4; ++r) {
             const bool keep = mask_t == 0 || (mask_t == 1 ? (rloc + r >= c) : (rloc + r > c));
-            if (keep) sacc = fma((double)v[cc][r], vin_rows[(rloc + r) * NR + k], sacc);
+            if (keep) sacc = fma((double)v[cc][r], xr[r], sacc);
           }
           w[cc] = sacc;
         }
         const double sum = butterfly<CH>(w, lane);
         if ((lane & LOWBITS) == 0)
-          colsum_smem[(warp * 16 + cb + col_of_lane<CH>(lane)) * NR + k] = sum;
+          colsum_smem[k * RB + warp * 16 + cb + col_of_lane<CH>(lane)] = sum;
       }
     }
   }
@@ -177,14 +182,14 @@ __device__ __forceinline__ void flush_rows(double (&acc)[4][NR], double* red, do
 #pragma unroll
   for (int r = 0; r < 4; ++r)
 #pragma unroll
-    for (int k = 0; k < NR; ++k) red[(warp * RB + 4 * lane + r) * NR + k] = acc[r][k];
+    for (int k = 0; k < NR; ++k) red[(warp * NR + k) * RB + 4 * lane + r] = acc[r][k];
   __syncthreads();
   for (int e = threadIdx.x; e < RB * NR; e += NTH) {
-    const int r = e / NR, k = e % NR;
+    const int k = e / RB, r = e % RB;
     if (r < nvalid) {
       double s = 0.0;
 #pragma unroll
-      for (int w = 0; w < NTH / 32; ++w) s += red[(w * RB + r) * NR + k];
+      for (int w = 0; w < NTH / 32; ++w) s += red[(w * NR + k) * RB + r];
       atomicAdd(&out[(size_t)k * n + row0 + r], sign * s);
     }
   }
@@ -195,8 +200,9 @@ __device__ __forceinline__ void flush_rows(double (&acc)[4][NR], double* red, do
 // lines of the same arrays in L1.
 template <int NR>
 __device__ __forceinline__ void load_vec(const double* x, int n, int row0, int nvalid, double* s) {
+  // k-major in shared memory (s[k * RB + r]): a lane's rows are contiguous
   for (int e = threadIdx.x; e < RB * NR; e += NTH) {
-    const int r = e / NR, k = e % NR;
+    const int k = e / RB, r = e % RB;
     s[e] = (r < nvalid) ? __ldcg(x + (size_t)k * n + row0 + r) : 0.0;
   }
 }
@@ -218,8 +224,8 @@ __device__ __forceinline__ void
 symv_body(const TA* __restrict__ A, int lda, int n, const double* __restrict__ x,
             double* __restrict__ y, const int* skip, uint3 bid) {
   if (skip != nullptr && *skip) return;
-  __shared__ double s_xJ[RB * NR];
-  __shared__ double s_xI[RB * NR];
+  __shared__ __align__(16) double s_xJ[RB * NR];
+  __shared__ __align__(16) double s_xI[RB * NR];
   __shared__ double s_col[RB * NR];
   extern __shared__ double s_red[];
   int I, J;
@@ -236,7 +242,7 @@ symv_body(const TA* __restrict__ A, int lda, int n, const double* __restrict__ x
   __syncthreads();
   // column sums go to y_J
   for (int e = threadIdx.x; e < RB * NR; e += NTH) {
-    const int c = e / NR, k = e % NR;
+    const int k = e / RB, c = e % RB;
     if (c < nj) atomicAdd(&y[(size_t)k * n + j0 + c], s_col[e]);
   }
   flush_rows<NR>(acc, s_red, y, n, i0, ni, 1.0);
@@ -470,7 +476,7 @@ __device__ __forceinline__ void
 trmv_super_body(const float* __restrict__ W, int n, int s0, int rs, const double* __restrict__ in,
                   double* __restrict__ out, const int* skip, uint3 bid) {
   if (skip != nullptr && *skip) return;
-  __shared__ double s_v[RB * NR];
+  __shared__ __align__(16) double s_v[RB * NR];
   __shared__ double s_col[RB * NR];
   extern __shared__ double s_red[];
   int i, j;
@@ -488,7 +494,7 @@ trmv_super_body(const float* __restrict__ W, int n, int s0, int rs, const double
     flush_rows<NR>(acc, s_red, out, n, ri0, ni, 1.0);
   } else {
     for (int e = threadIdx.x; e < RB * NR; e += NTH) {
-      const int c = e / NR, k = e % NR;
+      const int k = e / RB, c = e % RB;
       if (c < nj) atomicAdd(&out[(size_t)k * n + rj0 + c], s_col[e]);
     }
   }
@@ -509,7 +515,7 @@ __device__ __forceinline__ void
 panel_body(const float* __restrict__ L, int ldl, int n, int s0, int rs,
              const double* __restrict__ v, double* __restrict__ w, const int* skip, uint3 bid) {
   if (skip != nullptr && *skip) return;
-  __shared__ double s_v[RB * NR];
+  __shared__ __align__(16) double s_v[RB * NR];
   __shared__ double s_col[RB * NR];
   extern __shared__ double s_red[];
   int r0, c0, nr_, nc_;
@@ -531,7 +537,7 @@ panel_body(const float* __restrict__ L, int ldl, int n, int s0, int rs,
     flush_rows<NR>(acc, s_red, w, n, r0, nr_, -1.0);
   } else {
     for (int e = threadIdx.x; e < RB * NR; e += NTH) {
-      const int c = e / NR, k = e % NR;
+      const int k = e / RB, c = e % RB;
       if (c < nc_) atomicAdd(&w[(size_t)k * n + c0 + c], -s_col[e]);
     }
   }
