@@ -145,6 +145,12 @@ struct mpchol_factor {
   double* h_scal = nullptr;   // pinned
   PcgGraph graph;             // captured iteration pair (see run_pcg)
   cudaStream_t capture_stream = nullptr;   // private stream used only to capture graphs
+  // look-ahead: the bulk of each step's trailing update runs on aux while
+  // the next diagonal block is factored on the caller's stream
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ev_next = nullptr;   // the next block's columns are updated
+  cudaEvent_t ev_rest = nullptr;   // the rest of the step's update is done
+  int nsm = 0;
   CUtensorMap tmap32;         // TMA map over A, 32 x 32 boxes
   CUtensorMap tmapX;          // TMA map over A, 64 x b boxes (panel slabs)
 };
@@ -189,6 +195,9 @@ void free_factor(mpchol_factor_t* f) {
     if (p) cudaFree(p);
   if (f->graph.exec) cudaGraphExecDestroy(f->graph.exec);
   if (f->capture_stream) cudaStreamDestroy(f->capture_stream);
+  if (f->aux) cudaStreamDestroy(f->aux);
+  if (f->ev_next) cudaEventDestroy(f->ev_next);
+  if (f->ev_rest) cudaEventDestroy(f->ev_rest);
   if (f->h_done) cudaFreeHost(f->h_done);
   if (f->h_scal) cudaFreeHost(f->h_scal);
   delete f;
@@ -205,35 +214,88 @@ DecisionParams make_dp(const mpchol_opts& o) {
   return dp;
 }
 
-// One factorization of f->A in place, on `stream`.
+// One factorization of f->A in place, on `stream`, right-looking with a
+// look-ahead of one block.  Step k: the panel solve (with the step decision
+// and the panel quantization), then the trailing update of the tile columns
+// that hold block k+1 (SEL_NEXT), then -- on the caller's stream -- the
+// POTRF of block k+1, while the rest of step k's update runs on the aux
+// stream on all SMs but one.  The panel solve of step k+1 waits for that
+// rest.  Every C tile receives the same updates in the same order as
+// without the split, so the factor is unchanged by it.
 mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream) {
   const mpchol_opts& o = f->opts;
   const int n = f->n, ld = f->ld, b = f->b;
   PotrfParams pp{o.diag_pert, o.pert, o.pivot_floor};
   const DecisionParams dp = make_dp(o);
+  if (f->aux == nullptr) {
+    MPCHOL_CUDA_TRY(cudaStreamCreateWithFlags(&f->aux, cudaStreamNonBlocking));
+    MPCHOL_CUDA_TRY(cudaEventCreateWithFlags(&f->ev_next, cudaEventDisableTiming));
+    MPCHOL_CUDA_TRY(cudaEventCreateWithFlags(&f->ev_rest, cudaEventDisableTiming));
+    MPCHOL_CUDA_TRY(cudaDeviceGetAttribute(&f->nsm, cudaDevAttrMultiProcessorCount, f->device));
+  }
+  const int cap = f->nsm > 1 ? f->nsm - 1 : 1;   // SMs for the concurrent part of the update
   MPCHOL_CUDA_TRY(cudaMemsetAsync(f->status, 0, sizeof(DevStatus), stream));
   MPCHOL_CUDA_TRY(cudaMemsetAsync(f->steps, 0, sizeof(StepState) * (f->nsteps + 1), stream));
   MPCHOL_CUDA_TRY(cudaMemsetAsync(f->sh, 0, sizeof(float) * n, stream));
   PHASE(MPCHOL_PH_SETUP, 1, stream, launch_extract_diag(f->A, ld, n, f->d, f->dtilde, stream));
   const bool fixed = o.precision != MPCHOL_PREC_SWITCHING;
-  std::vector<int> tc_fmts;
+  unsigned tc_mask = 0;   // tensor-core formats a switching step may pick
   bool f32_possible = fixed || o.switch_mode == 1 || o.ladder_len == 0;
   if (!fixed) {
-    if (o.switch_mode == 1) tc_fmts = {FP16, E4M3};
+    if (o.switch_mode == 1) tc_mask = (1u << FP16) | (1u << E4M3);
     else
       for (int i = 0; i < o.ladder_len; ++i) {
-        if (o.ladder[i] != FP32) tc_fmts.push_back(o.ladder[i]);
+        if (o.ladder[i] != FP32) tc_mask |= 1u << o.ladder[i];
         else f32_possible = true;
       }
   }
+  auto potrf = [&](int k) -> mpchol_status {
+    const int s = k * b;
+    PHASE(MPCHOL_PH_POTRF, o.floor > 0.0f ? 2 : 1, stream,
+          launch_potrf(f->tmap32, f->A, ld, n, s, std::min(b, n - s), f->d, f->sh, pp,
+                       &f->steps[k].fp64_diag, f->scratch64, f->winv, f->status, o.floor > 0.0f,
+                       stream));
+    return MPCHOL_OK;
+  };
+  // step k's trailing update over the tiles `sel` picks, on stream `ss`
+  auto syrk = [&](int k, TileSel sel, int max_sms, cudaStream_t ss) -> mpchol_status {
+    const int s = k * b;
+    const int bs = std::min(b, n - s);
+    const int m = n - s - bs;
+    float* P = f->A + (size_t)s * ld + s + bs;
+    float* C = f->A + (size_t)(s + bs) * ld + s + bs;
+    if (fixed) {
+      if (o.precision == FP32)
+        PHASE(MPCHOL_PH_SYRK_F32, 1, ss,
+              launch_syrk_f32(C, ld, m, bs, P, ld, nullptr, f->status, ss, sel, max_sms));
+      else
+        PHASE(MPCHOL_PH_SYRK_TC, 1, ss,
+              launch_syrk_tc(C, ld, m, bs, o.precision, f->q, bs, f->rowexp, f->mxexp, bs / 32,
+                             nullptr, f->status, ss, sel, max_sms));
+      return MPCHOL_OK;
+    }
+    const int* pick = &f->steps[k].prec;
+    if (f32_possible)
+      PHASE(MPCHOL_PH_SYRK_F32, 1, ss,
+            launch_syrk_f32(C, ld, m, bs, P, ld, pick, f->status, ss, sel, max_sms));
+    if (tc_mask != 0)
+      PHASE(MPCHOL_PH_SYRK_TC, 1, ss,
+            launch_syrk_tc_dispatch(C, ld, m, bs, tc_mask, f->q, bs, f->rowexp, f->mxexp, bs / 32,
+                                    pick, f->status, ss, sel, max_sms));
+    return MPCHOL_OK;
+  };
+  mpchol_status rs = potrf(0);
+  if (rs != MPCHOL_OK) return rs;
+  bool rest_pending = false;
   for (int k = 0; k < f->nsteps; ++k) {
     const int s = k * b;
     const int bs = std::min(b, n - s);
     const int m = n - s - bs;
-    PHASE(MPCHOL_PH_POTRF, o.floor > 0.0f ? 2 : 1, stream,
-          launch_potrf(f->tmap32, f->A, ld, n, s, bs, f->d, f->sh, pp, &f->steps[k].fp64_diag,
-                       f->scratch64, f->winv, f->status, o.floor > 0.0f, stream));
     if (m <= 0) break;
+    if (rest_pending) {
+      MPCHOL_CUDA_TRY(cudaStreamWaitEvent(stream, f->ev_rest, 0));
+      rest_pending = false;
+    }
     const int next_bs = std::min(b, m);
     // panel solve, step decision and panel quantization in one launch
     const QuantOut qo{f->q, bs, f->rowexp, f->mxexp, bs / 32, o.diag_pert ? f->sh + s + bs : nullptr};
@@ -241,23 +303,18 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream) {
           launch_trsm_panel(f->tmapX, f->tmap32, f->A, ld, n, s, bs, f->winv, f->d, f->dtilde,
                             f->rowsq, &f->steps[k], &f->steps[k + 1], next_bs, dp, qo, f->status,
                             stream));
-    float* P = f->A + (size_t)s * ld + s + bs;
-    float* C = f->A + (size_t)(s + bs) * ld + s + bs;
-    if (fixed) {
-      if (o.precision == FP32)
-        PHASE(MPCHOL_PH_SYRK_F32, 1, stream, launch_syrk_f32(C, ld, m, bs, P, ld, nullptr, f->status, stream));
-      else
-        PHASE(MPCHOL_PH_SYRK_TC, 1, stream, launch_syrk_tc(C, ld, m, bs, o.precision, f->q, bs, f->rowexp, f->mxexp,
-                                       bs / 32, nullptr, f->status, stream));
-    } else {
-      const int* sel = &f->steps[k].prec;
-      if (f32_possible)
-        PHASE(MPCHOL_PH_SYRK_F32, 1, stream, launch_syrk_f32(C, ld, m, bs, P, ld, sel, f->status, stream));
-      for (int fmt : tc_fmts)
-        PHASE(MPCHOL_PH_SYRK_TC, 1, stream, launch_syrk_tc(C, ld, m, bs, fmt, f->q, bs, f->rowexp, f->mxexp, bs / 32,
-                                       sel, f->status, stream));
+    const int jc = ceil_div(next_bs, 128);   // 128-tile columns of block k+1
+    if ((rs = syrk(k, TileSel{SEL_NEXT, jc}, 0, stream)) != MPCHOL_OK) return rs;
+    if (ceil_div(m, 128) > jc) {
+      MPCHOL_CUDA_TRY(cudaEventRecord(f->ev_next, stream));
+      MPCHOL_CUDA_TRY(cudaStreamWaitEvent(f->aux, f->ev_next, 0));
+      if ((rs = syrk(k, TileSel{SEL_REST, jc}, cap, f->aux)) != MPCHOL_OK) return rs;
+      MPCHOL_CUDA_TRY(cudaEventRecord(f->ev_rest, f->aux));
+      rest_pending = true;
     }
+    if ((rs = potrf(k + 1)) != MPCHOL_OK) return rs;
   }
+  if (rest_pending) MPCHOL_CUDA_TRY(cudaStreamWaitEvent(stream, f->ev_rest, 0));
   f->solve_ready = false;
   return MPCHOL_OK;
 }

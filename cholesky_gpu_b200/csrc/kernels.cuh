@@ -76,17 +76,73 @@ cudaError_t launch_quantize_hash(unsigned long long first, unsigned long long co
                                  cudaStream_t stream);
 
 // ---- trailing update ----------------------------------------------------
-// FP32 SIMT SYRK: C(m x m, lower) -= P P^T, P = m x k column-major (ldp).
-// Skips (returns immediately on device) unless *prec_sel == FP32 when
-// prec_sel is non-null.
+// Which lower 128 x 128 tiles (I >= J) of the trailing block C a launch
+// updates: all of them, only the tile columns J < jc that hold the next
+// diagonal block and its panel (SEL_NEXT), or the rest, J >= jc (SEL_REST).
+// Splitting a step's update this way lets the next diagonal block be factored
+// while the rest of the update runs (look-ahead).
+enum TileSelMode { SEL_ALL = 0, SEL_NEXT = 1, SEL_REST = 2 };
+struct TileSel {
+  int mode;
+  int jc;
+};
+constexpr TileSel kAllTiles{SEL_ALL, 0};
+
+__host__ __device__ inline int sel_tile_count(int T, TileSel s) {
+  if (s.mode == SEL_NEXT) {
+    int c = 0;
+    for (int j = 0; j < s.jc && j < T; ++j) c += T - j;
+    return c;
+  }
+  if (s.mode == SEL_REST) {
+    const int r = T - s.jc;
+    return r > 0 ? r * (r + 1) / 2 : 0;
+  }
+  return T * (T + 1) / 2;
+}
+
+// Tile t of the selection -> (I, J).  SEL_NEXT runs down tile column 0, then
+// column 1, ...; the others run along the rows of the lower triangle.
+__device__ __forceinline__ void sel_tile(int t, TileSel s, int T, int& I, int& J) {
+  if (s.mode == SEL_NEXT) {
+    int j = 0;
+    while (t >= T - j) { t -= T - j; ++j; }
+    J = j;
+    I = j + t;
+    return;
+  }
+  int i = (int)((sqrtf(8.0f * t + 1.0f) - 1.0f) * 0.5f);
+  while (i * (i + 1) / 2 > t) --i;
+  while ((i + 1) * (i + 2) / 2 <= t) ++i;
+  I = i;
+  J = t - i * (i + 1) / 2;
+  if (s.mode == SEL_REST) { I += s.jc; J += s.jc; }
+}
+
+// FP32 SIMT SYRK: C(m x m, lower) -= P P^T, P = m x k column-major (ldp),
+// over the tiles `sel` picks.  Skips (returns immediately on device) unless
+// *prec_sel == FP32 when prec_sel is non-null.  max_sms > 0: a persistent
+// launch on at most that many SMs (one CTA of two 256-thread tile groups per
+// SM), so the other SMs stay free.
 cudaError_t launch_syrk_f32(float* C, int ldc, int m, int k, const float* P, int ldp,
-                            const int* prec_sel, DevStatus* st, cudaStream_t stream);
-// tcgen05 SYRK from the K-major quantized panel (FP16 / E4M3 / E5M2 / MXFP8).
-struct TcPanel;  // defined in syrk_tc.cu
+                            const int* prec_sel, DevStatus* st, cudaStream_t stream,
+                            TileSel sel = kAllTiles, int max_sms = 0);
+// tcgen05 SYRK from the K-major quantized panel (FP16 / E4M3 / E5M2 / MXFP8 /
+// FP16X2), one format per launch.
 bool syrk_tc_supported(int fmt, int k);
 cudaError_t launch_syrk_tc(float* C, int ldc, int m, int k, int fmt, const void* q, int ldq,
                            const int8_t* rowexp, const uint8_t* mxexp, int ldmx,
-                           const int* prec_sel, DevStatus* st, cudaStream_t stream);
+                           const int* prec_sel, DevStatus* st, cudaStream_t stream,
+                           TileSel sel = kAllTiles, int max_sms = 0);
+// The same with the format read on the device from *prec_sel (the step's
+// resolved precision); fmt_mask (bit f for format f) lists the formats the
+// step may pick.  The launch returns at once when the pick is not among
+// them (FP32 steps go to launch_syrk_f32).  max_sms > 0 caps the grid.
+cudaError_t launch_syrk_tc_dispatch(float* C, int ldc, int m, int k, unsigned fmt_mask,
+                                    const void* q, int ldq, const int8_t* rowexp,
+                                    const uint8_t* mxexp, int ldmx, const int* prec_sel,
+                                    DevStatus* st, cudaStream_t stream, TileSel sel = kAllTiles,
+                                    int max_sms = 0);
 
 // ---- batched factorization and solve of many independent systems --------
 // Systems are ordered by decreasing n, so the systems still active at a

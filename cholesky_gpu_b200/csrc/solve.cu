@@ -218,6 +218,192 @@ __device__ __forceinline__ void tri_of(int t, int& i, int& j) {
 template <typename TA> struct ChunkOf { static constexpr int value = 16; };
 template <> struct ChunkOf<double> { static constexpr int value = 8; };
 
+// ---- tiles staged in shared memory -------------------------------------------
+// The streaming kernels (SYMV, the persistent triangular solve) copy each
+// 128 x 128 FP32 tile into shared memory with cp.async, one or two tiles
+// ahead of its use: the copies hold no registers, so an SM keeps 128-192 KB
+// of HBM reads in flight while it computes on the current tile.
+constexpr int TILE_ELEMS = RB * RB;   // 64 KB of FP32
+constexpr int SCH = 8;                // columns per widened chunk
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, int src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(
+                   (uint32_t)__cvta_generic_to_shared(dst)),
+               "l"(src), "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src, int src_bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(
+                   (uint32_t)__cvta_generic_to_shared(dst)),
+               "l"(src), "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Copy the rows_valid x cols_valid tile at T (column-major, leading dimension
+// ld; T and ld keep 16-byte alignment) into a dense 128 x 128 column-major
+// tile; everything outside the valid part is zero-filled by the copies.
+// A warp copies one 512-byte column per instruction.
+__device__ __forceinline__ void stage_tile(float* dst, const float* T, int ld, int rows_valid,
+                                           int cols_valid) {
+#pragma unroll 4
+  for (int e = threadIdx.x; e < TILE_ELEMS / 4; e += NTH) {
+    const int c = e / (RB / 4), r = 4 * (e % (RB / 4));
+    const bool ok = c < cols_valid && r < rows_valid;
+    cp_async16(dst + c * RB + r, ok ? T + (size_t)c * ld + r : T, ok ? 4 * min(4, rows_valid - r) : 0);
+  }
+}
+
+// x[k * n + row0 + r] -> s[k * RB + r], zero for r >= nvalid (8-byte copies:
+// n may be odd)
+template <int NR>
+__device__ __forceinline__ void stage_vec(const double* x, int n, int row0, int nvalid, double* s) {
+  for (int e = threadIdx.x; e < RB * NR; e += NTH) {
+    const int k = e / RB, r = e % RB;
+    const bool ok = r < nvalid;
+    cp_async8(s + e, ok ? x + (size_t)k * n + row0 + r : x, ok ? 8 : 0);
+  }
+}
+
+// tile_pass on a staged tile.  Each lane widens its 4 x SCH chunk to FP64
+// once and uses it for every rhs of both products.  DIAG: a diagonal tile of
+// a symmetric operator stored lower -- NOTRANS keeps r >= c, TRANS r > c.
+template <int NR, bool DIAG>
+__device__ __forceinline__ void tile_pass_staged(const float* Ts, const double* vin_cols,
+                                                 const double* vin_rows, double (&acc)[4][NR],
+                                                 double* colsum_smem, bool do_nt, bool do_t) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int rloc = 4 * lane;
+  constexpr int LOWBITS = 3;   // lanes holding the same column sum (SCH = 8)
+#pragma unroll
+  for (int cb = 0; cb < 16; cb += SCH) {
+    double dv[SCH][4];
+#pragma unroll
+    for (int cc = 0; cc < SCH; ++cc) {
+      const int c = warp * 16 + cb + cc;
+      const float4 f = *reinterpret_cast<const float4*>(Ts + c * RB + rloc);
+      dv[cc][0] = f.x; dv[cc][1] = f.y; dv[cc][2] = f.z; dv[cc][3] = f.w;
+      if (DIAG) {
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+          if (rloc + r < c) dv[cc][r] = 0.0;
+      }
+    }
+    if (do_nt) {
+#pragma unroll
+      for (int cc = 0; cc < SCH; cc += 2) {
+        const int c = warp * 16 + cb + cc;
+#pragma unroll
+        for (int k = 0; k < NR; ++k) {
+          const double2 xc = *reinterpret_cast<const double2*>(vin_cols + k * RB + c);
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            acc[r][k] = fma(dv[cc][r], xc.x, acc[r][k]);
+            acc[r][k] = fma(dv[cc + 1][r], xc.y, acc[r][k]);
+          }
+        }
+      }
+    }
+    if (do_t) {
+#pragma unroll 1
+      for (int k = 0; k < NR; ++k) {
+        const double2 x01 = *reinterpret_cast<const double2*>(vin_rows + k * RB + rloc);
+        const double2 x23 = *reinterpret_cast<const double2*>(vin_rows + k * RB + rloc + 2);
+        const double xr[4] = {x01.x, x01.y, x23.x, x23.y};
+        double w[SCH];
+#pragma unroll
+        for (int cc = 0; cc < SCH; ++cc) {
+          const int c = warp * 16 + cb + cc;
+          double sacc = 0.0;
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            const double a = (DIAG && rloc + r == c) ? 0.0 : dv[cc][r];
+            sacc = fma(a, xr[r], sacc);
+          }
+          w[cc] = sacc;
+        }
+        const double sum = butterfly<SCH>(w, lane);
+        if ((lane & LOWBITS) == 0)
+          colsum_smem[k * RB + warp * 16 + cb + col_of_lane<SCH>(lane)] = sum;
+      }
+    }
+  }
+}
+
+// Shared memory of the staged SYMV: STAGES x (tile + x_J + x_I) + column sums.
+template <int NR>
+constexpr int symv_stages() { return NR >= 8 ? 2 : 3; }
+template <int NR>
+constexpr size_t symv_staged_smem() {
+  return (size_t)symv_stages<NR>() * (TILE_ELEMS * sizeof(float) + 2 * RB * NR * sizeof(double)) +
+         (size_t)RB * NR * sizeof(double);
+}
+
+// ---- y += A x, FP32 symmetric A (lower triangle), persistent over the tiles.
+// CTA b takes tiles b, b + grid, ...; each tile is staged symv_stages - 1
+// tiles ahead together with its two vector segments.  The row partials are
+// reduced in the stage's own tile buffer once the tile has been used.
+template <int NR>
+__global__ void __launch_bounds__(NTH, 1)
+symv_staged_kernel(const float* __restrict__ A, int lda, int n, const double* __restrict__ x,
+                   double* __restrict__ y, const int* skip) {
+  if (skip != nullptr && *skip) return;
+  constexpr int STAGES = symv_stages<NR>();
+  constexpr int VEC = RB * NR;
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  float* tiles = reinterpret_cast<float*>(sm_raw);
+  double* vecs = reinterpret_cast<double*>(tiles + STAGES * TILE_ELEMS);   // [stage][xJ, xI]
+  double* s_col = vecs + STAGES * 2 * VEC;
+  const int T = ceil_div(n, RB);
+  const int ntiles = T * (T + 1) / 2;
+  auto issue = [&](int t, int stage) {
+    int I, J;
+    tri_of(t, I, J);
+    const int i0 = I * RB, j0 = J * RB;
+    const int ni = min(RB, n - i0), nj = min(RB, n - j0);
+    stage_tile(tiles + stage * TILE_ELEMS, A + (size_t)j0 * lda + i0, lda, ni, nj);
+    stage_vec<NR>(x, n, j0, nj, vecs + (2 * stage) * VEC);
+    stage_vec<NR>(x, n, i0, ni, vecs + (2 * stage + 1) * VEC);
+  };
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; ++s) {
+    const int t = blockIdx.x + s * gridDim.x;
+    if (t < ntiles) issue(t, s);
+    cp_async_commit();
+  }
+  int stage = 0;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    {
+      const int tn = t + (STAGES - 1) * gridDim.x;
+      if (tn < ntiles) issue(tn, (stage + STAGES - 1) % STAGES);
+      cp_async_commit();
+    }
+    cp_async_wait<STAGES - 1>();
+    __syncthreads();
+    int I, J;
+    tri_of(t, I, J);
+    const int i0 = I * RB, j0 = J * RB;
+    const int ni = min(RB, n - i0), nj = min(RB, n - j0);
+    float* Ts = tiles + stage * TILE_ELEMS;
+    const double* xJ = vecs + (2 * stage) * VEC;
+    const double* xI = xJ + VEC;
+    double acc[4][NR] = {};
+    if (I == J) tile_pass_staged<NR, true>(Ts, xJ, xI, acc, s_col, true, true);
+    else tile_pass_staged<NR, false>(Ts, xJ, xI, acc, s_col, true, true);
+    __syncthreads();
+    for (int e = threadIdx.x; e < VEC; e += NTH) {
+      const int k = e / RB, c = e % RB;
+      if (c < nj) atomicAdd(&y[(size_t)k * n + j0 + c], s_col[e]);
+    }
+    flush_rows<NR>(acc, reinterpret_cast<double*>(Ts), y, n, i0, ni, 1.0);
+    __syncthreads();   // the stage and s_col are free again
+    stage = (stage + 1) % STAGES;
+  }
+  cp_async_wait<0>();
+}
+
 // ---- y += A x, symmetric A, lower triangle only (one CTA per lower tile) ----
 template <typename TA, int NR>
 __device__ __forceinline__ void
@@ -587,72 +773,160 @@ __device__ __forceinline__ void signal_count(int* ctr) {
   if (threadIdx.x == 0) atomicAdd(ctr, 1);
 }
 
+// One unit of the solve: a tile, the vector segment it reads, where its
+// result goes and the counters it waits on and signals.
+struct TrsvJob {
+  const float* T;       // tile origin (column-major)
+  int ld, nrow, ncol;   // leading dimension, valid rows / columns
+  int vin_row0, vin_n;  // input segment (of out for panels, of work for TRMV)
+  int out_row0, out_n;  // output segment
+  bool nt;              // NOTRANS (row sums) or TRANS (column sums)
+  bool panel;           // L panel tile (reads out, writes work) or W_S tile
+  const int* wait_ctr;
+  int wait_need;
+  int* sig_ctr;
+};
+
+// Decode unit u in the topological order (per super-step: the TRMV tiles,
+// then the panel tiles); returns false past the last unit.
+template <bool TRANS>
+__device__ __forceinline__ bool trsv_job(int u, const float* L, int ldl, int n, const float* wsup,
+                                         int* seg_in, int* seg_out, TrsvJob& jb) {
+  const int ntiles = ceil_div(n, RB);
+  const int NS = ceil_div(n, RS);
+  for (int t = 0; t < NS; ++t) {
+    const int S = TRANS ? NS - 1 - t : t;
+    const int s0 = S * RS;
+    const int rs = min(RS, n - s0);
+    const int nsub = ceil_div(rs, RB);
+    const int g0 = s0 / RB;                 // first global segment of S
+    const int ntr = nsub * (nsub + 1) / 2;
+    const int span = TRANS ? g0 : ceil_div(n - s0 - rs, RB);
+    const int npan = span * nsub;
+    if (u < ntr) {
+      int i, j;
+      tri_of(u, i, j);
+      const int ri0 = s0 + i * RB, rj0 = s0 + j * RB;
+      jb.T = wsup + (size_t)S * RS * RS + (size_t)(j * RB) * RS + i * RB;
+      jb.ld = RS;
+      jb.nrow = min(RB, s0 + rs - ri0);
+      jb.ncol = min(RB, s0 + rs - rj0);
+      jb.panel = false;
+      if (!TRANS) {
+        // y_S(i) += W(i,j) w_S(j): w_S(j) has all g0 panel contributions
+        jb.nt = true;
+        jb.vin_row0 = rj0; jb.vin_n = jb.ncol;
+        jb.out_row0 = ri0; jb.out_n = jb.nrow;
+        jb.wait_ctr = seg_in + g0 + j; jb.wait_need = g0;
+        jb.sig_ctr = seg_out + g0 + i;
+      } else {
+        // z_S(j) += W(i,j)^T w_S(i): w_S(i) has the contributions of every
+        // segment below S
+        jb.nt = false;
+        jb.vin_row0 = ri0; jb.vin_n = jb.nrow;
+        jb.out_row0 = rj0; jb.out_n = jb.ncol;
+        jb.wait_ctr = seg_in + g0 + i; jb.wait_need = ntiles - g0 - nsub;
+        jb.sig_ctr = seg_out + g0 + j;
+      }
+      return true;
+    }
+    if (u < ntr + npan) {
+      const int p = u - ntr;
+      jb.panel = true;
+      jb.ld = ldl;
+      if (!TRANS) {
+        // w(row segment r below S) -= L(r, S col c) y_S(c); rows nearest S first
+        const int r = p / nsub, c = p % nsub;
+        const int r0 = s0 + rs + r * RB, c0 = s0 + c * RB;
+        jb.T = L + (size_t)c0 * ldl + r0;
+        jb.nrow = min(RB, n - r0); jb.ncol = min(RB, s0 + rs - c0);
+        jb.nt = true;
+        jb.vin_row0 = c0; jb.vin_n = jb.ncol;
+        jb.out_row0 = r0; jb.out_n = jb.nrow;
+        jb.wait_ctr = seg_out + g0 + c; jb.wait_need = c + 1;
+        jb.sig_ctr = seg_in + g0 + nsub + r;
+      } else {
+        // w(col segment c left of S) -= L(S row rt, c)^T z_S(rt); columns nearest S first
+        const int c = span - 1 - p / nsub, rt = p % nsub;
+        const int r0 = s0 + rt * RB, c0 = c * RB;
+        jb.T = L + (size_t)c0 * ldl + r0;
+        jb.nrow = min(RB, s0 + rs - r0); jb.ncol = min(RB, s0 - c0);
+        jb.nt = false;
+        jb.vin_row0 = r0; jb.vin_n = jb.nrow;
+        jb.out_row0 = c0; jb.out_n = jb.ncol;
+        jb.wait_ctr = seg_out + g0 + rt; jb.wait_need = nsub - rt;
+        jb.sig_ctr = seg_in + c;
+      }
+      return true;
+    }
+    u -= ntr + npan;
+  }
+  return false;
+}
+
+template <int NR>
+constexpr size_t trsv_staged_smem() {
+  return 2 * (size_t)TILE_ELEMS * sizeof(float) + 2 * (size_t)RB * NR * sizeof(double);
+}
+
+// Units are taken one ahead: the tile of the next unit is copied into the
+// second stage while this unit waits for its input segment and computes.
+// A CTA holds at most two units and finishes the earlier one first; every
+// unit depends only on earlier ones, so the earliest unfinished unit always
+// belongs to a CTA that is working on it, and every wait ends.
 template <int NR, bool TRANS>
-__global__ void __launch_bounds__(NTH)
+__global__ void __launch_bounds__(NTH, 1)
 trsv_persistent_kernel(const float* __restrict__ L, int ldl, int n, const float* __restrict__ wsup,
                        double* __restrict__ work, double* __restrict__ out, int* ctr,
                        const int* skip, DevStatus* st) {
   if (skip != nullptr && *skip) return;
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  float* tiles = reinterpret_cast<float*>(sm_raw);                        // 2 stages
+  double* s_v = reinterpret_cast<double*>(tiles + 2 * TILE_ELEMS);        // RB x NR
+  double* s_col = s_v + RB * NR;                                          // RB x NR
   __shared__ int s_unit;
   int* next = ctr;
   int* seg_in = ctr + 1;
-  const int ntiles = ceil_div(n, RB);
-  int* seg_out = seg_in + ntiles;
-  const int NS = ceil_div(n, RS);
-  for (;;) {
+  int* seg_out = seg_in + ceil_div(n, RB);
+  auto grab = [&]() {
     if (threadIdx.x == 0) s_unit = atomicAdd(next, 1);
     __syncthreads();
-    int u = s_unit;
+    return s_unit;
+  };
+  TrsvJob cur, nxt;
+  int ucur = grab();
+  bool have = trsv_job<TRANS>(ucur, L, ldl, n, wsup, seg_in, seg_out, cur);
+  if (have) stage_tile(tiles, cur.T, cur.ld, cur.nrow, cur.ncol);
+  cp_async_commit();
+  for (int stage = 0; have; stage ^= 1) {
+    const int unxt = grab();
+    const bool have_nxt = trsv_job<TRANS>(unxt, L, ldl, n, wsup, seg_in, seg_out, nxt);
+    if (have_nxt) stage_tile(tiles + (stage ^ 1) * TILE_ELEMS, nxt.T, nxt.ld, nxt.nrow, nxt.ncol);
+    cp_async_commit();
+    wait_count(cur.wait_ctr, cur.wait_need, st, ucur);
+    load_vec<NR>(cur.panel ? out : work, n, cur.vin_row0, cur.vin_n, s_v);
+    cp_async_wait<1>();
     __syncthreads();
-    bool found = false;
-    for (int t = 0; t < NS && !found; ++t) {
-      const int S = TRANS ? NS - 1 - t : t;
-      const int s0 = S * RS;
-      const int rs = min(RS, n - s0);
-      const int nsub = ceil_div(rs, RB);
-      const int g0 = s0 / RB;                 // first global segment of S
-      const int ntr = nsub * (nsub + 1) / 2;
-      const int span = TRANS ? g0 : ceil_div(n - s0 - rs, RB);
-      const int npan = span * nsub;
-      const float* W = wsup + (size_t)S * RS * RS;
-      if (u < ntr) {
-        found = true;
-        int i, j;
-        tri_of(u, i, j);
-        if (!TRANS) {
-          // y_S(i) += W(i,j) w_S(j): w_S(j) has all g0 panel contributions
-          wait_count(seg_in + g0 + j, g0, st, u);
-          trmv_super_body<NR, false>(W, n, s0, rs, work, out, nullptr, make_uint3(u, 0, 0));
-          signal_count(seg_out + g0 + i);
-        } else {
-          // z_S(j) += W(i,j)^T w_S(i): w_S(i) has the contributions of every
-          // segment below S
-          wait_count(seg_in + g0 + i, ntiles - g0 - nsub, st, u);
-          trmv_super_body<NR, true>(W, n, s0, rs, work, out, nullptr, make_uint3(u, 0, 0));
-          signal_count(seg_out + g0 + j);
-        }
-      } else if (u < ntr + npan) {
-        found = true;
-        const int p = u - ntr;
-        if (!TRANS) {
-          // w(row segment r below S) -= L(r, S col c) y_S(c); rows nearest S first
-          const int r = p / nsub, c = p % nsub;
-          wait_count(seg_out + g0 + c, c + 1, st, u);
-          panel_body<NR, false>(L, ldl, n, s0, rs, out, work, nullptr, make_uint3(r, c, 0));
-          signal_count(seg_in + g0 + nsub + r);
-        } else {
-          // w(col segment c left of S) -= L(S row rt, c)^T z_S(rt); columns nearest S first
-          const int c = span - 1 - p / nsub, rt = p % nsub;
-          wait_count(seg_out + g0 + rt, nsub - rt, st, u);
-          panel_body<NR, true>(L, ldl, n, s0, rs, out, work, nullptr, make_uint3(c, rt, 0));
-          signal_count(seg_in + c);
-        }
-      } else {
-        u -= ntr + npan;
+    float* Ts = tiles + stage * TILE_ELEMS;
+    double acc[4][NR] = {};
+    tile_pass_staged<NR, false>(Ts, s_v, s_v, acc, s_col, cur.nt, !cur.nt);
+    __syncthreads();
+    double* dst = cur.panel ? work : out;
+    const double sign = cur.panel ? -1.0 : 1.0;
+    if (cur.nt) {
+      flush_rows<NR>(acc, reinterpret_cast<double*>(Ts), dst, n, cur.out_row0, cur.out_n, sign);
+    } else {
+      for (int e = threadIdx.x; e < RB * NR; e += NTH) {
+        const int k = e / RB, c = e % RB;
+        if (c < cur.out_n) atomicAdd(&dst[(size_t)k * n + cur.out_row0 + c], sign * s_col[e]);
       }
     }
-    if (!found) return;                         // past the last unit
+    signal_count(cur.sig_ctr);   // its barrier also frees this stage, s_v and s_col
+    cur = nxt;
+    ucur = unxt;
+    have = have_nxt;
   }
+  cp_async_wait<0>();
 }
 
 // ---- batched variants: one launch serves every system of a batch --------
@@ -799,8 +1073,9 @@ cudaError_t solve_set_attributes() {
   SET_NR(1) SET_NR(2) SET_NR(4) SET_NR(8)
 #undef SET_NR
 #define SET_NRP(NRC)                                                                              \
-  if ((e = set_dyn(trsv_persistent_kernel<NRC, false>, red_bytes(NRC))) != cudaSuccess) return e; \
-  if ((e = set_dyn(trsv_persistent_kernel<NRC, true>, red_bytes(NRC))) != cudaSuccess) return e;
+  if ((e = set_dyn(trsv_persistent_kernel<NRC, false>, trsv_staged_smem<NRC>())) != cudaSuccess) return e; \
+  if ((e = set_dyn(trsv_persistent_kernel<NRC, true>, trsv_staged_smem<NRC>())) != cudaSuccess) return e; \
+  if ((e = set_dyn(symv_staged_kernel<NRC>, symv_staged_smem<NRC>())) != cudaSuccess) return e;
   SET_NRP(1) SET_NRP(2) SET_NRP(4) SET_NRP(8)
 #undef SET_NRP
   if ((e = set_dyn(block_inverse_batched_kernel, inv)) != cudaSuccess) return e;
@@ -815,13 +1090,33 @@ cudaError_t solve_set_attributes() {
   return cudaSuccess;
 }
 
+int sm_count() {
+  static int cache[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+  int& c = cache[dev & 63];
+  if (c == 0 && cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) c = 148;
+  return c;
+}
+
+// FP32 operators whose columns start on 16-byte boundaries stream through
+// the staged persistent kernel; others (and FP64 operators) take one CTA per
+// tile with register loads.
 template <typename TA>
 cudaError_t launch_symv_skip(const TA* A, int lda, int n, const double* x, double* y, int nrhs,
                              const int* skip, cudaStream_t stream) {
   const long long cnt = (long long)n * nrhs;
   zero_vec_kernel<<<148, 256, 0, stream>>>(y, cnt, skip);
   const int T = ceil_div(n, RB);
-  NR_SWITCH(nrhs, (symv_kernel<TA, NRC><<<T * (T + 1) / 2, NTH, red_bytes(NRC), stream>>>(A, lda, n, x, y, skip)));
+  const int ntiles = T * (T + 1) / 2;
+  const bool staged = sizeof(TA) == 4 && (reinterpret_cast<uintptr_t>(A) & 15) == 0 && lda % 4 == 0;
+  if (staged) {
+    const int grid = std::min(ntiles, sm_count());
+    const float* Af = reinterpret_cast<const float*>(A);
+    NR_SWITCH(nrhs, (symv_staged_kernel<NRC><<<grid, NTH, symv_staged_smem<NRC>(), stream>>>(Af, lda, n, x, y, skip)));
+  } else {
+    NR_SWITCH(nrhs, (symv_kernel<TA, NRC><<<ntiles, NTH, red_bytes(NRC), stream>>>(A, lda, n, x, y, skip)));
+  }
   return cudaGetLastError();
 }
 template cudaError_t launch_symv_skip<float>(const float*, int, int, const double*, double*, int, const int*, cudaStream_t);
@@ -916,11 +1211,12 @@ cudaError_t launch_trsv_persistent(bool backward, const float* L, int ldl, int n
   if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
   const int nri = nrhs == 1 ? 0 : nrhs == 2 ? 1 : nrhs == 4 ? 2 : 3;
   int& grid = grid_cache[dev & 63][backward ? 1 : 0][nri];
+  const size_t smem = 2 * (size_t)TILE_ELEMS * sizeof(float) + 2 * (size_t)RB * nrhs * sizeof(double);
   auto launch = [&](auto kernel) -> cudaError_t {
     if (grid == 0) {
       int per_sm = 0, nsm = 0;
       cudaError_t ee = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, NTH,
-                                                                     red_bytes(nrhs));
+                                                                     smem);
       if (ee == cudaSuccess) ee = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
       if (ee != cudaSuccess) return ee;
       grid = std::max(1, per_sm) * nsm;
@@ -928,7 +1224,7 @@ cudaError_t launch_trsv_persistent(bool backward, const float* L, int ldl, int n
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(NTH);
-    cfg.dynamicSmemBytes = red_bytes(nrhs);
+    cfg.dynamicSmemBytes = smem;
     cfg.stream = stream;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeCooperative;

@@ -5,6 +5,8 @@
 // prototype (src/sChol.cuh:284-306).  Unlike the reference it updates only the
 // lower-triangle tiles (a SYRK, half the flops of the full GEMM it issues).
 // 128 x 128 output tiles, 256 threads, 8 x 8 register tile per thread.
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -13,25 +15,16 @@ namespace {
 
 constexpr int BM = 128, BK = 8, NTH = 256;
 
-__device__ __forceinline__ void tile_of(int t, int& I, int& J) {
-  int i = (int)((sqrtf(8.0f * t + 1.0f) - 1.0f) * 0.5f);
-  while (i * (i + 1) / 2 > t) --i;
-  while ((i + 1) * (i + 2) / 2 <= t) ++i;
-  I = i;
-  J = t - i * (i + 1) / 2;
+__device__ __forceinline__ void group_sync(int group) {
+  // named barrier of one 256-thread tile group (barrier 0 is __syncthreads)
+  asm volatile("bar.sync %0, %1;" ::"r"(group + 1), "r"(NTH) : "memory");
 }
 
-__global__ void __launch_bounds__(NTH)
-syrk_f32_kernel(float* __restrict__ C, int ldc, int m, int k, const float* __restrict__ P, int ldp,
-                const int* prec_sel, DevStatus* st) {
-  if (st != nullptr && st->code != 0) return;
-  if (prec_sel != nullptr && *prec_sel != FP32) return;
-  __shared__ __align__(16) float As[BK][BM];
-  __shared__ __align__(16) float Bs[BK][BM];
-  int I, J;
-  tile_of(blockIdx.x, I, J);
+// One 128 x 128 output tile (I, J) by the 256 threads of a tile group.
+__device__ __forceinline__ void syrk_f32_tile(float* __restrict__ C, int ldc, int m, int k,
+                                              const float* __restrict__ P, int ldp, int I, int J,
+                                              float (*As)[BM], float (*Bs)[BM], int tid, int group) {
   const int i0 = I * BM, j0 = J * BM;
-  const int tid = threadIdx.x;
   const int tx = tid % 16, ty = tid / 16;    // rows follow tx (coalesced C access)
   float acc[8][8];
 #pragma unroll
@@ -48,7 +41,7 @@ syrk_f32_kernel(float* __restrict__ C, int ldc, int m, int k, const float* __res
       As[kk][r] = (ia < m && kc < k) ? P[(size_t)kc * ldp + ia] : 0.0f;
       Bs[kk][r] = (jb < m && kc < k) ? P[(size_t)kc * ldp + jb] : 0.0f;
     }
-    __syncthreads();
+    group_sync(group);
 #pragma unroll
     for (int kk = 0; kk < BK; ++kk) {
       const float4 a0 = *reinterpret_cast<const float4*>(&As[kk][tx * 4]);
@@ -62,7 +55,7 @@ syrk_f32_kernel(float* __restrict__ C, int ldc, int m, int k, const float* __res
 #pragma unroll
         for (int b = 0; b < 8; ++b) acc[a][b] = fmaf(av[a], bv[b], acc[a][b]);
     }
-    __syncthreads();
+    group_sync(group);
   }
 #pragma unroll
   for (int b = 0; b < 8; ++b) {
@@ -76,13 +69,54 @@ syrk_f32_kernel(float* __restrict__ C, int ldc, int m, int k, const float* __res
   }
 }
 
+// One tile per CTA.
+__global__ void __launch_bounds__(NTH)
+syrk_f32_kernel(float* __restrict__ C, int ldc, int m, int k, const float* __restrict__ P, int ldp,
+                const int* prec_sel, DevStatus* st, TileSel sel) {
+  if (st != nullptr && st->code != 0) return;
+  if (prec_sel != nullptr && *prec_sel != FP32) return;
+  __shared__ __align__(16) float As[BK][BM];
+  __shared__ __align__(16) float Bs[BK][BM];
+  int I, J;
+  sel_tile(blockIdx.x, sel, ceil_div(m, BM), I, J);
+  syrk_f32_tile(C, ldc, m, k, P, ldp, I, J, As, Bs, threadIdx.x, 0);
+}
+
+// Persistent: two independent 256-thread tile groups per CTA (one CTA per SM
+// by its register use), each walking the selected tiles with stride
+// 2 * gridDim.x.
+__global__ void __launch_bounds__(2 * NTH, 1)
+syrk_f32_persistent_kernel(float* __restrict__ C, int ldc, int m, int k,
+                           const float* __restrict__ P, int ldp, const int* prec_sel,
+                           DevStatus* st, TileSel sel) {
+  if (st != nullptr && st->code != 0) return;
+  if (prec_sel != nullptr && *prec_sel != FP32) return;
+  __shared__ __align__(16) float As[2][BK][BM];
+  __shared__ __align__(16) float Bs[2][BK][BM];
+  const int group = threadIdx.x / NTH, tid = threadIdx.x % NTH;
+  const int T = ceil_div(m, BM);
+  const int ntiles = sel_tile_count(T, sel);
+  for (int t = 2 * blockIdx.x + group; t < ntiles; t += 2 * gridDim.x) {
+    int I, J;
+    sel_tile(t, sel, T, I, J);
+    syrk_f32_tile(C, ldc, m, k, P, ldp, I, J, As[group], Bs[group], tid, group);
+  }
+}
+
 }  // namespace
 
 cudaError_t launch_syrk_f32(float* C, int ldc, int m, int k, const float* P, int ldp,
-                            const int* prec_sel, DevStatus* st, cudaStream_t stream) {
+                            const int* prec_sel, DevStatus* st, cudaStream_t stream, TileSel sel,
+                            int max_sms) {
   if (m <= 0) return cudaSuccess;
-  const int T = ceil_div(m, BM);
-  syrk_f32_kernel<<<T * (T + 1) / 2, NTH, 0, stream>>>(C, ldc, m, k, P, ldp, prec_sel, st);
+  const int ntiles = sel_tile_count(ceil_div(m, BM), sel);
+  if (ntiles <= 0) return cudaSuccess;
+  if (max_sms > 0) {
+    const int grid = std::min(max_sms, ceil_div(ntiles, 2));
+    syrk_f32_persistent_kernel<<<grid, 2 * NTH, 0, stream>>>(C, ldc, m, k, P, ldp, prec_sel, st, sel);
+  } else {
+    syrk_f32_kernel<<<ntiles, NTH, 0, stream>>>(C, ldc, m, k, P, ldp, prec_sel, st, sel);
+  }
   return cudaGetLastError();
 }
 

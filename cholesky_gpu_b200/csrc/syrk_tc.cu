@@ -27,6 +27,8 @@
 //           with coalesced loads and stores instead).
 // The two TMEM accumulators let the epilogue of one tile overlap the MMAs of
 // the next.  Every mbarrier wait is bounded.
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.cuh"
 #include "tc_ptx.cuh"
@@ -40,14 +42,6 @@ constexpr int CHUNK = 128;                 // bytes of K per row per stage
 constexpr int STRIP = TM * CHUNK;          // 16 KB: one operand strip chunk
 constexpr int EPI_WARPS = 8;               // two per TMEM lane quarter, half the columns each
 constexpr int NTHREADS = 64 + 32 * EPI_WARPS;
-
-__device__ __forceinline__ void tile_of(int t, int& I, int& J) {
-  int i = (int)((sqrtf(8.0f * t + 1.0f) - 1.0f) * 0.5f);
-  while (i * (i + 1) / 2 > t) --i;
-  while ((i + 1) * (i + 2) / 2 <= t) ++i;
-  I = i;
-  J = t - i * (i + 1) / 2;
-}
 
 template <int FMT> struct TcCfg;
 template <> struct TcCfg<FP16> {
@@ -126,10 +120,11 @@ struct TileCtx {
 };
 
 template <bool BATCH>
-__device__ __forceinline__ TileCtx tile_ctx(int t, const TcBatch& bt, float* C, int ldc, int m) {
+__device__ __forceinline__ TileCtx tile_ctx(int t, const TcBatch& bt, float* C, int ldc, int m,
+                                            TileSel sel) {
   TileCtx c;
   if (!BATCH) {
-    tile_of(t, c.I, c.J);
+    sel_tile(t, sel, (m + TM - 1) / TM, c.I, c.J);
     c.C = C; c.ldc = ldc; c.m = m; c.row0 = 0;
     return c;
   }
@@ -140,7 +135,7 @@ __device__ __forceinline__ TileCtx tile_ctx(int t, const TcBatch& bt, float* C, 
   }
   const BatchSys& S = bt.sys[lo];
   const BatchStep& T = bt.steps[lo];
-  tile_of(t - T.tile0, c.I, c.J);
+  sel_tile(t - T.tile0, kAllTiles, (T.m + TM - 1) / TM, c.I, c.J);
   c.C = S.A + (size_t)(bt.s + bt.b) * S.ld + bt.s + bt.b;
   c.ldc = S.ld;
   c.m = T.m;
@@ -148,14 +143,16 @@ __device__ __forceinline__ TileCtx tile_ctx(int t, const TcBatch& bt, float* C, 
   return c;
 }
 
+// The kernel body for one format.  mhi / mlo / mc point at tensor maps in the
+// launch's parameter space (TMA reads them from there).
 template <int FMT, bool BATCH>
-__global__ void __launch_bounds__(NTHREADS, 1)
-syrk_tc_kernel(const __grid_constant__ TcMaps maps, float* __restrict__ C, int ldc, int m, int k,
-               const int8_t* __restrict__ rowexp, const uint8_t* __restrict__ mxexp, int ldmx,
-               const int* prec_sel, DevStatus* st, TcBatch bt, int ntiles_b) {
+__device__ __forceinline__ void
+syrk_tc_body(const CUtensorMap* mhi, const CUtensorMap* mlo, const CUtensorMap* mc,
+             float* __restrict__ C, int ldc, int m, int k, const int8_t* __restrict__ rowexp,
+             const uint8_t* __restrict__ mxexp, int ldmx, DevStatus* st, const TcBatch& bt,
+             int ntiles_b, TileSel sel) {
   using Cfg = TcCfg<FMT>;
   if (st != nullptr && st->code != 0) return;
-  if (prec_sel != nullptr && *prec_sel != FMT) return;
   constexpr int NS = Cfg::NSTAGE;
   constexpr int NSETS = Cfg::NSETS;
   constexpr bool MX = Cfg::MX;
@@ -180,15 +177,15 @@ syrk_tc_kernel(const __grid_constant__ TcMaps maps, float* __restrict__ C, int l
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int T = (m + TM - 1) / TM;
-  const int ntiles = BATCH ? ntiles_b : T * (T + 1) / 2;
+  const int ntiles = BATCH ? ntiles_b : sel_tile_count(T, sel);
   const int nchunks = (k * Cfg::ESIZE) / CHUNK;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < NS; ++s) { tc::mbar_init(&full_bar[s], 1); tc::mbar_init(&empty_bar[s], 1); }
     for (int b = 0; b < 2; ++b) { tc::mbar_init(&accf_bar[b], 1); tc::mbar_init(&acce_bar[b], EPI_WARPS); }
     tc::fence_mbar_init();
-    tc::prefetch_tmap(&maps.hi);
-    if (NSETS == 2) tc::prefetch_tmap(&maps.lo);
+    tc::prefetch_tmap(mhi);
+    if (NSETS == 2) tc::prefetch_tmap(mlo);
     abort_sh = 0;
   }
   if (warp == 1) tc::tmem_alloc(&tmem_base_sh, TMEM_COLS);
@@ -204,7 +201,7 @@ syrk_tc_kernel(const __grid_constant__ TcMaps maps, float* __restrict__ C, int l
     int c = 0;   // global chunk counter
     bool failed = false;
     for (int t = blockIdx.x; t < ntiles && !failed; t += gridDim.x) {
-      const TileCtx tc_ = tile_ctx<BATCH>(t, bt, C, ldc, m);
+      const TileCtx tc_ = tile_ctx<BATCH>(t, bt, C, ldc, m, sel);
       const int I = tc_.I, J = tc_.J;
       const bool diag = (I == J);
       const uint32_t bytes = (uint32_t)((diag ? 1 : 2) * NSETS * STRIP);
@@ -235,12 +232,12 @@ syrk_tc_kernel(const __grid_constant__ TcMaps maps, float* __restrict__ C, int l
           tc::mbar_expect_tx(&full_bar[s], bytes);
           const int x = kc * ELEMS_PER_CHUNK;
           const int yi = tc_.row0 + I * TM, yj = tc_.row0 + J * TM;
-          tc::tma_load_2d(base, &maps.hi, &full_bar[s], x, yi);
-          if (NSETS == 2) tc::tma_load_2d(base + STRIP, &maps.lo, &full_bar[s], x, yi);
+          tc::tma_load_2d(base, mhi, &full_bar[s], x, yi);
+          if (NSETS == 2) tc::tma_load_2d(base + STRIP, mlo, &full_bar[s], x, yi);
           if (!diag) {
-            tc::tma_load_2d(base + NSETS * STRIP, &maps.hi, &full_bar[s], x, yj);
+            tc::tma_load_2d(base + NSETS * STRIP, mhi, &full_bar[s], x, yj);
             if (NSETS == 2)
-              tc::tma_load_2d(base + (NSETS + 1) * STRIP, &maps.lo, &full_bar[s], x, yj);
+              tc::tma_load_2d(base + (NSETS + 1) * STRIP, mlo, &full_bar[s], x, yj);
           }
         }
       }
@@ -250,7 +247,7 @@ syrk_tc_kernel(const __grid_constant__ TcMaps maps, float* __restrict__ C, int l
     if (lane == 0) {
       int c = 0, tcount = 0;
       for (int t = blockIdx.x; t < ntiles && !abort_sh; t += gridDim.x, ++tcount) {
-        const TileCtx tc_ = tile_ctx<BATCH>(t, bt, C, ldc, m);
+        const TileCtx tc_ = tile_ctx<BATCH>(t, bt, C, ldc, m, sel);
         const bool diag = (tc_.I == tc_.J);
         const int buf = tcount & 1;
         const uint32_t use = (uint32_t)(tcount >> 1);
@@ -318,7 +315,7 @@ syrk_tc_kernel(const __grid_constant__ TcMaps maps, float* __restrict__ C, int l
     float* stg = reinterpret_cast<float*>(smem + (size_t)NS * STAGE_BYTES + (size_t)(warp - 2) * STAGE_C);
     int tcount = 0;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++tcount) {
-      const TileCtx tc_ = tile_ctx<BATCH>(t, bt, C, ldc, m);
+      const TileCtx tc_ = tile_ctx<BATCH>(t, bt, C, ldc, m, sel);
       const int I = tc_.I, J = tc_.J;
       float* Ct = tc_.C;
       const int ldct = tc_.ldc, mt = tc_.m;
@@ -361,7 +358,7 @@ syrk_tc_kernel(const __grid_constant__ TcMaps maps, float* __restrict__ C, int l
             tc::fence_proxy_async_smem();
             __syncwarp();
             if (lane == 0) {
-              tc::tma_reduce_add_2d(&maps.c, stg, i0, j0);
+              tc::tma_reduce_add_2d(mc, stg, i0, j0);
               tc::bulk_commit();
             }
           }
@@ -392,29 +389,83 @@ syrk_tc_kernel(const __grid_constant__ TcMaps maps, float* __restrict__ C, int l
 }
 
 template <int FMT, bool BATCH>
+__global__ void __launch_bounds__(NTHREADS, 1)
+syrk_tc_kernel(const __grid_constant__ TcMaps maps, float* __restrict__ C, int ldc, int m, int k,
+               const int8_t* __restrict__ rowexp, const uint8_t* __restrict__ mxexp, int ldmx,
+               const int* prec_sel, DevStatus* st, TcBatch bt, int ntiles_b, TileSel sel) {
+  if (prec_sel != nullptr && *prec_sel != FMT) return;
+  syrk_tc_body<FMT, BATCH>(&maps.hi, &maps.lo, &maps.c, C, ldc, m, k, rowexp, mxexp, ldmx, st, bt,
+                           ntiles_b, sel);
+}
+
+// Maps for every format: 8-bit codes, FP16 hi and lo panels, C.
+struct TcMapsAll {
+  CUtensorMap h8;
+  CUtensorMap h16;
+  CUtensorMap l16;
+  CUtensorMap c;
+};
+
+// One launch whatever the step picked: the format is read on the device.
+__global__ void __launch_bounds__(NTHREADS, 1)
+syrk_tc_dispatch_kernel(const __grid_constant__ TcMapsAll maps, float* __restrict__ C, int ldc,
+                        int m, int k, const int8_t* __restrict__ rowexp,
+                        const uint8_t* __restrict__ mxexp, int ldmx, unsigned fmt_mask,
+                        const int* prec_sel, DevStatus* st, TileSel sel) {
+  const int f = *prec_sel;
+  if (f < 0 || f > 31 || ((fmt_mask >> f) & 1u) == 0) return;
+  const TcBatch nb{};
+  switch (f) {
+    case FP16:
+      syrk_tc_body<FP16, false>(&maps.h16, &maps.l16, &maps.c, C, ldc, m, k, rowexp, mxexp, ldmx, st, nb, 0, sel);
+      break;
+    case FP16X2:
+      syrk_tc_body<FP16X2, false>(&maps.h16, &maps.l16, &maps.c, C, ldc, m, k, rowexp, mxexp, ldmx, st, nb, 0, sel);
+      break;
+    case E4M3:
+      syrk_tc_body<E4M3, false>(&maps.h8, &maps.h8, &maps.c, C, ldc, m, k, rowexp, mxexp, ldmx, st, nb, 0, sel);
+      break;
+    case E5M2:
+      syrk_tc_body<E5M2, false>(&maps.h8, &maps.h8, &maps.c, C, ldc, m, k, rowexp, mxexp, ldmx, st, nb, 0, sel);
+      break;
+    case MXFP8:
+      syrk_tc_body<MXFP8, false>(&maps.h8, &maps.h8, &maps.c, C, ldc, m, k, rowexp, mxexp, ldmx, st, nb, 0, sel);
+      break;
+    default:
+      break;
+  }
+}
+
+template <int FMT, bool BATCH>
 size_t tc_smem() {
   using Cfg = TcCfg<FMT>;
   return (size_t)Cfg::NSTAGE * (2 * Cfg::NSETS * STRIP + (Cfg::MX ? 2 * SF_BYTES : 0)) +
          (BATCH ? 0 : (size_t)EPI_WARPS * STAGE_C) + 1024;
 }
 
-template <int FMT, bool BATCH>
-cudaError_t launch_fmt(const TcMaps& maps, float* C, int ldc, int m, int k, const int8_t* rowexp,
-                       const uint8_t* mxexp, int ldmx, const int* prec_sel, DevStatus* st,
-                       const TcBatch& bt, int ntiles_b, cudaStream_t stream) {
-  const size_t smem = tc_smem<FMT, BATCH>();
-  cudaError_t e = cudaFuncSetAttribute(syrk_tc_kernel<FMT, BATCH>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
+int grid_for(int ntiles, int max_sms) {
   int nsm = 148;
   int dev = 0;
   if (cudaGetDevice(&dev) == cudaSuccess)
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  const int T = ceil_div(m, TM);
-  const int ntiles = BATCH ? ntiles_b : T * (T + 1) / 2;
-  const int grid = ntiles < nsm ? ntiles : nsm;
+  if (max_sms > 0 && max_sms < nsm) nsm = max_sms;
+  return ntiles < nsm ? ntiles : nsm;
+}
+
+template <int FMT, bool BATCH>
+cudaError_t launch_fmt(const TcMaps& maps, float* C, int ldc, int m, int k, const int8_t* rowexp,
+                       const uint8_t* mxexp, int ldmx, const int* prec_sel, DevStatus* st,
+                       const TcBatch& bt, int ntiles_b, cudaStream_t stream,
+                       TileSel sel = kAllTiles, int max_sms = 0) {
+  const size_t smem = tc_smem<FMT, BATCH>();
+  cudaError_t e = cudaFuncSetAttribute(syrk_tc_kernel<FMT, BATCH>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const int ntiles = BATCH ? ntiles_b : sel_tile_count(ceil_div(m, TM), sel);
+  if (ntiles <= 0) return cudaSuccess;
+  const int grid = grid_for(ntiles, max_sms);
   syrk_tc_kernel<FMT, BATCH><<<grid, NTHREADS, smem, stream>>>(maps, C, ldc, m, k, rowexp, mxexp,
-                                                               ldmx, prec_sel, st, bt, ntiles_b);
+                                                               ldmx, prec_sel, st, bt, ntiles_b, sel);
   return cudaGetLastError();
 }
 
@@ -428,7 +479,8 @@ bool syrk_tc_supported(int fmt, int k) {
 
 cudaError_t launch_syrk_tc(float* C, int ldc, int m, int k, int fmt, const void* q, int ldq,
                            const int8_t* rowexp, const uint8_t* mxexp, int ldmx,
-                           const int* prec_sel, DevStatus* st, cudaStream_t stream) {
+                           const int* prec_sel, DevStatus* st, cudaStream_t stream, TileSel sel,
+                           int max_sms) {
   if (m <= 0) return cudaSuccess;
   if (fmt == MXFP8 && (mxexp == nullptr || ldmx < k / 32 ||
                        (reinterpret_cast<uintptr_t>(mxexp) & 3) != 0 || (ldmx & 3) != 0))
@@ -451,13 +503,64 @@ cudaError_t launch_syrk_tc(float* C, int ldc, int m, int k, int fmt, const void*
       return cudaErrorInvalidValue;
   }
   switch (fmt) {
-    case FP16: return launch_fmt<FP16, false>(maps, C, ldc, m, k, rowexp, mxexp, ldmx, prec_sel, st, TcBatch{}, 0, stream);
-    case E4M3: return launch_fmt<E4M3, false>(maps, C, ldc, m, k, rowexp, mxexp, ldmx, prec_sel, st, TcBatch{}, 0, stream);
-    case E5M2: return launch_fmt<E5M2, false>(maps, C, ldc, m, k, rowexp, mxexp, ldmx, prec_sel, st, TcBatch{}, 0, stream);
-    case FP16X2: return launch_fmt<FP16X2, false>(maps, C, ldc, m, k, rowexp, mxexp, ldmx, prec_sel, st, TcBatch{}, 0, stream);
-    case MXFP8: return launch_fmt<MXFP8, false>(maps, C, ldc, m, k, rowexp, mxexp, ldmx, prec_sel, st, TcBatch{}, 0, stream);
+    case FP16: return launch_fmt<FP16, false>(maps, C, ldc, m, k, rowexp, mxexp, ldmx, prec_sel, st, TcBatch{}, 0, stream, sel, max_sms);
+    case E4M3: return launch_fmt<E4M3, false>(maps, C, ldc, m, k, rowexp, mxexp, ldmx, prec_sel, st, TcBatch{}, 0, stream, sel, max_sms);
+    case E5M2: return launch_fmt<E5M2, false>(maps, C, ldc, m, k, rowexp, mxexp, ldmx, prec_sel, st, TcBatch{}, 0, stream, sel, max_sms);
+    case FP16X2: return launch_fmt<FP16X2, false>(maps, C, ldc, m, k, rowexp, mxexp, ldmx, prec_sel, st, TcBatch{}, 0, stream, sel, max_sms);
+    case MXFP8: return launch_fmt<MXFP8, false>(maps, C, ldc, m, k, rowexp, mxexp, ldmx, prec_sel, st, TcBatch{}, 0, stream, sel, max_sms);
     default: return cudaErrorInvalidValue;
   }
+}
+
+cudaError_t launch_syrk_tc_dispatch(float* C, int ldc, int m, int k, unsigned fmt_mask,
+                                    const void* q, int ldq, const int8_t* rowexp,
+                                    const uint8_t* mxexp, int ldmx, const int* prec_sel,
+                                    DevStatus* st, cudaStream_t stream, TileSel sel, int max_sms) {
+  if (m <= 0 || prec_sel == nullptr) return m <= 0 ? cudaSuccess : cudaErrorInvalidValue;
+  const int ntiles = sel_tile_count(ceil_div(m, TM), sel);
+  if (ntiles <= 0) return cudaSuccess;
+  const bool any8 = (fmt_mask & ((1u << E4M3) | (1u << E5M2) | (1u << MXFP8))) != 0;
+  const bool any16 = (fmt_mask & ((1u << FP16) | (1u << FP16X2))) != 0;
+  for (int f : {FP16, E4M3, E5M2, FP16X2, MXFP8})
+    if (((fmt_mask >> f) & 1u) && !syrk_tc_supported(f, k)) return cudaErrorInvalidValue;
+  if (((fmt_mask >> MXFP8) & 1u) &&
+      (mxexp == nullptr || ldmx < k / 32 || (reinterpret_cast<uintptr_t>(mxexp) & 3) != 0 ||
+       (ldmx & 3) != 0))
+    return cudaErrorInvalidValue;
+  TcMapsAll maps;
+  if (!encode_tmap_2d(&maps.c, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, C, (uint64_t)m, (uint64_t)m,
+                      (uint64_t)ldc, 32, 32, CU_TENSOR_MAP_SWIZZLE_NONE))
+    return cudaErrorInvalidValue;
+  maps.h8 = maps.h16 = maps.l16 = maps.c;   // unused slots
+  if (any8 && !encode_tmap_2d(&maps.h8, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, q, (uint64_t)k, (uint64_t)m,
+                              (uint64_t)ldq, CHUNK, TM, CU_TENSOR_MAP_SWIZZLE_128B))
+    return cudaErrorInvalidValue;
+  if (any16) {
+    if (!encode_tmap_2d(&maps.h16, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, q, (uint64_t)k, (uint64_t)m,
+                        (uint64_t)ldq, CHUNK / 2, TM, CU_TENSOR_MAP_SWIZZLE_128B))
+      return cudaErrorInvalidValue;
+    const uint16_t* lo = reinterpret_cast<const uint16_t*>(q) + (size_t)m * ldq;
+    if (!encode_tmap_2d(&maps.l16, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, lo, (uint64_t)k, (uint64_t)m,
+                        (uint64_t)ldq, CHUNK / 2, TM, CU_TENSOR_MAP_SWIZZLE_128B))
+      return cudaErrorInvalidValue;
+  }
+  size_t smem = 0;
+  if ((fmt_mask >> FP16) & 1u) smem = std::max(smem, tc_smem<FP16, false>());
+  if ((fmt_mask >> E4M3) & 1u) smem = std::max(smem, tc_smem<E4M3, false>());
+  if ((fmt_mask >> E5M2) & 1u) smem = std::max(smem, tc_smem<E5M2, false>());
+  if ((fmt_mask >> FP16X2) & 1u) smem = std::max(smem, tc_smem<FP16X2, false>());
+  if ((fmt_mask >> MXFP8) & 1u) smem = std::max(smem, tc_smem<MXFP8, false>());
+  if (smem == 0) return cudaSuccess;
+  const size_t smem_all = std::max({tc_smem<FP16, false>(), tc_smem<E4M3, false>(),
+                                    tc_smem<E5M2, false>(), tc_smem<FP16X2, false>(),
+                                    tc_smem<MXFP8, false>()});
+  cudaError_t e = cudaFuncSetAttribute(syrk_tc_dispatch_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_all);
+  if (e != cudaSuccess) return e;
+  const int grid = grid_for(ntiles, max_sms);
+  syrk_tc_dispatch_kernel<<<grid, NTHREADS, smem, stream>>>(maps, C, ldc, m, k, rowexp, mxexp, ldmx,
+                                                            fmt_mask, prec_sel, st, sel);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_syrk_tc_batched(BatchSys* sys, const BatchStep* steps, int nact, int ntiles,
