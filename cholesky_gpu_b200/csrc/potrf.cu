@@ -27,6 +27,16 @@ constexpr int TSZ = TS * TS;    // elements per dense tile
 
 __device__ __forceinline__ int tidx(int I, int J) { return I * (I + 1) / 2 + J; }
 
+// 16-byte shared-memory vector load of 4 floats or 2 doubles.
+__device__ __forceinline__ void load_vec16(const float* p, float (&v)[4]) {
+  const float4 w = *reinterpret_cast<const float4*>(p);
+  v[0] = w.x; v[1] = w.y; v[2] = w.z; v[3] = w.w;
+}
+__device__ __forceinline__ void load_vec16(const double* p, double (&v)[2]) {
+  const double2 w = *reinterpret_cast<const double2*>(p);
+  v[0] = w.x; v[1] = w.y;
+}
+
 template <typename T>
 __device__ __forceinline__ T drsqrt(T x);
 template <>
@@ -86,27 +96,23 @@ __device__ bool factor_diag_tile(T* t, T* inv, int lane, int nreal, const T* shi
     const T lik = (lane > k) ? a[k] * rk : T(0);
     a[k] = mine ? piv * r : ((lane > k) ? lik : a[k]);
     if (k + 1 < TS) dnext = fma(-lik, lik, a[k + 1]);
-    col[lane] = lik;
+    // two multiplier buffers used in turn: the next column's write cannot
+    // overtake a lane still reading this one, so one warp barrier suffices
+    T* cb = col + (k & 1) * TS;
+    cb[lane] = lik;
     __syncwarp();
     constexpr int V = 16 / sizeof(T);
 #pragma unroll
     for (int q = 0; q < TS / V; ++q) {
       if (V * q + V - 1 <= k) continue;
       T l[V];
-      if (V == 4) {
-        const float4 w = *reinterpret_cast<const float4*>(col + V * q);
-        l[0] = w.x; l[1] = w.y; l[2 % V] = w.z; l[3 % V] = w.w;
-      } else {
-        const double2 w = *reinterpret_cast<const double2*>(col + V * q);
-        l[0] = w.x; l[1 % V] = w.y;
-      }
+      load_vec16(cb + V * q, l);
 #pragma unroll
       for (int e = 0; e < V; ++e) {
         const int j = V * q + e;
         if (j > k) a[j] = fma(-lik, l[e], a[j]);
       }
     }
-    __syncwarp();
   }
 #pragma unroll
   for (int j = 0; j < TS; ++j)
@@ -121,39 +127,81 @@ __device__ bool factor_diag_tile(T* t, T* inv, int lane, int nreal, const T* shi
 }
 
 // X L^T = B for one tile (B in x, overwritten); lane i owns row i.
+// Right-looking: once x(i, m) is final it is applied to the later columns,
+// whose multipliers L(m+1.., m) are contiguous in the column-major tile l and
+// arrive as 16-byte broadcasts.
 template <typename T>
 __device__ void trsm_tile(T* x, const T* l, const T* inv, int lane) {
+  constexpr int V = 16 / sizeof(T);
   T b[TS];
 #pragma unroll
   for (int m = 0; m < TS; ++m) b[m] = x[m * TS + lane];
 #pragma unroll
-  for (int j = 0; j < TS; ++j) {
-    T acc = b[j];
+  for (int m = 0; m < TS; ++m) {
+    b[m] *= inv[m];
 #pragma unroll
-    for (int m = 0; m < j; ++m) acc -= b[m] * l[m * TS + j];
-    b[j] = acc * inv[j];
+    for (int q = (m + 1) / V; q < TS / V; ++q) {
+      T lv[V];
+      load_vec16(l + m * TS + V * q, lv);
+#pragma unroll
+      for (int e = 0; e < V; ++e)
+        if (V * q + e > m) b[V * q + e] = fma(-b[m], lv[e], b[V * q + e]);
+    }
   }
 #pragma unroll
   for (int m = 0; m < TS; ++m) x[m * TS + lane] = b[m];
 }
 
-// C -= A B^T for 32 x 32 tiles; lane i owns row i of C and of A.
+// Columns c0..c0+7 of C -= A B^T for 32 x 32 tiles; lane i owns row i of C
+// and holds row i of A in ar.  B's column values arrive as 16-byte
+// broadcasts; with TWO, a second tile of the same tile column
+// (C2 -= A2 B^T, A2's row in ar2) shares every broadcast.
+template <typename T, bool TWO>
+__device__ __forceinline__ void syrk_cols8(T* c, T* c2, const T (&ar)[TS], const T (&ar2)[TS],
+                                           const T* b, int lane, int c0) {
+  constexpr int V = 16 / sizeof(T);
+  T acc[8], acc2[8];
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    acc[u] = c[(c0 + u) * TS + lane];
+    acc2[u] = TWO ? c2[(c0 + u) * TS + lane] : T(0);
+  }
+#pragma unroll
+  for (int m = 0; m < TS; ++m) {
+#pragma unroll
+    for (int q = 0; q < 8 / V; ++q) {
+      T bv[V];
+      load_vec16(b + m * TS + c0 + V * q, bv);
+#pragma unroll
+      for (int e = 0; e < V; ++e) {
+        acc[V * q + e] = fma(-ar[m], bv[e], acc[V * q + e]);
+        if (TWO) acc2[V * q + e] = fma(-ar2[m], bv[e], acc2[V * q + e]);
+      }
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    c[(c0 + u) * TS + lane] = acc[u];
+    if (TWO) c2[(c0 + u) * TS + lane] = acc2[u];
+  }
+}
+
+// C -= A B^T over columns [c_begin, c_end) (multiples of 8), and C2 -= A2 B^T
+// over the same columns when c2 is set.
 template <typename T>
-__device__ void syrk_tile(T* c, const T* a, const T* b, int lane) {
-  T ar[TS];
+__device__ void syrk_tiles(T* c, const T* a, T* c2, const T* a2, const T* b, int lane,
+                           int c_begin = 0, int c_end = TS) {
+  T ar[TS], ar2[TS];
 #pragma unroll
   for (int m = 0; m < TS; ++m) ar[m] = a[m * TS + lane];
+  if (c2 != nullptr) {
+#pragma unroll
+    for (int m = 0; m < TS; ++m) ar2[m] = a2[m * TS + lane];
 #pragma unroll 1
-  for (int c0 = 0; c0 < TS; c0 += 8) {
-    T acc[8];
-#pragma unroll
-    for (int u = 0; u < 8; ++u) acc[u] = c[(c0 + u) * TS + lane];
-#pragma unroll
-    for (int m = 0; m < TS; ++m)
-#pragma unroll
-      for (int u = 0; u < 8; ++u) acc[u] -= ar[m] * b[m * TS + c0 + u];
-#pragma unroll
-    for (int u = 0; u < 8; ++u) c[(c0 + u) * TS + lane] = acc[u];
+    for (int c0 = c_begin; c0 < c_end; c0 += 8) syrk_cols8<T, true>(c, c2, ar, ar2, b, lane, c0);
+  } else {
+#pragma unroll 1
+    for (int c0 = c_begin; c0 < c_end; c0 += 8) syrk_cols8<T, false>(c, nullptr, ar, ar, b, lane, c0);
   }
 }
 
@@ -188,7 +236,7 @@ __device__ void potrf_block(const CUtensorMap* tmap, T* tiles, float* A, int lda
   __shared__ T s_shift[256];
   __shared__ T s_pmin[256];
   __shared__ T s_inv[256];
-  __shared__ __align__(16) T s_col[TS];
+  __shared__ __align__(16) T s_col[2 * TS];
   __shared__ int s_fail, s_pert, s_ok;
   __shared__ __align__(8) uint64_t bar;
   if (tid == 0) { s_fail = -1; s_pert = 0; s_ok = 1; }
@@ -249,10 +297,12 @@ __device__ void potrf_block(const CUtensorMap* tmap, T* tiles, float* A, int lda
     }
   }
   __syncthreads();
-  // Look-ahead: warp 0 owns the diagonal tiles.  At step J it applies column
-  // J to tile (J+1, J+1) -- its last update -- and factors it at once, while
-  // the other warps update the rest of the trailing tiles; so the factor of
-  // the next diagonal tile overlaps the trailing update.
+  // Step J: (A) the tiles below diagonal tile J are solved, one per warp;
+  // (B) warps 0-3 apply column J to diagonal tile J+1 (8 columns each, one
+  // warp per SM sub-partition) and warp 0 factors it at once, while warps
+  // 1.. update the other trailing tiles, two tiles of a tile column at a time
+  // so that each broadcast of column J's values feeds both.  The factor of
+  // the next diagonal tile thus overlaps the trailing update (look-ahead).
   auto factor_tile = [&](int J) {
     int nreal = bs - J * TS;
     nreal = nreal > TS ? TS : nreal;
@@ -273,22 +323,27 @@ __device__ void potrf_block(const CUtensorMap* tmap, T* tiles, float* A, int lda
       trsm_tile<T>(tiles + tidx(I, J) * TSZ, tiles + tidx(J, J) * TSZ, s_inv + J * TS, lane);
     __syncthreads();
     if (J + 1 < NT) {
-      if (warp == 0) {
-        syrk_tile<T>(tiles + tidx(J + 1, J + 1) * TSZ, tiles + tidx(J + 1, J) * TSZ,
-                     tiles + tidx(J + 1, J) * TSZ, lane);
-        __syncwarp();
-        factor_tile(J + 1);
-      } else {
-        // trailing tiles (I, K), J < K <= I < NT, except (J+1, J+1)
-        const int T_ = NT - J - 1;
-        const int nupd = T_ * (T_ + 1) / 2;
-        for (int u = warp; u < nupd; u += nwarps - 1) {
-          int i = 0;
-          while ((i + 1) * (i + 2) / 2 <= u) ++i;
-          const int k = u - i * (i + 1) / 2;
-          const int I = J + 1 + i, K = J + 1 + k;
-          syrk_tile<T>(tiles + tidx(I, K) * TSZ, tiles + tidx(I, J) * TSZ,
-                       tiles + tidx(K, J) * TSZ, lane);
+      if (warp < 4) {
+        T* dt = tiles + tidx(J + 1, J + 1) * TSZ;
+        const T* pj = tiles + tidx(J + 1, J) * TSZ;
+        syrk_tiles<T>(dt, pj, nullptr, nullptr, pj, lane, 8 * warp, 8 * warp + 8);
+        asm volatile("bar.sync 1, 128;" ::: "memory");   // warps 0-3
+        if (warp == 0) factor_tile(J + 1);
+      }
+      if (warp >= 1) {
+        // work items: pairs of vertically adjacent tiles (I, K), (I+1, K) of
+        // each trailing tile column K, J < K <= I, diagonal tile J+1 excluded
+        int item = 0;
+        for (int K = J + 1; K < NT; ++K) {
+          const int i0 = (K == J + 1) ? K + 1 : K;
+          for (int I = i0; I < NT; I += 2, ++item) {
+            if (item % (nwarps - 1) != warp - 1) continue;
+            const bool two = I + 1 < NT;
+            syrk_tiles<T>(tiles + tidx(I, K) * TSZ, tiles + tidx(I, J) * TSZ,
+                          two ? tiles + tidx(I + 1, K) * TSZ : nullptr,
+                          two ? tiles + tidx(I + 1, J) * TSZ : nullptr,
+                          tiles + tidx(K, J) * TSZ, lane);
+          }
         }
       }
     }

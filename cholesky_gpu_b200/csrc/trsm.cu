@@ -36,42 +36,60 @@ __device__ __forceinline__ int tl(int I, int M) { return I * (I - 1) / 2 + M; } 
 
 size_t trsm_smem_floats(int bs) {
   const int NT = bs / 32;
-  return (size_t)bs * XLD + (size_t)(NT * (NT - 1) / 2) * TSZ + (size_t)NT * TSZ;
+  return (size_t)bs * XLD + (size_t)(NT * (NT - 1) / 2) * TSZ + (size_t)NT * TSZ + (size_t)TR * 32;
 }
 
 // Solve the staged 64-row slab in place: for each 32-column tile J,
-// X_J -= X_{<J} L_{J,<J}^T (register-tiled), then X_J = X_J L_JJ^-T.
-__device__ void trsm_slab(float* Xs, const float* Lt, const float* Wt, int NT, int tid) {
-  const int tr = tid % 16, tc_ = tid / 16;   // rows 4*tr..4*tr+3, columns CPT*tc_..
+// X_J -= X_{<J} L_{J,<J}^T, then X_J = X_J L_JJ^-T.
+// The update splits K between two 128-thread groups: a thread keeps 4 rows x
+// 4 columns of X_J in registers and does 16 FMAs per 16-byte load of X and of
+// L.  Group 1's partial sums reach group 0 through red (64 x 32).
+__device__ void trsm_slab(float* Xs, const float* Lt, const float* Wt, float* red, int NT, int tid) {
+  const int g = tid / 128, t = tid % 128;
+  const int r4 = t % 16, c4 = t / 16;        // update: rows 4*r4.., columns 4*c4.. of X_J
+  const int tr = tid % 16, tc_ = tid / 16;   // inverse: rows 4*tr.., columns CPT*tc_..
   for (int J = 0; J < NT; ++J) {
     const int kend = 32 * J;
-    float acc[4][CPT];
+    if (J > 0) {
+      float acc[4][4];
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int j = 0; j < CPT; ++j) acc[i][j] = Xs[(kend + CPT * tc_ + j) * XLD + 4 * tr + i];
-    // X_J -= X_{<J} L_{J,<J}^T
-    for (int kt = 0; kt < J; ++kt) {
-      const float* lt = Lt + tl(J, kt) * TSZ + CPT * tc_;
-      const float* xt = Xs + (32 * kt) * XLD + 4 * tr;
+      for (int j = 0; j < 4; ++j) {
+        const float4 v = (g == 0) ? *reinterpret_cast<const float4*>(&Xs[(kend + 4 * c4 + j) * XLD + 4 * r4])
+                                  : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        acc[0][j] = v.x; acc[1][j] = v.y; acc[2][j] = v.z; acc[3][j] = v.w;
+      }
+      for (int kt = 0; kt < J; ++kt) {
+        const float* lt = Lt + tl(J, kt) * TSZ + 4 * c4 + 16 * g * 32;
+        const float* xt = Xs + (32 * kt + 16 * g) * XLD + 4 * r4;
 #pragma unroll 8
-      for (int kk = 0; kk < 32; ++kk) {
-        const float4 xv = *reinterpret_cast<const float4*>(xt + kk * XLD);
-        const float xr[4] = {xv.x, xv.y, xv.z, xv.w};
+        for (int kk = 0; kk < 16; ++kk) {
+          const float4 xv = *reinterpret_cast<const float4*>(xt + kk * XLD);
+          const float4 lv = *reinterpret_cast<const float4*>(lt + kk * 32);
+          const float xr[4] = {xv.x, xv.y, xv.z, xv.w};
+          const float lr[4] = {lv.x, lv.y, lv.z, lv.w};
 #pragma unroll
-        for (int j = 0; j < CPT; ++j) {
-          const float lv = lt[kk * 32 + j];
+          for (int i = 0; i < 4; ++i)
 #pragma unroll
-          for (int i = 0; i < 4; ++i) acc[i][j] -= xr[i] * lv;
+            for (int j = 0; j < 4; ++j) acc[i][j] -= xr[i] * lr[j];
         }
       }
+      if (g == 1) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          *reinterpret_cast<float4*>(&red[(4 * c4 + j) * TR + 4 * r4]) =
+              make_float4(acc[0][j], acc[1][j], acc[2][j], acc[3][j]);
+      }
+      __syncthreads();
+      if (g == 0) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const float4 p = *reinterpret_cast<const float4*>(&red[(4 * c4 + j) * TR + 4 * r4]);
+          *reinterpret_cast<float4*>(&Xs[(kend + 4 * c4 + j) * XLD + 4 * r4]) =
+              make_float4(acc[0][j] + p.x, acc[1][j] + p.y, acc[2][j] + p.z, acc[3][j] + p.w);
+        }
+      }
+      __syncthreads();
     }
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int j = 0; j < CPT; ++j) Xs[(kend + CPT * tc_ + j) * XLD + 4 * tr + i] = acc[i][j];
-    __syncthreads();
     // X_J = X_J * L_JJ^-T :  x[r][c] = sum_{m<=c} a[r][m] * (L^-1)[c][m]
     float out[4][CPT] = {};
     const float* W = Wt + J * TSZ + CPT * tc_;
@@ -119,6 +137,7 @@ trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_consta
   float* Xs = sm;                                        // [bs][XLD]
   float* Lt = Xs + (size_t)bs * XLD;                     // strictly-lower tiles of L11
   float* Wt = Lt + (size_t)(NT * (NT - 1) / 2) * TSZ;    // inverses of the diagonal tiles
+  float* red = Wt + (size_t)NT * TSZ;                    // partial sums of the split update
   __shared__ float red_max[NTHR / 32];
   __shared__ int red_lit[NTHR / 32];
   __shared__ __align__(8) uint64_t bar;
@@ -161,7 +180,7 @@ trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_consta
     }
     __syncthreads();
     if (!s_ok) break;
-    trsm_slab(Xs, Lt, Wt, NT, tid);
+    trsm_slab(Xs, Lt, Wt, red, NT, tid);
     // ---- write the solved slab back (coalesced; rows past n skipped) -----
     for (int e = tid; e < bs * TR; e += NTHR) {
       const int c = e / TR, r = e % TR;
@@ -253,6 +272,7 @@ trsm_batched_kernel(BatchSys* __restrict__ sys, int s, int b) {
   float* Xs = sm;
   float* Lt = Xs + (size_t)bs * XLD;
   float* Wt = Lt + (size_t)(NT * (NT - 1) / 2) * TSZ;
+  float* red = Wt + (size_t)NT * TSZ;
   const int tid = threadIdx.x;
   const float* A = S.A;
   const int ld = S.ld;
@@ -268,7 +288,7 @@ trsm_batched_kernel(BatchSys* __restrict__ sys, int s, int b) {
       }
   for (int e = tid; e < NT * TSZ; e += NTHR) Wt[e] = S.winv[e];
   __syncthreads();
-  trsm_slab(Xs, Lt, Wt, NT, tid);
+  trsm_slab(Xs, Lt, Wt, red, NT, tid);
   for (int e = tid; e < bs * TR; e += NTHR) {
     const int c = e / TR, r = e % TR;
     if (r < nrows) S.A[(size_t)(s + c) * ld + row0 + r] = Xs[c * XLD + r];
