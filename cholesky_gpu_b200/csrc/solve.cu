@@ -866,48 +866,47 @@ __device__ __forceinline__ bool trsv_job(int u, const float* L, int ldl, int n, 
 
 template <int NR>
 constexpr size_t trsv_staged_smem() {
-  return 2 * (size_t)TILE_ELEMS * sizeof(float) + 2 * (size_t)RB * NR * sizeof(double);
+  return (size_t)TILE_ELEMS * sizeof(float) + 2 * (size_t)RB * NR * sizeof(double);
 }
 
-// Units are taken one ahead: the tile of the next unit is copied into the
-// second stage while this unit waits for its input segment and computes.
-// A CTA holds at most two units and finishes the earlier one first; every
-// unit depends only on earlier ones, so the earliest unfinished unit always
-// belongs to a CTA that is working on it, and every wait ends.
+// Two CTAs per SM, each with one tile stage: a unit's tile copy is issued
+// as soon as the unit is taken and overlaps the wait for its input segment;
+// while one CTA waits on L2 round trips (unit counter, dependency counter,
+// vector segment, fence) the other computes.  The next unit number is taken
+// one unit ahead.  A CTA holds at most two units and finishes the earlier
+// one first; every unit depends only on earlier ones, so the earliest
+// unfinished unit always belongs to a CTA that is working on it, and every
+// wait ends.
 template <int NR, bool TRANS>
-__global__ void __launch_bounds__(NTH, 1)
+__global__ void __launch_bounds__(NTH, 2)
 trsv_persistent_kernel(const float* __restrict__ L, int ldl, int n, const float* __restrict__ wsup,
                        double* __restrict__ work, double* __restrict__ out, int* ctr,
                        const int* skip, DevStatus* st) {
   if (skip != nullptr && *skip) return;
   extern __shared__ __align__(16) unsigned char sm_raw[];
-  float* tiles = reinterpret_cast<float*>(sm_raw);                        // 2 stages
-  double* s_v = reinterpret_cast<double*>(tiles + 2 * TILE_ELEMS);        // RB x NR
+  float* Ts = reinterpret_cast<float*>(sm_raw);                           // one stage
+  double* s_v = reinterpret_cast<double*>(Ts + TILE_ELEMS);               // RB x NR
   double* s_col = s_v + RB * NR;                                          // RB x NR
-  __shared__ int s_unit;
+  __shared__ int s_unit[2];
   int* next = ctr;
   int* seg_in = ctr + 1;
   int* seg_out = seg_in + ceil_div(n, RB);
-  auto grab = [&]() {
-    if (threadIdx.x == 0) s_unit = atomicAdd(next, 1);
-    __syncthreads();
-    return s_unit;
-  };
-  TrsvJob cur, nxt;
-  int ucur = grab();
+  if (threadIdx.x == 0) s_unit[0] = atomicAdd(next, 1);
+  __syncthreads();
+  int ucur = s_unit[0];
+  TrsvJob cur;
   bool have = trsv_job<TRANS>(ucur, L, ldl, n, wsup, seg_in, seg_out, cur);
-  if (have) stage_tile(tiles, cur.T, cur.ld, cur.nrow, cur.ncol);
-  cp_async_commit();
-  for (int stage = 0; have; stage ^= 1) {
-    const int unxt = grab();
-    const bool have_nxt = trsv_job<TRANS>(unxt, L, ldl, n, wsup, seg_in, seg_out, nxt);
-    if (have_nxt) stage_tile(tiles + (stage ^ 1) * TILE_ELEMS, nxt.T, nxt.ld, nxt.nrow, nxt.ncol);
+  for (int it = 1; have; ++it) {
+    stage_tile(Ts, cur.T, cur.ld, cur.nrow, cur.ncol);
     cp_async_commit();
+    // the next unit number, taken by a thread of warp 1 so that its round
+    // trip overlaps warp 0's dependency poll; read after this unit's
+    // barriers (s_unit[it & 1] is not read again before its next write)
+    if (threadIdx.x == 32) s_unit[it & 1] = atomicAdd(next, 1);
     wait_count(cur.wait_ctr, cur.wait_need, st, ucur);
     load_vec<NR>(cur.panel ? out : work, n, cur.vin_row0, cur.vin_n, s_v);
-    cp_async_wait<1>();
+    cp_async_wait<0>();
     __syncthreads();
-    float* Ts = tiles + stage * TILE_ELEMS;
     double acc[4][NR] = {};
     tile_pass_staged<NR, false>(Ts, s_v, s_v, acc, s_col, cur.nt, !cur.nt);
     __syncthreads();
@@ -921,12 +920,10 @@ trsv_persistent_kernel(const float* __restrict__ L, int ldl, int n, const float*
         if (c < cur.out_n) atomicAdd(&dst[(size_t)k * n + cur.out_row0 + c], sign * s_col[e]);
       }
     }
-    signal_count(cur.sig_ctr);   // its barrier also frees this stage, s_v and s_col
-    cur = nxt;
-    ucur = unxt;
-    have = have_nxt;
+    signal_count(cur.sig_ctr);   // its barrier also frees the stage, s_v and s_col
+    ucur = s_unit[it & 1];
+    have = trsv_job<TRANS>(ucur, L, ldl, n, wsup, seg_in, seg_out, cur);
   }
-  cp_async_wait<0>();
 }
 
 // ---- batched variants: one launch serves every system of a batch --------
@@ -1211,7 +1208,7 @@ cudaError_t launch_trsv_persistent(bool backward, const float* L, int ldl, int n
   if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
   const int nri = nrhs == 1 ? 0 : nrhs == 2 ? 1 : nrhs == 4 ? 2 : 3;
   int& grid = grid_cache[dev & 63][backward ? 1 : 0][nri];
-  const size_t smem = 2 * (size_t)TILE_ELEMS * sizeof(float) + 2 * (size_t)RB * nrhs * sizeof(double);
+  const size_t smem = (size_t)TILE_ELEMS * sizeof(float) + 2 * (size_t)RB * nrhs * sizeof(double);
   auto launch = [&](auto kernel) -> cudaError_t {
     if (grid == 0) {
       int per_sm = 0, nsm = 0;
