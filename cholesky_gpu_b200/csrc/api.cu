@@ -127,8 +127,13 @@ struct mpchol_factor {
   float* sh = nullptr;        // accumulated rounding-shift estimate
   float* winv = nullptr;      // inverses of the 32x32 diagonal tiles of one block
   double* scratch64 = nullptr;
-  void* q = nullptr;          // quantized panel (K-major), n x b x 2 bytes
-  int8_t* rowexp = nullptr;
+  // the step's panel quantized in every format the step may pick (K-major,
+  // row i = trailing row i): 8-bit codes (E4M3, E5M2, MXFP8; n x b each),
+  // FP16 / FP16X2-hi codes then FP16X2-lo codes (n x b each), per-row
+  // exponents (E4M3, E5M2, FP16; n each) and MXFP8 block scales
+  uint8_t* q8 = nullptr;
+  uint16_t* q16 = nullptr;
+  int8_t* rexp = nullptr;
   uint8_t* mxexp = nullptr;
   StepState* steps = nullptr;
   DevStatus* status = nullptr;
@@ -188,8 +193,8 @@ cudaError_t dmalloc(T** p, size_t count) {
 
 void free_factor(mpchol_factor_t* f) {
   if (f == nullptr) return;
-  void* ptrs[] = {f->A, f->d, f->dtilde, f->rowsq, f->sh, f->winv, f->scratch64, f->q,
-                  f->rowexp, f->mxexp, f->steps, f->status, f->wsup, f->trsv_ctr,
+  void* ptrs[] = {f->A, f->d, f->dtilde, f->rowsq, f->sh, f->winv, f->scratch64, f->q8,
+                  f->q16, f->rexp, f->mxexp, f->steps, f->status, f->wsup, f->trsv_ctr,
                   f->vec, f->partials, f->scal, f->done};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -257,6 +262,17 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream) {
                        stream));
     return MPCHOL_OK;
   };
+  // where the panel solve writes the codes of each candidate format
+  QuantAll qa{};
+  qa.cand = fixed ? (o.precision != FP32 ? 1u << o.precision : 0u) : tc_mask;
+  qa.ldq = b;
+  for (int i = 0; i < 3; ++i) {
+    qa.q8[i] = f->q8 + (size_t)i * n * b;
+    qa.rexp[i] = f->rexp + (size_t)i * n;
+  }
+  qa.q16 = f->q16;
+  qa.mxexp = f->mxexp;
+  qa.ldmx = b / 32;
   // step k's trailing update over the tiles `sel` picks, on stream `ss`
   auto syrk = [&](int k, TileSel sel, int max_sms, cudaStream_t ss) -> mpchol_status {
     const int s = k * b;
@@ -270,8 +286,12 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream) {
               launch_syrk_f32(C, ld, m, bs, P, ld, nullptr, f->status, ss, sel, max_sms));
       else
         PHASE(MPCHOL_PH_SYRK_TC, 1, ss,
-              launch_syrk_tc(C, ld, m, bs, o.precision, f->q, bs, f->rowexp, f->mxexp, bs / 32,
-                             nullptr, f->status, ss, sel, max_sms));
+              launch_syrk_tc(C, ld, m, bs, o.precision,
+                             (o.precision == FP16 || o.precision == FP16X2)
+                                 ? static_cast<const void*>(qa.q16)
+                                 : static_cast<const void*>(qa.q8[q8_slot(o.precision)]),
+                             bs, qa.rexp[rexp_slot(o.precision)], qa.mxexp, bs / 32, nullptr,
+                             f->status, ss, sel, max_sms));
       return MPCHOL_OK;
     }
     const int* pick = &f->steps[k].prec;
@@ -280,8 +300,7 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream) {
             launch_syrk_f32(C, ld, m, bs, P, ld, pick, f->status, ss, sel, max_sms));
     if (tc_mask != 0)
       PHASE(MPCHOL_PH_SYRK_TC, 1, ss,
-            launch_syrk_tc_dispatch(C, ld, m, bs, tc_mask, f->q, bs, f->rowexp, f->mxexp, bs / 32,
-                                    pick, f->status, ss, sel, max_sms));
+            launch_syrk_tc_dispatch(C, ld, m, bs, tc_mask, qa, pick, f->status, ss, sel, max_sms));
     return MPCHOL_OK;
   };
   mpchol_status rs = potrf(0);
@@ -298,10 +317,10 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream) {
     }
     const int next_bs = std::min(b, m);
     // panel solve, step decision and panel quantization in one launch
-    const QuantOut qo{f->q, bs, f->rowexp, f->mxexp, bs / 32, o.diag_pert ? f->sh + s + bs : nullptr};
+    qa.sh = o.diag_pert ? f->sh + s + bs : nullptr;
     PHASE(MPCHOL_PH_TRSM, 1, stream,
           launch_trsm_panel(f->tmapX, f->tmap32, f->A, ld, n, s, bs, f->winv, f->d, f->dtilde,
-                            f->rowsq, &f->steps[k], &f->steps[k + 1], next_bs, dp, qo, f->status,
+                            f->rowsq, &f->steps[k], &f->steps[k + 1], next_bs, dp, qa, f->status,
                             stream));
     const int jc = ceil_div(next_bs, 128);   // 128-tile columns of block k+1
     if ((rs = syrk(k, TileSel{SEL_NEXT, jc}, 0, stream)) != MPCHOL_OK) return rs;
@@ -646,8 +665,9 @@ mpchol_status mpchol_factor_create(const mpchol_opts* opts, int n, mpchol_factor
             dmalloc(&f->rowsq, n) == cudaSuccess && dmalloc(&f->sh, n) == cudaSuccess &&
             dmalloc(&f->winv, (size_t)8 * 32 * 32) == cudaSuccess &&
             dmalloc(&f->scratch64, potrf_scratch64_elems(256)) == cudaSuccess &&
-            dmalloc(reinterpret_cast<uint8_t**>(&f->q), (size_t)n * f->b * 4) == cudaSuccess &&
-            dmalloc(&f->rowexp, n) == cudaSuccess &&
+            dmalloc(&f->q8, (size_t)3 * n * f->b) == cudaSuccess &&
+            dmalloc(&f->q16, (size_t)2 * n * f->b) == cudaSuccess &&
+            dmalloc(&f->rexp, (size_t)3 * n) == cudaSuccess &&
             dmalloc(&f->mxexp, (size_t)n * (f->b / 32)) == cudaSuccess &&
             dmalloc(&f->steps, f->nsteps + 1) == cudaSuccess &&
             dmalloc(&f->status, 1) == cudaSuccess &&

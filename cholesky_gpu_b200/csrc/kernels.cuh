@@ -42,27 +42,34 @@ cudaError_t launch_potrf(const CUtensorMap& tmap32, float* A, int lda, int n, in
                          bool may_fp64, cudaStream_t stream);
 
 // ---- panel TRSM + fused diagonal tracker, decision and quantization ------
-// Where the fused panel solve writes the quantized panel: K-major codes q
-// (row stride ldq elements), per-row exponents or per-32 E8M0 scales, and
-// the rounding-shift accumulator of the trailing rows (nullable).
-struct QuantOut {
-  void* q;
+// Where the panel solve writes the quantized panel: one K-major code panel
+// per format the step may pick (row i of a panel holds the codes of trailing
+// row i, ldq elements apart), with its scales, and the rounding-shift
+// accumulator of the trailing rows (nullable).  FP16X2 keeps its hi codes in
+// the FP16 panel (same scale rule) and its lo codes m rows further on.
+struct QuantAll {
+  unsigned cand;        // bit f set: format f is a candidate of the step
   int ldq;
-  int8_t* rowexp;
-  uint8_t* mxexp;
+  uint8_t* q8[3];       // E4M3, E5M2, MXFP8 codes (slot q8_slot)
+  uint16_t* q16;        // FP16 / FP16X2 hi codes, then FP16X2 lo codes
+  int8_t* rexp[3];      // per-row pow-2 exponents: E4M3, E5M2, FP16 / FP16X2
+  uint8_t* mxexp;       // MXFP8 E8M0 scales, ldmx per row
   int ldmx;
   float* sh;
 };
-// Solves X * L11^T = A21 in place for rows [s+bs, n) of block column s,
-// subtracts each row's sum of squares from dtilde, stores it in rowsq, folds
-// the switching statistics into step (and the FP64 flag of the next diagonal
-// block into next), then resolves the step precision (step->prec) and writes
-// the quantized panel.  tmapX: TMA map over A with 64 x bs boxes; tmap32 as
-// for launch_potrf.  Cooperative launch (grid barrier inside).
+__host__ __device__ inline int q8_slot(int fmt) { return fmt == E4M3 ? 0 : (fmt == E5M2 ? 1 : 2); }
+__host__ __device__ inline int rexp_slot(int fmt) { return fmt == E4M3 ? 0 : (fmt == E5M2 ? 1 : 2); }
+// Solves X * L11^T = A21 in place for rows [s+bs, n) of block column s, one
+// 64-row slab per CTA; subtracts each row's sum of squares from dtilde,
+// stores it in rowsq, folds the switching statistics into step (and the FP64
+// flag of the next diagonal block into next), and writes the slab's codes in
+// every candidate format.  The last CTA to finish resolves the step precision
+// (step->prec) and adds the step's rounding shift to qa.sh.  tmapX: TMA map
+// over A with 64 x bs boxes; tmap32 as for launch_potrf.
 cudaError_t launch_trsm_panel(const CUtensorMap& tmapX, const CUtensorMap& tmap32, float* A,
                               int lda, int n, int s, int bs, const float* winv, const float* d,
                               float* dtilde, float* rowsq, StepState* step, StepState* next,
-                              int next_bs, const DecisionParams& dp, const QuantOut& qo,
+                              int next_bs, const DecisionParams& dp, const QuantAll& qa,
                               DevStatus* st, cudaStream_t stream);
 
 // ---- panel quantization ---------------------------------------------------
@@ -138,11 +145,11 @@ cudaError_t launch_syrk_tc(float* C, int ldc, int m, int k, int fmt, const void*
 // resolved precision); fmt_mask (bit f for format f) lists the formats the
 // step may pick.  The launch returns at once when the pick is not among
 // them (FP32 steps go to launch_syrk_f32).  max_sms > 0 caps the grid.
+// The panels and scales of each format are those of qa (the panel solve's
+// outputs).
 cudaError_t launch_syrk_tc_dispatch(float* C, int ldc, int m, int k, unsigned fmt_mask,
-                                    const void* q, int ldq, const int8_t* rowexp,
-                                    const uint8_t* mxexp, int ldmx, const int* prec_sel,
-                                    DevStatus* st, cudaStream_t stream, TileSel sel = kAllTiles,
-                                    int max_sms = 0);
+                                    const QuantAll& qa, const int* prec_sel, DevStatus* st,
+                                    cudaStream_t stream, TileSel sel = kAllTiles, int max_sms = 0);
 
 // ---- batched factorization and solve of many independent systems --------
 // Systems are ordered by decreasing n, so the systems still active at a

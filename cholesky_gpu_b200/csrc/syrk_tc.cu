@@ -328,7 +328,7 @@ syrk_tc_body(const CUtensorMap* mhi, const CUtensorMap* mlo, const CUtensorMap* 
       }
       tc::tc_fence_after();
       const int i = I * TM + q * 32 + lane;
-      const float si = (i < mt) ? (MX ? 1.0f : pow2f(rexp[i])) : 0.0f;
+      const float si = (i < mt) ? (MX ? 1.0f : pow2f(__ldg(rexp + i))) : 0.0f;
       const uint32_t taddr = tmem + (uint32_t)(buf * TM) + ((uint32_t)(q * 32) << 16);
 #pragma unroll 1
       for (int c0 = half * (TM / 2); c0 < (half + 1) * (TM / 2); c0 += 32) {
@@ -354,7 +354,7 @@ syrk_tc_body(const CUtensorMap* mhi, const CUtensorMap* mlo, const CUtensorMap* 
             for (int u = 0; u < 32; ++u)
               stg[u * 32 + lane] = (I == J && j0 + u > i)
                                        ? -0.0f
-                                       : -((v[u] * si) * (MX ? 1.0f : pow2f(rexp[j0 + u])));
+                                       : -((v[u] * si) * (MX ? 1.0f : pow2f(__ldg(rexp + j0 + u))));
             tc::fence_proxy_async_smem();
             __syncwarp();
             if (lane == 0) {
@@ -373,7 +373,7 @@ syrk_tc_body(const CUtensorMap* mhi, const CUtensorMap* mlo, const CUtensorMap* 
           for (int u = 0; u < 32; ++u) {
             const int j = j0 + u;
             if (j < mt && i >= j)
-              Ct[(size_t)j * ldct + i] = cv[u] - (v[u] * si) * (MX ? 1.0f : pow2f(rexp[j]));
+              Ct[(size_t)j * ldct + i] = cv[u] - (v[u] * si) * (MX ? 1.0f : pow2f(__ldg(rexp + j)));
           }
         }
       }
@@ -398,18 +398,19 @@ syrk_tc_kernel(const __grid_constant__ TcMaps maps, float* __restrict__ C, int l
                            ntiles_b, sel);
 }
 
-// Maps for every format: 8-bit codes, FP16 hi and lo panels, C.
+// Maps for every format: the three 8-bit code panels (slot q8_slot), the
+// FP16 hi and lo panels, C.
 struct TcMapsAll {
-  CUtensorMap h8;
+  CUtensorMap h8[3];
   CUtensorMap h16;
   CUtensorMap l16;
   CUtensorMap c;
 };
-
 // One launch whatever the step picked: the format is read on the device.
 __global__ void __launch_bounds__(NTHREADS, 1)
 syrk_tc_dispatch_kernel(const __grid_constant__ TcMapsAll maps, float* __restrict__ C, int ldc,
-                        int m, int k, const int8_t* __restrict__ rowexp,
+                        int m, int k, const int8_t* __restrict__ rexp_e4m3,
+                        const int8_t* __restrict__ rexp_e5m2, const int8_t* __restrict__ rexp_f16,
                         const uint8_t* __restrict__ mxexp, int ldmx, unsigned fmt_mask,
                         const int* prec_sel, DevStatus* st, TileSel sel) {
   const int f = *prec_sel;
@@ -417,19 +418,24 @@ syrk_tc_dispatch_kernel(const __grid_constant__ TcMapsAll maps, float* __restric
   const TcBatch nb{};
   switch (f) {
     case FP16:
-      syrk_tc_body<FP16, false>(&maps.h16, &maps.l16, &maps.c, C, ldc, m, k, rowexp, mxexp, ldmx, st, nb, 0, sel);
+      syrk_tc_body<FP16, false>(&maps.h16, &maps.l16, &maps.c, C, ldc, m, k, rexp_f16, nullptr, 0,
+                                st, nb, 0, sel);
       break;
     case FP16X2:
-      syrk_tc_body<FP16X2, false>(&maps.h16, &maps.l16, &maps.c, C, ldc, m, k, rowexp, mxexp, ldmx, st, nb, 0, sel);
+      syrk_tc_body<FP16X2, false>(&maps.h16, &maps.l16, &maps.c, C, ldc, m, k, rexp_f16, nullptr,
+                                  0, st, nb, 0, sel);
       break;
     case E4M3:
-      syrk_tc_body<E4M3, false>(&maps.h8, &maps.h8, &maps.c, C, ldc, m, k, rowexp, mxexp, ldmx, st, nb, 0, sel);
+      syrk_tc_body<E4M3, false>(&maps.h8[0], &maps.h8[0], &maps.c, C, ldc, m, k, rexp_e4m3, nullptr,
+                                0, st, nb, 0, sel);
       break;
     case E5M2:
-      syrk_tc_body<E5M2, false>(&maps.h8, &maps.h8, &maps.c, C, ldc, m, k, rowexp, mxexp, ldmx, st, nb, 0, sel);
+      syrk_tc_body<E5M2, false>(&maps.h8[1], &maps.h8[1], &maps.c, C, ldc, m, k, rexp_e5m2, nullptr,
+                                0, st, nb, 0, sel);
       break;
     case MXFP8:
-      syrk_tc_body<MXFP8, false>(&maps.h8, &maps.h8, &maps.c, C, ldc, m, k, rowexp, mxexp, ldmx, st, nb, 0, sel);
+      syrk_tc_body<MXFP8, false>(&maps.h8[2], &maps.h8[2], &maps.c, C, ldc, m, k, nullptr, mxexp,
+                                 ldmx, st, nb, 0, sel);
       break;
     default:
       break;
@@ -513,35 +519,36 @@ cudaError_t launch_syrk_tc(float* C, int ldc, int m, int k, int fmt, const void*
 }
 
 cudaError_t launch_syrk_tc_dispatch(float* C, int ldc, int m, int k, unsigned fmt_mask,
-                                    const void* q, int ldq, const int8_t* rowexp,
-                                    const uint8_t* mxexp, int ldmx, const int* prec_sel,
-                                    DevStatus* st, cudaStream_t stream, TileSel sel, int max_sms) {
-  if (m <= 0 || prec_sel == nullptr) return m <= 0 ? cudaSuccess : cudaErrorInvalidValue;
+                                    const QuantAll& qa, const int* prec_sel, DevStatus* st,
+                                    cudaStream_t stream, TileSel sel, int max_sms) {
+  if (m <= 0) return cudaSuccess;
+  if (prec_sel == nullptr) return cudaErrorInvalidValue;
   const int ntiles = sel_tile_count(ceil_div(m, TM), sel);
   if (ntiles <= 0) return cudaSuccess;
-  const bool any8 = (fmt_mask & ((1u << E4M3) | (1u << E5M2) | (1u << MXFP8))) != 0;
-  const bool any16 = (fmt_mask & ((1u << FP16) | (1u << FP16X2))) != 0;
   for (int f : {FP16, E4M3, E5M2, FP16X2, MXFP8})
     if (((fmt_mask >> f) & 1u) && !syrk_tc_supported(f, k)) return cudaErrorInvalidValue;
   if (((fmt_mask >> MXFP8) & 1u) &&
-      (mxexp == nullptr || ldmx < k / 32 || (reinterpret_cast<uintptr_t>(mxexp) & 3) != 0 ||
-       (ldmx & 3) != 0))
+      (qa.mxexp == nullptr || qa.ldmx < k / 32 || (reinterpret_cast<uintptr_t>(qa.mxexp) & 3) != 0 ||
+       (qa.ldmx & 3) != 0))
     return cudaErrorInvalidValue;
   TcMapsAll maps;
   if (!encode_tmap_2d(&maps.c, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, C, (uint64_t)m, (uint64_t)m,
                       (uint64_t)ldc, 32, 32, CU_TENSOR_MAP_SWIZZLE_NONE))
     return cudaErrorInvalidValue;
-  maps.h8 = maps.h16 = maps.l16 = maps.c;   // unused slots
-  if (any8 && !encode_tmap_2d(&maps.h8, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, q, (uint64_t)k, (uint64_t)m,
-                              (uint64_t)ldq, CHUNK, TM, CU_TENSOR_MAP_SWIZZLE_128B))
-    return cudaErrorInvalidValue;
-  if (any16) {
-    if (!encode_tmap_2d(&maps.h16, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, q, (uint64_t)k, (uint64_t)m,
-                        (uint64_t)ldq, CHUNK / 2, TM, CU_TENSOR_MAP_SWIZZLE_128B))
+  maps.h8[0] = maps.h8[1] = maps.h8[2] = maps.h16 = maps.l16 = maps.c;   // unused slots
+  for (int f : {E4M3, E5M2, MXFP8})
+    if (((fmt_mask >> f) & 1u) &&
+        !encode_tmap_2d(&maps.h8[q8_slot(f)], CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, qa.q8[q8_slot(f)],
+                        (uint64_t)k, (uint64_t)m, (uint64_t)qa.ldq, CHUNK, TM,
+                        CU_TENSOR_MAP_SWIZZLE_128B))
       return cudaErrorInvalidValue;
-    const uint16_t* lo = reinterpret_cast<const uint16_t*>(q) + (size_t)m * ldq;
+  if (fmt_mask & ((1u << FP16) | (1u << FP16X2))) {
+    if (!encode_tmap_2d(&maps.h16, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, qa.q16, (uint64_t)k,
+                        (uint64_t)m, (uint64_t)qa.ldq, CHUNK / 2, TM, CU_TENSOR_MAP_SWIZZLE_128B))
+      return cudaErrorInvalidValue;
+    const uint16_t* lo = qa.q16 + (size_t)m * qa.ldq;
     if (!encode_tmap_2d(&maps.l16, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, lo, (uint64_t)k, (uint64_t)m,
-                        (uint64_t)ldq, CHUNK / 2, TM, CU_TENSOR_MAP_SWIZZLE_128B))
+                        (uint64_t)qa.ldq, CHUNK / 2, TM, CU_TENSOR_MAP_SWIZZLE_128B))
       return cudaErrorInvalidValue;
   }
   size_t smem = 0;
@@ -558,8 +565,9 @@ cudaError_t launch_syrk_tc_dispatch(float* C, int ldc, int m, int k, unsigned fm
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_all);
   if (e != cudaSuccess) return e;
   const int grid = grid_for(ntiles, max_sms);
-  syrk_tc_dispatch_kernel<<<grid, NTHREADS, smem, stream>>>(maps, C, ldc, m, k, rowexp, mxexp, ldmx,
-                                                            fmt_mask, prec_sel, st, sel);
+  syrk_tc_dispatch_kernel<<<grid, NTHREADS, smem, stream>>>(maps, C, ldc, m, k, qa.rexp[0], qa.rexp[1],
+                                                            qa.rexp[2], qa.mxexp, qa.ldmx, fmt_mask,
+                                                            prec_sel, st, sel);
   return cudaGetLastError();
 }
 

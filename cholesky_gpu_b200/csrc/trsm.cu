@@ -113,73 +113,147 @@ __device__ void trsm_slab(float* Xs, const float* Lt, const float* Wt, float* re
   }
 }
 
-constexpr long long kGridBarPolls = 1ll << 24;
-static_assert(NTHR == QTHR, "the fused quantizer runs with the panel solve's threads");
+static_assert(NTHR == 4 * TR, "the epilogue maps four threads to each slab row");
 
-// Persistent panel solve with the quantization of the panel fused in.
-// Phase 1: CTA c solves the 64-row slabs c, c + grid, ... (L11's tiles and
-// tile inverses are staged once per CTA by TMA, each slab by one 2-D box),
-// writes them back, and folds their rows into the diagonal tracker and the
-// switching statistics.  A grid barrier (the launch is cooperative, so all
-// CTAs are resident; the wait is bounded) then makes the statistics and the
-// solved panel complete.  Phase 2: every CTA resolves the same step
-// precision and quantizes 32-row tiles of the panel (read back from L2) into
-// the K-major codes the trailing update reads, adding the step's rounding
-// shift u_p * sum_j L_ij^2 to sh.
+// Codes of one solved slab in one format.  Xs: the slab (bs columns x TR
+// rows, column-major, stride XLD).  Thread (r, part) = (tid % TR, tid / TR)
+// converts row r's contiguous columns [part*bs/4, (part+1)*bs/4) -- for
+// MXFP8 whole 32-column blocks, whose scales it forms itself -- into packed
+// words of a shared staging panel (row stride bs/4 + 1 words for 8-bit codes,
+// bs/2 + 1 for 16-bit ones, so the column-wise writes of 32 consecutive rows
+// hit 32 banks); the CTA then copies the staged rows out as coalesced
+// 4-byte words.
+__device__ void quantize_slab(const float* Xs, int bs, int nrows, int gi0, int m, int fmt, float rmax,
+                              const QuantAll& qa, uint32_t* stage, int tid) {
+  const int r = tid % TR, part = tid / TR;
+  const int cw = bs / 4;                       // columns per thread
+  const int c0 = part * cw;
+  const int gi = gi0 + r;
+  const bool live = r < nrows;
+  if (fmt == FP16 || fmt == FP16X2) {
+    const int sw = bs / 2 + 1;
+    uint32_t* hi = stage;
+    uint32_t* lo = stage + TR * sw;
+    const int e = row_scale_exp(rmax, FP16);
+    const float inv = pow2f(-e);
+    for (int c = c0; c < c0 + cw; c += 2) {
+      const float x0 = Xs[c * XLD + r] * inv, x1 = Xs[(c + 1) * XLD + r] * inv;
+      const __half h0 = __float2half_rn(x0), h1 = __float2half_rn(x1);
+      hi[r * sw + c / 2] = (uint32_t)__half_as_ushort(h0) | ((uint32_t)__half_as_ushort(h1) << 16);
+      if (fmt == FP16X2)   // x - hi is exact in FP32
+        lo[r * sw + c / 2] = (uint32_t)f32_to_f16(x0 - __half2float(h0)) |
+                             ((uint32_t)f32_to_f16(x1 - __half2float(h1)) << 16);
+    }
+    if (live && part == 0) qa.rexp[2][gi] = (int8_t)e;
+    __syncthreads();
+    const int wpr = bs / 2;                    // words per row
+    for (int q = tid; q < nrows * wpr; q += NTHR) {
+      const int rr = q / wpr, w = q % wpr;
+      reinterpret_cast<uint32_t*>(qa.q16 + (size_t)(gi0 + rr) * qa.ldq)[w] = hi[rr * sw + w];
+      if (fmt == FP16X2)
+        reinterpret_cast<uint32_t*>(qa.q16 + (size_t)(m + gi0 + rr) * qa.ldq)[w] = lo[rr * sw + w];
+    }
+  } else {
+    const int sw = bs / 4 + 1;
+    int e = 0;
+    float inv = 1.0f;
+    if (fmt != MXFP8) {
+      e = row_scale_exp(rmax, fmt);
+      inv = pow2f(-e);
+      if (live && part == 0) qa.rexp[rexp_slot(fmt)][gi] = (int8_t)e;
+    }
+    for (int cb = c0; cb < c0 + cw; cb += 32) {
+      if (fmt == MXFP8) {
+        // one E8M0 scale per 32 consecutive columns (OCP MX)
+        float bmax = 0.0f;
+        for (int c = cb; c < cb + 32; ++c) bmax = fmaxf(bmax, fabsf(Xs[c * XLD + r]));
+        const int eb = mx_scale_exp(bmax);
+        inv = pow2f(-eb);
+        if (live) qa.mxexp[(size_t)gi * qa.ldmx + cb / 32] = (uint8_t)(eb + 127);
+      }
+      for (int c = cb; c < cb + 32; c += 4) {
+        uint32_t w = 0;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const float x = Xs[(c + u) * XLD + r] * inv;
+          const uint8_t code = (fmt == E5M2) ? f32_to_e5m2(x) : f32_to_e4m3(x);
+          w |= (uint32_t)code << (8 * u);
+        }
+        stage[r * sw + c / 4] = w;
+      }
+    }
+    __syncthreads();
+    uint8_t* q = qa.q8[q8_slot(fmt)];
+    const int wpr = bs / 4;
+    for (int q4 = tid; q4 < nrows * wpr; q4 += NTHR) {
+      const int rr = q4 / wpr, w = q4 % wpr;
+      reinterpret_cast<uint32_t*>(q + (size_t)(gi0 + rr) * qa.ldq)[w] = stage[rr * sw + w];
+    }
+  }
+  __syncthreads();                             // the staging panel is reused
+}
+
+// Panel solve with the quantization of the panel fused in; one 64-row slab
+// per CTA (the launch may exceed the resident CTAs: no CTA waits on
+// another).  Each CTA stages L11's tiles, its tile inverses and its slab by
+// TMA, solves the slab, writes it back, folds its rows into the diagonal
+// tracker and the switching statistics, and writes the slab's codes in every
+// candidate format (the step's precision is not known yet; the trailing
+// update reads the panel of the one the step picks).  The CTA that finishes
+// last (a ticket counter) resolves the step precision and adds the step's
+// rounding shift u_p * sum_j L_ij^2 to sh.
 __global__ void __launch_bounds__(NTHR, 1)
 trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_constant__ CUtensorMap tmap32,
                   float* __restrict__ A, int lda, int n, int s, int bs, const float* __restrict__ winv,
                   const float* __restrict__ d, float* __restrict__ dtilde, float* __restrict__ rowsq,
                   StepState* step, StepState* next, int next_bs, DecisionParams dp, DevStatus* st,
-                  QuantOut qo) {
+                  QuantAll qa) {
   extern __shared__ __align__(128) float sm[];
   const int NT = bs / 32;
   float* Xs = sm;                                        // [bs][XLD]
   float* Lt = Xs + (size_t)bs * XLD;                     // strictly-lower tiles of L11
   float* Wt = Lt + (size_t)(NT * (NT - 1) / 2) * TSZ;    // inverses of the diagonal tiles
   float* red = Wt + (size_t)NT * TSZ;                    // partial sums of the split update
+  uint32_t* stage = reinterpret_cast<uint32_t*>(Lt);     // code staging, once L11 is used
   __shared__ float red_max[NTHR / 32];
   __shared__ int red_lit[NTHR / 32];
+  __shared__ float s_rmax[4][TR];
   __shared__ __align__(8) uint64_t bar;
-  __shared__ int s_ok;
+  __shared__ int s_ok, s_last;
 
   const int tid = threadIdx.x;
   const int m = n - s - bs;
-  const int nslab = ceil_div(m, TR);
+  const int slab = blockIdx.x;
+  const int row0 = s + bs + slab * TR;                   // first global row of the slab
+  const int nrows = min(TR, n - row0);
   if (tid == 0) {
     s_ok = st->code == 0;
     tc::mbar_init(&bar, 1);
     tc::fence_mbar_init();
   }
   __syncthreads();
-  uint32_t phase = 0;
-  float bm = 0.0f;   // this CTA's max d/dtilde and literal code over its slabs
+  float bm = 0.0f;   // this CTA's max d/dtilde and literal code
   int bl = 0;
-  for (int slab = blockIdx.x; slab < nslab && s_ok; slab += gridDim.x, phase ^= 1u) {
-    const int row0 = s + bs + slab * TR;                 // first global row of the slab
-    const int nrows = min(TR, n - row0);
+  if (s_ok) {
     // ---- stage with TMA (rows past n arrive as zeros) ---------------------
     if (tid == 0) {
-      const bool first = slab == (int)blockIdx.x;
       const int nlt = NT * (NT - 1) / 2;
-      uint32_t bytes = (uint32_t)(bs * XLD * sizeof(float));
-      if (first) bytes += (uint32_t)((nlt * TSZ + NT * TSZ) * sizeof(float));
+      const uint32_t bytes = (uint32_t)((bs * XLD + nlt * TSZ + NT * TSZ) * sizeof(float));
       tc::mbar_expect_tx(&bar, bytes);
       tc::tma_load_2d(Xs, &tmapX, &bar, row0, s);
-      if (first) {
-        for (int I = 1; I < NT; ++I)
-          for (int M = 0; M < I; ++M)
-            tc::tma_load_2d(Lt + tl(I, M) * TSZ, &tmap32, &bar, s + 32 * I, s + 32 * M);
-        tc::bulk_load_1d(Wt, winv, (uint32_t)(NT * TSZ * sizeof(float)), &bar);
-      }
-      if (!tc::mbar_wait(&bar, phase)) {
+      for (int I = 1; I < NT; ++I)
+        for (int M = 0; M < I; ++M)
+          tc::tma_load_2d(Lt + tl(I, M) * TSZ, &tmap32, &bar, s + 32 * I, s + 32 * M);
+      tc::bulk_load_1d(Wt, winv, (uint32_t)(NT * TSZ * sizeof(float)), &bar);
+      if (!tc::mbar_wait(&bar, 0)) {
         s_ok = 0;
         set_status(st, MPCHOL_ERR_TIMEOUT, row0);
-        tc::mbar_wait(&bar, phase);
+        tc::mbar_wait(&bar, 0);
       }
     }
     __syncthreads();
-    if (!s_ok) break;
+  }
+  if (s_ok) {
     trsm_slab(Xs, Lt, Wt, red, NT, tid);
     // ---- write the solved slab back (coalesced; rows past n skipped) -----
     for (int e = tid; e < bs * TR; e += NTHR) {
@@ -208,14 +282,31 @@ trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_consta
           dt <= dp.floor_ratio * di)
         next->fp64_diag = 1;
     }
-    __syncthreads();                                     // Xs is restaged next
+    // ---- the slab's codes in every candidate format -------------------------
+    if (qa.cand != 0) {
+      {
+        const int r = tid % TR, part = tid / TR, cw = bs / 4;
+        float amax = 0.0f;
+        for (int c = part * cw; c < (part + 1) * cw; ++c) amax = fmaxf(amax, fabsf(Xs[c * XLD + r]));
+        s_rmax[part][r] = amax;
+      }
+      __syncthreads();   // also: L11's tiles are no longer read, the staging may reuse them
+      const int r = tid % TR;
+      const float rmax = fmaxf(fmaxf(s_rmax[0][r], s_rmax[1][r]), fmaxf(s_rmax[2][r], s_rmax[3][r]));
+      const int gi0 = slab * TR;                         // first trailing row of the slab
+      const bool f16 = (qa.cand >> FP16) & 1u, f16x2 = (qa.cand >> FP16X2) & 1u;
+      if (f16 || f16x2) quantize_slab(Xs, bs, nrows, gi0, m, f16x2 ? FP16X2 : FP16, rmax, qa, stage, tid);
+      const int f8[3] = {E4M3, E5M2, MXFP8};
+      for (int i = 0; i < 3; ++i)
+        if ((qa.cand >> f8[i]) & 1u) quantize_slab(Xs, bs, nrows, gi0, m, f8[i], rmax, qa, stage, tid);
+    }
   }
-  // ---- statistics of the CTA, then the grid barrier ----------------------
+  // ---- statistics of the CTA; the last CTA resolves the step --------------
   bm = warp_max(bm);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) bl = max(bl, __shfl_xor_sync(0xffffffffu, bl, o));
   if ((tid & 31) == 0) { red_max[tid >> 5] = bm; red_lit[tid >> 5] = bl; }
-  __threadfence();                                       // this thread's panel writes
+  __threadfence();                                       // this thread's panel, code and row writes
   __syncthreads();
   if (tid == 0) {
     float cm = 0.0f; int cl = 0;
@@ -223,37 +314,20 @@ trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_consta
     atomicMax(&step->max_ratio_bits, __float_as_uint(cm));
     atomicMax(&step->literal_code, cl);
     __threadfence();
-    atomicAdd(&step->grid_bar, 1);
-    long long it = 0;
-    while (*reinterpret_cast<volatile int*>(&step->grid_bar) < (int)gridDim.x) {
-      if (++it > kGridBarPolls) {
-        set_status(st, MPCHOL_ERR_TIMEOUT, s);
-        break;
-      }
-      __nanosleep(32);
-    }
-    __threadfence();
+    s_last = atomicAdd(&step->grid_bar, 1) == (int)gridDim.x - 1;
   }
   __syncthreads();
+  if (!s_last) return;
+  __threadfence();                                       // every CTA's statistics and rows
   if (*reinterpret_cast<volatile int*>(&st->code) != 0) return;
-  // ---- phase 2: the step precision and the quantized panel ----------------
   StepState ss;
   ss.max_ratio_bits = *reinterpret_cast<volatile unsigned int*>(&step->max_ratio_bits);
   ss.literal_code = *reinterpret_cast<volatile int*>(&step->literal_code);
   const int p = resolve_precision(&ss, dp);
-  if (blockIdx.x == 0 && tid == 0) step->prec = p;
-  if (p == FP32) return;
-  const float* P = A + (size_t)s * lda + s + bs;
+  if (tid == 0) step->prec = p;
+  if (p == FP32 || qa.sh == nullptr) return;
   const float u = unit_roundoff(p);
-  for (int t = blockIdx.x; t * QROWS < m; t += gridDim.x) {
-    if (qo.sh != nullptr)
-      for (int r = tid; r < QROWS; r += NTHR) {
-        const int gi = t * QROWS + r;
-        if (gi < m) qo.sh[gi] += u * rowsq[s + bs + gi];
-      }
-    quantize_tile(P, lda, m, bs, p, qo.q, qo.ldq, qo.rowexp, qo.mxexp, qo.ldmx, Xs, m, t * QROWS);
-    __syncthreads();                                     // the staging tile is reused
-  }
+  for (int gi = tid; gi < m; gi += NTHR) qa.sh[gi] += u * __ldcg(rowsq + s + bs + gi);
 }
 
 // Batched: blockIdx.y = system, blockIdx.x = 64-row slab.  Staging by
@@ -307,7 +381,7 @@ trsm_batched_kernel(BatchSys* __restrict__ sys, int s, int b) {
 cudaError_t launch_trsm_panel(const CUtensorMap& tmapX, const CUtensorMap& tmap32, float* A,
                               int lda, int n, int s, int bs, const float* winv, const float* d,
                               float* dtilde, float* rowsq, StepState* step, StepState* next,
-                              int next_bs, const DecisionParams& dp, const QuantOut& qo,
+                              int next_bs, const DecisionParams& dp, const QuantAll& qa,
                               DevStatus* st, cudaStream_t stream) {
   const int m = n - s - bs;
   if (m <= 0) return cudaSuccess;
@@ -316,34 +390,9 @@ cudaError_t launch_trsm_panel(const CUtensorMap& tmapX, const CUtensorMap& tmap3
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)(trsm_smem_floats(256) * sizeof(float)));
   if (e != cudaSuccess) return e;
-  // one CTA per SM at most (shared memory), all resident: the launch is
-  // cooperative because the CTAs meet at a grid barrier
-  static int nsm_cache[64] = {};
-  int dev = 0;
-  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
-  int& nsm = nsm_cache[dev & 63];
-  if (nsm == 0) {
-    int per_sm = 0, sms = 0;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-             &per_sm, trsm_panel_kernel, NTHR, trsm_smem_floats(256) * sizeof(float))) != cudaSuccess)
-      return e;
-    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
-      return e;
-    nsm = std::max(1, per_sm) * sms;
-  }
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(std::min(ceil_div(m, TR), nsm));
-  cfg.blockDim = dim3(NTHR);
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = stream;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeCooperative;
-  attr[0].val.cooperative = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  e = cudaLaunchKernelEx(&cfg, trsm_panel_kernel, tmapX, tmap32, A, lda, n, s, bs, winv, d, dtilde,
-                         rowsq, step, next, next_bs, dp, st, qo);
-  if (e != cudaSuccess) return e;
+  trsm_panel_kernel<<<ceil_div(m, TR), NTHR, smem, stream>>>(tmapX, tmap32, A, lda, n, s, bs, winv, d,
+                                                             dtilde, rowsq, step, next, next_bs, dp, st,
+                                                             qa);
   return cudaGetLastError();
 }
 
