@@ -157,7 +157,7 @@ struct mpchol_factor {
   cudaEvent_t ev_rest = nullptr;   // the rest of the step's update is done
   int nsm = 0;
   CUtensorMap tmap32;         // TMA map over A, 32 x 32 boxes
-  CUtensorMap tmapX;          // TMA map over A, 64 x b boxes (panel slabs)
+  CUtensorMap tmapX;          // TMA map over A, 32 x b boxes (panel slabs)
 };
 
 namespace {
@@ -691,7 +691,7 @@ mpchol_status mpchol_factor_create(const mpchol_opts* opts, int n, mpchol_factor
   // never written)
   if (!encode_tmap_2d(&f->tmap32, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, f->A, n, n, f->ld, 32, 32,
                       CU_TENSOR_MAP_SWIZZLE_NONE) ||
-      !encode_tmap_2d(&f->tmapX, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, f->A, n, n, f->ld, 64,
+      !encode_tmap_2d(&f->tmapX, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, f->A, n, n, f->ld, 32,
                       f->b, CU_TENSOR_MAP_SWIZZLE_NONE)) {
     free_factor(f);
     return MPCHOL_ERR_CUDA;

@@ -60,12 +60,12 @@ struct QuantAll {
 __host__ __device__ inline int q8_slot(int fmt) { return fmt == E4M3 ? 0 : (fmt == E5M2 ? 1 : 2); }
 __host__ __device__ inline int rexp_slot(int fmt) { return fmt == E4M3 ? 0 : (fmt == E5M2 ? 1 : 2); }
 // Solves X * L11^T = A21 in place for rows [s+bs, n) of block column s, one
-// 64-row slab per CTA; subtracts each row's sum of squares from dtilde,
+// 32-row slab per CTA; subtracts each row's sum of squares from dtilde,
 // stores it in rowsq, folds the switching statistics into step (and the FP64
 // flag of the next diagonal block into next), and writes the slab's codes in
 // every candidate format.  The last CTA to finish resolves the step precision
 // (step->prec) and adds the step's rounding shift to qa.sh.  tmapX: TMA map
-// over A with 64 x bs boxes; tmap32 as for launch_potrf.
+// over A with 32 x bs boxes; tmap32 as for launch_potrf.
 cudaError_t launch_trsm_panel(const CUtensorMap& tmapX, const CUtensorMap& tmap32, float* A,
                               int lda, int n, int s, int bs, const float* winv, const float* d,
                               float* dtilde, float* rowsq, StepState* step, StepState* next,

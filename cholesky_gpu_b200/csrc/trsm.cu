@@ -6,16 +6,18 @@
 // (src/kernels_macros.cuh:191-211).
 //
 // X * L11^T = A21 for the m rows below the diagonal block.  Rows are
-// independent, so one CTA owns 64 rows for the whole solve.  One thread stages
-// everything the CTA needs with TMA in a single round: its 64 x b slab of the
-// panel (one 2-D box), the strictly-lower 32 x 32 tiles of L11 (2-D boxes) and
-// the inverses of L11's diagonal tiles (a 1-D bulk copy of what the POTRF
-// kernel wrote).  The CTA then walks the 32-column tiles J:
-// X_J -= X_{<J} L_{J,<J}^T (register-tiled), X_J = X_J L_JJ^-T, writes the
-// slab back with one TMA store and, in the epilogue, folds each row's sum of
-// squares into the Schur-diagonal tracker dtilde and reduces the switching
-// statistics (max d/dtilde, reference-literal choice) and the near-indefinite
-// flag of the next diagonal block.
+// independent, so one CTA owns a 32-row slab.  TMA stages the slab (one 2-D
+// box) and streams L11 one 32-row tile row at a time (the strictly-lower
+// tiles L_{J,<J} as 2-D boxes and the inverse of the diagonal tile L_JJ, which
+// the POTRF kernel wrote, as a 1-D bulk copy) two rows ahead of its use, so a
+// CTA needs about 108 KB of shared memory and two CTAs share an SM.  The CTA
+// walks the 32-column tiles J: X_J -= X_{<J} L_{J,<J}^T (register-tiled,
+// K split over four thread groups), X_J = X_J L_JJ^-T, writes the slab back
+// and, in the epilogue, folds each row's sum of squares into the
+// Schur-diagonal tracker dtilde, reduces the switching statistics
+// (max d/dtilde, reference-literal choice) and the near-indefinite flag of
+// the next diagonal block, and writes the slab's codes in every candidate
+// format.
 #include <algorithm>
 
 #include "common.cuh"
@@ -26,108 +28,116 @@
 namespace mpchol {
 namespace {
 
-constexpr int TR = 64;       // rows per CTA
-constexpr int NTHR = 256;    // 8 warps: 4 rows x 2 columns of each tile per thread
-constexpr int CPT = 32 / (NTHR / 16);   // tile columns per thread
+constexpr int TR = 32;       // rows per CTA
+constexpr int NTHR = 256;    // 8 warps
 constexpr int TSZ = 32 * 32; // dense 32 x 32 tile
 constexpr int XLD = TR;      // X staged column-major, rows contiguous
+constexpr int KG = 4;        // groups the update's K dimension is split over
+constexpr int KPG = 32 / KG; // K values of each L tile per group
+static_assert(NTHR == KG * (TR / 4) * 8, "a group maps 4 x 4 outputs to each of its threads");
 
 __device__ __forceinline__ int tl(int I, int M) { return I * (I - 1) / 2 + M; }  // I > M
 
+// Shared memory of the streaming panel kernel: the slab, two buffers of one
+// tile row of L11 (up to NT - 1 tiles) and of one tile inverse, the partial
+// sums of the split update.
 size_t trsm_smem_floats(int bs) {
   const int NT = bs / 32;
-  return (size_t)bs * XLD + (size_t)(NT * (NT - 1) / 2) * TSZ + (size_t)NT * TSZ + (size_t)TR * 32;
+  return (size_t)bs * XLD + 2 * (size_t)(NT - 1) * TSZ + 2 * (size_t)TSZ + (size_t)(KG - 1) * TR * 32;
+}
+// Shared memory of the batched kernel: the slab, all of L11's tiles and
+// inverses, the partial sums.
+size_t trsm_batched_smem_floats(int bs) {
+  const int NT = bs / 32;
+  return (size_t)bs * XLD + (size_t)(NT * (NT - 1) / 2) * TSZ + (size_t)NT * TSZ +
+         (size_t)(KG - 1) * TR * 32;
 }
 
-// Solve the staged 64-row slab in place: for each 32-column tile J,
-// X_J -= X_{<J} L_{J,<J}^T, then X_J = X_J L_JJ^-T.
-// The update splits K between two 128-thread groups: a thread keeps 4 rows x
+// Step J of the slab solve: X_J -= X_{<J} L_{J,<J}^T, then X_J = X_J L_JJ^-T.
+// LJ: the tiles L_{J,0..J-1} (column-major 32 x 32, contiguous); WJ: L_JJ^-1.
+// The update splits K over four groups of 64 threads: a thread keeps 4 rows x
 // 4 columns of X_J in registers and does 16 FMAs per 16-byte load of X and of
-// L.  Group 1's partial sums reach group 0 through red (64 x 32).
-__device__ void trsm_slab(float* Xs, const float* Lt, const float* Wt, float* red, int NT, int tid) {
-  const int g = tid / 128, t = tid % 128;
-  const int r4 = t % 16, c4 = t / 16;        // update: rows 4*r4.., columns 4*c4.. of X_J
-  const int tr = tid % 16, tc_ = tid / 16;   // inverse: rows 4*tr.., columns CPT*tc_..
-  for (int J = 0; J < NT; ++J) {
-    const int kend = 32 * J;
-    if (J > 0) {
-      float acc[4][4];
+// L; groups 1-3 hand their partial sums to group 0 through red, which adds
+// them in group order.  Every output's operations, and so its rounding, are
+// fixed by this split.
+__device__ void trsm_step(float* Xs, const float* LJ, const float* WJ, float* red, int J, int tid) {
+  const int g = tid / 64, t = tid % 64;
+  const int r4 = t % (TR / 4), c4 = t / (TR / 4);   // rows 4*r4.., columns 4*c4.. of X_J
+  const int kend = 32 * J;
+  if (J > 0) {
+    float acc[4][4];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const float4 v = (g == 0) ? *reinterpret_cast<const float4*>(&Xs[(kend + 4 * c4 + j) * XLD + 4 * r4])
-                                  : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        acc[0][j] = v.x; acc[1][j] = v.y; acc[2][j] = v.z; acc[3][j] = v.w;
+    for (int j = 0; j < 4; ++j) {
+      const float4 v = (g == 0) ? *reinterpret_cast<const float4*>(&Xs[(kend + 4 * c4 + j) * XLD + 4 * r4])
+                                : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      acc[0][j] = v.x; acc[1][j] = v.y; acc[2][j] = v.z; acc[3][j] = v.w;
+    }
+    for (int kt = 0; kt < J; ++kt) {
+      const float* lt = LJ + kt * TSZ + 4 * c4 + KPG * g * 32;
+      const float* xt = Xs + (32 * kt + KPG * g) * XLD + 4 * r4;
+#pragma unroll
+      for (int kk = 0; kk < KPG; ++kk) {
+        const float4 xv = *reinterpret_cast<const float4*>(xt + kk * XLD);
+        const float4 lv = *reinterpret_cast<const float4*>(lt + kk * 32);
+        const float xr[4] = {xv.x, xv.y, xv.z, xv.w};
+        const float lr[4] = {lv.x, lv.y, lv.z, lv.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[i][j] -= xr[i] * lr[j];
       }
-      for (int kt = 0; kt < J; ++kt) {
-        const float* lt = Lt + tl(J, kt) * TSZ + 4 * c4 + 16 * g * 32;
-        const float* xt = Xs + (32 * kt + 16 * g) * XLD + 4 * r4;
-#pragma unroll 8
-        for (int kk = 0; kk < 16; ++kk) {
-          const float4 xv = *reinterpret_cast<const float4*>(xt + kk * XLD);
-          const float4 lv = *reinterpret_cast<const float4*>(lt + kk * 32);
-          const float xr[4] = {xv.x, xv.y, xv.z, xv.w};
-          const float lr[4] = {lv.x, lv.y, lv.z, lv.w};
+    }
+    if (g > 0) {
+      float* rg = red + (g - 1) * TR * 32;
 #pragma unroll
-          for (int i = 0; i < 4; ++i)
+      for (int j = 0; j < 4; ++j)
+        *reinterpret_cast<float4*>(&rg[(4 * c4 + j) * TR + 4 * r4]) =
+            make_float4(acc[0][j], acc[1][j], acc[2][j], acc[3][j]);
+    }
+    __syncthreads();
+    if (g == 0) {
 #pragma unroll
-            for (int j = 0; j < 4; ++j) acc[i][j] -= xr[i] * lr[j];
-        }
-      }
-      if (g == 1) {
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-          *reinterpret_cast<float4*>(&red[(4 * c4 + j) * TR + 4 * r4]) =
-              make_float4(acc[0][j], acc[1][j], acc[2][j], acc[3][j]);
-      }
-      __syncthreads();
-      if (g == 0) {
+      for (int q = 0; q < KG - 1; ++q) {
+        const float* rg = red + q * TR * 32;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-          const float4 p = *reinterpret_cast<const float4*>(&red[(4 * c4 + j) * TR + 4 * r4]);
-          *reinterpret_cast<float4*>(&Xs[(kend + 4 * c4 + j) * XLD + 4 * r4]) =
-              make_float4(acc[0][j] + p.x, acc[1][j] + p.y, acc[2][j] + p.z, acc[3][j] + p.w);
+          const float4 pv = *reinterpret_cast<const float4*>(&rg[(4 * c4 + j) * TR + 4 * r4]);
+          acc[0][j] += pv.x; acc[1][j] += pv.y; acc[2][j] += pv.z; acc[3][j] += pv.w;
         }
       }
-      __syncthreads();
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        *reinterpret_cast<float4*>(&Xs[(kend + 4 * c4 + j) * XLD + 4 * r4]) =
+            make_float4(acc[0][j], acc[1][j], acc[2][j], acc[3][j]);
     }
-    // X_J = X_J * L_JJ^-T :  x[r][c] = sum_{m<=c} a[r][m] * (L^-1)[c][m]
-    float out[4][CPT] = {};
-    const float* W = Wt + J * TSZ + CPT * tc_;
-#pragma unroll 8
-    for (int m = 0; m < 32; ++m) {
-      const float4 av = *reinterpret_cast<const float4*>(&Xs[(kend + m) * XLD + 4 * tr]);
-      const float ar[4] = {av.x, av.y, av.z, av.w};
-#pragma unroll
-      for (int j = 0; j < CPT; ++j) {
-        const float wv = W[m * 32 + j];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) out[i][j] += ar[i] * wv;
-      }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int j = 0; j < CPT; ++j) Xs[(kend + CPT * tc_ + j) * XLD + 4 * tr + i] = out[i][j];
     __syncthreads();
   }
+  // X_J = X_J * L_JJ^-T :  x[r][c] = sum_{m<=c} a[r][m] * (L^-1)[c][m]
+  const int tr = tid % (TR / 4), tc_ = tid / (TR / 4);   // rows 4*tr.., column tc_
+  float out[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll 8
+  for (int m = 0; m < 32; ++m) {
+    const float4 av = *reinterpret_cast<const float4*>(&Xs[(kend + m) * XLD + 4 * tr]);
+    const float wv = WJ[m * 32 + tc_];
+    out[0] += av.x * wv; out[1] += av.y * wv; out[2] += av.z * wv; out[3] += av.w * wv;
+  }
+  __syncthreads();
+  *reinterpret_cast<float4*>(&Xs[(kend + tc_) * XLD + 4 * tr]) = make_float4(out[0], out[1], out[2], out[3]);
+  __syncthreads();
 }
-
-static_assert(NTHR == 4 * TR, "the epilogue maps four threads to each slab row");
 
 // Codes of one solved slab in one format.  Xs: the slab (bs columns x TR
 // rows, column-major, stride XLD).  Thread (r, part) = (tid % TR, tid / TR)
-// converts row r's contiguous columns [part*bs/4, (part+1)*bs/4) -- for
-// MXFP8 whole 32-column blocks, whose scales it forms itself -- into packed
-// words of a shared staging panel (row stride bs/4 + 1 words for 8-bit codes,
-// bs/2 + 1 for 16-bit ones, so the column-wise writes of 32 consecutive rows
-// hit 32 banks); the CTA then copies the staged rows out as coalesced
-// 4-byte words.
+// converts row r's 32-column block `part` (for MXFP8 with its own scale)
+// into packed words of a shared staging panel (row stride bs/4 + 1 words for
+// 8-bit codes, bs/2 + 1 for 16-bit ones, so the column-wise writes of 32
+// consecutive rows hit 32 banks); the CTA then copies the staged rows out as
+// coalesced 4-byte words.
 __device__ void quantize_slab(const float* Xs, int bs, int nrows, int gi0, int m, int fmt, float rmax,
                               const QuantAll& qa, uint32_t* stage, int tid) {
   const int r = tid % TR, part = tid / TR;
-  const int cw = bs / 4;                       // columns per thread
-  const int c0 = part * cw;
+  const int cw = part < bs / 32 ? 32 : 0;      // columns of this thread
+  const int c0 = part * 32;
   const int gi = gi0 + r;
   const bool live = r < nrows;
   if (fmt == FP16 || fmt == FP16X2) {
@@ -193,16 +203,16 @@ __device__ void quantize_slab(const float* Xs, int bs, int nrows, int gi0, int m
   __syncthreads();                             // the staging panel is reused
 }
 
-// Panel solve with the quantization of the panel fused in; one 64-row slab
-// per CTA (the launch may exceed the resident CTAs: no CTA waits on
-// another).  Each CTA stages L11's tiles, its tile inverses and its slab by
+// Panel solve with the quantization of the panel fused in; one 32-row slab
+// per CTA, two CTAs per SM (the launch may exceed the resident CTAs: no CTA
+// waits on another).  Each CTA stages its slab and streams L11's tile rows by
 // TMA, solves the slab, writes it back, folds its rows into the diagonal
 // tracker and the switching statistics, and writes the slab's codes in every
 // candidate format (the step's precision is not known yet; the trailing
 // update reads the panel of the one the step picks).  The CTA that finishes
 // last (a ticket counter) resolves the step precision and adds the step's
 // rounding shift u_p * sum_j L_ij^2 to sh.
-__global__ void __launch_bounds__(NTHR, 1)
+__global__ void __launch_bounds__(NTHR, 2)
 trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_constant__ CUtensorMap tmap32,
                   float* __restrict__ A, int lda, int n, int s, int bs, const float* __restrict__ winv,
                   const float* __restrict__ d, float* __restrict__ dtilde, float* __restrict__ rowsq,
@@ -211,14 +221,14 @@ trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_consta
   extern __shared__ __align__(128) float sm[];
   const int NT = bs / 32;
   float* Xs = sm;                                        // [bs][XLD]
-  float* Lt = Xs + (size_t)bs * XLD;                     // strictly-lower tiles of L11
-  float* Wt = Lt + (size_t)(NT * (NT - 1) / 2) * TSZ;    // inverses of the diagonal tiles
-  float* red = Wt + (size_t)NT * TSZ;                    // partial sums of the split update
-  uint32_t* stage = reinterpret_cast<uint32_t*>(Lt);     // code staging, once L11 is used
+  float* Lb = Xs + (size_t)bs * XLD;                     // 2 x (NT - 1) tiles: rows of L11
+  float* Wb = Lb + 2 * (size_t)(NT - 1) * TSZ;           // 2 x 1 tile: inverses of L_JJ
+  float* red = Wb + 2 * (size_t)TSZ;                     // partial sums of the split update
+  uint32_t* stage = reinterpret_cast<uint32_t*>(Lb);     // code staging, once L11 is used
   __shared__ float red_max[NTHR / 32];
   __shared__ int red_lit[NTHR / 32];
-  __shared__ float s_rmax[4][TR];
-  __shared__ __align__(8) uint64_t bar;
+  __shared__ float s_rmax[NTHR / TR][TR];
+  __shared__ __align__(8) uint64_t barx, barl[2];
   __shared__ int s_ok, s_last;
 
   const int tid = threadIdx.x;
@@ -226,35 +236,60 @@ trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_consta
   const int slab = blockIdx.x;
   const int row0 = s + bs + slab * TR;                   // first global row of the slab
   const int nrows = min(TR, n - row0);
+  // tile row J of L11 (tiles L_{J,0..J-1} and L_JJ^-1) into buffer J % 2
+  auto issue_row = [&](int J) {
+    const int buf = J & 1;
+    tc::mbar_expect_tx(&barl[buf], (uint32_t)((J + 1) * TSZ * sizeof(float)));
+    for (int M = 0; M < J; ++M)
+      tc::tma_load_2d(Lb + ((size_t)buf * (NT - 1) + M) * TSZ, &tmap32, &barl[buf], s + 32 * J, s + 32 * M);
+    tc::bulk_load_1d(Wb + buf * TSZ, winv + J * TSZ, (uint32_t)(TSZ * sizeof(float)), &barl[buf]);
+  };
   if (tid == 0) {
     s_ok = st->code == 0;
-    tc::mbar_init(&bar, 1);
+    tc::mbar_init(&barx, 1);
+    tc::mbar_init(&barl[0], 1);
+    tc::mbar_init(&barl[1], 1);
     tc::fence_mbar_init();
+  }
+  __syncthreads();
+  int issued = 0, consumed = 0;   // tile rows issued / waited for (thread 0's counts)
+  if (s_ok && tid == 0) {
+    tc::mbar_expect_tx(&barx, (uint32_t)(bs * XLD * sizeof(float)));
+    tc::tma_load_2d(Xs, &tmapX, &barx, row0, s);
+    for (; issued < 2 && issued < NT; ++issued) issue_row(issued);
+    if (!tc::mbar_wait(&barx, 0)) {
+      s_ok = 0;
+      set_status(st, MPCHOL_ERR_TIMEOUT, row0);
+      tc::mbar_wait(&barx, 0);
+    }
   }
   __syncthreads();
   float bm = 0.0f;   // this CTA's max d/dtilde and literal code
   int bl = 0;
   if (s_ok) {
-    // ---- stage with TMA (rows past n arrive as zeros) ---------------------
-    if (tid == 0) {
-      const int nlt = NT * (NT - 1) / 2;
-      const uint32_t bytes = (uint32_t)((bs * XLD + nlt * TSZ + NT * TSZ) * sizeof(float));
-      tc::mbar_expect_tx(&bar, bytes);
-      tc::tma_load_2d(Xs, &tmapX, &bar, row0, s);
-      for (int I = 1; I < NT; ++I)
-        for (int M = 0; M < I; ++M)
-          tc::tma_load_2d(Lt + tl(I, M) * TSZ, &tmap32, &bar, s + 32 * I, s + 32 * M);
-      tc::bulk_load_1d(Wt, winv, (uint32_t)(NT * TSZ * sizeof(float)), &bar);
-      if (!tc::mbar_wait(&bar, 0)) {
-        s_ok = 0;
-        set_status(st, MPCHOL_ERR_TIMEOUT, row0);
-        tc::mbar_wait(&bar, 0);
+    for (int J = 0; J < NT; ++J) {
+      if (tid == 0 && s_ok) {
+        if (tc::mbar_wait(&barl[J & 1], (uint32_t)((J >> 1) & 1))) {
+          consumed = J + 1;
+        } else {
+          s_ok = 0;
+          set_status(st, MPCHOL_ERR_TIMEOUT, row0);
+        }
       }
+      __syncthreads();
+      if (!s_ok) break;
+      trsm_step(Xs, Lb + (size_t)(J & 1) * (NT - 1) * TSZ, Wb + (J & 1) * TSZ, red, J, tid);
+      // trsm_step ends with a barrier: buffer J % 2 is free for row J + 2
+      if (tid == 0 && issued < NT) issue_row(issued++);
     }
-    __syncthreads();
+    if (tid == 0) {
+      // rows still in flight after an abort (bounded waits): their copies
+      // must land before the CTA's shared memory is released
+      for (int J = consumed; J < issued; ++J) tc::mbar_wait(&barl[J & 1], (uint32_t)((J >> 1) & 1));
+    }
   }
+  __syncthreads();
   if (s_ok) {
-    trsm_slab(Xs, Lt, Wt, red, NT, tid);
     // ---- write the solved slab back (coalesced; rows past n skipped) -----
     for (int e = tid; e < bs * TR; e += NTHR) {
       const int c = e / TR, r = e % TR;
@@ -285,14 +320,17 @@ trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_consta
     // ---- the slab's codes in every candidate format -------------------------
     if (qa.cand != 0) {
       {
-        const int r = tid % TR, part = tid / TR, cw = bs / 4;
+        const int r = tid % TR, part = tid / TR;
         float amax = 0.0f;
-        for (int c = part * cw; c < (part + 1) * cw; ++c) amax = fmaxf(amax, fabsf(Xs[c * XLD + r]));
+        if (part < NT)
+          for (int c = part * 32; c < part * 32 + 32; ++c) amax = fmaxf(amax, fabsf(Xs[c * XLD + r]));
         s_rmax[part][r] = amax;
       }
-      __syncthreads();   // also: L11's tiles are no longer read, the staging may reuse them
+      __syncthreads();
       const int r = tid % TR;
-      const float rmax = fmaxf(fmaxf(s_rmax[0][r], s_rmax[1][r]), fmaxf(s_rmax[2][r], s_rmax[3][r]));
+      float rmax = 0.0f;
+#pragma unroll
+      for (int q = 0; q < NTHR / TR; ++q) rmax = fmaxf(rmax, s_rmax[q][r]);
       const int gi0 = slab * TR;                         // first trailing row of the slab
       const bool f16 = (qa.cand >> FP16) & 1u, f16x2 = (qa.cand >> FP16X2) & 1u;
       if (f16 || f16x2) quantize_slab(Xs, bs, nrows, gi0, m, f16x2 ? FP16X2 : FP16, rmax, qa, stage, tid);
@@ -330,7 +368,7 @@ trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_consta
   for (int gi = tid; gi < m; gi += NTHR) qa.sh[gi] += u * __ldcg(rowsq + s + bs + gi);
 }
 
-// Batched: blockIdx.y = system, blockIdx.x = 64-row slab.  Staging by
+// Batched: blockIdx.y = system, blockIdx.x = 32-row slab.  Staging by
 // plain coalesced loads (no per-system tensor maps); the epilogue keeps the
 // row sums of squares (rounding-shift estimate) and the diagonal tracker.
 __global__ void __launch_bounds__(NTHR)
@@ -362,7 +400,7 @@ trsm_batched_kernel(BatchSys* __restrict__ sys, int s, int b) {
       }
   for (int e = tid; e < NT * TSZ; e += NTHR) Wt[e] = S.winv[e];
   __syncthreads();
-  trsm_slab(Xs, Lt, Wt, red, NT, tid);
+  for (int J = 0; J < NT; ++J) trsm_step(Xs, Lt + tl(J, 0) * TSZ, Wt + J * TSZ, red, J, tid);
   for (int e = tid; e < bs * TR; e += NTHR) {
     const int c = e / TR, r = e % TR;
     if (r < nrows) S.A[(size_t)(s + c) * ld + row0 + r] = Xs[c * XLD + r];
@@ -399,7 +437,7 @@ cudaError_t launch_trsm_panel(const CUtensorMap& tmapX, const CUtensorMap& tmap3
 cudaError_t launch_trsm_batched(BatchSys* sys, int nact, int s, int b, int max_m,
                                 cudaStream_t stream) {
   if (nact <= 0 || max_m <= 0) return cudaSuccess;
-  const size_t smem = trsm_smem_floats(b) * sizeof(float);
+  const size_t smem = trsm_batched_smem_floats(b) * sizeof(float);
   cudaError_t e = cudaFuncSetAttribute(trsm_batched_kernel,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
