@@ -341,6 +341,9 @@ syrk_tc_body(const CUtensorMap* mhi, const CUtensorMap* mlo, const CUtensorMap* 
           if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tc::smem_u32(&acce_bar[buf])) : "memory");
         }
         const int j0 = J * TM + c0;
+        // column scales of the box: lane u loads s_{j0+u} once, the element
+        // loops take it by shuffle
+        const float sj_lane = (!MX && j0 + lane < mt) ? pow2f(__ldg(rexp + j0 + lane)) : 1.0f;
         if (RED) {
           // C(rows i0.., cols j0..) += -(s_i s_j acc) as one 32 x 32 TMA
           // reduce-add; boxes wholly above the diagonal or past m are skipped,
@@ -351,10 +354,10 @@ syrk_tc_body(const CUtensorMap* mhi, const CUtensorMap* mlo, const CUtensorMap* 
             if (lane == 0) tc::bulk_wait_read();     // this warp's previous box has been read
             __syncwarp();
 #pragma unroll
-            for (int u = 0; u < 32; ++u)
-              stg[u * 32 + lane] = (I == J && j0 + u > i)
-                                       ? -0.0f
-                                       : -((v[u] * si) * (MX ? 1.0f : pow2f(__ldg(rexp + j0 + u))));
+            for (int u = 0; u < 32; ++u) {
+              const float sj = MX ? 1.0f : __shfl_sync(0xffffffffu, sj_lane, u);
+              stg[u * 32 + lane] = (I == J && j0 + u > i) ? -0.0f : -((v[u] * si) * sj);
+            }
             tc::fence_proxy_async_smem();
             __syncwarp();
             if (lane == 0) {
@@ -362,18 +365,20 @@ syrk_tc_body(const CUtensorMap* mhi, const CUtensorMap* mlo, const CUtensorMap* 
               tc::bulk_commit();
             }
           }
-        } else if (i < mt) {
+        } else {
+          // every lane takes part (the shuffles); rows past m only skip the stores
+          const bool row_ok = i < mt;
           float cv[32];
 #pragma unroll
           for (int u = 0; u < 32; ++u) {
             const int j = j0 + u;
-            cv[u] = (j < mt && i >= j) ? Ct[(size_t)j * ldct + i] : 0.0f;
+            cv[u] = (row_ok && j < mt && i >= j) ? Ct[(size_t)j * ldct + i] : 0.0f;
           }
 #pragma unroll
           for (int u = 0; u < 32; ++u) {
             const int j = j0 + u;
-            if (j < mt && i >= j)
-              Ct[(size_t)j * ldct + i] = cv[u] - (v[u] * si) * (MX ? 1.0f : pow2f(__ldg(rexp + j)));
+            const float sj = MX ? 1.0f : __shfl_sync(0xffffffffu, sj_lane, u);
+            if (row_ok && j < mt && i >= j) Ct[(size_t)j * ldct + i] = cv[u] - (v[u] * si) * sj;
           }
         }
       }
