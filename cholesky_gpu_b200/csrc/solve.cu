@@ -465,13 +465,24 @@ block_inverse_body(const float* __restrict__ L, int ldl, int n, float* __restric
   const int g = bid.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int i0 = g * RB;
   const int nb = min(RB, n - i0);
-  for (int e = tid; e < RB * RB; e += NTH) {
-    const int col = e / RB, row = e % RB;
-    float v;
-    if (row < nb && col < nb) v = (row >= col) ? L[(size_t)(i0 + col) * ldl + i0 + row] : 0.0f;
-    else v = (row == col) ? 1.0f : 0.0f;
-    Ls[col * BLD + row] = v;
-    W[col * BLD + row] = 0.0;
+  // 16 loads in flight per thread before their shared-memory stores
+  constexpr int LB = 16;
+  for (int e0 = tid; e0 < RB * RB; e0 += LB * NTH) {
+    float v[LB];
+#pragma unroll
+    for (int u = 0; u < LB; ++u) {
+      const int e = e0 + u * NTH;
+      const int col = e / RB, row = e % RB;
+      if (row < nb && col < nb) v[u] = (row >= col) ? L[(size_t)(i0 + col) * ldl + i0 + row] : 0.0f;
+      else v[u] = (row == col) ? 1.0f : 0.0f;
+    }
+#pragma unroll
+    for (int u = 0; u < LB; ++u) {
+      const int e = e0 + u * NTH;
+      const int col = e / RB, row = e % RB;
+      Ls[col * BLD + row] = v[u];
+      W[col * BLD + row] = 0.0;
+    }
   }
   __syncthreads();
   // 32-row diagonal tiles: warp t, lane j solves L_tt w = e_j (right-looking,
@@ -493,21 +504,28 @@ block_inverse_body(const float* __restrict__ L, int ldl, int n, float* __restric
   __syncthreads();
   // doublings h = 32 (two pairs) and h = 64 (one pair) inside the block;
   // output e of a level: row r = e % h, column c = (e / h) % h of pair e / h^2
+  // Every output of a doubling runs over the whole k range of its pair: the
+  // inverses stored in W are zero above their diagonals, so the extra terms
+  // add zeros, and a thread's outputs advance together (independent
+  // accumulators instead of one dependent chain after another).
   for (int h = 32; h < RB; h *= 2) {
     const int per = (RB / (2 * h)) * h * h / NTH;    // outputs per thread: 8 or 16
+    int pa[16], pb[16];                               // per output: operand bases
     double acc[16];
-    // T = B A^-1 -> the pair's upper-right block (scratch)
+    // T = B A^-1 -> the pair's upper-right block (scratch):
+    // T[r][c] = sum_k L[a0+h+r][a0+k] * Ainv[k][c]
 #pragma unroll
     for (int q = 0; q < 16; ++q) {
+      const int e = tid + NTH * q;
+      const int r = e % h, c = (e / h) % h, a0 = (e / (h * h)) * 2 * h;
+      pa[q] = a0 * BLD + a0 + h + r;                  // Ls[(a0 + k) * BLD + a0 + h + r]
+      pb[q] = (a0 + c) * BLD + a0;                    // W[(a0 + c) * BLD + a0 + k]
       acc[q] = 0.0;
-      if (q < per) {
-        const int e = tid + NTH * q;
-        const int r = e % h, c = (e / h) % h, a0 = (e / (h * h)) * 2 * h;
-        double sacc = 0.0;
-        for (int k = c; k < h; ++k)
-          sacc += (double)Ls[(a0 + k) * BLD + a0 + h + r] * W[(a0 + c) * BLD + a0 + k];
-        acc[q] = sacc;
-      }
+    }
+    for (int k = 0; k < h; ++k) {
+#pragma unroll
+      for (int q = 0; q < 16; ++q)
+        if (q < per) acc[q] += (double)Ls[pa[q] + k * BLD] * W[pb[q] + k];
     }
     __syncthreads();
 #pragma unroll
@@ -518,17 +536,20 @@ block_inverse_body(const float* __restrict__ L, int ldl, int n, float* __restric
         W[(a0 + h + c) * BLD + a0 + r] = acc[q];
       }
     __syncthreads();
-    // X = -C^-1 T -> the pair's lower-left block; the scratch is cleared
+    // X = -C^-1 T -> the pair's lower-left block; the scratch is cleared:
+    // X[r][c] = -sum_k Cinv[r][k] * T[k][c]
 #pragma unroll
     for (int q = 0; q < 16; ++q) {
-      if (q < per) {
-        const int e = tid + NTH * q;
-        const int r = e % h, c = (e / h) % h, a0 = (e / (h * h)) * 2 * h;
-        double sacc = 0.0;
-        for (int k = 0; k <= r; ++k)
-          sacc += W[(a0 + h + k) * BLD + a0 + h + r] * W[(a0 + h + c) * BLD + a0 + k];
-        acc[q] = -sacc;
-      }
+      const int e = tid + NTH * q;
+      const int r = e % h, c = (e / h) % h, a0 = (e / (h * h)) * 2 * h;
+      pa[q] = (a0 + h) * BLD + a0 + h + r;            // W[(a0 + h + k) * BLD + a0 + h + r]
+      pb[q] = (a0 + h + c) * BLD + a0;                // W[(a0 + h + c) * BLD + a0 + k]
+      acc[q] = 0.0;
+    }
+    for (int k = 0; k < h; ++k) {
+#pragma unroll
+      for (int q = 0; q < 16; ++q)
+        if (q < per) acc[q] += W[pa[q] + k * BLD] * W[pb[q] + k];
     }
     __syncthreads();
 #pragma unroll
@@ -536,7 +557,7 @@ block_inverse_body(const float* __restrict__ L, int ldl, int n, float* __restric
       if (q < per) {
         const int e = tid + NTH * q;
         const int r = e % h, c = (e / h) % h, a0 = (e / (h * h)) * 2 * h;
-        W[(a0 + c) * BLD + a0 + h + r] = acc[q];
+        W[(a0 + c) * BLD + a0 + h + r] = -acc[q];
         W[(a0 + h + c) * BLD + a0 + r] = 0.0;
       }
     __syncthreads();
