@@ -143,6 +143,32 @@ class Factor:
         Z = Z.t()
         return Z.reshape(R.shape) if R.dim() == 1 else Z
 
+    def solve_host(self, A: torch.Tensor, B: torch.Tensor, rel_tol: float = 1e-10,
+                   max_it: int = 200, x0_precond: bool = True,
+                   check_every: int = 4) -> tuple[torch.Tensor, Report]:
+        """Factor A and solve A X = B with A (FP32) and B (FP64, n or n x nrhs)
+        in host memory (page-locked for full-speed copies).  Only A's lower
+        triangle reaches the device.  Returns X on the host."""
+        if A.device.type != "cpu" or B.device.type != "cpu":
+            raise ValueError("solve_host takes host (CPU) tensors")
+        if A.dtype != torch.float32 or B.dtype != torch.float64:
+            raise ValueError("A must be float32 and B float64")
+        Ac, lda = _col_major(A)
+        Bc = _host_col_major(B, self.n)
+        nrhs = Bc.shape[1]
+        X = torch.empty((nrhs, self.n), dtype=torch.float64, pin_memory=A.is_pinned()).t()
+        po = _lib.default_pcg_opts(rel_tol=rel_tol, max_it=max_it, x0_precond=int(x0_precond),
+                                   check_every=check_every)
+        rep = _lib.Report()
+        st = self.lib.mpchol_solve_host(self.handle, Ac.data_ptr(), lda, Bc.data_ptr(),
+                                        X.data_ptr(), nrhs, ctypes.byref(po), ctypes.byref(rep),
+                                        _stream_handle())
+        if st not in (_lib.OK, _lib.PCG_MAXIT):
+            check(st, "mpchol_solve_host")
+        Xo = X.reshape(B.shape) if B.dim() == 1 else X
+        return Xo, Report(rep.iterations, bool(rep.converged), rep.rel_residual,
+                          rep.backward_error, rep.precond_residual, st)
+
     def pcg(self, A: torch.Tensor, B: torch.Tensor, rel_tol: float = 1e-10, max_it: int = 200,
             x0_precond: bool = True, check_every: int = 4) -> tuple[torch.Tensor, Report]:
         """Solve A X = B (B: n or n x nrhs FP64 CUDA tensor) with PCG on this factor."""
@@ -166,6 +192,16 @@ class Factor:
         Xo = Xo.reshape(B.shape) if B.dim() == 1 else Xo
         return Xo, Report(rep.iterations, bool(rep.converged), rep.rel_residual,
                           rep.backward_error, rep.precond_residual, st)
+
+
+def _host_col_major(M: torch.Tensor, n: int) -> torch.Tensor:
+    """n x nrhs (or n) CPU FP64 tensor as column-major storage (no copy for one
+    column or an already column-major view)."""
+    M2 = M.reshape(n, 1) if M.dim() == 1 else M
+    if M2.stride(0) == 1 and (M2.shape[1] == 1 or M2.stride(1) == n):
+        return M2
+    Mc = M2.t().contiguous()
+    return Mc.t()
 
 
 def _wrap_device(ptr: int, shape: tuple, dtype: torch.dtype) -> torch.Tensor:

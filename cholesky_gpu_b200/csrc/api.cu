@@ -152,6 +152,10 @@ struct mpchol_factor {
   cudaStream_t capture_stream = nullptr;   // private stream used only to capture graphs
   // look-ahead: the bulk of each step's trailing update runs on aux while
   // the next diagonal block is factored on the caller's stream
+  // host-buffer solves: the operator's lower triangle and the rhs / solution
+  float* op = nullptr;        // n columns x ld, lower triangle
+  double* hb = nullptr;       // n x 8
+  double* hx = nullptr;       // n x 8
   cudaStream_t aux = nullptr;
   cudaEvent_t ev_next = nullptr;   // the next block's columns are updated
   cudaEvent_t ev_rest = nullptr;   // the rest of the step's update is done
@@ -195,7 +199,7 @@ void free_factor(mpchol_factor_t* f) {
   if (f == nullptr) return;
   void* ptrs[] = {f->A, f->d, f->dtilde, f->rowsq, f->sh, f->winv, f->scratch64, f->q8,
                   f->q16, f->rexp, f->mxexp, f->steps, f->status, f->wsup, f->trsv_ctr,
-                  f->vec, f->partials, f->scal, f->done};
+                  f->vec, f->partials, f->scal, f->done, f->op, f->hb, f->hx};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (f->graph.exec) cudaGraphExecDestroy(f->graph.exec);
@@ -217,6 +221,22 @@ DecisionParams make_dp(const mpchol_opts& o) {
   dp.ladder_len = o.ladder_len;
   for (int i = 0; i < 4; ++i) dp.ladder[i] = o.ladder[i];
   return dp;
+}
+
+// The lower triangle of an n x n column-major matrix, block column by block
+// column (rows from the block's diagonal down): one 2-D copy per block
+// column, about half of the matrix's bytes.  The factorization and the
+// operator products read nothing above the diagonal.
+cudaError_t copy_lower_blocks(float* dst, int ldd, const float* src, int lds, int n, int b,
+                              cudaMemcpyKind kind, cudaStream_t s) {
+  for (int c = 0; c < n; c += b) {
+    const int w = std::min(b, n - c);
+    cudaError_t e = cudaMemcpy2DAsync(dst + (size_t)c * ldd + c, sizeof(float) * ldd,
+                                      src + (size_t)c * lds + c, sizeof(float) * lds,
+                                      sizeof(float) * (n - c), w, kind, s);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 // One factorization of f->A in place, on `stream`, right-looking with a
@@ -704,9 +724,33 @@ mpchol_status mpchol_factor_compute(mpchol_factor_t* f, const float* dA, int lda
                                     mpchol_stream_t stream) {
   if (f == nullptr || dA == nullptr || lda < f->n) return MPCHOL_ERR_BAD_ARG;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  MPCHOL_CUDA_TRY(cudaMemcpy2DAsync(f->A, sizeof(float) * f->ld, dA, sizeof(float) * lda,
-                                    sizeof(float) * f->n, f->n, cudaMemcpyDeviceToDevice, s));
+  MPCHOL_CUDA_TRY(copy_lower_blocks(f->A, f->ld, dA, lda, f->n, f->b, cudaMemcpyDeviceToDevice, s));
   return run_factor(f, s);
+}
+
+mpchol_status mpchol_solve_host(mpchol_factor_t* f, const float* hA, int lda, const double* hB,
+                                double* hX, int nrhs, const mpchol_pcg_opts* opts,
+                                mpchol_report* rep, mpchol_stream_t stream) {
+  if (f == nullptr || hA == nullptr || hB == nullptr || hX == nullptr || lda < f->n ||
+      nrhs < 1 || nrhs > 8)
+    return MPCHOL_ERR_BAD_ARG;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const int n = f->n;
+  if (f->op == nullptr) {
+    MPCHOL_CUDA_TRY(dmalloc(&f->op, (size_t)f->ld * n));
+    MPCHOL_CUDA_TRY(dmalloc(&f->hb, (size_t)n * 8));
+    MPCHOL_CUDA_TRY(dmalloc(&f->hx, (size_t)n * 8));
+  }
+  MPCHOL_CUDA_TRY(copy_lower_blocks(f->op, f->ld, hA, lda, n, f->b, cudaMemcpyHostToDevice, s));
+  MPCHOL_CUDA_TRY(cudaMemcpyAsync(f->hb, hB, sizeof(double) * n * nrhs, cudaMemcpyHostToDevice, s));
+  MPCHOL_CUDA_TRY(copy_lower_blocks(f->A, f->ld, f->op, f->ld, n, f->b, cudaMemcpyDeviceToDevice, s));
+  mpchol_status st = run_factor(f, s);
+  if (st != MPCHOL_OK) return st;
+  st = run_pcg<float>(f, f->op, f->ld, f->hb, f->hx, nrhs, opts, rep, s);
+  if (st != MPCHOL_OK && st != MPCHOL_PCG_MAXIT) return st;
+  MPCHOL_CUDA_TRY(cudaMemcpyAsync(hX, f->hx, sizeof(double) * n * nrhs, cudaMemcpyDeviceToHost, s));
+  MPCHOL_CUDA_TRY(cudaStreamSynchronize(s));
+  return st;
 }
 
 mpchol_status mpchol_factor(const mpchol_opts* opts, int n, const float* dA, int lda,

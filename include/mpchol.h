@@ -181,6 +181,22 @@ MPCHOL_API mpchol_status mpchol_pcg(mpchol_factor_t* f, const float* dA, int lda
 MPCHOL_API mpchol_status mpchol_pcg_f64(mpchol_factor_t* f, const double* dA, int lda, const double* dB,
                              double* dX, int nrhs, const mpchol_pcg_opts* opts,
                              mpchol_report* report, mpchol_stream_t stream);
+/* Factor and solve from host memory: the step precond_CG
+ * (src/mixed_cholesky.cu:76-229) performs on device buffers, for a caller
+ * whose matrix and right-hand sides are in host memory.  hA: FP32 symmetric,
+ * column-major, leading dimension lda; only its lower triangle is read, and
+ * only that part is copied to the device (the diagonal-down part of each
+ * block column, about half of A, one 2-D copy per block column), once into an
+ * operator buffer the factor object keeps and once, device to device, into
+ * the factor's storage.  hB / hX: n x nrhs FP64 (ld = n), nrhs 1..8.
+ * Page-locked host buffers let the copies run at full link speed.  The first
+ * call on a factor object allocates the operator and vector buffers (n x lda
+ * FP32, 2 x n x 8 FP64); later calls allocate nothing.  Returns like
+ * mpchol_pcg; the stream is synchronized before returning. */
+MPCHOL_API mpchol_status mpchol_solve_host(mpchol_factor_t* f, const float* hA, int lda,
+                                           const double* hB, double* hX, int nrhs,
+                                           const mpchol_pcg_opts* opts, mpchol_report* report,
+                                           mpchol_stream_t stream);
 /* dZ = (L L^T)^-1 dR for nrhs vectors (n x nrhs, ld = n), i.e. Dpotrs
  * (src/mixed_cholesky.cu:204-206) on the FP32 factor with FP64 vectors. */
 MPCHOL_API mpchol_status mpchol_apply_precond(mpchol_factor_t* f, const double* dR, double* dZ, int nrhs,

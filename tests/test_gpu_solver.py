@@ -188,3 +188,28 @@ def test_reference_shaped_switching_chol(cuda):
     L64 = np.linalg.cholesky(A.double().numpy())
     assert np.linalg.norm(Lg - L64) / np.linalg.norm(L64) < 2e-3
     np.testing.assert_allclose(d.cpu().numpy(), np.diag(A.numpy()))
+
+
+@pytest.mark.parametrize("n,nrhs", [(1000, 2), (768, 1)])
+def test_solve_host_matches_device_path(cuda, n, nrhs):
+    """mpchol_solve_host (host buffers, lower triangle copied by block columns)
+    gives the device path's solution: same factor, same operator, same PCG
+    iteration count.  The solutions agree to 1e-8 relative: the operator and
+    preconditioner products combine partial sums with FP64 atomics, whose
+    order varies from run to run (differences ~1e-10 relative)."""
+    A = matgen.spd_matrix(n, 1e4, 41)
+    B = matgen.rhs(n, nrhs, 42).to(torch.float64)
+    opts = dict(block_size=256, precision="switching", eps_prime=1e-5,
+                ladder=["e4m3", "fp16", "fp16x2"])
+    f_dev = mp.Factor(n, **opts)
+    f_dev.compute(A.cuda())
+    Xd, rd = f_dev.pcg(A.cuda(), B.cuda(), rel_tol=1e-10)
+    f_host = mp.Factor(n, **opts)
+    for _ in range(2):   # the second call reuses the buffers the first allocated
+        Xh, rh = f_host.solve_host(A.pin_memory(), B.pin_memory(), rel_tol=1e-10)
+        assert rh.converged and rh.iterations == rd.iterations
+        assert Xh.device.type == "cpu" and Xh.shape == B.shape
+        err = np.linalg.norm(Xh.numpy() - Xd.cpu().numpy()) / np.linalg.norm(Xd.cpu().numpy())
+        assert err < 1e-8, err
+    xd = O.dense_solve(A.numpy().astype(np.float64), B.numpy())
+    assert np.linalg.norm(Xh.numpy() - xd) / np.linalg.norm(xd) < 1e-6
