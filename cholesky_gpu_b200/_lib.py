@@ -121,6 +121,7 @@ SIGNATURES = {
     "mpchol_pcg": (_i, [_vp, _vp, _i, _vp, _vp, _i, ctypes.POINTER(PcgOpts), ctypes.POINTER(Report), _vp]),
     "mpchol_pcg_f64": (_i, [_vp, _vp, _i, _vp, _vp, _i, ctypes.POINTER(PcgOpts), ctypes.POINTER(Report), _vp]),
     "mpchol_solve_host": (_i, [_vp, _vp, _i, _vp, _vp, _i, ctypes.POINTER(PcgOpts), ctypes.POINTER(Report), _vp]),
+    "mpchol_factor_codes": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp]),
     "mpchol_apply_precond": (_i, [_vp, _vp, _vp, _i, _vp]),
     "mpchol_symv": (_i, [_vp, _i, _i, _vp, _vp, _i, _vp]),
     "mpchol_precond_cg": (_i, [_vp, _vp, _vp, _i, _i, _d, _f, _f, _i, _i, _d, _i, _vp]),

@@ -123,6 +123,30 @@ class Factor:
         del nbytes
         return buf[:, : self.n].t().tril()
 
+    def panel_codes(self, fmt: int):
+        """The last trailing update's quantized panel in format fmt (a step
+        candidate): (codes, scales, col0) as host numpy arrays; codes are rows x
+        block (FP16X2: hi rows then lo rows, as uint16), scales int8 per row or
+        (MXFP8) uint8 rows x block/32.  The panel covers L[col0+block:, col0:col0+block]."""
+        import numpy as np
+        pc, ps = ctypes.c_void_p(), ctypes.c_void_p()
+        ldq, rows, col0 = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(self.lib.mpchol_factor_codes(self.handle, fmt, ctypes.byref(pc), ctypes.byref(ps),
+                                           ctypes.byref(ldq), ctypes.byref(rows),
+                                           ctypes.byref(col0)), "mpchol_factor_codes")
+        torch.cuda.current_stream().synchronize()
+        k, m = ldq.value, rows.value
+        if fmt in (_lib.PREC_FP16, _lib.PREC_FP16X2):
+            nrow = 2 * m if fmt == _lib.PREC_FP16X2 else m
+            codes = _wrap_device(pc.value, (nrow, k), torch.int16).cpu().numpy().view(np.uint16)
+        else:
+            codes = _wrap_device(pc.value, (m, k), torch.uint8).cpu().numpy()
+        if fmt == _lib.PREC_MXFP8:
+            scales = _wrap_device(ps.value, (m, k // 32), torch.uint8).cpu().numpy()
+        else:
+            scales = _wrap_device(ps.value, (m,), torch.int8).cpu().numpy()
+        return codes, scales, col0.value
+
     def diags(self) -> tuple[torch.Tensor, torch.Tensor]:
         pd = ctypes.c_void_p()
         pt = ctypes.c_void_p()
@@ -214,7 +238,8 @@ def _wrap_device(ptr: int, shape: tuple, dtype: torch.dtype) -> torch.Tensor:
     class _Holder:
         __cuda_array_interface__ = {
             "shape": tuple(shape),
-            "typestr": {torch.float32: "<f4", torch.float64: "<f8"}[dtype],
+            "typestr": {torch.float32: "<f4", torch.float64: "<f8", torch.uint8: "|u1",
+                        torch.int8: "|i1", torch.int16: "<i2"}[dtype],
             "data": (ptr, False),
             "version": 3,
             "strides": None,

@@ -728,6 +728,30 @@ mpchol_status mpchol_factor_compute(mpchol_factor_t* f, const float* dA, int lda
   return run_factor(f, s);
 }
 
+mpchol_status mpchol_factor_codes(const mpchol_factor_t* f, int fmt, const void** dCodes,
+                                  const void** dScales, int* ldq, int* rows, int* col0) {
+  if (f == nullptr || dCodes == nullptr || dScales == nullptr || ldq == nullptr ||
+      rows == nullptr || col0 == nullptr)
+    return MPCHOL_ERR_BAD_ARG;
+  if (f->nsteps < 2) return MPCHOL_ERR_BAD_ARG;          // no trailing update
+  if (fmt != FP16 && fmt != FP16X2 && fmt != E4M3 && fmt != E5M2 && fmt != MXFP8)
+    return MPCHOL_ERR_BAD_ARG;
+  const int s = (f->nsteps - 2) * f->b;                   // the last step with trailing rows
+  const size_t nb = (size_t)f->n * f->b;
+  if (fmt == FP16 || fmt == FP16X2) {
+    *dCodes = f->q16;
+    *dScales = f->rexp + 2 * (size_t)f->n;
+  } else {
+    *dCodes = f->q8 + q8_slot(fmt) * nb;
+    *dScales = fmt == MXFP8 ? static_cast<const void*>(f->mxexp)
+                            : static_cast<const void*>(f->rexp + (size_t)rexp_slot(fmt) * f->n);
+  }
+  *ldq = f->b;
+  *rows = f->n - s - f->b;
+  *col0 = s;
+  return MPCHOL_OK;
+}
+
 mpchol_status mpchol_solve_host(mpchol_factor_t* f, const float* hA, int lda, const double* hB,
                                 double* hX, int nrhs, const mpchol_pcg_opts* opts,
                                 mpchol_report* rep, mpchol_stream_t stream) {

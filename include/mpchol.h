@@ -162,6 +162,15 @@ MPCHOL_API mpchol_status mpchol_factor_info_get(const mpchol_factor_t* f, mpchol
                                      int* hStepPrec, int* hStepFp64, mpchol_stream_t stream);
 /* Device pointer to the factor L (lower triangle valid; upper unspecified). */
 MPCHOL_API mpchol_status mpchol_factor_lower(const mpchol_factor_t* f, const float** dL, int* ldl, int* n);
+/* Inspection of the last trailing update's quantized panel (the codes the
+ * panel solve of the factorization's last step wrote for format fmt, one of
+ * the step's candidates): dCodes, K-major, *rows rows of *ldq codes (FP16X2:
+ * the hi rows, then the lo rows), and dScales (per-row pow-2 exponents, int8,
+ * or for MXFP8 *ldq/32 E8M0 bytes per row).  The panel holds L's rows
+ * [*col0 + ldq, n) of columns [*col0, *col0 + ldq).  No counterpart in the
+ * reference: it lets tests check the fused quantization against the oracle. */
+MPCHOL_API mpchol_status mpchol_factor_codes(const mpchol_factor_t* f, int fmt, const void** dCodes,
+                                             const void** dScales, int* ldq, int* rows, int* col0);
 /* Device pointers to the tracked diagonals d (original) and dtilde (Schur). */
 MPCHOL_API mpchol_status mpchol_factor_diags(const mpchol_factor_t* f, const float** dD, const float** dDtilde);
 /* Prepare the solve-side data (diagonal-block inverses).  Called implicitly

@@ -178,3 +178,25 @@ def test_symv_matches_fp64(cuda, n, nrhs):
     got = Yd.cpu().numpy().T
     want = A.astype(np.float64) @ X
     assert np.abs(got - want).max() / np.abs(want).max() < 1e-13
+
+
+@pytest.mark.parametrize("n", [640, 1000])
+def test_fused_panel_codes_match_oracle(cuda, n):
+    """The panel solve writes the step's panel in every candidate format from
+    shared memory; those codes and scales must equal the oracle's quantization
+    of the solved panel (read back from L) bit for bit.  n = 1000 leaves a
+    partial 32-row slab at the bottom of the panel."""
+    import cholesky_gpu_b200 as mp
+    A = matgen.spd_matrix(n, 1e3, 17)
+    f = mp.Factor(n, block_size=256, precision="switching", eps_prime=1e-5,
+                  ladder=["e4m3", "e5m2", "mxfp8", "fp16x2"])
+    f.compute(A.cuda())
+    L = f.lower().cpu().numpy()
+    for fmt in (O.E4M3, O.E5M2, O.MXFP8, O.FP16X2):
+        codes, scales, s0 = f.panel_codes(fmt)
+        P = np.ascontiguousarray(L[s0 + 256:, s0:s0 + 256])
+        wc, ws = O.quantize_rows(P, fmt)
+        assert codes.shape == wc.shape
+        bad = np.nonzero(codes != wc)
+        assert bad[0].size == 0, (fmt, bad[0][:5], bad[1][:5])
+        assert np.array_equal(scales.astype(np.int32), ws.astype(np.int32)), fmt
