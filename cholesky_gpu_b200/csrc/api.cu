@@ -419,6 +419,10 @@ mpchol_status run_pcg(mpchol_factor_t* f, const TA* dA, int lda, const double* d
   double* part_rr = part_pAp + (size_t)VG * 8;
   double* part_rz = part_rr + (size_t)VG * 8;
   double* part_misc = part_rz + (size_t)VG * 8;
+  // shares of ||A||_F^2 (for the backward error), filled by the first
+  // operator product when it streams A through the staged kernel
+  double* part_fro = part_misc + (size_t)VG * 8;
+  const bool fro_fused = symv_staged_ok(dA, lda);
   double* rho[2] = {f->scal, f->scal + 8};
   double* alpha = f->scal + 16;
   double* bnorm2 = f->scal + 24;
@@ -444,7 +448,8 @@ mpchol_status run_pcg(mpchol_factor_t* f, const TA* dA, int lda, const double* d
   const int max_restarts = 3;
   for (int restart = 0;; ++restart) {
     // r = b - A x ; z = M^-1 r ; p = z ; rho = r^T z
-    PHASE(MPCHOL_PH_SYMV, 1, stream, launch_symv_skip<TA>(dA, lda, n, x, Ap, nr, nullptr, stream));
+    PHASE(MPCHOL_PH_SYMV, 1, stream, launch_symv_skip<TA>(dA, lda, n, x, Ap, nr, nullptr, stream,
+                                                          fro_fused ? part_fro : nullptr, VG));
     PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_residual(bb, Ap, r, n, nr, part_rr, stream));
     PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_reduce_partials(part_rr, misc, nr, stream));
     // convergence of the true residual
@@ -551,8 +556,12 @@ mpchol_status run_pcg(mpchol_factor_t* f, const TA* dA, int lda, const double* d
   if (rep != nullptr) {
     PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_dot(x, x, n, nr, part_misc, nullptr, stream));
     PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_reduce_partials(part_misc, misc + 8, nr, stream));
-    PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_frob_lower<TA>(dA, lda, n, part_misc, stream));
-    PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_reduce_partials(part_misc, misc + 16, 1, stream));
+    if (fro_fused) {
+      PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_reduce_partials(part_fro, misc + 16, 1, stream));
+    } else {
+      PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_frob_lower<TA>(dA, lda, n, part_misc, stream));
+      PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_reduce_partials(part_misc, misc + 16, 1, stream));
+    }
     PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_dot(r, z, n, nr, part_rz, nullptr, stream));
     PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_reduce_partials(part_rz, misc + 24, nr, stream));
     MPCHOL_CUDA_TRY(cudaMemcpyAsync(f->h_scal, misc, sizeof(double) * 32, cudaMemcpyDeviceToHost, stream));
@@ -694,7 +703,7 @@ mpchol_status mpchol_factor_create(const mpchol_opts* opts, int n, mpchol_factor
             dmalloc(&f->wsup, solve_wsup_elems(n)) == cudaSuccess &&
             dmalloc(&f->trsv_ctr, trsv_counter_ints(n)) == cudaSuccess &&
             dmalloc(&f->vec, 8 * nv) == cudaSuccess &&
-            dmalloc(&f->partials, (size_t)4 * pcg_vgrid() * 8) == cudaSuccess &&
+            dmalloc(&f->partials, (size_t)5 * pcg_vgrid() * 8) == cudaSuccess &&
             dmalloc(&f->scal, 64) == cudaSuccess && dmalloc(&f->done, 2) == cudaSuccess &&
             cudaMallocHost(reinterpret_cast<void**>(&f->h_done), 2 * sizeof(int)) == cudaSuccess &&
             cudaMallocHost(reinterpret_cast<void**>(&f->h_scal), sizeof(double) * 64) == cudaSuccess;

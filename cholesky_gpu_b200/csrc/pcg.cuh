@@ -14,7 +14,12 @@ size_t solve_wsup_elems(int n);
 int solve_setup_launches(int n);
 template <typename TA>
 cudaError_t launch_symv_skip(const TA* A, int lda, int n, const double* x, double* y, int nrhs,
-                             const int* skip, cudaStream_t stream);
+                             const int* skip, cudaStream_t stream, double* fro = nullptr,
+                             int nfro = 0);
+// True when launch_symv_skip streams A through the staged kernel (FP32, 16-byte
+// aligned columns); only then does it fill `fro` (per-CTA shares of ||A||_F^2).
+template <typename TA>
+bool symv_staged_ok(const TA* A, int lda);
 // 128-block inverses into winv, then the super-block inverses into wsup.
 cudaError_t launch_solve_setup(const float* L, int ldl, int n, float* wsup, cudaStream_t stream);
 // out = L^-1 in (forward) or L^-T in (backward); work is an n x nrhs scratch.

@@ -270,10 +270,13 @@ __device__ __forceinline__ void stage_vec(const double* x, int n, int row0, int 
 // tile_pass on a staged tile.  Each lane widens its 4 x SCH chunk to FP64
 // once and uses it for every rhs of both products.  DIAG: a diagonal tile of
 // a symmetric operator stored lower -- NOTRANS keeps r >= c, TRANS r > c.
-template <int NR, bool DIAG>
+// FRO: also adds the tile's share of ||A||_F^2 to *fsq (the lower triangle,
+// off-diagonal entries twice).
+template <int NR, bool DIAG, bool FRO = false>
 __device__ __forceinline__ void tile_pass_staged(const float* Ts, const double* vin_cols,
                                                  const double* vin_rows, double (&acc)[4][NR],
-                                                 double* colsum_smem, bool do_nt, bool do_t) {
+                                                 double* colsum_smem, bool do_nt, bool do_t,
+                                                 double* fsq = nullptr) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int rloc = 4 * lane;
   constexpr int LOWBITS = 3;   // lanes holding the same column sum (SCH = 8)
@@ -289,6 +292,11 @@ __device__ __forceinline__ void tile_pass_staged(const float* Ts, const double* 
 #pragma unroll
         for (int r = 0; r < 4; ++r)
           if (rloc + r < c) dv[cc][r] = 0.0;
+      }
+      if (FRO) {
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+          *fsq = fma((DIAG && rloc + r == c) ? dv[cc][r] : 2.0 * dv[cc][r], dv[cc][r], *fsq);
       }
     }
     if (do_nt) {
@@ -345,10 +353,12 @@ constexpr size_t symv_staged_smem() {
 // CTA b takes tiles b, b + grid, ...; each tile is staged symv_stages - 1
 // tiles ahead together with its two vector segments.  The row partials are
 // reduced in the stage's own tile buffer once the tile has been used.
+// fro != nullptr: CTA b also writes its share of ||A||_F^2 (lower triangle,
+// off-diagonal entries twice) to fro[b] and zeroes fro[gridDim.x ..nfro).
 template <int NR>
 __global__ void __launch_bounds__(NTH, 1)
 symv_staged_kernel(const float* __restrict__ A, int lda, int n, const double* __restrict__ x,
-                   double* __restrict__ y, const int* skip) {
+                   double* __restrict__ y, const int* skip, double* fro, int nfro) {
   if (skip != nullptr && *skip) return;
   constexpr int STAGES = symv_stages<NR>();
   constexpr int VEC = RB * NR;
@@ -374,6 +384,7 @@ symv_staged_kernel(const float* __restrict__ A, int lda, int n, const double* __
     cp_async_commit();
   }
   int stage = 0;
+  double fsq = 0.0;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     {
       const int tn = t + (STAGES - 1) * gridDim.x;
@@ -390,8 +401,13 @@ symv_staged_kernel(const float* __restrict__ A, int lda, int n, const double* __
     const double* xJ = vecs + (2 * stage) * VEC;
     const double* xI = xJ + VEC;
     double acc[4][NR] = {};
-    if (I == J) tile_pass_staged<NR, true>(Ts, xJ, xI, acc, s_col, true, true);
-    else tile_pass_staged<NR, false>(Ts, xJ, xI, acc, s_col, true, true);
+    if (fro != nullptr) {
+      if (I == J) tile_pass_staged<NR, true, true>(Ts, xJ, xI, acc, s_col, true, true, &fsq);
+      else tile_pass_staged<NR, false, true>(Ts, xJ, xI, acc, s_col, true, true, &fsq);
+    } else {
+      if (I == J) tile_pass_staged<NR, true>(Ts, xJ, xI, acc, s_col, true, true);
+      else tile_pass_staged<NR, false>(Ts, xJ, xI, acc, s_col, true, true);
+    }
     __syncthreads();
     for (int e = threadIdx.x; e < VEC; e += NTH) {
       const int k = e / RB, c = e % RB;
@@ -402,6 +418,22 @@ symv_staged_kernel(const float* __restrict__ A, int lda, int n, const double* __
     stage = (stage + 1) % STAGES;
   }
   cp_async_wait<0>();
+  if (fro != nullptr) {
+    // block sum in a fixed order: warps, then the CTA's warps in turn
+    double v = fsq;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    double* wsum = reinterpret_cast<double*>(tiles);   // the stages are free
+    if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < NTH / 32; ++w) t += wsum[w];
+      fro[blockIdx.x] = t;
+    }
+    for (int e = gridDim.x + blockIdx.x; e < nfro; e += gridDim.x)
+      if (threadIdx.x == 0) fro[e] = 0.0;
+  }
 }
 
 // ---- y += A x, symmetric A, lower triangle only (one CTA per lower tile) ----
@@ -1121,24 +1153,30 @@ int sm_count() {
 // the staged persistent kernel; others (and FP64 operators) take one CTA per
 // tile with register loads.
 template <typename TA>
+bool symv_staged_ok(const TA* A, int lda) {
+  return sizeof(TA) == 4 && (reinterpret_cast<uintptr_t>(A) & 15) == 0 && lda % 4 == 0;
+}
+template bool symv_staged_ok<float>(const float*, int);
+template bool symv_staged_ok<double>(const double*, int);
+
+template <typename TA>
 cudaError_t launch_symv_skip(const TA* A, int lda, int n, const double* x, double* y, int nrhs,
-                             const int* skip, cudaStream_t stream) {
+                             const int* skip, cudaStream_t stream, double* fro, int nfro) {
   const long long cnt = (long long)n * nrhs;
   zero_vec_kernel<<<148, 256, 0, stream>>>(y, cnt, skip);
   const int T = ceil_div(n, RB);
   const int ntiles = T * (T + 1) / 2;
-  const bool staged = sizeof(TA) == 4 && (reinterpret_cast<uintptr_t>(A) & 15) == 0 && lda % 4 == 0;
-  if (staged) {
+  if (symv_staged_ok(A, lda)) {
     const int grid = std::min(ntiles, sm_count());
     const float* Af = reinterpret_cast<const float*>(A);
-    NR_SWITCH(nrhs, (symv_staged_kernel<NRC><<<grid, NTH, symv_staged_smem<NRC>(), stream>>>(Af, lda, n, x, y, skip)));
+    NR_SWITCH(nrhs, (symv_staged_kernel<NRC><<<grid, NTH, symv_staged_smem<NRC>(), stream>>>(Af, lda, n, x, y, skip, fro, nfro)));
   } else {
     NR_SWITCH(nrhs, (symv_kernel<TA, NRC><<<ntiles, NTH, red_bytes(NRC), stream>>>(A, lda, n, x, y, skip)));
   }
   return cudaGetLastError();
 }
-template cudaError_t launch_symv_skip<float>(const float*, int, int, const double*, double*, int, const int*, cudaStream_t);
-template cudaError_t launch_symv_skip<double>(const double*, int, int, const double*, double*, int, const int*, cudaStream_t);
+template cudaError_t launch_symv_skip<float>(const float*, int, int, const double*, double*, int, const int*, cudaStream_t, double*, int);
+template cudaError_t launch_symv_skip<double>(const double*, int, int, const double*, double*, int, const int*, cudaStream_t, double*, int);
 
 cudaError_t launch_solve_setup(const float* L, int ldl, int n, float* wsup, cudaStream_t stream) {
   const size_t inv = (size_t)RB * BLD * (sizeof(double) + sizeof(float));

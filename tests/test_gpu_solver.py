@@ -213,3 +213,21 @@ def test_solve_host_matches_device_path(cuda, n, nrhs):
         assert err < 1e-8, err
     xd = O.dense_solve(A.numpy().astype(np.float64), B.numpy())
     assert np.linalg.norm(Xh.numpy() - xd) / np.linalg.norm(xd) < 1e-6
+
+
+@pytest.mark.parametrize("n", [1000, 999])
+def test_reported_backward_error_matches_numpy(cuda, n):
+    """The report's backward error ||b - Ax|| / (||A||_F ||x|| + ||b||) matches
+    numpy's.  n = 1000 takes ||A||_F from the first operator product (staged
+    SYMV, columns 16-byte aligned); n = 999 (odd leading dimension) from the
+    separate norm kernel."""
+    A = matgen.spd_matrix(n, 1e4, 31)
+    b = matgen.rhs(n, 1, 32)
+    f = mp.factor(A.cuda(), block_size=256, precision="fp16x2")
+    X, rep = f.pcg(A.cuda(), b.cuda(), rel_tol=1e-10)
+    assert rep.converged
+    A64 = A.double().numpy()
+    x = X.cpu().numpy()
+    bb = b.numpy()
+    be = np.linalg.norm(bb - A64 @ x) / (np.linalg.norm(A64) * np.linalg.norm(x) + np.linalg.norm(bb))
+    assert rep.backward_error == pytest.approx(be, rel=0.05), (rep.backward_error, be)
