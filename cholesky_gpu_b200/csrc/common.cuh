@@ -83,6 +83,18 @@ __device__ __forceinline__ uint8_t f32_to_e5m2(float x) {
 __device__ __forceinline__ uint16_t f32_to_f16(float x) {
   return __half_as_ushort(__float2half_rn(x));
 }
+// Two elements per conversion (low half / byte = a), rounded as the scalar
+// forms above.
+__device__ __forceinline__ uint32_t f32x2_to_f16x2(float a, float b) {
+  const __half2 h = __floats2half2_rn(a, b);
+  return *reinterpret_cast<const uint32_t*>(&h);
+}
+__device__ __forceinline__ uint16_t f32x2_to_e4m3x2(float a, float b) {
+  return (uint16_t)__nv_cvt_float2_to_fp8x2(make_float2(a, b), __NV_SATFINITE, __NV_E4M3);
+}
+__device__ __forceinline__ uint16_t f32x2_to_e5m2x2(float a, float b) {
+  return (uint16_t)__nv_cvt_float2_to_fp8x2(make_float2(a, b), __NV_SATFINITE, __NV_E5M2);
+}
 
 // Unit roundoff of each storage format (used by the switching criterion).
 __host__ __device__ __forceinline__ float unit_roundoff(int fmt) {

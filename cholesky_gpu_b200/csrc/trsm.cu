@@ -148,11 +148,12 @@ __device__ void quantize_slab(const float* Xs, int bs, int nrows, int gi0, int m
     const float inv = pow2f(-e);
     for (int c = c0; c < c0 + cw; c += 2) {
       const float x0 = Xs[c * XLD + r] * inv, x1 = Xs[(c + 1) * XLD + r] * inv;
-      const __half h0 = __float2half_rn(x0), h1 = __float2half_rn(x1);
-      hi[r * sw + c / 2] = (uint32_t)__half_as_ushort(h0) | ((uint32_t)__half_as_ushort(h1) << 16);
-      if (fmt == FP16X2)   // x - hi is exact in FP32
-        lo[r * sw + c / 2] = (uint32_t)f32_to_f16(x0 - __half2float(h0)) |
-                             ((uint32_t)f32_to_f16(x1 - __half2float(h1)) << 16);
+      const __half2 h = __floats2half2_rn(x0, x1);
+      hi[r * sw + c / 2] = *reinterpret_cast<const uint32_t*>(&h);
+      if (fmt == FP16X2) {   // x - hi is exact in FP32
+        const float2 hf = __half22float2(h);
+        lo[r * sw + c / 2] = f32x2_to_f16x2(x0 - hf.x, x1 - hf.y);
+      }
     }
     if (live && part == 0) qa.rexp[2][gi] = (int8_t)e;
     __syncthreads();
@@ -182,14 +183,12 @@ __device__ void quantize_slab(const float* Xs, int bs, int nrows, int gi0, int m
         if (live) qa.mxexp[(size_t)gi * qa.ldmx + cb / 32] = (uint8_t)(eb + 127);
       }
       for (int c = cb; c < cb + 32; c += 4) {
-        uint32_t w = 0;
+        float x[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const float x = Xs[(c + u) * XLD + r] * inv;
-          const uint8_t code = (fmt == E5M2) ? f32_to_e5m2(x) : f32_to_e4m3(x);
-          w |= (uint32_t)code << (8 * u);
-        }
-        stage[r * sw + c / 4] = w;
+        for (int u = 0; u < 4; ++u) x[u] = Xs[(c + u) * XLD + r] * inv;
+        const uint32_t w01 = (fmt == E5M2) ? f32x2_to_e5m2x2(x[0], x[1]) : f32x2_to_e4m3x2(x[0], x[1]);
+        const uint32_t w23 = (fmt == E5M2) ? f32x2_to_e5m2x2(x[2], x[3]) : f32x2_to_e4m3x2(x[2], x[3]);
+        stage[r * sw + c / 4] = w01 | (w23 << 16);
       }
     }
     __syncthreads();
