@@ -241,10 +241,10 @@ cudaError_t copy_lower_blocks(float* dst, int ldd, const float* src, int lds, in
 
 // One factorization of f->A in place, on `stream`, right-looking with a
 // look-ahead of one block.  Step k: the panel solve (with the step decision
-// and the panel quantization), then the trailing update of the tile columns
-// that hold block k+1 (SEL_NEXT), then -- on the caller's stream -- the
-// POTRF of block k+1, while the rest of step k's update runs on the aux
-// stream on all SMs but one.  The panel solve of step k+1 waits for that
+// and the panel quantization), then the trailing update of the tiles of
+// diagonal block k+1 (SEL_NEXT), then -- on the caller's stream -- the POTRF
+// of block k+1, while the rest of step k's update (block k+1's panel
+// included) runs on the aux stream on all SMs but one.  The panel solve of step k+1 waits for that
 // rest.  Every C tile receives the same updates in the same order as
 // without the split, so the factor is unchanged by it.
 mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream) {
@@ -344,7 +344,7 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream) {
                             stream));
     const int jc = ceil_div(next_bs, 128);   // 128-tile columns of block k+1
     if ((rs = syrk(k, TileSel{SEL_NEXT, jc}, 0, stream)) != MPCHOL_OK) return rs;
-    if (ceil_div(m, 128) > jc) {
+    if (sel_tile_count(ceil_div(m, 128), TileSel{SEL_REST, jc}) > 0) {
       MPCHOL_CUDA_TRY(cudaEventRecord(f->ev_next, stream));
       MPCHOL_CUDA_TRY(cudaStreamWaitEvent(f->aux, f->ev_next, 0));
       if ((rs = syrk(k, TileSel{SEL_REST, jc}, cap, f->aux)) != MPCHOL_OK) return rs;

@@ -84,10 +84,12 @@ cudaError_t launch_quantize_hash(unsigned long long first, unsigned long long co
 
 // ---- trailing update ----------------------------------------------------
 // Which lower 128 x 128 tiles (I >= J) of the trailing block C a launch
-// updates: all of them, only the tile columns J < jc that hold the next
-// diagonal block and its panel (SEL_NEXT), or the rest, J >= jc (SEL_REST).
-// Splitting a step's update this way lets the next diagonal block be factored
-// while the rest of the update runs (look-ahead).
+// updates: all of them, only the tiles of the next diagonal block (I, J < jc:
+// SEL_NEXT), or the rest (I >= jc: SEL_REST), which includes the next
+// block's panel.  Splitting a step's update this way lets the next diagonal
+// block be factored while the rest of the update runs (look-ahead).  The
+// tiles are numbered along the rows of the lower triangle, so SEL_NEXT is
+// the first jc(jc+1)/2 of them and SEL_REST the remainder.
 enum TileSelMode { SEL_ALL = 0, SEL_NEXT = 1, SEL_REST = 2 };
 struct TileSel {
   int mode;
@@ -96,34 +98,25 @@ struct TileSel {
 constexpr TileSel kAllTiles{SEL_ALL, 0};
 
 __host__ __device__ inline int sel_tile_count(int T, TileSel s) {
-  if (s.mode == SEL_NEXT) {
-    int c = 0;
-    for (int j = 0; j < s.jc && j < T; ++j) c += T - j;
-    return c;
-  }
-  if (s.mode == SEL_REST) {
-    const int r = T - s.jc;
-    return r > 0 ? r * (r + 1) / 2 : 0;
-  }
-  return T * (T + 1) / 2;
+  const int all = T * (T + 1) / 2;
+  const int j = s.jc < T ? s.jc : T;
+  const int head = j * (j + 1) / 2;
+  if (s.mode == SEL_NEXT) return head;
+  if (s.mode == SEL_REST) return all - head;
+  return all;
 }
 
-// Tile t of the selection -> (I, J).  SEL_NEXT runs down tile column 0, then
-// column 1, ...; the others run along the rows of the lower triangle.
+// Tile t of the selection -> (I, J).
 __device__ __forceinline__ void sel_tile(int t, TileSel s, int T, int& I, int& J) {
-  if (s.mode == SEL_NEXT) {
-    int j = 0;
-    while (t >= T - j) { t -= T - j; ++j; }
-    J = j;
-    I = j + t;
-    return;
+  if (s.mode == SEL_REST) {
+    const int j = s.jc < T ? s.jc : T;
+    t += j * (j + 1) / 2;
   }
   int i = (int)((sqrtf(8.0f * t + 1.0f) - 1.0f) * 0.5f);
   while (i * (i + 1) / 2 > t) --i;
   while ((i + 1) * (i + 2) / 2 <= t) ++i;
   I = i;
   J = t - i * (i + 1) / 2;
-  if (s.mode == SEL_REST) { I += s.jc; J += s.jc; }
 }
 
 // FP32 SIMT SYRK: C(m x m, lower) -= P P^T, P = m x k column-major (ldp),

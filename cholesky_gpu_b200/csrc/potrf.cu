@@ -250,15 +250,22 @@ __device__ void potrf_block(const CUtensorMap* tmap, T* tiles, float* A, int lda
     s_pmin[i] = pm;
   }
   if (TMA) {
-    // stage the lower tiles with TMA; rows/columns past n arrive as zeros
-    if (tid == 0) {
-      tc::mbar_init(&bar, 1);
-      tc::fence_mbar_init();
-      tc::mbar_expect_tx(&bar, (uint32_t)(ntiles * TSZ * sizeof(float)));
-      for (int I = 0; I < NT; ++I)
-        for (int J = 0; J <= I; ++J)
-          tc::tma_load_2d(tiles + tidx(I, J) * TSZ, tmap, &bar, s + I * TS, s + J * TS);
-      if (!tc::mbar_wait(&bar, 0)) {
+    // stage the lower tiles with TMA (the lanes of warp 0 issue the copies);
+    // rows/columns past n arrive as zeros
+    if (warp == 0) {
+      if (lane == 0) {
+        tc::mbar_init(&bar, 1);
+        tc::fence_mbar_init();
+        tc::mbar_expect_tx(&bar, (uint32_t)(ntiles * TSZ * sizeof(float)));
+      }
+      __syncwarp();
+      for (int t = lane; t < ntiles; t += 32) {
+        int I = 0;
+        while ((I + 1) * (I + 2) / 2 <= t) ++I;
+        const int J = t - I * (I + 1) / 2;
+        tc::tma_load_2d(tiles + t * TSZ, tmap, &bar, s + I * TS, s + J * TS);
+      }
+      if (lane == 0 && !tc::mbar_wait(&bar, 0)) {
         s_ok = 0;
         set_status(st, MPCHOL_ERR_TIMEOUT, s);
         tc::mbar_wait(&bar, 0);
@@ -355,14 +362,17 @@ __device__ void potrf_block(const CUtensorMap* tmap, T* tiles, float* A, int lda
   }
   // write back: TMA stores of the lower tiles (FP32 path), or a coalesced loop
   // that rounds the FP64 tiles to FP32.  The strictly upper part of a
-  // diagonal tile still holds the matrix's own upper-triangle values.
+  // diagonal tile is written back as it was staged; it is never read as data.
   if (TMA) {
     tc::fence_proxy_async_smem();
     __syncthreads();
-    if (tid == 0) {
-      for (int I = 0; I < NT; ++I)
-        for (int J = 0; J <= I; ++J)
-          tc::tma_store_2d(tmap, tiles + tidx(I, J) * TSZ, s + I * TS, s + J * TS);
+    if (warp == 0) {   // the lanes of warp 0 issue the stores
+      for (int t = lane; t < ntiles; t += 32) {
+        int I = 0;
+        while ((I + 1) * (I + 2) / 2 <= t) ++I;
+        const int J = t - I * (I + 1) / 2;
+        tc::tma_store_2d(tmap, tiles + t * TSZ, s + I * TS, s + J * TS);
+      }
       tc::bulk_commit();
     }
   } else {
@@ -378,7 +388,7 @@ __device__ void potrf_block(const CUtensorMap* tmap, T* tiles, float* A, int lda
   for (int J = warp; J < NT; J += nwarps)
     invert_tile<T>(tiles + tidx(J, J) * TSZ, s_inv + J * TS, winv + J * TS * TS, lane);
   if (tid == 0 && s_pert) atomicAdd(&st->perturbed, s_pert);
-  if (TMA && tid == 0) tc::bulk_wait_read();   // smem must outlive the stores' reads
+  if (TMA && warp == 0) tc::bulk_wait_read();   // smem must outlive the stores' reads
   (void)n;
 }
 
