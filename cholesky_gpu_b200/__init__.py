@@ -9,8 +9,10 @@ from ._lib import (  # noqa: F401
     PREC_E4M3, PREC_E5M2, PREC_FP16, PREC_FP32, PREC_MXFP8, PREC_SWITCHING, PREC_NAMES,
     MpcholError, load,
 )
-from .api import Batch, Factor, FactorInfo, Report, factor, precond_CG, solve, switching_chol  # noqa: F401
+from .api import (  # noqa: F401
+    Batch, Factor, FactorInfo, Report, copy_plan, factor, precond_CG, solve, switching_chol,
+)
 from .autograd import RBFSolve, rbf_build, rbf_solve  # noqa: F401
 
 __all__ = ["Factor", "FactorInfo", "Report", "factor", "solve", "precond_CG", "switching_chol",
-           "load", "MpcholError"]
+           "copy_plan", "load", "MpcholError"]

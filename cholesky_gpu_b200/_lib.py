@@ -122,6 +122,8 @@ SIGNATURES = {
     "mpchol_pcg_f64": (_i, [_vp, _vp, _i, _vp, _vp, _i, ctypes.POINTER(PcgOpts), ctypes.POINTER(Report), _vp]),
     "mpchol_solve_host": (_i, [_vp, _vp, _i, _vp, _vp, _i, ctypes.POINTER(PcgOpts), ctypes.POINTER(Report), _vp]),
     "mpchol_factor_codes": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp]),
+    "mpchol_set_copy_plan": (_i, [_vp, _i, _vp, _vp]),
+    "mpchol_copy_plan": (_i, [_i, _i, _vp, _vp, _i]),
     "mpchol_apply_precond": (_i, [_vp, _vp, _vp, _i, _vp]),
     "mpchol_symv": (_i, [_vp, _i, _i, _vp, _vp, _i, _vp]),
     "mpchol_precond_cg": (_i, [_vp, _vp, _vp, _i, _i, _d, _f, _f, _i, _i, _d, _i, _vp]),

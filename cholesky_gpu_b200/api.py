@@ -167,12 +167,28 @@ class Factor:
         Z = Z.t()
         return Z.reshape(R.shape) if R.dim() == 1 else Z
 
+    def set_copy_plan(self, cuts=None, join=None) -> None:
+        """Fix the copy groups of solve_host: cuts (block columns where groups
+        start, increasing) and join (the step at which each later group joins
+        the trailing updates); cuts=[] copies all of A before factoring, None
+        restores the automatic plan."""
+        if cuts is None:
+            check(self.lib.mpchol_set_copy_plan(self.handle, 0, None, None), "mpchol_set_copy_plan")
+            return
+        ng = len(cuts) + 1
+        if join is None or len(join) != len(cuts):
+            raise ValueError("join needs one step per cut")
+        c = (ctypes.c_int * max(1, len(cuts)))(*cuts)
+        j = (ctypes.c_int * max(1, len(join)))(*join)
+        check(self.lib.mpchol_set_copy_plan(self.handle, ng, c, j), "mpchol_set_copy_plan")
+
     def solve_host(self, A: torch.Tensor, B: torch.Tensor, rel_tol: float = 1e-10,
                    max_it: int = 200, x0_precond: bool = True,
                    check_every: int = 4) -> tuple[torch.Tensor, Report]:
         """Factor A and solve A X = B with A (FP32) and B (FP64, n or n x nrhs)
         in host memory (page-locked for full-speed copies).  Only A's lower
-        triangle reaches the device.  Returns X on the host."""
+        triangle reaches the device, in groups of block columns that overlap
+        the factorization (copy_plan).  Returns X on the host."""
         if A.device.type != "cpu" or B.device.type != "cpu":
             raise ValueError("solve_host takes host (CPU) tensors")
         if A.dtype != torch.float32 or B.dtype != torch.float64:
@@ -247,6 +263,17 @@ def _wrap_device(ptr: int, shape: tuple, dtype: torch.dtype) -> torch.Tensor:
 
     del numel, itemsize
     return torch.as_tensor(_Holder(), device="cuda")
+
+
+def copy_plan(n: int, block_size: int = 256) -> tuple[list[int], list[int]]:
+    """The automatic copy groups of Factor.solve_host for order n: (cuts,
+    join), block columns where groups 2.. start and the step each joins at;
+    ([], []) means copy all of A, then factor.  Host-only."""
+    lib = _lib.load()
+    cuts = (ctypes.c_int * 8)()
+    join = (ctypes.c_int * 8)()
+    ng = lib.mpchol_copy_plan(n, block_size, cuts, join, 8)
+    return list(cuts[: max(0, ng - 1)]), list(join[: max(0, ng - 1)])
 
 
 def factor(A: torch.Tensor, **opts) -> Factor:

@@ -4,8 +4,9 @@
 // The driver replaces switching_chol's host loop (src/switching_chol.cuh:76-224)
 // and precond_CG (src/mixed_cholesky.cu:76-229).  Differences that matter to a
 // caller are deliberate: nothing is allocated per step, the precision decision
-// never leaves the device, the caller's stream is the only stream used, and no
-// caller-owned handle or stream is ever destroyed.
+// never leaves the device, the work is ordered on the caller's stream (the
+// library's own streams wait on it and it waits on them), and no caller-owned
+// handle or stream is ever destroyed.
 #include <cstdio>
 #include <algorithm>
 #include <cmath>
@@ -99,6 +100,19 @@ void add_launch_counts(const long long* nk, long long times) {
   for (int i = 0; i < MPCHOL_NPHASES; ++i) g_launches[i] += nk[i] * times;
 }
 
+// How a host-buffer solve overlaps the copy of A with the factorization: A's
+// block columns are copied in groups, group g = block columns [c0[g], c1[g]).
+// Group 0 is on the device before step 0; group g > 0 joins the trailing
+// updates at step join[g] (<= c0[g] - 1), after a catch-up that applies
+// panels 0 .. join[g]-1 to its tiles in step order.  Every tile of C thus
+// receives the same updates in the same order as in the one-group
+// factorization, so the factor is the same bit for bit.
+constexpr int kMaxGroups = 8;
+struct CopyPlan {
+  int ng = 1;
+  int c0[kMaxGroups] = {}, c1[kMaxGroups] = {}, join[kMaxGroups] = {};
+};
+
 // A captured pair of PCG iterations and what it was captured for.
 struct PcgGraph {
   cudaGraphExec_t exec = nullptr;
@@ -159,6 +173,22 @@ struct mpchol_factor {
   cudaStream_t aux = nullptr;
   cudaEvent_t ev_next = nullptr;   // the next block's columns are updated
   cudaEvent_t ev_rest = nullptr;   // the rest of the step's update is done
+  // host-buffer solves with the copy of A overlapped (see CopyPlan): the
+  // copy stream, one event per arrived group, the pinned diagonal of A, and
+  // the quantized panels of the steps that late groups catch up with
+  cudaStream_t cp = nullptr;
+  cudaEvent_t ev_grp[kMaxGroups] = {};
+  cudaEvent_t ev_start = nullptr;  // prior work on the caller's stream is done
+  cudaEvent_t ev_catch = nullptr;  // a step's catch-ups are done
+  cudaEvent_t ev_diag = nullptr;   // the pinned diagonal has been copied
+  float* h_diag = nullptr;
+  uint8_t* hq8 = nullptr;
+  uint16_t* hq16 = nullptr;
+  int8_t* hrexp = nullptr;
+  uint8_t* hmx = nullptr;
+  int hist_steps = 0;              // steps the panel history holds
+  int plan_mode = -1;              // -1: automatic, otherwise set by mpchol_set_copy_plan
+  CopyPlan plan;
   int nsm = 0;
   CUtensorMap tmap32;         // TMA map over A, 32 x 32 boxes
   CUtensorMap tmapX;          // TMA map over A, 32 x b boxes (panel slabs)
@@ -199,7 +229,8 @@ void free_factor(mpchol_factor_t* f) {
   if (f == nullptr) return;
   void* ptrs[] = {f->A, f->d, f->dtilde, f->rowsq, f->sh, f->winv, f->scratch64, f->q8,
                   f->q16, f->rexp, f->mxexp, f->steps, f->status, f->wsup, f->trsv_ctr,
-                  f->vec, f->partials, f->scal, f->done, f->op, f->hb, f->hx};
+                  f->vec, f->partials, f->scal, f->done, f->op, f->hb, f->hx,
+                  f->hq8, f->hq16, f->hrexp, f->hmx};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (f->graph.exec) cudaGraphExecDestroy(f->graph.exec);
@@ -207,6 +238,12 @@ void free_factor(mpchol_factor_t* f) {
   if (f->aux) cudaStreamDestroy(f->aux);
   if (f->ev_next) cudaEventDestroy(f->ev_next);
   if (f->ev_rest) cudaEventDestroy(f->ev_rest);
+  if (f->cp) cudaStreamDestroy(f->cp);
+  for (cudaEvent_t e : f->ev_grp)
+    if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : {f->ev_start, f->ev_catch, f->ev_diag})
+    if (e) cudaEventDestroy(e);
+  if (f->h_diag) cudaFreeHost(f->h_diag);
   if (f->h_done) cudaFreeHost(f->h_done);
   if (f->h_scal) cudaFreeHost(f->h_scal);
   delete f;
@@ -227,9 +264,10 @@ DecisionParams make_dp(const mpchol_opts& o) {
 // column (rows from the block's diagonal down): one 2-D copy per block
 // column, about half of the matrix's bytes.  The factorization and the
 // operator products read nothing above the diagonal.
-cudaError_t copy_lower_blocks(float* dst, int ldd, const float* src, int lds, int n, int b,
-                              cudaMemcpyKind kind, cudaStream_t s) {
-  for (int c = 0; c < n; c += b) {
+// Block columns [j0, j1) only: copy_lower_cols.
+cudaError_t copy_lower_cols(float* dst, int ldd, const float* src, int lds, int n, int b, int j0,
+                            int j1, cudaMemcpyKind kind, cudaStream_t s) {
+  for (int c = j0 * b; c < n && c < j1 * b; c += b) {
     const int w = std::min(b, n - c);
     cudaError_t e = cudaMemcpy2DAsync(dst + (size_t)c * ldd + c, sizeof(float) * ldd,
                                       src + (size_t)c * lds + c, sizeof(float) * lds,
@@ -237,6 +275,125 @@ cudaError_t copy_lower_blocks(float* dst, int ldd, const float* src, int lds, in
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
+}
+cudaError_t copy_lower_blocks(float* dst, int ldd, const float* src, int lds, int n, int b,
+                              cudaMemcpyKind kind, cudaStream_t s) {
+  return copy_lower_cols(dst, ldd, src, lds, n, b, 0, ceil_div(n, b), kind, s);
+}
+
+// Timeline model of a copy-overlap plan, in microseconds: the lower block
+// columns cross PCIe at 50 GB/s in group order; on the caller's stream each
+// step runs the panel solve ((25 + 22 m / 8192) b / 256), the head update
+// (8) and the next POTRF (0.28 per column), the panel solve waiting for the
+// previous step's second-stream work; on the second stream a group's
+// catch-up (one launch per earlier panel) and each step's rest update cost
+// 6 + (C elements * 8 B) / (3 TB/s) per launch.  The constants are B200
+// measurements of the kernels at n = 8192, b = 256.
+double model_copy_plan(int n, int b, const CopyPlan& p) {
+  const int nb = ceil_div(n, b);
+  std::vector<double> el(nb + 1, 0.0);   // prefix sums of lower block-column elements
+  for (int j = 0; j < nb; ++j)
+    el[j + 1] = el[j] + (double)(n - j * b) * std::min(b, n - j * b);
+  auto cols = [&](int j0, int j1) { return el[std::min(j1, nb)] - el[std::min(j0, nb)]; };
+  auto syrk_us = [](double e) { return 6.0 + e * 8.0 / 3.0e6; };
+  std::vector<double> arr(p.ng);
+  double t = 0.0;
+  for (int g = 0; g < p.ng; ++g) {
+    t += cols(p.c0[g], p.c1[g]) * 4.0 / 50.0e3;
+    arr[g] = t;
+  }
+  double main_t = arr[0] + 0.28 * std::min(b, n), aux = 0.0, rest_done = 0.0;
+  int joined = 1;
+  for (int k = 0; k + 1 < nb; ++k) {
+    double catch_end = -1.0;
+    int first_new = -1;
+    while (joined < p.ng && p.join[joined] == k) {
+      aux = std::max(aux, arr[joined]);
+      for (int s = 0; s < k; ++s) aux += syrk_us(cols(p.c0[joined], p.c1[joined]));
+      catch_end = aux;
+      if (first_new < 0) first_new = joined;
+      ++joined;
+    }
+    const double m = n - (double)(k + 1) * b;
+    main_t = std::max(main_t, rest_done) + (25.0 + 22.0 * m / 8192.0) * b / 256.0;
+    if (first_new >= 0 && k + 1 >= p.c0[first_new]) main_t = std::max(main_t, catch_end);
+    main_t += 8.0;
+    aux = std::max(aux, main_t) + syrk_us(cols(k + 1, p.c1[joined - 1]));
+    rest_done = aux;
+    main_t += 0.28 * std::min(b, n - (k + 1) * b);
+  }
+  return std::max(main_t, rest_done);
+}
+
+// The plan with the least modelled time: up to 5 groups, cuts among at most
+// 16 block-column positions, each group joining 1-3 steps before its first
+// block column is solved.  One group (copy everything, then factor) unless
+// the 128-row tiles of the trailing update align with block columns (b a
+// multiple of 128) and overlap saves at least 2 %.
+CopyPlan choose_copy_plan(int n, int b) {
+  const int nb = ceil_div(n, b);
+  CopyPlan best;
+  best.ng = 1;
+  best.c0[0] = 0;
+  best.c1[0] = nb;
+  if (b % 128 != 0 || nb < 4) return best;
+  const double t1 = model_copy_plan(n, b, best);
+  double tbest = t1;
+  std::vector<int> pos;
+  const int npos = nb - 2;   // candidate cuts 1 .. nb-2
+  for (int i = 0; i < std::min(npos, 16); ++i)
+    pos.push_back(1 + (int)((long long)i * npos / std::min(npos, 16)));
+  pos.erase(std::unique(pos.begin(), pos.end()), pos.end());
+  std::vector<int> idx;
+  CopyPlan p;
+  // enumerate increasing index tuples of length ncut over pos
+  auto rec = [&](auto&& self, int start, int ncut) -> void {
+    if ((int)idx.size() == ncut) {
+      p.ng = ncut + 1;
+      p.c0[0] = 0;
+      for (int g = 0; g < ncut; ++g) {
+        p.c1[g] = pos[idx[g]];
+        p.c0[g + 1] = pos[idx[g]];
+      }
+      p.c1[ncut] = nb;
+      for (int lag = 1; lag <= 3; ++lag) {
+        p.join[0] = 0;
+        for (int g = 1; g < p.ng; ++g) p.join[g] = std::max(p.join[g - 1], std::max(0, p.c0[g] - lag));
+        bool ok = true;
+        for (int g = 1; g < p.ng; ++g) ok = ok && p.join[g] <= p.c0[g] - 1;
+        if (!ok) continue;
+        const double tp = model_copy_plan(n, b, p);
+        if (tp < tbest) {
+          tbest = tp;
+          best = p;
+        }
+      }
+      return;
+    }
+    for (int i = start; i < (int)pos.size(); ++i) {
+      idx.push_back(i);
+      self(self, i + 1, ncut);
+      idx.pop_back();
+    }
+  };
+  for (int ncut = 1; ncut <= 4; ++ncut) rec(rec, 0, ncut);
+  if (tbest > 0.98 * t1) {
+    best = CopyPlan{};
+    best.c1[0] = nb;
+  }
+  return best;
+}
+
+// Checks a plan given by cuts (block columns) and join steps.
+bool valid_copy_plan(const CopyPlan& p, int nb) {
+  if (p.ng < 1 || p.ng > kMaxGroups || p.c0[0] != 0 || p.c1[p.ng - 1] != nb) return false;
+  for (int g = 0; g < p.ng; ++g) {
+    if (p.c1[g] <= p.c0[g]) return false;
+    if (g > 0 && (p.c0[g] != p.c1[g - 1] || p.join[g] < 0 || p.join[g] > p.c0[g] - 1 ||
+                  p.join[g] < p.join[g - 1]))
+      return false;
+  }
+  return true;
 }
 
 // One factorization of f->A in place, on `stream`, right-looking with a
@@ -247,7 +404,14 @@ cudaError_t copy_lower_blocks(float* dst, int ldd, const float* src, int lds, in
 // included) runs on the aux stream on all SMs but one.  The panel solve of step k+1 waits for that
 // rest.  Every C tile receives the same updates in the same order as
 // without the split, so the factor is unchanged by it.
-mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream) {
+//
+// With a copy plan (host-buffer solves), A's block columns are still being
+// copied on f->cp while the factorization runs: f->d / f->dtilde were filled
+// by the caller, step 0 waits for group 0, the rest updates cover only the
+// groups that have joined, and a joining group first receives the earlier
+// panels' updates (one SEL_BAND launch per panel, in step order, from the
+// panel history) on the aux stream.
+mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream, const CopyPlan* plan = nullptr) {
   const mpchol_opts& o = f->opts;
   const int n = f->n, ld = f->ld, b = f->b;
   PotrfParams pp{o.diag_pert, o.pert, o.pivot_floor};
@@ -256,13 +420,16 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream) {
     MPCHOL_CUDA_TRY(cudaStreamCreateWithFlags(&f->aux, cudaStreamNonBlocking));
     MPCHOL_CUDA_TRY(cudaEventCreateWithFlags(&f->ev_next, cudaEventDisableTiming));
     MPCHOL_CUDA_TRY(cudaEventCreateWithFlags(&f->ev_rest, cudaEventDisableTiming));
+    MPCHOL_CUDA_TRY(cudaEventCreateWithFlags(&f->ev_catch, cudaEventDisableTiming));
     MPCHOL_CUDA_TRY(cudaDeviceGetAttribute(&f->nsm, cudaDevAttrMultiProcessorCount, f->device));
   }
+  const bool streamed = plan != nullptr && plan->ng > 1;
   const int cap = f->nsm > 1 ? f->nsm - 1 : 1;   // SMs for the concurrent part of the update
   MPCHOL_CUDA_TRY(cudaMemsetAsync(f->status, 0, sizeof(DevStatus), stream));
   MPCHOL_CUDA_TRY(cudaMemsetAsync(f->steps, 0, sizeof(StepState) * (f->nsteps + 1), stream));
   MPCHOL_CUDA_TRY(cudaMemsetAsync(f->sh, 0, sizeof(float) * n, stream));
-  PHASE(MPCHOL_PH_SETUP, 1, stream, launch_extract_diag(f->A, ld, n, f->d, f->dtilde, stream));
+  if (streamed) MPCHOL_CUDA_TRY(cudaStreamWaitEvent(stream, f->ev_grp[0], 0));
+  else PHASE(MPCHOL_PH_SETUP, 1, stream, launch_extract_diag(f->A, ld, n, f->d, f->dtilde, stream));
   const bool fixed = o.precision != MPCHOL_PREC_SWITCHING;
   unsigned tc_mask = 0;   // tensor-core formats a switching step may pick
   bool f32_possible = fixed || o.switch_mode == 1 || o.ladder_len == 0;
@@ -282,17 +449,27 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream) {
                        stream));
     return MPCHOL_OK;
   };
-  // where the panel solve writes the codes of each candidate format
-  QuantAll qa{};
-  qa.cand = fixed ? (o.precision != FP32 ? 1u << o.precision : 0u) : tc_mask;
-  qa.ldq = b;
-  for (int i = 0; i < 3; ++i) {
-    qa.q8[i] = f->q8 + (size_t)i * n * b;
-    qa.rexp[i] = f->rexp + (size_t)i * n;
-  }
-  qa.q16 = f->q16;
-  qa.mxexp = f->mxexp;
-  qa.ldmx = b / 32;
+  // where the panel solve of step k writes the codes of each candidate
+  // format: the shared buffers, or the panel history for steps that a late
+  // group catches up with
+  const size_t nbq = (size_t)n * b;
+  auto qa_for = [&](int k) -> QuantAll {
+    QuantAll q{};
+    q.cand = fixed ? (o.precision != FP32 ? 1u << o.precision : 0u) : tc_mask;
+    q.ldq = b;
+    q.ldmx = b / 32;
+    const bool hist = streamed && k < f->hist_steps;
+    uint8_t* q8 = hist ? f->hq8 + (size_t)k * 3 * nbq : f->q8;
+    int8_t* rexp = hist ? f->hrexp + (size_t)k * 3 * n : f->rexp;
+    for (int i = 0; i < 3; ++i) {
+      q.q8[i] = q8 + (size_t)i * nbq;
+      q.rexp[i] = rexp + (size_t)i * n;
+    }
+    q.q16 = hist ? f->hq16 + (size_t)k * 2 * nbq : f->q16;
+    q.mxexp = hist ? f->hmx + (size_t)k * (nbq / 32) : f->mxexp;
+    q.sh = o.diag_pert ? f->sh + k * b + std::min(b, n - k * b) : nullptr;
+    return q;
+  };
   // step k's trailing update over the tiles `sel` picks, on stream `ss`
   auto syrk = [&](int k, TileSel sel, int max_sms, cudaStream_t ss) -> mpchol_status {
     const int s = k * b;
@@ -300,6 +477,7 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream) {
     const int m = n - s - bs;
     float* P = f->A + (size_t)s * ld + s + bs;
     float* C = f->A + (size_t)(s + bs) * ld + s + bs;
+    const QuantAll qa = qa_for(k);
     if (fixed) {
       if (o.precision == FP32)
         PHASE(MPCHOL_PH_SYRK_F32, 1, ss,
@@ -323,9 +501,13 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream) {
             launch_syrk_tc_dispatch(C, ld, m, bs, tc_mask, qa, pick, f->status, ss, sel, max_sms));
     return MPCHOL_OK;
   };
+  // 128-tile column of step k's trailing matrix where block column j starts
+  auto tcol = [&](int k, int j) { return ceil_div(std::min(j * b, n) - (k + 1) * b, 128); };
   mpchol_status rs = potrf(0);
   if (rs != MPCHOL_OK) return rs;
   bool rest_pending = false;
+  int joined = 1;                                  // groups in the trailing updates
+  int joined_end = streamed ? plan->c1[0] : f->nsteps;   // block columns on the device
   for (int k = 0; k < f->nsteps; ++k) {
     const int s = k * b;
     const int bs = std::min(b, n - s);
@@ -337,23 +519,49 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream) {
     }
     const int next_bs = std::min(b, m);
     // panel solve, step decision and panel quantization in one launch
-    qa.sh = o.diag_pert ? f->sh + s + bs : nullptr;
+    const QuantAll qa = qa_for(k);
     PHASE(MPCHOL_PH_TRSM, 1, stream,
           launch_trsm_panel(f->tmapX, f->tmap32, f->A, ld, n, s, bs, f->winv, f->d, f->dtilde,
                             f->rowsq, &f->steps[k], &f->steps[k + 1], next_bs, dp, qa, f->status,
                             stream));
+    // groups joining at this step catch up with panels 0 .. k-1 (aux is
+    // already ordered after those panels and after the previous rest)
+    bool caught = false, head_waits = false;
+    while (streamed && joined < plan->ng && plan->join[joined] == k) {
+      const int g = joined;
+      MPCHOL_CUDA_TRY(cudaStreamWaitEvent(f->aux, f->ev_grp[g], 0));
+      for (int p = 0; p < k; ++p) {
+        TileSel band{SEL_BAND, 0, tcol(p, plan->c0[g]), tcol(p, plan->c1[g]), 0};
+        if ((rs = syrk(p, band, cap, f->aux)) != MPCHOL_OK) return rs;
+      }
+      caught = true;
+      head_waits = head_waits || k + 1 >= plan->c0[g];
+      joined_end = plan->c1[g];
+      ++joined;
+    }
+    if (caught) {
+      MPCHOL_CUDA_TRY(cudaEventRecord(f->ev_catch, f->aux));
+      if (head_waits) MPCHOL_CUDA_TRY(cudaStreamWaitEvent(stream, f->ev_catch, 0));
+    }
     const int jc = ceil_div(next_bs, 128);   // 128-tile columns of block k+1
     if ((rs = syrk(k, TileSel{SEL_NEXT, jc}, 0, stream)) != MPCHOL_OK) return rs;
-    if (sel_tile_count(ceil_div(m, 128), TileSel{SEL_REST, jc}) > 0) {
+    // the rest of the update, over the block columns on the device
+    const int T = ceil_div(m, 128);
+    const int jend = tcol(k, joined_end);
+    const TileSel rest = jend >= T ? TileSel{SEL_REST, jc} : TileSel{SEL_BAND, jc, 0, jend, jc};
+    if (sel_tile_count(T, rest) > 0) {
       MPCHOL_CUDA_TRY(cudaEventRecord(f->ev_next, stream));
       MPCHOL_CUDA_TRY(cudaStreamWaitEvent(f->aux, f->ev_next, 0));
-      if ((rs = syrk(k, TileSel{SEL_REST, jc}, cap, f->aux)) != MPCHOL_OK) return rs;
+      if ((rs = syrk(k, rest, cap, f->aux)) != MPCHOL_OK) return rs;
       MPCHOL_CUDA_TRY(cudaEventRecord(f->ev_rest, f->aux));
       rest_pending = true;
+    } else if (caught) {
+      MPCHOL_CUDA_TRY(cudaStreamWaitEvent(stream, f->ev_catch, 0));
     }
     if ((rs = potrf(k + 1)) != MPCHOL_OK) return rs;
   }
   if (rest_pending) MPCHOL_CUDA_TRY(cudaStreamWaitEvent(stream, f->ev_rest, 0));
+  if (streamed) MPCHOL_CUDA_TRY(cudaStreamWaitEvent(stream, f->ev_grp[plan->ng - 1], 0));
   f->solve_ready = false;
   return MPCHOL_OK;
 }
@@ -768,22 +976,106 @@ mpchol_status mpchol_solve_host(mpchol_factor_t* f, const float* hA, int lda, co
       nrhs < 1 || nrhs > 8)
     return MPCHOL_ERR_BAD_ARG;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  const int n = f->n;
+  const int n = f->n, b = f->b;
   if (f->op == nullptr) {
     MPCHOL_CUDA_TRY(dmalloc(&f->op, (size_t)f->ld * n));
     MPCHOL_CUDA_TRY(dmalloc(&f->hb, (size_t)n * 8));
     MPCHOL_CUDA_TRY(dmalloc(&f->hx, (size_t)n * 8));
   }
-  MPCHOL_CUDA_TRY(copy_lower_blocks(f->op, f->ld, hA, lda, n, f->b, cudaMemcpyHostToDevice, s));
-  MPCHOL_CUDA_TRY(cudaMemcpyAsync(f->hb, hB, sizeof(double) * n * nrhs, cudaMemcpyHostToDevice, s));
-  MPCHOL_CUDA_TRY(copy_lower_blocks(f->A, f->ld, f->op, f->ld, n, f->b, cudaMemcpyDeviceToDevice, s));
-  mpchol_status st = run_factor(f, s);
-  if (st != MPCHOL_OK) return st;
-  st = run_pcg<float>(f, f->op, f->ld, f->hb, f->hx, nrhs, opts, rep, s);
+  if (f->plan_mode < 0 && f->plan.c1[0] == 0) f->plan = choose_copy_plan(n, b);
+  const CopyPlan& plan = f->plan;
+  if (plan.ng <= 1) {
+    MPCHOL_CUDA_TRY(copy_lower_blocks(f->op, f->ld, hA, lda, n, b, cudaMemcpyHostToDevice, s));
+    MPCHOL_CUDA_TRY(cudaMemcpyAsync(f->hb, hB, sizeof(double) * n * nrhs, cudaMemcpyHostToDevice, s));
+    MPCHOL_CUDA_TRY(copy_lower_blocks(f->A, f->ld, f->op, f->ld, n, b, cudaMemcpyDeviceToDevice, s));
+    mpchol_status st = run_factor(f, s);
+    if (st != MPCHOL_OK) return st;
+  } else {
+    if (f->cp == nullptr) {
+      MPCHOL_CUDA_TRY(cudaStreamCreateWithFlags(&f->cp, cudaStreamNonBlocking));
+      for (cudaEvent_t& e : f->ev_grp) MPCHOL_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      MPCHOL_CUDA_TRY(cudaEventCreateWithFlags(&f->ev_start, cudaEventDisableTiming));
+      MPCHOL_CUDA_TRY(cudaEventCreateWithFlags(&f->ev_diag, cudaEventDisableTiming));
+      MPCHOL_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&f->h_diag), sizeof(float) * n));
+    }
+    // panel history for the steps that late groups catch up with
+    const int hist = plan.join[plan.ng - 1];
+    if (hist > f->hist_steps) {
+      for (void* p : {(void*)f->hq8, (void*)f->hq16, (void*)f->hrexp, (void*)f->hmx})
+        if (p) MPCHOL_CUDA_TRY(cudaFree(p));
+      f->hq8 = nullptr; f->hq16 = nullptr; f->hrexp = nullptr; f->hmx = nullptr;
+      f->hist_steps = 0;
+      const size_t nbq = (size_t)n * b;
+      MPCHOL_CUDA_TRY(dmalloc(&f->hq8, (size_t)hist * 3 * nbq));
+      MPCHOL_CUDA_TRY(dmalloc(&f->hq16, (size_t)hist * 2 * nbq));
+      MPCHOL_CUDA_TRY(dmalloc(&f->hrexp, (size_t)hist * 3 * n));
+      MPCHOL_CUDA_TRY(dmalloc(&f->hmx, (size_t)hist * (nbq / 32)));
+      f->hist_steps = hist;
+    }
+    // the copies wait for earlier work on the caller's stream (which may
+    // still read the operator and the factor), then run group by group
+    MPCHOL_CUDA_TRY(cudaEventRecord(f->ev_start, s));
+    MPCHOL_CUDA_TRY(cudaStreamWaitEvent(f->cp, f->ev_start, 0));
+    for (int g = 0; g < plan.ng; ++g) {
+      MPCHOL_CUDA_TRY(copy_lower_cols(f->op, f->ld, hA, lda, n, b, plan.c0[g], plan.c1[g],
+                                      cudaMemcpyHostToDevice, f->cp));
+      MPCHOL_CUDA_TRY(copy_lower_cols(f->A, f->ld, f->op, f->ld, n, b, plan.c0[g], plan.c1[g],
+                                      cudaMemcpyDeviceToDevice, f->cp));
+      MPCHOL_CUDA_TRY(cudaEventRecord(f->ev_grp[g], f->cp));
+    }
+    // the diagonal of A (the switching statistics of step 0 read all of
+    // it) is gathered on the host while the first group is copied
+    MPCHOL_CUDA_TRY(cudaEventSynchronize(f->ev_diag));
+    for (int i = 0; i < n; ++i) f->h_diag[i] = hA[(size_t)i * lda + i];
+    MPCHOL_CUDA_TRY(cudaMemcpyAsync(f->d, f->h_diag, sizeof(float) * n, cudaMemcpyHostToDevice, s));
+    MPCHOL_CUDA_TRY(cudaMemcpyAsync(f->dtilde, f->d, sizeof(float) * n, cudaMemcpyDeviceToDevice, s));
+    MPCHOL_CUDA_TRY(cudaEventRecord(f->ev_diag, s));
+    MPCHOL_CUDA_TRY(cudaMemcpyAsync(f->hb, hB, sizeof(double) * n * nrhs, cudaMemcpyHostToDevice, s));
+    mpchol_status st = run_factor(f, s, &plan);
+    if (st != MPCHOL_OK) return st;
+  }
+  mpchol_status st = run_pcg<float>(f, f->op, f->ld, f->hb, f->hx, nrhs, opts, rep, s);
   if (st != MPCHOL_OK && st != MPCHOL_PCG_MAXIT) return st;
   MPCHOL_CUDA_TRY(cudaMemcpyAsync(hX, f->hx, sizeof(double) * n * nrhs, cudaMemcpyDeviceToHost, s));
   MPCHOL_CUDA_TRY(cudaStreamSynchronize(s));
   return st;
+}
+
+mpchol_status mpchol_set_copy_plan(mpchol_factor_t* f, int ngroups, const int* cuts,
+                                   const int* join) {
+  if (f == nullptr) return MPCHOL_ERR_BAD_ARG;
+  if (ngroups <= 0) {           // automatic
+    f->plan_mode = -1;
+    f->plan = CopyPlan{};
+    return MPCHOL_OK;
+  }
+  const int nb = f->nsteps;
+  CopyPlan p;
+  p.ng = ngroups;
+  if (ngroups > kMaxGroups || (ngroups > 1 && (cuts == nullptr || join == nullptr)))
+    return MPCHOL_ERR_BAD_ARG;
+  if (ngroups > 1 && f->b % 128 != 0) return MPCHOL_ERR_NOT_SUPPORTED;
+  p.c0[0] = 0;
+  for (int g = 1; g < ngroups; ++g) {
+    p.c1[g - 1] = cuts[g - 1];
+    p.c0[g] = cuts[g - 1];
+    p.join[g] = join[g - 1];
+  }
+  p.c1[ngroups - 1] = nb;
+  if (!valid_copy_plan(p, nb)) return MPCHOL_ERR_BAD_ARG;
+  f->plan = p;
+  f->plan_mode = 1;
+  return MPCHOL_OK;
+}
+
+int mpchol_copy_plan(int n, int block_size, int* cuts, int* join, int cap) {
+  if (n <= 0 || block_size < 32 || block_size > 256 || block_size % 32 != 0) return 0;
+  const CopyPlan p = choose_copy_plan(n, block_size);
+  for (int g = 1; g < p.ng && g - 1 < cap; ++g) {
+    if (cuts) cuts[g - 1] = p.c0[g];
+    if (join) join[g - 1] = p.join[g];
+  }
+  return p.ng;
 }
 
 mpchol_status mpchol_factor(const mpchol_opts* opts, int n, const float* dA, int lda,

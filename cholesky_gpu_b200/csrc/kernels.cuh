@@ -90,14 +90,28 @@ cudaError_t launch_quantize_hash(unsigned long long first, unsigned long long co
 // block be factored while the rest of the update runs (look-ahead).  The
 // tiles are numbered along the rows of the lower triangle, so SEL_NEXT is
 // the first jc(jc+1)/2 of them and SEL_REST the remainder.
-enum TileSelMode { SEL_ALL = 0, SEL_NEXT = 1, SEL_REST = 2 };
+// SEL_BAND picks the tiles of tile columns [jlo, jhi) with I >= max(J, ilo),
+// numbered down each column: the columns of A that are on the device while
+// the rest is still being copied (ilo = jc: the rest of a step's update over
+// those columns), or the late columns' update by an earlier panel (ilo = 0).
+enum TileSelMode { SEL_ALL = 0, SEL_NEXT = 1, SEL_REST = 2, SEL_BAND = 3 };
 struct TileSel {
   int mode;
   int jc;
+  int jlo = 0, jhi = 0, ilo = 0;   // SEL_BAND only
 };
 constexpr TileSel kAllTiles{SEL_ALL, 0};
 
 __host__ __device__ inline int sel_tile_count(int T, TileSel s) {
+  if (s.mode == SEL_BAND) {
+    const int j1 = s.jhi < T ? s.jhi : T;
+    int c = 0;
+    for (int j = s.jlo < 0 ? 0 : s.jlo; j < j1; ++j) {
+      const int i0 = j > s.ilo ? j : s.ilo;
+      if (i0 < T) c += T - i0;
+    }
+    return c;
+  }
   const int all = T * (T + 1) / 2;
   const int j = s.jc < T ? s.jc : T;
   const int head = j * (j + 1) / 2;
@@ -106,8 +120,19 @@ __host__ __device__ inline int sel_tile_count(int T, TileSel s) {
   return all;
 }
 
-// Tile t of the selection -> (I, J).
-__device__ __forceinline__ void sel_tile(int t, TileSel s, int T, int& I, int& J) {
+// Tile t (< sel_tile_count) of the selection -> (I, J).
+__host__ __device__ __forceinline__ void sel_tile(int t, TileSel s, int T, int& I, int& J) {
+  if (s.mode == SEL_BAND) {
+    const int j1 = s.jhi < T ? s.jhi : T;
+    for (int j = s.jlo < 0 ? 0 : s.jlo; j < j1; ++j) {
+      const int i0 = j > s.ilo ? j : s.ilo;
+      const int cnt = T - i0 > 0 ? T - i0 : 0;
+      if (t < cnt) { I = i0 + t; J = j; return; }
+      t -= cnt;
+    }
+    I = J = 0;   // not reached for t < sel_tile_count(T, s)
+    return;
+  }
   if (s.mode == SEL_REST) {
     const int j = s.jc < T ? s.jc : T;
     t += j * (j + 1) / 2;

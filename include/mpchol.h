@@ -198,14 +198,35 @@ MPCHOL_API mpchol_status mpchol_pcg_f64(mpchol_factor_t* f, const double* dA, in
  * block column, about half of A, one 2-D copy per block column), once into an
  * operator buffer the factor object keeps and once, device to device, into
  * the factor's storage.  hB / hX: n x nrhs FP64 (ld = n), nrhs 1..8.
- * Page-locked host buffers let the copies run at full link speed.  The first
- * call on a factor object allocates the operator and vector buffers (n x lda
- * FP32, 2 x n x 8 FP64); later calls allocate nothing.  Returns like
- * mpchol_pcg; the stream is synchronized before returning. */
+ * Page-locked host buffers let the copies run at full link speed.
+ * When block_size is a multiple of 128 the copy overlaps the factorization:
+ * the block columns cross the link in groups on a library stream, step 0
+ * starts once the first group (and the diagonal of A, read on the host) is on
+ * the device, and each later group joins the trailing updates after
+ * receiving the earlier panels' updates in step order -- the factor is
+ * identical bit for bit to the one computed after a full copy.  The groups
+ * come from a timeline model of the copy and the factor steps
+ * (mpchol_copy_plan) unless mpchol_set_copy_plan fixed them.  The first call
+ * on a factor object allocates the operator and vector buffers (n x lda FP32,
+ * 2 x n x 8 FP64), and with copy overlap the quantized panels of the steps
+ * that late groups catch up with (about 7 n b bytes per step); later calls
+ * allocate nothing.  Returns like mpchol_pcg; the stream is synchronized
+ * before returning.  No counterpart in the reference (its precond_CG takes
+ * device buffers). */
 MPCHOL_API mpchol_status mpchol_solve_host(mpchol_factor_t* f, const float* hA, int lda,
                                            const double* hB, double* hX, int nrhs,
                                            const mpchol_pcg_opts* opts, mpchol_report* report,
                                            mpchol_stream_t stream);
+/* Copy groups of mpchol_solve_host.  ngroups <= 0: the automatic plan;
+ * ngroups == 1: copy all of A, then factor; ngroups 2..8: block columns
+ * [0, cuts[0]), [cuts[0], cuts[1]), ..., group g >= 1 joining at step
+ * join[g-1] (0 <= join[g-1] <= cuts[g-1] - 1, non-decreasing).  Needs
+ * block_size % 128 == 0 for ngroups > 1 (MPCHOL_ERR_NOT_SUPPORTED). */
+MPCHOL_API mpchol_status mpchol_set_copy_plan(mpchol_factor_t* f, int ngroups, const int* cuts,
+                                              const int* join);
+/* The automatic plan for order n and block_size: returns the number of
+ * groups and writes up to cap cuts / join steps (host only, no device). */
+MPCHOL_API int mpchol_copy_plan(int n, int block_size, int* cuts, int* join, int cap);
 /* dZ = (L L^T)^-1 dR for nrhs vectors (n x nrhs, ld = n), i.e. Dpotrs
  * (src/mixed_cholesky.cu:204-206) on the FP32 factor with FP64 vectors. */
 MPCHOL_API mpchol_status mpchol_apply_precond(mpchol_factor_t* f, const double* dR, double* dZ, int nrhs,
