@@ -446,7 +446,7 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream, const CopyPlan
     PHASE(MPCHOL_PH_POTRF, o.floor > 0.0f ? 2 : 1, stream,
           launch_potrf(f->tmap32, f->A, ld, n, s, std::min(b, n - s), f->d, f->sh, pp,
                        &f->steps[k].fp64_diag, f->scratch64, f->winv, f->status, o.floor > 0.0f,
-                       stream));
+                       stream, k > 0 ? &f->steps[k - 1] : nullptr, f->rowsq));
     return MPCHOL_OK;
   };
   // where the panel solve of step k writes the codes of each candidate
@@ -523,7 +523,7 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream, const CopyPlan
     PHASE(MPCHOL_PH_TRSM, 1, stream,
           launch_trsm_panel(f->tmapX, f->tmap32, f->A, ld, n, s, bs, f->winv, f->d, f->dtilde,
                             f->rowsq, &f->steps[k], &f->steps[k + 1], next_bs, dp, qa, f->status,
-                            stream));
+                            stream, k > 0 ? &f->steps[k - 1] : nullptr));
     // groups joining at this step catch up with panels 0 .. k-1 (aux is
     // already ordered after those panels and after the previous rest)
     bool caught = false, head_waits = false;

@@ -36,10 +36,13 @@ size_t potrf_scratch64_elems(int bs);
 // Also writes the inverses of the 32x32 diagonal tiles of the factored block
 // to winv (ceil(bs/32) tiles, column-major 32x32 each) for the panel solve.
 // tmap32: TMA map over A (FP32, n x n, column stride lda) with 32 x 32 boxes.
+// With diagonal perturbation, the block's rows first receive the previous
+// step's rounding shift, sh += u(prev->prec) * rowsq (prev null: none).
 cudaError_t launch_potrf(const CUtensorMap& tmap32, float* A, int lda, int n, int s, int bs,
-                         const float* d, const float* sh, const PotrfParams& p,
+                         const float* d, float* sh, const PotrfParams& p,
                          const int* fp64_flag, double* scratch64, float* winv, DevStatus* st,
-                         bool may_fp64, cudaStream_t stream);
+                         bool may_fp64, cudaStream_t stream, const StepState* prev = nullptr,
+                         const float* rowsq = nullptr);
 
 // ---- panel TRSM + fused diagonal tracker, decision and quantization ------
 // Where the panel solve writes the quantized panel: one K-major code panel
@@ -64,13 +67,16 @@ __host__ __device__ inline int rexp_slot(int fmt) { return fmt == E4M3 ? 0 : (fm
 // stores it in rowsq, folds the switching statistics into step (and the FP64
 // flag of the next diagonal block into next), and writes the slab's codes in
 // every candidate format.  The last CTA to finish resolves the step precision
-// (step->prec) and adds the step's rounding shift to qa.sh.  tmapX: TMA map
-// over A with 32 x bs boxes; tmap32 as for launch_potrf.
+// (step->prec).  Before its rows' sums of squares are overwritten, each CTA
+// adds the previous step's rounding shift u(prev->prec) * rowsq to qa.sh for
+// its rows (prev null: first step); the rows of the next diagonal block get
+// theirs in its POTRF.  tmapX: TMA map over A with 32 x bs boxes; tmap32 as
+// for launch_potrf.
 cudaError_t launch_trsm_panel(const CUtensorMap& tmapX, const CUtensorMap& tmap32, float* A,
                               int lda, int n, int s, int bs, const float* winv, const float* d,
                               float* dtilde, float* rowsq, StepState* step, StepState* next,
                               int next_bs, const DecisionParams& dp, const QuantAll& qa,
-                              DevStatus* st, cudaStream_t stream);
+                              DevStatus* st, cudaStream_t stream, const StepState* prev = nullptr);
 
 // ---- panel quantization ---------------------------------------------------
 // Fixed-format variant (test entry point): no decision, no shift.

@@ -228,8 +228,9 @@ __device__ void invert_tile(const T* l, const T* inv, float* out, int lane) {
 
 template <typename T, bool TMA>
 __device__ void potrf_block(const CUtensorMap* tmap, T* tiles, float* A, int lda, int n, int s,
-                            int bs, const float* d, const float* sh, const PotrfParams& p,
-                            float* winv, DevStatus* st) {
+                            int bs, const float* d, float* sh, const PotrfParams& p,
+                            float* winv, DevStatus* st, const StepState* prev = nullptr,
+                            const float* rowsq = nullptr) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
   const int NT = (bs + TS - 1) / TS;
   const int ntiles = NT * (NT + 1) / 2;
@@ -240,10 +241,18 @@ __device__ void potrf_block(const CUtensorMap* tmap, T* tiles, float* A, int lda
   __shared__ int s_fail, s_pert, s_ok;
   __shared__ __align__(8) uint64_t bar;
   if (tid == 0) { s_fail = -1; s_pert = 0; s_ok = 1; }
+  const int prev_prec = (prev != nullptr && p.diag_pert && sh) ? prev->prec : FP32;
   for (int i = tid; i < NT * TS; i += blockDim.x) {
     T shv = T(0), pm = T(0);
     if (i < bs) {
-      if (p.diag_pert && sh) shv = T(p.pert) * T(sh[s + i]);
+      if (p.diag_pert && sh) {
+        float shf = sh[s + i];
+        if (prev_prec != FP32) {   // the previous step's shift for this row
+          shf = __fmaf_rn(unit_roundoff(prev_prec), rowsq[s + i], shf);
+          sh[s + i] = shf;
+        }
+        shv = T(p.pert) * T(shf);
+      }
       pm = T(p.pivot_floor) * T(d[s + i]);
     }
     s_shift[i] = shv;
@@ -396,13 +405,13 @@ __device__ void potrf_block(const CUtensorMap* tmap, T* tiles, float* A, int lda
 // the two precisions keep the FP64 register footprint out of the FP32 path.
 __global__ void __launch_bounds__(512, 1)
 potrf_f32_kernel(const __grid_constant__ CUtensorMap tmap, float* A, int lda, int n, int s, int bs,
-                 const float* d, const float* sh, PotrfParams p, const int* fp64_flag, float* winv,
-                 DevStatus* st) {
+                 const float* d, float* sh, PotrfParams p, const int* fp64_flag, float* winv,
+                 DevStatus* st, const StepState* prev, const float* rowsq) {
   if (st->code != 0) return;
   if (fp64_flag != nullptr && *fp64_flag != 0) return;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   potrf_block<float, true>(&tmap, reinterpret_cast<float*>(smem_raw), A, lda, n, s, bs, d, sh, p,
-                           winv, st);
+                           winv, st, prev, rowsq);
 }
 
 // Batched: CTA i factors the current diagonal block of system i (tiles in
@@ -420,11 +429,12 @@ potrf_batched_kernel(BatchSys* __restrict__ sys, int s, int b, PotrfParams p) {
 
 // FP64 blocks (flagged near-indefinite): tiles in a global scratch.
 __global__ void __launch_bounds__(256, 1)
-potrf_f64_kernel(float* A, int lda, int n, int s, int bs, const float* d, const float* sh,
-                 PotrfParams p, const int* fp64_flag, double* scratch64, float* winv, DevStatus* st) {
+potrf_f64_kernel(float* A, int lda, int n, int s, int bs, const float* d, float* sh,
+                 PotrfParams p, const int* fp64_flag, double* scratch64, float* winv, DevStatus* st,
+                 const StepState* prev, const float* rowsq) {
   if (st->code != 0) return;
   if (fp64_flag == nullptr || *fp64_flag == 0) return;
-  potrf_block<double, false>(nullptr, scratch64, A, lda, n, s, bs, d, sh, p, winv, st);
+  potrf_block<double, false>(nullptr, scratch64, A, lda, n, s, bs, d, sh, p, winv, st, prev, rowsq);
 }
 
 }  // namespace
@@ -437,17 +447,19 @@ size_t potrf_scratch64_elems(int bs) {
 size_t potrf_smem_bytes(int bs) { return potrf_scratch64_elems(bs) * sizeof(float); }
 
 cudaError_t launch_potrf(const CUtensorMap& tmap32, float* A, int lda, int n, int s, int bs,
-                         const float* d, const float* sh, const PotrfParams& p,
+                         const float* d, float* sh, const PotrfParams& p,
                          const int* fp64_flag, double* scratch64, float* winv, DevStatus* st,
-                         bool may_fp64, cudaStream_t stream) {
+                         bool may_fp64, cudaStream_t stream, const StepState* prev,
+                         const float* rowsq) {
   const size_t smem = potrf_smem_bytes(256);
   cudaError_t e = cudaFuncSetAttribute(potrf_f32_kernel,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   potrf_f32_kernel<<<1, 512, smem, stream>>>(tmap32, A, lda, n, s, bs, d, sh, p,
-                                             may_fp64 ? fp64_flag : nullptr, winv, st);
+                                             may_fp64 ? fp64_flag : nullptr, winv, st, prev, rowsq);
   if (may_fp64)
-    potrf_f64_kernel<<<1, 256, 0, stream>>>(A, lda, n, s, bs, d, sh, p, fp64_flag, scratch64, winv, st);
+    potrf_f64_kernel<<<1, 256, 0, stream>>>(A, lda, n, s, bs, d, sh, p, fp64_flag, scratch64, winv, st,
+                                            prev, rowsq);
   return cudaGetLastError();
 }
 

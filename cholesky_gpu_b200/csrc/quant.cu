@@ -40,7 +40,7 @@ quantize_batched_kernel(BatchSys* __restrict__ sys, const BatchStep* __restrict_
     const float u = unit_roundoff(fmt);
     for (int r = threadIdx.x; r < QROWS; r += QTHR) {
       const int gi = blockIdx.x * QROWS + r;
-      if (gi < m) S.sh[s + bs + gi] += u * S.rowsq[s + bs + gi];
+      if (gi < m) S.sh[s + bs + gi] = __fmaf_rn(u, S.rowsq[s + bs + gi], S.sh[s + bs + gi]);
     }
   }
   const size_t esz = (fmt == FP16 || fmt == FP16X2) ? 2 : 1;

@@ -126,6 +126,33 @@ __device__ void trsm_step(float* Xs, const float* LJ, const float* WJ, float* re
   __syncthreads();
 }
 
+// Per-row sum of squares and max |x| of the solved slab, by all threads:
+// thread (r, part) = (tid % TR, tid / TR) covers row r's 32 columns `part`
+// (sums of squares as a chain of FMAs in column order), leaving the partials
+// in s_sq / s_amax [part][r]; the row's sum is then the partials added in
+// part order (row_sq).  One fixed order for the streaming and the batched
+// kernel, so both give the same bits.
+__device__ __forceinline__ void slab_row_partials(const float* Xs, int NT, float (*s_sq)[TR],
+                                                  float (*s_amax)[TR], int tid) {
+  const int r = tid % TR, part = tid / TR;
+  float sq = 0.0f, amax = 0.0f;
+  if (part < NT) {
+#pragma unroll 8
+    for (int c = part * 32; c < part * 32 + 32; ++c) {
+      const float v = Xs[c * XLD + r];
+      sq = __fmaf_rn(v, v, sq);
+      amax = fmaxf(amax, fabsf(v));
+    }
+  }
+  s_sq[part][r] = sq;
+  if (s_amax != nullptr) s_amax[part][r] = amax;
+}
+__device__ __forceinline__ float row_sq(float (*s_sq)[TR], int NT, int r) {
+  float sq = s_sq[0][r];
+  for (int q = 1; q < NT; ++q) sq += s_sq[q][r];
+  return sq;
+}
+
 // Codes of one solved slab in one format.  Xs: the slab (bs columns x TR
 // rows, column-major, stride XLD).  Thread (r, part) = (tid % TR, tid / TR)
 // converts row r's 32-column block `part` (for MXFP8 with its own scale)
@@ -146,18 +173,22 @@ __device__ void quantize_slab(const float* Xs, int bs, int nrows, int gi0, int m
     uint32_t* lo = stage + TR * sw;
     const int e = row_scale_exp(rmax, FP16);
     const float inv = pow2f(-e);
-    for (int c = c0; c < c0 + cw; c += 2) {
-      const float x0 = Xs[c * XLD + r] * inv, x1 = Xs[(c + 1) * XLD + r] * inv;
-      const __half2 h = __floats2half2_rn(x0, x1);
-      hi[r * sw + c / 2] = *reinterpret_cast<const uint32_t*>(&h);
-      if (fmt == FP16X2) {   // x - hi is exact in FP32
-        const float2 hf = __half22float2(h);
-        lo[r * sw + c / 2] = f32x2_to_f16x2(x0 - hf.x, x1 - hf.y);
+    if (cw == 32) {
+#pragma unroll
+      for (int c = c0; c < c0 + 32; c += 2) {
+        const float x0 = Xs[c * XLD + r] * inv, x1 = Xs[(c + 1) * XLD + r] * inv;
+        const __half2 h = __floats2half2_rn(x0, x1);
+        hi[r * sw + c / 2] = *reinterpret_cast<const uint32_t*>(&h);
+        if (fmt == FP16X2) {   // x - hi is exact in FP32
+          const float2 hf = __half22float2(h);
+          lo[r * sw + c / 2] = f32x2_to_f16x2(x0 - hf.x, x1 - hf.y);
+        }
       }
     }
     if (live && part == 0) qa.rexp[2][gi] = (int8_t)e;
     __syncthreads();
     const int wpr = bs / 2;                    // words per row
+#pragma unroll 4
     for (int q = tid; q < nrows * wpr; q += NTHR) {
       const int rr = q / wpr, w = q % wpr;
       reinterpret_cast<uint32_t*>(qa.q16 + (size_t)(gi0 + rr) * qa.ldq)[w] = hi[rr * sw + w];
@@ -182,6 +213,7 @@ __device__ void quantize_slab(const float* Xs, int bs, int nrows, int gi0, int m
         inv = pow2f(-eb);
         if (live) qa.mxexp[(size_t)gi * qa.ldmx + cb / 32] = (uint8_t)(eb + 127);
       }
+#pragma unroll
       for (int c = cb; c < cb + 32; c += 4) {
         float x[4];
 #pragma unroll
@@ -194,6 +226,7 @@ __device__ void quantize_slab(const float* Xs, int bs, int nrows, int gi0, int m
     __syncthreads();
     uint8_t* q = qa.q8[q8_slot(fmt)];
     const int wpr = bs / 4;
+#pragma unroll 4
     for (int q4 = tid; q4 < nrows * wpr; q4 += NTHR) {
       const int rr = q4 / wpr, w = q4 % wpr;
       reinterpret_cast<uint32_t*>(q + (size_t)(gi0 + rr) * qa.ldq)[w] = stage[rr * sw + w];
@@ -216,7 +249,7 @@ trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_consta
                   float* __restrict__ A, int lda, int n, int s, int bs, const float* __restrict__ winv,
                   const float* __restrict__ d, float* __restrict__ dtilde, float* __restrict__ rowsq,
                   StepState* step, StepState* next, int next_bs, DecisionParams dp, DevStatus* st,
-                  QuantAll qa) {
+                  QuantAll qa, const StepState* prev) {
   extern __shared__ __align__(128) float sm[];
   const int NT = bs / 32;
   float* Xs = sm;                                        // [bs][XLD]
@@ -227,6 +260,7 @@ trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_consta
   __shared__ float red_max[NTHR / 32];
   __shared__ int red_lit[NTHR / 32];
   __shared__ float s_rmax[NTHR / TR][TR];
+  __shared__ float s_sq[NTHR / TR][TR];
   __shared__ __align__(8) uint64_t barx, barl[2];
   __shared__ int s_ok, s_last;
 
@@ -235,6 +269,15 @@ trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_consta
   const int slab = blockIdx.x;
   const int row0 = s + bs + slab * TR;                   // first global row of the slab
   const int nrows = min(TR, n - row0);
+  // the previous step's rounding shift for the slab's rows, before this
+  // step's sums of squares replace the previous ones in rowsq
+  if (prev != nullptr && qa.sh != nullptr && tid < nrows) {
+    const int pp = prev->prec;
+    if (pp != FP32) {
+      float* shp = qa.sh + slab * TR + tid;
+      *shp = __fmaf_rn(unit_roundoff(pp), rowsq[row0 + tid], *shp);
+    }
+  }
   // tile row J of L11 (tiles L_{J,0..J-1} and L_JJ^-1) into buffer J % 2
   auto issue_row = [&](int J) {
     const int buf = J & 1;
@@ -290,15 +333,17 @@ trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_consta
   __syncthreads();
   if (s_ok) {
     // ---- write the solved slab back (coalesced; rows past n skipped) -----
+#pragma unroll 8
     for (int e = tid; e < bs * TR; e += NTHR) {
       const int c = e / TR, r = e % TR;
       if (r < nrows) A[(size_t)(s + c) * lda + row0 + r] = Xs[c * XLD + r];
     }
     // ---- Schur diagonal tracker and switching statistics of the slab -----
+    slab_row_partials(Xs, NT, s_sq, s_rmax, tid);
+    __syncthreads();
     if (tid < nrows) {
       const int gi = row0 + tid;
-      float sq = 0.0f;
-      for (int c = 0; c < bs; ++c) { const float v = Xs[c * XLD + tid]; sq += v * v; }
+      const float sq = row_sq(s_sq, NT, tid);
       rowsq[gi] = sq;
       const float dt = dtilde[gi] - sq;
       dtilde[gi] = dt;
@@ -318,14 +363,6 @@ trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_consta
     }
     // ---- the slab's codes in every candidate format -------------------------
     if (qa.cand != 0) {
-      {
-        const int r = tid % TR, part = tid / TR;
-        float amax = 0.0f;
-        if (part < NT)
-          for (int c = part * 32; c < part * 32 + 32; ++c) amax = fmaxf(amax, fabsf(Xs[c * XLD + r]));
-        s_rmax[part][r] = amax;
-      }
-      __syncthreads();
       const int r = tid % TR;
       float rmax = 0.0f;
 #pragma unroll
@@ -343,7 +380,6 @@ trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_consta
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) bl = max(bl, __shfl_xor_sync(0xffffffffu, bl, o));
   if ((tid & 31) == 0) { red_max[tid >> 5] = bm; red_lit[tid >> 5] = bl; }
-  __threadfence();                                       // this thread's panel, code and row writes
   __syncthreads();
   if (tid == 0) {
     float cm = 0.0f; int cl = 0;
@@ -355,16 +391,13 @@ trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_consta
   }
   __syncthreads();
   if (!s_last) return;
-  __threadfence();                                       // every CTA's statistics and rows
+  if (tid != 0) return;
+  __threadfence();                                       // every CTA's statistics
   if (*reinterpret_cast<volatile int*>(&st->code) != 0) return;
   StepState ss;
   ss.max_ratio_bits = *reinterpret_cast<volatile unsigned int*>(&step->max_ratio_bits);
   ss.literal_code = *reinterpret_cast<volatile int*>(&step->literal_code);
-  const int p = resolve_precision(&ss, dp);
-  if (tid == 0) step->prec = p;
-  if (p == FP32 || qa.sh == nullptr) return;
-  const float u = unit_roundoff(p);
-  for (int gi = tid; gi < m; gi += NTHR) qa.sh[gi] += u * __ldcg(rowsq + s + bs + gi);
+  step->prec = resolve_precision(&ss, dp);
 }
 
 // Batched: blockIdx.y = system, blockIdx.x = 32-row slab.  Staging by
@@ -404,10 +437,12 @@ trsm_batched_kernel(BatchSys* __restrict__ sys, int s, int b) {
     const int c = e / TR, r = e % TR;
     if (r < nrows) S.A[(size_t)(s + c) * ld + row0 + r] = Xs[c * XLD + r];
   }
+  __shared__ float s_sq[NTHR / TR][TR];
+  slab_row_partials(Xs, NT, s_sq, nullptr, tid);
+  __syncthreads();
   if (tid < nrows) {
     const int gi = row0 + tid;
-    float sq = 0.0f;
-    for (int c = 0; c < bs; ++c) { const float v = Xs[c * XLD + tid]; sq += v * v; }
+    const float sq = row_sq(s_sq, NT, tid);
     S.rowsq[gi] = sq;
     S.dtilde[gi] -= sq;
   }
@@ -419,7 +454,7 @@ cudaError_t launch_trsm_panel(const CUtensorMap& tmapX, const CUtensorMap& tmap3
                               int lda, int n, int s, int bs, const float* winv, const float* d,
                               float* dtilde, float* rowsq, StepState* step, StepState* next,
                               int next_bs, const DecisionParams& dp, const QuantAll& qa,
-                              DevStatus* st, cudaStream_t stream) {
+                              DevStatus* st, cudaStream_t stream, const StepState* prev) {
   const int m = n - s - bs;
   if (m <= 0) return cudaSuccess;
   const size_t smem = trsm_smem_floats(bs) * sizeof(float);
@@ -429,7 +464,7 @@ cudaError_t launch_trsm_panel(const CUtensorMap& tmapX, const CUtensorMap& tmap3
   if (e != cudaSuccess) return e;
   trsm_panel_kernel<<<ceil_div(m, TR), NTHR, smem, stream>>>(tmapX, tmap32, A, lda, n, s, bs, winv, d,
                                                              dtilde, rowsq, step, next, next_bs, dp, st,
-                                                             qa);
+                                                             qa, prev);
   return cudaGetLastError();
 }
 
