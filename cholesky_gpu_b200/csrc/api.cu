@@ -113,9 +113,11 @@ struct CopyPlan {
   int c0[kMaxGroups] = {}, c1[kMaxGroups] = {}, join[kMaxGroups] = {};
 };
 
-// A captured pair of PCG iterations and what it was captured for.
+// The captured device-side PCG loop (a WHILE node whose body is one
+// iteration) and what it was captured for; nk: kernels per iteration.
 struct PcgGraph {
   cudaGraphExec_t exec = nullptr;
+  bool failed = false;        // the runtime refused the graph: iterations are launched directly
   const void* A = nullptr;
   int lda = 0, nr = 0, elem = 0;
   double tol2 = 0.0;
@@ -162,7 +164,8 @@ struct mpchol_factor {
   int* done = nullptr;        // [0] converged flag, [1] iteration counter
   int* h_done = nullptr;      // pinned
   double* h_scal = nullptr;   // pinned
-  PcgGraph graph;             // captured iteration pair (see run_pcg)
+  PcgGraph graph;             // captured PCG loop (see run_pcg)
+  int* loop_ctl = nullptr;    // its iteration count and budget
   cudaStream_t capture_stream = nullptr;   // private stream used only to capture graphs
   // look-ahead: the bulk of each step's trailing update runs on aux while
   // the next diagonal block is factored on the caller's stream
@@ -229,7 +232,7 @@ void free_factor(mpchol_factor_t* f) {
   if (f == nullptr) return;
   void* ptrs[] = {f->A, f->d, f->dtilde, f->rowsq, f->sh, f->winv, f->scratch64, f->q8,
                   f->q16, f->rexp, f->mxexp, f->steps, f->status, f->wsup, f->trsv_ctr,
-                  f->vec, f->partials, f->scal, f->done, f->op, f->hb, f->hx,
+                  f->vec, f->partials, f->scal, f->done, f->loop_ctl, f->op, f->hb, f->hx,
                   f->hq8, f->hq16, f->hrexp, f->hmx};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -574,10 +577,10 @@ mpchol_status ensure_solve(mpchol_factor_t* f, cudaStream_t stream) {
   return MPCHOL_OK;
 }
 
-// kernels per triangular solve: copy, zero, the persistent solve
+// kernels per triangular solve: the input preparation, the persistent solve
 int trsv_launch_count(int n) {
   (void)n;
-  return 3;
+  return 2;
 }
 
 // z = M^-1 r for NR-padded vectors (tmp, work: n x nr scratch)
@@ -688,57 +691,86 @@ mpchol_status run_pcg(mpchol_factor_t* f, const TA* dA, int lda, const double* d
                                  bnorm2, tol2, f->done, f->done, f->done + 1, s));
       return MPCHOL_OK;
     };
-    // Iteration pairs (which return the rho buffers to their starting roles)
-    // run as one CUDA graph, captured once per operator / rhs-count / tolerance.
-    const bool use_graph = !profiling_on();
-    if (use_graph) {
-      PcgGraph& g = f->graph;
-      if (g.exec == nullptr || g.A != (const void*)dA || g.lda != lda || g.nr != nr ||
-          g.elem != (int)sizeof(TA) || g.tol2 != tol2) {
+    // The iterations run in a device-side loop: one launch of a CUDA graph
+    // whose WHILE node repeats one iteration until the recursive residual
+    // meets the tolerance, an error is recorded or the budget is spent, with
+    // no host round trip in between.  Captured once per operator / rhs
+    // count / tolerance.
+    PcgGraph& g = f->graph;
+    bool use_graph = !profiling_on() && !g.failed;
+    if (use_graph && (g.exec == nullptr || g.A != (const void*)dA || g.lda != lda || g.nr != nr ||
+                      g.elem != (int)sizeof(TA) || g.tol2 != tol2)) {
+      if (g.exec) cudaGraphExecDestroy(g.exec);
+      g.exec = nullptr;
+      // capture on a private stream (the caller's may be the legacy default
+      // stream, which cannot be captured); the graph is launched into the
+      // caller's stream
+      if (f->capture_stream == nullptr)
+        MPCHOL_CUDA_TRY(cudaStreamCreateWithFlags(&f->capture_stream, cudaStreamNonBlocking));
+      long long before[MPCHOL_NPHASES];
+      launch_counts(before);
+      cudaGraph_t graph = nullptr;
+      cudaGraphConditionalHandle handle = 0;
+      cudaGraphNodeParams cp = {};
+      cudaGraphNode_t node = nullptr;
+      bool ok = cudaGraphCreate(&graph, 0) == cudaSuccess &&
+                cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault) ==
+                    cudaSuccess;
+      if (ok) {
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = handle;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        ok = cudaGraphAddNode(&node, graph, nullptr, 0, &cp) == cudaSuccess;
+      }
+      if (ok) {
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        ok = cudaStreamBeginCaptureToGraph(f->capture_stream, body, nullptr, nullptr, 0,
+                                           cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+        if (ok) {
+          const mpchol_status s0 = iteration(0, f->capture_stream);
+          const bool cond_ok =
+              s0 == MPCHOL_OK && launch_pcg_loop_cond(handle, f->loop_ctl, f->done, f->status,
+                                                      f->scal, nr, f->capture_stream) == cudaSuccess;
+          cudaGraph_t captured = nullptr;
+          const cudaError_t ce = cudaStreamEndCapture(f->capture_stream, &captured);
+          ok = cond_ok && ce == cudaSuccess && cudaGraphInstantiate(&g.exec, graph, 0) == cudaSuccess;
+        }
+      }
+      if (graph) cudaGraphDestroy(graph);
+      long long after[MPCHOL_NPHASES];
+      launch_counts(after);
+      for (int i = 0; i < MPCHOL_NPHASES; ++i) g.nk[i] = after[i] - before[i];
+      add_launch_counts(g.nk, -1);   // nothing ran during capture
+      g.nk[MPCHOL_PH_PCG_VEC] += 1;  // the loop condition kernel
+      if (!ok) {
+        cudaGetLastError();            // the refusal is not an error of this call
         if (g.exec) cudaGraphExecDestroy(g.exec);
         g.exec = nullptr;
-        long long before[MPCHOL_NPHASES];
-        launch_counts(before);
-        cudaGraph_t graph = nullptr;
-        // capture on a private stream (the caller's may be the legacy default
-        // stream, which cannot be captured); the graph is launched into the
-        // caller's stream
-        if (f->capture_stream == nullptr)
-          MPCHOL_CUDA_TRY(cudaStreamCreateWithFlags(&f->capture_stream, cudaStreamNonBlocking));
-        MPCHOL_CUDA_TRY(cudaStreamBeginCapture(f->capture_stream, cudaStreamCaptureModeThreadLocal));
-        mpchol_status s0 = iteration(0, f->capture_stream);
-        if (s0 == MPCHOL_OK) s0 = iteration(1, f->capture_stream);
-        cudaError_t ce = cudaStreamEndCapture(f->capture_stream, &graph);
-        if (s0 != MPCHOL_OK) return s0;
-        MPCHOL_CUDA_TRY(ce);
-        long long after[MPCHOL_NPHASES];
-        launch_counts(after);
-        for (int i = 0; i < MPCHOL_NPHASES; ++i) g.nk[i] = after[i] - before[i];
-        add_launch_counts(g.nk, -1);   // nothing ran during capture
-        ce = cudaGraphInstantiate(&g.exec, graph, 0);
-        cudaGraphDestroy(graph);
-        MPCHOL_CUDA_TRY(ce);
+        g.failed = true;
+        use_graph = false;
+      } else {
         g.A = dA; g.lda = lda; g.nr = nr; g.elem = (int)sizeof(TA); g.tol2 = tol2;
       }
+    }
+    if (use_graph) {
+      PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_pcg_loop_init(f->loop_ctl, po.max_it - launched, stream));
+      MPCHOL_CUDA_TRY(cudaGraphLaunch(g.exec, stream));
+      MPCHOL_CUDA_TRY(cudaMemcpyAsync(f->h_done, f->done, 2 * sizeof(int), cudaMemcpyDeviceToHost, stream));
+      DevStatus st;
+      MPCHOL_CUDA_TRY(cudaMemcpyAsync(&st, f->status, sizeof(DevStatus), cudaMemcpyDeviceToHost, stream));
+      MPCHOL_CUDA_TRY(cudaStreamSynchronize(stream));
+      if (st.code == MPCHOL_ERR_TIMEOUT) return MPCHOL_ERR_TIMEOUT;
+      add_launch_counts(g.nk, f->h_done[1] - it);
+      it = f->h_done[1];                // iterations actually executed on the device
+      launched = it;
+      continue;                         // the true residual decides (residual replacement restart)
     }
     int cur = 0;
     bool stop = false;
     while (launched < po.max_it && !stop) {
       const int chunk = std::min(po.check_every, po.max_it - launched);
-      int c = 0;
-      if (use_graph) {
-        if (cur == 1 && c < chunk) {
-          mpchol_status s3 = iteration(cur, stream);
-          if (s3 != MPCHOL_OK) return s3;
-          cur ^= 1;
-          ++c;
-        }
-        for (; chunk - c >= 2; c += 2) {
-          MPCHOL_CUDA_TRY(cudaGraphLaunch(f->graph.exec, stream));
-          add_launch_counts(f->graph.nk, 1);
-        }
-      }
-      for (; c < chunk; ++c) {
+      for (int c = 0; c < chunk; ++c) {
         mpchol_status s3 = iteration(cur, stream);
         if (s3 != MPCHOL_OK) return s3;
         cur ^= 1;
@@ -913,6 +945,7 @@ mpchol_status mpchol_factor_create(const mpchol_opts* opts, int n, mpchol_factor
             dmalloc(&f->vec, 8 * nv) == cudaSuccess &&
             dmalloc(&f->partials, (size_t)5 * pcg_vgrid() * 8) == cudaSuccess &&
             dmalloc(&f->scal, 64) == cudaSuccess && dmalloc(&f->done, 2) == cudaSuccess &&
+            dmalloc(&f->loop_ctl, 2) == cudaSuccess &&
             cudaMallocHost(reinterpret_cast<void**>(&f->h_done), 2 * sizeof(int)) == cudaSuccess &&
             cudaMallocHost(reinterpret_cast<void**>(&f->h_scal), sizeof(double) * 64) == cudaSuccess;
   if (!ok) {

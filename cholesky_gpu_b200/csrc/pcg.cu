@@ -514,4 +514,36 @@ cudaError_t launch_frob_batched(const BatchSys* sys, int nsys, cudaStream_t stre
   return cudaGetLastError();
 }
 
+
+namespace {
+// Loop control of the device-side PCG loop: ctl[0] counts the iterations run
+// by this launch of the loop, ctl[1] is how many it may run.
+__global__ void pcg_loop_init_kernel(int* ctl, int max_iters) {
+  ctl[0] = 0;
+  ctl[1] = max_iters;
+}
+// After each iteration: the new r^T z becomes the current one (rho[8..] ->
+// rho[0..]), and the loop runs again only if the recursive residual has not
+// met the tolerance, no error was recorded and the iteration budget is not
+// spent.  The budget alone ends the loop, whatever the other flags hold.
+__global__ void pcg_loop_cond_kernel(cudaGraphConditionalHandle handle, int* ctl, const int* done,
+                                     const DevStatus* st, double* rho, int nr) {
+  const int c = ctl[0] + 1;
+  ctl[0] = c;
+  for (int k = 0; k < nr; ++k) rho[k] = rho[8 + k];
+  const bool more = c < ctl[1] && done[0] == 0 && st->code == 0;
+  cudaGraphSetConditional(handle, more ? 1u : 0u);
+}
+}  // namespace
+
+cudaError_t launch_pcg_loop_init(int* ctl, int max_iters, cudaStream_t stream) {
+  pcg_loop_init_kernel<<<1, 1, 0, stream>>>(ctl, max_iters);
+  return cudaGetLastError();
+}
+cudaError_t launch_pcg_loop_cond(cudaGraphConditionalHandle handle, int* ctl, const int* done,
+                                 const DevStatus* st, double* rho, int nr, cudaStream_t stream) {
+  pcg_loop_cond_kernel<<<1, 1, 0, stream>>>(handle, ctl, done, st, rho, nr);
+  return cudaGetLastError();
+}
+
 }  // namespace mpchol

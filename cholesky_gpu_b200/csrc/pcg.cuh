@@ -49,6 +49,13 @@ cudaError_t launch_reduce_partials(const double* partials, double* out, int nrhs
 cudaError_t launch_residual(const double* b, const double* y, double* r, int n, int nrhs,
                             double* rr_partials, cudaStream_t stream);
 cudaError_t launch_copy(const double* a, double* b, int n, int nrhs, cudaStream_t stream);
+// Device-side PCG loop (a WHILE node of a CUDA graph): ctl[0] <- 0,
+// ctl[1] <- max_iters before the loop; after each iteration the condition
+// kernel copies rho[8..8+nr) to rho[0..nr) and sets the loop condition
+// (continue while ctl[0] < ctl[1], *done == 0 and no recorded error).
+cudaError_t launch_pcg_loop_init(int* ctl, int max_iters, cudaStream_t stream);
+cudaError_t launch_pcg_loop_cond(cudaGraphConditionalHandle handle, int* ctl, const int* done,
+                                 const DevStatus* st, double* rho, int nr, cudaStream_t stream);
 
 // misc device utilities (util.cu)
 cudaError_t launch_extract_diag(const float* A, int lda, int n, float* d, float* dtilde,

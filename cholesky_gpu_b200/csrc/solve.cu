@@ -1064,6 +1064,21 @@ __global__ void copy_vec_kernel(const double* __restrict__ a, double* __restrict
     b[i] = a[i];
 }
 
+// The persistent solve's inputs: work <- in, out <- 0 and its dependency
+// counters cleared, in one launch.
+__global__ void trsv_prep_kernel(const double* __restrict__ in, double* __restrict__ work,
+                                 double* __restrict__ out, long long count, int* counters,
+                                 int ncounters, const int* skip) {
+  if (skip != nullptr && *skip) return;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long t0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  for (long long i = t0; i < count; i += stride) {
+    work[i] = in[i];
+    out[i] = 0.0;
+  }
+  for (long long i = t0; i < ncounters; i += stride) counters[i] = 0;
+}
+
 __global__ void zero_vec_kernel(double* __restrict__ a, long long count, const int* skip) {
   if (skip != nullptr && *skip) return;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
@@ -1251,17 +1266,17 @@ cudaError_t launch_trsv_batched(bool backward, const BatchSys* sys, int nsys, in
 
 size_t trsv_counter_ints(int n) { return 1 + 2 * (size_t)ceil_div(n, RB); }
 
-// The persistent solve: counters (trsv_counter_ints(n) ints) are cleared,
-// work <- in, out <- 0, then one cooperative launch over every resident CTA.
+// The persistent solve: work <- in, out <- 0 and the counters
+// (trsv_counter_ints(n) ints) cleared in one launch, then one cooperative
+// launch over every resident CTA.
 cudaError_t launch_trsv_persistent(bool backward, const float* L, int ldl, int n,
                                    const float* wsup, const double* in, double* out,
                                    double* work, int nrhs, int* counters, const int* skip,
                                    DevStatus* st, cudaStream_t stream) {
   const long long cnt = (long long)n * nrhs;
-  cudaError_t e = cudaMemsetAsync(counters, 0, sizeof(int) * trsv_counter_ints(n), stream);
-  if (e != cudaSuccess) return e;
-  copy_vec_kernel<1><<<148, 256, 0, stream>>>(in, work, cnt, skip);
-  zero_vec_kernel<<<148, 256, 0, stream>>>(out, cnt, skip);
+  cudaError_t e;
+  trsv_prep_kernel<<<148, 256, 0, stream>>>(in, work, out, cnt, counters, (int)trsv_counter_ints(n),
+                                            skip);
   static int grid_cache[64][2][4] = {};
   int dev = 0;
   if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
