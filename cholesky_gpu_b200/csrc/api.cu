@@ -113,6 +113,19 @@ struct CopyPlan {
   int c0[kMaxGroups] = {}, c1[kMaxGroups] = {}, join[kMaxGroups] = {};
 };
 
+// The factorization captured as one CUDA graph (its copies included for a
+// host-buffer solve with a copy plan) and what it was captured for.
+struct FactorGraph {
+  cudaGraphExec_t exec = nullptr;
+  bool failed = false;        // the runtime refused the graph: the work is launched directly
+  bool streamed = false;
+  CopyPlan plan;
+  const float* hA = nullptr;
+  const float* hA_dev = nullptr;
+  int lda = 0;
+  long long nk[MPCHOL_NPHASES] = {};
+};
+
 // The captured device-side PCG loop (a WHILE node whose body is one
 // iteration) and what it was captured for; nk: kernels per iteration.
 struct PcgGraph {
@@ -165,6 +178,7 @@ struct mpchol_factor {
   int* h_done = nullptr;      // pinned
   double* h_scal = nullptr;   // pinned
   PcgGraph graph;             // captured PCG loop (see run_pcg)
+  FactorGraph fgraph;         // captured factorization (see launch_factor)
   int* loop_ctl = nullptr;    // its iteration count and budget
   cudaStream_t capture_stream = nullptr;   // private stream used only to capture graphs
   // look-ahead: the bulk of each step's trailing update runs on aux while
@@ -237,6 +251,7 @@ void free_factor(mpchol_factor_t* f) {
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (f->graph.exec) cudaGraphExecDestroy(f->graph.exec);
+  if (f->fgraph.exec) cudaGraphExecDestroy(f->fgraph.exec);
   if (f->capture_stream) cudaStreamDestroy(f->capture_stream);
   if (f->aux) cudaStreamDestroy(f->aux);
   if (f->ev_next) cudaEventDestroy(f->ev_next);
@@ -399,6 +414,18 @@ bool valid_copy_plan(const CopyPlan& p, int nb) {
   return true;
 }
 
+// The second stream of the look-ahead and its events (created once, outside
+// any stream capture).
+mpchol_status ensure_factor_streams(mpchol_factor_t* f) {
+  if (f->aux != nullptr) return MPCHOL_OK;
+  MPCHOL_CUDA_TRY(cudaStreamCreateWithFlags(&f->aux, cudaStreamNonBlocking));
+  MPCHOL_CUDA_TRY(cudaEventCreateWithFlags(&f->ev_next, cudaEventDisableTiming));
+  MPCHOL_CUDA_TRY(cudaEventCreateWithFlags(&f->ev_rest, cudaEventDisableTiming));
+  MPCHOL_CUDA_TRY(cudaEventCreateWithFlags(&f->ev_catch, cudaEventDisableTiming));
+  MPCHOL_CUDA_TRY(cudaDeviceGetAttribute(&f->nsm, cudaDevAttrMultiProcessorCount, f->device));
+  return MPCHOL_OK;
+}
+
 // One factorization of f->A in place, on `stream`, right-looking with a
 // look-ahead of one block.  Step k: the panel solve (with the step decision
 // and the panel quantization), then the trailing update of the tiles of
@@ -419,13 +446,8 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream, const CopyPlan
   const int n = f->n, ld = f->ld, b = f->b;
   PotrfParams pp{o.diag_pert, o.pert, o.pivot_floor};
   const DecisionParams dp = make_dp(o);
-  if (f->aux == nullptr) {
-    MPCHOL_CUDA_TRY(cudaStreamCreateWithFlags(&f->aux, cudaStreamNonBlocking));
-    MPCHOL_CUDA_TRY(cudaEventCreateWithFlags(&f->ev_next, cudaEventDisableTiming));
-    MPCHOL_CUDA_TRY(cudaEventCreateWithFlags(&f->ev_rest, cudaEventDisableTiming));
-    MPCHOL_CUDA_TRY(cudaEventCreateWithFlags(&f->ev_catch, cudaEventDisableTiming));
-    MPCHOL_CUDA_TRY(cudaDeviceGetAttribute(&f->nsm, cudaDevAttrMultiProcessorCount, f->device));
-  }
+  mpchol_status es = ensure_factor_streams(f);
+  if (es != MPCHOL_OK) return es;
   const bool streamed = plan != nullptr && plan->ng > 1;
   const int cap = f->nsm > 1 ? f->nsm - 1 : 1;   // SMs for the concurrent part of the update
   MPCHOL_CUDA_TRY(cudaMemsetAsync(f->status, 0, sizeof(DevStatus), stream));
@@ -565,6 +587,95 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream, const CopyPlan
   }
   if (rest_pending) MPCHOL_CUDA_TRY(cudaStreamWaitEvent(stream, f->ev_rest, 0));
   if (streamed) MPCHOL_CUDA_TRY(cudaStreamWaitEvent(stream, f->ev_grp[plan->ng - 1], 0));
+  f->solve_ready = false;
+  return MPCHOL_OK;
+}
+
+bool same_plan(const CopyPlan& a, const CopyPlan& b) {
+  if (a.ng != b.ng) return false;
+  for (int g = 0; g < a.ng; ++g)
+    if (a.c0[g] != b.c0[g] || a.c1[g] != b.c1[g] || a.join[g] != b.join[g]) return false;
+  return true;
+}
+
+// Everything one factorization enqueues on `stream`.  With a copy plan: the
+// copy stream forks from `stream` and copies A's lower block columns group by
+// group (into the operator buffer, then device to device into the factor's
+// storage); the diagonal of A comes straight from the caller's page-locked
+// buffer (hA_dev, its device-side address) or, for pageable memory, from
+// f->h_diag, which the caller filled.
+mpchol_status enqueue_factor(mpchol_factor_t* f, cudaStream_t stream, const CopyPlan* plan,
+                             const float* hA, int lda, const float* hA_dev) {
+  if (plan == nullptr || plan->ng <= 1) return run_factor(f, stream);
+  const int n = f->n, b = f->b;
+  MPCHOL_CUDA_TRY(cudaEventRecord(f->ev_start, stream));
+  MPCHOL_CUDA_TRY(cudaStreamWaitEvent(f->cp, f->ev_start, 0));
+  for (int g = 0; g < plan->ng; ++g) {
+    MPCHOL_CUDA_TRY(copy_lower_cols(f->op, f->ld, hA, lda, n, b, plan->c0[g], plan->c1[g],
+                                    cudaMemcpyHostToDevice, f->cp));
+    MPCHOL_CUDA_TRY(copy_lower_cols(f->A, f->ld, f->op, f->ld, n, b, plan->c0[g], plan->c1[g],
+                                    cudaMemcpyDeviceToDevice, f->cp));
+    MPCHOL_CUDA_TRY(cudaEventRecord(f->ev_grp[g], f->cp));
+  }
+  // the switching statistics of step 0 read the whole diagonal
+  if (hA_dev != nullptr) {
+    PHASE(MPCHOL_PH_SETUP, 1, stream, launch_extract_diag(hA_dev, lda, n, f->d, f->dtilde, stream));
+  } else {
+    MPCHOL_CUDA_TRY(cudaMemcpyAsync(f->d, f->h_diag, sizeof(float) * n, cudaMemcpyHostToDevice, stream));
+    MPCHOL_CUDA_TRY(cudaMemcpyAsync(f->dtilde, f->d, sizeof(float) * n, cudaMemcpyDeviceToDevice, stream));
+  }
+  return run_factor(f, stream, plan);
+}
+
+// One factorization as a CUDA graph: captured on the first call (and again
+// when the copy plan or the host buffer changes), then relaunched, which
+// removes most of the launch gaps between the dependent kernels of the
+// critical path (panel solve -> head update -> POTRF -> next panel solve).
+// Profiling runs, and runtimes that refuse the graph, enqueue directly.
+mpchol_status launch_factor(mpchol_factor_t* f, cudaStream_t stream, const CopyPlan* plan = nullptr,
+                            const float* hA = nullptr, int lda = 0, const float* hA_dev = nullptr) {
+  const bool streamed = plan != nullptr && plan->ng > 1;
+  FactorGraph& g = f->fgraph;
+  if (profiling_on() || g.failed) return enqueue_factor(f, stream, plan, hA, lda, hA_dev);
+  const bool match = g.exec != nullptr && g.streamed == streamed &&
+                     (!streamed || (same_plan(g.plan, *plan) && g.hA == hA && g.lda == lda &&
+                                    g.hA_dev == hA_dev));
+  if (!match) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    g.exec = nullptr;
+    mpchol_status es = ensure_factor_streams(f);
+    if (es != MPCHOL_OK) return es;
+    if (f->capture_stream == nullptr)
+      MPCHOL_CUDA_TRY(cudaStreamCreateWithFlags(&f->capture_stream, cudaStreamNonBlocking));
+    long long before[MPCHOL_NPHASES];
+    launch_counts(before);
+    bool ok = cudaStreamBeginCapture(f->capture_stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (ok) {
+      const mpchol_status st = enqueue_factor(f, f->capture_stream, plan, hA, lda, hA_dev);
+      cudaGraph_t graph = nullptr;
+      const cudaError_t ce = cudaStreamEndCapture(f->capture_stream, &graph);
+      ok = st == MPCHOL_OK && ce == cudaSuccess && cudaGraphInstantiate(&g.exec, graph, 0) == cudaSuccess;
+      if (graph) cudaGraphDestroy(graph);
+    }
+    long long after[MPCHOL_NPHASES];
+    launch_counts(after);
+    for (int i = 0; i < MPCHOL_NPHASES; ++i) g.nk[i] = after[i] - before[i];
+    add_launch_counts(g.nk, -1);   // nothing ran during capture
+    if (!ok) {
+      cudaGetLastError();
+      if (g.exec) cudaGraphExecDestroy(g.exec);
+      g.exec = nullptr;
+      g.failed = true;
+      return enqueue_factor(f, stream, plan, hA, lda, hA_dev);
+    }
+    g.streamed = streamed;
+    if (streamed) g.plan = *plan;
+    g.hA = hA;
+    g.lda = lda;
+    g.hA_dev = hA_dev;
+  }
+  MPCHOL_CUDA_TRY(cudaGraphLaunch(g.exec, stream));
+  add_launch_counts(g.nk, 1);
   f->solve_ready = false;
   return MPCHOL_OK;
 }
@@ -975,7 +1086,7 @@ mpchol_status mpchol_factor_compute(mpchol_factor_t* f, const float* dA, int lda
   if (f == nullptr || dA == nullptr || lda < f->n) return MPCHOL_ERR_BAD_ARG;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   MPCHOL_CUDA_TRY(copy_lower_blocks(f->A, f->ld, dA, lda, f->n, f->b, cudaMemcpyDeviceToDevice, s));
-  return run_factor(f, s);
+  return launch_factor(f, s);
 }
 
 mpchol_status mpchol_factor_codes(const mpchol_factor_t* f, int fmt, const void** dCodes,
@@ -1021,7 +1132,7 @@ mpchol_status mpchol_solve_host(mpchol_factor_t* f, const float* hA, int lda, co
     MPCHOL_CUDA_TRY(copy_lower_blocks(f->op, f->ld, hA, lda, n, b, cudaMemcpyHostToDevice, s));
     MPCHOL_CUDA_TRY(cudaMemcpyAsync(f->hb, hB, sizeof(double) * n * nrhs, cudaMemcpyHostToDevice, s));
     MPCHOL_CUDA_TRY(copy_lower_blocks(f->A, f->ld, f->op, f->ld, n, b, cudaMemcpyDeviceToDevice, s));
-    mpchol_status st = run_factor(f, s);
+    mpchol_status st = launch_factor(f, s);
     if (st != MPCHOL_OK) return st;
   } else {
     if (f->cp == nullptr) {
@@ -1045,27 +1156,24 @@ mpchol_status mpchol_solve_host(mpchol_factor_t* f, const float* hA, int lda, co
       MPCHOL_CUDA_TRY(dmalloc(&f->hmx, (size_t)hist * (nbq / 32)));
       f->hist_steps = hist;
     }
-    // the copies wait for earlier work on the caller's stream (which may
-    // still read the operator and the factor), then run group by group
-    MPCHOL_CUDA_TRY(cudaEventRecord(f->ev_start, s));
-    MPCHOL_CUDA_TRY(cudaStreamWaitEvent(f->cp, f->ev_start, 0));
-    for (int g = 0; g < plan.ng; ++g) {
-      MPCHOL_CUDA_TRY(copy_lower_cols(f->op, f->ld, hA, lda, n, b, plan.c0[g], plan.c1[g],
-                                      cudaMemcpyHostToDevice, f->cp));
-      MPCHOL_CUDA_TRY(copy_lower_cols(f->A, f->ld, f->op, f->ld, n, b, plan.c0[g], plan.c1[g],
-                                      cudaMemcpyDeviceToDevice, f->cp));
-      MPCHOL_CUDA_TRY(cudaEventRecord(f->ev_grp[g], f->cp));
+    // The copies wait for earlier work on the caller's stream (which may
+    // still read the operator and the factor).  A page-locked A is read by
+    // the device directly for its diagonal; for pageable memory the host
+    // gathers it (after the previous call's copy of it has finished).
+    const float* hA_dev = nullptr;
+    cudaPointerAttributes pa{};
+    if (cudaPointerGetAttributes(&pa, hA) == cudaSuccess && pa.type == cudaMemoryTypeHost &&
+        pa.devicePointer != nullptr)
+      hA_dev = static_cast<const float*>(pa.devicePointer);
+    cudaGetLastError();
+    if (hA_dev == nullptr) {
+      MPCHOL_CUDA_TRY(cudaEventSynchronize(f->ev_diag));
+      for (int i = 0; i < n; ++i) f->h_diag[i] = hA[(size_t)i * lda + i];
     }
-    // the diagonal of A (the switching statistics of step 0 read all of
-    // it) is gathered on the host while the first group is copied
-    MPCHOL_CUDA_TRY(cudaEventSynchronize(f->ev_diag));
-    for (int i = 0; i < n; ++i) f->h_diag[i] = hA[(size_t)i * lda + i];
-    MPCHOL_CUDA_TRY(cudaMemcpyAsync(f->d, f->h_diag, sizeof(float) * n, cudaMemcpyHostToDevice, s));
-    MPCHOL_CUDA_TRY(cudaMemcpyAsync(f->dtilde, f->d, sizeof(float) * n, cudaMemcpyDeviceToDevice, s));
-    MPCHOL_CUDA_TRY(cudaEventRecord(f->ev_diag, s));
     MPCHOL_CUDA_TRY(cudaMemcpyAsync(f->hb, hB, sizeof(double) * n * nrhs, cudaMemcpyHostToDevice, s));
-    mpchol_status st = run_factor(f, s, &plan);
+    mpchol_status st = launch_factor(f, s, &plan, hA, lda, hA_dev);
     if (st != MPCHOL_OK) return st;
+    MPCHOL_CUDA_TRY(cudaEventRecord(f->ev_diag, s));
   }
   mpchol_status st = run_pcg<float>(f, f->op, f->ld, f->hb, f->hx, nrhs, opts, rep, s);
   if (st != MPCHOL_OK && st != MPCHOL_PCG_MAXIT) return st;
