@@ -118,6 +118,7 @@ struct CopyPlan {
 struct FactorGraph {
   cudaGraphExec_t exec = nullptr;
   bool failed = false;        // the runtime refused the graph: the work is launched directly
+  bool seen = false;          // the key below was that of the previous call
   bool streamed = false;
   CopyPlan plan;
   const float* hA = nullptr;
@@ -627,22 +628,33 @@ mpchol_status enqueue_factor(mpchol_factor_t* f, cudaStream_t stream, const Copy
   return run_factor(f, stream, plan);
 }
 
-// One factorization as a CUDA graph: captured on the first call (and again
-// when the copy plan or the host buffer changes), then relaunched, which
-// removes most of the launch gaps between the dependent kernels of the
-// critical path (panel solve -> head update -> POTRF -> next panel solve).
+// One factorization as a CUDA graph, relaunched while the copy plan and the
+// host buffer stay the same, which removes most of the launch gaps between
+// the dependent kernels of the critical path (panel solve -> head update ->
+// POTRF -> next panel solve).  The graph is captured on the second
+// consecutive call with the same key: a factor object used once, or a
+// caller that passes a new host buffer every time, pays no capture.
 // Profiling runs, and runtimes that refuse the graph, enqueue directly.
 mpchol_status launch_factor(mpchol_factor_t* f, cudaStream_t stream, const CopyPlan* plan = nullptr,
                             const float* hA = nullptr, int lda = 0, const float* hA_dev = nullptr) {
   const bool streamed = plan != nullptr && plan->ng > 1;
   FactorGraph& g = f->fgraph;
   if (profiling_on() || g.failed) return enqueue_factor(f, stream, plan, hA, lda, hA_dev);
-  const bool match = g.exec != nullptr && g.streamed == streamed &&
-                     (!streamed || (same_plan(g.plan, *plan) && g.hA == hA && g.lda == lda &&
-                                    g.hA_dev == hA_dev));
-  if (!match) {
+  const bool same_key = g.seen && g.streamed == streamed &&
+                        (!streamed || (same_plan(g.plan, *plan) && g.hA == hA && g.lda == lda &&
+                                       g.hA_dev == hA_dev));
+  if (!same_key) {
     if (g.exec) cudaGraphExecDestroy(g.exec);
     g.exec = nullptr;
+    g.seen = true;
+    g.streamed = streamed;
+    if (streamed) g.plan = *plan;
+    g.hA = hA;
+    g.lda = lda;
+    g.hA_dev = hA_dev;
+    return enqueue_factor(f, stream, plan, hA, lda, hA_dev);
+  }
+  if (g.exec == nullptr) {
     mpchol_status es = ensure_factor_streams(f);
     if (es != MPCHOL_OK) return es;
     if (f->capture_stream == nullptr)
@@ -668,11 +680,6 @@ mpchol_status launch_factor(mpchol_factor_t* f, cudaStream_t stream, const CopyP
       g.failed = true;
       return enqueue_factor(f, stream, plan, hA, lda, hA_dev);
     }
-    g.streamed = streamed;
-    if (streamed) g.plan = *plan;
-    g.hA = hA;
-    g.lda = lda;
-    g.hA_dev = hA_dev;
   }
   MPCHOL_CUDA_TRY(cudaGraphLaunch(g.exec, stream));
   add_launch_counts(g.nk, 1);
