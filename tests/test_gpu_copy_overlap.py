@@ -41,8 +41,12 @@ def test_streamed_factor_is_bit_identical(cuda, n, b, opts, cuts, join):
     f_host = mp.Factor(n, block_size=b, **opts)
     if cuts is not None:
         f_host.set_copy_plan(cuts, join)
-    for _ in range(2):   # the second call reuses the copy stream and the panel history
-        X, rep = f_host.solve_host(A.pin_memory(), B.pin_memory(), rel_tol=1e-10)
+    A_pin, B_pin = A.pin_memory(), B.pin_memory()
+    # call 1 launches the factorization directly, call 2 (same buffer, same
+    # plan) captures it as a CUDA graph, call 3 relaunches that graph; all
+    # reuse the copy stream and the panel history
+    for _ in range(3):
+        X, rep = f_host.solve_host(A_pin, B_pin, rel_tol=1e-10)
         assert rep.converged
         i_host = f_host.info()
         assert i_host.step_prec == i_dev.step_prec
@@ -65,3 +69,22 @@ def test_copy_plan_is_validated(cuda):
     g = mp.Factor(2048, block_size=64, precision="fp16x2")
     with pytest.raises(mp.MpcholError):
         g.set_copy_plan([4], [2])          # 128-row tiles would straddle groups
+
+
+@pytest.mark.parametrize("opts", [LADDER, dict(precision="fp32")])
+def test_factor_graph_relaunch_is_bit_identical(cuda, opts):
+    """Repeated compute() on one factor object: the first call launches the
+    kernels directly, the second captures the factorization as a CUDA graph,
+    later calls relaunch it.  Every factor must be the same bits."""
+    n = 1536
+    A = matgen.spd_matrix(n, 1e5, 61).cuda()
+    f = mp.Factor(n, block_size=256, **opts)
+    ref = None
+    for _ in range(4):
+        f.compute(A)
+        L = f.lower().cpu().numpy()
+        if ref is None:
+            ref, prec = L, f.info().step_prec
+        else:
+            assert np.array_equal(L, ref)
+            assert f.info().step_prec == prec
