@@ -95,7 +95,8 @@ typedef struct {
   double rel_tol;      /* stop when the FP64 true residual ||b-Ax||/||b|| <= rel_tol (every rhs) */
   int max_it;          /* iteration cap (the reference uses 200, src/mixed_cholesky.cu:82) */
   int x0_precond;      /* 1: x0 = M^-1 b as the reference (src/mixed_cholesky.cu:145-149); 0: x0 = 0 */
-  int check_every;     /* iterations between host convergence checks (>= 1) */
+  int check_every;     /* iterations between host convergence checks (>= 1) when
+                          the iterations are launched directly (see mpchol_pcg) */
 } mpchol_pcg_opts;
 
 typedef struct {
@@ -149,7 +150,10 @@ MPCHOL_API const char* mpchol_last_error(void);
 MPCHOL_API mpchol_status mpchol_factor_create(const mpchol_opts* opts, int n, mpchol_factor_t** out);
 /* Copy the lower triangle of dA (n x n, lda >= n) into the object and factor
  * it on `stream`.  Asynchronous: failures inside kernels are reported by
- * mpchol_factor_info. */
+ * mpchol_factor_info.  The second and later calls on one object run the
+ * factorization as a CUDA graph the object captures (on a private stream) and
+ * keeps; the first launches the kernels directly.  The factor is the same
+ * either way. */
 MPCHOL_API mpchol_status mpchol_factor_compute(mpchol_factor_t* f, const float* dA, int lda, mpchol_stream_t stream);
 /* create + compute. */
 MPCHOL_API mpchol_status mpchol_factor(const mpchol_opts* opts, int n, const float* dA, int lda,
@@ -180,9 +184,13 @@ MPCHOL_API mpchol_status mpchol_factor_prepare_solve(mpchol_factor_t* f, mpchol_
 /* ---- PCG (precond_CG, src/mixed_cholesky.cu:76-229) ---------------------- */
 /* Solve A X = B for nrhs (1..8) right-hand sides with M = L L^T.  dA is the
  * FP32 operator (full symmetric storage), dB/dX are n x nrhs FP64 (ld = n).
- * Synchronizes `stream` every check_every iterations (convergence test on
- * the recursive residual; the final answer is re-checked on the true
- * residual).  report may be NULL. */
+ * The iterations run in a device-side loop (a CUDA graph the object keeps)
+ * that stops when the recursive residual meets the tolerance or max_it is
+ * reached; `stream` is synchronized after each such loop and the answer is
+ * re-checked on the true residual (restarting from it if needed).  When the
+ * runtime refuses the graph, or profiling is on, iterations are launched
+ * directly and `stream` is synchronized every check_every iterations.
+ * report may be NULL. */
 MPCHOL_API mpchol_status mpchol_pcg(mpchol_factor_t* f, const float* dA, int lda, const double* dB,
                          double* dX, int nrhs, const mpchol_pcg_opts* opts, mpchol_report* report,
                          mpchol_stream_t stream);
