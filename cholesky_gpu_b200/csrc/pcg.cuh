@@ -22,18 +22,15 @@ template <typename TA>
 bool symv_staged_ok(const TA* A, int lda);
 // 128-block inverses into winv, then the super-block inverses into wsup.
 cudaError_t launch_solve_setup(const float* L, int ldl, int n, float* wsup, cudaStream_t stream);
-// out = L^-1 in (forward) or L^-T in (backward); work is an n x nrhs scratch.
-// *launches receives the number of kernels launched.
-// The same solve as one persistent cooperative launch (plus counter reset and
-// two vector kernels); counters: trsv_counter_ints(n) ints of scratch.
+// out = L^-1 in (forward) or L^-T in (backward) through the super-block
+// inverses wsup: one launch that prepares work <- in, out <- 0 and clears the
+// counters, then one persistent cooperative launch; work is an n x nrhs
+// scratch, counters trsv_counter_ints(n) ints.
 size_t trsv_counter_ints(int n);
 cudaError_t launch_trsv_persistent(bool backward, const float* L, int ldl, int n,
                                    const float* wsup, const double* in, double* out,
                                    double* work, int nrhs, int* counters, const int* skip,
                                    DevStatus* st, cudaStream_t stream);
-cudaError_t launch_trsv_super(bool backward, const float* L, int ldl, int n, const float* wsup,
-                              const double* in, double* out, double* work, int nrhs,
-                              const int* skip, cudaStream_t stream, int* launches);
 cudaError_t launch_dot(const double* a, const double* b, int n, int nrhs, double* partials,
                        const int* skip, cudaStream_t stream);
 cudaError_t launch_update_xr(double* x, double* r, const double* p, const double* Ap, int n,

@@ -739,12 +739,6 @@ trmv_super_body(const float* __restrict__ W, int n, int s0, int rs, const double
   }
 }
 
-template <int NR, bool TRANS>
-__global__ void __launch_bounds__(NTH)
-trmv_super_kernel(const float* __restrict__ W, int n, int s0, int rs, const double* __restrict__ in,
-                  double* __restrict__ out, const int* skip) {
-  trmv_super_body<NR, TRANS>(W, n, s0, rs, in, out, skip, blockIdx);
-}
 
 // ---- panel updates ---------------------------------------------------------
 // forward: w[rows below the super-block] -= L(rows, super-block cols) y_S
@@ -782,12 +776,6 @@ panel_body(const float* __restrict__ L, int ldl, int n, int s0, int rs,
   }
 }
 
-template <int NR, bool TRANS>
-__global__ void __launch_bounds__(NTH)
-panel_kernel(const float* __restrict__ L, int ldl, int n, int s0, int rs,
-             const double* __restrict__ v, double* __restrict__ w, const int* skip) {
-  panel_body<NR, TRANS>(L, ldl, n, s0, rs, v, w, skip, blockIdx);
-}
 
 // ---- persistent triangular solve -------------------------------------------
 // One launch per solve.  The tiles of a solve form a dependency DAG: for
@@ -1055,15 +1043,6 @@ panel_batched_kernel(const BatchSys* __restrict__ sys, int sup, int v_slot, int 
                         use_skip ? S.done : nullptr, make_uint3(blockIdx.x, blockIdx.y, 0));
 }
 
-template <int NR>
-__global__ void copy_vec_kernel(const double* __restrict__ a, double* __restrict__ b, long long count,
-                                const int* skip) {
-  if (skip != nullptr && *skip) return;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
-       i += (long long)gridDim.x * blockDim.x)
-    b[i] = a[i];
-}
-
 // The persistent solve's inputs: work <- in, out <- 0 and its dependency
 // counters cleared, in one launch.
 __global__ void trsv_prep_kernel(const double* __restrict__ in, double* __restrict__ work,
@@ -1130,11 +1109,7 @@ cudaError_t solve_set_attributes() {
   if ((e = set_dyn(block_inverse_kernel, inv)) != cudaSuccess) return e;
 #define SET_NR(NRC)                                                                         \
   if ((e = set_dyn(symv_kernel<float, NRC>, red_bytes(NRC))) != cudaSuccess) return e;      \
-  if ((e = set_dyn(symv_kernel<double, NRC>, red_bytes(NRC))) != cudaSuccess) return e;     \
-  if ((e = set_dyn(trmv_super_kernel<NRC, false>, red_bytes(NRC))) != cudaSuccess) return e; \
-  if ((e = set_dyn(trmv_super_kernel<NRC, true>, red_bytes(NRC))) != cudaSuccess) return e;  \
-  if ((e = set_dyn(panel_kernel<NRC, false>, red_bytes(NRC))) != cudaSuccess) return e;      \
-  if ((e = set_dyn(panel_kernel<NRC, true>, red_bytes(NRC))) != cudaSuccess) return e;
+  if ((e = set_dyn(symv_kernel<double, NRC>, red_bytes(NRC))) != cudaSuccess) return e;
   SET_NR(1) SET_NR(2) SET_NR(4) SET_NR(8)
 #undef SET_NR
 #define SET_NRP(NRC)                                                                              \
@@ -1313,40 +1288,5 @@ cudaError_t launch_trsv_persistent(bool backward, const float* L, int ldl, int n
   return cudaGetLastError();
 }
 
-// out = L^-1 in (forward) or L^-T in (backward); work is an n x nrhs scratch.
-cudaError_t launch_trsv_super(bool backward, const float* L, int ldl, int n, const float* wsup,
-                              const double* in, double* out, double* work, int nrhs,
-                              const int* skip, cudaStream_t stream, int* launches) {
-  const long long cnt = (long long)n * nrhs;
-  copy_vec_kernel<1><<<148, 256, 0, stream>>>(in, work, cnt, skip);
-  zero_vec_kernel<<<148, 256, 0, stream>>>(out, cnt, skip);
-  int nl = 2;
-  const int nbs = ceil_div(n, RS);
-  for (int t = 0; t < nbs; ++t) {
-    const int S = backward ? nbs - 1 - t : t;
-    const int s0 = S * RS;
-    const int rs = min(RS, n - s0);
-    const int nsub = ceil_div(rs, RB);
-    const float* W = wsup + (size_t)S * RS * RS;
-    if (!backward) {
-      NR_SWITCH(nrhs, (trmv_super_kernel<NRC, false><<<nsub * (nsub + 1) / 2, NTH, red_bytes(NRC), stream>>>(W, n, s0, rs, work, out, skip)));
-      ++nl;
-      const int below = n - s0 - rs;
-      if (below > 0) {
-        NR_SWITCH(nrhs, (panel_kernel<NRC, false><<<dim3(ceil_div(below, RB), nsub), NTH, red_bytes(NRC), stream>>>(L, ldl, n, s0, rs, out, work, skip)));
-        ++nl;
-      }
-    } else {
-      NR_SWITCH(nrhs, (trmv_super_kernel<NRC, true><<<nsub * (nsub + 1) / 2, NTH, red_bytes(NRC), stream>>>(W, n, s0, rs, work, out, skip)));
-      ++nl;
-      if (s0 > 0) {
-        NR_SWITCH(nrhs, (panel_kernel<NRC, true><<<dim3(ceil_div(s0, RB), nsub), NTH, red_bytes(NRC), stream>>>(L, ldl, n, s0, rs, out, work, skip)));
-        ++nl;
-      }
-    }
-  }
-  if (launches) *launches = nl;
-  return cudaGetLastError();
-}
 
 }  // namespace mpchol
