@@ -10,9 +10,10 @@ from ._lib import (  # noqa: F401
     MpcholError, load,
 )
 from .api import (  # noqa: F401
-    Batch, Factor, FactorInfo, Report, copy_plan, factor, precond_CG, solve, switching_chol,
+    Batch, Factor, FactorInfo, Report, copy_plan, factor, factor_blob_info, precond_CG, solve,
+    switching_chol,
 )
 from .autograd import RBFSolve, rbf_build, rbf_solve  # noqa: F401
 
 __all__ = ["Factor", "FactorInfo", "Report", "factor", "solve", "precond_CG", "switching_chol",
-           "copy_plan", "load", "MpcholError"]
+           "copy_plan", "factor_blob_info", "load", "MpcholError"]

@@ -123,6 +123,9 @@ SIGNATURES = {
     "mpchol_solve_host": (_i, [_vp, _vp, _i, _vp, _vp, _i, ctypes.POINTER(PcgOpts), ctypes.POINTER(Report), _vp]),
     "mpchol_factor_codes": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp]),
     "mpchol_set_copy_plan": (_i, [_vp, _i, _vp, _vp]),
+    "mpchol_factor_save": (_i, [_vp, _vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t), _vp]),
+    "mpchol_factor_load": (_i, [_vp, _vp, ctypes.c_size_t, _vp]),
+    "mpchol_factor_blob_check": (_i, [_vp, ctypes.c_size_t, ctypes.POINTER(_i), ctypes.POINTER(_i)]),
     "mpchol_copy_plan": (_i, [_i, _i, _vp, _vp, _i]),
     "mpchol_apply_precond": (_i, [_vp, _vp, _vp, _i, _vp]),
     "mpchol_symv": (_i, [_vp, _i, _i, _vp, _vp, _i, _vp]),

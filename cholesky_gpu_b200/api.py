@@ -167,6 +167,26 @@ class Factor:
         Z = Z.t()
         return Z.reshape(R.shape) if R.dim() == 1 else Z
 
+    def save(self) -> bytes:
+        """The computed factor as a byte blob (header, L's lower block columns,
+        per-step states, diagonals, status) that load() restores into a factor
+        object of the same order and block size, so solves can reuse it
+        without refactoring."""
+        size = ctypes.c_size_t()
+        check(self.lib.mpchol_factor_save(self.handle, None, 0, ctypes.byref(size), _stream_handle()),
+              "mpchol_factor_save")
+        buf = ctypes.create_string_buffer(size.value)
+        check(self.lib.mpchol_factor_save(self.handle, buf, size.value, ctypes.byref(size),
+                                          _stream_handle()), "mpchol_factor_save")
+        return buf.raw
+
+    def load(self, blob: bytes) -> "Factor":
+        """Replace this object's factor by a saved one (same n and block size)."""
+        data = bytes(blob)
+        check(self.lib.mpchol_factor_load(self.handle, data, len(data), _stream_handle()),
+              "mpchol_factor_load")
+        return self
+
     def set_copy_plan(self, cuts=None, join=None) -> None:
         """Fix the copy groups of solve_host: cuts (block columns where groups
         start, increasing) and join (the step at which each later group joins
@@ -263,6 +283,17 @@ def _wrap_device(ptr: int, shape: tuple, dtype: torch.dtype) -> torch.Tensor:
 
     del numel, itemsize
     return torch.as_tensor(_Holder(), device="cuda")
+
+
+def factor_blob_info(blob: bytes) -> tuple[int, int]:
+    """(n, block_size) of a factor blob from Factor.save(), after checking its
+    header, sizes and checksum on the host; raises MpcholError if invalid."""
+    lib = _lib.load()
+    data = bytes(blob)
+    n, b = ctypes.c_int(), ctypes.c_int()
+    check(lib.mpchol_factor_blob_check(data, len(data), ctypes.byref(n), ctypes.byref(b)),
+          "mpchol_factor_blob_check")
+    return n.value, b.value
 
 
 def copy_plan(n: int, block_size: int = 256) -> tuple[list[int], list[int]]:

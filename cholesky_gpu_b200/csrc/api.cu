@@ -947,6 +947,78 @@ mpchol_status run_pcg(mpchol_factor_t* f, const TA* dA, int lda, const double* d
   return converged ? MPCHOL_OK : MPCHOL_PCG_MAXIT;
 }
 
+// ---- factor blobs (mpchol_factor_save / _load / _blob_check) --------------
+struct FactorBlobHeader {
+  char magic[8];               // "MPCHOLF1"
+  uint32_t version;            // 1
+  uint32_t header_bytes;       // sizeof(FactorBlobHeader)
+  int32_t n, b, nsteps;
+  uint32_t step_bytes;         // sizeof(StepState)
+  uint64_t l_bytes;            // L's lower block columns, packed
+  uint64_t total_bytes;        // header + payload
+  uint64_t checksum;           // blob_hash of the payload
+  uint64_t reserved;
+};
+static_assert(sizeof(FactorBlobHeader) == 64, "the blob header is 64 bytes");
+constexpr char kBlobMagic[8] = {'M', 'P', 'C', 'H', 'O', 'L', 'F', '1'};
+
+// Bytes of the lower block columns of an n x n matrix with block b: each
+// block column from its diagonal down.
+uint64_t blob_l_bytes(int n, int b) {
+  uint64_t t = 0;
+  for (int c = 0; c < n; c += b) t += (uint64_t)(n - c) * std::min(b, n - c) * sizeof(float);
+  return t;
+}
+uint64_t blob_total_bytes(int n, int b, int nsteps) {
+  return sizeof(FactorBlobHeader) + blob_l_bytes(n, b) + (uint64_t)(nsteps + 1) * sizeof(StepState) +
+         2 * (uint64_t)n * sizeof(float) + sizeof(DevStatus);
+}
+// 64-bit FNV-1a over little-endian 8-byte words (the tail zero-padded).
+uint64_t blob_hash(const unsigned char* p, size_t len) {
+  uint64_t h = 0xcbf29ce484222325ull;
+  size_t i = 0;
+  for (; i + 8 <= len; i += 8) {
+    uint64_t w;
+    memcpy(&w, p + i, 8);
+    h = (h ^ w) * 0x100000001b3ull;
+  }
+  if (i < len) {
+    uint64_t w = 0;
+    memcpy(&w, p + i, len - i);
+    h = (h ^ w) * 0x100000001b3ull;
+  }
+  return h;
+}
+// Host <-> device copies of a factor's state in blob order; `host` points
+// just past the header.
+cudaError_t blob_copy(mpchol_factor_t* f, unsigned char* host, bool to_host, cudaStream_t s) {
+  const int n = f->n, b = f->b;
+  const cudaMemcpyKind kind = to_host ? cudaMemcpyDeviceToHost : cudaMemcpyHostToDevice;
+  unsigned char* p = host;
+  for (int c = 0; c < n; c += b) {
+    const int w = std::min(b, n - c);
+    const size_t col = sizeof(float) * (n - c);
+    float* dev = f->A + (size_t)c * f->ld + c;
+    cudaError_t e = to_host
+        ? cudaMemcpy2DAsync(p, col, dev, sizeof(float) * f->ld, col, w, kind, s)
+        : cudaMemcpy2DAsync(dev, sizeof(float) * f->ld, p, col, col, w, kind, s);
+    if (e != cudaSuccess) return e;
+    p += col * w;
+  }
+  struct Part { void* dev; size_t bytes; };
+  const Part parts[] = {{f->steps, sizeof(StepState) * (f->nsteps + 1)},
+                        {f->d, sizeof(float) * n},
+                        {f->dtilde, sizeof(float) * n},
+                        {f->status, sizeof(DevStatus)}};
+  for (const Part& q : parts) {
+    cudaError_t e = to_host ? cudaMemcpyAsync(p, q.dev, q.bytes, kind, s)
+                            : cudaMemcpyAsync(q.dev, p, q.bytes, kind, s);
+    if (e != cudaSuccess) return e;
+    p += q.bytes;
+  }
+  return cudaSuccess;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1276,6 +1348,67 @@ mpchol_status mpchol_factor_lower(const mpchol_factor_t* f, const float** dL, in
   if (dL) *dL = f->A;
   if (ldl) *ldl = f->ld;
   if (n) *n = f->n;
+  return MPCHOL_OK;
+}
+
+mpchol_status mpchol_factor_blob_check(const void* blob, size_t size, int* n, int* block_size) {
+  if (blob == nullptr || size < sizeof(FactorBlobHeader)) return MPCHOL_ERR_BAD_ARG;
+  FactorBlobHeader h;
+  memcpy(&h, blob, sizeof(h));
+  if (memcmp(h.magic, kBlobMagic, 8) != 0 || h.version != 1 ||
+      h.header_bytes != sizeof(FactorBlobHeader) || h.step_bytes != sizeof(StepState))
+    return MPCHOL_ERR_BAD_ARG;
+  if (h.n < 1 || h.b < 32 || h.b > 256 || h.b % 32 != 0 || h.nsteps != (h.n + h.b - 1) / h.b)
+    return MPCHOL_ERR_BAD_ARG;
+  if (h.l_bytes != blob_l_bytes(h.n, h.b) || h.total_bytes != blob_total_bytes(h.n, h.b, h.nsteps) ||
+      size < h.total_bytes)
+    return MPCHOL_ERR_BAD_ARG;
+  const unsigned char* p = static_cast<const unsigned char*>(blob);
+  if (blob_hash(p + sizeof(h), h.total_bytes - sizeof(h)) != h.checksum) return MPCHOL_ERR_BAD_ARG;
+  if (n) *n = h.n;
+  if (block_size) *block_size = h.b;
+  return MPCHOL_OK;
+}
+
+mpchol_status mpchol_factor_save(const mpchol_factor_t* fc, void* blob, size_t cap, size_t* size,
+                                 mpchol_stream_t stream) {
+  mpchol_factor_t* f = const_cast<mpchol_factor_t*>(fc);
+  if (f == nullptr || size == nullptr) return MPCHOL_ERR_BAD_ARG;
+  const uint64_t total = blob_total_bytes(f->n, f->b, f->nsteps);
+  *size = (size_t)total;
+  if (blob == nullptr) return MPCHOL_OK;
+  if (cap < total) return MPCHOL_ERR_BAD_ARG;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  unsigned char* out = static_cast<unsigned char*>(blob);
+  MPCHOL_CUDA_TRY(blob_copy(f, out + sizeof(FactorBlobHeader), true, s));
+  MPCHOL_CUDA_TRY(cudaStreamSynchronize(s));
+  FactorBlobHeader h{};
+  memcpy(h.magic, kBlobMagic, 8);
+  h.version = 1;
+  h.header_bytes = sizeof(FactorBlobHeader);
+  h.n = f->n;
+  h.b = f->b;
+  h.nsteps = f->nsteps;
+  h.step_bytes = sizeof(StepState);
+  h.l_bytes = blob_l_bytes(f->n, f->b);
+  h.total_bytes = total;
+  h.checksum = blob_hash(out + sizeof(h), total - sizeof(h));
+  memcpy(out, &h, sizeof(h));
+  return MPCHOL_OK;
+}
+
+mpchol_status mpchol_factor_load(mpchol_factor_t* f, const void* blob, size_t size,
+                                 mpchol_stream_t stream) {
+  if (f == nullptr) return MPCHOL_ERR_BAD_ARG;
+  int n = 0, b = 0;
+  const mpchol_status st = mpchol_factor_blob_check(blob, size, &n, &b);
+  if (st != MPCHOL_OK) return st;
+  if (n != f->n || b != f->b) return MPCHOL_ERR_BAD_ARG;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  unsigned char* in = const_cast<unsigned char*>(static_cast<const unsigned char*>(blob));
+  MPCHOL_CUDA_TRY(blob_copy(f, in + sizeof(FactorBlobHeader), false, s));
+  MPCHOL_CUDA_TRY(cudaStreamSynchronize(s));
+  f->solve_ready = false;
   return MPCHOL_OK;
 }
 

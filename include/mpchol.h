@@ -166,6 +166,30 @@ MPCHOL_API mpchol_status mpchol_factor_info_get(const mpchol_factor_t* f, mpchol
                                      int* hStepPrec, int* hStepFp64, mpchol_stream_t stream);
 /* Device pointer to the factor L (lower triangle valid; upper unspecified). */
 MPCHOL_API mpchol_status mpchol_factor_lower(const mpchol_factor_t* f, const float** dL, int* ldl, int* n);
+/* ---- factor serialization (reuse without refactoring) ------------------ */
+/* A computed factor as a host byte blob: a 64-byte header (magic "MPCHOLF1",
+ * version 1, n, block size, step count, payload sizes, a 64-bit checksum of
+ * the payload), then L's lower block columns packed (each block column from
+ * its diagonal down, column by column, FP32), the per-step states (chosen
+ * precision, FP64-diagonal flag, switching statistics), the diagonals d and
+ * d-tilde, and the status word (perturbed pivots, failure).  The panel codes
+ * are not saved: PCG needs only L.  The blob is for the same library build
+ * and byte order.
+ * mpchol_factor_save: *size receives the blob size; blob == NULL only
+ * queries it; cap < size is MPCHOL_ERR_BAD_ARG.  Synchronizes `stream`
+ * (the factor must have been computed on it or before it).
+ * mpchol_factor_load: replaces the factor of f (same n and block size as the
+ * blob, else MPCHOL_ERR_BAD_ARG) and its solve-side data is rebuilt on the
+ * next solve; synchronizes `stream`.
+ * mpchol_factor_blob_check: host-only validation of a blob (magic, version,
+ * sizes, checksum); writes n and the block size.  No counterpart in the
+ * reference, which refactors for every solve. */
+MPCHOL_API mpchol_status mpchol_factor_save(const mpchol_factor_t* f, void* blob, size_t cap,
+                                            size_t* size, mpchol_stream_t stream);
+MPCHOL_API mpchol_status mpchol_factor_load(mpchol_factor_t* f, const void* blob, size_t size,
+                                            mpchol_stream_t stream);
+MPCHOL_API mpchol_status mpchol_factor_blob_check(const void* blob, size_t size, int* n,
+                                                  int* block_size);
 /* Inspection of the last trailing update's quantized panel (the codes the
  * panel solve of the factorization's last step wrote for format fmt, one of
  * the step's candidates): dCodes, K-major, *rows rows of *ldq codes (FP16X2:

@@ -231,3 +231,32 @@ def test_reported_backward_error_matches_numpy(cuda, n):
     bb = b.numpy()
     be = np.linalg.norm(bb - A64 @ x) / (np.linalg.norm(A64) * np.linalg.norm(x) + np.linalg.norm(bb))
     assert rep.backward_error == pytest.approx(be, rel=0.05), (rep.backward_error, be)
+
+
+def test_factor_save_load_round_trip(cuda):
+    """A saved factor restored into a new object gives the same L bits, the
+    same step precisions and the same PCG solve without refactoring; a blob
+    of another order or block size is refused."""
+    n = 1000
+    A = matgen.spd_matrix(n, 1e4, 71)
+    B = matgen.rhs(n, 2, 72).to(torch.float64)
+    opts = dict(block_size=256, precision="switching", eps_prime=1e-5,
+                ladder=["e4m3", "fp16", "fp16x2"])
+    f = mp.Factor(n, **opts)
+    f.compute(A.cuda())
+    X1, r1 = f.pcg(A.cuda(), B.cuda(), rel_tol=1e-10)
+    blob = f.save()
+    assert mp.factor_blob_info(blob) == (n, 256)
+    g = mp.Factor(n, **opts).load(blob)
+    assert torch.equal(g.lower(), f.lower())
+    fi, gi = f.info(), g.info()
+    assert gi.step_prec == fi.step_prec and gi.step_fp64 == fi.step_fp64
+    assert gi.status == fi.status and gi.n_perturbed == fi.n_perturbed
+    X2, r2 = g.pcg(A.cuda(), B.cuda(), rel_tol=1e-10)
+    assert r2.converged and r2.iterations == r1.iterations
+    x1, x2 = X1.cpu().numpy(), X2.cpu().numpy()
+    assert np.linalg.norm(x2 - x1) / np.linalg.norm(x1) < 1e-8
+    with pytest.raises(mp.MpcholError):
+        mp.Factor(n + 1, **opts).load(blob)
+    with pytest.raises(mp.MpcholError):
+        mp.Factor(n, **dict(opts, block_size=128)).load(blob)
