@@ -772,7 +772,8 @@ mpchol_status run_pcg(mpchol_factor_t* f, const TA* dA, int lda, const double* d
   }
   const double tol2 = po.rel_tol * po.rel_tol;
   int it = 0;         // iterations executed on the device
-  int launched = 0;   // iterations enqueued (later ones return at once after convergence)
+  int launched = 0;   // iterations counted against max_it (the direct path also counts
+                      // iterations enqueued past convergence, which return at once)
   bool converged = false;
   const int max_restarts = 3;
   for (int restart = 0;; ++restart) {
