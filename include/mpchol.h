@@ -214,7 +214,9 @@ MPCHOL_API mpchol_status mpchol_factor_prepare_solve(mpchol_factor_t* f, mpchol_
  * re-checked on the true residual (restarting from it if needed).  When the
  * runtime refuses the graph, or profiling is on, iterations are launched
  * directly and `stream` is synchronized every check_every iterations.
- * report may be NULL. */
+ * report may be NULL.  The solve reuses the factor object's device status
+ * word (for breakdown and timeouts), so read mpchol_factor_info_get's
+ * n_perturbed and fail_row before solving. */
 MPCHOL_API mpchol_status mpchol_pcg(mpchol_factor_t* f, const float* dA, int lda, const double* dB,
                          double* dX, int nrhs, const mpchol_pcg_opts* opts, mpchol_report* report,
                          mpchol_stream_t stream);
