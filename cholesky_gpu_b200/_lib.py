@@ -48,6 +48,8 @@ class Opts(ctypes.Structure):
         ("ladder_len", ctypes.c_int),
         ("ladder", ctypes.c_int * 4),
         ("left", ctypes.c_int),
+        ("coherence", ctypes.c_int),
+        ("equilibrate", ctypes.c_int),
     ]
 
 
@@ -120,6 +122,8 @@ SIGNATURES = {
     "mpchol_factor_prepare_solve": (_i, [_vp, _vp]),
     "mpchol_pcg": (_i, [_vp, _vp, _i, _vp, _vp, _i, ctypes.POINTER(PcgOpts), ctypes.POINTER(Report), _vp]),
     "mpchol_pcg_f64": (_i, [_vp, _vp, _i, _vp, _vp, _i, ctypes.POINTER(PcgOpts), ctypes.POINTER(Report), _vp]),
+    "mpchol_adjoint_solve": (_i, [_vp, _vp, _i, _vp, _vp, _vp, _i, _vp, _i, ctypes.POINTER(PcgOpts),
+                                  ctypes.POINTER(Report), _vp]),
     "mpchol_solve_host": (_i, [_vp, _vp, _i, _vp, _vp, _i, ctypes.POINTER(PcgOpts), ctypes.POINTER(Report), _vp]),
     "mpchol_factor_codes": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp]),
     "mpchol_set_copy_plan": (_i, [_vp, _i, _vp, _vp]),

@@ -253,6 +253,40 @@ class Factor:
         return Xo, Report(rep.iterations, bool(rep.converged), rep.rel_residual,
                           rep.backward_error, rep.precond_residual, st)
 
+    def adjoint_solve(self, A: torch.Tensor, X: torch.Tensor, G: torch.Tensor,
+                      rel_tol: float = 1e-10, max_it: int = 200, grad_a: bool = False):
+        """Backward of the solve X = A^-1 B: Lam = A^-1 G (G = dL/dX) by PCG
+        with this factor as preconditioner (mpchol_adjoint_solve; A the FP64
+        operator of the forward solve).  Returns (Lam, dL/dA or None, report);
+        dL/dA = -(Lam X^T + X Lam^T) / 2 (lower triangle filled) when grad_a."""
+        _require_cuda(A, torch.float64, "A")
+        _require_cuda(X, torch.float64, "X")
+        _require_cuda(G, torch.float64, "G")
+        Ac, lda = _col_major(A)
+        X2 = X.reshape(self.n, 1) if X.dim() == 1 else X
+        G2 = G.reshape(self.n, 1) if G.dim() == 1 else G
+        if X2.shape != G2.shape:
+            raise ValueError("X and G must have the same shape")
+        nrhs = G2.shape[1]
+        Xc = X2.t().contiguous()
+        Gc = G2.t().contiguous()
+        Lam = torch.empty_like(Gc)
+        GA = torch.zeros((self.n, self.n), dtype=torch.float64, device=A.device) if grad_a else None
+        po = _lib.default_pcg_opts(rel_tol=rel_tol, max_it=max_it)
+        rep = _lib.Report()
+        st = self.lib.mpchol_adjoint_solve(self.handle, Ac.data_ptr(), lda, Xc.data_ptr(),
+                                           Gc.data_ptr(), Lam.data_ptr(), nrhs,
+                                           None if GA is None else GA.data_ptr(), self.n,
+                                           ctypes.byref(po), ctypes.byref(rep), _stream_handle())
+        if st not in (_lib.OK, _lib.PCG_MAXIT):
+            check(st, "mpchol_adjoint_solve")
+        L = Lam.t()
+        L = L.reshape(G.shape) if G.dim() == 1 else L
+        # the cotangent was written column-major: its transpose view is the matrix
+        return L, (None if GA is None else GA.t()), Report(
+            rep.iterations, bool(rep.converged), rep.rel_residual, rep.backward_error,
+            rep.precond_residual, st)
+
 
 def _host_col_major(M: torch.Tensor, n: int) -> torch.Tensor:
     """n x nrhs (or n) CPU FP64 tensor as column-major storage (no copy for one

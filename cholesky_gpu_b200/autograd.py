@@ -8,7 +8,8 @@ reuses the forward's factor as its preconditioner, then
 ``mpchol_rbf_grad`` recomputes the K tiles from X to contract the cotangent
 G_K = -(a x^T + x a^T) / 2 into the gradients for X, the lengthscale, the
 nugget and y.  There is no counterpart in the reference (its RBF file is a
-stub, src/RBF.cu:1-45).
+stub, src/RBF.cu:1-45).  The adjoint solve is the C ABI's mpchol_adjoint_solve,
+so a caller outside Python can compose the same backward pass.
 """
 from __future__ import annotations
 
@@ -93,8 +94,9 @@ class RBFSolve(torch.autograd.Function):
         rel_tol, max_it = ctx.solve
         ell = ctx.ell
         g = gx.detach().double()
-        # adjoint solve, preconditioned by the forward's factor
-        a, rep = ctx.factor.pcg(ctx.K64, g, rel_tol=rel_tol, max_it=max_it)
+        # adjoint solve, preconditioned by the forward's factor (the C ABI's
+        # mpchol_adjoint_solve; the matrix cotangent stays implicit)
+        a, _, rep = ctx.factor.adjoint_solve(ctx.K64, x, g, rel_tol=rel_tol, max_it=max_it)
         if not rep.converged:
             raise RuntimeError(f"adjoint PCG did not converge: {rep}")
         ctx.adjoint_report = rep

@@ -166,7 +166,10 @@ struct mpchol_factor {
   int8_t* rexp = nullptr;
   uint8_t* mxexp = nullptr;
   StepState* steps = nullptr;
-  DevStatus* status = nullptr;
+  DevStatus* status = nullptr;    // the factorization's status word
+  DevStatus* pstatus = nullptr;   // the solves' status word (breakdown, timeouts)
+  double* colacc = nullptr;       // coherence rule: each step's panel column sums (b per step)
+  int8_t* eqexp = nullptr;        // equilibration exponents e_i (row i scaled by 2^-e_i)
   // solve side
   float* wsup = nullptr;      // inverses of the 1024-row diagonal super-blocks
   int* trsv_ctr = nullptr;    // dependency counters of the persistent triangular solve
@@ -221,6 +224,8 @@ mpchol_status validate_opts(const mpchol_opts* o, int n) {
   if (o->left != 0) return MPCHOL_ERR_NOT_SUPPORTED;
   if (o->diag_pert && !(o->pivot_floor > 0.0f)) return MPCHOL_ERR_BAD_ARG;
   if (o->switch_mode != 0 && o->switch_mode != 1) return MPCHOL_ERR_BAD_ARG;
+  if ((o->coherence != 0 && o->coherence != 1) || (o->equilibrate != 0 && o->equilibrate != 1))
+    return MPCHOL_ERR_BAD_ARG;
   if (o->ladder_len < 0 || o->ladder_len > 4) return MPCHOL_ERR_BAD_ARG;
   auto tc_ok = [&](int fmt) { return fmt == MPCHOL_PREC_FP32 || syrk_tc_supported(fmt, o->block_size); };
   if (o->precision != MPCHOL_PREC_SWITCHING && !tc_ok(o->precision)) return MPCHOL_ERR_NOT_SUPPORTED;
@@ -246,7 +251,8 @@ cudaError_t dmalloc(T** p, size_t count) {
 void free_factor(mpchol_factor_t* f) {
   if (f == nullptr) return;
   void* ptrs[] = {f->A, f->d, f->dtilde, f->rowsq, f->sh, f->winv, f->scratch64, f->q8,
-                  f->q16, f->rexp, f->mxexp, f->steps, f->status, f->wsup, f->trsv_ctr,
+                  f->q16, f->rexp, f->mxexp, f->steps, f->status, f->pstatus, f->colacc,
+                  f->eqexp, f->wsup, f->trsv_ctr,
                   f->vec, f->partials, f->scal, f->done, f->loop_ctl, f->op, f->hb, f->hx,
                   f->hq8, f->hq16, f->hrexp, f->hmx};
   for (void* p : ptrs)
@@ -276,6 +282,7 @@ DecisionParams make_dp(const mpchol_opts& o) {
   dp.floor_ratio = o.floor;
   dp.ladder_len = o.ladder_len;
   for (int i = 0; i < 4; ++i) dp.ladder[i] = o.ladder[i];
+  dp.coherence = (o.precision == MPCHOL_PREC_SWITCHING && o.switch_mode == 0 && o.coherence) ? 1 : 0;
   return dp;
 }
 
@@ -454,8 +461,19 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream, const CopyPlan
   MPCHOL_CUDA_TRY(cudaMemsetAsync(f->status, 0, sizeof(DevStatus), stream));
   MPCHOL_CUDA_TRY(cudaMemsetAsync(f->steps, 0, sizeof(StepState) * (f->nsteps + 1), stream));
   MPCHOL_CUDA_TRY(cudaMemsetAsync(f->sh, 0, sizeof(float) * n, stream));
-  if (streamed) MPCHOL_CUDA_TRY(cudaStreamWaitEvent(stream, f->ev_grp[0], 0));
-  else PHASE(MPCHOL_PH_SETUP, 1, stream, launch_extract_diag(f->A, ld, n, f->d, f->dtilde, stream));
+  if (dp.coherence)
+    MPCHOL_CUDA_TRY(cudaMemsetAsync(f->colacc, 0, sizeof(double) * (size_t)f->nsteps * b, stream));
+  if (streamed) {
+    MPCHOL_CUDA_TRY(cudaStreamWaitEvent(stream, f->ev_grp[0], 0));
+  } else {
+    if (o.equilibrate) {
+      // D A D with D = diag(2^-e_i): exponents from A's diagonal, then the
+      // lower triangle scaled in place (exact powers of two)
+      PHASE(MPCHOL_PH_SETUP, 2, stream, launch_equil_exps(f->A, ld, n, f->eqexp, stream));
+      MPCHOL_CUDA_TRY(launch_equil_scale(f->A, ld, n, f->eqexp, 0, n, false, stream));
+    }
+    PHASE(MPCHOL_PH_SETUP, 1, stream, launch_extract_diag(f->A, ld, n, f->d, f->dtilde, stream));
+  }
   const bool fixed = o.precision != MPCHOL_PREC_SWITCHING;
   unsigned tc_mask = 0;   // tensor-core formats a switching step may pick
   bool f32_possible = fixed || o.switch_mode == 1 || o.ladder_len == 0;
@@ -549,7 +567,8 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream, const CopyPlan
     PHASE(MPCHOL_PH_TRSM, 1, stream,
           launch_trsm_panel(f->tmapX, f->tmap32, f->A, ld, n, s, bs, f->winv, f->d, f->dtilde,
                             f->rowsq, &f->steps[k], &f->steps[k + 1], next_bs, dp, qa, f->status,
-                            stream, k > 0 ? &f->steps[k - 1] : nullptr));
+                            stream, k > 0 ? &f->steps[k - 1] : nullptr,
+                            dp.coherence ? f->colacc + (size_t)k * b : nullptr));
     // groups joining at this step catch up with panels 0 .. k-1 (aux is
     // already ordered after those panels and after the previous rest)
     bool caught = false, head_waits = false;
@@ -588,6 +607,9 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream, const CopyPlan
   }
   if (rest_pending) MPCHOL_CUDA_TRY(cudaStreamWaitEvent(stream, f->ev_rest, 0));
   if (streamed) MPCHOL_CUDA_TRY(cudaStreamWaitEvent(stream, f->ev_grp[plan->ng - 1], 0));
+  // equilibrated: L of A is D^-1 times the factor of D A D (rows times 2^e_i)
+  if (o.equilibrate && !streamed)
+    PHASE(MPCHOL_PH_SETUP, 1, stream, launch_equil_scale(f->A, ld, n, f->eqexp, 0, n, true, stream));
   f->solve_ready = false;
   return MPCHOL_OK;
 }
@@ -708,15 +730,15 @@ mpchol_status apply_precond(mpchol_factor_t* f, const double* r, double* tmp, do
   const int nk = trsv_launch_count(f->n);
   PHASE(MPCHOL_PH_TRSV, nk, stream,
         launch_trsv_persistent(false, f->A, f->ld, f->n, f->wsup, r, tmp, work, nr, f->trsv_ctr,
-                               skip, f->status, stream));
+                               skip, f->pstatus, stream));
   PHASE(MPCHOL_PH_TRSV, nk, stream,
         launch_trsv_persistent(true, f->A, f->ld, f->n, f->wsup, tmp, z, work, nr, f->trsv_ctr,
-                               skip, f->status, stream));
+                               skip, f->pstatus, stream));
   return MPCHOL_OK;
 }
 
-int read_status(mpchol_factor_t* f, cudaStream_t stream, DevStatus* out) {
-  if (cudaMemcpyAsync(out, f->status, sizeof(DevStatus), cudaMemcpyDeviceToHost, stream) != cudaSuccess)
+int read_status(const DevStatus* src, cudaStream_t stream, DevStatus* out) {
+  if (cudaMemcpyAsync(out, src, sizeof(DevStatus), cudaMemcpyDeviceToHost, stream) != cudaSuccess)
     return -1;
   if (cudaStreamSynchronize(stream) != cudaSuccess) return -1;
   return 0;
@@ -758,7 +780,7 @@ mpchol_status run_pcg(mpchol_factor_t* f, const TA* dA, int lda, const double* d
   double* misc = f->scal + 32;   // [0..7] rr true, [8..15] xnorm2, [16] frob2
   mpchol_status ss = ensure_solve(f, stream);
   if (ss != MPCHOL_OK) return ss;
-  MPCHOL_CUDA_TRY(cudaMemsetAsync(f->status, 0, sizeof(DevStatus), stream));
+  MPCHOL_CUDA_TRY(cudaMemsetAsync(f->pstatus, 0, sizeof(DevStatus), stream));
   MPCHOL_CUDA_TRY(cudaMemsetAsync(f->done, 0, 2 * sizeof(int), stream));
   PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_pad_columns(dB, n, nrhs, bb, nr, stream));
   PHASE(MPCHOL_PH_PCG_VEC, 1, stream, launch_dot(bb, bb, n, nr, part_misc, nullptr, stream));
@@ -785,7 +807,20 @@ mpchol_status run_pcg(mpchol_factor_t* f, const TA* dA, int lda, const double* d
     // convergence of the true residual
     MPCHOL_CUDA_TRY(cudaMemcpyAsync(f->h_scal, misc, sizeof(double) * 8, cudaMemcpyDeviceToHost, stream));
     MPCHOL_CUDA_TRY(cudaMemcpyAsync(f->h_scal + 8, bnorm2, sizeof(double) * 8, cudaMemcpyDeviceToHost, stream));
+    // the factorization's status rides along with the first check: a failed
+    // factor (NOT_SPD, TIMEOUT) is not iterated with
+    if (restart == 0)
+      MPCHOL_CUDA_TRY(cudaMemcpyAsync(f->h_scal + 48, f->status, sizeof(DevStatus),
+                                      cudaMemcpyDeviceToHost, stream));
     MPCHOL_CUDA_TRY(cudaStreamSynchronize(stream));
+    if (restart == 0) {
+      DevStatus fst;
+      memcpy(&fst, f->h_scal + 48, sizeof(DevStatus));
+      if (fst.code != 0) {
+        if (rep != nullptr) memset(rep, 0, sizeof(*rep));
+        return (mpchol_status)fst.code;
+      }
+    }
     converged = true;
     for (int k = 0; k < nrhs; ++k)
       if (!(f->h_scal[k] <= tol2 * f->h_scal[8 + k])) converged = false;
@@ -802,7 +837,7 @@ mpchol_status run_pcg(mpchol_factor_t* f, const TA* dA, int lda, const double* d
       PHASE(MPCHOL_PH_SYMV, 2, s, launch_symv_skip<TA>(dA, lda, n, p, Ap, nr, f->done, s));
       PHASE(MPCHOL_PH_PCG_VEC, 1, s, launch_dot(p, Ap, n, nr, part_pAp, f->done, s));
       PHASE(MPCHOL_PH_PCG_VEC, 1, s, launch_update_xr(x, r, p, Ap, n, nr, part_pAp, rho[cur], alpha, part_rr,
-                                  f->done, f->status, s));
+                                  f->done, f->pstatus, s));
       mpchol_status s2 = apply_precond(f, r, tmp, z, nr, f->done, s);
       if (s2 != MPCHOL_OK) return s2;
       PHASE(MPCHOL_PH_PCG_VEC, 1, s, launch_dot(r, z, n, nr, part_rz, f->done, s));
@@ -849,7 +884,7 @@ mpchol_status run_pcg(mpchol_factor_t* f, const TA* dA, int lda, const double* d
         if (ok) {
           const mpchol_status s0 = iteration(0, f->capture_stream);
           const bool cond_ok =
-              s0 == MPCHOL_OK && launch_pcg_loop_cond(handle, f->loop_ctl, f->done, f->status,
+              s0 == MPCHOL_OK && launch_pcg_loop_cond(handle, f->loop_ctl, f->done, f->pstatus,
                                                       f->scal, nr, f->capture_stream) == cudaSuccess;
           cudaGraph_t captured = nullptr;
           const cudaError_t ce = cudaStreamEndCapture(f->capture_stream, &captured);
@@ -877,7 +912,7 @@ mpchol_status run_pcg(mpchol_factor_t* f, const TA* dA, int lda, const double* d
       MPCHOL_CUDA_TRY(cudaGraphLaunch(g.exec, stream));
       MPCHOL_CUDA_TRY(cudaMemcpyAsync(f->h_done, f->done, 2 * sizeof(int), cudaMemcpyDeviceToHost, stream));
       DevStatus st;
-      MPCHOL_CUDA_TRY(cudaMemcpyAsync(&st, f->status, sizeof(DevStatus), cudaMemcpyDeviceToHost, stream));
+      MPCHOL_CUDA_TRY(cudaMemcpyAsync(&st, f->pstatus, sizeof(DevStatus), cudaMemcpyDeviceToHost, stream));
       MPCHOL_CUDA_TRY(cudaStreamSynchronize(stream));
       if (st.code == MPCHOL_ERR_TIMEOUT) return MPCHOL_ERR_TIMEOUT;
       add_launch_counts(g.nk, f->h_done[1] - it);
@@ -897,7 +932,7 @@ mpchol_status run_pcg(mpchol_factor_t* f, const TA* dA, int lda, const double* d
       launched += chunk;
       MPCHOL_CUDA_TRY(cudaMemcpyAsync(f->h_done, f->done, 2 * sizeof(int), cudaMemcpyDeviceToHost, stream));
       DevStatus st;
-      MPCHOL_CUDA_TRY(cudaMemcpyAsync(&st, f->status, sizeof(DevStatus), cudaMemcpyDeviceToHost, stream));
+      MPCHOL_CUDA_TRY(cudaMemcpyAsync(&st, f->pstatus, sizeof(DevStatus), cudaMemcpyDeviceToHost, stream));
       MPCHOL_CUDA_TRY(cudaStreamSynchronize(stream));
       if (st.code == MPCHOL_ERR_TIMEOUT) return MPCHOL_ERR_TIMEOUT;
       it = f->h_done[1];                // iterations actually executed on the device
@@ -909,7 +944,7 @@ mpchol_status run_pcg(mpchol_factor_t* f, const TA* dA, int lda, const double* d
   }
   // report
   DevStatus st;
-  if (read_status(f, stream, &st) != 0) return MPCHOL_ERR_CUDA;
+  if (read_status(f->pstatus, stream, &st) != 0) return MPCHOL_ERR_CUDA;
   MPCHOL_CUDA_TRY(cudaMemcpy2DAsync(dX, sizeof(double) * n, x, sizeof(double) * n,
                                     sizeof(double) * n, nrhs, cudaMemcpyDeviceToDevice, stream));
   if (rep != nullptr) {
@@ -967,7 +1002,7 @@ constexpr char kBlobMagic[8] = {'M', 'P', 'C', 'H', 'O', 'L', 'F', '1'};
 // block column from its diagonal down.
 uint64_t blob_l_bytes(int n, int b) {
   uint64_t t = 0;
-  for (int c = 0; c < n; c += b) t += (uint64_t)(n - c) * std::min(b, n - c) * sizeof(float);
+  for (int64_t c = 0; c < n; c += b) t += (uint64_t)(n - c) * std::min<int64_t>(b, n - c) * sizeof(float);
   return t;
 }
 uint64_t blob_total_bytes(int n, int b, int nsteps) {
@@ -1097,6 +1132,8 @@ void mpchol_opts_default(mpchol_opts* o) {
   o->ladder[2] = MPCHOL_PREC_FP32;
   o->ladder[3] = MPCHOL_PREC_FP32;
   o->left = 0;
+  o->coherence = 1;
+  o->equilibrate = 0;
 }
 
 void mpchol_pcg_opts_default(mpchol_pcg_opts* o) {
@@ -1130,7 +1167,9 @@ mpchol_status mpchol_factor_create(const mpchol_opts* opts, int n, mpchol_factor
             dmalloc(&f->rexp, (size_t)3 * n) == cudaSuccess &&
             dmalloc(&f->mxexp, (size_t)n * (f->b / 32)) == cudaSuccess &&
             dmalloc(&f->steps, f->nsteps + 1) == cudaSuccess &&
-            dmalloc(&f->status, 1) == cudaSuccess &&
+            dmalloc(&f->status, 1) == cudaSuccess && dmalloc(&f->pstatus, 1) == cudaSuccess &&
+            dmalloc(&f->colacc, (size_t)f->nsteps * f->b) == cudaSuccess &&
+            dmalloc(&f->eqexp, n) == cudaSuccess &&
             dmalloc(&f->wsup, solve_wsup_elems(n)) == cudaSuccess &&
             dmalloc(&f->trsv_ctr, trsv_counter_ints(n)) == cudaSuccess &&
             dmalloc(&f->vec, 8 * nv) == cudaSuccess &&
@@ -1206,7 +1245,16 @@ mpchol_status mpchol_solve_host(mpchol_factor_t* f, const float* hA, int lda, co
     MPCHOL_CUDA_TRY(dmalloc(&f->hb, (size_t)n * 8));
     MPCHOL_CUDA_TRY(dmalloc(&f->hx, (size_t)n * 8));
   }
-  if (f->plan_mode < 0 && f->plan.c1[0] == 0) f->plan = choose_copy_plan(n, b);
+  if (f->plan_mode < 0 && f->plan.c1[0] == 0) {
+    // equilibration scales A's lower triangle in one pass before step 0, so
+    // the copy does not overlap the factorization then
+    if (f->opts.equilibrate) {
+      f->plan = CopyPlan{};
+      f->plan.c1[0] = f->nsteps;
+    } else {
+      f->plan = choose_copy_plan(n, b);
+    }
+  }
   const CopyPlan& plan = f->plan;
   if (plan.ng <= 1) {
     MPCHOL_CUDA_TRY(copy_lower_blocks(f->op, f->ld, hA, lda, n, b, cudaMemcpyHostToDevice, s));
@@ -1275,7 +1323,7 @@ mpchol_status mpchol_set_copy_plan(mpchol_factor_t* f, int ngroups, const int* c
   p.ng = ngroups;
   if (ngroups > kMaxGroups || (ngroups > 1 && (cuts == nullptr || join == nullptr)))
     return MPCHOL_ERR_BAD_ARG;
-  if (ngroups > 1 && f->b % 128 != 0) return MPCHOL_ERR_NOT_SUPPORTED;
+  if (ngroups > 1 && (f->b % 128 != 0 || f->opts.equilibrate)) return MPCHOL_ERR_NOT_SUPPORTED;
   p.c0[0] = 0;
   for (int g = 1; g < ngroups; ++g) {
     p.c1[g - 1] = cuts[g - 1];
@@ -1359,7 +1407,10 @@ mpchol_status mpchol_factor_blob_check(const void* blob, size_t size, int* n, in
   if (memcmp(h.magic, kBlobMagic, 8) != 0 || h.version != 1 ||
       h.header_bytes != sizeof(FactorBlobHeader) || h.step_bytes != sizeof(StepState))
     return MPCHOL_ERR_BAD_ARG;
-  if (h.n < 1 || h.b < 32 || h.b > 256 || h.b % 32 != 0 || h.nsteps != (h.n + h.b - 1) / h.b)
+  // bound n before any arithmetic on it (a hostile header must not overflow
+  // the step count or make the size loop run away)
+  if (h.n < 1 || h.n > MPCHOL_BLOB_MAX_N || h.b < 32 || h.b > 256 || h.b % 32 != 0 ||
+      (int64_t)h.nsteps != ((int64_t)h.n + h.b - 1) / h.b)
     return MPCHOL_ERR_BAD_ARG;
   if (h.l_bytes != blob_l_bytes(h.n, h.b) || h.total_bytes != blob_total_bytes(h.n, h.b, h.nsteps) ||
       size < h.total_bytes)
@@ -1380,6 +1431,10 @@ mpchol_status mpchol_factor_save(const mpchol_factor_t* fc, void* blob, size_t c
   if (blob == nullptr) return MPCHOL_OK;
   if (cap < total) return MPCHOL_ERR_BAD_ARG;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  // a failed factorization is not saved
+  DevStatus fst;
+  if (read_status(f->status, s, &fst) != 0) return MPCHOL_ERR_CUDA;
+  if (fst.code != 0) return (mpchol_status)fst.code;
   unsigned char* out = static_cast<unsigned char*>(blob);
   MPCHOL_CUDA_TRY(blob_copy(f, out + sizeof(FactorBlobHeader), true, s));
   MPCHOL_CUDA_TRY(cudaStreamSynchronize(s));
@@ -1410,7 +1465,12 @@ mpchol_status mpchol_factor_load(mpchol_factor_t* f, const void* blob, size_t si
   MPCHOL_CUDA_TRY(blob_copy(f, in + sizeof(FactorBlobHeader), false, s));
   MPCHOL_CUDA_TRY(cudaStreamSynchronize(s));
   f->solve_ready = false;
-  return MPCHOL_OK;
+  // the saved status word is the blob's last field
+  DevStatus fst;
+  memcpy(&fst, in + sizeof(FactorBlobHeader) + (blob_total_bytes(n, b, f->nsteps) -
+                                                sizeof(FactorBlobHeader) - sizeof(DevStatus)),
+         sizeof(DevStatus));
+  return (mpchol_status)fst.code;
 }
 
 mpchol_status mpchol_factor_diags(const mpchol_factor_t* f, const float** dD, const float** dDt) {
@@ -1437,6 +1497,24 @@ mpchol_status mpchol_pcg_f64(mpchol_factor_t* f, const double* dA, int lda, cons
   return run_pcg<double>(f, dA, lda, dB, dX, nrhs, opts, rep, reinterpret_cast<cudaStream_t>(stream));
 }
 
+mpchol_status mpchol_adjoint_solve(mpchol_factor_t* f, const double* dA, int lda,
+                                   const double* dX, const double* dG, double* dLam, int nrhs,
+                                   double* dGradA, int ldg, const mpchol_pcg_opts* opts,
+                                   mpchol_report* rep, mpchol_stream_t stream) {
+  if (f == nullptr || dA == nullptr || dX == nullptr || dG == nullptr || dLam == nullptr)
+    return MPCHOL_ERR_BAD_ARG;
+  if (nrhs < 1 || nrhs > 8 || lda < f->n || (dGradA != nullptr && ldg < f->n))
+    return MPCHOL_ERR_BAD_ARG;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  // A symmetric: the adjoint system A^T lambda = g is the forward operator
+  // with the cotangent as right-hand side, preconditioned by the same factor
+  const mpchol_status st = run_pcg<double>(f, dA, lda, dG, dLam, nrhs, opts, rep, s);
+  if (st != MPCHOL_OK && st != MPCHOL_PCG_MAXIT) return st;
+  if (dGradA != nullptr)
+    PHASE(MPCHOL_PH_PCG_VEC, 1, s, launch_sym_outer(dLam, dX, f->n, nrhs, dGradA, ldg, s));
+  return st;
+}
+
 mpchol_status mpchol_apply_precond(mpchol_factor_t* f, const double* dR, double* dZ, int nrhs,
                                    mpchol_stream_t stream) {
   if (f == nullptr || dR == nullptr || dZ == nullptr || nrhs < 1 || nrhs > 8) return MPCHOL_ERR_BAD_ARG;
@@ -1448,14 +1526,14 @@ mpchol_status mpchol_apply_precond(mpchol_factor_t* f, const double* dR, double*
   double* rp = f->vec + 5 * nv;     // bb slot
   double* tmp = f->vec + 6 * nv;
   double* zp = f->vec + 2 * nv;     // z slot
-  MPCHOL_CUDA_TRY(cudaMemsetAsync(f->status, 0, sizeof(DevStatus), s));
+  MPCHOL_CUDA_TRY(cudaMemsetAsync(f->pstatus, 0, sizeof(DevStatus), s));
   PHASE(MPCHOL_PH_PCG_VEC, 1, s, launch_pad_columns(dR, f->n, nrhs, rp, nr, s));
   ss = apply_precond(f, rp, tmp, zp, nr, nullptr, s);
   if (ss != MPCHOL_OK) return ss;
   MPCHOL_CUDA_TRY(cudaMemcpy2DAsync(dZ, sizeof(double) * f->n, zp, sizeof(double) * f->n,
                                     sizeof(double) * f->n, nrhs, cudaMemcpyDeviceToDevice, s));
   DevStatus st;
-  if (read_status(f, s, &st) != 0) return MPCHOL_ERR_CUDA;
+  if (read_status(f->pstatus, s, &st) != 0) return MPCHOL_ERR_CUDA;
   return (mpchol_status)st.code;
 }
 

@@ -180,7 +180,7 @@ mpchol_status mpchol_batch_create(const mpchol_opts* opts, int count, const int*
   if (fmt < 0 || fmt > MPCHOL_PREC_FP16X2) return MPCHOL_ERR_BAD_ARG;
   if (b < 32 || b > 256 || b % 32 != 0) return MPCHOL_ERR_BAD_ARG;
   if (!syrk_tc_supported(fmt, b)) return MPCHOL_ERR_NOT_SUPPORTED;
-  if (opts->left != 0) return MPCHOL_ERR_NOT_SUPPORTED;
+  if (opts->left != 0 || opts->equilibrate != 0) return MPCHOL_ERR_NOT_SUPPORTED;
   if (opts->diag_pert && !(opts->pivot_floor > 0.0f)) return MPCHOL_ERR_BAD_ARG;
   for (int i = 0; i < count; ++i)
     if (ns[i] < 1) return MPCHOL_ERR_BAD_ARG;

@@ -19,6 +19,12 @@ struct StepState {
   int prec;                     // chosen trailing-update precision (Fmt)
   int fp64_diag;                // 1: factor this step's diagonal block in FP64
   int grid_bar;                 // arrivals at the panel solve's grid barrier
+  unsigned int not_min_dt_bits; // ~(float bits of min_i dtilde_i) over trailing rows (atomicMax of
+                                // the complement gives the minimum; a non-positive or NaN dtilde
+                                // counts as 0)
+  unsigned int coh_bits;        // coherence ratio (||P^T 1||^2 / m) / min_i dtilde_i (float bits;
+                                // +inf when min dtilde <= 0), set by the resolving CTA
+  int pad;
 };
 
 struct DecisionParams {
@@ -28,6 +34,7 @@ struct DecisionParams {
   float floor_ratio;   // near-indefinite flag threshold
   int ladder_len;
   int ladder[4];
+  int coherence;       // switch_mode 0: also bound u_p * coherence ratio by eps'
 };
 
 // ---- POTRF of the diagonal block (one CTA) ------------------------------
@@ -72,11 +79,14 @@ __host__ __device__ inline int rexp_slot(int fmt) { return fmt == E4M3 ? 0 : (fm
 // its rows (prev null: first step); the rows of the next diagonal block get
 // theirs in its POTRF.  tmapX: TMA map over A with 32 x bs boxes; tmap32 as
 // for launch_potrf.
+// colacc (coherence rule, nullable otherwise): bs FP64 accumulators, zeroed
+// before the launch, that receive the panel's column sums.
 cudaError_t launch_trsm_panel(const CUtensorMap& tmapX, const CUtensorMap& tmap32, float* A,
                               int lda, int n, int s, int bs, const float* winv, const float* d,
                               float* dtilde, float* rowsq, StepState* step, StepState* next,
                               int next_bs, const DecisionParams& dp, const QuantAll& qa,
-                              DevStatus* st, cudaStream_t stream, const StepState* prev = nullptr);
+                              DevStatus* st, cudaStream_t stream, const StepState* prev = nullptr,
+                              double* colacc = nullptr);
 
 // ---- panel quantization ---------------------------------------------------
 // Fixed-format variant (test entry point): no decision, no shift.

@@ -59,6 +59,15 @@ cudaError_t launch_extract_diag(const float* A, int lda, int n, float* d, float*
                                 cudaStream_t stream);
 cudaError_t launch_f64_to_f32(const double* src, int lds, float* dst, int ldd, int n,
                               cudaStream_t stream);
+// Equilibration: ex[i] = exponent of row i from A's diagonal; then the lower
+// triangle of columns [c0, c1) is scaled to D A D
+// (unscale_rows = false) or the factor's rows scaled back by 2^ex[i] (true).
+cudaError_t launch_equil_exps(const float* A, int lda, int n, int8_t* ex, cudaStream_t stream);
+cudaError_t launch_equil_scale(float* A, int lda, int n, const int8_t* ex, int c0, int c1,
+                               bool unscale_rows, cudaStream_t stream);
+// G = -(Lam X^T + X Lam^T) / 2, lower triangle (n x nrhs column-major inputs).
+cudaError_t launch_sym_outer(const double* lam, const double* x, int n, int nrhs, double* G,
+                             int ldg, cudaStream_t stream);
 template <typename TA>
 cudaError_t launch_frob_lower(const TA* A, int lda, int n, double* partials, cudaStream_t stream);
 cudaError_t launch_pad_columns(const double* src, int n, int ncols, double* dst, int ncols_pad,

@@ -74,17 +74,21 @@ __device__ bool factor_diag_tile(T* t, T* inv, int lane, int nreal, const T* shi
     // branch on the chain); lane k's value is the pivot, broadcast as 1/sqrt
     const bool real = k < nreal;   // identity padding beyond the real block
     T piv = real ? dnext + my_shift : T(1);
-    bool pert = false, bad = false;
+    // a NaN or infinite pivot means the Schur complement has overflowed
+    // (earlier pivots floored far below the rounding error of a low-precision
+    // update): no repair makes that factor usable, so it fails as NOT_SPD
+    const bool nonfin = real && !(piv - piv == T(0));
+    bool pert = false, bad = nonfin;
     if (diag_pert) {
       // repair: max(|pivot|, floor), the reference's fixDiag rule
-      // (src/kernels_macros.cuh:90-99); a NaN pivot takes the floor
-      pert = real && !(piv > my_pmin);
+      // (src/kernels_macros.cuh:90-99)
+      pert = real && !nonfin && !(piv > my_pmin);
       const T ap = piv < T(0) ? -piv : piv;
       piv = pert ? (ap > my_pmin ? ap : my_pmin) : piv;
     } else {
-      bad = real && !(piv > T(0));
-      piv = bad ? T(1) : piv;   // keep the arithmetic finite; the caller discards the result
+      bad = bad || (real && !(piv > T(0)));
     }
+    piv = bad ? T(1) : piv;   // keep the arithmetic finite; the caller discards the result
     // one SFU reciprocal square root on the dependency chain:
     // r = 1/sqrt(piv), L(k,k) = piv * r
     const T r = drsqrt<T>(piv);

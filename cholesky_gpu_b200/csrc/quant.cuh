@@ -17,9 +17,11 @@ __device__ __forceinline__ int resolve_precision(const StepState* step, const De
     return choice == 0 ? FP32 : (choice == 1 ? FP16 : E4M3);
   }
   const float ratio = __uint_as_float(step->max_ratio_bits);
+  const float coh = dp.coherence ? __uint_as_float(step->coh_bits) : 0.0f;
   for (int k = 0; k < dp.ladder_len; ++k) {
     const int p = dp.ladder[k];
-    if (unit_roundoff(p) * ratio <= dp.eps_prime) return p;
+    const float u = unit_roundoff(p);
+    if (u * ratio <= dp.eps_prime && u * coh <= dp.eps_prime) return p;
   }
   // no entry meets the bound: the ladder's most precise (last) entry
   return dp.ladder_len > 0 ? dp.ladder[dp.ladder_len - 1] : FP32;

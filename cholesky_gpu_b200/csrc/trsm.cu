@@ -249,7 +249,7 @@ trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_consta
                   float* __restrict__ A, int lda, int n, int s, int bs, const float* __restrict__ winv,
                   const float* __restrict__ d, float* __restrict__ dtilde, float* __restrict__ rowsq,
                   StepState* step, StepState* next, int next_bs, DecisionParams dp, DevStatus* st,
-                  QuantAll qa, const StepState* prev) {
+                  QuantAll qa, const StepState* prev, double* __restrict__ colacc) {
   extern __shared__ __align__(128) float sm[];
   const int NT = bs / 32;
   float* Xs = sm;                                        // [bs][XLD]
@@ -259,6 +259,8 @@ trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_consta
   uint32_t* stage = reinterpret_cast<uint32_t*>(Lb);     // code staging, once L11 is used
   __shared__ float red_max[NTHR / 32];
   __shared__ int red_lit[NTHR / 32];
+  __shared__ float red_min[NTHR / 32];
+  __shared__ double red_coh[NTHR / 32];
   __shared__ float s_rmax[NTHR / TR][TR];
   __shared__ float s_sq[NTHR / TR][TR];
   __shared__ __align__(8) uint64_t barx, barl[2];
@@ -306,7 +308,8 @@ trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_consta
     }
   }
   __syncthreads();
-  float bm = 0.0f;   // this CTA's max d/dtilde and literal code
+  float bm = 0.0f;   // this CTA's max d/dtilde, min dtilde and literal code
+  float bmin = INFINITY;
   int bl = 0;
   if (s_ok) {
     for (int J = 0; J < NT; ++J) {
@@ -351,6 +354,7 @@ trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_consta
       float ratio = dt > 0.0f ? di / dt : INFINITY;
       if (isnan(ratio)) ratio = INFINITY;
       bm = fmaxf(bm, ratio);
+      bmin = dt > 0.0f ? fminf(bmin, dt) : 0.0f;
       // reference list {FP32, FP16, E4M3} with the reference's machine epsilons
       const float ref_eps[3] = {1.1920929e-7f, 0.0009765625f, 0.125f};
       int pick = 0;
@@ -360,6 +364,24 @@ trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_consta
       if (next != nullptr && dp.floor_ratio > 0.0f && gi - (s + bs) < next_bs &&
           dt <= dp.floor_ratio * di)
         next->fp64_diag = 1;
+    }
+    // ---- column sums of the slab (coherence rule): thread c sums column c
+    // over the slab's rows, starting at row c % 32 so that the 32 threads of
+    // a warp read 32 different banks (a fixed order per column), and adds it
+    // into colacc.  The sums reach colacc as FP64 atomics of FP32 partials,
+    // which are exact while a column's partials span less than 2^20 in
+    // magnitude; the order of the atomics then does not change the result
+    if (colacc != nullptr) {
+      if (tid < bs) {
+        float cs = 0.0f;
+#pragma unroll 8
+        for (int q = 0; q < TR; ++q) {
+          const int r = (q + tid) & (TR - 1);
+          cs += (r < nrows) ? Xs[tid * XLD + r] : 0.0f;
+        }
+        atomicAdd(colacc + tid, (double)cs);
+      }
+      __threadfence();
     }
     // ---- the slab's codes in every candidate format -------------------------
     if (qa.cand != 0) {
@@ -378,25 +400,56 @@ trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_consta
   // ---- statistics of the CTA; the last CTA resolves the step --------------
   bm = warp_max(bm);
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) bl = max(bl, __shfl_xor_sync(0xffffffffu, bl, o));
-  if ((tid & 31) == 0) { red_max[tid >> 5] = bm; red_lit[tid >> 5] = bl; }
+  for (int o = 16; o > 0; o >>= 1) {
+    bl = max(bl, __shfl_xor_sync(0xffffffffu, bl, o));
+    bmin = fminf(bmin, __shfl_xor_sync(0xffffffffu, bmin, o));
+  }
+  if ((tid & 31) == 0) { red_max[tid >> 5] = bm; red_lit[tid >> 5] = bl; red_min[tid >> 5] = bmin; }
   __syncthreads();
   if (tid == 0) {
-    float cm = 0.0f; int cl = 0;
-    for (int w = 0; w < NTHR / 32; ++w) { cm = fmaxf(cm, red_max[w]); cl = max(cl, red_lit[w]); }
+    float cm = 0.0f, cmin = INFINITY; int cl = 0;
+    for (int w = 0; w < NTHR / 32; ++w) {
+      cm = fmaxf(cm, red_max[w]);
+      cl = max(cl, red_lit[w]);
+      cmin = fminf(cmin, red_min[w]);
+    }
     atomicMax(&step->max_ratio_bits, __float_as_uint(cm));
     atomicMax(&step->literal_code, cl);
+    if (cmin < INFINITY) atomicMax(&step->not_min_dt_bits, ~__float_as_uint(fmaxf(cmin, 0.0f)));
     __threadfence();
     s_last = atomicAdd(&step->grid_bar, 1) == (int)gridDim.x - 1;
   }
   __syncthreads();
   if (!s_last) return;
-  if (tid != 0) return;
   __threadfence();                                       // every CTA's statistics
+  // coherence ratio (||P^T 1||^2 / m) / min dtilde: the column sums' squares
+  // summed in a fixed order (warp butterflies, then warps in order)
+  if (colacc != nullptr) {
+    double c2 = 0.0;
+    if (tid < bs) {
+      const double cs = *reinterpret_cast<volatile double*>(colacc + tid);
+      c2 = cs * cs;
+    }
+    c2 = warp_sum(c2);
+    if ((tid & 31) == 0) red_coh[tid >> 5] = c2;
+    __syncthreads();
+  }
+  if (tid != 0) return;
   if (*reinterpret_cast<volatile int*>(&st->code) != 0) return;
   StepState ss;
   ss.max_ratio_bits = *reinterpret_cast<volatile unsigned int*>(&step->max_ratio_bits);
   ss.literal_code = *reinterpret_cast<volatile int*>(&step->literal_code);
+  float coh = 0.0f;
+  if (colacc != nullptr) {
+    double c2 = 0.0;
+    for (int w = 0; w < NTHR / 32; ++w) c2 += red_coh[w];
+    const float mind = __uint_as_float(~*reinterpret_cast<volatile unsigned int*>(&step->not_min_dt_bits));
+    const double g = c2 / (double)m;
+    coh = (mind > 0.0f) ? (float)(g / (double)mind) : INFINITY;
+    if (isnan(coh)) coh = INFINITY;
+    step->coh_bits = __float_as_uint(coh);
+  }
+  ss.coh_bits = __float_as_uint(coh);
   step->prec = resolve_precision(&ss, dp);
 }
 
@@ -454,7 +507,8 @@ cudaError_t launch_trsm_panel(const CUtensorMap& tmapX, const CUtensorMap& tmap3
                               int lda, int n, int s, int bs, const float* winv, const float* d,
                               float* dtilde, float* rowsq, StepState* step, StepState* next,
                               int next_bs, const DecisionParams& dp, const QuantAll& qa,
-                              DevStatus* st, cudaStream_t stream, const StepState* prev) {
+                              DevStatus* st, cudaStream_t stream, const StepState* prev,
+                              double* colacc) {
   const int m = n - s - bs;
   if (m <= 0) return cudaSuccess;
   const size_t smem = trsm_smem_floats(bs) * sizeof(float);
@@ -464,7 +518,7 @@ cudaError_t launch_trsm_panel(const CUtensorMap& tmapX, const CUtensorMap& tmap3
   if (e != cudaSuccess) return e;
   trsm_panel_kernel<<<ceil_div(m, TR), NTHR, smem, stream>>>(tmapX, tmap32, A, lda, n, s, bs, winv, d,
                                                              dtilde, rowsq, step, next, next_bs, dp, st,
-                                                             qa, prev);
+                                                             qa, prev, colacc);
   return cudaGetLastError();
 }
 

@@ -79,6 +79,19 @@ typedef struct {
                           a step no entry qualifies for takes the last (most precise) entry */
   int ladder[4];
   int left;            /* 0: right-looking (only value built); settings.json "left" */
+  int coherence;       /* switch_mode 0 only.  1 (default): a ladder entry p must also satisfy
+                          u_p * ||P^T 1||^2 / m <= eps' * min_i dtilde_i, where P is the step's
+                          m x b panel: a panel whose columns share one sign pattern across the
+                          trailing rows (the constant mode of a kernel matrix) turns rounding
+                          errors into a coherent rank-2 perturbation of norm ~u_p ||P^T 1||^2/m,
+                          which the per-row ratio test cannot see.  0: ratio test only. */
+  int equilibrate;     /* 1: factor D A D with D = diag(2^-e_i), e_i = floor((floor(log2 a_ii)
+                          + 1) / 2) clamped to [-63, 63] (0 for a non-positive a_ii), so the
+                          scaled diagonal lies in [0.5, 2); when the factorization ends L's rows
+                          are scaled back by 2^e_i (exact), so L L^T still approximates A and
+                          the solves are unchanged.  mpchol_factor_diags then returns the scaled
+                          diagonals.  The diagonal equilibration intent of
+                          src/kernels_macros.cuh:137-158.  0 (default): off. */
 } mpchol_opts;
 
 /* Per-factor results, filled by mpchol_factor_info (synchronizes the stream). */
@@ -177,13 +190,18 @@ MPCHOL_API mpchol_status mpchol_factor_lower(const mpchol_factor_t* f, const flo
  * and byte order.
  * mpchol_factor_save: *size receives the blob size; blob == NULL only
  * queries it; cap < size is MPCHOL_ERR_BAD_ARG.  Synchronizes `stream`
- * (the factor must have been computed on it or before it).
+ * (the factor must have been computed on it or before it).  A factor whose
+ * factorization failed is not saved: save returns its status (NOT_SPD,
+ * TIMEOUT) and writes nothing.
  * mpchol_factor_load: replaces the factor of f (same n and block size as the
  * blob, else MPCHOL_ERR_BAD_ARG) and its solve-side data is rebuilt on the
- * next solve; synchronizes `stream`.
+ * next solve; synchronizes `stream`.  A blob whose saved status is not OK
+ * is loaded and its status returned, so the caller learns the factor is
+ * unusable (the solves refuse it too).
  * mpchol_factor_blob_check: host-only validation of a blob (magic, version,
- * sizes, checksum); writes n and the block size.  No counterpart in the
- * reference, which refactors for every solve. */
+ * sizes, n <= MPCHOL_BLOB_MAX_N, checksum); writes n and the block size.
+ * No counterpart in the reference, which refactors for every solve. */
+#define MPCHOL_BLOB_MAX_N (1 << 24)
 MPCHOL_API mpchol_status mpchol_factor_save(const mpchol_factor_t* f, void* blob, size_t cap,
                                             size_t* size, mpchol_stream_t stream);
 MPCHOL_API mpchol_status mpchol_factor_load(mpchol_factor_t* f, const void* blob, size_t size,
@@ -214,9 +232,11 @@ MPCHOL_API mpchol_status mpchol_factor_prepare_solve(mpchol_factor_t* f, mpchol_
  * re-checked on the true residual (restarting from it if needed).  When the
  * runtime refuses the graph, or profiling is on, iterations are launched
  * directly and `stream` is synchronized every check_every iterations.
- * report may be NULL.  The solve reuses the factor object's device status
- * word (for breakdown and timeouts), so read mpchol_factor_info_get's
- * n_perturbed and fail_row before solving. */
+ * report may be NULL.  A factor whose factorization failed (NOT_SPD,
+ * TIMEOUT) is not used: the solve returns the factor's status without
+ * iterating.  The solve has a device status word of its own (breakdown,
+ * timeouts), so mpchol_factor_info_get reports the factorization's status,
+ * failing row and perturbed-pivot count before and after any solve. */
 MPCHOL_API mpchol_status mpchol_pcg(mpchol_factor_t* f, const float* dA, int lda, const double* dB,
                          double* dX, int nrhs, const mpchol_pcg_opts* opts, mpchol_report* report,
                          mpchol_stream_t stream);
@@ -224,6 +244,21 @@ MPCHOL_API mpchol_status mpchol_pcg(mpchol_factor_t* f, const float* dA, int lda
 MPCHOL_API mpchol_status mpchol_pcg_f64(mpchol_factor_t* f, const double* dA, int lda, const double* dB,
                              double* dX, int nrhs, const mpchol_pcg_opts* opts,
                              mpchol_report* report, mpchol_stream_t stream);
+/* Adjoint solve of a differentiable solve x = A^-1 b (A symmetric, the FP64
+ * operator dA of the forward solve).  Given the forward solution dX and the
+ * cotangent dG = dL/dx (both n x nrhs FP64, ld = n), solves A lambda = dG by
+ * PCG preconditioned by the forward's factor f -- no refactoring -- and
+ * writes dLam = lambda, which is dL/db.  The matrix cotangent is
+ * dL/dA = -(lambda x^T + x lambda^T) / 2 summed over the rhs: its factors are
+ * dLam and dX; dGradA (nullable; n x n FP64, ld = ldg >= n) receives it
+ * densely, lower triangle only.  Returns like mpchol_pcg.  The backward pass
+ * of a differentiable solve for callers outside Python (the torch wrapper
+ * composes the same steps); no counterpart in the reference. */
+MPCHOL_API mpchol_status mpchol_adjoint_solve(mpchol_factor_t* f, const double* dA, int lda,
+                                              const double* dX, const double* dG, double* dLam,
+                                              int nrhs, double* dGradA, int ldg,
+                                              const mpchol_pcg_opts* opts, mpchol_report* report,
+                                              mpchol_stream_t stream);
 /* Factor and solve from host memory: the step precond_CG
  * (src/mixed_cholesky.cu:76-229) performs on device buffers, for a caller
  * whose matrix and right-hand sides are in host memory.  hA: FP32 symmetric,
@@ -255,7 +290,8 @@ MPCHOL_API mpchol_status mpchol_solve_host(mpchol_factor_t* f, const float* hA, 
  * ngroups == 1: copy all of A, then factor; ngroups 2..8: block columns
  * [0, cuts[0]), [cuts[0], cuts[1]), ..., group g >= 1 joining at step
  * join[g-1] (0 <= join[g-1] <= cuts[g-1] - 1, non-decreasing).  Needs
- * block_size % 128 == 0 for ngroups > 1 (MPCHOL_ERR_NOT_SUPPORTED). */
+ * block_size % 128 == 0 and equilibrate == 0 for ngroups > 1
+ * (MPCHOL_ERR_NOT_SUPPORTED); an equilibrated factor copies all of A first. */
 MPCHOL_API mpchol_status mpchol_set_copy_plan(mpchol_factor_t* f, int ngroups, const int* cuts,
                                               const int* join);
 /* The automatic plan for order n and block_size: returns the number of
@@ -320,7 +356,8 @@ MPCHOL_API mpchol_status mpchol_syrk_update(float* dC, int ldc, int m, int k, in
 /* ---- batches of independent systems of uneven size --------------------- */
 /* No counterpart in the reference (one system per precond_CG call).  All
  * systems share the options (a fixed tensor-core precision: FP16, E4M3,
- * E5M2, MXFP8 or FP16X2; not FP32 or SWITCHING) and the rhs count; every
+ * E5M2, MXFP8 or FP16X2; not FP32 or SWITCHING; no equilibration) and the
+ * rhs count; every
  * kernel launch serves all of them.  ns[i] is the order of system i; arrays
  * passed to the calls below are indexed in that same (caller) order and hold
  * device pointers.  Matrices are FP32 column-major (ld lda[i]) with the lower

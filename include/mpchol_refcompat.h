@@ -53,6 +53,16 @@ inline int precond_CG(double* A, double* x, double* b, int n, int r, double norm
                            stream);
 }
 
+/* The reference's switching_chol returns nothing, so a failure (a
+ * non-positive pivot, a bad argument) cannot reach its caller through the
+ * signature.  The shim keeps the mpchol_status of the calling thread's last
+ * switching_chol here; a caller that wants it reads it after the call. */
+inline int& mpchol_refcompat_status_slot() {
+  static thread_local int status = 0;
+  return status;
+}
+inline int mpchol_refcompat_last_status() { return mpchol_refcompat_status_slot(); }
+
 inline void switching_chol(float* d_A, int n, int b, float* d_diagVals, float* updated_diag,
                            float eps_prime, bool perturb_diag, int microscal_size,
                            cusolverDnHandle_t cusolverH, cublasLtHandle_t cublasltH,
@@ -60,8 +70,9 @@ inline void switching_chol(float* d_A, int n, int b, float* d_diagVals, float* u
   (void)cusolverH;
   (void)cublasltH;
   (void)cublasH;
-  (void)mpchol_switching_chol(d_A, n, b, d_diagVals, updated_diag, eps_prime,
-                              perturb_diag ? 1 : 0, microscal_size, stream, scales);
+  mpchol_refcompat_status_slot() =
+      mpchol_switching_chol(d_A, n, b, d_diagVals, updated_diag, eps_prime,
+                            perturb_diag ? 1 : 0, microscal_size, stream, scales);
 }
 #endif /* __cplusplus */
 

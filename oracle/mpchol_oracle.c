@@ -237,6 +237,8 @@ typedef struct {
   int ladder[4];
   const int* force_prec;   /* nullable: per-step precision override */
   const int* force_fp64;   /* nullable: per-step FP64 diag override */
+  int coherence;        /* switch_mode 0: also require u_p * coh <= eps' */
+  int equilibrate;      /* 1: factor D A D, D = diag(2^-e_i), then unscale L's rows */
 } orc_chol_opts;
 
 typedef struct {
@@ -268,12 +270,42 @@ static float ref_mach_eps(int fmt) {
 /*
  * Step precision choice.  mode 0 (build criterion): the first ladder entry p
  * (lowest precision first) with u_p * max_i d_i / dtilde_i <= eps_prime over
- * the trailing rows; the last (most precise) entry if none.  mode 1 (reference-literal): per row, the
+ * the trailing rows -- and, with the coherence rule, u_p * coh <= eps_prime,
+ * coh = (||P^T 1||^2 / m) / min_i dtilde_i (orc_coherence_ratio) -- the last
+ * (most precise) entry if none.  mode 1 (reference-literal): per row, the
  * first entry of the reference list {FP32, FP16, E4M3} with
  * mach_eps_p * dtilde_i >= eps_prime * d_i (src/kernels_macros.cuh:191-211);
  * rows with no match choose FP32; the step takes the most precise row choice.
  */
-int orc_choose_precision(const float* d, const float* dt, int m, const orc_chol_opts* o) {
+/* Coherence ratio of a solved panel P (m x bs, column-major, ld lda) with
+ * the Schur diagonal dt after the step: (||P^T 1||^2 / m) / min_i dt_i, +inf
+ * when some dt_i <= 0.  The column sums are formed as the GPU forms them: a
+ * float sum per 32-row slab, column c's rows taken from row c % 32 on, and the
+ * slab sums added in double. */
+float orc_coherence_ratio(const float* P, int lda, int m, int bs, const float* dt) {
+  if (m <= 0) return 0.0f;
+  float mind = INFINITY;
+  for (int i = 0; i < m; ++i) mind = dt[i] > 0.0f ? (dt[i] < mind ? dt[i] : mind) : 0.0f;
+  double c2 = 0.0;
+  for (int c = 0; c < bs; ++c) {
+    double cs = 0.0;
+    for (int r0 = 0; r0 < m; r0 += 32) {
+      const int nr = m - r0 < 32 ? m - r0 : 32;
+      float part = 0.0f;
+      for (int q = 0; q < 32; ++q) {
+        const int r = (q + c) & 31;
+        part += r < nr ? P[(size_t)c * lda + r0 + r] : 0.0f;
+      }
+      cs += (double)part;
+    }
+    c2 += cs * cs;
+  }
+  if (!(mind > 0.0f)) return INFINITY;
+  const float coh = (float)((c2 / (double)m) / (double)mind);
+  return coh != coh ? INFINITY : coh;
+}
+
+int orc_choose_precision(const float* d, const float* dt, int m, float coh, const orc_chol_opts* o) {
   if (m <= 0) return ORC_FP32;
   if (o->switch_mode == 1) {
     const int list[3] = {ORC_FP32, ORC_FP16, ORC_E4M3};
@@ -294,7 +326,8 @@ int orc_choose_precision(const float* d, const float* dt, int m, const orc_chol_
   }
   for (int k = 0; k < o->ladder_len; ++k) {
     const int p = o->ladder[k];
-    if (orc_unit_roundoff(p) * ratio <= o->eps_prime) return p;
+    const float u = orc_unit_roundoff(p);
+    if (u * ratio <= o->eps_prime && (!o->coherence || u * coh <= o->eps_prime)) return p;
   }
   return o->ladder_len > 0 ? o->ladder[o->ladder_len - 1] : ORC_FP32;
 }
@@ -308,6 +341,7 @@ int orc_choose_precision(const float* d, const float* dt, int m, const orc_chol_
     for (int k = 0; k < nb; ++k) {                                                    \
       T piv = a[k + (size_t)k * ld];                                                  \
       if (shift) piv += shift[k];                                                     \
+      if (!(piv - piv == 0)) return k; /* NaN / inf: overflowed, not repairable */    \
       if (pivmin) {                                                                   \
         if (!(piv > pivmin[k])) { /* max(|piv|, floor): fixDiag, src/kernels_macros.cuh:90-99 */ \
           const T ap = piv < 0 ? -piv : piv;                                          \
@@ -445,7 +479,11 @@ int orc_blocked_chol(float* A, int n, int lda, const float* d, float* dt, float*
     /* 4. precision for this step's trailing update */
     int p;
     if (o->force_prec) p = o->force_prec[k];
-    else if (o->precision == ORC_SWITCHING) p = orc_choose_precision(d + s + bs, dtt, m, o);
+    else if (o->precision == ORC_SWITCHING) {
+      const float coh = (o->switch_mode == 0 && o->coherence)
+                            ? orc_coherence_ratio(P, lda, m, bs, dtt) : 0.0f;
+      p = orc_choose_precision(d + s + bs, dtt, m, coh, o);
+    }
     else p = o->precision;
     if (step_prec) step_prec[k] = p;
     /* near-indefinite flag for the next diagonal block */

@@ -48,6 +48,8 @@ class CholOpts(ctypes.Structure):
         ("ladder", ctypes.c_int * 4),
         ("force_prec", ctypes.POINTER(ctypes.c_int)),
         ("force_fp64", ctypes.POINTER(ctypes.c_int)),
+        ("coherence", ctypes.c_int),
+        ("equilibrate", ctypes.c_int),
     ]
 
 
@@ -93,7 +95,10 @@ def lib() -> ctypes.CDLL:
         L.orc_potrs_f32_f64.argtypes = [fp, ctypes.c_int, ctypes.c_int, dp, dp]
         L.orc_num_threads.restype = ctypes.c_int
         L.orc_choose_precision.restype = ctypes.c_int
-        L.orc_choose_precision.argtypes = [fp, fp, ctypes.c_int, ctypes.POINTER(CholOpts)]
+        L.orc_choose_precision.argtypes = [fp, fp, ctypes.c_int, ctypes.c_float,
+                                           ctypes.POINTER(CholOpts)]
+        L.orc_coherence_ratio.restype = ctypes.c_float
+        L.orc_coherence_ratio.argtypes = [fp, ctypes.c_int, ctypes.c_int, ctypes.c_int, fp]
         _lib = L
     return _lib
 
@@ -203,14 +208,32 @@ def ref_micro_cholesky(A: np.ndarray) -> tuple[np.ndarray, int]:
 # ---- factorization ----------------------------------------------------------
 
 def make_opts(block_size=256, precision=SWITCHING, eps_prime=0.5, floor=0.0, diag_pert=0,
-              pert=1.0, pivot_floor=1e-7, switch_mode=0, ladder=(E4M3, FP16, FP32)) -> CholOpts:
+              pert=1.0, pivot_floor=1e-7, switch_mode=0, ladder=(E4M3, FP16, FP32),
+              coherence=1, equilibrate=0) -> CholOpts:
     o = CholOpts()
     o.block_size, o.precision, o.eps_prime, o.floor_ratio = block_size, precision, eps_prime, floor
     o.diag_pert, o.pert, o.pivot_floor, o.switch_mode = diag_pert, pert, pivot_floor, switch_mode
+    o.coherence, o.equilibrate = coherence, equilibrate
     o.ladder_len = len(ladder)
     for i in range(4):
         o.ladder[i] = ladder[i] if i < len(ladder) else FP32
     return o
+
+
+OPTS_FIELDS = ("block_size", "precision", "eps_prime", "floor", "diag_pert", "pert",
+               "pivot_floor", "switch_mode")
+
+
+def factor_kwargs(opts) -> dict:
+    """make_opts keyword arguments equal to a library options struct (the
+    ctypes mpchol_opts of cholesky_gpu_b200._lib, or any object with the same
+    field names), so that the oracle restates a GPU factor with the options it
+    was computed with -- the diagonal shifts and pivot floor included."""
+    kw = {f: getattr(opts, f) for f in OPTS_FIELDS}
+    kw["ladder"] = tuple(int(opts.ladder[i]) for i in range(int(opts.ladder_len)))
+    kw["coherence"] = int(getattr(opts, "coherence", 0))
+    kw["equilibrate"] = int(getattr(opts, "equilibrate", 0))
+    return kw
 
 
 def blocked_chol(A: np.ndarray, force_prec=None, force_fp64=None, **kw):
@@ -220,6 +243,12 @@ def blocked_chol(A: np.ndarray, force_prec=None, force_fp64=None, **kw):
     n = A.shape[0]
     o = make_opts(**kw)
     F = np.array(A, dtype=np.float32, order="F", copy=True)
+    ex = None
+    if o.equilibrate:
+        # D A D with D = diag(2^-e_i) (exact power-of-two scaling), then the
+        # factor's rows are scaled back by 2^e_i
+        ex = equilibration_exponents(np.diag(F))
+        F = np.asfortranarray(np.ldexp(F, -(ex[:, None] + ex[None, :])).astype(np.float32))
     d = np.ascontiguousarray(np.diag(F).astype(np.float32))
     dt = d.copy()
     sh = np.zeros(n, dtype=np.float32)
@@ -239,15 +268,40 @@ def blocked_chol(A: np.ndarray, force_prec=None, force_fp64=None, **kw):
     lib().orc_blocked_chol(_fptr(F), n, n, _fptr(d), _fptr(dt), _fptr(sh), ctypes.byref(o),
                            sp.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
                            s64.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), ctypes.byref(info))
-    return dict(L=np.tril(np.asarray(F)), d=d, dtilde=dt, step_prec=sp, step_fp64=s64,
-                status=info.status, fail_row=info.fail_row, n_perturbed=info.n_perturbed)
+    L = np.tril(np.asarray(F))
+    if ex is not None:
+        L = np.ldexp(L, ex[:, None]).astype(np.float32)
+    return dict(L=L, d=d, dtilde=dt, step_prec=sp, step_fp64=s64,
+                status=info.status, fail_row=info.fail_row, n_perturbed=info.n_perturbed,
+                eq_exp=ex)
 
 
-def choose_precision(d: np.ndarray, dtilde: np.ndarray, **kw) -> int:
+def equilibration_exponents(diag: np.ndarray) -> np.ndarray:
+    """e_i = floor((floor(log2 a_ii) + 1) / 2), clamped to [-63, 63], so that
+    a_ii * 2^(-2 e_i) lies in [0.5, 2); 0 for a non-positive or non-finite
+    diagonal entry.  (The diagonal scaling intent of src/kernels_macros.cuh:137-158.)"""
+    a = np.asarray(diag, dtype=np.float32).astype(np.float64)
+    ok = np.isfinite(a) & (a > 0)
+    _, fe = np.frexp(np.where(ok, a, 1.0))
+    E = fe.astype(np.int64) - 1                      # floor(log2 a)
+    e = np.clip((E + 1) // 2, -63, 63)
+    return np.where(ok, e, 0).astype(np.int32)
+
+
+def coherence_ratio(P: np.ndarray, dtilde: np.ndarray) -> float:
+    """(||P^T 1||^2 / m) / min dtilde of a solved panel P (m x b), as the
+    factor's switching rule computes it."""
+    P = np.asfortranarray(P, dtype=np.float32)
+    dt = np.ascontiguousarray(dtilde, dtype=np.float32)
+    m, bs = P.shape
+    return float(lib().orc_coherence_ratio(_fptr(P), max(m, 1), m, bs, _fptr(dt)))
+
+
+def choose_precision(d: np.ndarray, dtilde: np.ndarray, coh: float = 0.0, **kw) -> int:
     o = make_opts(**kw)
     d = np.ascontiguousarray(d, dtype=np.float32)
     dt = np.ascontiguousarray(dtilde, dtype=np.float32)
-    return lib().orc_choose_precision(_fptr(d), _fptr(dt), d.size, ctypes.byref(o))
+    return lib().orc_choose_precision(_fptr(d), _fptr(dt), d.size, float(coh), ctypes.byref(o))
 
 
 def micro_cholesky(A: np.ndarray) -> tuple[np.ndarray, int]:

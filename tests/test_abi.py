@@ -78,3 +78,21 @@ def test_null_and_size_arguments_rejected():
     assert lib.mpchol_quantize_hash(0, 16, 0, 2, None, None) == _lib.ERR_BAD_ARG
     assert lib.mpchol_factor_destroy(None) == _lib.ERR_BAD_ARG
     assert lib.mpchol_precond_cg(None, None, None, 4, 2, 0.0, 0.0, 0.0, 0, 32, 0.0, 10, None) < 0
+
+
+def test_smoke_checks_the_factor_with_its_own_options():
+    """smoke() restates its factor with the oracle under the options the
+    factor was computed with: the library defaults (rounding-error shifts,
+    pivot floor, coherence rule) plus the smoke case's block size and
+    precision -- not the oracle's own defaults."""
+    import __graft_entry__ as ge
+    from oracle import oracle as O
+    opts = _lib.default_opts(**ge.SMOKE_OPTS)
+    kw = ge.smoke_oracle_kwargs(opts)
+    d = _lib.default_opts()
+    assert kw["diag_pert"] == d.diag_pert == 1
+    assert kw["pert"] == pytest.approx(d.pert) and kw["pivot_floor"] == pytest.approx(d.pivot_floor)
+    assert kw["block_size"] == ge.SMOKE_OPTS["block_size"]
+    assert kw["precision"] == O.SWITCHING and kw["coherence"] == d.coherence
+    # the oracle accepts exactly these keywords
+    O.make_opts(**kw)

@@ -10,7 +10,7 @@ import pytest
 import cholesky_gpu_b200 as mp
 from cholesky_gpu_b200 import MpcholError
 
-STEP_BYTES = 20      # StepState: five 32-bit fields
+STEP_BYTES = 32      # StepState: eight 32-bit fields
 STATUS_BYTES = 16    # DevStatus: four 32-bit fields
 
 
@@ -66,5 +66,15 @@ def test_invalid_blob_is_rejected(what):
         "truncated": lambda: blob[:-1],
         "short": lambda: blob[:40],
     }[what]()
+    with pytest.raises(MpcholError):
+        mp.factor_blob_info(bad)
+
+
+@pytest.mark.parametrize("n", [(1 << 24) + 1, 2**31 - 1, 2**31 - 200])
+def test_hostile_order_is_rejected_before_size_arithmetic(n):
+    """An order near INT_MAX (whose step count and size loop would overflow
+    or run for a very long time) is rejected by the bound on n alone."""
+    blob = make_blob(300, 64, seed=4)
+    bad = corrupt(corrupt(blob, 16, "<i", n), 24, "<i", -(-n // 64))
     with pytest.raises(MpcholError):
         mp.factor_blob_info(bad)

@@ -6,6 +6,8 @@ back from the GPU), by relative Frobenius error of the lower triangle with a
 per-precision bar.  Solutions are checked against the FP64 dense Cholesky
 solve, with the FP64 true residual, backward error and iteration count.
 """
+import ctypes
+
 import numpy as np
 import pytest
 import torch
@@ -25,12 +27,11 @@ def factor_parity(A: np.ndarray, **opts):
     f = mp.factor(torch.from_numpy(A).cuda(), **opts)
     info = f.info()
     Lg = f.lower().cpu().numpy()
-    ref = O.blocked_chol(A, block_size=opts.get("block_size", 256),
-                         precision=O.SWITCHING, force_prec=info.step_prec,
-                         force_fp64=info.step_fp64,
-                         eps_prime=opts.get("eps_prime", 0.5), floor=opts.get("floor", 0.0),
-                         diag_pert=opts.get("diag_pert", 1), pert=opts.get("pert", 1.0),
-                         pivot_floor=opts.get("pivot_floor", 1e-7))
+    # the oracle with the factor's own options (library defaults included),
+    # run with the GPU's per-step precisions and FP64-diagonal flags
+    kw = O.factor_kwargs(f.opts)
+    kw["precision"] = O.SWITCHING
+    ref = O.blocked_chol(A, force_prec=info.step_prec, force_fp64=info.step_fp64, **kw)
     Lo = ref["L"]
     err = np.linalg.norm(Lg - Lo) / np.linalg.norm(Lo)
     return f, info, ref, err
@@ -234,26 +235,42 @@ def test_reported_backward_error_matches_numpy(cuda, n):
 
 
 def test_factor_save_load_round_trip(cuda):
-    """A saved factor restored into a new object gives the same L bits, the
-    same step precisions and the same PCG solve without refactoring; a blob
-    of another order or block size is refused."""
+    """A factor saved before a solve, restored into a new object, gives the
+    same L bits, step precisions, status word (floored pivots) and PCG solve
+    without refactoring; a solve does not change the factor's status word, so
+    a factor saved after the solve carries the same status; the target's
+    storage outside L's lower triangle is never read (NaN-filled before the
+    load); a blob of another order or block size is refused."""
     n = 1000
-    A = matgen.spd_matrix(n, 1e4, 71)
+    # kappa = 1e6 with a pivot floor of 1e-3 d_i: a few hundred pivots are
+    # raised to the floor (a modified-Cholesky preconditioner, still SPD)
+    A = matgen.spd_matrix(n, 1e6, 71)
     B = matgen.rhs(n, 2, 72).to(torch.float64)
-    opts = dict(block_size=256, precision="switching", eps_prime=1e-5,
+    opts = dict(block_size=256, precision="switching", eps_prime=1e-5, pivot_floor=1e-3,
                 ladder=["e4m3", "fp16", "fp16x2"])
     f = mp.Factor(n, **opts)
     f.compute(A.cuda())
-    X1, r1 = f.pcg(A.cuda(), B.cuda(), rel_tol=1e-10)
-    blob = f.save()
+    fi = f.info()
+    assert fi.status == 0 and fi.n_perturbed > 0
+    blob = f.save()                          # before any solve
+    X1, r1 = f.pcg(A.cuda(), B.cuda(), rel_tol=1e-10, max_it=400)
+    assert f.info().n_perturbed == fi.n_perturbed
+    assert f.save() == blob                  # the solve left the factor's state alone
     assert mp.factor_blob_info(blob) == (n, 256)
-    g = mp.Factor(n, **opts).load(blob)
+    g = mp.Factor(n, **opts)
+    p = ctypes.c_void_p()
+    ld = ctypes.c_int()
+    nn = ctypes.c_int()
+    g.lib.mpchol_factor_lower(g.handle, ctypes.byref(p), ctypes.byref(ld), ctypes.byref(nn))
+    from cholesky_gpu_b200.api import _wrap_device
+    _wrap_device(p.value, (n, ld.value), torch.float32).fill_(float("nan"))
+    g.load(blob)
     assert torch.equal(g.lower(), f.lower())
-    fi, gi = f.info(), g.info()
+    gi = g.info()
     assert gi.step_prec == fi.step_prec and gi.step_fp64 == fi.step_fp64
     assert gi.status == fi.status and gi.n_perturbed == fi.n_perturbed
-    X2, r2 = g.pcg(A.cuda(), B.cuda(), rel_tol=1e-10)
-    assert r2.converged and r2.iterations == r1.iterations
+    X2, r2 = g.pcg(A.cuda(), B.cuda(), rel_tol=1e-10, max_it=400)
+    assert r1.converged and r2.converged and r2.iterations == r1.iterations
     x1, x2 = X1.cpu().numpy(), X2.cpu().numpy()
     assert np.linalg.norm(x2 - x1) / np.linalg.norm(x1) < 1e-8
     with pytest.raises(mp.MpcholError):

@@ -2,7 +2,9 @@
 
 Its factor is compared with the one mpchol_factor computes for the same block
 (a single-step factorization runs the same diagonal kernel), on two calls in
-a row so the second call sees the static scratch the first one left behind.
+a row so the second call sees the static scratch the first one left behind,
+and with the oracle: the restated reference micro_cholesky
+(src/micro_chol.hpp:14-44, FP32, unblocked) and an FP64 Cholesky.
 The file is named to be collected last; it passes alone and after the rest.
 """
 import ctypes
@@ -13,9 +15,14 @@ import torch
 
 import cholesky_gpu_b200 as mp
 from cholesky_gpu_b200 import _lib, matgen
+from oracle import oracle as O
 
 # both paths run the same kernel on the same input: the bound is FP32-level
 TOL = 1e-6
+# against another FP32 Cholesky (the oracle's unblocked micro_cholesky, which
+# orders its operations differently) and FP64: two FP32 factorizations of a
+# kappa = 1e3 matrix differ by up to ~kappa * u32 = 6e-5
+TOL_ORACLE = 1e-4
 
 
 def static_potrf(A: np.ndarray, pivot_floor: float):
@@ -46,8 +53,14 @@ def test_static_potrf_matches_factor_on_two_calls_in_a_row(cuda):
         assert info == 0
         Lf = factor_lower(A)
         err = np.linalg.norm(L - Lf) / np.linalg.norm(Lf)
-        print(f"n={n}: static vs factor rel Frobenius {err:.2e}")
+        Lm, rc = O.micro_cholesky(A)
+        L64 = np.linalg.cholesky(A.astype(np.float64))
+        err_m = np.linalg.norm(L - Lm) / np.linalg.norm(Lm)
+        err_64 = np.linalg.norm(L - L64) / np.linalg.norm(L64)
+        print(f"n={n}: static vs factor {err:.2e}, vs micro_cholesky {err_m:.2e}, "
+              f"vs FP64 {err_64:.2e}")
         assert err <= TOL
+        assert rc == 0 and err_m <= TOL_ORACLE and err_64 <= TOL_ORACLE
 
 
 @pytest.mark.gpu
