@@ -1,23 +1,30 @@
 """Time-to-solution benchmark for the mixed-precision Cholesky-preconditioned PCG.
 
 Metric: time to a 1e-10 FP64-checked relative residual ||b - A x|| / ||b|| on
-one B200, for the switching mixed-precision factor (E4M3 / FP16 / FP32 trailing
-updates chosen per step) next to the plain FP32-factor PCG on the same GPU.
+one B200, for the switching mixed-precision factor (MXFP8 / FP16 / FP16X2
+trailing updates chosen per step) next to the plain FP32-factor PCG on the
+same GPU.
 
-Workload (default): n = 8192 dense SPD A = Q diag(sigma) Q^T in FP32 storage,
-Q from QR of a seeded N(0,1) matrix, sigma geometric 1 -> 1e-6 (kappa = 1e6),
-block 256, one right-hand side b ~ N(0,1).  Synthetic seeded inputs stand in
-for the reference's generated matrices.  One "step" = factor + PCG to 1e-10 of
-that system.  A (256 MiB) is larger than the 126 MB L2, so every step streams
-it from HBM; no separate L2 flush is needed.
+Workload (default, the precision-at-scale configuration): the Gaussian RBF
+kernel matrix K_ij = exp(-||x_i - x_j||^2 / (2 l^2)) + 1e-3 delta_ij of
+n = 16384 points in [0,1]^784 whose coordinates are 0 with probability 0.8
+and U(0,1) otherwise (the seeded stand-in for the image data, which is not
+available), l = the exact median pairwise distance, FP32 storage, block 256,
+8 right-hand sides ~ N(0,1).  The mixed arm switches per step over the ladder
+MXFP8 -> FP16 -> FP16X2 with eps' = 2 (the coherence rule keeps the constant
+mode's step off FP8).  One "step" = factor + PCG to 1e-10 of all 8 rhs.  K
+(1 GiB) is larger than the 126 MB L2, so every step streams it from HBM; no
+separate L2 flush is needed.  `--workload spd` is the n = 8192, kappa = 1e6
+SPD configuration; `rbf-grad` and `batch` the differentiation and batching
+workloads.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mpchol|reference]
 
 Under torchrun with N > 1 every rank solves its own system (replicas, no
 collective on the data path): value = max over ranks of the time to solution.
-`--impl reference` times the reference's own CPU path (its micro_cholesky,
-src/micro_chol.hpp, built from the reference sources into oracle/_ref, or the
-oracle's restatement of it) on the host cores.
+`--impl reference` runs the reference's own CPU path (its micro_cholesky,
+src/micro_chol.hpp, built from the reference sources into oracle/_ref, and a
+host FP64 PCG) on the full workload, one step.
 """
 from __future__ import annotations
 
@@ -46,25 +53,37 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mpchol", choices=["mpchol", "reference"])
-    ap.add_argument("--n", type=int, default=8192)
+    ap.add_argument("--workload", default="rbf", choices=["rbf", "spd", "rbf-grad", "batch"],
+                    help="rbf (default): Gaussian RBF kernel matrix, n=16384 points in [0,1]^784 "
+                         "with 80%% zero coordinates, nugget 1e-3, 8 rhs, MXFP8 switching ladder; "
+                         "spd: n=8192 Q diag(sigma) Q^T, kappa=1e6, 1 rhs; rbf-grad: forward + "
+                         "adjoint gradients of 1/2 y^T K^-1 y, n=8192, d=64; batch: 512 SPD "
+                         "systems of order U[64, 2048]")
+    ap.add_argument("--n", type=int, default=None)
+    ap.add_argument("--rhs", type=int, default=None)
     ap.add_argument("--kappa", type=float, default=1e6)
     ap.add_argument("--block", type=int, default=256)
-    ap.add_argument("--eps-prime", type=float, default=1e-5)
+    ap.add_argument("--eps-prime", type=float, default=None)
     ap.add_argument("--precision", default="switching",
-                    help="policy of the mixed arm: switching, e4m3, e5m2, fp16, fp16x2")
-    ap.add_argument("--ladder", default="e4m3,fp16,fp16x2",
+                    help="policy of the mixed arm: switching, e4m3, e5m2, mxfp8, fp16, fp16x2")
+    ap.add_argument("--ladder", default=None,
                     help="switching ladder, lowest precision first (its last entry is the "
                          "fallback)")
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--max-it", type=int, default=400)
     ap.add_argument("--check-every", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="spd", choices=["spd", "rbf", "rbf-grad", "batch"],
-                    help="spd: the dense SPD time-to-solution workload (default); rbf: Gaussian "
-                         "RBF kernel matrix, n=16384 points in [0,1]^784, 8 rhs; rbf-grad: "
-                         "forward + adjoint gradients of 1/2 y^T K^-1 y, n=8192, d=64; batch: "
-                         "512 SPD systems of order U[64, 2048]")
-    return ap.parse_args()
+    args = ap.parse_args()
+    w = WORKLOADS.get(args.workload, {})
+    if args.n is None:
+        args.n = w.get("n", 8192)
+    if args.rhs is None:
+        args.rhs = w.get("rhs", 1)
+    if args.ladder is None:
+        args.ladder = w.get("ladder", "e4m3,fp16,fp16x2")
+    if args.eps_prime is None:
+        args.eps_prime = w.get("eps", 1e-5)
+    return args
 
 
 def dist_init(args):
@@ -210,10 +229,58 @@ def profiled_traffic(kernel: str, n: int):
 
 
 # ---------------------------------------------------------------- GPU arm
+PREC_LETTER = {0: "S", 1: "h", 2: "e", 3: "f", 4: "M", 6: "X"}   # per-step sequence letters
+PREC_KEYS = ((0, "fp32"), (1, "fp16"), (2, "e4m3"), (3, "e5m2"), (4, "mxfp8"), (6, "fp16x2"))
+
+# Per-workload defaults of the mixed arm: the switching ladder (lowest
+# precision first) and eps'.  RBF: MXFP8 wherever the criterion allows it
+# (every step after the constant mode at eps' = 2); SPD kappa = 1e6: FP8 is
+# rejected by the Schur ratio at any useful eps', FP16X2 carries the factor.
+WORKLOADS = {
+    "rbf": dict(n=16384, ladder="mxfp8,fp16,fp16x2", eps=2.0, rhs=8),
+    "spd": dict(n=8192, ladder="e4m3,fp16,fp16x2", eps=1e-5, rhs=1),
+}
+
+
+def workload_inputs(args, rank, dev):
+    """The system of the time-to-solution workloads, generated outside any
+    timed region: (A FP32 n x n on the device, lower triangle valid; B FP64
+    n x rhs; description)."""
+    import torch
+    from cholesky_gpu_b200 import autograd as AG, matgen
+    n = args.n
+    if args.workload == "rbf":
+        # 16384 points in [0,1]^784, 80 % zero coordinates, the rest U(0,1)
+        # (the seeded stand-in for the image data); l = exact median pairwise
+        # distance; nugget 1e-3; K built on the device in FP64, stored FP32
+        X = torch.from_numpy(matgen.mnist_like_points(n, 784, 4 + rank)).to(dev)
+        ell = matgen.median_pairwise_distance(X)
+        _, A = AG.rbf_build(X, ell, 1e-3, fp64=False)
+        del X
+        B = matgen.rhs(n, args.rhs, 5 + rank, device=dev)
+        desc = {"workload": (f"rbf n={n} d=784 zeros=0.8 l=median({ell:.4f}) nugget=1e-3 "
+                             f"rhs={args.rhs} block={args.block} ladder={args.ladder} "
+                             f"eps'={args.eps_prime:g}"),
+                "n": n, "d": 784, "lengthscale": round(ell, 6), "nugget": 1e-3}
+        data = "synthetic (seeded sparse points in [0,1]^784 standing in for image data; RBF kernel)"
+    else:
+        A = matgen.spd_matrix(n, args.kappa, 3 + rank, device=dev)
+        B = matgen.rhs(n, args.rhs, 100 + rank, device=dev)
+        B = B.reshape(n, -1)
+        desc = {"workload": (f"spd n={n} kappa={args.kappa:g} rhs={args.rhs} block={args.block} "
+                             f"ladder={args.ladder} eps'={args.eps_prime:g}"),
+                "n": n, "kappa": args.kappa}
+        data = "synthetic (seeded Q diag(sigma) Q^T, geometric spectrum)"
+    B = B.reshape(n, -1).contiguous()
+    desc.update({"rhs": args.rhs, "block": args.block, "tol": args.tol,
+                 "l2": "inputs larger than L2 (A = %d MiB)" % (n * n * 4 // (1 << 20))})
+    return A, B, desc, data
+
+
 def run_gpu(args, world, rank, local):
     import torch
     import cholesky_gpu_b200 as mp
-    from cholesky_gpu_b200 import _lib, matgen
+    from cholesky_gpu_b200 import _lib
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -225,34 +292,21 @@ def run_gpu(args, world, rank, local):
         pg = dist
     lib = _lib.load()
     n, b = args.n, args.block
-    seed = 3 + rank
-    A = matgen.spd_matrix(n, args.kappa, seed, device=dev)
-    B = matgen.rhs(n, 1, 100 + rank, device=dev)
-    A_host = A.cpu().pin_memory()
-    B_host = B.cpu().pin_memory()
+    A, B, desc, data = workload_inputs(args, rank, dev)
     stream = torch.cuda.current_stream(dev)
-
-    def solve_once(precision, Ad, Bd):
-        f = mp.Factor(n, block_size=b, precision=precision, eps_prime=args.eps_prime)
-        f.compute(Ad)
-        X, rep = f.pcg(Ad, Bd, rel_tol=args.tol, max_it=args.max_it, check_every=args.check_every)
-        return f, X, rep
-
-    # factor objects are created outside the timed region (allocation is setup)
-    # "switching" is the mixed-precision arm (its policy from --precision /
-    # --ladder), "fp32" the plain FP32-factor comparator
     ladder = [x.strip() for x in args.ladder.split(",") if x.strip()]
-    fobj = {"switching": mp.Factor(n, block_size=b, precision=args.precision,
-                                   eps_prime=args.eps_prime, ladder=ladder),
+    mixed_opts = dict(block_size=b, precision=args.precision, eps_prime=args.eps_prime,
+                      ladder=ladder)
+    # factor objects are created outside the timed region (allocation is setup)
+    fobj = {"mixed": mp.Factor(n, **mixed_opts),
             "fp32": mp.Factor(n, block_size=b, precision="fp32")}
 
-    def step(precision):
-        f = fobj[precision]
+    def step(name, f=None):
+        f = f or fobj[name]
         f.compute(A)
-        X, rep = f.pcg(A, B, rel_tol=args.tol, max_it=args.max_it, check_every=args.check_every)
-        return X, rep
+        return f.pcg(A, B, rel_tol=args.tol, max_it=args.max_it, check_every=args.check_every)
 
-    def timed(precision, k):
+    def timed(name, k):
         times, reps = [], []
         for _ in range(k):
             if pg:
@@ -261,7 +315,7 @@ def run_gpu(args, world, rank, local):
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            X, rep = step(precision)
+            _, rep = step(name)
             e1.record(stream)
             torch.cuda.synchronize()
             times.append(e0.elapsed_time(e1))
@@ -269,14 +323,14 @@ def run_gpu(args, world, rank, local):
         return times, reps
 
     for _ in range(args.warmup):
-        step("switching")
+        step("mixed")
         step("fp32")
     launches0 = lib.mpchol_kernel_launches()
     with ClockSampler(local, pci_bus_id(torch, local)) as clk:
-        t_sw, r_sw = timed("switching", args.steps)
-        launches_sw = lib.mpchol_kernel_launches() - launches0
+        t_mx, r_mx = timed("mixed", args.steps)
+        launches_mx = lib.mpchol_kernel_launches() - launches0
         t_32, r_32 = timed("fp32", args.steps)
-    info_sw = fobj["switching"].info()
+    info_mx = fobj["mixed"].info()
 
     def mx(v):
         if pg:
@@ -285,47 +339,160 @@ def run_gpu(args, world, rank, local):
             return t.item()
         return v
 
-    ms_sw = mx(statistics.median(t_sw))
+    ms_mx = mx(statistics.median(t_mx))
     ms_32 = mx(statistics.median(t_32))
 
-    # end-to-end through the public API with host buffers: Factor.solve_host
+    # end to end through the public API with host buffers: Factor.solve_host
     # (mpchol_solve_host) copies A's lower triangle (block columns from the
-    # diagonal down) and b to the device, factors, runs PCG and copies x back
-    e2e_times = []
-    for i in range(max(2, min(args.steps, 3)) + 1):
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        xh, rep = fobj["switching"].solve_host(A_host, B_host, rel_tol=args.tol,
-                                               max_it=args.max_it, check_every=args.check_every)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        if i > 0:
-            e2e_times.append(e0.elapsed_time(e1))
+    # diagonal down, overlapped with the factorization) and B to the device,
+    # factors, runs PCG and copies X back -- for both arms
+    A_host = A.cpu().pin_memory()
+    B_host = B.cpu().pin_memory()
+    e2e = {}
+    for name in ("mixed", "fp32"):
+        ts = []
+        for i in range(max(2, min(args.steps, 4)) + 1):
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            _, rep_h = fobj[name].solve_host(A_host, B_host, rel_tol=args.tol, max_it=args.max_it,
+                                             check_every=args.check_every)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if i > 0:
+                ts.append(e0.elapsed_time(e1))
+            if not rep_h.converged:
+                raise RuntimeError(f"{name} host-buffer solve did not converge: {rep_h}")
+        e2e[name] = mx(statistics.median(ts))
     e2e_h2d = sum((n - c) * min(b, n - c) for c in range(0, n, b)) * 4 + B_host.numel() * 8
-    e2e_ms = mx(statistics.median(e2e_times))
 
-    # per-phase breakdown of one profiled step (events inside the library)
+    # per-phase breakdown of one profiled mixed step (events inside the library)
+    phases, calls = profiled_phases(lib, lambda: step("mixed"))
+    roof = roofline(args, lib, fobj["mixed"].info(), phases, calls, n, b)
+
+    # forced-format arms: time to solution (or the failure) when every step
+    # takes one format, with and without larger rounding-error shifts
+    arms = {}
+    for name, opts in forced_arms(args):
+        f = mp.Factor(n, block_size=b, **opts)
+        arms[name] = forced_arm(f, lambda f=f: step(None, f), stream)
+
+    steps_used = {nm: info_mx.steps_by_prec[i] for i, nm in PREC_KEYS if info_mx.steps_by_prec[i]}
+    result = {
+        "metric": METRIC,
+        "value": round(ms_mx, 3),
+        "unit": "ms",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms_mx, 3),
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "%s factor, fp64 pcg" % "/".join(steps_used),
+        "data": data,
+        "config": dict(desc, parallelism=f"replicas x{world}" if world > 1 else "single GPU"),
+        "comparator_fp32_factor_ms": round(ms_32, 3),
+        "speedup_vs_fp32_factor": round(ms_32 / ms_mx, 3),
+        "e2e": {"value": round(e2e["mixed"], 3), "unit": "ms",
+                "h2d_bytes_per_step": int(e2e_h2d), "d2h_bytes_per_step": int(B.numel() * 8)},
+        "e2e_comparator_fp32_factor_ms": round(e2e["fp32"], 3),
+        "e2e_speedup_vs_fp32_factor": round(e2e["fp32"] / e2e["mixed"], 3),
+        "iterations": {"mixed": r_mx[-1].iterations, "fp32": r_32[-1].iterations},
+        "rel_residual": {"mixed": r_mx[-1].rel_residual, "fp32": r_32[-1].rel_residual},
+        "backward_error": {"mixed": r_mx[-1].backward_error, "fp32": r_32[-1].backward_error},
+        "converged": {"mixed": r_mx[-1].converged, "fp32": r_32[-1].converged},
+        "step_precisions": steps_used,
+        "step_sequence": "".join(PREC_LETTER.get(p, "?") for p in info_mx.step_prec[:-1]),
+        "forced_arms": arms,
+        "phase_ms_mixed_step": phases,
+        "phase_calls_mixed_step": calls,
+        "gpu_launches": int(launches_mx),
+        "roofline": roof,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        A64 = A_host.numpy()
+        result["cpu_baseline"] = cpu_baseline(args, A64, B_host.numpy(), r_32[-1].iterations)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return result if rank == 0 else None
+
+
+def forced_arms(args):
+    """Fixed-format factors timed beside the switching arm.  FP8 everywhere
+    (E4M3 and MXFP8, with the default rounding-error shifts and with four
+    times larger ones) shows what the switching rule avoids; FP16X2 and FP16
+    everywhere bracket it from the precise side."""
+    out = [("fp16x2", dict(precision="fp16x2")), ("fp16", dict(precision="fp16"))]
+    for p in ("mxfp8", "e4m3"):
+        out.append((p, dict(precision=p)))
+        out.append((p + "_pert4", dict(precision=p, pert=4.0)))
+    return out
+
+
+def forced_arm(f, solve, stream, k=2):
+    """Time (median of k after one warm-up) and outcome of one forced arm;
+    a factor or solve that fails is recorded with its status."""
+    import torch
+    from cholesky_gpu_b200 import MpcholError
+    try:
+        solve()
+        times, rep = [], None
+        for _ in range(k):
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            _, rep = solve()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        info = f.info()
+        return {"ms": round(statistics.median(times), 3), "iterations": rep.iterations,
+                "converged": rep.converged, "rel_residual": rep.rel_residual,
+                "n_perturbed": info.n_perturbed}
+    except MpcholError as e:
+        info = f.info()
+        return {"status": _status_name(e.status), "fail_row": info.fail_row,
+                "n_perturbed": info.n_perturbed}
+
+
+def _status_name(st):
+    from cholesky_gpu_b200 import _lib
+    return _lib.load().mpchol_status_str(st).decode()
+
+
+def profiled_phases(lib, fn):
+    """Per-phase device time and call count of one call of fn (CUDA events the
+    library records on the launching streams)."""
+    import torch
+    from cholesky_gpu_b200 import _lib
     lib.mpchol_profile_enable(1)
-    prof0 = _lib.Profile()
-    lib.mpchol_profile_read(prof0, 1)
-    _, rep_p = step("switching")
+    p0 = _lib.Profile()
+    lib.mpchol_profile_read(p0, 1)
+    fn()
     torch.cuda.synchronize()
-    prof = _lib.Profile()
-    lib.mpchol_profile_read(prof, 1)
+    p = _lib.Profile()
+    lib.mpchol_profile_read(p, 1)
     lib.mpchol_profile_enable(0)
-    phases = {nm: round(prof.ms[i], 4) for i, nm in enumerate(_lib.PHASE_NAMES) if prof.calls[i]}
-    calls = {nm: int(prof.calls[i]) for i, nm in enumerate(_lib.PHASE_NAMES) if prof.calls[i]}
+    phases = {nm: round(p.ms[i], 4) for i, nm in enumerate(_lib.PHASE_NAMES) if p.calls[i]}
+    calls = {nm: int(p.calls[i]) for i, nm in enumerate(_lib.PHASE_NAMES) if p.calls[i]}
+    return phases, calls
 
-    # rooflines of the bandwidth- and tensor-bound phases of the profiled step;
-    # the headline one is the phase with the largest device time
+
+def roofline(args, lib, info, phases, calls, n, b):
+    """Rooflines of the bandwidth- and tensor-bound phases of the profiled
+    step; the headline is the phase with the largest device time."""
+    from cholesky_gpu_b200 import _lib
     hbm, bf16, peak_kind = measured_peaks()
-    info_p = fobj["switching"].info()
+    nr = 1 if args.rhs <= 1 else (2 if args.rhs <= 2 else (4 if args.rhs <= 4 else 8))
     tc_flops, tc_bytes, tc_exec, tc_fmts = 0.0, 0.0, 0, {}
     panel_bytes = {_lib.PREC_FP16: 2, _lib.PREC_E4M3: 1, _lib.PREC_E5M2: 1, _lib.PREC_MXFP8: 1,
                    _lib.PREC_FP16X2: 4}
-    for k, pr in enumerate(info_p.step_prec):
+    for k, pr in enumerate(info.step_prec):
         s0 = k * b
         bs = min(b, n - s0)
         m = n - s0 - bs
@@ -333,8 +500,10 @@ def run_gpu(args, world, rank, local):
             break
         if pr != _lib.PREC_FP32:
             tc_flops += float(m) * (m + 1) * bs       # lower triangle, algorithmic
-            # C lower triangle read + written in FP32, the quantized panel read once
-            tc_bytes += float(m) * (m + 1) / 2 * 8 + float(m) * bs * panel_bytes.get(pr, 1)
+            # C lower triangle read + written in FP32, the quantized panel read
+            # once (plus its E8M0 scales for MXFP8)
+            tc_bytes += (float(m) * (m + 1) / 2 * 8 + float(m) * bs * panel_bytes.get(pr, 1)
+                         + (float(m) * bs / 32 if pr == _lib.PREC_MXFP8 else 0.0))
             tc_exec += 1
             tc_fmts[pr] = tc_fmts.get(pr, 0) + 1
     by_phase = {}
@@ -350,21 +519,22 @@ def run_gpu(args, world, rank, local):
                           "work_per_launch": work, "launches": launches,
                           "ms": phases[name], "note": note}
 
-    tri = n * (n + 1) / 2 * 4 + 3 * n * 8
+    tri = n * (n + 1) / 2 * 4 + 3 * n * 8 * nr
     add("trsv", "hbm", "GB/s", hbm, tri, calls.get("trsv", 0),
-        "one triangular solve: lower triangle of L in FP32 + FP64 vectors")
-    add("symv", "hbm", "GB/s", hbm, n * (n + 1) / 2 * 4 + 2 * n * 8, calls.get("symv", 0),
-        "A x from the lower triangle of A in FP32, FP64 vectors")
+        f"one triangular solve: lower triangle of L in FP32 + FP64 vectors ({nr} rhs)")
+    add("symv", "hbm", "GB/s", hbm, n * (n + 1) / 2 * 4 + 2 * n * 8 * nr, calls.get("symv", 0),
+        f"A X from the lower triangle of A in FP32, FP64 vectors ({nr} rhs)")
     if tc_exec:
-        # At b = 256 the trailing update moves 8 bytes of C per 2b (x3 for FP16X2)
-        # flops: below the B200 ridge point, so HBM is the binding roof; the
-        # tensor rate is reported beside it.
+        # At b = 256 the trailing update moves 8 bytes of C per 2b flops (x3
+        # for FP16X2): below the B200 ridge point, so HBM is the binding roof;
+        # the useful tensor rate is reported beside it against the dense FP8
+        # peak (2 x the measured bf16 rate) when FP8 steps dominate
         fp8 = sum(v for k_, v in tc_fmts.items() if k_ in (_lib.PREC_E4M3, _lib.PREC_E5M2,
                                                              _lib.PREC_MXFP8))
         tpeak = 2 * bf16 if fp8 * 2 > tc_exec else bf16
         add("syrk_tc", "hbm", "GB/s", hbm, tc_bytes / tc_exec, tc_exec,
             "trailing update: C lower triangle read+write (FP32) + quantized panel per "
-            "executing launch; tensor_tflops = m(m+1)b useful flops / time (FP16X2 issues 3x)")
+            "executing step; tensor_tflops = m(m+1)b useful flops / time")
         if "syrk_tc" in by_phase:
             tt = tc_flops / (phases["syrk_tc"] * 1e-3) / 1e12
             by_phase["syrk_tc"]["tensor_tflops"] = round(tt, 1)
@@ -373,122 +543,159 @@ def run_gpu(args, world, rank, local):
     dom = max(by_phase, key=lambda k_: by_phase[k_]["ms"]) if by_phase else None
     if dom:
         r = by_phase[dom]
-        roof = {"kernel": dom, "bound": r["bound"], "achieved": r["achieved"], "peak": r["peak"],
+        return {"kernel": dom, "bound": r["bound"], "achieved": r["achieved"], "peak": r["peak"],
                 "peak_kind": peak_kind, "unit": r["unit"], "frac": r["frac"],
                 "algorithmic_per_launch": r["work_per_launch"],
                 "traffic": profiled_traffic(dom, n), "by_phase": by_phase}
-    else:
-        roof = {"kernel": None, "bound": "hbm", "achieved": None, "peak": hbm,
-                "peak_kind": peak_kind, "unit": "GB/s", "frac": None, "traffic": None}
-
-    result = {
-        "metric": METRIC,
-        "value": round(ms_sw, 3),
-        "unit": "ms",
-        "n_gpus": world,
-        "steps": args.steps,
-        "warmup": args.warmup,
-        "ms_per_step": round(ms_sw, 3),
-        "higher_is_better": False,
-        "scaling": "weak",
-        "vs_baseline": None,
-        "dtype": "%s factor, fp64 pcg" % "/".join(
-            nm for i, nm in ((2, "e4m3"), (3, "e5m2"), (1, "fp16"), (6, "fp16x2"), (0, "fp32"))
-            if info_sw.steps_by_prec[i]),
-        "data": "synthetic (seeded Q diag(sigma) Q^T, geometric spectrum)",
-        "config": {"workload": (f"spd n={n} kappa={args.kappa:g} block={b} {args.precision}"
-                                f" ladder={args.ladder} eps'={args.eps_prime}"),
-                   "n": n, "kappa": args.kappa, "block": b, "rhs": 1, "tol": args.tol,
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   "l2": "inputs larger than L2 (A = %d MiB)" % (n * n * 4 // (1 << 20))},
-        "comparator_fp32_factor_ms": round(ms_32, 3),
-        "speedup_vs_fp32_factor": round(ms_32 / ms_sw, 3),
-        "iterations": {"switching": r_sw[-1].iterations, "fp32": r_32[-1].iterations},
-        "rel_residual": {"switching": r_sw[-1].rel_residual, "fp32": r_32[-1].rel_residual},
-        "backward_error": {"switching": r_sw[-1].backward_error, "fp32": r_32[-1].backward_error},
-        "step_precisions": {nm: info_sw.steps_by_prec[i]
-                            for i, nm in ((0, "fp32"), (1, "fp16"), (2, "e4m3"), (3, "e5m2"),
-                                          (4, "mxfp8"), (6, "fp16x2"))},
-        "phase_ms_switching_step": phases,
-        "phase_calls_switching_step": calls,
-        "e2e": {"value": round(e2e_ms, 3), "unit": "ms",
-                "h2d_bytes_per_step": int(e2e_h2d),
-                "d2h_bytes_per_step": int(n * 8)},
-        "gpu_launches": int(launches_sw),
-        "roofline": roof,
-        "clocks": clk.summary(),
-    }
-    if rank == 0 and not args.no_cpu_baseline:
-        result["cpu_baseline"] = cpu_baseline(args, A_host.numpy(), B_host.numpy(),
-                                              r_32[-1].iterations)
-    if pg:
-        pg.barrier()
-        pg.destroy_process_group()
-    return result if rank == 0 else None
+    return {"kernel": None, "bound": "hbm", "achieved": None, "peak": hbm,
+            "peak_kind": peak_kind, "unit": "GB/s", "frac": None, "traffic": None}
 
 
 # ---------------------------------------------------------------- CPU side
-def cpu_baseline(args, A: np.ndarray, b: np.ndarray, iters: int, budget_s: float = 20.0):
-    """Reference CPU path on a bounded sample: micro_cholesky (FP32,
-    unblocked, single thread) on the leading n_s x n_s block, extrapolated by
-    (n/n_s)^3, plus the measured cost of one FP64 PCG iteration at full n
-    (FP32 GEMV + FP32-factor triangular solves) times the FP32 path's GPU
-    iteration count."""
+def cpu_pcg(A32: np.ndarray, L32: np.ndarray, B: np.ndarray, tol: float, max_it: int):
+    """FP64 PCG (the reference's loop, src/mixed_cholesky.cu:143-217, stopped
+    on the true residual) on the host: operator A (FP32 values), M = L L^T with
+    the FP32 factor, x0 = M^-1 b.  Returns (iterations, max relative
+    residual)."""
+    from scipy.linalg import solve_triangular
+    A64 = A32.astype(np.float64)
+    L64 = np.tril(L32).astype(np.float64)
+
+    def prec(r):
+        y = solve_triangular(L64, r, lower=True, check_finite=False)
+        return solve_triangular(L64, y, lower=True, trans="T", check_finite=False)
+
+    B = np.asarray(B, dtype=np.float64).reshape(A32.shape[0], -1)
+    nb = np.linalg.norm(B, axis=0)
+    x = prec(B)
+    r = B - A64 @ x
+    it = 0
+    if np.any(np.linalg.norm(r, axis=0) > tol * nb):
+        z = prec(r)
+        p = z.copy()
+        rho = np.sum(r * z, axis=0)
+        while it < max_it:
+            Ap = A64 @ p
+            alpha = rho / np.sum(p * Ap, axis=0)
+            x += alpha * p
+            r -= alpha * Ap
+            it += 1
+            if np.all(np.linalg.norm(r, axis=0) <= tol * nb):
+                r = B - A64 @ x                   # confirm on the true residual
+                if np.all(np.linalg.norm(r, axis=0) <= tol * nb):
+                    break
+            z = prec(r)
+            rho_new = np.sum(r * z, axis=0)
+            p = z + (rho_new / rho) * p
+            rho = rho_new
+    r = B - A64 @ x
+    return it, float(np.max(np.linalg.norm(r, axis=0) / nb))
+
+
+def cpu_baseline(args, A: np.ndarray, B: np.ndarray, iters: int):
+    """The reference's CPU path on a bounded sample (about 10-30 s of CPU
+    work): its micro_cholesky (src/micro_chol.hpp:14-44; FP32, unblocked, one
+    thread, built from the reference sources into oracle/_ref) on the leading
+    n_s x n_s block, scaled by (n/n_s)^3 -- a sample above the host caches, so
+    the scaling is close to measured full-size runs (the reference arm,
+    `--impl reference`, runs it at full n) -- plus the measured cost of one
+    FP64 PCG iteration at full n on the host (FP32 operator and factor, FP64
+    vectors, every rhs) times the FP32 arm's iteration count + 1.  Beside it,
+    the OpenMP blocked restatement of the same factorization on all host
+    cores, sampled and scaled the same way."""
     from oracle import oracle as O
+    import ctypes
 
     n = A.shape[0]
     kind = "reference" if O.REF_MICRO.exists() else "port"
-    ns = min(n, 1536)
+    ns = min(n, 4096)
     sub = np.array(A[:ns, :ns], dtype=np.float32, order="F")
     t0 = time.perf_counter()
-    if kind == "reference":
-        L, rc = O.ref_micro_cholesky(sub)
-    else:
-        L, rc = O.micro_cholesky(sub)
+    _, rc = O.ref_micro_cholesky(sub) if kind == "reference" else O.micro_cholesky(sub)
     t_sub = time.perf_counter() - t0
     t_factor = t_sub * (n / ns) ** 3
-    # one PCG iteration at full n: GEMV (n^2 FP32) + two triangular solves
+    t0 = time.perf_counter()
+    _, rc2 = O.chol_fp32_omp(sub, 256)
+    t_omp = time.perf_counter() - t0
+    cores = O.num_threads()
+    # one PCG iteration at full n for one rhs: GEMV + two triangular solves
     F = np.asfortranarray(A.astype(np.float32))
     lib = O.lib()
-    import ctypes
-    x = np.ascontiguousarray(b, dtype=np.float64)
+    x = np.ascontiguousarray(B.reshape(n, -1)[:, 0], dtype=np.float64)
     y = np.zeros(n)
     dp = ctypes.POINTER(ctypes.c_double)
+    fp = ctypes.POINTER(ctypes.c_float)
     t0 = time.perf_counter()
-    lib.orc_gemv_f32_f64(F.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), n, n,
-                         x.ctypes.data_as(dp), y.ctypes.data_as(dp))
-    lib.orc_potrs_f32_f64(F.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), n, n,
-                          x.ctypes.data_as(dp), y.ctypes.data_as(dp))
-    t_it = time.perf_counter() - t0
+    lib.orc_gemv_f32_f64(F.ctypes.data_as(fp), n, n, x.ctypes.data_as(dp), y.ctypes.data_as(dp))
+    lib.orc_potrs_f32_f64(F.ctypes.data_as(fp), n, n, x.ctypes.data_as(dp), y.ctypes.data_as(dp))
+    t_it = (time.perf_counter() - t0) * args.rhs
     total_ms = (t_factor + (iters + 1) * t_it) * 1e3
+    omp_ms = (t_omp * (n / ns) ** 3 + (iters + 1) * t_it) * 1e3
     return {"value": round(total_ms, 1), "unit": "ms", "cores": 1, "kind": kind,
-            "sample": (f"micro_cholesky on the leading {ns}x{ns} block ({t_sub:.2f} s) "
-                       f"extrapolated by (n/{ns})^3 to n={n}, plus {iters + 1} x one measured "
-                       f"FP64 PCG iteration at full n ({t_it * 1e3:.0f} ms)")}
+            "sample": (f"micro_cholesky on the leading {ns}x{ns} block ({t_sub:.2f} s, rc {rc}) "
+                       f"scaled by (n/{ns})^3 to n={n}, plus {iters + 1} x one measured FP64 PCG "
+                       f"iteration at full n for {args.rhs} rhs ({t_it * 1e3:.0f} ms)"),
+            "omp_port": {"value": round(omp_ms, 1), "unit": "ms", "cores": cores, "kind": "port",
+                         "sample": (f"OpenMP blocked FP32 restatement (block 256) on the same "
+                                    f"{ns}x{ns} block ({t_omp:.2f} s on {cores} threads, rc "
+                                    f"{rc2}) scaled by (n/{ns})^3, plus the same PCG cost")}}
 
 
 def run_reference(args, world, rank):
+    """The reference's own CPU path at the full workload: micro_cholesky
+    (src/micro_chol.hpp:14-44, built from the reference sources into
+    oracle/_ref; one thread, as written) factors the full FP32 matrix, then
+    FP64 PCG with that factor runs to the tolerance on the host.  One full
+    solve takes minutes, so the arm runs one step (no warm-up) whatever
+    --steps asks and says so; the value is that step's measured time."""
     if rank != 0:
         return None
+    import torch
+    from oracle import oracle as O
     from cholesky_gpu_b200 import matgen
     n = args.n
-    A = matgen.spd_matrix(n, args.kappa, 3).numpy()
-    b = matgen.rhs(n, 1, 100).numpy()
-    vals = []
-    for _ in range(max(1, args.steps)):
-        cb = cpu_baseline(args, A, b, iters=8)
-        vals.append(cb["value"])
-    v = statistics.median(vals)
-    cb["value"] = v
+    t_gen = time.perf_counter()
+    if args.workload == "rbf":
+        X = torch.from_numpy(matgen.mnist_like_points(n, 784, 4))
+        ell = matgen.median_pairwise_distance(X)
+        A = matgen.rbf_matrix(X, ell, 1e-3).numpy()
+        del X
+        B = matgen.rhs(n, args.rhs, 5).numpy().reshape(n, -1)
+        workload = (f"rbf n={n} d=784 zeros=0.8 l=median({ell:.4f}) nugget=1e-3 rhs={args.rhs} "
+                    f"(host micro_cholesky + FP64 PCG)")
+        data = "synthetic (seeded sparse points in [0,1]^784 standing in for image data; RBF kernel)"
+    else:
+        A = matgen.spd_matrix(n, args.kappa, 3).numpy()
+        B = matgen.rhs(n, args.rhs, 100).numpy().reshape(n, -1)
+        workload = f"spd n={n} kappa={args.kappa:g} rhs={args.rhs} (host micro_cholesky + FP64 PCG)"
+        data = "synthetic (seeded Q diag(sigma) Q^T, geometric spectrum)"
+    t_gen = time.perf_counter() - t_gen
+    kind = "reference" if O.REF_MICRO.exists() else "port"
+    t0 = time.perf_counter()
+    L, rc = O.ref_micro_cholesky(A) if kind == "reference" else O.micro_cholesky(A)
+    t_fac = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    its, rel = cpu_pcg(A, L, B, args.tol, args.max_it) if rc == 0 else (0, float("nan"))
+    t_pcg = time.perf_counter() - t0
+    v = (t_fac + t_pcg) * 1e3
+    cb = {"value": round(v, 1), "unit": "ms", "cores": 1, "kind": kind,
+          "sample": (f"the full workload, one step: micro_cholesky at n={n} ({t_fac:.1f} s, rc {rc}) "
+                     f"+ host FP64 PCG to {args.tol:g} ({its} iterations, {t_pcg:.1f} s, "
+                     f"rel residual {rel:.1e})")}
     return {
-        "impl": "reference", "metric": METRIC, "value": v, "unit": "ms", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "fp32 factor, fp64 pcg",
-        "data": "synthetic (seeded Q diag(sigma) Q^T, geometric spectrum)",
-        "config": {"workload": f"spd n={n} kappa={args.kappa:g} block={args.block} (CPU micro_cholesky)",
-                   "n": n, "kappa": args.kappa},
+        "impl": "reference", "metric": METRIC, "value": round(v, 1), "unit": "ms",
+        "n_gpus": world, "steps": 1, "warmup": 0, "steps_requested": args.steps,
+        "warmup_requested": args.warmup,
+        "note": ("one full-size step: the reference's single-threaded micro_cholesky takes "
+                 "minutes at this n, so the arm measures one solve instead of extrapolating"),
+        "ms_per_step": round(v, 1), "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "fp32 factor, fp64 pcg", "data": data,
+        "config": {"workload": workload, "n": n, "rhs": args.rhs, "tol": args.tol,
+                   "input_generation_s": round(t_gen, 1)},
+        "iterations": its, "rel_residual": rel, "converged": bool(rel <= args.tol),
         "cpu_baseline": cb,
-        "e2e": {"value": v, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "e2e": {"value": round(v, 1), "unit": "ms", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
     }
 
 
@@ -535,54 +742,6 @@ def _base(args, world, value, unit, dtype, data, config, extra):
     return out
 
 
-def run_rbf(args, world, rank, local):
-    """Gaussian RBF kernel matrix: n = 16384 points, 80 % zero coordinates,
-    the rest U(0,1) in [0,1]^784 (seeded stand-in for image data);
-    l = exact median pairwise distance; nugget 1e-3; 8 rhs.  One step =
-    factor + PCG to the tolerance (the kernel-matrix build is timed apart)."""
-    import torch
-    import cholesky_gpu_b200 as mp
-    from cholesky_gpu_b200 import autograd as AG, matgen
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    n = args.n if args.n != 8192 else 16384
-    X = torch.from_numpy(matgen.mnist_like_points(n, 784, 4 + rank)).to(dev)
-    ell = matgen.median_pairwise_distance(X)
-    stream = torch.cuda.current_stream(dev)
-    t_build, (_, K32) = _timed(lambda: AG.rbf_build(X, ell, 1e-3, fp64=False), 1, 1, stream)
-    B = matgen.rhs(n, 8, 5 + rank, device=dev)
-    prec = args.precision
-    mixed = dict(block_size=args.block, precision=prec)
-    if prec == "switching":
-        # MXFP8 first: the criterion keeps it only where the Schur diagonal allows
-        mixed.update(eps_prime=args.eps_prime, ladder=["mxfp8", "fp16", "fp16x2"])
-    arms = {prec: mp.Factor(n, **mixed),
-            "fp32": mp.Factor(n, block_size=args.block, precision="fp32")}
-    res = {}
-    for name, f in arms.items():
-        def step(f=f):
-            f.compute(K32)
-            return f.pcg(K32, B, rel_tol=args.tol, max_it=args.max_it, check_every=args.check_every)
-        ms, (X_, rep) = _timed(step, args.steps, args.warmup, stream)
-        res[name] = (ms, rep, _phases(step))
-    ms, rep, _ = res[prec]
-    info = arms[prec].info()
-    steps_used = {nm: info.steps_by_prec[i] for i, nm in
-                  ((0, "fp32"), (1, "fp16"), (2, "e4m3"), (3, "e5m2"), (4, "mxfp8"), (6, "fp16x2"))
-                  if info.steps_by_prec[i]}
-    return _base(args, world, ms, "ms", f"{'/'.join(steps_used) or prec} factor, fp64 pcg",
-                 "synthetic (seeded sparse points in [0,1]^784, RBF kernel)",
-                 {"workload": f"rbf n={n} d=784 l=median({ell:.3f}) nugget=1e-3 rhs=8 {prec}",
-                  "n": n, "block": args.block, "rhs": 8, "tol": args.tol},
-                 {"comparator_fp32_factor_ms": round(res["fp32"][0], 3),
-                  "speedup_vs_fp32_factor": round(res["fp32"][0] / ms, 3),
-                  "iterations": {k: v[1].iterations for k, v in res.items()},
-                  "converged": {k: v[1].converged for k, v in res.items()},
-                  "rel_residual": {k: v[1].rel_residual for k, v in res.items()},
-                  "kernel_build_ms": round(t_build, 3), "step_precisions": steps_used,
-                  "phase_ms": {k: v[2] for k, v in res.items()}})
-
-
 def run_rbf_grad(args, world, rank, local):
     """Differentiation workload: RBF kernel, n = 8192 points x ~ N(0, I_64),
     l = 4, nugget 1e-2, y ~ N(0,1); one step = forward solve + backward
@@ -591,7 +750,7 @@ def run_rbf_grad(args, world, rank, local):
     from cholesky_gpu_b200 import autograd as AG, matgen
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    n = args.n if args.n != 8192 else 8192
+    n = args.n
     X0 = torch.from_numpy(matgen.gaussian_points(n, 64, 6 + rank)).to(dev)
     y = torch.from_numpy(np.random.default_rng(7 + rank).standard_normal(n)).to(dev)
     stream = torch.cuda.current_stream(dev)
@@ -682,8 +841,6 @@ def main():
     world, rank, local = dist_init(args)
     if args.impl == "reference":
         out = run_reference(args, world, rank)
-    elif args.workload == "rbf":
-        out = run_rbf(args, world, rank, local)
     elif args.workload == "rbf-grad":
         out = run_rbf_grad(args, world, rank, local)
     elif args.workload == "batch":
