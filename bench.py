@@ -73,6 +73,10 @@ def parse():
     ap.add_argument("--max-it", type=int, default=400)
     ap.add_argument("--check-every", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tune", action="store_true",
+                    help="batch workload: re-run the autotuner on this GPU and write its table")
+    ap.add_argument("--tune-out", default=None,
+                    help="where --tune writes the table (default: the package's tuned_batch.json)")
     args = ap.parse_args()
     w = WORKLOADS.get(args.workload, {})
     if args.n is None:
@@ -782,10 +786,12 @@ def run_rbf_grad(args, world, rank, local):
 
 def run_batch(args, world, rank, local):
     """512 SPD systems, n_i ~ U[64, 2048], kappa_i log-uniform in [1e2, 1e6]
-    (seeded), 4 rhs each; one step = batched factor + lockstep PCG of all."""
+    (seeded), 4 rhs each; one step = batched factor + lockstep PCG of all,
+    run by the plan the autotuner's table gives for this batch shape
+    (cholesky_gpu_b200/tuned_batch.json; --tune re-measures it on this GPU
+    and rewrites the table)."""
     import torch
-    import cholesky_gpu_b200 as mp
-    from cholesky_gpu_b200 import matgen
+    from cholesky_gpu_b200 import matgen, tune
     from cholesky_gpu_b200.shard import gather_by_system, max_over_ranks, partition_systems
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -794,26 +800,55 @@ def run_batch(args, world, rank, local):
         import torch.distributed as dist
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-    count = 512
+    count, nrhs = 512, 4
     # the same 512 systems for every world size; each rank owns a shard (no
     # data-path collective: systems are independent)
     ns_all = [int(v) for v in matgen.batch_sizes(count, 64, 2048, 8)]
     ks = matgen.batch_kappas(count, 1e2, 1e6, 9)
+    tuned = None
+    if args.tune and rank == 0:
+        tuned = tune.tune(ns_all, nrhs=nrhs, table=tune.load_table(),
+                          log=lambda m: print(m, file=sys.stderr, flush=True))
+        tune.save_table(tuned, args.tune_out)
+    table = tuned if tuned is not None else tune.load_table()
+    plan = tune.plan_for(ns_all, nrhs, table)
+    if args.precision != "switching":    # an explicit format overrides the table
+        plan = {"mode": "whole", "config": {"block_size": 128, "precision": args.precision}}
     mine = partition_systems(ns_all, world)[rank]
     ns = [ns_all[i] for i in mine]
     As = [matgen.spd_matrix(ns_all[i], float(ks[i]), i, device=dev) for i in mine]
-    Bs = [matgen.rhs(ns_all[i], 4, 7000 + i, device=dev) for i in mine]
+    Bs = [matgen.rhs(ns_all[i], nrhs, 7000 + i, device=dev) for i in mine]
     stream = torch.cuda.current_stream(dev)
-    prec = args.precision if args.precision != "switching" else "fp16x2"
-    bt = mp.Batch(ns, nrhs=4, block_size=128, precision=prec)
+    bt = tune.TunedBatch(ns, nrhs=nrhs, plan=plan)
 
     def step():
         if dist is not None:
             dist.barrier()
         bt.factor(As)
         return bt.pcg(As, Bs, rel_tol=args.tol, max_it=args.max_it, check_every=args.check_every)
-    ms, (Xs, reps, st) = _timed(step, args.steps, args.warmup, stream)
+    launches0 = _lib_launches()
+    with ClockSampler(local, pci_bus_id(torch, local)) as clk:
+        ms, (Xs, reps, st) = _timed(step, args.steps, args.warmup, stream)
+    launches = (_lib_launches() - launches0) // max(1, args.steps + args.warmup)
     ms = max_over_ranks(ms, dist)
+    # end to end: the systems and rhs in page-locked host memory, copied in,
+    # factored and solved, the solutions copied back, every step
+    Ah = [a.cpu().pin_memory() for a in As]
+    Bh = [b.cpu().pin_memory() for b in Bs]
+    Xh = [torch.empty(b.shape, dtype=torch.float64).pin_memory() for b in Bs]
+
+    def step_e2e():
+        for a, ah in zip(As, Ah):
+            a.copy_(ah, non_blocking=True)
+        for b, bh in zip(Bs, Bh):
+            b.copy_(bh, non_blocking=True)
+        X, R, S = step()
+        for xh, x in zip(Xh, X):
+            xh.copy_(x, non_blocking=True)
+        return X, R, S
+    ms_e2e, _ = _timed(step_e2e, max(2, min(args.steps, 4)), 1, stream)
+    ms_e2e = max_over_ranks(ms_e2e, dist)
+    h2d = sum(n * n * 4 + n * nrhs * 8 for n in ns)
     allrep = gather_by_system({i: (r.iterations, r.converged) for i, r in zip(mine, reps)},
                               count, dist)
     if dist is not None:
@@ -823,17 +858,56 @@ def run_batch(args, world, rank, local):
         return None
     its = [r[0] for r in allrep]
     flops = sum(n ** 3 / 3.0 for n in ns_all)
-    return _base(args, world, ms, "ms", f"{prec} factor, fp64 pcg",
-                 "synthetic (seeded Q diag(sigma) Q^T per system)",
-                 {"workload": f"batch 512 systems n~U[64,2048] kappa~logU[1e2,1e6] rhs=4 {prec}",
-                  "systems": count, "block": 128, "rhs": 4, "tol": args.tol,
-                  "parallelism": f"systems sharded over {world} GPUs" if world > 1 else "single GPU"},
-                 {"scaling": "strong",
-                  "solves_per_s": round(count / (ms * 1e-3), 1),
-                  "ms_per_system": round(ms / count, 4),
-                  "all_converged": all(r[1] for r in allrep),
-                  "iterations": {"max": max(its), "median": statistics.median(its)},
-                  "factor_tflops_equiv": round(flops / (ms * 1e-3) / 1e12, 2)})
+    out = _base(args, world, ms, "ms", "tuned batch factor, fp64 pcg",
+                "synthetic (seeded Q diag(sigma) Q^T per system)",
+                {"workload": f"batch 512 systems n~U[64,2048] kappa~logU[1e2,1e6] rhs=4",
+                 "systems": count, "rhs": nrhs, "tol": args.tol, "plan": plan,
+                 "parallelism": f"systems sharded over {world} GPUs" if world > 1 else "single GPU"},
+                {"scaling": "strong",
+                 "solves_per_s": round(count / (ms * 1e-3), 1),
+                 "ms_per_system": round(ms / count, 4),
+                 "all_converged": all(r[1] for r in allrep),
+                 "iterations": {"max": max(its), "median": statistics.median(its)},
+                 "factor_tflops_equiv": round(flops / (ms * 1e-3) / 1e12, 2),
+                 "e2e": {"value": round(ms_e2e, 3), "unit": "ms", "h2d_bytes_per_step": int(h2d),
+                         "d2h_bytes_per_step": int(sum(n * nrhs * 8 for n in ns))},
+                 "gpu_launches": int(launches),
+                 "clocks": clk.summary()})
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = batch_cpu_baseline(args, As, Bs, ns_all)
+    return out
+
+
+def _lib_launches():
+    from cholesky_gpu_b200 import _lib
+    return _lib.load().mpchol_kernel_launches()
+
+
+def batch_cpu_baseline(args, As, Bs, ns_all, budget_s: float = 15.0):
+    """The reference's CPU path (micro_cholesky + host FP64 PCG, one thread)
+    on a seeded sample of the batch's systems until about budget_s of work,
+    scaled to all 512 by the sample's share of sum n^3."""
+    from oracle import oracle as O
+    kind = "reference" if O.REF_MICRO.exists() else "port"
+    order = np.random.default_rng(1).permutation(len(As))
+    t_tot, done, cube = 0.0, 0, 0.0
+    for i in order:
+        A = As[i].cpu().numpy()
+        B = Bs[i].cpu().numpy()
+        t0 = time.perf_counter()
+        L, rc = O.ref_micro_cholesky(A) if kind == "reference" else O.micro_cholesky(A)
+        if rc == 0:
+            cpu_pcg(A, L, B, args.tol, args.max_it)
+        t_tot += time.perf_counter() - t0
+        done += 1
+        cube += float(A.shape[0]) ** 3
+        if t_tot > budget_s:
+            break
+    total = sum(float(n) ** 3 for n in ns_all)
+    v = t_tot * total / cube * 1e3
+    return {"value": round(v, 1), "unit": "ms", "cores": 1, "kind": kind,
+            "sample": (f"micro_cholesky + host FP64 PCG on {done} of the 512 systems "
+                       f"({t_tot:.1f} s), scaled by sum n^3")}
 
 
 def main():

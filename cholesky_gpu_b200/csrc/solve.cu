@@ -340,11 +340,124 @@ __device__ __forceinline__ void tile_pass_staged(const float* Ts, const double* 
   }
 }
 
+// ---- eight right-hand sides on the FP64 tensor cores ---------------------
+// With 8 rhs the tile passes are FP64-FMA bound (16 FMAs per tile element for
+// the symmetric product), so they run as mma.sync m8n8k4 FP64 (DMMA): a warp
+// owns 16 rows of the tile for the row sums and 16 columns for the column
+// sums, and its accumulator fragments hold finished 8 x 8 (rows x rhs)
+// blocks -- no butterflies and no cross-warp reduction.  Fragments follow the
+// PTX ISA for m8n8k4.f64: a = A[lane / 4][lane % 4], b = B[lane % 4][lane / 4],
+// d[i] = D[lane / 4][2 (lane % 4) + i].
+//
+// The tile is staged in a blocked layout in which both fragment patterns
+// read 32 distinct banks: 4-row x 8-column blocks of 32 floats (column-major
+// inside a block, so a 16-byte copy of 4 rows of one column lands contiguous),
+// 16 blocks per 4-row group, and the groups 528 floats apart (16 banks of
+// stagger between neighbouring groups).  Vector segments are staged k-major
+// with a row of XS = 132 doubles per rhs.
+constexpr int BL_RG = 16 * 32 + 16;          // floats per 4-row group
+constexpr int BL_TILE = (RB / 4) * BL_RG;    // floats per blocked tile
+constexpr int XS = RB + 4;                   // doubles per rhs in a staged segment
+
+__device__ __forceinline__ int bl_off(int r, int c) {
+  return (r >> 2) * BL_RG + (c >> 3) * 32 + (c & 7) * 4 + (r & 3);
+}
+
+__device__ __forceinline__ void dmma_m8n8k4(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
+// stage_tile into the blocked layout
+__device__ __forceinline__ void stage_tile_bl(float* dst, const float* T, int ld, int rows_valid,
+                                              int cols_valid) {
+#pragma unroll 4
+  for (int e = threadIdx.x; e < TILE_ELEMS / 4; e += NTH) {
+    const int c = e / (RB / 4), r = 4 * (e % (RB / 4));
+    const bool ok = c < cols_valid && r < rows_valid;
+    cp_async16(dst + bl_off(r, c), ok ? T + (size_t)c * ld + r : T,
+               ok ? 4 * min(4, rows_valid - r) : 0);
+  }
+}
+
+// x[k * n + row0 + r] -> s[k * XS + r] (zero past nvalid), 8 rhs
+__device__ __forceinline__ void stage_vec_x8(const double* x, int n, int row0, int nvalid, double* s) {
+  for (int e = threadIdx.x; e < RB * 8; e += NTH) {
+    const int k = e / RB, r = e % RB;
+    const bool ok = r < nvalid;
+    cp_async8(s + k * XS + r, ok ? x + (size_t)k * n + row0 + r : x, ok ? 8 : 0);
+  }
+}
+// the same through L2 loads (the persistent solve's segments are produced by
+// other CTAs' atomics)
+__device__ __forceinline__ void load_vec_x8(const double* x, int n, int row0, int nvalid, double* s) {
+  for (int e = threadIdx.x; e < RB * 8; e += NTH) {
+    const int k = e / RB, r = e % RB;
+    s[k * XS + r] = (r < nvalid) ? __ldcg(x + (size_t)k * n + row0 + r) : 0.0;
+  }
+}
+
+// One blocked tile T (rows i0.., columns j0..) times 8 rhs on the DMMA pipe:
+//   do_nt: y_rows[row0 + r] += sign * sum_c T[r][c] x_c[c]   (rows < nrows)
+//   do_t : y_cols[col0 + c] += sign * sum_r T[r][c] x_r[r]   (columns < ncols)
+// by FP64 atomics.  DIAG (a diagonal tile of a symmetric operator stored
+// lower): the row sums keep r >= c, the column sums r > c.  FRO: adds the
+// tile's share of ||A||_F^2 (off-diagonal entries twice) to *fsq.
+template <bool DIAG, bool FRO>
+__device__ __forceinline__ void tile_mma_x8(const float* Ts, const double* x_c, const double* x_r,
+                                            double* y_rows, int row0, int nrows, double* y_cols,
+                                            int col0, int ncols, int n, bool do_nt, bool do_t,
+                                            double sign, double* fsq) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int B0 = 16 * warp;
+  double dn[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+  double dt[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll 4
+  for (int k0 = 0; k0 < RB; k0 += 4) {
+    if (do_nt) {
+      const double b = x_c[g * XS + k0 + t];
+#pragma unroll
+      for (int mb = 0; mb < 2; ++mb) {
+        const int r = B0 + 8 * mb + g, c = k0 + t;
+        float v = Ts[bl_off(r, c)];
+        if (DIAG && r < c) v = 0.0f;
+        const double a = (double)v;
+        if (FRO) *fsq = fma((DIAG && r == c) ? a : 2.0 * a, a, *fsq);
+        dmma_m8n8k4(dn[mb], a, b);
+      }
+    }
+    if (do_t) {
+      const double b = x_r[g * XS + k0 + t];
+#pragma unroll
+      for (int mb = 0; mb < 2; ++mb) {
+        const int c = B0 + 8 * mb + g, r = k0 + t;
+        float v = Ts[bl_off(r, c)];
+        if (DIAG && r <= c) v = 0.0f;
+        dmma_m8n8k4(dt[mb], (double)v, b);
+      }
+    }
+  }
+#pragma unroll
+  for (int mb = 0; mb < 2; ++mb) {
+    const int idx = B0 + 8 * mb + g;
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const int k = 2 * t + i;
+      if (do_nt && idx < nrows) atomicAdd(&y_rows[(size_t)k * n + row0 + idx], sign * dn[mb][i]);
+      if (do_t && idx < ncols) atomicAdd(&y_cols[(size_t)k * n + col0 + idx], sign * dt[mb][i]);
+    }
+  }
+}
+
 // Shared memory of the staged SYMV: STAGES x (tile + x_J + x_I) + column sums.
 template <int NR>
 constexpr int symv_stages() { return NR >= 8 ? 2 : 3; }
 template <int NR>
 constexpr size_t symv_staged_smem() {
+  if (NR == 8)   // blocked tiles and padded segments, no column-sum buffer
+    return (size_t)symv_stages<NR>() * (BL_TILE * sizeof(float) + 2 * (size_t)XS * 8 * sizeof(double));
   return (size_t)symv_stages<NR>() * (TILE_ELEMS * sizeof(float) + 2 * RB * NR * sizeof(double)) +
          (size_t)RB * NR * sizeof(double);
 }
@@ -361,10 +474,12 @@ symv_staged_kernel(const float* __restrict__ A, int lda, int n, const double* __
                    double* __restrict__ y, const int* skip, double* fro, int nfro) {
   if (skip != nullptr && *skip) return;
   constexpr int STAGES = symv_stages<NR>();
-  constexpr int VEC = RB * NR;
+  constexpr bool MMA = NR == 8;
+  constexpr int TE = MMA ? BL_TILE : TILE_ELEMS;      // floats per staged tile
+  constexpr int VEC = MMA ? XS * 8 : RB * NR;         // doubles per staged segment
   extern __shared__ __align__(16) unsigned char sm_raw[];
   float* tiles = reinterpret_cast<float*>(sm_raw);
-  double* vecs = reinterpret_cast<double*>(tiles + STAGES * TILE_ELEMS);   // [stage][xJ, xI]
+  double* vecs = reinterpret_cast<double*>(tiles + STAGES * TE);   // [stage][xJ, xI]
   double* s_col = vecs + STAGES * 2 * VEC;
   const int T = ceil_div(n, RB);
   const int ntiles = T * (T + 1) / 2;
@@ -373,9 +488,15 @@ symv_staged_kernel(const float* __restrict__ A, int lda, int n, const double* __
     tri_of(t, I, J);
     const int i0 = I * RB, j0 = J * RB;
     const int ni = min(RB, n - i0), nj = min(RB, n - j0);
-    stage_tile(tiles + stage * TILE_ELEMS, A + (size_t)j0 * lda + i0, lda, ni, nj);
-    stage_vec<NR>(x, n, j0, nj, vecs + (2 * stage) * VEC);
-    stage_vec<NR>(x, n, i0, ni, vecs + (2 * stage + 1) * VEC);
+    if (MMA) {
+      stage_tile_bl(tiles + stage * TE, A + (size_t)j0 * lda + i0, lda, ni, nj);
+      stage_vec_x8(x, n, j0, nj, vecs + (2 * stage) * VEC);
+      stage_vec_x8(x, n, i0, ni, vecs + (2 * stage + 1) * VEC);
+    } else {
+      stage_tile(tiles + stage * TE, A + (size_t)j0 * lda + i0, lda, ni, nj);
+      stage_vec<NR>(x, n, j0, nj, vecs + (2 * stage) * VEC);
+      stage_vec<NR>(x, n, i0, ni, vecs + (2 * stage + 1) * VEC);
+    }
   };
 #pragma unroll
   for (int s = 0; s < STAGES - 1; ++s) {
@@ -397,9 +518,22 @@ symv_staged_kernel(const float* __restrict__ A, int lda, int n, const double* __
     tri_of(t, I, J);
     const int i0 = I * RB, j0 = J * RB;
     const int ni = min(RB, n - i0), nj = min(RB, n - j0);
-    float* Ts = tiles + stage * TILE_ELEMS;
+    float* Ts = tiles + stage * TE;
     const double* xJ = vecs + (2 * stage) * VEC;
     const double* xI = xJ + VEC;
+    if (MMA) {
+      // row sums to y_I, column sums to y_J, straight from the fragments
+      if (fro != nullptr) {
+        if (I == J) tile_mma_x8<true, true>(Ts, xJ, xI, y, i0, ni, y, j0, nj, n, true, true, 1.0, &fsq);
+        else tile_mma_x8<false, true>(Ts, xJ, xI, y, i0, ni, y, j0, nj, n, true, true, 1.0, &fsq);
+      } else {
+        if (I == J) tile_mma_x8<true, false>(Ts, xJ, xI, y, i0, ni, y, j0, nj, n, true, true, 1.0, nullptr);
+        else tile_mma_x8<false, false>(Ts, xJ, xI, y, i0, ni, y, j0, nj, n, true, true, 1.0, nullptr);
+      }
+      __syncthreads();   // the stage is free again
+      stage = (stage + 1) % STAGES;
+      continue;
+    }
     double acc[4][NR] = {};
     if (fro != nullptr) {
       if (I == J) tile_pass_staged<NR, true, true>(Ts, xJ, xI, acc, s_col, true, true, &fsq);
@@ -907,7 +1041,16 @@ __device__ __forceinline__ bool trsv_job(int u, const float* L, int ldl, int n, 
 
 template <int NR>
 constexpr size_t trsv_staged_smem() {
+  if (NR == 8) return (size_t)BL_TILE * sizeof(float) + (size_t)XS * 8 * sizeof(double);
   return (size_t)TILE_ELEMS * sizeof(float) + 2 * (size_t)RB * NR * sizeof(double);
+}
+size_t trsv_smem_bytes(int nrhs) {
+  switch (nrhs) {
+    case 1: return trsv_staged_smem<1>();
+    case 2: return trsv_staged_smem<2>();
+    case 4: return trsv_staged_smem<4>();
+    default: return trsv_staged_smem<8>();
+  }
 }
 
 // Two CTAs per SM, each with one tile stage: a unit's tile copy is issued
@@ -924,9 +1067,10 @@ trsv_persistent_kernel(const float* __restrict__ L, int ldl, int n, const float*
                        double* __restrict__ work, double* __restrict__ out, int* ctr,
                        const int* skip, DevStatus* st) {
   if (skip != nullptr && *skip) return;
+  constexpr bool MMA = NR == 8;
   extern __shared__ __align__(16) unsigned char sm_raw[];
   float* Ts = reinterpret_cast<float*>(sm_raw);                           // one stage
-  double* s_v = reinterpret_cast<double*>(Ts + TILE_ELEMS);               // RB x NR
+  double* s_v = reinterpret_cast<double*>(Ts + (MMA ? BL_TILE : TILE_ELEMS));   // RB x NR
   double* s_col = s_v + RB * NR;                                          // RB x NR
   __shared__ int s_unit[2];
   int* next = ctr;
@@ -938,13 +1082,26 @@ trsv_persistent_kernel(const float* __restrict__ L, int ldl, int n, const float*
   TrsvJob cur;
   bool have = trsv_job<TRANS>(ucur, L, ldl, n, wsup, seg_in, seg_out, cur);
   for (int it = 1; have; ++it) {
-    stage_tile(Ts, cur.T, cur.ld, cur.nrow, cur.ncol);
+    if (MMA) stage_tile_bl(Ts, cur.T, cur.ld, cur.nrow, cur.ncol);
+    else stage_tile(Ts, cur.T, cur.ld, cur.nrow, cur.ncol);
     cp_async_commit();
     // the next unit number, taken by a thread of warp 1 so that its round
     // trip overlaps warp 0's dependency poll; read after this unit's
     // barriers (s_unit[it & 1] is not read again before its next write)
     if (threadIdx.x == 32) s_unit[it & 1] = atomicAdd(next, 1);
     wait_count(cur.wait_ctr, cur.wait_need, st, ucur);
+    if (MMA) {
+      load_vec_x8(cur.panel ? out : work, n, cur.vin_row0, cur.vin_n, s_v);
+      cp_async_wait<0>();
+      __syncthreads();
+      double* dst = cur.panel ? work : out;
+      tile_mma_x8<false, false>(Ts, s_v, s_v, dst, cur.out_row0, cur.out_n, dst, cur.out_row0,
+                                cur.out_n, n, cur.nt, !cur.nt, cur.panel ? -1.0 : 1.0, nullptr);
+      signal_count(cur.sig_ctr);   // its barrier also frees the stage and s_v
+      ucur = s_unit[it & 1];
+      have = trsv_job<TRANS>(ucur, L, ldl, n, wsup, seg_in, seg_out, cur);
+      continue;
+    }
     load_vec<NR>(cur.panel ? out : work, n, cur.vin_row0, cur.vin_n, s_v);
     cp_async_wait<0>();
     __syncthreads();
@@ -1257,7 +1414,7 @@ cudaError_t launch_trsv_persistent(bool backward, const float* L, int ldl, int n
   if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
   const int nri = nrhs == 1 ? 0 : nrhs == 2 ? 1 : nrhs == 4 ? 2 : 3;
   int& grid = grid_cache[dev & 63][backward ? 1 : 0][nri];
-  const size_t smem = (size_t)TILE_ELEMS * sizeof(float) + 2 * (size_t)RB * nrhs * sizeof(double);
+  const size_t smem = trsv_smem_bytes(nrhs);
   auto launch = [&](auto kernel) -> cudaError_t {
     if (grid == 0) {
       int per_sm = 0, nsm = 0;

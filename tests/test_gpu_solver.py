@@ -117,6 +117,21 @@ def test_apply_precond_matches_oracle_potrs(cuda):
     assert abs(v @ Mu - u @ Mv) <= 1e-10 * abs(v @ Mu)
 
 
+@pytest.mark.parametrize("n,nrhs", [(2100, 8), (1024, 8)])
+def test_apply_precond_8_rhs_matches_oracle_potrs(cuda, n, nrhs):
+    """The triangular solves with 8 right-hand sides (the FP64 tensor-core
+    tile pass of the persistent solve), ragged super-blocks included."""
+    A = matgen.spd_matrix(n, 1e4, 12).numpy()
+    f = mp.factor(torch.from_numpy(A).cuda(), block_size=256, precision="fp16x2")
+    L = f.lower().cpu().numpy()
+    R = np.random.default_rng(3).standard_normal((n, nrhs))
+    Z = f.apply_precond(torch.from_numpy(R).cuda()).cpu().numpy()
+    want = O.potrs(L, R)
+    err = np.abs(Z - want).max() / np.abs(want).max()
+    print(f"apply_precond n={n} nrhs={nrhs} rel err {err:.2e}")
+    assert err < 1e-5
+
+
 @pytest.mark.parametrize("n,b,prec,kappa,nrhs", [
     (1024, 128, "fp16", 1e4, 1),     # plain-method workload
     (1024, 128, "fp32", 1e4, 2),
