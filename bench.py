@@ -53,12 +53,13 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mpchol", choices=["mpchol", "reference"])
-    ap.add_argument("--workload", default="rbf", choices=["rbf", "spd", "rbf-grad", "batch"],
+    ap.add_argument("--workload", default="rbf", choices=["rbf", "spd", "rbf-grad", "batch", "syrk"],
                     help="rbf (default): Gaussian RBF kernel matrix, n=16384 points in [0,1]^784 "
                          "with 80%% zero coordinates, nugget 1e-3, 8 rhs, MXFP8 switching ladder; "
                          "spd: n=8192 Q diag(sigma) Q^T, kappa=1e6, 1 rhs; rbf-grad: forward + "
                          "adjoint gradients of 1/2 y^T K^-1 y, n=8192, d=64; batch: 512 SPD "
-                         "systems of order U[64, 2048]")
+                         "systems of order U[64, 2048]; syrk: trailing-update microbenchmark "
+                         "against cuBLASLt MXFP8")
     ap.add_argument("--n", type=int, default=None)
     ap.add_argument("--rhs", type=int, default=None)
     ap.add_argument("--kappa", type=float, default=1e6)
@@ -826,10 +827,8 @@ def run_batch(args, world, rank, local):
             dist.barrier()
         bt.factor(As)
         return bt.pcg(As, Bs, rel_tol=args.tol, max_it=args.max_it, check_every=args.check_every)
-    launches0 = _lib_launches()
     with ClockSampler(local, pci_bus_id(torch, local)) as clk:
         ms, (Xs, reps, st) = _timed(step, args.steps, args.warmup, stream)
-    launches = (_lib_launches() - launches0) // max(1, args.steps + args.warmup)
     ms = max_over_ranks(ms, dist)
     # end to end: the systems and rhs in page-locked host memory, copied in,
     # factored and solved, the solutions copied back, every step
@@ -871,16 +870,10 @@ def run_batch(args, world, rank, local):
                  "factor_tflops_equiv": round(flops / (ms * 1e-3) / 1e12, 2),
                  "e2e": {"value": round(ms_e2e, 3), "unit": "ms", "h2d_bytes_per_step": int(h2d),
                          "d2h_bytes_per_step": int(sum(n * nrhs * 8 for n in ns))},
-                 "gpu_launches": int(launches),
                  "clocks": clk.summary()})
     if not args.no_cpu_baseline:
         out["cpu_baseline"] = batch_cpu_baseline(args, As, Bs, ns_all)
     return out
-
-
-def _lib_launches():
-    from cholesky_gpu_b200 import _lib
-    return _lib.load().mpchol_kernel_launches()
 
 
 def batch_cpu_baseline(args, As, Bs, ns_all, budget_s: float = 15.0):
@@ -910,6 +903,120 @@ def batch_cpu_baseline(args, As, Bs, ns_all, budget_s: float = 15.0):
                        f"({t_tot:.1f} s), scaled by sum n^3")}
 
 
+def run_syrk(args, world, rank, local):
+    """Trailing-update microbenchmark on the RBF workload's shapes (n = 16384):
+    C (m x m FP32, lower 128-tiles) -= P P^T with m = n - b (the first step)
+    and m = n / 2, for panel widths k = b in {256, 512, 1024}, through
+    mpchol_syrk_update in each tensor-core format, beside the reference's
+    sm_100 path for the same product -- cuBLASLt block-scaled MXFP8 (E4M3 with
+    one E8M0 scale per 32 along K, the reference's LtMxfp8Matmul) reached
+    through torch's scaled_mm -- and cuBLAS bf16.  The library GEMMs compute
+    the full m x m product into a new FP32 matrix (2 m^2 k flops, no C read);
+    the SYRK updates the lower triangle of C in place (m (m+1) k useful
+    flops, C read and written).  Codes are random valid values: the timing
+    does not depend on them."""
+    import torch
+    import torch.nn.functional as F
+    from cholesky_gpu_b200 import _lib
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    lib = _lib.load()
+    stream = torch.cuda.current_stream(dev)
+    hbm, bf16, peak_kind = measured_peaks()
+    n = 16384
+    g = torch.Generator(device=dev)
+    g.manual_seed(1)
+
+    def ev_time(fn, reps=5):
+        for _ in range(2):
+            fn()
+        ts = []
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return statistics.median(ts)
+
+    def codes8(m, k):
+        c = torch.randint(0, 0x7E, (m, k), dtype=torch.uint8, device=dev, generator=g)
+        sign = torch.randint(0, 2, (m, k), dtype=torch.uint8, device=dev, generator=g) << 7
+        return c | sign
+
+    rows = []
+    for k in (256, 512, 1024):
+        for m in (n - k, n // 2):
+            C = torch.zeros((m, m), dtype=torch.float32, device=dev)
+            ent = {"m": m, "k": k}
+            for fname, fmt in (("e4m3", _lib.PREC_E4M3), ("mxfp8", _lib.PREC_MXFP8),
+                               ("fp16", _lib.PREC_FP16), ("fp16x2", _lib.PREC_FP16X2)):
+                if fmt in (_lib.PREC_FP16, _lib.PREC_FP16X2):
+                    Q = (torch.randn((2 * m if fmt == _lib.PREC_FP16X2 else m, k), device=dev,
+                                     generator=g) * 0.1).half().view(torch.int16)
+                else:
+                    Q = codes8(m, k)
+                S = (torch.full((m, k // 32), 127, dtype=torch.uint8, device=dev)
+                     if fmt == _lib.PREC_MXFP8 else torch.zeros(m, dtype=torch.int8, device=dev))
+                st = lib.mpchol_syrk_update(C.data_ptr(), m, m, k, fmt, Q.data_ptr(), S.data_ptr(),
+                                            None, 0, stream.cuda_stream)
+                if st != 0:
+                    ent[fname] = {"status": st}
+                    continue
+                ms = ev_time(lambda: lib.mpchol_syrk_update(C.data_ptr(), m, m, k, fmt, Q.data_ptr(),
+                                                            S.data_ptr(), None, 0,
+                                                            stream.cuda_stream))
+                fl = float(m) * (m + 1) * k
+                byt = float(m) * (m + 1) / 2 * 8
+                mult = 3 if fmt == _lib.PREC_FP16X2 else 1
+                tpk = 2 * bf16 if fmt in (_lib.PREC_E4M3, _lib.PREC_MXFP8) else bf16
+                ent[fname] = {"ms": round(ms, 4), "useful_tflops": round(fl / ms / 1e9, 1),
+                              "issued_tflops": round(mult * fl / ms / 1e9, 1),
+                              "tensor_frac": round(mult * fl / ms / 1e9 / tpk, 4),
+                              "hbm_gbs": round(byt / ms / 1e6, 1),
+                              "hbm_frac": round(byt / ms / 1e6 / hbm, 4)}
+            del C
+            # the reference's path: cuBLASLt MXFP8 (block scales 1x32, E8M0), full GEMM
+            try:
+                a = codes8(m, k).view(torch.float8_e4m3fn)
+                bmat = codes8(m, k).view(torch.float8_e4m3fn)
+                rows_p = -(-m // 128) * 128
+                cols_p = -(-(k // 32) // 4) * 4
+                sa = torch.full((rows_p * cols_p,), 1.0, device=dev).to(torch.float8_e8m0fnu)
+                sb = torch.full((rows_p * cols_p,), 1.0, device=dev).to(torch.float8_e8m0fnu)
+
+                def lt():
+                    return F.scaled_mm(a, bmat.t(), sa, F.ScalingType.BlockWise1x32, sb,
+                                       F.ScalingType.BlockWise1x32,
+                                       swizzle_a=F.SwizzleType.SWIZZLE_32_4_4,
+                                       swizzle_b=F.SwizzleType.SWIZZLE_32_4_4,
+                                       output_dtype=torch.float32)
+                ms = ev_time(lt)
+                ent["cublaslt_mxfp8_gemm"] = {"ms": round(ms, 4),
+                                              "tflops": round(2.0 * m * m * k / ms / 1e9, 1),
+                                              "tensor_frac": round(2.0 * m * m * k / ms / 1e9 / (2 * bf16), 4)}
+            except Exception as e:      # noqa: BLE001 - record why the comparator did not run
+                ent["cublaslt_mxfp8_gemm"] = {"error": str(e).splitlines()[0][:200]}
+            try:
+                ah = torch.randn((m, k), device=dev, generator=g).bfloat16()
+                bh = torch.randn((m, k), device=dev, generator=g).bfloat16()
+                ms = ev_time(lambda: torch.matmul(ah, bh.t()))
+                ent["cublas_bf16_gemm"] = {"ms": round(ms, 4),
+                                           "tflops": round(2.0 * m * m * k / ms / 1e9, 1),
+                                           "tensor_frac": round(2.0 * m * m * k / ms / 1e9 / bf16, 4)}
+            except Exception as e:      # noqa: BLE001
+                ent["cublas_bf16_gemm"] = {"error": str(e).splitlines()[0][:200]}
+            rows.append(ent)
+            torch.cuda.empty_cache()
+    return {"metric": "trailing-update time (SYRK vs cuBLASLt MXFP8 GEMM), one B200",
+            "unit": "ms", "higher_is_better": False, "n_gpus": world, "data": "synthetic codes",
+            "peaks": {"hbm_gbs": hbm, "bf16_tflops": bf16, "fp8_tflops": 2 * bf16, "kind": peak_kind},
+            "config": {"workload": "syrk shapes of the rbf n=16384 factorization"}, "shapes": rows}
+
+
 def main():
     args = parse()
     world, rank, local = dist_init(args)
@@ -919,6 +1026,8 @@ def main():
         out = run_rbf_grad(args, world, rank, local)
     elif args.workload == "batch":
         out = run_batch(args, world, rank, local)
+    elif args.workload == "syrk":
+        out = run_syrk(args, world, rank, local)
     else:
         out = run_gpu(args, world, rank, local)
     if out is not None:

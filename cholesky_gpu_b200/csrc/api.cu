@@ -221,7 +221,7 @@ mpchol_status validate_opts(const mpchol_opts* o, int n) {
   if (o == nullptr || n <= 0) return MPCHOL_ERR_BAD_ARG;
   if (o->block_size < 32 || o->block_size > 256 || o->block_size % 32 != 0) return MPCHOL_ERR_BAD_ARG;
   if (o->precision < 0 || o->precision > MPCHOL_PREC_FP16X2) return MPCHOL_ERR_BAD_ARG;
-  if (o->left != 0) return MPCHOL_ERR_NOT_SUPPORTED;
+  if (o->left != 0 && o->left != 1) return MPCHOL_ERR_BAD_ARG;
   if (o->diag_pert && !(o->pivot_floor > 0.0f)) return MPCHOL_ERR_BAD_ARG;
   if (o->switch_mode != 0 && o->switch_mode != 1) return MPCHOL_ERR_BAD_ARG;
   if ((o->coherence != 0 && o->coherence != 1) || (o->equilibrate != 0 && o->equilibrate != 1))
@@ -502,7 +502,7 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream, const CopyPlan
     q.cand = fixed ? (o.precision != FP32 ? 1u << o.precision : 0u) : tc_mask;
     q.ldq = b;
     q.ldmx = b / 32;
-    const bool hist = streamed && k < f->hist_steps;
+    const bool hist = (streamed || o.left) && k < f->hist_steps;
     uint8_t* q8 = hist ? f->hq8 + (size_t)k * 3 * nbq : f->q8;
     int8_t* rexp = hist ? f->hrexp + (size_t)k * 3 * n : f->rexp;
     for (int i = 0; i < 3; ++i) {
@@ -547,6 +547,39 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream, const CopyPlan
   };
   // 128-tile column of step k's trailing matrix where block column j starts
   auto tcol = [&](int k, int j) { return ceil_div(std::min(j * b, n) - (k + 1) * b, 128); };
+  if (o.left) {
+    // Left-looking (settings.json "left"): block column k receives the
+    // updates of panels 0 .. k-1 just before it is factored -- one band
+    // launch per earlier panel, in step order, from the panels' quantized
+    // codes kept in the panel history -- then its diagonal block is factored
+    // and its panel solved.  Every tile receives the same FP32 updates in the
+    // same order as in the right-looking schedule, so the factor is the same
+    // bit for bit; the trailing matrix beyond block column k is never touched
+    // before its turn.
+    for (int k = 0; k < f->nsteps; ++k) {
+      for (int p = 0; p < k; ++p) {
+        TileSel band{SEL_BAND, 0, tcol(p, k), tcol(p, k + 1), 0};
+        mpchol_status rs = syrk(p, band, 0, stream);
+        if (rs != MPCHOL_OK) return rs;
+      }
+      mpchol_status rs = potrf(k);
+      if (rs != MPCHOL_OK) return rs;
+      const int s = k * b;
+      const int bs = std::min(b, n - s);
+      const int m = n - s - bs;
+      if (m <= 0) break;
+      const QuantAll qa = qa_for(k);
+      PHASE(MPCHOL_PH_TRSM, 1, stream,
+            launch_trsm_panel(f->tmapX, f->tmap32, f->A, ld, n, s, bs, f->winv, f->d, f->dtilde,
+                              f->rowsq, &f->steps[k], &f->steps[k + 1], std::min(b, m), dp, qa,
+                              f->status, stream, k > 0 ? &f->steps[k - 1] : nullptr,
+                              dp.coherence ? f->colacc + (size_t)k * b : nullptr));
+    }
+    if (o.equilibrate)
+      PHASE(MPCHOL_PH_SETUP, 1, stream, launch_equil_scale(f->A, ld, n, f->eqexp, 0, n, true, stream));
+    f->solve_ready = false;
+    return MPCHOL_OK;
+  }
   mpchol_status rs = potrf(0);
   if (rs != MPCHOL_OK) return rs;
   bool rest_pending = false;
@@ -1183,6 +1216,21 @@ mpchol_status mpchol_factor_create(const mpchol_opts* opts, int n, mpchol_factor
     free_factor(f);
     return MPCHOL_ERR_ALLOC;
   }
+  if (opts->left) {
+    // the quantized panels of every step (the left-looking schedule applies
+    // each panel to the later block columns one at a time)
+    const size_t nbq = (size_t)n * f->b;
+    const int hist = f->nsteps;
+    if (dmalloc(&f->hq8, (size_t)hist * 3 * nbq) != cudaSuccess ||
+        dmalloc(&f->hq16, (size_t)hist * 2 * nbq) != cudaSuccess ||
+        dmalloc(&f->hrexp, (size_t)hist * 3 * n) != cudaSuccess ||
+        dmalloc(&f->hmx, (size_t)hist * (nbq / 32)) != cudaSuccess) {
+      cudaGetLastError();
+      free_factor(f);
+      return MPCHOL_ERR_ALLOC;
+    }
+    f->hist_steps = hist;
+  }
   if (solve_init_attributes() != cudaSuccess) {
     free_factor(f);
     return MPCHOL_ERR_CUDA;
@@ -1218,13 +1266,20 @@ mpchol_status mpchol_factor_codes(const mpchol_factor_t* f, int fmt, const void*
     return MPCHOL_ERR_BAD_ARG;
   const int s = (f->nsteps - 2) * f->b;                   // the last step with trailing rows
   const size_t nb = (size_t)f->n * f->b;
+  // the left-looking schedule keeps every step's codes in the panel history
+  const int ks = f->nsteps - 2;
+  const bool hist = f->opts.left && ks < f->hist_steps;
+  const uint8_t* q8 = hist ? f->hq8 + (size_t)ks * 3 * nb : f->q8;
+  const uint16_t* q16 = hist ? f->hq16 + (size_t)ks * 2 * nb : f->q16;
+  const int8_t* rexp = hist ? f->hrexp + (size_t)ks * 3 * f->n : f->rexp;
+  const uint8_t* mx = hist ? f->hmx + (size_t)ks * (nb / 32) : f->mxexp;
   if (fmt == FP16 || fmt == FP16X2) {
-    *dCodes = f->q16;
-    *dScales = f->rexp + 2 * (size_t)f->n;
+    *dCodes = q16;
+    *dScales = rexp + 2 * (size_t)f->n;
   } else {
-    *dCodes = f->q8 + q8_slot(fmt) * nb;
-    *dScales = fmt == MXFP8 ? static_cast<const void*>(f->mxexp)
-                            : static_cast<const void*>(f->rexp + (size_t)rexp_slot(fmt) * f->n);
+    *dCodes = q8 + q8_slot(fmt) * nb;
+    *dScales = fmt == MXFP8 ? static_cast<const void*>(mx)
+                            : static_cast<const void*>(rexp + (size_t)rexp_slot(fmt) * f->n);
   }
   *ldq = f->b;
   *rows = f->n - s - f->b;
@@ -1246,9 +1301,10 @@ mpchol_status mpchol_solve_host(mpchol_factor_t* f, const float* hA, int lda, co
     MPCHOL_CUDA_TRY(dmalloc(&f->hx, (size_t)n * 8));
   }
   if (f->plan_mode < 0 && f->plan.c1[0] == 0) {
-    // equilibration scales A's lower triangle in one pass before step 0, so
-    // the copy does not overlap the factorization then
-    if (f->opts.equilibrate) {
+    // equilibration scales A's lower triangle in one pass before step 0, and
+    // the left-looking schedule has no trailing updates for late block
+    // columns to join: the copy does not overlap the factorization then
+    if (f->opts.equilibrate || f->opts.left) {
       f->plan = CopyPlan{};
       f->plan.c1[0] = f->nsteps;
     } else {
@@ -1323,7 +1379,8 @@ mpchol_status mpchol_set_copy_plan(mpchol_factor_t* f, int ngroups, const int* c
   p.ng = ngroups;
   if (ngroups > kMaxGroups || (ngroups > 1 && (cuts == nullptr || join == nullptr)))
     return MPCHOL_ERR_BAD_ARG;
-  if (ngroups > 1 && (f->b % 128 != 0 || f->opts.equilibrate)) return MPCHOL_ERR_NOT_SUPPORTED;
+  if (ngroups > 1 && (f->b % 128 != 0 || f->opts.equilibrate || f->opts.left))
+    return MPCHOL_ERR_NOT_SUPPORTED;
   p.c0[0] = 0;
   for (int g = 1; g < ngroups; ++g) {
     p.c1[g - 1] = cuts[g - 1];

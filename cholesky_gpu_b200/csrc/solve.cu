@@ -412,30 +412,54 @@ __device__ __forceinline__ void tile_mma_x8(const float* Ts, const double* x_c, 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int g = lane >> 2, t = lane & 3;
   const int B0 = 16 * warp;
-  double dn[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
-  double dt[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
-#pragma unroll 4
-  for (int k0 = 0; k0 < RB; k0 += 4) {
-    if (do_nt) {
-      const double b = x_c[g * XS + k0 + t];
+  // accumulators: [m-block][k-step parity] -- eight independent DMMA chains
+  // per warp when both products run
+  double dn[2][2][2] = {};
+  double dt[2][2][2] = {};
+  constexpr int KC = 8;                       // k-steps (of 4) per software-pipelined chunk
+#pragma unroll 1
+  for (int kb = 0; kb < RB; kb += 4 * KC) {
+    // every fragment of the chunk is loaded (and widened) before its DMMAs
+    float an[2][KC], at[2][KC];
+    double bn[KC], bt[KC];
 #pragma unroll
-      for (int mb = 0; mb < 2; ++mb) {
-        const int r = B0 + 8 * mb + g, c = k0 + t;
-        float v = Ts[bl_off(r, c)];
-        if (DIAG && r < c) v = 0.0f;
-        const double a = (double)v;
-        if (FRO) *fsq = fma((DIAG && r == c) ? a : 2.0 * a, a, *fsq);
-        dmma_m8n8k4(dn[mb], a, b);
+    for (int j = 0; j < KC; ++j) {
+      const int k0 = kb + 4 * j;
+      if (do_nt) {
+        bn[j] = x_c[g * XS + k0 + t];
+#pragma unroll
+        for (int mb = 0; mb < 2; ++mb) {
+          const int r = B0 + 8 * mb + g, c = k0 + t;
+          const float v = Ts[bl_off(r, c)];
+          an[mb][j] = (DIAG && r < c) ? 0.0f : v;
+        }
+      }
+      if (do_t) {
+        bt[j] = x_r[g * XS + k0 + t];
+#pragma unroll
+        for (int mb = 0; mb < 2; ++mb) {
+          const int c = B0 + 8 * mb + g, r = k0 + t;
+          const float v = Ts[bl_off(r, c)];
+          at[mb][j] = (DIAG && r <= c) ? 0.0f : v;
+        }
       }
     }
-    if (do_t) {
-      const double b = x_r[g * XS + k0 + t];
 #pragma unroll
-      for (int mb = 0; mb < 2; ++mb) {
-        const int c = B0 + 8 * mb + g, r = k0 + t;
-        float v = Ts[bl_off(r, c)];
-        if (DIAG && r <= c) v = 0.0f;
-        dmma_m8n8k4(dt[mb], (double)v, b);
+    for (int j = 0; j < KC; ++j) {
+      if (do_nt) {
+#pragma unroll
+        for (int mb = 0; mb < 2; ++mb) {
+          const double a = (double)an[mb][j];
+          if (FRO) {
+            const int r = B0 + 8 * mb + g, c = kb + 4 * j + t;
+            *fsq = fma((DIAG && r == c) ? a : 2.0 * a, a, *fsq);
+          }
+          dmma_m8n8k4(dn[mb][j & 1], a, bn[j]);
+        }
+      }
+      if (do_t) {
+#pragma unroll
+        for (int mb = 0; mb < 2; ++mb) dmma_m8n8k4(dt[mb][j & 1], (double)at[mb][j], bt[j]);
       }
     }
   }
@@ -445,8 +469,10 @@ __device__ __forceinline__ void tile_mma_x8(const float* Ts, const double* x_c, 
 #pragma unroll
     for (int i = 0; i < 2; ++i) {
       const int k = 2 * t + i;
-      if (do_nt && idx < nrows) atomicAdd(&y_rows[(size_t)k * n + row0 + idx], sign * dn[mb][i]);
-      if (do_t && idx < ncols) atomicAdd(&y_cols[(size_t)k * n + col0 + idx], sign * dt[mb][i]);
+      if (do_nt && idx < nrows)
+        atomicAdd(&y_rows[(size_t)k * n + row0 + idx], sign * (dn[mb][0][i] + dn[mb][1][i]));
+      if (do_t && idx < ncols)
+        atomicAdd(&y_cols[(size_t)k * n + col0 + idx], sign * (dt[mb][0][i] + dt[mb][1][i]));
     }
   }
 }

@@ -274,14 +274,15 @@ syrk_tc_body(const CUtensorMap* mhi, const CUtensorMap* mlo, const CUtensorMap* 
           const uint32_t a_lo = a_hi + STRIP;
           const uint32_t b_hi = diag ? a_hi : a_hi + NSETS * STRIP;
           const uint32_t b_lo = diag ? a_lo : a_hi + (NSETS + 1) * STRIP;
-          // MXFP8: this chunk's scales -> TMEM columns 2*TM + buf*16 + kc*8
-          // (A at +0, B at +4); chunks and accumulator buffers use separate
-          // columns, so no copy overwrites scales an unfinished MMA reads
+          // MXFP8: this chunk's scales -> TMEM columns 2*TM + buf*64 + kc*8
+          // (A at +0, B at +4; kc < 8 for K <= 1024); chunks and accumulator
+          // buffers use separate columns, so no copy overwrites scales an
+          // unfinished MMA reads
           uint32_t sfa_t = 0, sfb_t = 0;
           if (MX) {
             const uint32_t sfa_s = a_hi + 2 * NSETS * STRIP;
             const uint32_t sfb_s = diag ? sfa_s : sfa_s + SF_BYTES;
-            sfa_t = tmem + (uint32_t)(2 * TM + buf * 16 + kc * 8);
+            sfa_t = tmem + (uint32_t)(2 * TM + buf * 64 + kc * 8);
             sfb_t = sfa_t + 4;
             tc::utccp_32x128b_warpx4(sfa_t, tc::make_desc_plain(sfa_s, 128));
             tc::utccp_32x128b_warpx4(sfb_t, tc::make_desc_plain(sfb_s, 128));
@@ -482,9 +483,11 @@ cudaError_t launch_fmt(const TcMaps& maps, float* C, int ldc, int m, int k, cons
 
 }  // namespace
 
+// K up to 1024 (the factor uses K = block size <= 256; the kernel-level entry
+// point also takes the 512- and 1024-wide panels of larger-block schedules)
 bool syrk_tc_supported(int fmt, int k) {
-  if (fmt == FP16 || fmt == FP16X2) return k > 0 && (k * 2) % CHUNK == 0 && k <= 256;
-  if (fmt == E4M3 || fmt == E5M2 || fmt == MXFP8) return k > 0 && k % CHUNK == 0 && k <= 256;
+  if (fmt == FP16 || fmt == FP16X2) return k > 0 && (k * 2) % CHUNK == 0 && k <= 1024;
+  if (fmt == E4M3 || fmt == E5M2 || fmt == MXFP8) return k > 0 && k % CHUNK == 0 && k <= 1024;
   return false;
 }
 

@@ -78,7 +78,12 @@ typedef struct {
   int ladder_len;      /* switching ladder, lowest precision first (default {E4M3, FP16, FP32});
                           a step no entry qualifies for takes the last (most precise) entry */
   int ladder[4];
-  int left;            /* 0: right-looking (only value built); settings.json "left" */
+  int left;            /* settings.json "left".  0: right-looking with a one-block look-ahead.
+                          1: left-looking -- block column k receives the updates of panels
+                          0..k-1 (kept quantized, about 7 n b bytes per step) just before it is
+                          factored; the factor is identical bit for bit, the schedule has no
+                          look-ahead and one launch per (panel, block column) pair.  Batches:
+                          0 only. */
   int coherence;       /* switch_mode 0 only.  1 (default): a ladder entry p must also satisfy
                           u_p * ||P^T 1||^2 / m <= eps' * min_i dtilde_i, where P is the step's
                           m x b panel: a panel whose columns share one sign pattern across the
@@ -290,8 +295,9 @@ MPCHOL_API mpchol_status mpchol_solve_host(mpchol_factor_t* f, const float* hA, 
  * ngroups == 1: copy all of A, then factor; ngroups 2..8: block columns
  * [0, cuts[0]), [cuts[0], cuts[1]), ..., group g >= 1 joining at step
  * join[g-1] (0 <= join[g-1] <= cuts[g-1] - 1, non-decreasing).  Needs
- * block_size % 128 == 0 and equilibrate == 0 for ngroups > 1
- * (MPCHOL_ERR_NOT_SUPPORTED); an equilibrated factor copies all of A first. */
+ * block_size % 128 == 0, equilibrate == 0 and left == 0 for ngroups > 1
+ * (MPCHOL_ERR_NOT_SUPPORTED); an equilibrated or left-looking factor copies
+ * all of A first. */
 MPCHOL_API mpchol_status mpchol_set_copy_plan(mpchol_factor_t* f, int ngroups, const int* cuts,
                                               const int* join);
 /* The automatic plan for order n and block_size: returns the number of

@@ -54,7 +54,9 @@ def test_default_options():
     (dict(block_size=100), _lib.ERR_BAD_ARG),
     (dict(block_size=512), _lib.ERR_BAD_ARG),
     (dict(precision=9), _lib.ERR_BAD_ARG),
-    (dict(left=1), _lib.ERR_NOT_SUPPORTED),
+    (dict(left=2), _lib.ERR_BAD_ARG),
+    (dict(coherence=2), _lib.ERR_BAD_ARG),
+    (dict(equilibrate=-1), _lib.ERR_BAD_ARG),
     (dict(diag_pert=1, pivot_floor=0.0), _lib.ERR_BAD_ARG),
     (dict(switch_mode=3), _lib.ERR_BAD_ARG),
     (dict(precision="e4m3", block_size=64), _lib.ERR_NOT_SUPPORTED),

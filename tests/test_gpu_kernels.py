@@ -149,6 +149,32 @@ def test_tensor_core_syrk_matches_oracle(cuda, fmt, m, k):
     assert np.array_equal(got[~low], C[~low])
 
 
+@pytest.mark.parametrize("fmt", [O.MXFP8, O.FP16, O.E4M3])
+@pytest.mark.parametrize("m,k", [(700, 512), (1300, 1024)])
+def test_tensor_core_syrk_wide_panels(cuda, fmt, m, k):
+    """The kernel-level SYRK with 512- and 1024-wide quantized panels (codes
+    and scales from the oracle's quantizer): MXFP8 takes one E8M0 scale per
+    32 columns across all K chunks (tensor-memory scale columns per chunk and
+    accumulator buffer)."""
+    lib = _lib.load()
+    P = panel(m, k, 5)
+    codes, s = O.quantize_rows(P, fmt)
+    g = np.random.default_rng(6)
+    C = g.standard_normal((m, m)).astype(np.float32)
+    Cd = torch.from_numpy(C.T.copy()).cuda()
+    Qd = torch.from_numpy(np.ascontiguousarray(codes.view(np.int16) if fmt == O.FP16 else codes)).cuda()
+    Sd = torch.from_numpy(np.ascontiguousarray(s.view(np.uint8))).cuda()
+    _lib.check(lib.mpchol_syrk_update(Cd.data_ptr(), m, m, k, fmt, Qd.data_ptr(), Sd.data_ptr(),
+                                      None, 0, stream()))
+    got = Cd.cpu().numpy().T
+    want = syrk_ref(C, codes, s, fmt, m, k)
+    low = np.tril(np.ones((m, m), bool))
+    err = np.abs(got[low] - want[low]).max() / np.abs(want[low]).max()
+    print(f"tc syrk fmt={fmt} m={m} k={k} max rel err {err:.3e}")
+    assert err < {O.FP16: 4e-6}.get(fmt, 2e-4), err
+    assert np.array_equal(got[~low], C[~low])
+
+
 @pytest.mark.parametrize("m,k", [(640, 256), (333, 96)])
 def test_fp32_syrk_matches_fp64(cuda, m, k):
     lib = _lib.load()
