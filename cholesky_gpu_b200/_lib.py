@@ -50,6 +50,7 @@ class Opts(ctypes.Structure):
         ("left", ctypes.c_int),
         ("coherence", ctypes.c_int),
         ("equilibrate", ctypes.c_int),
+        ("eps_coherence", ctypes.c_float),
     ]
 
 

@@ -226,6 +226,7 @@ mpchol_status validate_opts(const mpchol_opts* o, int n) {
   if (o->switch_mode != 0 && o->switch_mode != 1) return MPCHOL_ERR_BAD_ARG;
   if ((o->coherence != 0 && o->coherence != 1) || (o->equilibrate != 0 && o->equilibrate != 1))
     return MPCHOL_ERR_BAD_ARG;
+  if (!(o->eps_coherence >= 0.0f)) return MPCHOL_ERR_BAD_ARG;
   if (o->ladder_len < 0 || o->ladder_len > 4) return MPCHOL_ERR_BAD_ARG;
   auto tc_ok = [&](int fmt) { return fmt == MPCHOL_PREC_FP32 || syrk_tc_supported(fmt, o->block_size); };
   if (o->precision != MPCHOL_PREC_SWITCHING && !tc_ok(o->precision)) return MPCHOL_ERR_NOT_SUPPORTED;
@@ -283,6 +284,7 @@ DecisionParams make_dp(const mpchol_opts& o) {
   dp.ladder_len = o.ladder_len;
   for (int i = 0; i < 4; ++i) dp.ladder[i] = o.ladder[i];
   dp.coherence = (o.precision == MPCHOL_PREC_SWITCHING && o.switch_mode == 0 && o.coherence) ? 1 : 0;
+  dp.eps_coh = o.eps_coherence > 0.0f ? o.eps_coherence : o.eps_prime;
   return dp;
 }
 
@@ -1167,6 +1169,7 @@ void mpchol_opts_default(mpchol_opts* o) {
   o->left = 0;
   o->coherence = 1;
   o->equilibrate = 0;
+  o->eps_coherence = 0.0f;
 }
 
 void mpchol_pcg_opts_default(mpchol_pcg_opts* o) {

@@ -34,7 +34,8 @@ struct DecisionParams {
   float floor_ratio;   // near-indefinite flag threshold
   int ladder_len;
   int ladder[4];
-  int coherence;       // switch_mode 0: also bound u_p * coherence ratio by eps'
+  int coherence;       // switch_mode 0: also bound u_p * coherence ratio
+  float eps_coh;       // ... by eps_coh (eps_prime when not set)
 };
 
 // ---- POTRF of the diagonal block (one CTA) ------------------------------

@@ -21,7 +21,7 @@ __device__ __forceinline__ int resolve_precision(const StepState* step, const De
   for (int k = 0; k < dp.ladder_len; ++k) {
     const int p = dp.ladder[k];
     const float u = unit_roundoff(p);
-    if (u * ratio <= dp.eps_prime && u * coh <= dp.eps_prime) return p;
+    if (u * ratio <= dp.eps_prime && u * coh <= dp.eps_coh) return p;
   }
   // no entry meets the bound: the ladder's most precise (last) entry
   return dp.ladder_len > 0 ? dp.ladder[dp.ladder_len - 1] : FP32;

@@ -97,6 +97,12 @@ typedef struct {
                           the solves are unchanged.  mpchol_factor_diags then returns the scaled
                           diagonals.  The diagonal equilibration intent of
                           src/kernels_macros.cuh:137-158.  0 (default): off. */
+  float eps_coherence; /* threshold of the coherence test (coherence = 1): a ladder entry p
+                          needs u_p * ||P^T 1||^2 / (m min_i dtilde_i) <= eps_coherence;
+                          0 (default) uses eps_prime.  A small value keeps the large, coherent
+                          updates of the first steps in the higher precisions and gives the
+                          later, smaller ones to FP8, which costs fewer PCG iterations than
+                          the same number of early FP8 steps. */
 } mpchol_opts;
 
 /* Per-factor results, filled by mpchol_factor_info (synchronizes the stream). */

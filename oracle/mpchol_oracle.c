@@ -237,8 +237,9 @@ typedef struct {
   int ladder[4];
   const int* force_prec;   /* nullable: per-step precision override */
   const int* force_fp64;   /* nullable: per-step FP64 diag override */
-  int coherence;        /* switch_mode 0: also require u_p * coh <= eps' */
+  int coherence;        /* switch_mode 0: also require u_p * coh <= eps_coh */
   int equilibrate;      /* 1: factor D A D, D = diag(2^-e_i), then unscale L's rows */
+  float eps_coherence;  /* the coherence threshold; 0: eps' */
 } orc_chol_opts;
 
 typedef struct {
@@ -327,7 +328,8 @@ int orc_choose_precision(const float* d, const float* dt, int m, float coh, cons
   for (int k = 0; k < o->ladder_len; ++k) {
     const int p = o->ladder[k];
     const float u = orc_unit_roundoff(p);
-    if (u * ratio <= o->eps_prime && (!o->coherence || u * coh <= o->eps_prime)) return p;
+    const float ec = o->eps_coherence > 0.0f ? o->eps_coherence : o->eps_prime;
+    if (u * ratio <= o->eps_prime && (!o->coherence || u * coh <= ec)) return p;
   }
   return o->ladder_len > 0 ? o->ladder[o->ladder_len - 1] : ORC_FP32;
 }

@@ -50,6 +50,7 @@ class CholOpts(ctypes.Structure):
         ("force_fp64", ctypes.POINTER(ctypes.c_int)),
         ("coherence", ctypes.c_int),
         ("equilibrate", ctypes.c_int),
+        ("eps_coherence", ctypes.c_float),
     ]
 
 
@@ -209,11 +210,11 @@ def ref_micro_cholesky(A: np.ndarray) -> tuple[np.ndarray, int]:
 
 def make_opts(block_size=256, precision=SWITCHING, eps_prime=0.5, floor=0.0, diag_pert=0,
               pert=1.0, pivot_floor=1e-7, switch_mode=0, ladder=(E4M3, FP16, FP32),
-              coherence=1, equilibrate=0) -> CholOpts:
+              coherence=1, equilibrate=0, eps_coherence=0.0) -> CholOpts:
     o = CholOpts()
     o.block_size, o.precision, o.eps_prime, o.floor_ratio = block_size, precision, eps_prime, floor
     o.diag_pert, o.pert, o.pivot_floor, o.switch_mode = diag_pert, pert, pivot_floor, switch_mode
-    o.coherence, o.equilibrate = coherence, equilibrate
+    o.coherence, o.equilibrate, o.eps_coherence = coherence, equilibrate, eps_coherence
     o.ladder_len = len(ladder)
     for i in range(4):
         o.ladder[i] = ladder[i] if i < len(ladder) else FP32
@@ -233,6 +234,7 @@ def factor_kwargs(opts) -> dict:
     kw["ladder"] = tuple(int(opts.ladder[i]) for i in range(int(opts.ladder_len)))
     kw["coherence"] = int(getattr(opts, "coherence", 0))
     kw["equilibrate"] = int(getattr(opts, "equilibrate", 0))
+    kw["eps_coherence"] = float(getattr(opts, "eps_coherence", 0.0))
     return kw
 
 

@@ -60,8 +60,8 @@ def test_coherence_rule_picks_mxfp8_after_the_constant_mode(cuda, rbf2048):
     print(f"rbf n={n} steps {gpu_steps}: factor rel Frobenius vs oracle {err:.2e}")
     # MXFP8 steps: a one-ulp FP32 difference in a panel value (accumulation
     # order) can move an E4M3 code by one step (2^-4 relative); measured
-    # 1e-3 on the B200, the bar leaves a margin of about 5x
-    assert err < 5e-3
+    # 2.9e-3 on the B200
+    assert err < 1e-2
     B = matgen.rhs(n, 2, 5).numpy()
     Ad = torch.from_numpy(A).cuda()
     X, rep = f.pcg(Ad, torch.from_numpy(B).cuda(), rel_tol=1e-10, max_it=100)
@@ -112,7 +112,7 @@ def test_fp8_factor_with_shifts_is_won_back_at_kappa_1e4(cuda, prec):
     X, rep = f.pcg(Ad, torch.from_numpy(B).cuda(), rel_tol=1e-10, max_it=400)
     _, it_o, _ = O.pcg(A, ref["L"], B, 1e-10, 400)
     print(f"{prec} kappa=1e4: factor err vs oracle {err:.2e}, it {rep.iterations} (oracle {it_o})")
-    assert err < 5e-2
+    assert err < 5e-3          # measured 1.5e-3 (E4M3) and 1.6e-3 (MXFP8) on the B200
     assert rep.converged and rep.rel_residual <= 1e-10
     assert abs(rep.iterations - it_o) <= max(10, it_o // 5)
 
