@@ -65,6 +65,8 @@ def parse():
     ap.add_argument("--kappa", type=float, default=1e6)
     ap.add_argument("--block", type=int, default=256)
     ap.add_argument("--eps-prime", type=float, default=None)
+    ap.add_argument("--eps-coherence", type=float, default=None,
+                    help="threshold of the switching rule's coherence test (0: eps')")
     ap.add_argument("--precision", default="switching",
                     help="policy of the mixed arm: switching, e4m3, e5m2, mxfp8, fp16, fp16x2")
     ap.add_argument("--ladder", default=None,
@@ -88,6 +90,8 @@ def parse():
         args.ladder = w.get("ladder", "e4m3,fp16,fp16x2")
     if args.eps_prime is None:
         args.eps_prime = w.get("eps", 1e-5)
+    if args.eps_coherence is None:
+        args.eps_coherence = w.get("eps_c", 0.0)
     return args
 
 
@@ -234,15 +238,19 @@ def profiled_traffic(kernel: str, n: int):
 
 
 # ---------------------------------------------------------------- GPU arm
-PREC_LETTER = {0: "S", 1: "h", 2: "e", 3: "f", 4: "M", 6: "X"}   # per-step sequence letters
-PREC_KEYS = ((0, "fp32"), (1, "fp16"), (2, "e4m3"), (3, "e5m2"), (4, "mxfp8"), (6, "fp16x2"))
+PREC_LETTER = {0: "S", 1: "h", 2: "e", 3: "f", 4: "M", 6: "X", 7: "a", 8: "b", 9: "q"}
+PREC_KEYS = ((0, "fp32"), (1, "fp16"), (2, "e4m3"), (3, "e5m2"), (4, "mxfp8"), (6, "fp16x2"),
+             (7, "mxfp6_e2m3"), (8, "mxfp6_e3m2"), (9, "mxfp4"))
 
 # Per-workload defaults of the mixed arm: the switching ladder (lowest
-# precision first) and eps'.  RBF: MXFP8 wherever the criterion allows it
-# (every step after the constant mode at eps' = 2); SPD kappa = 1e6: FP8 is
-# rejected by the Schur ratio at any useful eps', FP16X2 carries the factor.
+# precision first), eps' and the coherence threshold eps_c.  RBF: eps' = 2
+# admits MXFP8 after the constant mode; eps_c = 1/16 keeps the large, coherent
+# early updates in FP16 and hands the remaining steps (51 of 63) to MXFP8,
+# 5 PCG iterations (eps_c = eps' takes every step in MXFP8 and needs 14).
+# SPD kappa = 1e6: FP8 is rejected by the Schur ratio at any useful eps', FP16X2
+# carries the factor.
 WORKLOADS = {
-    "rbf": dict(n=16384, ladder="mxfp8,fp16,fp16x2", eps=2.0, rhs=8),
+    "rbf": dict(n=16384, ladder="mxfp8,fp16,fp16x2", eps=2.0, eps_c=0.0625, rhs=8),
     "spd": dict(n=8192, ladder="e4m3,fp16,fp16x2", eps=1e-5, rhs=1),
 }
 
@@ -265,7 +273,7 @@ def workload_inputs(args, rank, dev):
         B = matgen.rhs(n, args.rhs, 5 + rank, device=dev)
         desc = {"workload": (f"rbf n={n} d=784 zeros=0.8 l=median({ell:.4f}) nugget=1e-3 "
                              f"rhs={args.rhs} block={args.block} ladder={args.ladder} "
-                             f"eps'={args.eps_prime:g}"),
+                             f"eps'={args.eps_prime:g} eps_c={args.eps_coherence:g}"),
                 "n": n, "d": 784, "lengthscale": round(ell, 6), "nugget": 1e-3}
         data = "synthetic (seeded sparse points in [0,1]^784 standing in for image data; RBF kernel)"
     else:
@@ -301,7 +309,7 @@ def run_gpu(args, world, rank, local):
     stream = torch.cuda.current_stream(dev)
     ladder = [x.strip() for x in args.ladder.split(",") if x.strip()]
     mixed_opts = dict(block_size=b, precision=args.precision, eps_prime=args.eps_prime,
-                      ladder=ladder)
+                      eps_coherence=args.eps_coherence, ladder=ladder)
     # factor objects are created outside the timed region (allocation is setup)
     fobj = {"mixed": mp.Factor(n, **mixed_opts),
             "fp32": mp.Factor(n, block_size=b, precision="fp32")}
@@ -435,15 +443,22 @@ def forced_arms(args):
     for p in ("mxfp8", "e4m3"):
         out.append((p, dict(precision=p)))
         out.append((p + "_pert4", dict(precision=p, pert=4.0)))
+    # the switching arm's rule with an FP6 or FP4 MX format in the MXFP8 slot
+    for low in ("mxfp6e2m3", "mxfp4"):
+        out.append(("switching_" + low, dict(precision="switching", eps_prime=args.eps_prime,
+                                             eps_coherence=args.eps_coherence,
+                                             ladder=[low] + args.ladder.split(",")[1:])))
     return out
 
 
-def forced_arm(f, solve, stream, k=2):
-    """Time (median of k after one warm-up) and outcome of one forced arm;
-    a factor or solve that fails is recorded with its status."""
+def forced_arm(f, solve, stream, k=3):
+    """Time (median of k after two warm-ups: the second call captures the
+    factorization's graph) and outcome of one forced arm; a factor or solve
+    that fails is recorded with its status."""
     import torch
     from cholesky_gpu_b200 import MpcholError
     try:
+        solve()
         solve()
         times, rep = [], None
         for _ in range(k):

@@ -30,8 +30,12 @@ PREC_E5M2 = 3
 PREC_MXFP8 = 4
 PREC_SWITCHING = 5
 PREC_FP16X2 = 6
+PREC_MXFP6_E2M3 = 7
+PREC_MXFP6_E3M2 = 8
+PREC_MXFP4 = 9
 PREC_NAMES = {PREC_FP32: "fp32", PREC_FP16: "fp16", PREC_E4M3: "e4m3", PREC_E5M2: "e5m2",
-              PREC_MXFP8: "mxfp8", PREC_SWITCHING: "switching", PREC_FP16X2: "fp16x2"}
+              PREC_MXFP8: "mxfp8", PREC_SWITCHING: "switching", PREC_FP16X2: "fp16x2",
+              PREC_MXFP6_E2M3: "mxfp6e2m3", PREC_MXFP6_E3M2: "mxfp6e3m2", PREC_MXFP4: "mxfp4"}
 PREC_BY_NAME = {v: k for k, v in PREC_NAMES.items()}
 
 
@@ -61,7 +65,7 @@ class FactorInfo(ctypes.Structure):
         ("n_perturbed", ctypes.c_int),
         ("nsteps", ctypes.c_int),
         ("n_fp64_blocks", ctypes.c_int),
-        ("steps_by_prec", ctypes.c_int * 7),
+        ("steps_by_prec", ctypes.c_int * 10),
     ]
 
 

@@ -220,7 +220,7 @@ namespace {
 mpchol_status validate_opts(const mpchol_opts* o, int n) {
   if (o == nullptr || n <= 0) return MPCHOL_ERR_BAD_ARG;
   if (o->block_size < 32 || o->block_size > 256 || o->block_size % 32 != 0) return MPCHOL_ERR_BAD_ARG;
-  if (o->precision < 0 || o->precision > MPCHOL_PREC_FP16X2) return MPCHOL_ERR_BAD_ARG;
+  if (o->precision < 0 || o->precision > MPCHOL_PREC_MXFP4) return MPCHOL_ERR_BAD_ARG;
   if (o->left != 0 && o->left != 1) return MPCHOL_ERR_BAD_ARG;
   if (o->diag_pert && !(o->pivot_floor > 0.0f)) return MPCHOL_ERR_BAD_ARG;
   if (o->switch_mode != 0 && o->switch_mode != 1) return MPCHOL_ERR_BAD_ARG;
@@ -236,9 +236,13 @@ mpchol_status validate_opts(const mpchol_opts* o, int n) {
     } else {
       for (int i = 0; i < o->ladder_len; ++i) {
         const int p = o->ladder[i];
-        if (p < 0 || p > MPCHOL_PREC_FP16X2 || p == MPCHOL_PREC_SWITCHING) return MPCHOL_ERR_BAD_ARG;
+        if (p < 0 || p > MPCHOL_PREC_MXFP4 || p == MPCHOL_PREC_SWITCHING) return MPCHOL_ERR_BAD_ARG;
         if (!tc_ok(p)) return MPCHOL_ERR_NOT_SUPPORTED;
       }
+      // the MX formats share one code slot and scale buffer
+      int nmx = 0;
+      for (int i = 0; i < o->ladder_len; ++i) nmx += is_mx(o->ladder[i]) ? 1 : 0;
+      if (nmx > 1) return MPCHOL_ERR_NOT_SUPPORTED;
     }
   }
   return MPCHOL_OK;
@@ -1265,7 +1269,7 @@ mpchol_status mpchol_factor_codes(const mpchol_factor_t* f, int fmt, const void*
       rows == nullptr || col0 == nullptr)
     return MPCHOL_ERR_BAD_ARG;
   if (f->nsteps < 2) return MPCHOL_ERR_BAD_ARG;          // no trailing update
-  if (fmt != FP16 && fmt != FP16X2 && fmt != E4M3 && fmt != E5M2 && fmt != MXFP8)
+  if (fmt != FP16 && fmt != FP16X2 && fmt != E4M3 && fmt != E5M2 && !is_mx(fmt))
     return MPCHOL_ERR_BAD_ARG;
   const int s = (f->nsteps - 2) * f->b;                   // the last step with trailing rows
   const size_t nb = (size_t)f->n * f->b;
@@ -1281,7 +1285,7 @@ mpchol_status mpchol_factor_codes(const mpchol_factor_t* f, int fmt, const void*
     *dScales = rexp + 2 * (size_t)f->n;
   } else {
     *dCodes = q8 + q8_slot(fmt) * nb;
-    *dScales = fmt == MXFP8 ? static_cast<const void*>(mx)
+    *dScales = is_mx(fmt) ? static_cast<const void*>(mx)
                             : static_cast<const void*>(rexp + (size_t)rexp_slot(fmt) * f->n);
   }
   *ldq = f->b;
@@ -1447,7 +1451,7 @@ mpchol_status mpchol_factor_info_get(const mpchol_factor_t* fc, mpchol_factor_in
     if (hStepPrec) hStepPrec[k] = p;
     if (hStepFp64) hStepFp64[k] = steps[k].fp64_diag;
     if (steps[k].fp64_diag) info->n_fp64_blocks++;
-    if (m > 0 && p >= 0 && p < 7) info->steps_by_prec[p]++;
+    if (m > 0 && p >= 0 && p < kNumFmts) info->steps_by_prec[p]++;
   }
   return MPCHOL_OK;
 }
@@ -1690,10 +1694,10 @@ mpchol_status mpchol_quantize_rows(const float* dP, int m, int k, int ldp, int f
                                    void* dScale, mpchol_stream_t stream) {
   if (dP == nullptr || dQ == nullptr || dScale == nullptr || m < 0 || ldp < m) return MPCHOL_ERR_BAD_ARG;
   if (k < 32 || k > 256 || k % 32 != 0) return MPCHOL_ERR_BAD_ARG;
-  if (fmt != FP16 && fmt != E4M3 && fmt != E5M2 && fmt != MXFP8 && fmt != FP16X2)
+  if (fmt != FP16 && fmt != E4M3 && fmt != E5M2 && !is_mx(fmt) && fmt != FP16X2)
     return MPCHOL_ERR_BAD_ARG;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  if (fmt == MXFP8)
+  if (is_mx(fmt))
     PHASE(MPCHOL_PH_QUANT, 1, s, launch_quantize_rows(dP, ldp, m, k, fmt, dQ, k, nullptr,
                                          reinterpret_cast<uint8_t*>(dScale), k / 32, s));
   else
@@ -1724,7 +1728,7 @@ mpchol_status mpchol_syrk_update(float* dC, int ldc, int m, int k, int fmt, cons
   }
   if (!syrk_tc_supported(fmt, k)) return MPCHOL_ERR_NOT_SUPPORTED;
   if (dQ == nullptr || dScale == nullptr) return MPCHOL_ERR_BAD_ARG;
-  if (fmt == MXFP8)
+  if (is_mx(fmt))
     PHASE(MPCHOL_PH_SYRK_TC, 1, s, launch_syrk_tc(dC, ldc, m, k, fmt, dQ, k, nullptr,
                                    reinterpret_cast<const uint8_t*>(dScale), k / 32, nullptr,
                                    nullptr, s));

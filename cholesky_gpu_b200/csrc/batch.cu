@@ -177,7 +177,8 @@ mpchol_status mpchol_batch_create(const mpchol_opts* opts, int count, const int*
   const int fmt = opts->precision;
   const int b = opts->block_size;
   if (fmt == MPCHOL_PREC_FP32 || fmt == MPCHOL_PREC_SWITCHING) return MPCHOL_ERR_NOT_SUPPORTED;
-  if (fmt < 0 || fmt > MPCHOL_PREC_FP16X2) return MPCHOL_ERR_BAD_ARG;
+  if (fmt < 0 || fmt > MPCHOL_PREC_MXFP4) return MPCHOL_ERR_BAD_ARG;
+  if (fmt > MPCHOL_PREC_FP16X2) return MPCHOL_ERR_NOT_SUPPORTED;   // FP6/FP4: single systems only
   if (b < 32 || b > 256 || b % 32 != 0) return MPCHOL_ERR_BAD_ARG;
   if (!syrk_tc_supported(fmt, b)) return MPCHOL_ERR_NOT_SUPPORTED;
   if (opts->left != 0 || opts->equilibrate != 0) return MPCHOL_ERR_NOT_SUPPORTED;

@@ -10,7 +10,34 @@
 namespace mpchol {
 
 // Storage format ids match MPCHOL_PREC_*.
-enum Fmt : int { FP32 = 0, FP16 = 1, E4M3 = 2, E5M2 = 3, MXFP8 = 4, SWITCHING = 5, FP16X2 = 6 };
+enum Fmt : int {
+  FP32 = 0, FP16 = 1, E4M3 = 2, E5M2 = 3, MXFP8 = 4, SWITCHING = 5, FP16X2 = 6,
+  MXFP6E2M3 = 7, MXFP6E3M2 = 8, MXFP4 = 9
+};
+constexpr int kNumFmts = 10;
+
+// The OCP MX family: E8M0 scales per 32 elements along K with E4M3, E2M3,
+// E3M2 or E2M1 elements.  The FP6/FP4 element values are exactly
+// representable in E4M3, so they are stored as E4M3 codes of the same value
+// and multiplied by the block-scaled E4M3 MMA -- the products are those of a
+// native FP6/FP4 MMA (FP32 accumulation), the storage and speed are FP8's.
+__host__ __device__ __forceinline__ bool is_mx(int f) {
+  return f == MXFP8 || f == MXFP6E2M3 || f == MXFP6E3M2 || f == MXFP4;
+}
+struct MxElem {
+  int mbits;    // stored mantissa bits
+  int emin;     // exponent of the smallest normal binade (subnormal spacing 2^(emin - mbits))
+  int emax;     // exponent of the largest binade (the OCP MX scale is floor(log2 amax) - emax)
+  float maxv;   // largest finite value (saturation)
+};
+__host__ __device__ __forceinline__ MxElem mx_elem(int f) {
+  switch (f) {
+    case MXFP6E2M3: return {3, 0, 2, 7.5f};
+    case MXFP6E3M2: return {2, -2, 4, 28.0f};
+    case MXFP4: return {1, 0, 2, 6.0f};
+    default: return {3, -6, 8, 448.0f};      // E4M3
+  }
+}
 
 // Device-side status block shared by every kernel of one factor/solve.  A
 // kernel that detects a failure (non-SPD pivot, exhausted bounded wait, bad
@@ -65,12 +92,25 @@ __device__ __forceinline__ int row_scale_exp(float amax, int fmt) {
   return e;
 }
 
-// OCP MX shared exponent (E4M3 elements): floor(log2 amax) - 8, clamped to
-// [-127, 127]; amax == 0 gives -127 (E8M0 code 0).
-__device__ __forceinline__ int mx_scale_exp(float amax) {
+// OCP MX shared exponent: floor(log2 amax) - emax of the element format
+// (8 for E4M3), clamped to [-127, 127]; amax == 0 gives -127 (E8M0 code 0).
+__device__ __forceinline__ int mx_scale_exp(float amax, int fmt = MXFP8) {
   if (!(amax > 0.0f) || isinf(amax)) return -127;
-  int e = ilog2f_dev(amax) - 8;
+  int e = ilog2f_dev(amax) - mx_elem(fmt).emax;
   return e < -127 ? -127 : (e > 127 ? 127 : e);
+}
+
+// Round-to-nearest-even onto an FP6/FP4 element grid (OCP: no Inf/NaN codes,
+// saturating at the largest value; NaN stays NaN).  x / q and r * q are
+// exact: q is a power of two and x lies far inside the FP32 range.
+__device__ __forceinline__ float mx_round_elem(float x, const MxElem& m) {
+  const float a = fabsf(x);
+  if (!(a == a)) return x;
+  if (a >= m.maxv) return copysignf(m.maxv, x);
+  int e = (a > 0.0f) ? ilog2f_dev(a) : m.emin;
+  if (e < m.emin) e = m.emin;
+  const float q = pow2f(e - m.mbits);
+  return copysignf(fminf(rintf(a / q) * q, m.maxv), x);
 }
 
 // Hardware RNE + satfinite conversions (cvt.rn.satfinite.{e4m3,e5m2}x2.f32).
@@ -95,11 +135,23 @@ __device__ __forceinline__ uint16_t f32x2_to_e4m3x2(float a, float b) {
 __device__ __forceinline__ uint16_t f32x2_to_e5m2x2(float a, float b) {
   return (uint16_t)__nv_cvt_float2_to_fp8x2(make_float2(a, b), __NV_SATFINITE, __NV_E5M2);
 }
+// An MX-family element as its E4M3 code (two at a time): E4M3 directly,
+// FP6/FP4 rounded onto their grid first (the rounded value is exact in E4M3)
+__device__ __forceinline__ uint16_t mx_code_x2(float a, float b, int fmt) {
+  if (fmt != MXFP8) {
+    const MxElem m = mx_elem(fmt);
+    a = mx_round_elem(a, m);
+    b = mx_round_elem(b, m);
+  }
+  return f32x2_to_e4m3x2(a, b);
+}
 
 // Unit roundoff of each storage format (used by the switching criterion).
 __host__ __device__ __forceinline__ float unit_roundoff(int fmt) {
   switch (fmt) {
-    case E4M3: case MXFP8: return 0.0625f;
+    case E4M3: case MXFP8: case MXFP6E2M3: return 0.0625f;
+    case MXFP6E3M2: return 0.125f;
+    case MXFP4: return 0.25f;
     case E5M2: return 0.125f;
     case FP16: return 4.8828125e-4f;
     case FP16X2: return 2.3841858e-7f;   // hi + lo: 22 significant bits

@@ -61,17 +61,17 @@ cudaError_t launch_potrf(const CUtensorMap& tmap32, float* A, int lda, int n, in
 struct QuantAll {
   unsigned cand;        // bit f set: format f is a candidate of the step
   int ldq;
-  uint8_t* q8[3];       // E4M3, E5M2, MXFP8 codes (slot q8_slot)
+  uint8_t* q8[3];       // E4M3, E5M2, MX-family codes (slot q8_slot)
   uint16_t* q16;        // FP16 / FP16X2 hi codes, then FP16X2 lo codes
   int8_t* rexp[3];      // per-row pow-2 exponents: E4M3, E5M2, FP16 / FP16X2
-  uint8_t* mxexp;       // MXFP8 E8M0 scales, ldmx per row
+  uint8_t* mxexp;       // MX-family E8M0 scales, ldmx per row
   int ldmx;
   float* sh;
 };
 __host__ __device__ inline int q8_slot(int fmt) { return fmt == E4M3 ? 0 : (fmt == E5M2 ? 1 : 2); }
 __host__ __device__ inline int rexp_slot(int fmt) { return fmt == E4M3 ? 0 : (fmt == E5M2 ? 1 : 2); }
 // Solves X * L11^T = A21 in place for rows [s+bs, n) of block column s, one
-// 32-row slab per CTA; subtracts each row's sum of squares from dtilde,
+// slab of 32 or 64 rows per CTA; subtracts each row's sum of squares from dtilde,
 // stores it in rowsq, folds the switching statistics into step (and the FP64
 // flag of the next diagonal block into next), and writes the slab's codes in
 // every candidate format.  The last CTA to finish resolves the step precision

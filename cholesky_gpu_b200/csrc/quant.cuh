@@ -65,17 +65,17 @@ __device__ inline void quantize_tile(const float* __restrict__ P, int ldp, int m
       v[t] = (t < cpl) ? tile[(lane * cpl + t) * (QROWS + 1) + r] : 0.0f;
       amax = fmaxf(amax, fabsf(v[t]));
     }
-    if (fmt == MXFP8) {
+    if (is_mx(fmt)) {
       // one E8M0 scale per 32 consecutive columns = 32/cpl lanes
       const int lpb = 32 / cpl;
       float bmax = amax;
       for (int o = 1; o < lpb; o <<= 1) bmax = fmaxf(bmax, __shfl_xor_sync(0xffffffffu, bmax, o));
-      const int e = mx_scale_exp(bmax);
+      const int e = mx_scale_exp(bmax, fmt);
       const float inv = pow2f(-e);
       uint8_t* qr = reinterpret_cast<uint8_t*>(q) + (size_t)gi * ldq + lane * cpl;
 #pragma unroll
       for (int t = 0; t < 8; ++t)
-        if (t < cpl) qr[t] = f32_to_e4m3(v[t] * inv);
+        if (t < cpl) qr[t] = (uint8_t)mx_code_x2(v[t] * inv, 0.0f, fmt);
       if ((lane % lpb) == 0) mxexp[(size_t)gi * ldmx + lane / lpb] = (uint8_t)(e + 127);
     } else {
       const float rmax = warp_max(amax);

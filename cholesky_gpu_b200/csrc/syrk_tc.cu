@@ -352,7 +352,7 @@ syrk_tc_body(const CUtensorMap* mhi, const CUtensorMap* mlo, const CUtensorMap* 
           // (signed zeros included) as it was
           const int i0 = I * TM + q * 32;
           if (i0 < mt && j0 < mt && !(I == J && j0 >= i0 + 32)) {
-            if (lane == 0) tc::bulk_wait_read();     // this warp's previous box has been read
+            if (lane == 0) tc::bulk_wait_smem_read();   // this warp's previous box has been read
             __syncwarp();
 #pragma unroll
             for (int u = 0; u < 32; ++u) {
@@ -385,7 +385,7 @@ syrk_tc_body(const CUtensorMap* mhi, const CUtensorMap* mlo, const CUtensorMap* 
       }
     }
   }
-  if (RED && warp >= 2 && lane == 0) tc::bulk_wait_read();   // staging read before exit
+  if (RED && warp >= 2 && lane == 0) tc::bulk_wait_read();   // reduce-adds performed before exit
   tc::tc_fence_before();
   __syncthreads();
   if (warp == 1) {
@@ -440,6 +440,9 @@ syrk_tc_dispatch_kernel(const __grid_constant__ TcMapsAll maps, float* __restric
                                 0, st, nb, 0, sel);
       break;
     case MXFP8:
+    case MXFP6E2M3:    // FP6/FP4 element values stored as E4M3 codes: the same body
+    case MXFP6E3M2:
+    case MXFP4:
       syrk_tc_body<MXFP8, false>(&maps.h8[2], &maps.h8[2], &maps.c, C, ldc, m, k, nullptr, mxexp,
                                  ldmx, st, nb, 0, sel);
       break;
@@ -487,7 +490,7 @@ cudaError_t launch_fmt(const TcMaps& maps, float* C, int ldc, int m, int k, cons
 // point also takes the 512- and 1024-wide panels of larger-block schedules)
 bool syrk_tc_supported(int fmt, int k) {
   if (fmt == FP16 || fmt == FP16X2) return k > 0 && (k * 2) % CHUNK == 0 && k <= 1024;
-  if (fmt == E4M3 || fmt == E5M2 || fmt == MXFP8) return k > 0 && k % CHUNK == 0 && k <= 1024;
+  if (fmt == E4M3 || fmt == E5M2 || is_mx(fmt)) return k > 0 && k % CHUNK == 0 && k <= 1024;
   return false;
 }
 
@@ -496,6 +499,7 @@ cudaError_t launch_syrk_tc(float* C, int ldc, int m, int k, int fmt, const void*
                            const int* prec_sel, DevStatus* st, cudaStream_t stream, TileSel sel,
                            int max_sms) {
   if (m <= 0) return cudaSuccess;
+  if (is_mx(fmt)) fmt = MXFP8;    // the family shares the E4M3 block-scaled path
   if (fmt == MXFP8 && (mxexp == nullptr || ldmx < k / 32 ||
                        (reinterpret_cast<uintptr_t>(mxexp) & 3) != 0 || (ldmx & 3) != 0))
     return cudaErrorInvalidValue;
@@ -535,7 +539,11 @@ cudaError_t launch_syrk_tc_dispatch(float* C, int ldc, int m, int k, unsigned fm
   if (ntiles <= 0) return cudaSuccess;
   for (int f : {FP16, E4M3, E5M2, FP16X2, MXFP8})
     if (((fmt_mask >> f) & 1u) && !syrk_tc_supported(f, k)) return cudaErrorInvalidValue;
-  if (((fmt_mask >> MXFP8) & 1u) &&
+  // an FP6/FP4 MX format takes the MXFP8 maps and shared memory (the kernel
+  // still checks the step's own format against the full mask)
+  const unsigned kMxFamily = (1u << MXFP6E2M3) | (1u << MXFP6E3M2) | (1u << MXFP4);
+  const unsigned setup_mask = fmt_mask | ((fmt_mask & kMxFamily) ? (1u << MXFP8) : 0u);
+  if (((setup_mask >> MXFP8) & 1u) &&
       (qa.mxexp == nullptr || qa.ldmx < k / 32 || (reinterpret_cast<uintptr_t>(qa.mxexp) & 3) != 0 ||
        (qa.ldmx & 3) != 0))
     return cudaErrorInvalidValue;
@@ -545,12 +553,12 @@ cudaError_t launch_syrk_tc_dispatch(float* C, int ldc, int m, int k, unsigned fm
     return cudaErrorInvalidValue;
   maps.h8[0] = maps.h8[1] = maps.h8[2] = maps.h16 = maps.l16 = maps.c;   // unused slots
   for (int f : {E4M3, E5M2, MXFP8})
-    if (((fmt_mask >> f) & 1u) &&
+    if (((setup_mask >> f) & 1u) &&
         !encode_tmap_2d(&maps.h8[q8_slot(f)], CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, qa.q8[q8_slot(f)],
                         (uint64_t)k, (uint64_t)m, (uint64_t)qa.ldq, CHUNK, TM,
                         CU_TENSOR_MAP_SWIZZLE_128B))
       return cudaErrorInvalidValue;
-  if (fmt_mask & ((1u << FP16) | (1u << FP16X2))) {
+  if (setup_mask & ((1u << FP16) | (1u << FP16X2))) {
     if (!encode_tmap_2d(&maps.h16, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, qa.q16, (uint64_t)k,
                         (uint64_t)m, (uint64_t)qa.ldq, CHUNK / 2, TM, CU_TENSOR_MAP_SWIZZLE_128B))
       return cudaErrorInvalidValue;
@@ -560,11 +568,11 @@ cudaError_t launch_syrk_tc_dispatch(float* C, int ldc, int m, int k, unsigned fm
       return cudaErrorInvalidValue;
   }
   size_t smem = 0;
-  if ((fmt_mask >> FP16) & 1u) smem = std::max(smem, tc_smem<FP16, false>());
-  if ((fmt_mask >> E4M3) & 1u) smem = std::max(smem, tc_smem<E4M3, false>());
-  if ((fmt_mask >> E5M2) & 1u) smem = std::max(smem, tc_smem<E5M2, false>());
-  if ((fmt_mask >> FP16X2) & 1u) smem = std::max(smem, tc_smem<FP16X2, false>());
-  if ((fmt_mask >> MXFP8) & 1u) smem = std::max(smem, tc_smem<MXFP8, false>());
+  if ((setup_mask >> FP16) & 1u) smem = std::max(smem, tc_smem<FP16, false>());
+  if ((setup_mask >> E4M3) & 1u) smem = std::max(smem, tc_smem<E4M3, false>());
+  if ((setup_mask >> E5M2) & 1u) smem = std::max(smem, tc_smem<E5M2, false>());
+  if ((setup_mask >> FP16X2) & 1u) smem = std::max(smem, tc_smem<FP16X2, false>());
+  if ((setup_mask >> MXFP8) & 1u) smem = std::max(smem, tc_smem<MXFP8, false>());
   if (smem == 0) return cudaSuccess;
   const size_t smem_all = std::max({tc_smem<FP16, false>(), tc_smem<E4M3, false>(),
                                     tc_smem<E5M2, false>(), tc_smem<FP16X2, false>(),

@@ -87,6 +87,11 @@ __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.comm
 __device__ __forceinline__ void bulk_wait_read() {
   asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
 }
+// Wait until every committed bulk store has finished reading its shared-memory
+// source (the source may be overwritten; the global side may still be in flight).
+__device__ __forceinline__ void bulk_wait_smem_read() {
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
 // Make generic-proxy writes to shared memory visible to the async proxy (TMA).
 __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");

@@ -6,18 +6,23 @@
 // (src/kernels_macros.cuh:191-211).
 //
 // X * L11^T = A21 for the m rows below the diagonal block.  Rows are
-// independent, so one CTA owns a 32-row slab.  TMA stages the slab (one 2-D
-// box) and streams L11 one 32-row tile row at a time (the strictly-lower
-// tiles L_{J,<J} as 2-D boxes and the inverse of the diagonal tile L_JJ, which
-// the POTRF kernel wrote, as a 1-D bulk copy) two rows ahead of its use, so a
-// CTA needs about 108 KB of shared memory and two CTAs share an SM.  The CTA
-// walks the 32-column tiles J: X_J -= X_{<J} L_{J,<J}^T (register-tiled,
-// K split over four thread groups), X_J = X_J L_JJ^-T, writes the slab back
-// and, in the epilogue, folds each row's sum of squares into the
-// Schur-diagonal tracker dtilde, reduces the switching statistics
-// (max d/dtilde, reference-literal choice) and the near-indefinite flag of
-// the next diagonal block, and writes the slab's codes in every candidate
-// format.
+// independent, so one CTA of 16 warps owns a slab of 32 or 64 rows (64 while
+// the panel has more 32-row slabs than the GPU has SMs).  TMA stages the slab
+// and all of L11: the strictly-lower 32 x 32 tiles L_{J,M} as 2-D boxes and
+// the inverses of the diagonal tiles L_JJ, which the POTRF kernel wrote, as
+// 1-D bulk copies, one mbarrier per tile row.  The solve is a pipeline over
+// the 32-column tiles J of the slab, a warp pair per tile (each warp 16 of its
+// columns, each lane one or two rows):
+//   X_J = (A_J - sum_{K<J} X_K L_{J,K}^T) L_JJ^-T,
+// where the pair of tile J applies X_K as soon as the pair of tile K has
+// published it (an mbarrier per tile, bounded waits), so the only chain is
+// one tile update plus one diagonal multiply per tile column.  The epilogue
+// writes the slab back (TMA stores), folds each row's sum of squares into the
+// Schur-diagonal tracker dtilde, reduces the switching statistics (max
+// d/dtilde, min dtilde, the reference-literal choice, the panel's column sums)
+// and the near-indefinite flag of the next diagonal block, and writes the
+// slab's codes in every candidate format.  The last CTA to finish (a ticket
+// counter) resolves the step precision.
 #include <algorithm>
 
 #include "common.cuh"
@@ -28,118 +33,139 @@
 namespace mpchol {
 namespace {
 
-constexpr int TR = 32;       // rows per CTA
-constexpr int NTHR = 256;    // 8 warps
+constexpr int NTHR = 512;    // 16 warps: two per 32-column tile of a 256-wide block
 constexpr int TSZ = 32 * 32; // dense 32 x 32 tile
-constexpr int XLD = TR;      // X staged column-major, rows contiguous
-constexpr int KG = 4;        // groups the update's K dimension is split over
-constexpr int KPG = 32 / KG; // K values of each L tile per group
-static_assert(NTHR == KG * (TR / 4) * 8, "a group maps 4 x 4 outputs to each of its threads");
+constexpr int MAXNT = 8;     // tiles per block column (b <= 256)
 
 __device__ __forceinline__ int tl(int I, int M) { return I * (I - 1) / 2 + M; }  // I > M
 
-// Shared memory of the streaming panel kernel: the slab, two buffers of one
-// tile row of L11 (up to NT - 1 tiles) and of one tile inverse, the partial
-// sums of the split update.
-size_t trsm_smem_floats(int bs) {
-  const int NT = bs / 32;
-  return (size_t)bs * XLD + 2 * (size_t)(NT - 1) * TSZ + 2 * (size_t)TSZ + (size_t)(KG - 1) * TR * 32;
-}
-// Shared memory of the batched kernel: the slab, all of L11's tiles and
-// inverses, the partial sums.
-size_t trsm_batched_smem_floats(int bs) {
-  const int NT = bs / 32;
-  return (size_t)bs * XLD + (size_t)(NT * (NT - 1) / 2) * TSZ + (size_t)NT * TSZ +
-         (size_t)(KG - 1) * TR * 32;
+// The slab in shared memory: 32-row halves, each column-major with its 32
+// rows contiguous (the layout of a 32 x bs TMA box), so lane l reading row l
+// (or l + 32) of one column touches 32 different banks.
+__device__ __forceinline__ int xoff(int r, int c, int bs) {
+  return (r >> 5) * bs * 32 + c * 32 + (r & 31);
 }
 
-// Step J of the slab solve: X_J -= X_{<J} L_{J,<J}^T, then X_J = X_J L_JJ^-T.
-// LJ: the tiles L_{J,0..J-1} (column-major 32 x 32, contiguous); WJ: L_JJ^-1.
-// The update splits K over four groups of 64 threads: a thread keeps 4 rows x
-// 4 columns of X_J in registers and does 16 FMAs per 16-byte load of X and of
-// L; groups 1-3 hand their partial sums to group 0 through red, which adds
-// them in group order.  Every output's operations, and so its rounding, are
-// fixed by this split.
-__device__ void trsm_step(float* Xs, const float* LJ, const float* WJ, float* red, int J, int tid) {
-  const int g = tid / 64, t = tid % 64;
-  const int r4 = t % (TR / 4), c4 = t / (TR / 4);   // rows 4*r4.., columns 4*c4.. of X_J
-  const int kend = 32 * J;
-  if (J > 0) {
-    float acc[4][4];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const float4 v = (g == 0) ? *reinterpret_cast<const float4*>(&Xs[(kend + 4 * c4 + j) * XLD + 4 * r4])
-                                : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-      acc[0][j] = v.x; acc[1][j] = v.y; acc[2][j] = v.z; acc[3][j] = v.w;
-    }
-    for (int kt = 0; kt < J; ++kt) {
-      const float* lt = LJ + kt * TSZ + 4 * c4 + KPG * g * 32;
-      const float* xt = Xs + (32 * kt + KPG * g) * XLD + 4 * r4;
-#pragma unroll
-      for (int kk = 0; kk < KPG; ++kk) {
-        const float4 xv = *reinterpret_cast<const float4*>(xt + kk * XLD);
-        const float4 lv = *reinterpret_cast<const float4*>(lt + kk * 32);
-        const float xr[4] = {xv.x, xv.y, xv.z, xv.w};
-        const float lr[4] = {lv.x, lv.y, lv.z, lv.w};
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-          for (int j = 0; j < 4; ++j) acc[i][j] -= xr[i] * lr[j];
-      }
-    }
-    if (g > 0) {
-      float* rg = red + (g - 1) * TR * 32;
-#pragma unroll
-      for (int j = 0; j < 4; ++j)
-        *reinterpret_cast<float4*>(&rg[(4 * c4 + j) * TR + 4 * r4]) =
-            make_float4(acc[0][j], acc[1][j], acc[2][j], acc[3][j]);
-    }
-    __syncthreads();
-    if (g == 0) {
-#pragma unroll
-      for (int q = 0; q < KG - 1; ++q) {
-        const float* rg = red + q * TR * 32;
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const float4 pv = *reinterpret_cast<const float4*>(&rg[(4 * c4 + j) * TR + 4 * r4]);
-          acc[0][j] += pv.x; acc[1][j] += pv.y; acc[2][j] += pv.z; acc[3][j] += pv.w;
-        }
-      }
-#pragma unroll
-      for (int j = 0; j < 4; ++j)
-        *reinterpret_cast<float4*>(&Xs[(kend + 4 * c4 + j) * XLD + 4 * r4]) =
-            make_float4(acc[0][j], acc[1][j], acc[2][j], acc[3][j]);
-    }
-    __syncthreads();
-  }
-  // X_J = X_J * L_JJ^-T :  x[r][c] = sum_{m<=c} a[r][m] * (L^-1)[c][m]
-  const int tr = tid % (TR / 4), tc_ = tid / (TR / 4);   // rows 4*tr.., column tc_
-  float out[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-#pragma unroll 8
-  for (int m = 0; m < 32; ++m) {
-    const float4 av = *reinterpret_cast<const float4*>(&Xs[(kend + m) * XLD + 4 * tr]);
-    const float wv = WJ[m * 32 + tc_];
-    out[0] += av.x * wv; out[1] += av.y * wv; out[2] += av.z * wv; out[3] += av.w * wv;
-  }
-  __syncthreads();
-  *reinterpret_cast<float4*>(&Xs[(kend + tc_) * XLD + 4 * tr]) = make_float4(out[0], out[1], out[2], out[3]);
-  __syncthreads();
+// Code staging panel of the epilogue (32-bit words): FP16X2 hi + lo rows of
+// bs / 2 + 1 words, or 8-bit code rows of bs / 4 + 1 words.
+size_t stage_words(int tr, int bs) {
+  return std::max((size_t)2 * tr * (bs / 2 + 1), (size_t)tr * (bs / 4 + 1));
+}
+// Shared memory of both panel kernels (floats): the slab, then L11's
+// strictly-lower tiles and the inverses of its diagonal tiles (the code
+// staging panel reuses that space once the solve is done).
+size_t trsm_smem_floats(int tr, int bs) {
+  const int NT = bs / 32;
+  const size_t lw = (size_t)(NT * (NT - 1) / 2 + NT) * TSZ;
+  return (size_t)bs * tr + std::max(lw, stage_words(tr, bs));
 }
 
-// Per-row sum of squares and max |x| of the solved slab, by all threads:
-// thread (r, part) = (tid % TR, tid / TR) covers row r's 32 columns `part`
-// (sums of squares as a chain of FMAs in column order), leaving the partials
-// in s_sq / s_amax [part][r]; the row's sum is then the partials added in
-// part order (row_sq).  One fixed order for the streaming and the batched
-// kernel, so both give the same bits.
-__device__ __forceinline__ void slab_row_partials(const float* Xs, int NT, float (*s_sq)[TR],
+__device__ __forceinline__ void load16(const float* p, float (&v)[16]) {
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const float4 w = reinterpret_cast<const float4*>(p)[q];
+    v[4 * q] = w.x; v[4 * q + 1] = w.y; v[4 * q + 2] = w.z; v[4 * q + 3] = w.w;
+  }
+}
+__device__ __forceinline__ void pair_sync(int J) {   // the two warps of tile column J
+  asm volatile("bar.sync %0, 64;" ::"r"(J + 1) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tc::smem_u32(bar)) : "memory");
+}
+
+// The slab solve.  Warp w works on tile column J = w / 2, columns
+// 16 (w % 2) .. +15 of it, and lane l on slab rows l (and l + 32 when RPL =
+// 2).  Lt: L11's tiles L_{I,M} (I > M) at tl(I, M) * TSZ; Wt: the inverses
+// W_JJ = L_JJ^-1, tile J at J * TSZ; both column-major (L(c, m) at m * 32 + c,
+// W(c, m) zero for m > c).  lrow[J] (null: already staged) completes when
+// tile row J has landed; ready[J] (64 arrivals) when X_J is final.  Each
+// output is one fma chain in a fixed order: the update over K, then m; the
+// diagonal multiply over m.  Returns false if a bounded wait gave up.
+template <int RPL>
+__device__ bool slab_solve(float* Xs, int bs, const float* Lt, const float* Wt, uint64_t* lrow,
+                           uint64_t* ready, int tid) {
+  const int NT = bs / 32;
+  const int warp = tid >> 5, lane = tid & 31;
+  const int J = warp >> 1, h = warp & 1;
+  if (J >= NT) return true;
+  const int XH = bs * 32;                              // floats per 32-row half
+  bool ok = lrow == nullptr || tc::mbar_wait(&lrow[J], 0);
+  const int c0 = 32 * J + 16 * h;                      // first slab column of the warp
+  float acc[RPL][16];
+#pragma unroll
+  for (int q = 0; q < RPL; ++q)
+#pragma unroll
+    for (int u = 0; u < 16; ++u) acc[q][u] = Xs[q * XH + (c0 + u) * 32 + lane];
+#pragma unroll 1
+  for (int K = 0; K < J; ++K) {
+    ok = tc::mbar_wait(&ready[K], 0) && ok;
+    const float* L = Lt + (size_t)tl(J, K) * TSZ + 16 * h;
+    const float* xk = Xs + 32 * K * 32 + lane;
+#pragma unroll 4
+    for (int m = 0; m < 32; ++m) {
+      float x[RPL];
+#pragma unroll
+      for (int q = 0; q < RPL; ++q) x[q] = xk[q * XH + m * 32];
+      float l[16];
+      load16(L + m * 32, l);
+#pragma unroll
+      for (int q = 0; q < RPL; ++q)
+#pragma unroll
+        for (int u = 0; u < 16; ++u) acc[q][u] = fmaf(-x[q], l[u], acc[q][u]);
+    }
+  }
+  // both halves of the updated tile into the slab, then X_J = Y W_JJ^T
+#pragma unroll
+  for (int q = 0; q < RPL; ++q)
+#pragma unroll
+    for (int u = 0; u < 16; ++u) Xs[q * XH + (c0 + u) * 32 + lane] = acc[q][u];
+  pair_sync(J);
+  const float* W = Wt + (size_t)J * TSZ + 16 * h;
+  const float* y = Xs + 32 * J * 32 + lane;
+  float o[RPL][16];
+#pragma unroll
+  for (int q = 0; q < RPL; ++q)
+#pragma unroll
+    for (int u = 0; u < 16; ++u) o[q][u] = 0.0f;
+  const int mend = 16 * h + 16;                        // W(c, m) = 0 for m > c
+#pragma unroll 4
+  for (int m = 0; m < mend; ++m) {
+    float yv[RPL];
+#pragma unroll
+    for (int q = 0; q < RPL; ++q) yv[q] = y[q * XH + m * 32];
+    float w[16];
+    load16(W + m * 32, w);
+#pragma unroll
+    for (int q = 0; q < RPL; ++q)
+#pragma unroll
+      for (int u = 0; u < 16; ++u) o[q][u] = fmaf(yv[q], w[u], o[q][u]);
+  }
+  pair_sync(J);                                        // every read of Y is done
+#pragma unroll
+  for (int q = 0; q < RPL; ++q)
+#pragma unroll
+    for (int u = 0; u < 16; ++u) Xs[q * XH + (c0 + u) * 32 + lane] = o[q][u];
+  mbar_arrive(&ready[J]);                              // release: X_J to the later tiles
+  return ok;
+}
+
+// Per-row sum of squares and max |x| of the solved slab: thread (r, part) =
+// (tid % TR, tid / TR) covers row r's 32 columns `part` (sums of squares as a
+// chain of FMAs in column order), leaving the partials in s_sq / s_amax
+// [part][r]; the row's sum is then the partials added in part order (row_sq).
+// One fixed order for the streaming and the batched kernel, so both give the
+// same bits.
+template <int TR>
+__device__ __forceinline__ void slab_row_partials(const float* Xs, int bs, float (*s_sq)[TR],
                                                   float (*s_amax)[TR], int tid) {
+  const int NT = bs / 32;
   const int r = tid % TR, part = tid / TR;
   float sq = 0.0f, amax = 0.0f;
   if (part < NT) {
 #pragma unroll 8
     for (int c = part * 32; c < part * 32 + 32; ++c) {
-      const float v = Xs[c * XLD + r];
+      const float v = Xs[xoff(r, c, bs)];
       sq = __fmaf_rn(v, v, sq);
       amax = fmaxf(amax, fabsf(v));
     }
@@ -147,19 +173,20 @@ __device__ __forceinline__ void slab_row_partials(const float* Xs, int NT, float
   s_sq[part][r] = sq;
   if (s_amax != nullptr) s_amax[part][r] = amax;
 }
+template <int TR>
 __device__ __forceinline__ float row_sq(float (*s_sq)[TR], int NT, int r) {
   float sq = s_sq[0][r];
   for (int q = 1; q < NT; ++q) sq += s_sq[q][r];
   return sq;
 }
 
-// Codes of one solved slab in one format.  Xs: the slab (bs columns x TR
-// rows, column-major, stride XLD).  Thread (r, part) = (tid % TR, tid / TR)
-// converts row r's 32-column block `part` (for MXFP8 with its own scale)
-// into packed words of a shared staging panel (row stride bs/4 + 1 words for
-// 8-bit codes, bs/2 + 1 for 16-bit ones, so the column-wise writes of 32
-// consecutive rows hit 32 banks); the CTA then copies the staged rows out as
-// coalesced 4-byte words.
+// Codes of one solved slab in one format.  Thread (r, part) = (tid % TR,
+// tid / TR) converts row r's 32-column block `part` (for an MX format with
+// its own scale) into packed words of a shared staging panel (row stride
+// bs/4 + 1 words for 8-bit codes, bs/2 + 1 for 16-bit ones, so the
+// column-wise writes of 32 consecutive rows hit 32 banks); the CTA then
+// copies the staged rows out as coalesced 4-byte words.
+template <int TR>
 __device__ void quantize_slab(const float* Xs, int bs, int nrows, int gi0, int m, int fmt, float rmax,
                               const QuantAll& qa, uint32_t* stage, int tid) {
   const int r = tid % TR, part = tid / TR;
@@ -176,7 +203,7 @@ __device__ void quantize_slab(const float* Xs, int bs, int nrows, int gi0, int m
     if (cw == 32) {
 #pragma unroll
       for (int c = c0; c < c0 + 32; c += 2) {
-        const float x0 = Xs[c * XLD + r] * inv, x1 = Xs[(c + 1) * XLD + r] * inv;
+        const float x0 = Xs[xoff(r, c, bs)] * inv, x1 = Xs[xoff(r, c + 1, bs)] * inv;
         const __half2 h = __floats2half2_rn(x0, x1);
         hi[r * sw + c / 2] = *reinterpret_cast<const uint32_t*>(&h);
         if (fmt == FP16X2) {   // x - hi is exact in FP32
@@ -199,17 +226,17 @@ __device__ void quantize_slab(const float* Xs, int bs, int nrows, int gi0, int m
     const int sw = bs / 4 + 1;
     int e = 0;
     float inv = 1.0f;
-    if (fmt != MXFP8) {
+    if (!is_mx(fmt)) {
       e = row_scale_exp(rmax, fmt);
       inv = pow2f(-e);
       if (live && part == 0) qa.rexp[rexp_slot(fmt)][gi] = (int8_t)e;
     }
     for (int cb = c0; cb < c0 + cw; cb += 32) {
-      if (fmt == MXFP8) {
+      if (is_mx(fmt)) {
         // one E8M0 scale per 32 consecutive columns (OCP MX)
         float bmax = 0.0f;
-        for (int c = cb; c < cb + 32; ++c) bmax = fmaxf(bmax, fabsf(Xs[c * XLD + r]));
-        const int eb = mx_scale_exp(bmax);
+        for (int c = cb; c < cb + 32; ++c) bmax = fmaxf(bmax, fabsf(Xs[xoff(r, c, bs)]));
+        const int eb = mx_scale_exp(bmax, fmt);
         inv = pow2f(-eb);
         if (live) qa.mxexp[(size_t)gi * qa.ldmx + cb / 32] = (uint8_t)(eb + 127);
       }
@@ -217,9 +244,11 @@ __device__ void quantize_slab(const float* Xs, int bs, int nrows, int gi0, int m
       for (int c = cb; c < cb + 32; c += 4) {
         float x[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) x[u] = Xs[(c + u) * XLD + r] * inv;
-        const uint32_t w01 = (fmt == E5M2) ? f32x2_to_e5m2x2(x[0], x[1]) : f32x2_to_e4m3x2(x[0], x[1]);
-        const uint32_t w23 = (fmt == E5M2) ? f32x2_to_e5m2x2(x[2], x[3]) : f32x2_to_e4m3x2(x[2], x[3]);
+        for (int u = 0; u < 4; ++u) x[u] = Xs[xoff(r, c + u, bs)] * inv;
+        const uint32_t w01 = (fmt == E5M2) ? f32x2_to_e5m2x2(x[0], x[1])
+                             : (fmt == E4M3) ? f32x2_to_e4m3x2(x[0], x[1]) : mx_code_x2(x[0], x[1], fmt);
+        const uint32_t w23 = (fmt == E5M2) ? f32x2_to_e5m2x2(x[2], x[3])
+                             : (fmt == E4M3) ? f32x2_to_e4m3x2(x[2], x[3]) : mx_code_x2(x[2], x[3], fmt);
         stage[r * sw + c / 4] = w01 | (w23 << 16);
       }
     }
@@ -235,35 +264,35 @@ __device__ void quantize_slab(const float* Xs, int bs, int nrows, int gi0, int m
   __syncthreads();                             // the staging panel is reused
 }
 
-// Panel solve with the quantization of the panel fused in; one 32-row slab
-// per CTA, two CTAs per SM (the launch may exceed the resident CTAs: no CTA
-// waits on another).  Each CTA stages its slab and streams L11's tile rows by
-// TMA, solves the slab, writes it back, folds its rows into the diagonal
-// tracker and the switching statistics, and writes the slab's codes in every
-// candidate format (the step's precision is not known yet; the trailing
-// update reads the panel of the one the step picks).  The CTA that finishes
-// last (a ticket counter) resolves the step precision and adds the step's
-// rounding shift u_p * sum_j L_ij^2 to sh.
-__global__ void __launch_bounds__(NTHR, 2)
+// Panel solve with the quantization of the panel fused in; one slab of TR =
+// 32 * RPL rows per CTA (the launch may exceed the resident CTAs: no CTA
+// waits on another).  Each CTA stages its slab and L11 by TMA, solves the
+// slab, writes it back, folds its rows into the diagonal tracker and the
+// switching statistics, and writes the slab's codes in every candidate
+// format (the step's precision is not known yet; the trailing update reads
+// the panel of the one the step picks).  The CTA that finishes last (a
+// ticket counter) resolves the step precision.
+template <int RPL>
+__global__ void __launch_bounds__(NTHR, 1)
 trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_constant__ CUtensorMap tmap32,
                   float* __restrict__ A, int lda, int n, int s, int bs, const float* __restrict__ winv,
                   const float* __restrict__ d, float* __restrict__ dtilde, float* __restrict__ rowsq,
                   StepState* step, StepState* next, int next_bs, DecisionParams dp, DevStatus* st,
                   QuantAll qa, const StepState* prev, double* __restrict__ colacc) {
+  constexpr int TR = 32 * RPL;
   extern __shared__ __align__(128) float sm[];
   const int NT = bs / 32;
-  float* Xs = sm;                                        // [bs][XLD]
-  float* Lb = Xs + (size_t)bs * XLD;                     // 2 x (NT - 1) tiles: rows of L11
-  float* Wb = Lb + 2 * (size_t)(NT - 1) * TSZ;           // 2 x 1 tile: inverses of L_JJ
-  float* red = Wb + 2 * (size_t)TSZ;                     // partial sums of the split update
-  uint32_t* stage = reinterpret_cast<uint32_t*>(Lb);     // code staging, once L11 is used
+  float* Xs = sm;                                        // the slab (xoff layout)
+  float* Lt = Xs + (size_t)bs * TR;                      // L_{I,M}, I > M
+  float* Wt = Lt + (size_t)(NT * (NT - 1) / 2) * TSZ;    // L_JJ^-1
+  uint32_t* stage = reinterpret_cast<uint32_t*>(Lt);     // code staging, once L11 is used
   __shared__ float red_max[NTHR / 32];
   __shared__ int red_lit[NTHR / 32];
   __shared__ float red_min[NTHR / 32];
   __shared__ double red_coh[NTHR / 32];
   __shared__ float s_rmax[NTHR / TR][TR];
   __shared__ float s_sq[NTHR / TR][TR];
-  __shared__ __align__(8) uint64_t barx, barl[2];
+  __shared__ __align__(8) uint64_t barx, lrow[MAXNT], ready[MAXNT];
   __shared__ int s_ok, s_last;
 
   const int tid = threadIdx.x;
@@ -280,27 +309,27 @@ trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_consta
       *shp = __fmaf_rn(unit_roundoff(pp), rowsq[row0 + tid], *shp);
     }
   }
-  // tile row J of L11 (tiles L_{J,0..J-1} and L_JJ^-1) into buffer J % 2
-  auto issue_row = [&](int J) {
-    const int buf = J & 1;
-    tc::mbar_expect_tx(&barl[buf], (uint32_t)((J + 1) * TSZ * sizeof(float)));
-    for (int M = 0; M < J; ++M)
-      tc::tma_load_2d(Lb + ((size_t)buf * (NT - 1) + M) * TSZ, &tmap32, &barl[buf], s + 32 * J, s + 32 * M);
-    tc::bulk_load_1d(Wb + buf * TSZ, winv + J * TSZ, (uint32_t)(TSZ * sizeof(float)), &barl[buf]);
-  };
   if (tid == 0) {
     s_ok = st->code == 0;
     tc::mbar_init(&barx, 1);
-    tc::mbar_init(&barl[0], 1);
-    tc::mbar_init(&barl[1], 1);
+    for (int J = 0; J < NT; ++J) {
+      tc::mbar_init(&lrow[J], 1);
+      tc::mbar_init(&ready[J], 64);
+    }
     tc::fence_mbar_init();
   }
   __syncthreads();
-  int issued = 0, consumed = 0;   // tile rows issued / waited for (thread 0's counts)
-  if (s_ok && tid == 0) {
-    tc::mbar_expect_tx(&barx, (uint32_t)(bs * XLD * sizeof(float)));
-    tc::tma_load_2d(Xs, &tmapX, &barx, row0, s);
-    for (; issued < 2 && issued < NT; ++issued) issue_row(issued);
+  const bool issued = s_ok != 0;
+  if (issued && tid == 0) {
+    tc::mbar_expect_tx(&barx, (uint32_t)(RPL * bs * 32 * sizeof(float)));
+    for (int q = 0; q < RPL; ++q) tc::tma_load_2d(Xs + q * bs * 32, &tmapX, &barx, row0 + 32 * q, s);
+    for (int J = 0; J < NT; ++J) {
+      tc::mbar_expect_tx(&lrow[J], (uint32_t)((J + 1) * TSZ * sizeof(float)));
+      for (int M = 0; M < J; ++M)
+        tc::tma_load_2d(Lt + (size_t)tl(J, M) * TSZ, &tmap32, &lrow[J], s + 32 * J, s + 32 * M);
+      tc::bulk_load_1d(Wt + (size_t)J * TSZ, winv + (size_t)J * TSZ, (uint32_t)(TSZ * sizeof(float)),
+                       &lrow[J]);
+    }
     if (!tc::mbar_wait(&barx, 0)) {
       s_ok = 0;
       set_status(st, MPCHOL_ERR_TIMEOUT, row0);
@@ -308,45 +337,35 @@ trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_consta
     }
   }
   __syncthreads();
+  if (s_ok) {
+    if (!slab_solve<RPL>(Xs, bs, Lt, Wt, lrow, ready, tid)) {
+      s_ok = 0;
+      set_status(st, MPCHOL_ERR_TIMEOUT, row0);
+    }
+  }
+  // every copy into L11's space has landed before it is reused (bounded;
+  // immediate once the solve has seen each tile row)
+  if (issued && tid == 0)
+    for (int J = 0; J < NT; ++J) tc::mbar_wait(&lrow[J], 0);
+  __syncthreads();
   float bm = 0.0f;   // this CTA's max d/dtilde, min dtilde and literal code
   float bmin = INFINITY;
   int bl = 0;
   if (s_ok) {
-    for (int J = 0; J < NT; ++J) {
-      if (tid == 0 && s_ok) {
-        if (tc::mbar_wait(&barl[J & 1], (uint32_t)((J >> 1) & 1))) {
-          consumed = J + 1;
-        } else {
-          s_ok = 0;
-          set_status(st, MPCHOL_ERR_TIMEOUT, row0);
-        }
-      }
-      __syncthreads();
-      if (!s_ok) break;
-      trsm_step(Xs, Lb + (size_t)(J & 1) * (NT - 1) * TSZ, Wb + (J & 1) * TSZ, red, J, tid);
-      // trsm_step ends with a barrier: buffer J % 2 is free for row J + 2
-      if (tid == 0 && issued < NT) issue_row(issued++);
-    }
+    // ---- write the solved slab back (TMA stores; rows past n are clipped)
+    tc::fence_proxy_async_smem();
+    __syncthreads();
     if (tid == 0) {
-      // rows still in flight after an abort (bounded waits): their copies
-      // must land before the CTA's shared memory is released
-      for (int J = consumed; J < issued; ++J) tc::mbar_wait(&barl[J & 1], (uint32_t)((J >> 1) & 1));
-    }
-  }
-  __syncthreads();
-  if (s_ok) {
-    // ---- write the solved slab back (coalesced; rows past n skipped) -----
-#pragma unroll 8
-    for (int e = tid; e < bs * TR; e += NTHR) {
-      const int c = e / TR, r = e % TR;
-      if (r < nrows) A[(size_t)(s + c) * lda + row0 + r] = Xs[c * XLD + r];
+      for (int q = 0; q < RPL; ++q)
+        if (row0 + 32 * q < n) tc::tma_store_2d(&tmapX, Xs + q * bs * 32, row0 + 32 * q, s);
+      tc::bulk_commit();
     }
     // ---- Schur diagonal tracker and switching statistics of the slab -----
-    slab_row_partials(Xs, NT, s_sq, s_rmax, tid);
+    slab_row_partials<TR>(Xs, bs, s_sq, s_rmax, tid);
     __syncthreads();
     if (tid < nrows) {
       const int gi = row0 + tid;
-      const float sq = row_sq(s_sq, NT, tid);
+      const float sq = row_sq<TR>(s_sq, NT, tid);
       rowsq[gi] = sq;
       const float dt = dtilde[gi] - sq;
       dtilde[gi] = dt;
@@ -366,7 +385,7 @@ trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_consta
         next->fp64_diag = 1;
     }
     // ---- column sums of the slab (coherence rule): thread c sums column c
-    // over the slab's rows, starting at row c % 32 so that the 32 threads of
+    // over the slab's rows, starting at row c % TR so that the 32 threads of
     // a warp read 32 different banks (a fixed order per column), and adds it
     // into colacc.  The sums reach colacc as FP64 atomics of FP32 partials,
     // which are exact while a column's partials span less than 2^20 in
@@ -377,7 +396,7 @@ trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_consta
 #pragma unroll 8
         for (int q = 0; q < TR; ++q) {
           const int r = (q + tid) & (TR - 1);
-          cs += (r < nrows) ? Xs[tid * XLD + r] : 0.0f;
+          cs += (r < nrows) ? Xs[xoff(r, tid, bs)] : 0.0f;
         }
         atomicAdd(colacc + tid, (double)cs);
       }
@@ -391,11 +410,15 @@ trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_consta
       for (int q = 0; q < NTHR / TR; ++q) rmax = fmaxf(rmax, s_rmax[q][r]);
       const int gi0 = slab * TR;                         // first trailing row of the slab
       const bool f16 = (qa.cand >> FP16) & 1u, f16x2 = (qa.cand >> FP16X2) & 1u;
-      if (f16 || f16x2) quantize_slab(Xs, bs, nrows, gi0, m, f16x2 ? FP16X2 : FP16, rmax, qa, stage, tid);
-      const int f8[3] = {E4M3, E5M2, MXFP8};
-      for (int i = 0; i < 3; ++i)
-        if ((qa.cand >> f8[i]) & 1u) quantize_slab(Xs, bs, nrows, gi0, m, f8[i], rmax, qa, stage, tid);
+      if (f16 || f16x2)
+        quantize_slab<TR>(Xs, bs, nrows, gi0, m, f16x2 ? FP16X2 : FP16, rmax, qa, stage, tid);
+      // E4M3, E5M2 and the MX-family member of the candidates (at most one:
+      // they share the MX code slot and scales)
+      const int f8[6] = {E4M3, E5M2, MXFP8, MXFP6E2M3, MXFP6E3M2, MXFP4};
+      for (int i = 0; i < 6; ++i)
+        if ((qa.cand >> f8[i]) & 1u) quantize_slab<TR>(Xs, bs, nrows, gi0, m, f8[i], rmax, qa, stage, tid);
     }
+    if (tid == 0) tc::bulk_wait_read();   // the slab's stores are complete before the ticket
   }
   // ---- statistics of the CTA; the last CTA resolves the step --------------
   bm = warp_max(bm);
@@ -454,10 +477,12 @@ trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_consta
 }
 
 // Batched: blockIdx.y = system, blockIdx.x = 32-row slab.  Staging by
-// plain coalesced loads (no per-system tensor maps); the epilogue keeps the
-// row sums of squares (rounding-shift estimate) and the diagonal tracker.
-__global__ void __launch_bounds__(NTHR)
+// plain coalesced loads (no per-system tensor maps), the same slab solve;
+// the epilogue keeps the row sums of squares (rounding-shift estimate) and
+// the diagonal tracker.
+__global__ void __launch_bounds__(NTHR, 1)
 trsm_batched_kernel(BatchSys* __restrict__ sys, int s, int b) {
+  constexpr int TR = 32;
   const BatchSys& S = sys[blockIdx.y];
   const int n = S.n;
   const int bs = min(b, n - s);
@@ -467,15 +492,21 @@ trsm_batched_kernel(BatchSys* __restrict__ sys, int s, int b) {
   extern __shared__ __align__(128) float sm[];
   const int NT = bs / 32;                     // bs == b: only the last block can be partial
   float* Xs = sm;
-  float* Lt = Xs + (size_t)bs * XLD;
+  float* Lt = Xs + (size_t)bs * TR;
   float* Wt = Lt + (size_t)(NT * (NT - 1) / 2) * TSZ;
-  float* red = Wt + (size_t)NT * TSZ;
+  __shared__ __align__(8) uint64_t ready[MAXNT];
+  __shared__ int s_ok;
   const int tid = threadIdx.x;
   const float* A = S.A;
   const int ld = S.ld;
+  if (tid == 0) {
+    s_ok = 1;
+    for (int J = 0; J < NT; ++J) tc::mbar_init(&ready[J], 64);
+    tc::fence_mbar_init();
+  }
   for (int e = tid; e < bs * TR; e += NTHR) {
     const int c = e / TR, r = e % TR;
-    Xs[c * XLD + r] = (r < nrows) ? A[(size_t)(s + c) * ld + row0 + r] : 0.0f;
+    Xs[xoff(r, c, bs)] = (r < nrows) ? A[(size_t)(s + c) * ld + row0 + r] : 0.0f;
   }
   for (int I = 1; I < NT; ++I)
     for (int M = 0; M < I; ++M)
@@ -485,20 +516,57 @@ trsm_batched_kernel(BatchSys* __restrict__ sys, int s, int b) {
       }
   for (int e = tid; e < NT * TSZ; e += NTHR) Wt[e] = S.winv[e];
   __syncthreads();
-  for (int J = 0; J < NT; ++J) trsm_step(Xs, Lt + tl(J, 0) * TSZ, Wt + J * TSZ, red, J, tid);
+  if (!slab_solve<1>(Xs, bs, Lt, Wt, nullptr, ready, tid)) {
+    s_ok = 0;
+    set_status(S.st, MPCHOL_ERR_TIMEOUT, row0);
+  }
+  __syncthreads();
+  if (!s_ok) return;
   for (int e = tid; e < bs * TR; e += NTHR) {
     const int c = e / TR, r = e % TR;
-    if (r < nrows) S.A[(size_t)(s + c) * ld + row0 + r] = Xs[c * XLD + r];
+    if (r < nrows) S.A[(size_t)(s + c) * ld + row0 + r] = Xs[xoff(r, c, bs)];
   }
   __shared__ float s_sq[NTHR / TR][TR];
-  slab_row_partials(Xs, NT, s_sq, nullptr, tid);
+  slab_row_partials<TR>(Xs, bs, s_sq, nullptr, tid);
   __syncthreads();
   if (tid < nrows) {
     const int gi = row0 + tid;
-    const float sq = row_sq(s_sq, NT, tid);
+    const float sq = row_sq<TR>(s_sq, NT, tid);
     S.rowsq[gi] = sq;
     S.dtilde[gi] -= sq;
   }
+}
+
+int sm_count() {
+  static int nsm = 0;
+  if (nsm == 0) {
+    int dev = 0, v = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess)
+      nsm = v;
+    else
+      return 148;
+  }
+  return nsm;
+}
+
+template <int RPL>
+cudaError_t launch_panel(const CUtensorMap& tmapX, const CUtensorMap& tmap32, float* A, int lda,
+                         int n, int s, int bs, const float* winv, const float* d, float* dtilde,
+                         float* rowsq, StepState* step, StepState* next, int next_bs,
+                         const DecisionParams& dp, const QuantAll& qa, DevStatus* st,
+                         cudaStream_t stream, const StepState* prev, double* colacc) {
+  constexpr int TR = 32 * RPL;
+  const int m = n - s - bs;
+  const size_t smem = trsm_smem_floats(TR, bs) * sizeof(float);
+  cudaError_t e = cudaFuncSetAttribute(trsm_panel_kernel<RPL>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)(trsm_smem_floats(TR, 256) * sizeof(float)));
+  if (e != cudaSuccess) return e;
+  trsm_panel_kernel<RPL><<<ceil_div(m, TR), NTHR, smem, stream>>>(
+      tmapX, tmap32, A, lda, n, s, bs, winv, d, dtilde, rowsq, step, next, next_bs, dp, st, qa,
+      prev, colacc);
+  return cudaGetLastError();
 }
 
 }  // namespace
@@ -511,25 +579,26 @@ cudaError_t launch_trsm_panel(const CUtensorMap& tmapX, const CUtensorMap& tmap3
                               double* colacc) {
   const int m = n - s - bs;
   if (m <= 0) return cudaSuccess;
-  const size_t smem = trsm_smem_floats(bs) * sizeof(float);
-  cudaError_t e = cudaFuncSetAttribute(trsm_panel_kernel,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)(trsm_smem_floats(256) * sizeof(float)));
-  if (e != cudaSuccess) return e;
-  trsm_panel_kernel<<<ceil_div(m, TR), NTHR, smem, stream>>>(tmapX, tmap32, A, lda, n, s, bs, winv, d,
-                                                             dtilde, rowsq, step, next, next_bs, dp, st,
-                                                             qa, prev, colacc);
-  return cudaGetLastError();
+  if (bs % 32 != 0 || bs > 32 * MAXNT) return cudaErrorInvalidValue;
+  // 64-row slabs while the panel has more 32-row slabs than the GPU has SMs
+  // (throughput: L11 staged once per 64 rows); 32-row slabs otherwise
+  // (latency: the per-CTA chain is half as long)
+  if (ceil_div(m, 32) > sm_count())
+    return launch_panel<2>(tmapX, tmap32, A, lda, n, s, bs, winv, d, dtilde, rowsq, step, next,
+                           next_bs, dp, qa, st, stream, prev, colacc);
+  return launch_panel<1>(tmapX, tmap32, A, lda, n, s, bs, winv, d, dtilde, rowsq, step, next,
+                         next_bs, dp, qa, st, stream, prev, colacc);
 }
 
 cudaError_t launch_trsm_batched(BatchSys* sys, int nact, int s, int b, int max_m,
                                 cudaStream_t stream) {
   if (nact <= 0 || max_m <= 0) return cudaSuccess;
-  const size_t smem = trsm_batched_smem_floats(b) * sizeof(float);
+  if (b % 32 != 0 || b > 32 * MAXNT) return cudaErrorInvalidValue;
+  const size_t smem = trsm_smem_floats(32, b) * sizeof(float);
   cudaError_t e = cudaFuncSetAttribute(trsm_batched_kernel,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  trsm_batched_kernel<<<dim3(ceil_div(max_m, TR), nact), NTHR, smem, stream>>>(sys, s, b);
+  trsm_batched_kernel<<<dim3(ceil_div(max_m, 32), nact), NTHR, smem, stream>>>(sys, s, b);
   return cudaGetLastError();
 }
 

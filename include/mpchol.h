@@ -59,8 +59,17 @@ typedef enum {
   MPCHOL_PREC_E5M2 = 3,   /* per-row power-of-two scaled E5M2 */
   MPCHOL_PREC_MXFP8 = 4,  /* OCP MX: E4M3 + E8M0 scale per 32 elements along K */
   MPCHOL_PREC_SWITCHING = 5, /* per-step choice by the switching criterion */
-  MPCHOL_PREC_FP16X2 = 6     /* two-term FP16 split (hi + lo, per-row scaled): FP32-class
+  MPCHOL_PREC_FP16X2 = 6,    /* two-term FP16 split (hi + lo, per-row scaled): FP32-class
                                 accuracy on FP16 tensor cores */
+  /* OCP MX with FP6 / FP4 elements (E8M0 scale per 32 elements along K,
+   * scale 2^(floor(log2 amax) - emax_elem), round to nearest even, saturating,
+   * no Inf/NaN codes).  The element values are exactly representable in E4M3
+   * and are stored and multiplied as E4M3 codes by the block-scaled MMA, so
+   * the products are those of FP6/FP4 operands with FP8 storage and speed.
+   * A switching ladder holds at most one MX format (MXFP8 or one of these). */
+  MPCHOL_PREC_MXFP6_E2M3 = 7,   /* u = 2^-4, largest element 7.5 */
+  MPCHOL_PREC_MXFP6_E3M2 = 8,   /* u = 2^-3, largest element 28 */
+  MPCHOL_PREC_MXFP4 = 9         /* E2M1, u = 2^-2, largest element 6 */
 } mpchol_precision;
 
 /* Factorization options.  Field names follow the reference's settings.json
@@ -112,7 +121,7 @@ typedef struct {
   int n_perturbed;     /* pivots raised by diag_pert */
   int nsteps;          /* ceil(n / b) */
   int n_fp64_blocks;   /* diagonal blocks factored in FP64 */
-  int steps_by_prec[7];/* number of trailing updates done in each mpchol_precision */
+  int steps_by_prec[10];/* number of trailing updates done in each mpchol_precision */
 } mpchol_factor_info;
 
 typedef struct {

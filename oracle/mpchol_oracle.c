@@ -31,7 +31,10 @@
 
 /* Format ids shared with include/mpchol.h (MPCHOL_PREC_*). */
 enum { ORC_FP32 = 0, ORC_FP16 = 1, ORC_E4M3 = 2, ORC_E5M2 = 3, ORC_MXFP8 = 4, ORC_SWITCHING = 5,
-       ORC_FP16X2 = 6 };
+       ORC_FP16X2 = 6, ORC_MXFP6E2M3 = 7, ORC_MXFP6E3M2 = 8, ORC_MXFP4 = 9 };
+static int orc_is_mx(int p) {
+  return p == ORC_MXFP8 || p == ORC_MXFP6E2M3 || p == ORC_MXFP6E3M2 || p == ORC_MXFP4;
+}
 
 static inline uint32_t f2u(float x) { uint32_t u; memcpy(&u, &x, 4); return u; }
 static inline float u2f(uint32_t u) { float x; memcpy(&x, &u, 4); return x; }
@@ -179,6 +182,51 @@ static inline float pow2f(int e) {
   return ldexpf(1.0f, e);
 }
 
+/* The OCP MX element formats with FP6/FP4 elements (OCP Microscaling
+ * Formats spec v1.0, element types E2M3, E3M2, E2M1): stored mantissa bits,
+ * smallest normal exponent, largest exponent (the block scale is
+ * floor(log2 amax) - emax) and largest value. */
+static void orc_mx_elem(int p, int* mbits, int* emin, int* emax, float* maxv) {
+  switch (p) {
+    case ORC_MXFP6E2M3: *mbits = 3; *emin = 0; *emax = 2; *maxv = 7.5f; break;
+    case ORC_MXFP6E3M2: *mbits = 2; *emin = -2; *emax = 4; *maxv = 28.0f; break;
+    case ORC_MXFP4: *mbits = 1; *emin = 0; *emax = 2; *maxv = 6.0f; break;
+    default: *mbits = 3; *emin = -6; *emax = 8; *maxv = 448.0f; break;   /* E4M3 */
+  }
+}
+
+/* MX shared exponent of a block for element format p. */
+int orc_mx_scale_exp_fmt(float amax, int p) {
+  int mb, en, ex; float mv;
+  orc_mx_elem(p, &mb, &en, &ex, &mv);
+  if (!(amax > 0.0f) || isinf(amax)) return -127;
+  int e = ilog2f(amax) - ex;
+  if (e < -127) e = -127;
+  if (e > 127) e = 127;
+  return e;
+}
+
+/* Round to nearest even onto an FP6/FP4 element grid, saturating at the
+ * largest value; NaN stays NaN (the formats have no Inf/NaN codes: OCP).
+ * The steps of lo_float's ConvertImpl (src/lo_float.h:1960-2120) restricted
+ * to these targets: the quantum of x's binade (or of the subnormal range)
+ * and RNE of x to a multiple of it.  E4M3 (p = MXFP8) goes through the
+ * E4M3 conversion. */
+float orc_mx_round(float x, int p) {
+  if (p == ORC_MXFP8 || p == ORC_E4M3) return orc_e4m3_to_f32(orc_f32_to_e4m3(x, 1));
+  int mb, en, ex; float mv;
+  orc_mx_elem(p, &mb, &en, &ex, &mv);
+  const float a = fabsf(x);
+  if (a != a) return x;
+  if (a >= mv) return copysignf(mv, x);
+  int e = a > 0.0f ? ilog2f(a) : en;
+  if (e < en) e = en;
+  const float q = pow2f(e - mb);
+  float r = rintf(a / q) * q;          /* exact: q is a power of two; rintf is RNE */
+  if (r > mv) r = mv;
+  return copysignf(r, x);
+}
+
 /* Quantize `count` floats (already scaled) to format `fmt`; used by tests. */
 void orc_quantize(const float* x, void* out, long long count, int fmt) {
   for (long long i = 0; i < count; ++i) {
@@ -251,7 +299,9 @@ typedef struct {
 
 float orc_unit_roundoff(int fmt) {
   switch (fmt) {
-    case ORC_E4M3: case ORC_MXFP8: return 0.0625f;    /* 2^-4 */
+    case ORC_E4M3: case ORC_MXFP8: case ORC_MXFP6E2M3: return 0.0625f;    /* 2^-4 */
+    case ORC_MXFP6E3M2: return 0.125f;                 /* 2^-3 */
+    case ORC_MXFP4: return 0.25f;                      /* 2^-2 */
     case ORC_E5M2: return 0.125f;                     /* 2^-3 */
     case ORC_FP16: return 4.8828125e-4f;               /* 2^-11 */
     case ORC_FP16X2: return 2.3841858e-7f;             /* 2^-22: hi + lo */
@@ -377,15 +427,14 @@ int orc_micro_cholesky(float* A, int n, int ld) {
  * (or, for MXFP8, per-32-block) power-of-two scale; returns dequantized
  * values (exact products of code value and scale) in out[]. */
 static void quant_row(const float* row, int ld, int bs, int p, float* out) {
-  if (p == ORC_MXFP8) {
+  if (orc_is_mx(p)) {
     for (int kb = 0; kb < bs; kb += 32) {
       const int ke = kb + 32 < bs ? kb + 32 : bs;
       float amax = 0.0f;
       for (int k = kb; k < ke; ++k) { float v = fabsf(row[(size_t)k * ld]); if (v > amax) amax = v; }
-      const int e = orc_mx_scale_exp(amax);
+      const int e = orc_mx_scale_exp_fmt(amax, p);
       const float inv = pow2f(-e), sc = pow2f(e);
-      for (int k = kb; k < ke; ++k)
-        out[k] = orc_e4m3_to_f32(orc_f32_to_e4m3(row[(size_t)k * ld] * inv, 1)) * sc;
+      for (int k = kb; k < ke; ++k) out[k] = orc_mx_round(row[(size_t)k * ld] * inv, p) * sc;
     }
     return;
   }

@@ -29,7 +29,8 @@ LIB = HERE / "_build" / "liboracle.so"
 REF_LOFLOAT = HERE / "_ref" / "libref_lofloat.so"
 REF_MICRO = HERE / "_ref" / "libref_micro.so"
 
-FP32, FP16, E4M3, E5M2, MXFP8, SWITCHING, FP16X2 = range(7)
+FP32, FP16, E4M3, E5M2, MXFP8, SWITCHING, FP16X2, MXFP6E2M3, MXFP6E3M2, MXFP4 = range(10)
+MX_FAMILY = (MXFP8, MXFP6E2M3, MXFP6E3M2, MXFP4)
 
 _lib = None
 
@@ -83,6 +84,10 @@ def lib() -> ctypes.CDLL:
         L.orc_row_scale_exp.argtypes = [ctypes.c_float, ctypes.c_int]
         L.orc_mx_scale_exp.restype = ctypes.c_int
         L.orc_mx_scale_exp.argtypes = [ctypes.c_float]
+        L.orc_mx_scale_exp_fmt.restype = ctypes.c_int
+        L.orc_mx_scale_exp_fmt.argtypes = [ctypes.c_float, ctypes.c_int]
+        L.orc_mx_round.restype = ctypes.c_float
+        L.orc_mx_round.argtypes = [ctypes.c_float, ctypes.c_int]
         L.orc_blocked_chol.restype = ctypes.c_int
         L.orc_blocked_chol.argtypes = [fp, ctypes.c_int, ctypes.c_int, fp, fp, fp,
                                        ctypes.POINTER(CholOpts), ctypes.POINTER(ctypes.c_int),
@@ -134,8 +139,16 @@ def row_scale_exp(amax: float, fmt: int) -> int:
     return lib().orc_row_scale_exp(float(amax), fmt)
 
 
-def mx_scale_exp(amax: float) -> int:
-    return lib().orc_mx_scale_exp(float(amax))
+def mx_scale_exp(amax: float, fmt: int = MXFP8) -> int:
+    return lib().orc_mx_scale_exp_fmt(float(amax), fmt)
+
+
+def mx_round(x: np.ndarray, fmt: int) -> np.ndarray:
+    """RNE onto an MX element grid (E4M3, or the OCP FP6/FP4 element
+    formats), saturating; float32 values."""
+    x = np.ascontiguousarray(x, dtype=np.float32).ravel()
+    f = lib().orc_mx_round
+    return np.array([f(float(v), fmt) for v in x], dtype=np.float32)
 
 
 def decode(codes: np.ndarray, fmt: int) -> np.ndarray:
@@ -160,12 +173,17 @@ def quantize_rows(P: np.ndarray, fmt: int) -> tuple[np.ndarray, np.ndarray]:
     E8M0 codes (m x k/32) for MXFP8."""
     P = np.asarray(P, dtype=np.float32)
     m, k = P.shape
-    if fmt == MXFP8:
+    if fmt in MX_FAMILY:
+        # codes: E4M3 codes of the element values (FP6/FP4 values rounded on
+        # their own grid first -- exactly representable in E4M3)
         blocks = np.abs(P).reshape(m, k // 32, 32).max(axis=2)
-        ex = np.vectorize(mx_scale_exp, otypes=[np.int32])(blocks) if blocks.size else \
-            np.zeros((m, k // 32), np.int32)
+        ex = np.vectorize(lambda a: mx_scale_exp(a, fmt), otypes=[np.int32])(blocks) \
+            if blocks.size else np.zeros((m, k // 32), np.int32)
         inv = np.ldexp(np.float32(1.0), -np.repeat(ex, 32, axis=1)).astype(np.float32)
-        codes = quantize((P * inv).astype(np.float32), E4M3).reshape(m, k)
+        xs = (P * inv).astype(np.float32)
+        if fmt != MXFP8:
+            xs = mx_round(xs, fmt).reshape(m, k)
+        codes = quantize(xs, E4M3).reshape(m, k)
         return codes, (ex + 127).astype(np.uint8)
     amax = np.abs(P).max(axis=1) if k else np.zeros(m, np.float32)
     ex = np.array([row_scale_exp(a, fmt) for a in amax], dtype=np.int32)
@@ -192,6 +210,20 @@ def ref_lofloat(x: np.ndarray, fmt: int, saturate: bool = True) -> np.ndarray:
     x = np.ascontiguousarray(x, dtype=np.float32).ravel()
     out = np.empty(x.size, dtype=np.uint8)
     fn(_fptr(x), out.ctypes.data_as(ctypes.c_void_p), x.size, int(saturate))
+    return out
+
+
+def ref_lofloat_small(x: np.ndarray, fmt: int) -> np.ndarray:
+    """The reference lo_float's saturating RNE conversion of float32 x to
+    float6_e2m3 (MXFP6E2M3), float6_e3m2 (MXFP6E3M2) or float4_e2m1 (MXFP4),
+    as float32 values."""
+    L = ctypes.CDLL(str(REF_LOFLOAT))
+    fn = {MXFP6E2M3: L.ref_lofloat_f6e2m3, MXFP6E3M2: L.ref_lofloat_f6e3m2,
+          MXFP4: L.ref_lofloat_f4e2m1}[fmt]
+    fn.argtypes = [ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float), ctypes.c_longlong]
+    x = np.ascontiguousarray(x, dtype=np.float32).ravel()
+    out = np.empty(x.size, dtype=np.float32)
+    fn(_fptr(x), _fptr(out), x.size)
     return out
 
 

@@ -53,7 +53,8 @@ def test_default_options():
 @pytest.mark.parametrize("kw,status", [
     (dict(block_size=100), _lib.ERR_BAD_ARG),
     (dict(block_size=512), _lib.ERR_BAD_ARG),
-    (dict(precision=9), _lib.ERR_BAD_ARG),
+    (dict(precision=10), _lib.ERR_BAD_ARG),
+    (dict(precision="switching", ladder=["mxfp8", "mxfp4"]), _lib.ERR_NOT_SUPPORTED),
     (dict(left=2), _lib.ERR_BAD_ARG),
     (dict(coherence=2), _lib.ERR_BAD_ARG),
     (dict(equilibrate=-1), _lib.ERR_BAD_ARG),

@@ -182,3 +182,31 @@ def test_reference_literal_switching_mode_matches_oracle(cuda):
     Lg = f.lower().cpu().numpy()
     err = np.linalg.norm(Lg - forced["L"]) / np.linalg.norm(forced["L"])
     assert err < 5e-2
+
+
+@pytest.mark.parametrize("low", ["mxfp6e2m3", "mxfp6e3m2", "mxfp4"])
+def test_fp6_fp4_steps_on_the_kernel_matrix(cuda, rbf2048, low):
+    """FP6/FP4 trailing updates (OCP MX element formats) in a switching
+    ladder on the RBF matrix: the GPU's decisions are the oracle's, the factor
+    matches its restatement, and PCG wins the factor back to 1e-10."""
+    A = rbf2048
+    n = A.shape[0]
+    f = mp.factor(torch.from_numpy(A).cuda(), block_size=256, precision="switching",
+                  eps_prime=2.0, eps_coherence=0.25, ladder=[low, "fp16", "fp16x2"])
+    ref, info = oracle_factor(A, f, force=False)
+    assert info.status == 0 and ref["status"] == 0
+    assert list(ref["step_prec"][:-1]) == info.step_prec[:-1]
+    lowid = _lib.PREC_BY_NAME[low]
+    nlow = sum(p == lowid for p in info.step_prec[:-1])
+    Lg = f.lower().cpu().numpy()
+    err = np.linalg.norm(Lg - ref["L"]) / np.linalg.norm(ref["L"])
+    B = matgen.rhs(n, 2, 5).numpy()
+    Ad = torch.from_numpy(A).cuda()
+    X, rep = f.pcg(Ad, torch.from_numpy(B).cuda(), rel_tol=1e-10, max_it=300)
+    _, it_o, _ = O.pcg(A, ref["L"], B, 1e-10, 300)
+    print(f"{low}: steps {info.step_prec[:-1]} ({nlow} {low}), factor err {err:.2e}, "
+          f"it {rep.iterations} (oracle {it_o})")
+    assert nlow >= 1
+    assert err < 5e-2
+    assert rep.converged and rep.rel_residual <= 1e-10
+    assert abs(rep.iterations - it_o) <= max(3, it_o // 4)

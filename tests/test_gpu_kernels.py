@@ -72,14 +72,14 @@ def gpu_quantize_rows(P: np.ndarray, fmt: int):
     half = fmt in (O.FP16, O.FP16X2)
     q = torch.zeros(m * k * (2 if fmt == O.FP16X2 else 1), dtype=torch.int16 if half else torch.uint8,
                     device="cuda")
-    sc = torch.zeros(m * (k // 32 if fmt == O.MXFP8 else 1), dtype=torch.uint8, device="cuda")
+    sc = torch.zeros(m * (k // 32 if fmt in O.MX_FAMILY else 1), dtype=torch.uint8, device="cuda")
     _lib.check(lib.mpchol_quantize_rows(Pd.data_ptr(), m, k, m, fmt, q.data_ptr(), sc.data_ptr(),
                                         stream()))
     codes = q.cpu().numpy().reshape(-1, k)
     if half:
         codes = codes.view(np.uint16)
     s = sc.cpu().numpy()
-    s = s.reshape(m, k // 32) if fmt == O.MXFP8 else s.view(np.int8)
+    s = s.reshape(m, k // 32) if fmt in O.MX_FAMILY else s.view(np.int8)
     return codes, s
 
 
@@ -229,3 +229,40 @@ def test_fused_panel_codes_match_oracle(cuda, n):
         bad = np.nonzero(codes != wc)
         assert bad[0].size == 0, (fmt, bad[0][:5], bad[1][:5])
         assert np.array_equal(scales.astype(np.int32), ws.astype(np.int32)), fmt
+
+
+@pytest.mark.parametrize("fmt", [O.MXFP6E2M3, O.MXFP6E3M2, O.MXFP4])
+@pytest.mark.parametrize("m,k", [(300, 256), (129, 128)])
+def test_fp6_fp4_quantize_rows_matches_oracle(cuda, fmt, m, k):
+    """MX quantization with FP6/FP4 elements: block scales 2^(floor(log2
+    amax) - emax_elem) and the element values (E4M3 codes of the
+    FP6/FP4-rounded values) equal the oracle's bit for bit."""
+    P = panel(m, k, 11 + k)
+    codes, s = gpu_quantize_rows(P, fmt)
+    wc, ws = O.quantize_rows(P, fmt)
+    assert np.array_equal(s.astype(np.int64), ws.astype(np.int64))
+    assert np.array_equal(codes, wc)
+
+
+@pytest.mark.parametrize("fmt", [O.MXFP6E2M3, O.MXFP6E3M2, O.MXFP4])
+def test_fp6_fp4_syrk_matches_oracle(cuda, fmt):
+    """The trailing update with FP6/FP4 element values through the
+    block-scaled E4M3 MMA equals the FP64 product of the dequantized panel."""
+    lib = _lib.load()
+    m, k = 700, 256
+    P = panel(m, k, 21)
+    codes, s = gpu_quantize_rows(P, fmt)
+    g = np.random.default_rng(22)
+    C = g.standard_normal((m, m)).astype(np.float32)
+    Cd = torch.from_numpy(C.T.copy()).cuda()
+    # the operands stay referenced until the update has run (a temporary's
+    # device memory could be handed to the next allocation meanwhile)
+    Qd = torch.from_numpy(codes).cuda()
+    Sd = torch.from_numpy(s.view(np.uint8)).cuda()
+    _lib.check(lib.mpchol_syrk_update(Cd.data_ptr(), m, m, k, fmt, Qd.data_ptr(), Sd.data_ptr(),
+                                      None, 0, stream()))
+    got = Cd.cpu().numpy().T
+    want = syrk_ref(C, codes, s, O.MXFP8, m, k)
+    low = np.tril(np.ones((m, m), bool))
+    err = np.abs(got[low] - want[low]).max() / np.abs(want[low]).max()
+    assert err < 2e-4, err

@@ -78,6 +78,34 @@ def test_switching_decisions_match_oracle_rule(cuda):
     np.testing.assert_allclose(dt.cpu().numpy(), ref["dtilde"], rtol=1e-3, atol=2e-5)
 
 
+def test_factor_matches_oracle_at_full_c2_size(cuda):
+    """The C2 configuration at its full size: n = 8192, kappa = 1e6 (seed 3),
+    block 256, switching {E4M3, FP16, FP16X2} at eps' = 1e-5 -- the bench's
+    spd line.  The oracle (OpenMP restatement on the host cores) re-derives
+    every step's precision on its own and restates the factor; PCG on the GPU
+    reaches 1e-10 in the oracle PCG's iteration count on the GPU's factor."""
+    n, b = 8192, 256
+    A = matgen.spd_matrix(n, 1e6, 3).numpy()
+    opts = dict(block_size=b, precision="switching", eps_prime=1e-5,
+                ladder=["e4m3", "fp16", "fp16x2"])
+    f, info, ref, err = factor_parity(A, **opts)
+    kw = O.factor_kwargs(f.opts)
+    own = O.blocked_chol(A, **kw)
+    assert info.status == 0 and own["status"] == 0
+    assert list(own["step_prec"][:-1]) == info.step_prec[:-1]
+    print(f"C2 n={n}: steps {set(info.step_prec[:-1])}, rel Frobenius vs oracle {err:.2e}")
+    # FP16X2 steps at kappa = 1e6: two FP32-class factorizations differ by
+    # about kappa(L) * u32 in the last blocks
+    assert err < 1e-3
+    B = matgen.rhs(n, 1, 100).numpy()
+    Ad = torch.from_numpy(A).cuda()
+    X, rep = f.pcg(Ad, torch.from_numpy(B).cuda(), rel_tol=1e-10, max_it=100)
+    assert rep.converged and rep.rel_residual <= 1e-10
+    _, it_o, _ = O.pcg(A, f.lower().cpu().numpy(), B, 1e-10, 100)
+    print(f"  pcg it={rep.iterations} (oracle {it_o}) rel={rep.rel_residual:.2e}")
+    assert abs(rep.iterations - it_o) <= 1
+
+
 def test_not_spd_reports_failing_row(cuda):
     A = matgen.spd_matrix(512, 10.0, 4).numpy()
     A[300, 300] = -1.0

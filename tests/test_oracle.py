@@ -177,3 +177,31 @@ def test_rbf_oracle_gradients_match_central_differences():
         E[i, k] = h
         fd = (L(X + E, ell, lam) - L(X - E, ell, lam)) / (2 * h)
         assert abs(fd - dX[i, k]) <= 1e-6 * max(abs(dX[i, k]), 1e-3)
+
+
+@pytest.mark.parametrize("fmt,name", [(O.MXFP6E3M2, "f6e3m2"), (O.MXFP4, "f4e2m1"),
+                                      (O.MXFP6E2M3, "f6e2m3")])
+def test_fp6_fp4_element_rounding_matches_lo_float(fmt, name):
+    """The oracle's FP6/FP4 element rounding (OCP E2M3, E3M2, E2M1: RNE,
+    saturating) against the reference lo_float's float6_e2m3 / float6_e3m2 /
+    float4_e2m1 conversions (golden vectors).  lo_float reserves two codes
+    the OCP formats use as numbers: float4_e2m1's -0 (0x8) and float6_e2m3's
+    +-7.0 (0x1e, 0x3e) are NaN there.  Where lo_float returns that NaN for a
+    finite input, the oracle must return the OCP value (-0 or +-7.0);
+    everywhere else the two agree exactly."""
+    g = np.load(GOLDEN)
+    x = g["small_inputs"].view(np.float32)
+    want = g[name]
+    got = O.mx_round(x, fmt)
+    fin = np.isfinite(x)
+    assert np.all(np.isnan(got[np.isnan(x)]))
+    special = fin & np.isnan(want)
+    if fmt == O.MXFP4:
+        assert np.all(got[special] == 0.0) and np.all(np.signbit(got[special]))
+    elif fmt == O.MXFP6E2M3:
+        assert np.all(np.abs(got[special]) == 7.0)
+    else:
+        assert not special.any()
+    ok = fin & ~special
+    assert np.array_equal(got[ok], want[ok])
+    assert ok.sum() > 25000
