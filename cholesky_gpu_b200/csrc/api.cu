@@ -168,7 +168,7 @@ struct mpchol_factor {
   StepState* steps = nullptr;
   DevStatus* status = nullptr;    // the factorization's status word
   DevStatus* pstatus = nullptr;   // the solves' status word (breakdown, timeouts)
-  double* colacc = nullptr;       // coherence rule: each step's panel column sums (b per step)
+  double* colacc = nullptr;       // coherence rule: each step's panel column sums (kColCopies x b per step)
   int8_t* eqexp = nullptr;        // equilibration exponents e_i (row i scaled by 2^-e_i)
   // solve side
   float* wsup = nullptr;      // inverses of the 1024-row diagonal super-blocks
@@ -468,7 +468,8 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream, const CopyPlan
   MPCHOL_CUDA_TRY(cudaMemsetAsync(f->steps, 0, sizeof(StepState) * (f->nsteps + 1), stream));
   MPCHOL_CUDA_TRY(cudaMemsetAsync(f->sh, 0, sizeof(float) * n, stream));
   if (dp.coherence)
-    MPCHOL_CUDA_TRY(cudaMemsetAsync(f->colacc, 0, sizeof(double) * (size_t)f->nsteps * b, stream));
+    MPCHOL_CUDA_TRY(cudaMemsetAsync(f->colacc, 0, sizeof(double) * (size_t)f->nsteps * kColCopies * b,
+                                    stream));
   if (streamed) {
     MPCHOL_CUDA_TRY(cudaStreamWaitEvent(stream, f->ev_grp[0], 0));
   } else {
@@ -579,7 +580,7 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream, const CopyPlan
             launch_trsm_panel(f->tmapX, f->tmap32, f->A, ld, n, s, bs, f->winv, f->d, f->dtilde,
                               f->rowsq, &f->steps[k], &f->steps[k + 1], std::min(b, m), dp, qa,
                               f->status, stream, k > 0 ? &f->steps[k - 1] : nullptr,
-                              dp.coherence ? f->colacc + (size_t)k * b : nullptr));
+                              dp.coherence ? f->colacc + (size_t)k * kColCopies * b : nullptr));
     }
     if (o.equilibrate)
       PHASE(MPCHOL_PH_SETUP, 1, stream, launch_equil_scale(f->A, ld, n, f->eqexp, 0, n, true, stream));
@@ -607,7 +608,7 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream, const CopyPlan
           launch_trsm_panel(f->tmapX, f->tmap32, f->A, ld, n, s, bs, f->winv, f->d, f->dtilde,
                             f->rowsq, &f->steps[k], &f->steps[k + 1], next_bs, dp, qa, f->status,
                             stream, k > 0 ? &f->steps[k - 1] : nullptr,
-                            dp.coherence ? f->colacc + (size_t)k * b : nullptr));
+                            dp.coherence ? f->colacc + (size_t)k * kColCopies * b : nullptr));
     // groups joining at this step catch up with panels 0 .. k-1 (aux is
     // already ordered after those panels and after the previous rest)
     bool caught = false, head_waits = false;
@@ -1208,7 +1209,7 @@ mpchol_status mpchol_factor_create(const mpchol_opts* opts, int n, mpchol_factor
             dmalloc(&f->mxexp, (size_t)n * (f->b / 32)) == cudaSuccess &&
             dmalloc(&f->steps, f->nsteps + 1) == cudaSuccess &&
             dmalloc(&f->status, 1) == cudaSuccess && dmalloc(&f->pstatus, 1) == cudaSuccess &&
-            dmalloc(&f->colacc, (size_t)f->nsteps * f->b) == cudaSuccess &&
+            dmalloc(&f->colacc, (size_t)f->nsteps * kColCopies * f->b) == cudaSuccess &&
             dmalloc(&f->eqexp, n) == cudaSuccess &&
             dmalloc(&f->wsup, solve_wsup_elems(n)) == cudaSuccess &&
             dmalloc(&f->trsv_ctr, trsv_counter_ints(n)) == cudaSuccess &&

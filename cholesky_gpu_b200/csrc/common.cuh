@@ -101,16 +101,16 @@ __device__ __forceinline__ int mx_scale_exp(float amax, int fmt = MXFP8) {
 }
 
 // Round-to-nearest-even onto an FP6/FP4 element grid (OCP: no Inf/NaN codes,
-// saturating at the largest value; NaN stays NaN).  x / q and r * q are
-// exact: q is a power of two and x lies far inside the FP32 range.
+// saturating at the largest value; NaN stays NaN).  a / q = a * 2^(mbits - e)
+// and r * q are exact: q is a power of two and a lies far inside the FP32
+// range.
 __device__ __forceinline__ float mx_round_elem(float x, const MxElem& m) {
   const float a = fabsf(x);
   if (!(a == a)) return x;
   if (a >= m.maxv) return copysignf(m.maxv, x);
   int e = (a > 0.0f) ? ilog2f_dev(a) : m.emin;
   if (e < m.emin) e = m.emin;
-  const float q = pow2f(e - m.mbits);
-  return copysignf(fminf(rintf(a / q) * q, m.maxv), x);
+  return copysignf(fminf(rintf(a * pow2f(m.mbits - e)) * pow2f(e - m.mbits), m.maxv), x);
 }
 
 // Hardware RNE + satfinite conversions (cvt.rn.satfinite.{e4m3,e5m2}x2.f32).

@@ -80,8 +80,10 @@ __host__ __device__ inline int rexp_slot(int fmt) { return fmt == E4M3 ? 0 : (fm
 // its rows (prev null: first step); the rows of the next diagonal block get
 // theirs in its POTRF.  tmapX: TMA map over A with 32 x bs boxes; tmap32 as
 // for launch_potrf.
-// colacc (coherence rule, nullable otherwise): bs FP64 accumulators, zeroed
-// before the launch, that receive the panel's column sums.
+// colacc (coherence rule, nullable otherwise): kColCopies x bs FP64
+// accumulators, zeroed before the launch, that receive the panel's column
+// sums (slab i adds into copy i % kColCopies).
+constexpr int kColCopies = 8;
 cudaError_t launch_trsm_panel(const CUtensorMap& tmapX, const CUtensorMap& tmap32, float* A,
                               int lda, int n, int s, int bs, const float* winv, const float* d,
                               float* dtilde, float* rowsq, StepState* step, StepState* next,

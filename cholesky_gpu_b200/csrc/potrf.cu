@@ -44,6 +44,40 @@ __device__ __forceinline__ float drsqrt<float>(float x) { return rsqrtf(x); }
 template <>
 __device__ __forceinline__ double drsqrt<double>(double x) { return rsqrt(x); }
 
+// The pivot rule of column k, evaluated by every lane on its own candidate
+// (no divergent branch on the chain; lane k's value is the pivot).
+template <typename T>
+struct Pivot {
+  T piv, r;        // repaired pivot and 1/sqrt(piv)
+  bool pert, bad;  // repaired by the floor; failed (non-positive without repair, or not finite)
+};
+template <typename T>
+__device__ __forceinline__ Pivot<T> eval_pivot(T cand, bool real, T my_shift, T my_pmin,
+                                               int diag_pert) {
+  Pivot<T> p;
+  T piv = real ? cand + my_shift : T(1);
+  // a NaN or infinite pivot means the Schur complement has overflowed
+  // (earlier pivots floored far below the rounding error of a low-precision
+  // update): no repair makes that factor usable, so it fails as NOT_SPD
+  const bool nonfin = real && !(piv - piv == T(0));
+  p.pert = false;
+  p.bad = nonfin;
+  if (diag_pert) {
+    // repair: max(|pivot|, floor), the reference's fixDiag rule
+    // (src/kernels_macros.cuh:90-99)
+    p.pert = real && !nonfin && !(piv > my_pmin);
+    const T ap = piv < T(0) ? -piv : piv;
+    piv = p.pert ? (ap > my_pmin ? ap : my_pmin) : piv;
+  } else {
+    p.bad = p.bad || (real && !(piv > T(0)));
+  }
+  p.piv = p.bad ? T(1) : piv;   // keep the arithmetic finite; the caller discards the result
+  // one SFU reciprocal square root on the dependency chain:
+  // r = 1/sqrt(piv), L(k,k) = piv * r
+  p.r = drsqrt<T>(p.piv);
+  return p;
+}
+
 // Factor the 32 x 32 tile t in place (lower triangle).  inv[k] receives
 // 1 / L(k,k).  Returns false on a non-positive pivot when pivot flooring is
 // off (first failing local row in *fail_row).
@@ -64,42 +98,24 @@ __device__ bool factor_diag_tile(T* t, T* inv, int lane, int nreal, const T* shi
   const T my_pmin = pmin[lane];
   bool failed = false, perturbed = false;
   T my_inv = T(1);
-  // dnext: the next pivot candidate, formed by lane k+1 from its own
-  // multiplier (the same fma the rank-1 update applies to a[k+1]), so the
-  // pivot chain does not wait on the update's shared-memory round trip
-  T dnext = a[0];
+  // The pivot of column k + 1 is lane k + 1's candidate a[k+1] - L(k+1,k)^2
+  // (the same fma the rank-1 update applies to a[k+1]); it is evaluated,
+  // square-rooted and broadcast before column k's multipliers go through
+  // shared memory, so the pivot chain and the update's round trip overlap.
+  Pivot<T> pv = eval_pivot<T>(a[0], 0 < nreal, my_shift, my_pmin, diag_pert);
+  T rk = __shfl_sync(0xffffffffu, pv.r, 0);
 #pragma unroll
   for (int k = 0; k < TS; ++k) {
-    // every lane evaluates the pivot rule on its own candidate (no divergent
-    // branch on the chain); lane k's value is the pivot, broadcast as 1/sqrt
-    const bool real = k < nreal;   // identity padding beyond the real block
-    T piv = real ? dnext + my_shift : T(1);
-    // a NaN or infinite pivot means the Schur complement has overflowed
-    // (earlier pivots floored far below the rounding error of a low-precision
-    // update): no repair makes that factor usable, so it fails as NOT_SPD
-    const bool nonfin = real && !(piv - piv == T(0));
-    bool pert = false, bad = nonfin;
-    if (diag_pert) {
-      // repair: max(|pivot|, floor), the reference's fixDiag rule
-      // (src/kernels_macros.cuh:90-99)
-      pert = real && !nonfin && !(piv > my_pmin);
-      const T ap = piv < T(0) ? -piv : piv;
-      piv = pert ? (ap > my_pmin ? ap : my_pmin) : piv;
-    } else {
-      bad = bad || (real && !(piv > T(0)));
-    }
-    piv = bad ? T(1) : piv;   // keep the arithmetic finite; the caller discards the result
-    // one SFU reciprocal square root on the dependency chain:
-    // r = 1/sqrt(piv), L(k,k) = piv * r
-    const T r = drsqrt<T>(piv);
-    const T rk = __shfl_sync(0xffffffffu, r, k);
     const bool mine = lane == k;
-    perturbed = perturbed || (mine && pert);
-    failed = failed || (mine && bad);
-    my_inv = mine ? r : my_inv;
+    perturbed = perturbed || (mine && pv.pert);
+    failed = failed || (mine && pv.bad);
+    my_inv = mine ? pv.r : my_inv;
     const T lik = (lane > k) ? a[k] * rk : T(0);
-    a[k] = mine ? piv * r : ((lane > k) ? lik : a[k]);
-    if (k + 1 < TS) dnext = fma(-lik, lik, a[k + 1]);
+    a[k] = mine ? pv.piv * pv.r : ((lane > k) ? lik : a[k]);
+    if (k + 1 < TS) {
+      pv = eval_pivot<T>(fma(-lik, lik, a[k + 1]), k + 1 < nreal, my_shift, my_pmin, diag_pert);
+      rk = __shfl_sync(0xffffffffu, pv.r, k + 1);
+    }
     // two multiplier buffers used in turn: the next column's write cannot
     // overtake a lane still reading this one, so one warp barrier suffices
     T* cb = col + (k & 1) * TS;

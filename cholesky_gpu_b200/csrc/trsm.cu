@@ -11,8 +11,10 @@
 // and all of L11: the strictly-lower 32 x 32 tiles L_{J,M} as 2-D boxes and
 // the inverses of the diagonal tiles L_JJ, which the POTRF kernel wrote, as
 // 1-D bulk copies, one mbarrier per tile row.  The solve is a pipeline over
-// the 32-column tiles J of the slab, a warp pair per tile (each warp 16 of its
-// columns, each lane one or two rows):
+// the 32-column tiles J of the slab, a warp pair per tile (each thread a
+// register block of 4 or 8 rows x 4 columns, so a k step reads two or three
+// 16-byte vectors for 16 or 32 FMAs; the shared-memory return path, not the
+// FMA rate, bounds these small products):
 //   X_J = (A_J - sum_{K<J} X_K L_{J,K}^T) L_JJ^-T,
 // where the pair of tile J applies X_K as soon as the pair of tile K has
 // published it (an mbarrier per tile, bounded waits), so the only chain is
@@ -60,13 +62,6 @@ size_t trsm_smem_floats(int tr, int bs) {
   return (size_t)bs * tr + std::max(lw, stage_words(tr, bs));
 }
 
-__device__ __forceinline__ void load16(const float* p, float (&v)[16]) {
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const float4 w = reinterpret_cast<const float4*>(p)[q];
-    v[4 * q] = w.x; v[4 * q + 1] = w.y; v[4 * q + 2] = w.z; v[4 * q + 3] = w.w;
-  }
-}
 __device__ __forceinline__ void pair_sync(int J) {   // the two warps of tile column J
   asm volatile("bar.sync %0, 64;" ::"r"(J + 1) : "memory");
 }
@@ -74,14 +69,20 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tc::smem_u32(bar)) : "memory");
 }
 
-// The slab solve.  Warp w works on tile column J = w / 2, columns
-// 16 (w % 2) .. +15 of it, and lane l on slab rows l (and l + 32 when RPL =
-// 2).  Lt: L11's tiles L_{I,M} (I > M) at tl(I, M) * TSZ; Wt: the inverses
-// W_JJ = L_JJ^-1, tile J at J * TSZ; both column-major (L(c, m) at m * 32 + c,
-// W(c, m) zero for m > c).  lrow[J] (null: already staged) completes when
-// tile row J has landed; ready[J] (64 arrivals) when X_J is final.  Each
-// output is one fma chain in a fixed order: the update over K, then m; the
-// diagonal multiply over m.  Returns false if a bounded wait gave up.
+// The slab solve.  The warp pair of tile column J (warps 2J, 2J + 1; w = 2J +
+// h) computes the TR x 32 tile X_J: thread t of the pair (t = 32 h + lane)
+// holds a block of 4 RPL rows x 4 columns in registers, rows 4 rg .. 4 rg + 3
+// of each 32-row half (rg = t % 8) and columns 4 cg .. 4 cg + 3 (cg = t / 8),
+// so every k step of the tile products reads 16-byte vectors of X (one per
+// half) and of L (one), and a quarter-warp's eight X vectors are 128
+// contiguous bytes.  Lt: L11's tiles L_{I,M} (I > M) at tl(I, M) * TSZ; Wt:
+// the inverses W_JJ = L_JJ^-1, tile J at J * TSZ; both column-major (L(c, m)
+// at m * 32 + c, W(c, m) zero for m > c).  lrow[J] (null: already staged)
+// completes when tile row J has landed; ready[J] (64 arrivals) when X_J is
+// final:
+//   X_J = (A_J - sum_{K<J} X_K L_{J,K}^T) W_JJ^T.
+// Each output is one fma chain in a fixed order: the update over K, then m;
+// the diagonal multiply over m.  Returns false if a bounded wait gave up.
 template <int RPL>
 __device__ bool slab_solve(float* Xs, int bs, const float* Lt, const float* Wt, uint64_t* lrow,
                            uint64_t* ready, int tid) {
@@ -90,62 +91,77 @@ __device__ bool slab_solve(float* Xs, int bs, const float* Lt, const float* Wt, 
   const int J = warp >> 1, h = warp & 1;
   if (J >= NT) return true;
   const int XH = bs * 32;                              // floats per 32-row half
+  const int t = 32 * h + lane;
+  const int rg = t & 7, cg = t >> 3;
+  const int r0 = 4 * rg;                               // rows r0.. of each half
+  const int cl = 4 * cg;                               // columns cl.. of the tile
   bool ok = lrow == nullptr || tc::mbar_wait(&lrow[J], 0);
-  const int c0 = 32 * J + 16 * h;                      // first slab column of the warp
-  float acc[RPL][16];
+  float acc[RPL][4][4];                                // [half][row][column]
 #pragma unroll
   for (int q = 0; q < RPL; ++q)
 #pragma unroll
-    for (int u = 0; u < 16; ++u) acc[q][u] = Xs[q * XH + (c0 + u) * 32 + lane];
+    for (int j = 0; j < 4; ++j) {
+      const float4 v = *reinterpret_cast<const float4*>(Xs + q * XH + (32 * J + cl + j) * 32 + r0);
+      acc[q][0][j] = v.x; acc[q][1][j] = v.y; acc[q][2][j] = v.z; acc[q][3][j] = v.w;
+    }
 #pragma unroll 1
   for (int K = 0; K < J; ++K) {
     ok = tc::mbar_wait(&ready[K], 0) && ok;
-    const float* L = Lt + (size_t)tl(J, K) * TSZ + 16 * h;
-    const float* xk = Xs + 32 * K * 32 + lane;
-#pragma unroll 4
+    const float* L = Lt + (size_t)tl(J, K) * TSZ + cl;
+    const float* xk = Xs + 32 * K * 32 + r0;
+#pragma unroll 8
     for (int m = 0; m < 32; ++m) {
-      float x[RPL];
+      const float4 lv = *reinterpret_cast<const float4*>(L + m * 32);
+      const float l[4] = {lv.x, lv.y, lv.z, lv.w};
 #pragma unroll
-      for (int q = 0; q < RPL; ++q) x[q] = xk[q * XH + m * 32];
-      float l[16];
-      load16(L + m * 32, l);
+      for (int q = 0; q < RPL; ++q) {
+        const float4 xv = *reinterpret_cast<const float4*>(xk + q * XH + m * 32);
+        const float x[4] = {xv.x, xv.y, xv.z, xv.w};
 #pragma unroll
-      for (int q = 0; q < RPL; ++q)
+        for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int u = 0; u < 16; ++u) acc[q][u] = fmaf(-x[q], l[u], acc[q][u]);
+          for (int j = 0; j < 4; ++j) acc[q][i][j] = fmaf(-x[i], l[j], acc[q][i][j]);
+      }
     }
   }
-  // both halves of the updated tile into the slab, then X_J = Y W_JJ^T
+  // the updated tile into the slab, then X_J = Y W_JJ^T
+  float* xj = Xs + 32 * J * 32 + r0;
 #pragma unroll
   for (int q = 0; q < RPL; ++q)
 #pragma unroll
-    for (int u = 0; u < 16; ++u) Xs[q * XH + (c0 + u) * 32 + lane] = acc[q][u];
+    for (int j = 0; j < 4; ++j)
+      *reinterpret_cast<float4*>(xj + q * XH + (cl + j) * 32) =
+          make_float4(acc[q][0][j], acc[q][1][j], acc[q][2][j], acc[q][3][j]);
   pair_sync(J);
-  const float* W = Wt + (size_t)J * TSZ + 16 * h;
-  const float* y = Xs + 32 * J * 32 + lane;
-  float o[RPL][16];
+  const float* W = Wt + (size_t)J * TSZ + cl;
 #pragma unroll
   for (int q = 0; q < RPL; ++q)
 #pragma unroll
-    for (int u = 0; u < 16; ++u) o[q][u] = 0.0f;
-  const int mend = 16 * h + 16;                        // W(c, m) = 0 for m > c
-#pragma unroll 4
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[q][i][j] = 0.0f;
+  const int mend = 16 * h + 16;                        // W(c, m) = 0 for m > c (the warp's columns)
+#pragma unroll 8
   for (int m = 0; m < mend; ++m) {
-    float yv[RPL];
+    const float4 wv = *reinterpret_cast<const float4*>(W + m * 32);
+    const float w[4] = {wv.x, wv.y, wv.z, wv.w};
 #pragma unroll
-    for (int q = 0; q < RPL; ++q) yv[q] = y[q * XH + m * 32];
-    float w[16];
-    load16(W + m * 32, w);
+    for (int q = 0; q < RPL; ++q) {
+      const float4 yv = *reinterpret_cast<const float4*>(xj + q * XH + m * 32);
+      const float y[4] = {yv.x, yv.y, yv.z, yv.w};
 #pragma unroll
-    for (int q = 0; q < RPL; ++q)
+      for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int u = 0; u < 16; ++u) o[q][u] = fmaf(yv[q], w[u], o[q][u]);
+        for (int j = 0; j < 4; ++j) acc[q][i][j] = fmaf(y[i], w[j], acc[q][i][j]);
+    }
   }
   pair_sync(J);                                        // every read of Y is done
 #pragma unroll
   for (int q = 0; q < RPL; ++q)
 #pragma unroll
-    for (int u = 0; u < 16; ++u) Xs[q * XH + (c0 + u) * 32 + lane] = o[q][u];
+    for (int j = 0; j < 4; ++j)
+      *reinterpret_cast<float4*>(xj + q * XH + (cl + j) * 32) =
+          make_float4(acc[q][0][j], acc[q][1][j], acc[q][2][j], acc[q][3][j]);
   mbar_arrive(&ready[J]);                              // release: X_J to the later tiles
   return ok;
 }
@@ -178,6 +194,60 @@ __device__ __forceinline__ float row_sq(float (*s_sq)[TR], int NT, int r) {
   float sq = s_sq[0][r];
   for (int q = 1; q < NT; ++q) sq += s_sq[q][r];
   return sq;
+}
+
+// Two elements as 8-bit codes of format FMT (already scaled): E4M3 / E5M2
+// by the hardware conversion; the FP6/FP4 MX elements rounded onto their
+// grid first (the rounded value is exact in E4M3).
+template <int FMT>
+__device__ __forceinline__ uint32_t code8_x2(float a, float b) {
+  if constexpr (FMT == E5M2) return f32x2_to_e5m2x2(a, b);
+  else if constexpr (FMT == E4M3 || FMT == MXFP8) return f32x2_to_e4m3x2(a, b);
+  else {
+    const MxElem me = mx_elem(FMT);
+    return f32x2_to_e4m3x2(mx_round_elem(a, me), mx_round_elem(b, me));
+  }
+}
+
+// 8-bit codes of thread (r, part)'s 32-column block in format FMT into the
+// staging panel (row stride bs/4 + 1 words): the block's values are read once
+// into registers; an MX format takes the block's own E8M0 scale, the others
+// the row's power-of-two scale (from the row maximum rmax).
+template <int TR, int FMT>
+__device__ __forceinline__ void stage_codes8(const float* Xs, int bs, int nrows, int gi0, float rmax,
+                                             const QuantAll& qa, uint32_t* stage, int tid) {
+  constexpr bool MX = FMT == MXFP8 || FMT == MXFP6E2M3 || FMT == MXFP6E3M2 || FMT == MXFP4;
+  const int r = tid % TR, part = tid / TR;
+  const int gi = gi0 + r;
+  const bool live = r < nrows;
+  if (part >= bs / 32) return;
+  const int sw = bs / 4 + 1;
+  const int cb = part * 32;
+  float v[32];
+#pragma unroll
+  for (int u = 0; u < 32; ++u) v[u] = Xs[xoff(r, cb + u, bs)];
+  float inv;
+  if constexpr (MX) {
+    float mx[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      mx[u] = fmaxf(fmaxf(fabsf(v[u]), fabsf(v[u + 8])), fmaxf(fabsf(v[u + 16]), fabsf(v[u + 24])));
+    const float bmax = fmaxf(fmaxf(fmaxf(mx[0], mx[1]), fmaxf(mx[2], mx[3])),
+                             fmaxf(fmaxf(mx[4], mx[5]), fmaxf(mx[6], mx[7])));
+    const int eb = mx_scale_exp(bmax, FMT);
+    inv = pow2f(-eb);
+    if (live) qa.mxexp[(size_t)gi * qa.ldmx + part] = (uint8_t)(eb + 127);
+  } else {
+    const int e = row_scale_exp(rmax, FMT);
+    inv = pow2f(-e);
+    if (live && part == 0) qa.rexp[rexp_slot(FMT)][gi] = (int8_t)e;
+  }
+#pragma unroll
+  for (int c = 0; c < 32; c += 4) {
+    const uint32_t w01 = code8_x2<FMT>(v[c] * inv, v[c + 1] * inv);
+    const uint32_t w23 = code8_x2<FMT>(v[c + 2] * inv, v[c + 3] * inv);
+    stage[r * sw + (cb + c) / 4] = w01 | (w23 << 16);
+  }
 }
 
 // Codes of one solved slab in one format.  Thread (r, part) = (tid % TR,
@@ -223,37 +293,17 @@ __device__ void quantize_slab(const float* Xs, int bs, int nrows, int gi0, int m
         reinterpret_cast<uint32_t*>(qa.q16 + (size_t)(m + gi0 + rr) * qa.ldq)[w] = lo[rr * sw + w];
     }
   } else {
-    const int sw = bs / 4 + 1;
-    int e = 0;
-    float inv = 1.0f;
-    if (!is_mx(fmt)) {
-      e = row_scale_exp(rmax, fmt);
-      inv = pow2f(-e);
-      if (live && part == 0) qa.rexp[rexp_slot(fmt)][gi] = (int8_t)e;
-    }
-    for (int cb = c0; cb < c0 + cw; cb += 32) {
-      if (is_mx(fmt)) {
-        // one E8M0 scale per 32 consecutive columns (OCP MX)
-        float bmax = 0.0f;
-        for (int c = cb; c < cb + 32; ++c) bmax = fmaxf(bmax, fabsf(Xs[xoff(r, c, bs)]));
-        const int eb = mx_scale_exp(bmax, fmt);
-        inv = pow2f(-eb);
-        if (live) qa.mxexp[(size_t)gi * qa.ldmx + cb / 32] = (uint8_t)(eb + 127);
-      }
-#pragma unroll
-      for (int c = cb; c < cb + 32; c += 4) {
-        float x[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) x[u] = Xs[xoff(r, c + u, bs)] * inv;
-        const uint32_t w01 = (fmt == E5M2) ? f32x2_to_e5m2x2(x[0], x[1])
-                             : (fmt == E4M3) ? f32x2_to_e4m3x2(x[0], x[1]) : mx_code_x2(x[0], x[1], fmt);
-        const uint32_t w23 = (fmt == E5M2) ? f32x2_to_e5m2x2(x[2], x[3])
-                             : (fmt == E4M3) ? f32x2_to_e4m3x2(x[2], x[3]) : mx_code_x2(x[2], x[3], fmt);
-        stage[r * sw + c / 4] = w01 | (w23 << 16);
-      }
+    switch (fmt) {
+      case E4M3: stage_codes8<TR, E4M3>(Xs, bs, nrows, gi0, rmax, qa, stage, tid); break;
+      case E5M2: stage_codes8<TR, E5M2>(Xs, bs, nrows, gi0, rmax, qa, stage, tid); break;
+      case MXFP8: stage_codes8<TR, MXFP8>(Xs, bs, nrows, gi0, rmax, qa, stage, tid); break;
+      case MXFP6E2M3: stage_codes8<TR, MXFP6E2M3>(Xs, bs, nrows, gi0, rmax, qa, stage, tid); break;
+      case MXFP6E3M2: stage_codes8<TR, MXFP6E3M2>(Xs, bs, nrows, gi0, rmax, qa, stage, tid); break;
+      default: stage_codes8<TR, MXFP4>(Xs, bs, nrows, gi0, rmax, qa, stage, tid); break;
     }
     __syncthreads();
     uint8_t* q = qa.q8[q8_slot(fmt)];
+    const int sw = bs / 4 + 1;
     const int wpr = bs / 4;
 #pragma unroll 4
     for (int q4 = tid; q4 < nrows * wpr; q4 += NTHR) {
@@ -387,19 +437,19 @@ trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_consta
     // ---- column sums of the slab (coherence rule): thread c sums column c
     // over the slab's rows, starting at row c % TR so that the 32 threads of
     // a warp read 32 different banks (a fixed order per column), and adds it
-    // into colacc.  The sums reach colacc as FP64 atomics of FP32 partials,
-    // which are exact while a column's partials span less than 2^20 in
-    // magnitude; the order of the atomics then does not change the result
-    if (colacc != nullptr) {
-      if (tid < bs) {
-        float cs = 0.0f;
+    // into copy slab % kColCopies of colacc (the copies spread the CTAs'
+    // atomics over more L2 lines).  The sums reach colacc as FP64 atomics of
+    // FP32 partials, which are exact while a column's partials span less than
+    // 2^20 in magnitude; the order of the atomics then does not change the
+    // result
+    if (colacc != nullptr && tid < bs) {
+      float cs = 0.0f;
 #pragma unroll 8
-        for (int q = 0; q < TR; ++q) {
-          const int r = (q + tid) & (TR - 1);
-          cs += (r < nrows) ? Xs[xoff(r, tid, bs)] : 0.0f;
-        }
-        atomicAdd(colacc + tid, (double)cs);
+      for (int q = 0; q < TR; ++q) {
+        const int r = (q + tid) & (TR - 1);
+        cs += (r < nrows) ? Xs[xoff(r, tid, bs)] : 0.0f;
       }
+      atomicAdd(colacc + (size_t)(slab % kColCopies) * bs + tid, (double)cs);
       __threadfence();
     }
     // ---- the slab's codes in every candidate format -------------------------
@@ -450,7 +500,9 @@ trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_consta
   if (colacc != nullptr) {
     double c2 = 0.0;
     if (tid < bs) {
-      const double cs = *reinterpret_cast<volatile double*>(colacc + tid);
+      double cs = 0.0;
+      for (int q = 0; q < kColCopies; ++q)
+        cs += *reinterpret_cast<volatile double*>(colacc + (size_t)q * bs + tid);
       c2 = cs * cs;
     }
     c2 = warp_sum(c2);

@@ -237,8 +237,8 @@ def test_reference_shaped_switching_chol(cuda):
 @pytest.mark.parametrize("n,nrhs", [(1000, 2), (768, 1)])
 def test_solve_host_matches_device_path(cuda, n, nrhs):
     """mpchol_solve_host (host buffers, lower triangle copied by block columns)
-    gives the device path's solution: same factor, same operator, same PCG
-    iteration count.  The solutions agree to 1e-8 relative: the operator and
+    gives the device path's solution: same factor, same operator, the same PCG
+    iteration count (within one).  The solutions agree to 1e-8 relative: the operator and
     preconditioner products combine partial sums with FP64 atomics, whose
     order varies from run to run (differences ~1e-10 relative)."""
     A = matgen.spd_matrix(n, 1e4, 41)
@@ -251,7 +251,7 @@ def test_solve_host_matches_device_path(cuda, n, nrhs):
     f_host = mp.Factor(n, **opts)
     for _ in range(2):   # the second call reuses the buffers the first allocated
         Xh, rh = f_host.solve_host(A.pin_memory(), B.pin_memory(), rel_tol=1e-10)
-        assert rh.converged and rh.iterations == rd.iterations
+        assert rh.converged and abs(rh.iterations - rd.iterations) <= 1
         assert Xh.device.type == "cpu" and Xh.shape == B.shape
         err = np.linalg.norm(Xh.numpy() - Xd.cpu().numpy()) / np.linalg.norm(Xd.cpu().numpy())
         assert err < 1e-8, err
@@ -313,7 +313,9 @@ def test_factor_save_load_round_trip(cuda):
     assert gi.step_prec == fi.step_prec and gi.step_fp64 == fi.step_fp64
     assert gi.status == fi.status and gi.n_perturbed == fi.n_perturbed
     X2, r2 = g.pcg(A.cuda(), B.cuda(), rel_tol=1e-10, max_it=400)
-    assert r1.converged and r2.converged and r2.iterations == r1.iterations
+    # same factor bits; the solves themselves sum their FP64 products with
+    # atomics in no fixed order, so at kappa = 1e6 the count may differ by one
+    assert r1.converged and r2.converged and abs(r2.iterations - r1.iterations) <= 1
     x1, x2 = X1.cpu().numpy(), X2.cpu().numpy()
     assert np.linalg.norm(x2 - x1) / np.linalg.norm(x1) < 1e-8
     with pytest.raises(mp.MpcholError):
