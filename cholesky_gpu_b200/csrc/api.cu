@@ -455,6 +455,10 @@ mpchol_status ensure_factor_streams(mpchol_factor_t* f) {
 // groups that have joined, and a joining group first receives the earlier
 // panels' updates (one SEL_BAND launch per panel, in step order, from the
 // panel history) on the aux stream.
+// Trailing rows from which a step's concurrent update outlasts the POTRF
+// beside it (B200, b = 256: about 80 us of update at 7168 rows).
+constexpr int kCompactPotrfRows = 7168;
+
 mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream, const CopyPlan* plan = nullptr) {
   const mpchol_opts& o = f->opts;
   const int n = f->n, ld = f->ld, b = f->b;
@@ -492,12 +496,16 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream, const CopyPlan
         else f32_possible = true;
       }
   }
-  auto potrf = [&](int k) -> mpchol_status {
+  // beside: the POTRF of block k runs beside the rest of step k-1's trailing
+  // update; with at least kCompactPotrfRows trailing rows that update lasts
+  // longer than the POTRF itself, and the small-code POTRF variant is used
+  auto potrf = [&](int k, bool beside) -> mpchol_status {
     const int s = k * b;
+    const bool compact = beside && n - s >= kCompactPotrfRows;
     PHASE(MPCHOL_PH_POTRF, o.floor > 0.0f ? 2 : 1, stream,
           launch_potrf(f->tmap32, f->A, ld, n, s, std::min(b, n - s), f->d, f->sh, pp,
                        &f->steps[k].fp64_diag, f->scratch64, f->winv, f->status, o.floor > 0.0f,
-                       stream, k > 0 ? &f->steps[k - 1] : nullptr, f->rowsq));
+                       stream, k > 0 ? &f->steps[k - 1] : nullptr, f->rowsq, compact));
     return MPCHOL_OK;
   };
   // where the panel solve of step k writes the codes of each candidate
@@ -569,7 +577,7 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream, const CopyPlan
         mpchol_status rs = syrk(p, band, 0, stream);
         if (rs != MPCHOL_OK) return rs;
       }
-      mpchol_status rs = potrf(k);
+      mpchol_status rs = potrf(k, false);
       if (rs != MPCHOL_OK) return rs;
       const int s = k * b;
       const int bs = std::min(b, n - s);
@@ -587,7 +595,7 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream, const CopyPlan
     f->solve_ready = false;
     return MPCHOL_OK;
   }
-  mpchol_status rs = potrf(0);
+  mpchol_status rs = potrf(0, false);
   if (rs != MPCHOL_OK) return rs;
   bool rest_pending = false;
   int joined = 1;                                  // groups in the trailing updates
@@ -643,7 +651,7 @@ mpchol_status run_factor(mpchol_factor_t* f, cudaStream_t stream, const CopyPlan
     } else if (caught) {
       MPCHOL_CUDA_TRY(cudaStreamWaitEvent(stream, f->ev_catch, 0));
     }
-    if ((rs = potrf(k + 1)) != MPCHOL_OK) return rs;
+    if ((rs = potrf(k + 1, rest_pending)) != MPCHOL_OK) return rs;
   }
   if (rest_pending) MPCHOL_CUDA_TRY(cudaStreamWaitEvent(stream, f->ev_rest, 0));
   if (streamed) MPCHOL_CUDA_TRY(cudaStreamWaitEvent(stream, f->ev_grp[plan->ng - 1], 0));

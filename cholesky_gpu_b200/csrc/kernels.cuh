@@ -46,11 +46,14 @@ size_t potrf_scratch64_elems(int bs);
 // tmap32: TMA map over A (FP32, n x n, column stride lda) with 32 x 32 boxes.
 // With diagonal perturbation, the block's rows first receive the previous
 // step's rounding shift, sh += u(prev->prec) * rowsq (prev null: none).
+// compact: the small-code variant, for a POTRF that runs beside a long
+// trailing update (the fully unrolled one is faster on its own but slows
+// down several times when its instructions are refetched through a busy L2).
 cudaError_t launch_potrf(const CUtensorMap& tmap32, float* A, int lda, int n, int s, int bs,
                          const float* d, float* sh, const PotrfParams& p,
                          const int* fp64_flag, double* scratch64, float* winv, DevStatus* st,
                          bool may_fp64, cudaStream_t stream, const StepState* prev = nullptr,
-                         const float* rowsq = nullptr);
+                         const float* rowsq = nullptr, bool compact = false);
 
 // ---- panel TRSM + fused diagonal tracker, decision and quantization ------
 // Where the panel solve writes the quantized panel: one K-major code panel

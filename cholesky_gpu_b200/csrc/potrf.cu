@@ -82,15 +82,24 @@ __device__ __forceinline__ Pivot<T> eval_pivot(T cand, bool real, T my_shift, T 
 // 1 / L(k,k).  Returns false on a non-positive pivot when pivot flooring is
 // off (first failing local row in *fail_row).
 //
-// Lane i holds row i of the tile in registers for the whole factorization (the
-// column loop is unrolled so every register index is a constant): per column
-// lane k's pivot is repaired, one shuffle broadcasts 1/sqrt(pivot),
-// and the rank-1 update reads the column's multipliers from the 32-entry
-// shared buffer col as 16-byte broadcasts.  The tile itself is read once and
-// its lower triangle written once.
-template <typename T>
+// Lane i holds row i of the tile in registers (a[j], j relative to the
+// current block of CB columns): per column lane k's pivot is repaired, one
+// shuffle broadcasts 1/sqrt(pivot), and the rank-1 update reads the column's
+// multipliers from the 32-entry shared buffer col as 16-byte broadcasts.  The
+// columns run as a loop over blocks of CB whose body is unrolled: after a
+// block its finished columns are stored and the registers shift down by CB,
+// so register indices stay compile-time constants while the kernel's code
+// stays small (its instructions must stay cache-resident while the trailing
+// update saturates L2 beside it).  The pivot of column k + 1 is lane k + 1's
+// candidate a[k+1] - L(k+1,k)^2 (the same fma the rank-1 update applies to
+// a[k+1]); it is evaluated, square-rooted and broadcast before column k's
+// multipliers go through shared memory, so the pivot chain and the update's
+// round trip overlap.  Registers past the tile's last column are updated
+// with junk and never stored.
+template <typename T, int CB>
 __device__ bool factor_diag_tile(T* t, T* inv, int lane, int nreal, const T* shift, const T* pmin,
                                  int diag_pert, int* nperturbed, int* fail_row, T* col) {
+  constexpr int V = 16 / sizeof(T);
   T a[TS];
 #pragma unroll
   for (int j = 0; j < TS; ++j) a[j] = t[j * TS + lane];
@@ -98,45 +107,47 @@ __device__ bool factor_diag_tile(T* t, T* inv, int lane, int nreal, const T* shi
   const T my_pmin = pmin[lane];
   bool failed = false, perturbed = false;
   T my_inv = T(1);
-  // The pivot of column k + 1 is lane k + 1's candidate a[k+1] - L(k+1,k)^2
-  // (the same fma the rank-1 update applies to a[k+1]); it is evaluated,
-  // square-rooted and broadcast before column k's multipliers go through
-  // shared memory, so the pivot chain and the update's round trip overlap.
   Pivot<T> pv = eval_pivot<T>(a[0], 0 < nreal, my_shift, my_pmin, diag_pert);
   T rk = __shfl_sync(0xffffffffu, pv.r, 0);
+#pragma unroll 1
+  for (int c0 = 0; c0 < TS; c0 += CB) {
 #pragma unroll
-  for (int k = 0; k < TS; ++k) {
-    const bool mine = lane == k;
-    perturbed = perturbed || (mine && pv.pert);
-    failed = failed || (mine && pv.bad);
-    my_inv = mine ? pv.r : my_inv;
-    const T lik = (lane > k) ? a[k] * rk : T(0);
-    a[k] = mine ? pv.piv * pv.r : ((lane > k) ? lik : a[k]);
-    if (k + 1 < TS) {
-      pv = eval_pivot<T>(fma(-lik, lik, a[k + 1]), k + 1 < nreal, my_shift, my_pmin, diag_pert);
-      rk = __shfl_sync(0xffffffffu, pv.r, k + 1);
-    }
-    // two multiplier buffers used in turn: the next column's write cannot
-    // overtake a lane still reading this one, so one warp barrier suffices
-    T* cb = col + (k & 1) * TS;
-    cb[lane] = lik;
-    __syncwarp();
-    constexpr int V = 16 / sizeof(T);
+    for (int c = 0; c < CB; ++c) {
+      const int k = c0 + c;
+      const bool mine = lane == k;
+      perturbed = perturbed || (mine && pv.pert);
+      failed = failed || (mine && pv.bad);
+      my_inv = mine ? pv.r : my_inv;
+      const T lik = (lane > k) ? a[c] * rk : T(0);
+      a[c] = mine ? pv.piv * pv.r : ((lane > k) ? lik : a[c]);
+      if (k + 1 < TS) {
+        pv = eval_pivot<T>(fma(-lik, lik, a[c + 1]), k + 1 < nreal, my_shift, my_pmin, diag_pert);
+        rk = __shfl_sync(0xffffffffu, pv.r, k + 1);
+      }
+      // two multiplier buffers used in turn: the next column's write cannot
+      // overtake a lane still reading this one, so one warp barrier suffices
+      T* cb = col + (k & 1) * TS;
+      cb[lane] = lik;
+      __syncwarp();
 #pragma unroll
-    for (int q = 0; q < TS / V; ++q) {
-      if (V * q + V - 1 <= k) continue;
-      T l[V];
-      load_vec16(cb + V * q, l);
+      for (int q = (c + 1) / V; q < TS / V; ++q) {
+        if (c0 + V * q < TS) {
+          T l[V];
+          load_vec16(cb + c0 + V * q, l);
 #pragma unroll
-      for (int e = 0; e < V; ++e) {
-        const int j = V * q + e;
-        if (j > k) a[j] = fma(-lik, l[e], a[j]);
+          for (int e = 0; e < V; ++e) {
+            const int j = V * q + e;
+            if (j > c) a[j] = fma(-lik, l[e], a[j]);
+          }
+        }
       }
     }
-  }
 #pragma unroll
-  for (int j = 0; j < TS; ++j)
-    if (j <= lane) t[j * TS + lane] = a[j];
+    for (int c = 0; c < CB; ++c)
+      if (c0 + c <= lane) t[(c0 + c) * TS + lane] = a[c];
+#pragma unroll
+    for (int j = 0; j < TS - CB; ++j) a[j] = a[j + CB];
+  }
   inv[lane] = my_inv;
   const unsigned fm = __ballot_sync(0xffffffffu, failed);
   const unsigned pm = __ballot_sync(0xffffffffu, perturbed);
@@ -149,104 +160,134 @@ __device__ bool factor_diag_tile(T* t, T* inv, int lane, int nreal, const T* shi
 // X L^T = B for one tile (B in x, overwritten); lane i owns row i.
 // Right-looking: once x(i, m) is final it is applied to the later columns,
 // whose multipliers L(m+1.., m) are contiguous in the column-major tile l and
-// arrive as 16-byte broadcasts.
-template <typename T>
+// arrive as 16-byte broadcasts.  Blocks of CB columns with register rotation,
+// as in factor_diag_tile.
+template <typename T, int CB>
 __device__ void trsm_tile(T* x, const T* l, const T* inv, int lane) {
   constexpr int V = 16 / sizeof(T);
   T b[TS];
 #pragma unroll
   for (int m = 0; m < TS; ++m) b[m] = x[m * TS + lane];
+#pragma unroll 1
+  for (int m0 = 0; m0 < TS; m0 += CB) {
 #pragma unroll
-  for (int m = 0; m < TS; ++m) {
-    b[m] *= inv[m];
+    for (int c = 0; c < CB; ++c) {
+      const int m = m0 + c;
+      b[c] *= inv[m];
 #pragma unroll
-    for (int q = (m + 1) / V; q < TS / V; ++q) {
-      T lv[V];
-      load_vec16(l + m * TS + V * q, lv);
+      for (int q = (c + 1) / V; q < TS / V; ++q) {
+        if (m0 + V * q < TS) {
+          T lv[V];
+          load_vec16(l + m * TS + m0 + V * q, lv);
 #pragma unroll
-      for (int e = 0; e < V; ++e)
-        if (V * q + e > m) b[V * q + e] = fma(-b[m], lv[e], b[V * q + e]);
-    }
-  }
-#pragma unroll
-  for (int m = 0; m < TS; ++m) x[m * TS + lane] = b[m];
-}
-
-// Columns c0..c0+7 of C -= A B^T for 32 x 32 tiles; lane i owns row i of C
-// and holds row i of A in ar.  B's column values arrive as 16-byte
-// broadcasts; with TWO, a second tile of the same tile column
-// (C2 -= A2 B^T, A2's row in ar2) shares every broadcast.
-template <typename T, bool TWO>
-__device__ __forceinline__ void syrk_cols8(T* c, T* c2, const T (&ar)[TS], const T (&ar2)[TS],
-                                           const T* b, int lane, int c0) {
-  constexpr int V = 16 / sizeof(T);
-  T acc[8], acc2[8];
-#pragma unroll
-  for (int u = 0; u < 8; ++u) {
-    acc[u] = c[(c0 + u) * TS + lane];
-    acc2[u] = TWO ? c2[(c0 + u) * TS + lane] : T(0);
-  }
-#pragma unroll
-  for (int m = 0; m < TS; ++m) {
-#pragma unroll
-    for (int q = 0; q < 8 / V; ++q) {
-      T bv[V];
-      load_vec16(b + m * TS + c0 + V * q, bv);
-#pragma unroll
-      for (int e = 0; e < V; ++e) {
-        acc[V * q + e] = fma(-ar[m], bv[e], acc[V * q + e]);
-        if (TWO) acc2[V * q + e] = fma(-ar2[m], bv[e], acc2[V * q + e]);
+          for (int e = 0; e < V; ++e)
+            if (V * q + e > c) b[V * q + e] = fma(-b[c], lv[e], b[V * q + e]);
+        }
       }
     }
-  }
 #pragma unroll
-  for (int u = 0; u < 8; ++u) {
-    c[(c0 + u) * TS + lane] = acc[u];
-    if (TWO) c2[(c0 + u) * TS + lane] = acc2[u];
+    for (int c = 0; c < CB; ++c) x[(m0 + c) * TS + lane] = b[c];
+#pragma unroll
+    for (int j = 0; j < TS - CB; ++j) b[j] = b[j + CB];
   }
 }
 
-// C -= A B^T over columns [c_begin, c_end) (multiples of 8), and C2 -= A2 B^T
-// over the same columns when c2 is set.
-template <typename T>
-__device__ void syrk_tiles(T* c, const T* a, T* c2, const T* a2, const T* b, int lane,
-                           int c_begin = 0, int c_end = TS) {
-  T ar[TS], ar2[TS];
+// N contiguous elements of a shared tile (16-byte vectors, an 8-byte
+// remainder; p aligned to the access size).
+template <int N, typename T>
+__device__ __forceinline__ void load_n(const T* p, T (&v)[N]) {
+  constexpr int V = 16 / sizeof(T);
 #pragma unroll
-  for (int m = 0; m < TS; ++m) ar[m] = a[m * TS + lane];
-  if (c2 != nullptr) {
+  for (int q = 0; q < N / V; ++q) {
+    T w[V];
+    load_vec16(p + V * q, w);
 #pragma unroll
-    for (int m = 0; m < TS; ++m) ar2[m] = a2[m * TS + lane];
-#pragma unroll 1
-    for (int c0 = c_begin; c0 < c_end; c0 += 8) syrk_cols8<T, true>(c, c2, ar, ar2, b, lane, c0);
-  } else {
-#pragma unroll 1
-    for (int c0 = c_begin; c0 < c_end; c0 += 8) syrk_cols8<T, false>(c, nullptr, ar, ar, b, lane, c0);
+    for (int e = 0; e < V; ++e) v[V * q + e] = w[e];
   }
+  if constexpr (N % V != 0) {
+    static_assert(sizeof(T) == 4 && N % V == 2, "8-byte remainder of a float block");
+    const float2 w = *reinterpret_cast<const float2*>(p + N - 2);
+    v[N - 2] = w.x;
+    v[N - 1] = w.y;
+  }
+}
+
+// C(r0 .. r0+RR-1, c0 .. c0+CC-1) -= A B^T over the tiles' 32 k (32 x 32
+// tiles, column-major).  The thread keeps its RR x CC block in registers and
+// reads, per k, RR values of A's column and CC of B's as vectors, so a warp's
+// shared-memory traffic per FMA is (RR + CC) / (RR CC) of a value (the
+// return path of shared memory, not the FMA pipe, bounds these updates).
+// Each output is the same fma chain in k order as a row-by-row update.
+template <typename T, int RR, int CC>
+__device__ __forceinline__ void syrk_block(T* c, const T* a, const T* b, int r0, int c0) {
+  T acc[RR][CC];
+#pragma unroll
+  for (int j = 0; j < CC; ++j)
+#pragma unroll
+    for (int i = 0; i < RR; ++i) acc[i][j] = c[(c0 + j) * TS + r0 + i];
+#pragma unroll 4
+  for (int k = 0; k < TS; ++k) {
+    T av[RR], bv[CC];
+    load_n<RR>(a + k * TS + r0, av);
+    load_n<CC>(b + k * TS + c0, bv);
+#pragma unroll
+    for (int i = 0; i < RR; ++i)
+#pragma unroll
+      for (int j = 0; j < CC; ++j) acc[i][j] = fma(-av[i], bv[j], acc[i][j]);
+  }
+#pragma unroll
+  for (int j = 0; j < CC; ++j)
+#pragma unroll
+    for (int i = 0; i < RR; ++i) c[(c0 + j) * TS + r0 + i] = acc[i][j];
+}
+
+// A whole 32 x 32 tile C -= A B^T by one warp: lane (rg, cg) = (lane % 4,
+// lane / 4) owns rows 8 rg .. and columns 4 cg .. (a quarter-warp reads four
+// distinct 32-byte row groups and two column groups: no bank conflict).
+template <typename T>
+__device__ __forceinline__ void syrk_tile(T* c, const T* a, const T* b, int lane) {
+  syrk_block<T, 8, 4>(c, a, b, 8 * (lane & 3), 4 * (lane >> 2));
 }
 
 // Inverse of the lower-triangular tile l into out (32 x 32 column-major,
 // FP32).  Lane j solves L w = e_j for column j of L^-1, right-looking with the
-// column held in registers; the column of L used at each step is a shared
-// broadcast.  Each lane then stores its column as 16-byte vectors.
-template <typename T>
+// column held in registers; the column of L used at each step arrives as
+// 16-byte broadcasts.  Blocks of CB steps with register rotation, as in
+// factor_diag_tile; each block's finished entries go out as 16-byte vectors.
+template <typename T, int CB>
 __device__ void invert_tile(const T* l, const T* inv, float* out, int lane) {
+  constexpr int V = 16 / sizeof(T);
   T w[TS];
 #pragma unroll
   for (int i = 0; i < TS; ++i) w[i] = (i == lane) ? T(1) : T(0);
+#pragma unroll 1
+  for (int k0 = 0; k0 < TS; k0 += CB) {
 #pragma unroll
-  for (int k = 0; k < TS; ++k) {
-    w[k] *= inv[k];
+    for (int c = 0; c < CB; ++c) {
+      const int k = k0 + c;
+      w[c] *= inv[k];
 #pragma unroll
-    for (int i = k + 1; i < TS; ++i) w[i] -= l[k * TS + i] * w[k];
+      for (int q = (c + 1) / V; q < TS / V; ++q) {
+        if (k0 + V * q < TS) {
+          T lv[V];
+          load_vec16(l + k * TS + k0 + V * q, lv);
+#pragma unroll
+          for (int e = 0; e < V; ++e)
+            if (V * q + e > c) w[V * q + e] = fma(-lv[e], w[c], w[V * q + e]);
+        }
+      }
+    }
+    // the finished entries k0 .. k0 + CB - 1 of column lane
+    float4* o = reinterpret_cast<float4*>(out + lane * TS + k0);
+#pragma unroll
+    for (int q = 0; q < CB / 4; ++q)
+      o[q] = make_float4((float)w[4 * q], (float)w[4 * q + 1], (float)w[4 * q + 2], (float)w[4 * q + 3]);
+#pragma unroll
+    for (int j = 0; j < TS - CB; ++j) w[j] = w[j + CB];
   }
-  float4* o = reinterpret_cast<float4*>(out + lane * TS);
-#pragma unroll
-  for (int q = 0; q < TS / 4; ++q)
-    o[q] = make_float4((float)w[4 * q], (float)w[4 * q + 1], (float)w[4 * q + 2], (float)w[4 * q + 3]);
 }
 
-template <typename T, bool TMA>
+template <typename T, bool TMA, int CB>
 __device__ void potrf_block(const CUtensorMap* tmap, T* tiles, float* A, int lda, int n, int s,
                             int bs, const float* d, float* sh, const PotrfParams& p,
                             float* winv, DevStatus* st, const StepState* prev = nullptr,
@@ -336,14 +377,14 @@ __device__ void potrf_block(const CUtensorMap* tmap, T* tiles, float* A, int lda
   // Step J: (A) the tiles below diagonal tile J are solved, one per warp;
   // (B) warps 0-3 apply column J to diagonal tile J+1 (8 columns each, one
   // warp per SM sub-partition) and warp 0 factors it at once, while warps
-  // 1.. update the other trailing tiles, two tiles of a tile column at a time
-  // so that each broadcast of column J's values feeds both.  The factor of
-  // the next diagonal tile thus overlaps the trailing update (look-ahead).
+  // 1.. update the other trailing tiles, one tile per warp with 2-D register
+  // blocks.  The factor of the next diagonal tile thus overlaps the trailing
+  // update (look-ahead).
   auto factor_tile = [&](int J) {
     int nreal = bs - J * TS;
     nreal = nreal > TS ? TS : nreal;
     int fail = -1, npert = 0;
-    const bool ok = factor_diag_tile<T>(tiles + tidx(J, J) * TSZ, s_inv + J * TS, lane, nreal,
+    const bool ok = factor_diag_tile<T, CB>(tiles + tidx(J, J) * TSZ, s_inv + J * TS, lane, nreal,
                                         s_shift + J * TS, s_pmin + J * TS, p.diag_pert, &npert,
                                         &fail, s_col);
     if (lane == 0) {
@@ -351,35 +392,47 @@ __device__ void potrf_block(const CUtensorMap* tmap, T* tiles, float* A, int lda
       s_pert += npert;
     }
   };
-  if (warp == 0) factor_tile(0);
-  __syncthreads();
-  for (int J = 0; J < NT; ++J) {
-    if (s_fail >= 0) break;
-    for (int I = J + 1 + warp; I < NT; I += nwarps)
-      trsm_tile<T>(tiles + tidx(I, J) * TSZ, tiles + tidx(J, J) * TSZ, s_inv + J * TS, lane);
-    __syncthreads();
-    if (J + 1 < NT) {
-      if (warp < 4) {
+  // J = -1 factors diagonal tile 0 alone; the factor has one call site, so
+  // its code is in the kernel once.  Warp 0 carries the chain (the solve of
+  // tile (J+1, J) and the factor of diagonal tile J+1) and has its SM
+  // sub-partition to itself: the other warps of that sub-partition (warp %
+  // 4 == 0) stay idle, and the helper warps (warp % 4 != 0) take the other
+  // tile solves and the trailing updates.
+  const int helper = (warp & 3) ? warp - (warp >> 2) - 1 : -1;
+  const int nhelp = nwarps - nwarps / 4;
+  for (int J = -1; J < NT - 1; ++J) {
+    if (J >= 0) {
+      if (s_fail >= 0) break;
+      // warp 0 solves tile (J+1, J), the one the next diagonal tile waits
+      // on; the helpers take the others
+      if (warp == 0 && J + 1 < NT)
+        trsm_tile<T, CB>(tiles + tidx(J + 1, J) * TSZ, tiles + tidx(J, J) * TSZ, s_inv + J * TS, lane);
+      if (helper >= 0)
+        for (int I = J + 2 + helper; I < NT; I += nhelp)
+          trsm_tile<T, CB>(tiles + tidx(I, J) * TSZ, tiles + tidx(J, J) * TSZ, s_inv + J * TS, lane);
+      __syncthreads();
+    }
+    if (warp < 4) {
+      if (J >= 0) {
+        // columns 8 warp .. +7 of diagonal tile J+1: lane (rg, cg) = (lane %
+        // 8, lane / 8) owns rows 4 rg .. and columns 8 warp + 2 cg ..
         T* dt = tiles + tidx(J + 1, J + 1) * TSZ;
         const T* pj = tiles + tidx(J + 1, J) * TSZ;
-        syrk_tiles<T>(dt, pj, nullptr, nullptr, pj, lane, 8 * warp, 8 * warp + 8);
+        syrk_block<T, 4, 2>(dt, pj, pj, 4 * (lane & 7), 8 * warp + 2 * (lane >> 3));
         asm volatile("bar.sync 1, 128;" ::: "memory");   // warps 0-3
-        if (warp == 0) factor_tile(J + 1);
       }
-      if (warp >= 1) {
-        // work items: pairs of vertically adjacent tiles (I, K), (I+1, K) of
-        // each trailing tile column K, J < K <= I, diagonal tile J+1 excluded
-        int item = 0;
-        for (int K = J + 1; K < NT; ++K) {
-          const int i0 = (K == J + 1) ? K + 1 : K;
-          for (int I = i0; I < NT; I += 2, ++item) {
-            if (item % (nwarps - 1) != warp - 1) continue;
-            const bool two = I + 1 < NT;
-            syrk_tiles<T>(tiles + tidx(I, K) * TSZ, tiles + tidx(I, J) * TSZ,
-                          two ? tiles + tidx(I + 1, K) * TSZ : nullptr,
-                          two ? tiles + tidx(I + 1, J) * TSZ : nullptr,
-                          tiles + tidx(K, J) * TSZ, lane);
-          }
+      if (warp == 0) factor_tile(J + 1);
+    }
+    if (J >= 0 && helper >= 0) {
+      // work items: the trailing tiles (I, K), J < K <= I, diagonal tile J+1
+      // excluded, numbered down each tile column; one helper warp per tile
+      int item = 0;
+      for (int K = J + 1; K < NT; ++K) {
+        const int i0 = (K == J + 1) ? K + 1 : K;
+        for (int I = i0; I < NT; ++I, ++item) {
+          if (item % nhelp != helper) continue;
+          syrk_tile<T>(tiles + tidx(I, K) * TSZ, tiles + tidx(I, J) * TSZ,
+                       tiles + tidx(K, J) * TSZ, lane);
         }
       }
     }
@@ -415,7 +468,7 @@ __device__ void potrf_block(const CUtensorMap* tmap, T* tiles, float* A, int lda
   }
   // inverses of the diagonal tiles, used by the panel solve
   for (int J = warp; J < NT; J += nwarps)
-    invert_tile<T>(tiles + tidx(J, J) * TSZ, s_inv + J * TS, winv + J * TS * TS, lane);
+    invert_tile<T, CB>(tiles + tidx(J, J) * TSZ, s_inv + J * TS, winv + J * TS * TS, lane);
   if (tid == 0 && s_pert) atomicAdd(&st->perturbed, s_pert);
   if (TMA && warp == 0) tc::bulk_wait_read();   // smem must outlive the stores' reads
   (void)n;
@@ -423,6 +476,10 @@ __device__ void potrf_block(const CUtensorMap* tmap, T* tiles, float* A, int lda
 
 // FP32 blocks: tiles in shared memory, staged by TMA.  Separate kernels for
 // the two precisions keep the FP64 register footprint out of the FP32 path.
+// CB = TS unrolls the tile loops fully (fastest on its own); CB = 4 keeps the
+// kernel's code about a quarter of that size, so it stays cache-resident and
+// fast while a trailing update saturates L2 beside it.
+template <int CB>
 __global__ void __launch_bounds__(512, 1)
 potrf_f32_kernel(const __grid_constant__ CUtensorMap tmap, float* A, int lda, int n, int s, int bs,
                  const float* d, float* sh, PotrfParams p, const int* fp64_flag, float* winv,
@@ -430,7 +487,7 @@ potrf_f32_kernel(const __grid_constant__ CUtensorMap tmap, float* A, int lda, in
   if (st->code != 0) return;
   if (fp64_flag != nullptr && *fp64_flag != 0) return;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  potrf_block<float, true>(&tmap, reinterpret_cast<float*>(smem_raw), A, lda, n, s, bs, d, sh, p,
+  potrf_block<float, true, CB>(&tmap, reinterpret_cast<float*>(smem_raw), A, lda, n, s, bs, d, sh, p,
                            winv, st, prev, rowsq);
 }
 
@@ -443,7 +500,7 @@ potrf_batched_kernel(BatchSys* __restrict__ sys, int s, int b, PotrfParams p) {
   const int bs = min(b, S.n - s);
   if (bs <= 0 || S.st->code != 0) return;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  potrf_block<float, false>(nullptr, reinterpret_cast<float*>(smem_raw), S.A, S.ld, S.n, s, bs,
+  potrf_block<float, false, TS>(nullptr, reinterpret_cast<float*>(smem_raw), S.A, S.ld, S.n, s, bs,
                             S.d, S.sh, p, S.winv, S.st);
 }
 
@@ -454,7 +511,7 @@ potrf_f64_kernel(float* A, int lda, int n, int s, int bs, const float* d, float*
                  const StepState* prev, const float* rowsq) {
   if (st->code != 0) return;
   if (fp64_flag == nullptr || *fp64_flag == 0) return;
-  potrf_block<double, false>(nullptr, scratch64, A, lda, n, s, bs, d, sh, p, winv, st, prev, rowsq);
+  potrf_block<double, false, 8>(nullptr, scratch64, A, lda, n, s, bs, d, sh, p, winv, st, prev, rowsq);
 }
 
 }  // namespace
@@ -470,13 +527,20 @@ cudaError_t launch_potrf(const CUtensorMap& tmap32, float* A, int lda, int n, in
                          const float* d, float* sh, const PotrfParams& p,
                          const int* fp64_flag, double* scratch64, float* winv, DevStatus* st,
                          bool may_fp64, cudaStream_t stream, const StepState* prev,
-                         const float* rowsq) {
+                         const float* rowsq, bool compact) {
   const size_t smem = potrf_smem_bytes(256);
-  cudaError_t e = cudaFuncSetAttribute(potrf_f32_kernel,
+  cudaError_t e = cudaFuncSetAttribute(potrf_f32_kernel<4>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(potrf_f32_kernel<TS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
   if (e != cudaSuccess) return e;
-  potrf_f32_kernel<<<1, 512, smem, stream>>>(tmap32, A, lda, n, s, bs, d, sh, p,
-                                             may_fp64 ? fp64_flag : nullptr, winv, st, prev, rowsq);
+  if (compact)
+    potrf_f32_kernel<4><<<1, 512, smem, stream>>>(tmap32, A, lda, n, s, bs, d, sh, p,
+                                                  may_fp64 ? fp64_flag : nullptr, winv, st, prev, rowsq);
+  else
+    potrf_f32_kernel<TS><<<1, 512, smem, stream>>>(tmap32, A, lda, n, s, bs, d, sh, p,
+                                                   may_fp64 ? fp64_flag : nullptr, winv, st, prev, rowsq);
   if (may_fp64)
     potrf_f64_kernel<<<1, 256, 0, stream>>>(A, lda, n, s, bs, d, sh, p, fp64_flag, scratch64, winv, st,
                                             prev, rowsq);
