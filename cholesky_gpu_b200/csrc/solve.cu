@@ -938,19 +938,19 @@ panel_body(const float* __restrict__ L, int ldl, int n, int s0, int rs,
 
 
 // ---- persistent triangular solve -------------------------------------------
-// One launch per solve.  The tiles of a solve form a dependency DAG: for
-// super-step S the TRMV tiles of W_S (which need every panel contribution to
-// their input segment) and then the panel tiles below (forward) or left of
-// (backward) S (which need their segment of y_S / z_S complete).  Units are
-// handed out in that topological order by an atomic counter, so a unit only
-// ever waits on units already taken by running CTAs; the launch is
-// cooperative, so all CTAs are resident and every wait ends.  Completion is
+// One launch per solve.  The tiles of a solve form a dependency DAG: the
+// TRMV tiles of W_S (which need every panel contribution to their input
+// segment) and the panel tiles below (forward) or left of (backward) S (which
+// need their segment of y_S / z_S complete).  Units are handed out by an
+// atomic counter in a topological order (trsv_job: grouped by the
+// super-block they feed), so a unit only ever waits on units already taken
+// by running CTAs; the launch is cooperative, so all CTAs are resident and
+// every wait ends.  Completion is
 // counted per 128-row segment:
 //   seg_in[g]   panel contributions received by segment g (global 128-tile g)
 //   seg_out[g]  TRMV tiles finished that write segment g of the result
 // Waits are bounded; a wait that runs out records MPCHOL_ERR_TIMEOUT and the
 // unit proceeds (the result is then wrong, but no CTA waits forever).
-constexpr int SEGS = RS / RB;                 // 128-row segments per super-block
 constexpr long long kTrsvMaxPolls = 1ll << 24;
 
 __device__ __forceinline__ void wait_count(const int* ctr, int need, DevStatus* st, int unit) {
@@ -988,79 +988,99 @@ struct TrsvJob {
   int* sig_ctr;
 };
 
-// Decode unit u in the topological order (per super-step: the TRMV tiles,
-// then the panel tiles); returns false past the last unit.
+// Decode unit u.  Units are grouped by the super-block B they feed, in solve
+// order (forward: B = 0, 1, ..; backward: B = NS-1, NS-2, ..): group B holds
+// the panel tiles that carry an earlier super-block's finished segment of the
+// solution into B's input (sources in solve order, so the ones ready longest
+// come first), then the TRMV tiles of W_B.  Every unit depends only on units
+// of earlier groups or earlier in its own group, so the order is topological
+// (the deadlock-freedom of the persistent loop needs that), and a CTA is
+// never handed far-off panel work while the chain's next TRMV waits in the
+// queue behind it.  Returns false past the last unit.
 template <bool TRANS>
 __device__ __forceinline__ bool trsv_job(int u, const float* L, int ldl, int n, const float* wsup,
                                          int* seg_in, int* seg_out, TrsvJob& jb) {
   const int ntiles = ceil_div(n, RB);
   const int NS = ceil_div(n, RS);
+  constexpr int NSUB = RS / RB;              // segments of a full super-block
   for (int t = 0; t < NS; ++t) {
-    const int S = TRANS ? NS - 1 - t : t;
-    const int s0 = S * RS;
-    const int rs = min(RS, n - s0);
-    const int nsub = ceil_div(rs, RB);
-    const int g0 = s0 / RB;                 // first global segment of S
-    const int ntr = nsub * (nsub + 1) / 2;
-    const int span = TRANS ? g0 : ceil_div(n - s0 - rs, RB);
-    const int npan = span * nsub;
-    if (u < ntr) {
-      int i, j;
-      tri_of(u, i, j);
-      const int ri0 = s0 + i * RB, rj0 = s0 + j * RB;
-      jb.T = wsup + (size_t)S * RS * RS + (size_t)(j * RB) * RS + i * RB;
-      jb.ld = RS;
-      jb.nrow = min(RB, s0 + rs - ri0);
-      jb.ncol = min(RB, s0 + rs - rj0);
-      jb.panel = false;
-      if (!TRANS) {
-        // y_S(i) += W(i,j) w_S(j): w_S(j) has all g0 panel contributions
-        jb.nt = true;
-        jb.vin_row0 = rj0; jb.vin_n = jb.ncol;
-        jb.out_row0 = ri0; jb.out_n = jb.nrow;
-        jb.wait_ctr = seg_in + g0 + j; jb.wait_need = g0;
-        jb.sig_ctr = seg_out + g0 + i;
-      } else {
-        // z_S(j) += W(i,j)^T w_S(i): w_S(i) has the contributions of every
-        // segment below S
-        jb.nt = false;
-        jb.vin_row0 = ri0; jb.vin_n = jb.nrow;
-        jb.out_row0 = rj0; jb.out_n = jb.ncol;
-        jb.wait_ctr = seg_in + g0 + i; jb.wait_need = ntiles - g0 - nsub;
-        jb.sig_ctr = seg_out + g0 + j;
-      }
-      return true;
-    }
-    if (u < ntr + npan) {
-      const int p = u - ntr;
+    const int B = TRANS ? NS - 1 - t : t;
+    const int b0 = B * RS;
+    const int rb = min(RS, n - b0);
+    const int nsubB = ceil_div(rb, RB);
+    const int gB = b0 / RB;                  // first global segment of B
+    // panel tiles feeding B: forward from every T < B (NSUB columns of T x
+    // nsubB rows of B); backward from every T > B (the rows of T x NSUB
+    // columns of B)
+    const int npan = TRANS ? (ntiles - gB - nsubB) * NSUB : B * NSUB * nsubB;
+    if (u < npan) {
       jb.panel = true;
       jb.ld = ldl;
       if (!TRANS) {
-        // w(row segment r below S) -= L(r, S col c) y_S(c); rows nearest S first
-        const int r = p / nsub, c = p % nsub;
-        const int r0 = s0 + rs + r * RB, c0 = s0 + c * RB;
+        // w(rows r of B) -= L(r, T col c) y_T(c)
+        const int T = u / (NSUB * nsubB), q = u % (NSUB * nsubB);
+        const int r = q / NSUB, c = q % NSUB;
+        const int r0 = b0 + r * RB, c0 = T * RS + c * RB;
         jb.T = L + (size_t)c0 * ldl + r0;
-        jb.nrow = min(RB, n - r0); jb.ncol = min(RB, s0 + rs - c0);
+        jb.nrow = min(RB, n - r0); jb.ncol = RB;
         jb.nt = true;
-        jb.vin_row0 = c0; jb.vin_n = jb.ncol;
+        jb.vin_row0 = c0; jb.vin_n = RB;
         jb.out_row0 = r0; jb.out_n = jb.nrow;
-        jb.wait_ctr = seg_out + g0 + c; jb.wait_need = c + 1;
-        jb.sig_ctr = seg_in + g0 + nsub + r;
+        jb.wait_ctr = seg_out + T * NSUB + c; jb.wait_need = c + 1;
+        jb.sig_ctr = seg_in + gB + r;
       } else {
-        // w(col segment c left of S) -= L(S row rt, c)^T z_S(rt); columns nearest S first
-        const int c = span - 1 - p / nsub, rt = p % nsub;
-        const int r0 = s0 + rt * RB, c0 = c * RB;
+        // w(col segment c of B) -= L(T row rt, c)^T z_T(rt); sources T from
+        // the last super-block down
+        int q = u, T = NS - 1;
+        for (;; --T) {
+          const int nsubT = ceil_div(min(RS, n - T * RS), RB);
+          if (q < nsubT * NSUB) break;
+          q -= nsubT * NSUB;
+        }
+        const int rt = q / NSUB, c = q % NSUB;
+        const int t0 = T * RS;
+        const int nsubT = ceil_div(min(RS, n - t0), RB);
+        const int r0 = t0 + rt * RB, c0 = b0 + c * RB;
         jb.T = L + (size_t)c0 * ldl + r0;
-        jb.nrow = min(RB, s0 + rs - r0); jb.ncol = min(RB, s0 - c0);
+        jb.nrow = min(RB, n - r0); jb.ncol = RB;
         jb.nt = false;
         jb.vin_row0 = r0; jb.vin_n = jb.nrow;
-        jb.out_row0 = c0; jb.out_n = jb.ncol;
-        jb.wait_ctr = seg_out + g0 + rt; jb.wait_need = nsub - rt;
-        jb.sig_ctr = seg_in + c;
+        jb.out_row0 = c0; jb.out_n = RB;
+        jb.wait_ctr = seg_out + T * NSUB + rt; jb.wait_need = nsubT - rt;
+        jb.sig_ctr = seg_in + gB + c;
       }
       return true;
     }
-    u -= ntr + npan;
+    u -= npan;
+    const int ntr = nsubB * (nsubB + 1) / 2;
+    if (u < ntr) {
+      int i, j;
+      tri_of(u, i, j);
+      const int ri0 = b0 + i * RB, rj0 = b0 + j * RB;
+      jb.T = wsup + (size_t)B * RS * RS + (size_t)(j * RB) * RS + i * RB;
+      jb.ld = RS;
+      jb.nrow = min(RB, b0 + rb - ri0);
+      jb.ncol = min(RB, b0 + rb - rj0);
+      jb.panel = false;
+      if (!TRANS) {
+        // y_B(i) += W(i,j) w_B(j): w_B(j) has all gB panel contributions
+        jb.nt = true;
+        jb.vin_row0 = rj0; jb.vin_n = jb.ncol;
+        jb.out_row0 = ri0; jb.out_n = jb.nrow;
+        jb.wait_ctr = seg_in + gB + j; jb.wait_need = gB;
+        jb.sig_ctr = seg_out + gB + i;
+      } else {
+        // z_B(j) += W(i,j)^T w_B(i): w_B(i) has the contributions of every
+        // segment below B
+        jb.nt = false;
+        jb.vin_row0 = ri0; jb.vin_n = jb.nrow;
+        jb.out_row0 = rj0; jb.out_n = jb.ncol;
+        jb.wait_ctr = seg_in + gB + i; jb.wait_need = ntiles - gB - nsubB;
+        jb.sig_ctr = seg_out + gB + j;
+      }
+      return true;
+    }
+    u -= ntr;
   }
   return false;
 }
