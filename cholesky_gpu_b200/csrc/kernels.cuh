@@ -6,6 +6,24 @@
 
 namespace mpchol {
 
+// Launch configuration with programmatic stream serialization: the kernel
+// may be scheduled while the kernel ahead of it in the stream finishes, and
+// waits on griddepcontrol.wait before its first dependent access.
+struct PdlLaunch {
+  cudaLaunchConfig_t cfg{};
+  cudaLaunchAttribute attr[1];
+  PdlLaunch(dim3 grid, dim3 block, size_t smem, cudaStream_t stream) {
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+  }
+};
+
 struct PotrfParams {
   int diag_pert;
   float pert;

@@ -484,6 +484,8 @@ __global__ void __launch_bounds__(512, 1)
 potrf_f32_kernel(const __grid_constant__ CUtensorMap tmap, float* A, int lda, int n, int s, int bs,
                  const float* d, float* sh, PotrfParams p, const int* fp64_flag, float* winv,
                  DevStatus* st, const StepState* prev, const float* rowsq) {
+  tc::grid_dep_wait();      // the block's update and the step state are final
+  tc::grid_dep_trigger();   // the next kernel may be scheduled (it waits too)
   if (st->code != 0) return;
   if (fp64_flag != nullptr && *fp64_flag != 0) return;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -535,12 +537,13 @@ cudaError_t launch_potrf(const CUtensorMap& tmap32, float* A, int lda, int n, in
     e = cudaFuncSetAttribute(potrf_f32_kernel<TS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem);
   if (e != cudaSuccess) return e;
-  if (compact)
-    potrf_f32_kernel<4><<<1, 512, smem, stream>>>(tmap32, A, lda, n, s, bs, d, sh, p,
-                                                  may_fp64 ? fp64_flag : nullptr, winv, st, prev, rowsq);
-  else
-    potrf_f32_kernel<TS><<<1, 512, smem, stream>>>(tmap32, A, lda, n, s, bs, d, sh, p,
-                                                   may_fp64 ? fp64_flag : nullptr, winv, st, prev, rowsq);
+  PdlLaunch L(dim3(1), dim3(512), smem, stream);
+  const int* flag = may_fp64 ? fp64_flag : nullptr;
+  e = compact ? cudaLaunchKernelEx(&L.cfg, potrf_f32_kernel<4>, tmap32, A, lda, n, s, bs, d, sh, p,
+                                   flag, winv, st, prev, rowsq)
+              : cudaLaunchKernelEx(&L.cfg, potrf_f32_kernel<TS>, tmap32, A, lda, n, s, bs, d, sh, p,
+                                   flag, winv, st, prev, rowsq);
+  if (e != cudaSuccess) return e;
   if (may_fp64)
     potrf_f64_kernel<<<1, 256, 0, stream>>>(A, lda, n, s, bs, d, sh, p, fp64_flag, scratch64, winv, st,
                                             prev, rowsq);

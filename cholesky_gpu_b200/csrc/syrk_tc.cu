@@ -419,6 +419,8 @@ syrk_tc_dispatch_kernel(const __grid_constant__ TcMapsAll maps, float* __restric
                         const int8_t* __restrict__ rexp_e5m2, const int8_t* __restrict__ rexp_f16,
                         const uint8_t* __restrict__ mxexp, int ldmx, unsigned fmt_mask,
                         const int* prec_sel, DevStatus* st, TileSel sel) {
+  tc::grid_dep_wait();      // the panel solve that resolved the step is complete
+  tc::grid_dep_trigger();   // the POTRF after this (head) launch may be scheduled
   const int f = *prec_sel;
   if (f < 0 || f > 31 || ((fmt_mask >> f) & 1u) == 0) return;
   const TcBatch nb{};
@@ -581,9 +583,10 @@ cudaError_t launch_syrk_tc_dispatch(float* C, int ldc, int m, int k, unsigned fm
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_all);
   if (e != cudaSuccess) return e;
   const int grid = grid_for(ntiles, max_sms);
-  syrk_tc_dispatch_kernel<<<grid, NTHREADS, smem, stream>>>(maps, C, ldc, m, k, qa.rexp[0], qa.rexp[1],
-                                                            qa.rexp[2], qa.mxexp, qa.ldmx, fmt_mask,
-                                                            prec_sel, st, sel);
+  PdlLaunch L(dim3(grid), dim3(NTHREADS), smem, stream);
+  e = cudaLaunchKernelEx(&L.cfg, syrk_tc_dispatch_kernel, maps, C, ldc, m, k, qa.rexp[0],
+                         qa.rexp[1], qa.rexp[2], qa.mxexp, qa.ldmx, fmt_mask, prec_sel, st, sel);
+  if (e != cudaSuccess) return e;
   return cudaGetLastError();
 }
 

@@ -350,6 +350,7 @@ trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_consta
   const int slab = blockIdx.x;
   const int row0 = s + bs + slab * TR;                   // first global row of the slab
   const int nrows = min(TR, n - row0);
+  tc::grid_dep_wait();   // the POTRF (and the trailing update) before it are complete
   // the previous step's rounding shift for the slab's rows, before this
   // step's sums of squares replace the previous ones in rowsq
   if (prev != nullptr && qa.sh != nullptr && tid < nrows) {
@@ -470,6 +471,9 @@ trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_consta
     }
     if (tid == 0) tc::bulk_wait_read();   // the slab's stores are complete before the ticket
   }
+  // the next kernel (the head of the trailing update) may be scheduled once
+  // every CTA is past its solve; it waits for this grid before reading
+  tc::grid_dep_trigger();
   // ---- statistics of the CTA; the last CTA resolves the step --------------
   bm = warp_max(bm);
 #pragma unroll
@@ -615,9 +619,10 @@ cudaError_t launch_panel(const CUtensorMap& tmapX, const CUtensorMap& tmap32, fl
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)(trsm_smem_floats(TR, 256) * sizeof(float)));
   if (e != cudaSuccess) return e;
-  trsm_panel_kernel<RPL><<<ceil_div(m, TR), NTHR, smem, stream>>>(
-      tmapX, tmap32, A, lda, n, s, bs, winv, d, dtilde, rowsq, step, next, next_bs, dp, st, qa,
-      prev, colacc);
+  PdlLaunch L(dim3(ceil_div(m, TR)), dim3(NTHR), smem, stream);
+  e = cudaLaunchKernelEx(&L.cfg, trsm_panel_kernel<RPL>, tmapX, tmap32, A, lda, n, s, bs, winv, d,
+                         dtilde, rowsq, step, next, next_bs, dp, st, qa, prev, colacc);
+  if (e != cudaSuccess) return e;
   return cudaGetLastError();
 }
 
