@@ -45,29 +45,29 @@ constexpr int NTHREADS = 64 + 32 * EPI_WARPS;
 
 template <int FMT> struct TcCfg;
 template <> struct TcCfg<FP16> {
-  static constexpr int ESIZE = 2, NSETS = 1, NSTAGE = 4;
+  static constexpr int ESIZE = 2, NSETS = 1, NSTAGE = 4, EPI_BUFS = 2;
   static constexpr bool MX = false;
   static constexpr uint32_t IDESC = tc::make_idesc(0, 0, TM, TM);
 };
 template <> struct TcCfg<E4M3> {
-  static constexpr int ESIZE = 1, NSETS = 1, NSTAGE = 4;
+  static constexpr int ESIZE = 1, NSETS = 1, NSTAGE = 4, EPI_BUFS = 2;
   static constexpr bool MX = false;
   static constexpr uint32_t IDESC = tc::make_idesc(0, 0, TM, TM);
 };
 template <> struct TcCfg<E5M2> {
-  static constexpr int ESIZE = 1, NSETS = 1, NSTAGE = 4;
+  static constexpr int ESIZE = 1, NSETS = 1, NSTAGE = 4, EPI_BUFS = 2;
   static constexpr bool MX = false;
   static constexpr uint32_t IDESC = tc::make_idesc(1, 1, TM, TM);
 };
 template <> struct TcCfg<FP16X2> {
-  static constexpr int ESIZE = 2, NSETS = 2, NSTAGE = 3;
+  static constexpr int ESIZE = 2, NSETS = 2, NSTAGE = 3, EPI_BUFS = 1;
   static constexpr bool MX = false;
   static constexpr uint32_t IDESC = tc::make_idesc(0, 0, TM, TM);
 };
 // MXFP8: E4M3 codes with one E8M0 scale per 32 K-elements, applied by the
 // block-scaled MMA (kind::mxf8f6f4) from scales staged in tensor memory.
 template <> struct TcCfg<MXFP8> {
-  static constexpr int ESIZE = 1, NSETS = 1, NSTAGE = 4;
+  static constexpr int ESIZE = 1, NSETS = 1, NSTAGE = 4, EPI_BUFS = 2;
   static constexpr bool MX = true;
   static constexpr uint32_t IDESC = tc::make_idesc_mx(0, 0, TM, TM);
 };
@@ -313,7 +313,12 @@ syrk_tc_body(const CUtensorMap* mhi, const CUtensorMap* mlo, const CUtensorMap* 
     // ---------------- epilogue (warps 2..5) ----------------
     const int q = warp & 3;                  // TMEM lane quarter this warp may access
     const int half = (warp - 2) >> 2;        // which 64 columns of the tile
-    float* stg = reinterpret_cast<float*>(smem + (size_t)NS * STAGE_BYTES + (size_t)(warp - 2) * STAGE_C);
+    // EPI_BUFS staging boxes per warp, used in turn: with two, a box is
+    // filled while the previous one is still being read by its reduce-add
+    constexpr int EB = Cfg::EPI_BUFS;
+    float* stg0 = reinterpret_cast<float*>(smem + (size_t)NS * STAGE_BYTES +
+                                           (size_t)(warp - 2) * STAGE_C * EB);
+    int nbox = 0;
     int tcount = 0;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++tcount) {
       const TileCtx tc_ = tile_ctx<BATCH>(t, bt, C, ldc, m, sel);
@@ -352,7 +357,13 @@ syrk_tc_body(const CUtensorMap* mhi, const CUtensorMap* mlo, const CUtensorMap* 
           // (signed zeros included) as it was
           const int i0 = I * TM + q * 32;
           if (i0 < mt && j0 < mt && !(I == J && j0 >= i0 + 32)) {
-            if (lane == 0) tc::bulk_wait_smem_read();   // this warp's previous box has been read
+            float* stg = stg0 + (nbox % EB) * (STAGE_C / 4);
+            ++nbox;
+            // the box that last used this buffer has been read
+            if (lane == 0) {
+              if (EB == 2) tc::bulk_wait_smem_read_1();
+              else tc::bulk_wait_smem_read();
+            }
             __syncwarp();
 #pragma unroll
             for (int u = 0; u < 32; ++u) {
@@ -457,7 +468,7 @@ template <int FMT, bool BATCH>
 size_t tc_smem() {
   using Cfg = TcCfg<FMT>;
   return (size_t)Cfg::NSTAGE * (2 * Cfg::NSETS * STRIP + (Cfg::MX ? 2 * SF_BYTES : 0)) +
-         (BATCH ? 0 : (size_t)EPI_WARPS * STAGE_C) + 1024;
+         (BATCH ? 0 : (size_t)EPI_WARPS * STAGE_C * Cfg::EPI_BUFS) + 1024;
 }
 
 int grid_for(int ntiles, int max_sms) {

@@ -92,6 +92,10 @@ __device__ __forceinline__ void bulk_wait_read() {
 __device__ __forceinline__ void bulk_wait_smem_read() {
   asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
 }
+// The same for all but the most recently committed group.
+__device__ __forceinline__ void bulk_wait_smem_read_1() {
+  asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+}
 // Make generic-proxy writes to shared memory visible to the async proxy (TMA).
 __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
