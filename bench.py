@@ -872,6 +872,21 @@ def run_batch(args, world, rank, local):
         return None
     its = [r[0] for r in allrep]
     flops = sum(n ** 3 / 3.0 for n in ns_all)
+    # roofline of the whole step against HBM: algorithmic bytes of every
+    # system's factor (each step's trailing lower triangle read and written
+    # in FP32, the panel read) and of its solves (the initial residual and
+    # x0 = M^-1 b, then per iteration one operator product and two triangular
+    # solves, each a pass over an FP32 lower triangle); small systems keep
+    # the batch latency-bound, which the fraction shows
+    hbm, _, peak_kind = measured_peaks()
+    bsz = plan["config"]["block_size"] if plan["mode"] == "whole" else 128
+    alg = 0.0
+    for n, it in zip(ns_all, its):
+        for k in range(0, n, bsz):
+            m = n - k - min(bsz, n - k)
+            alg += m * (m + 1) / 2 * 8 + m * min(bsz, n - k) * 4
+        alg += (it + 2) * 3 * n * (n + 1) / 2 * 4
+    achieved = alg / (ms * 1e-3) / 1e9
     out = _base(args, world, ms, "ms", "tuned batch factor, fp64 pcg",
                 "synthetic (seeded Q diag(sigma) Q^T per system)",
                 {"workload": f"batch 512 systems n~U[64,2048] kappa~logU[1e2,1e6] rhs=4",
@@ -885,6 +900,10 @@ def run_batch(args, world, rank, local):
                  "factor_tflops_equiv": round(flops / (ms * 1e-3) / 1e12, 2),
                  "e2e": {"value": round(ms_e2e, 3), "unit": "ms", "h2d_bytes_per_step": int(h2d),
                          "d2h_bytes_per_step": int(sum(n * nrhs * 8 for n in ns))},
+                 "roofline": {"kernel": "whole step (factor + PCG of all systems)", "bound": "hbm",
+                              "achieved": round(achieved, 1), "peak": hbm, "peak_kind": peak_kind,
+                              "unit": "GB/s", "frac": round(achieved / hbm, 4),
+                              "algorithmic_per_step": alg, "traffic": None},
                  "clocks": clk.summary()})
     if not args.no_cpu_baseline:
         out["cpu_baseline"] = batch_cpu_baseline(args, As, Bs, ns_all)
