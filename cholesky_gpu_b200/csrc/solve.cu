@@ -478,8 +478,11 @@ __device__ __forceinline__ void tile_mma_x8(const float* Ts, const double* x_c, 
 }
 
 // Shared memory of the staged SYMV: STAGES x (tile + x_J + x_I) + column sums.
+// 8 rhs: one 84 KB stage per CTA and two CTAs per SM (each CTA's load
+// overlaps the other's tile pass; 16 warps hide the DMMA and shared-memory
+// latencies better than one CTA with two stages: 306 vs 331 us at n = 16384)
 template <int NR>
-constexpr int symv_stages() { return NR >= 8 ? 2 : 3; }
+constexpr int symv_stages() { return NR >= 8 ? 1 : 3; }
 template <int NR>
 constexpr size_t symv_staged_smem() {
   if (NR == 8)   // blocked tiles and padded segments, no column-sum buffer
@@ -495,7 +498,7 @@ constexpr size_t symv_staged_smem() {
 // fro != nullptr: CTA b also writes its share of ||A||_F^2 (lower triangle,
 // off-diagonal entries twice) to fro[b] and zeroes fro[gridDim.x ..nfro).
 template <int NR>
-__global__ void __launch_bounds__(NTH, 1)
+__global__ void __launch_bounds__(NTH, NR >= 8 ? 2 : 1)
 symv_staged_kernel(const float* __restrict__ A, int lda, int n, const double* __restrict__ x,
                    double* __restrict__ y, const int* skip, double* fro, int nfro) {
   if (skip != nullptr && *skip) return;
@@ -1360,7 +1363,8 @@ cudaError_t launch_symv_skip(const TA* A, int lda, int n, const double* x, doubl
   const int T = ceil_div(n, RB);
   const int ntiles = T * (T + 1) / 2;
   if (symv_staged_ok(A, lda)) {
-    const int grid = std::min(ntiles, sm_count());
+    int grid = std::min(ntiles, (nrhs >= 8 ? 2 : 1) * sm_count());
+    if (fro != nullptr) grid = std::min(grid, nfro);   // one Frobenius partial per CTA
     const float* Af = reinterpret_cast<const float*>(A);
     NR_SWITCH(nrhs, (symv_staged_kernel<NRC><<<grid, NTH, symv_staged_smem<NRC>(), stream>>>(Af, lda, n, x, y, skip, fro, nfro)));
   } else {
