@@ -76,6 +76,9 @@ def parse():
     ap.add_argument("--max-it", type=int, default=400)
     ap.add_argument("--check-every", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--factor-only", type=int, default=0, metavar="K",
+                    help="run the mixed arm's factorization K times and exit without "
+                         "timing or output (an entry point for profilers)")
     ap.add_argument("--tune", action="store_true",
                     help="batch workload: re-run the autotuner on this GPU and write its table")
     ap.add_argument("--tune-out", default=None,
@@ -318,6 +321,12 @@ def run_gpu(args, world, rank, local):
         f = f or fobj[name]
         f.compute(A)
         return f.pcg(A, B, rel_tol=args.tol, max_it=args.max_it, check_every=args.check_every)
+
+    if args.factor_only > 0:
+        for _ in range(args.factor_only):
+            fobj["mixed"].compute(A)
+        torch.cuda.synchronize()
+        return None
 
     def timed(name, k):
         times, reps = [], []

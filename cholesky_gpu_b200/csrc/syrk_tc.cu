@@ -20,11 +20,17 @@
 //           commits each stage back to the producer and each finished tile to
 //           the epilogue;
 //   warps 2-9 epilogue, two per 32-lane TMEM quarter (64 columns each):
-//           tcgen05.ld of the accumulator, the scaled update staged as 32 x 32
-//           boxes in shared memory and added into C by TMA reduce-adds, so the
-//           read-modify-write of C happens in L2 instead of through the SM
-//           (batched launches, whose C differs per system, read and write C
-//           with coalesced loads and stores instead).
+//           tcgen05.ld of the accumulator and the scaled update of C in
+//           32 x 32 boxes.  Each warp prefetches its boxes of C for the next
+//           tile by TMA loads while it finishes the current one, subtracts
+//           the update in shared memory and writes the boxes back by TMA
+//           stores: C crosses DRAM once each way with the reads issued a tile
+//           ahead.  (Adding the update by TMA reduce-adds instead leaves the
+//           read of C to the L2, which fetches each line from DRAM when the
+//           reduction arrives; at n = 16384 that ran DRAM at half its
+//           bandwidth.  FP16X2, whose three operand sets leave no room for
+//           the prefetch boxes, still adds by reduce-adds; batched launches,
+//           whose C differs per system, use coalesced loads and stores.)
 // The two TMEM accumulators let the epilogue of one tile overlap the MMAs of
 // the next.  Every mbarrier wait is bounded.
 #include <algorithm>
@@ -43,33 +49,46 @@ constexpr int STRIP = TM * CHUNK;          // 16 KB: one operand strip chunk
 constexpr int EPI_WARPS = 8;               // two per TMEM lane quarter, half the columns each
 constexpr int NTHREADS = 64 + 32 * EPI_WARPS;
 
+// NSTAGE: operand stages of batched launches (no epilogue boxes);
+// LDST_STAGES: operand stages beside the four C boxes per epilogue warp of
+// the load / store epilogue (0: reduce-add epilogue with EPI_BUFS boxes).
 template <int FMT> struct TcCfg;
 template <> struct TcCfg<FP16> {
-  static constexpr int ESIZE = 2, NSETS = 1, NSTAGE = 4, EPI_BUFS = 2;
+  static constexpr int ESIZE = 2, NSETS = 1, NSTAGE = 4, EPI_BUFS = 2, LDST_STAGES = 3;
   static constexpr bool MX = false;
   static constexpr uint32_t IDESC = tc::make_idesc(0, 0, TM, TM);
 };
 template <> struct TcCfg<E4M3> {
-  static constexpr int ESIZE = 1, NSETS = 1, NSTAGE = 4, EPI_BUFS = 2;
+  static constexpr int ESIZE = 1, NSETS = 1, NSTAGE = 4, EPI_BUFS = 2, LDST_STAGES = 3;
   static constexpr bool MX = false;
   static constexpr uint32_t IDESC = tc::make_idesc(0, 0, TM, TM);
 };
 template <> struct TcCfg<E5M2> {
-  static constexpr int ESIZE = 1, NSETS = 1, NSTAGE = 4, EPI_BUFS = 2;
+  static constexpr int ESIZE = 1, NSETS = 1, NSTAGE = 4, EPI_BUFS = 2, LDST_STAGES = 3;
   static constexpr bool MX = false;
   static constexpr uint32_t IDESC = tc::make_idesc(1, 1, TM, TM);
 };
 template <> struct TcCfg<FP16X2> {
-  static constexpr int ESIZE = 2, NSETS = 2, NSTAGE = 3, EPI_BUFS = 1;
+  static constexpr int ESIZE = 2, NSETS = 2, NSTAGE = 3, EPI_BUFS = 1, LDST_STAGES = 0;
   static constexpr bool MX = false;
   static constexpr uint32_t IDESC = tc::make_idesc(0, 0, TM, TM);
 };
 // MXFP8: E4M3 codes with one E8M0 scale per 32 K-elements, applied by the
 // block-scaled MMA (kind::mxf8f6f4) from scales staged in tensor memory.
+// Two stages hold a whole K = 256 tile.
 template <> struct TcCfg<MXFP8> {
-  static constexpr int ESIZE = 1, NSETS = 1, NSTAGE = 4, EPI_BUFS = 2;
+  static constexpr int ESIZE = 1, NSETS = 1, NSTAGE = 4, EPI_BUFS = 2, LDST_STAGES = 2;
   static constexpr bool MX = true;
   static constexpr uint32_t IDESC = tc::make_idesc_mx(0, 0, TM, TM);
+};
+// The epilogue of a launch: load / store (LDST), reduce-add (RED) or, for
+// batched launches, neither (coalesced loads and stores of C).
+template <int FMT, bool BATCH> struct TcPlan {
+  using Cfg = TcCfg<FMT>;
+  static constexpr bool LDST = !BATCH && Cfg::LDST_STAGES > 0;
+  static constexpr bool RED = !BATCH && !LDST;
+  static constexpr int NSTAGE = LDST ? Cfg::LDST_STAGES : Cfg::NSTAGE;
+  static constexpr int EPI_BOXES = BATCH ? 0 : (LDST ? 4 : Cfg::EPI_BUFS);   // per epilogue warp
 };
 
 // Scales of one stage (a 128-element K chunk = four 32-element blocks) for
@@ -94,9 +113,9 @@ __device__ __forceinline__ void stage_scales(uint8_t* sf, const uint8_t* __restr
 struct TcMaps {
   CUtensorMap hi;   // main (or hi) panel: rows m, K-major
   CUtensorMap lo;   // lo panel (FP16X2 only)
-  CUtensorMap c;    // the trailing block C (FP32, m x m, 32 x 32 boxes): TMA reduce-add target
+  CUtensorMap c;    // the trailing block C (FP32, m x m, 32 x 32 boxes)
 };
-constexpr int STAGE_C = 32 * 32 * 4;        // one epilogue warp's 32 x 32 FP32 staging box
+constexpr int STAGE_C = 32 * 32 * 4;        // one 32 x 32 FP32 box of C
 
 // Batched launches: the tiles of all active systems are numbered in one
 // sequence (system i owns [steps[i].tile0, steps[i+1].tile0)); each system's
@@ -152,16 +171,16 @@ syrk_tc_body(const CUtensorMap* mhi, const CUtensorMap* mlo, const CUtensorMap* 
              const uint8_t* __restrict__ mxexp, int ldmx, DevStatus* st, const TcBatch& bt,
              int ntiles_b, TileSel sel) {
   using Cfg = TcCfg<FMT>;
+  using Plan = TcPlan<FMT, BATCH>;
   if (st != nullptr && st->code != 0) return;
-  constexpr int NS = Cfg::NSTAGE;
+  constexpr int NS = Plan::NSTAGE;
   constexpr int NSETS = Cfg::NSETS;
   constexpr bool MX = Cfg::MX;
   // A sets, B sets, then (MXFP8) the A and B scales of the chunk
   constexpr int STAGE_BYTES = 2 * NSETS * STRIP + (MX ? 2 * SF_BYTES : 0);
   constexpr uint32_t TMEM_COLS = MX ? 4 * TM : 2 * TM;  // accumulators (+ scales)
-  // single-matrix launches hand the update to the L2 with TMA reduce-adds
-  // (no C traffic through the SM); batched launches read-modify-write C
-  constexpr bool RED = !BATCH;
+  constexpr bool RED = Plan::RED;
+  constexpr bool LDST = Plan::LDST;
   constexpr int KSTEP = 32;                             // bytes of K per MMA
   constexpr int ELEMS_PER_CHUNK = CHUNK / Cfg::ESIZE;
 
@@ -172,6 +191,7 @@ syrk_tc_body(const CUtensorMap* mhi, const CUtensorMap* mlo, const CUtensorMap* 
   __shared__ __align__(8) uint64_t empty_bar[NS];
   __shared__ __align__(8) uint64_t accf_bar[2];
   __shared__ __align__(8) uint64_t acce_bar[2];
+  __shared__ __align__(8) uint64_t cld_bar[EPI_WARPS][2];   // LDST: each warp's C boxes landed
   __shared__ uint32_t tmem_base_sh;
   __shared__ volatile int abort_sh;
 
@@ -183,6 +203,8 @@ syrk_tc_body(const CUtensorMap* mhi, const CUtensorMap* mlo, const CUtensorMap* 
   if (threadIdx.x == 0) {
     for (int s = 0; s < NS; ++s) { tc::mbar_init(&full_bar[s], 1); tc::mbar_init(&empty_bar[s], 1); }
     for (int b = 0; b < 2; ++b) { tc::mbar_init(&accf_bar[b], 1); tc::mbar_init(&acce_bar[b], EPI_WARPS); }
+    if (LDST)
+      for (int w = 0; w < EPI_WARPS; ++w) { tc::mbar_init(&cld_bar[w][0], 1); tc::mbar_init(&cld_bar[w][1], 1); }
     tc::fence_mbar_init();
     tc::prefetch_tmap(mhi);
     if (NSETS == 2) tc::prefetch_tmap(mlo);
@@ -313,13 +335,41 @@ syrk_tc_body(const CUtensorMap* mhi, const CUtensorMap* mlo, const CUtensorMap* 
     // ---------------- epilogue (warps 2..5) ----------------
     const int q = warp & 3;                  // TMEM lane quarter this warp may access
     const int half = (warp - 2) >> 2;        // which 64 columns of the tile
-    // EPI_BUFS staging boxes per warp, used in turn: with two, a box is
-    // filled while the previous one is still being read by its reduce-add
-    constexpr int EB = Cfg::EPI_BUFS;
+    const int ew = warp - 2;
+    // RED: EPI_BUFS staging boxes per warp, used in turn (with two, a box is
+    // filled while the previous one is still being read by its reduce-add).
+    // LDST: two sets of the warp's two boxes of C, one for the tile being
+    // finished and one for the next tile's prefetch.
+    constexpr int EB = Plan::EPI_BOXES;
     float* stg0 = reinterpret_cast<float*>(smem + (size_t)NS * STAGE_BYTES +
-                                           (size_t)(warp - 2) * STAGE_C * EB);
+                                           (size_t)ew * STAGE_C * (EB > 0 ? EB : 1));
+    // box hb (0, 1) of this warp in tile (I, J): rows I*TM + 32 q, columns
+    // J*TM + 64 half + 32 hb; boxes wholly above the diagonal or past m are
+    // skipped
+    auto box_ok = [&](int I, int J, int mt, int hb) {
+      const int i0 = I * TM + q * 32, j0 = J * TM + half * (TM / 2) + hb * 32;
+      return i0 < mt && j0 < mt && !(I == J && j0 >= i0 + 32);
+    };
+    // LDST: TMA loads of tile t's boxes into set `set` (lane 0)
+    auto load_boxes = [&](int t, int set) {
+      const TileCtx x = tile_ctx<BATCH>(t, bt, C, ldc, m, sel);
+      uint32_t bytes = 0;
+      for (int hb = 0; hb < 2; ++hb) bytes += box_ok(x.I, x.J, x.m, hb) ? (uint32_t)STAGE_C : 0u;
+      tc::mbar_expect_tx(&cld_bar[ew][set], bytes);
+      for (int hb = 0; hb < 2; ++hb)
+        if (box_ok(x.I, x.J, x.m, hb))
+          tc::tma_load_2d(stg0 + (set * 2 + hb) * (STAGE_C / 4), mc, &cld_bar[ew][set],
+                          x.I * TM + q * 32, x.J * TM + half * (TM / 2) + hb * 32);
+    };
     int nbox = 0;
     int tcount = 0;
+    // LDST: per set, the phase parity of loads issued and not yet waited for
+    // (-1: none)
+    int opar0 = -1, opar1 = -1;
+    if (LDST && blockIdx.x < ntiles) {
+      if (lane == 0) load_boxes(blockIdx.x, 0);
+      opar0 = 0;
+    }
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++tcount) {
       const TileCtx tc_ = tile_ctx<BATCH>(t, bt, C, ldc, m, sel);
       const int I = tc_.I, J = tc_.J;
@@ -328,9 +378,27 @@ syrk_tc_body(const CUtensorMap* mhi, const CUtensorMap* mlo, const CUtensorMap* 
       const int8_t* rexp = rowexp + tc_.row0;
       const int buf = tcount & 1;
       const uint32_t use = (uint32_t)(tcount >> 1);
+      if (LDST && t + (int)gridDim.x < ntiles) {
+        // prefetch the next tile's boxes into the other set, once the stores
+        // of the tile that used it have read their boxes
+        if (lane == 0) {
+          tc::bulk_wait_smem_read();
+          load_boxes(t + gridDim.x, buf ^ 1);
+        }
+        __syncwarp();
+        const int par = (int)(((tcount + 1) >> 1) & 1);
+        if (buf) opar0 = par; else opar1 = par;
+      }
       if (!tc::mbar_wait(&accf_bar[buf], use & 1u)) {
         if (lane == 0) { abort_sh = 1; if (st != nullptr) set_status(st, MPCHOL_ERR_TIMEOUT, t); }
         break;
+      }
+      if (LDST) {
+        if (!tc::mbar_wait(&cld_bar[ew][buf], use & 1u)) {
+          if (lane == 0) { abort_sh = 1; if (st != nullptr) set_status(st, MPCHOL_ERR_TIMEOUT, t); }
+          break;
+        }
+        if (buf) opar1 = -1; else opar0 = -1;
       }
       tc::tc_fence_after();
       const int i = I * TM + q * 32 + lane;
@@ -350,14 +418,34 @@ syrk_tc_body(const CUtensorMap* mhi, const CUtensorMap* mlo, const CUtensorMap* 
         // column scales of the box: lane u loads s_{j0+u} once, the element
         // loops take it by shuffle
         const float sj_lane = (!MX && j0 + lane < mt) ? pow2f(__ldg(rexp + j0 + lane)) : 1.0f;
-        if (RED) {
+        if (LDST) {
+          // C(rows i0.., cols j0..) -= s_i s_j acc in the prefetched box, then
+          // one TMA store; entries above the diagonal keep their value
+          const int i0 = I * TM + q * 32;
+          const int hb = (c0 - half * (TM / 2)) / 32;
+          if (box_ok(I, J, mt, hb)) {
+            float* bx = stg0 + (buf * 2 + hb) * (STAGE_C / 4);
+#pragma unroll
+            for (int u = 0; u < 32; ++u) {
+              const float sj = MX ? 1.0f : __shfl_sync(0xffffffffu, sj_lane, u);
+              const float cv = bx[u * 32 + lane];
+              bx[u * 32 + lane] = (I == J && j0 + u > i) ? cv : cv - (v[u] * si) * sj;
+            }
+            tc::fence_proxy_async_smem();
+            __syncwarp();
+            if (lane == 0) {
+              tc::tma_store_2d(mc, bx, i0, j0);
+              tc::bulk_commit();
+            }
+          }
+        } else if (RED) {
           // C(rows i0.., cols j0..) += -(s_i s_j acc) as one 32 x 32 TMA
           // reduce-add; boxes wholly above the diagonal or past m are skipped,
           // and entries above the diagonal add -0.0, which leaves every value
           // (signed zeros included) as it was
           const int i0 = I * TM + q * 32;
           if (i0 < mt && j0 < mt && !(I == J && j0 >= i0 + 32)) {
-            float* stg = stg0 + (nbox % EB) * (STAGE_C / 4);
+            float* stg = stg0 + (EB > 0 ? nbox % EB : 0) * (STAGE_C / 4);
             ++nbox;
             // the box that last used this buffer has been read
             if (lane == 0) {
@@ -395,8 +483,15 @@ syrk_tc_body(const CUtensorMap* mhi, const CUtensorMap* mlo, const CUtensorMap* 
         }
       }
     }
+    // a prefetch left behind by an aborted loop lands before the CTA exits
+    if (LDST && lane == 0)
+    {
+      if (opar0 >= 0) tc::mbar_wait(&cld_bar[ew][0], (uint32_t)opar0);
+      if (opar1 >= 0) tc::mbar_wait(&cld_bar[ew][1], (uint32_t)opar1);
+    }
   }
-  if (RED && warp >= 2 && lane == 0) tc::bulk_wait_read();   // reduce-adds performed before exit
+  // reduce-adds and stores performed before exit
+  if ((RED || LDST) && warp >= 2 && lane == 0) tc::bulk_wait_read();
   tc::tc_fence_before();
   __syncthreads();
   if (warp == 1) {
@@ -467,8 +562,9 @@ syrk_tc_dispatch_kernel(const __grid_constant__ TcMapsAll maps, float* __restric
 template <int FMT, bool BATCH>
 size_t tc_smem() {
   using Cfg = TcCfg<FMT>;
-  return (size_t)Cfg::NSTAGE * (2 * Cfg::NSETS * STRIP + (Cfg::MX ? 2 * SF_BYTES : 0)) +
-         (BATCH ? 0 : (size_t)EPI_WARPS * STAGE_C * Cfg::EPI_BUFS) + 1024;
+  using Plan = TcPlan<FMT, BATCH>;
+  return (size_t)Plan::NSTAGE * (2 * Cfg::NSETS * STRIP + (Cfg::MX ? 2 * SF_BYTES : 0)) +
+         (size_t)EPI_WARPS * STAGE_C * Plan::EPI_BOXES + 1024;
 }
 
 int grid_for(int ntiles, int max_sms) {
