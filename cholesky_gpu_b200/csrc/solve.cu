@@ -404,11 +404,18 @@ __device__ __forceinline__ void load_vec_x8(const double* x, int n, int row0, in
 // by FP64 atomics.  DIAG (a diagonal tile of a symmetric operator stored
 // lower): the row sums keep r >= c, the column sums r > c.  FRO: adds the
 // tile's share of ||A||_F^2 (off-diagonal entries twice) to *fsq.
-template <bool DIAG, bool FRO>
+// KC k-steps of fragments are loaded (and widened) per chunk and UNR chunks
+// are unrolled, so the next chunk's loads overlap this chunk's DMMAs; ONLY
+// fixes the product at compile time (1: row sums, 2: column sums, 0: by
+// do_nt / do_t).  Both products: KC = 8, UNR = 2 (the 128 registers of two
+// CTAs per SM allow no more); one product: KC = 4 fully unrolled.
+template <bool DIAG, bool FRO, int KC = 8, int UNR = 2, int ONLY = 0>
 __device__ __forceinline__ void tile_mma_x8(const float* Ts, const double* x_c, const double* x_r,
                                             double* y_rows, int row0, int nrows, double* y_cols,
-                                            int col0, int ncols, int n, bool do_nt, bool do_t,
+                                            int col0, int ncols, int n, bool do_nt_rt, bool do_t_rt,
                                             double sign, double* fsq) {
+  const bool do_nt = ONLY == 1 ? true : (ONLY == 2 ? false : do_nt_rt);
+  const bool do_t = ONLY == 2 ? true : (ONLY == 1 ? false : do_t_rt);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int g = lane >> 2, t = lane & 3;
   const int B0 = 16 * warp;
@@ -416,8 +423,8 @@ __device__ __forceinline__ void tile_mma_x8(const float* Ts, const double* x_c, 
   // per warp when both products run
   double dn[2][2][2] = {};
   double dt[2][2][2] = {};
-  constexpr int KC = 8;                       // k-steps (of 4) per software-pipelined chunk
-#pragma unroll 1
+  static_assert(KC % 2 == 0, "k-step parity picks the accumulator: chunks hold an even count");
+#pragma unroll(UNR)
   for (int kb = 0; kb < RB; kb += 4 * KC) {
     // every fragment of the chunk is loaded (and widened) before its DMMAs
     float an[2][KC], at[2][KC];
@@ -1144,8 +1151,14 @@ trsv_persistent_kernel(const float* __restrict__ L, int ldl, int n, const float*
       cp_async_wait<0>();
       __syncthreads();
       double* dst = cur.panel ? work : out;
-      tile_mma_x8<false, false>(Ts, s_v, s_v, dst, cur.out_row0, cur.out_n, dst, cur.out_row0,
-                                cur.out_n, n, cur.nt, !cur.nt, cur.panel ? -1.0 : 1.0, nullptr);
+      if (cur.nt)
+        tile_mma_x8<false, false, 4, RB / 16, 1>(Ts, s_v, s_v, dst, cur.out_row0, cur.out_n, dst,
+                                                 cur.out_row0, cur.out_n, n, true, false,
+                                                 cur.panel ? -1.0 : 1.0, nullptr);
+      else
+        tile_mma_x8<false, false, 4, RB / 16, 2>(Ts, s_v, s_v, dst, cur.out_row0, cur.out_n, dst,
+                                                 cur.out_row0, cur.out_n, n, false, true,
+                                                 cur.panel ? -1.0 : 1.0, nullptr);
       signal_count(cur.sig_ctr);   // its barrier also frees the stage and s_v
       ucur = s_unit[it & 1];
       have = trsv_job<TRANS>(ucur, L, ldl, n, wsup, seg_in, seg_out, cur);
