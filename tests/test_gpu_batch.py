@@ -69,3 +69,31 @@ def test_batch_matches_single_pcg_iterations(cuda):
         # pair granularity of the batched loop and the restart points
         assert abs(reps[i].iterations - r1.iterations) <= 3, (i, reps[i], r1)
         assert torch.allclose(Xs[i], X1, rtol=0, atol=1e-8 * X1.abs().max().item())
+
+
+def test_batch_of_512_systems(cuda):
+    """The batch at the scale of the 512-system workload (orders U[64, 512],
+    kappa up to 1e4, one rhs, FP16 trailing updates, block 128): every system
+    reaches a 1e-10 FP64 true residual, and a sample of eight systems keeps
+    the factor of the single-system path bit for bit."""
+    count = 512
+    ns = [int(n) for n in matgen.batch_sizes(count, 64, 512, 21)]
+    kappas = matgen.batch_kappas(count, 1e2, 1e4, 22)
+    Ad = [matgen.spd_matrix(n, float(k), 1000 + i, device="cuda") for i, (n, k) in enumerate(zip(ns, kappas))]
+    bt = mp.Batch(ns, nrhs=1, block_size=128, precision="fp16").factor(Ad)
+    st, rows, _ = bt.info()
+    assert all(s_ == 0 for s_ in st), [i for i, s_ in enumerate(st) if s_ != 0]
+    g = torch.Generator(device="cpu").manual_seed(23)
+    Bd = [torch.randn(n, generator=g, dtype=torch.float64).cuda() for n in ns]
+    Xs, reps, status = bt.pcg(Ad, Bd, rel_tol=1e-10, max_it=400)
+    assert status == 0
+    worst = 0.0
+    for i, (A, B, X, r) in enumerate(zip(Ad, Bd, Xs, reps)):
+        res = (torch.linalg.norm(B - A.double() @ X) / torch.linalg.norm(B)).item()
+        assert r.converged and res <= 1.5e-10, (i, ns[i], r, res)
+        worst = max(worst, res)
+    print(f"512 systems: worst FP64 residual {worst:.2e}, iterations "
+          f"{min(r.iterations for r in reps)}-{max(r.iterations for r in reps)}")
+    for i in np.random.default_rng(24).choice(count, 8, replace=False):
+        f = mp.factor(Ad[i], block_size=128, precision="fp16")
+        assert torch.equal(bt.lower(int(i)), f.lower()), f"system {i} (n={ns[i]}) factor differs"
