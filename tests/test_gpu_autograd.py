@@ -57,7 +57,8 @@ def test_rbf_grad_contraction_matches_dense(cuda):
     assert abs(s.item() - s_want) <= 1e-12 * abs(s_want)
 
 
-@pytest.mark.parametrize("precision,n,d", [("e4m3", 512, 64), ("fp16", 640, 16)])
+@pytest.mark.parametrize("precision,n,d", [("e4m3", 512, 64), ("fp16", 640, 16),
+                                            ("mxfp8", 2048, 64), ("fp16x2", 3072, 32)])
 def test_rbf_solve_gradients_match_fp64(cuda, precision, n, d):
     """Loss 1/2 y^T K^-1 y of the differentiation workload's construction
     (x ~ N(0, I_d), l = 4, nugget = 1e-2, y ~ N(0,1)) at a size the dense
