@@ -49,27 +49,32 @@ constexpr int STRIP = TM * CHUNK;          // 16 KB: one operand strip chunk
 constexpr int EPI_WARPS = 8;               // two per TMEM lane quarter, half the columns each
 constexpr int NTHREADS = 64 + 32 * EPI_WARPS;
 
-// NSTAGE: operand stages of batched launches (no epilogue boxes);
-// LDST_STAGES: operand stages beside the four C boxes per epilogue warp of
-// the load / store epilogue (0: reduce-add epilogue with EPI_BUFS boxes).
+// NSTAGE: operand stages of batched launches (no epilogue boxes) and of the
+// reduce-add epilogue (with EPI_BUFS boxes per epilogue warp); LDST_STAGES:
+// operand stages beside the four C boxes per epilogue warp of the load /
+// store epilogue (0: none), which a launch uses for K <= LDST_MAX_K.  Beyond
+// that K the fewer stages starve the MMAs while C's traffic per flop falls
+// (B200, m = 15360-16128: MXFP8 at K = 512 0.254 ms with load / store
+// against 0.238 ms with reduce-adds, FP16 at K = 1024 0.414 against 0.361;
+// E4M3 at K = 512 0.196 against 0.234).
 template <int FMT> struct TcCfg;
 template <> struct TcCfg<FP16> {
-  static constexpr int ESIZE = 2, NSETS = 1, NSTAGE = 4, EPI_BUFS = 2, LDST_STAGES = 3;
+  static constexpr int ESIZE = 2, NSETS = 1, NSTAGE = 4, EPI_BUFS = 2, LDST_STAGES = 3, LDST_MAX_K = 256;
   static constexpr bool MX = false;
   static constexpr uint32_t IDESC = tc::make_idesc(0, 0, TM, TM);
 };
 template <> struct TcCfg<E4M3> {
-  static constexpr int ESIZE = 1, NSETS = 1, NSTAGE = 4, EPI_BUFS = 2, LDST_STAGES = 3;
+  static constexpr int ESIZE = 1, NSETS = 1, NSTAGE = 4, EPI_BUFS = 2, LDST_STAGES = 3, LDST_MAX_K = 512;
   static constexpr bool MX = false;
   static constexpr uint32_t IDESC = tc::make_idesc(0, 0, TM, TM);
 };
 template <> struct TcCfg<E5M2> {
-  static constexpr int ESIZE = 1, NSETS = 1, NSTAGE = 4, EPI_BUFS = 2, LDST_STAGES = 3;
+  static constexpr int ESIZE = 1, NSETS = 1, NSTAGE = 4, EPI_BUFS = 2, LDST_STAGES = 3, LDST_MAX_K = 512;
   static constexpr bool MX = false;
   static constexpr uint32_t IDESC = tc::make_idesc(1, 1, TM, TM);
 };
 template <> struct TcCfg<FP16X2> {
-  static constexpr int ESIZE = 2, NSETS = 2, NSTAGE = 3, EPI_BUFS = 1, LDST_STAGES = 0;
+  static constexpr int ESIZE = 2, NSETS = 2, NSTAGE = 3, EPI_BUFS = 1, LDST_STAGES = 0, LDST_MAX_K = 0;
   static constexpr bool MX = false;
   static constexpr uint32_t IDESC = tc::make_idesc(0, 0, TM, TM);
 };
@@ -77,15 +82,15 @@ template <> struct TcCfg<FP16X2> {
 // block-scaled MMA (kind::mxf8f6f4) from scales staged in tensor memory.
 // Two stages hold a whole K = 256 tile.
 template <> struct TcCfg<MXFP8> {
-  static constexpr int ESIZE = 1, NSETS = 1, NSTAGE = 4, EPI_BUFS = 2, LDST_STAGES = 2;
+  static constexpr int ESIZE = 1, NSETS = 1, NSTAGE = 4, EPI_BUFS = 2, LDST_STAGES = 2, LDST_MAX_K = 256;
   static constexpr bool MX = true;
   static constexpr uint32_t IDESC = tc::make_idesc_mx(0, 0, TM, TM);
 };
 // The epilogue of a launch: load / store (LDST), reduce-add (RED) or, for
 // batched launches, neither (coalesced loads and stores of C).
-template <int FMT, bool BATCH> struct TcPlan {
+template <int FMT, bool BATCH, bool WIDE> struct TcPlan {
   using Cfg = TcCfg<FMT>;
-  static constexpr bool LDST = !BATCH && Cfg::LDST_STAGES > 0;
+  static constexpr bool LDST = !BATCH && !WIDE && Cfg::LDST_STAGES > 0;
   static constexpr bool RED = !BATCH && !LDST;
   static constexpr int NSTAGE = LDST ? Cfg::LDST_STAGES : Cfg::NSTAGE;
   static constexpr int EPI_BOXES = BATCH ? 0 : (LDST ? 4 : Cfg::EPI_BUFS);   // per epilogue warp
@@ -164,14 +169,14 @@ __device__ __forceinline__ TileCtx tile_ctx(int t, const TcBatch& bt, float* C, 
 
 // The kernel body for one format.  mhi / mlo / mc point at tensor maps in the
 // launch's parameter space (TMA reads them from there).
-template <int FMT, bool BATCH>
+template <int FMT, bool BATCH, bool WIDE>
 __device__ __forceinline__ void
 syrk_tc_body(const CUtensorMap* mhi, const CUtensorMap* mlo, const CUtensorMap* mc,
              float* __restrict__ C, int ldc, int m, int k, const int8_t* __restrict__ rowexp,
              const uint8_t* __restrict__ mxexp, int ldmx, DevStatus* st, const TcBatch& bt,
              int ntiles_b, TileSel sel) {
   using Cfg = TcCfg<FMT>;
-  using Plan = TcPlan<FMT, BATCH>;
+  using Plan = TcPlan<FMT, BATCH, WIDE>;
   if (st != nullptr && st->code != 0) return;
   constexpr int NS = Plan::NSTAGE;
   constexpr int NSETS = Cfg::NSETS;
@@ -500,14 +505,19 @@ syrk_tc_body(const CUtensorMap* mhi, const CUtensorMap* mlo, const CUtensorMap* 
   }
 }
 
-template <int FMT, bool BATCH>
+template <int FMT, bool BATCH, bool WIDE>
 __global__ void __launch_bounds__(NTHREADS, 1)
 syrk_tc_kernel(const __grid_constant__ TcMaps maps, float* __restrict__ C, int ldc, int m, int k,
                const int8_t* __restrict__ rowexp, const uint8_t* __restrict__ mxexp, int ldmx,
                const int* prec_sel, DevStatus* st, TcBatch bt, int ntiles_b, TileSel sel) {
   if (prec_sel != nullptr && *prec_sel != FMT) return;
-  syrk_tc_body<FMT, BATCH>(&maps.hi, &maps.lo, &maps.c, C, ldc, m, k, rowexp, mxexp, ldmx, st, bt,
-                           ntiles_b, sel);
+  syrk_tc_body<FMT, BATCH, WIDE>(&maps.hi, &maps.lo, &maps.c, C, ldc, m, k, rowexp, mxexp, ldmx, st,
+                                 bt, ntiles_b, sel);
+}
+
+// K beyond the format's load / store epilogue (see TcCfg)
+template <int FMT> __host__ __device__ constexpr bool tc_wide(int k) {
+  return k > TcCfg<FMT>::LDST_MAX_K;
 }
 
 // Maps for every format: the three 8-bit code panels (slot q8_slot), the
@@ -530,41 +540,51 @@ syrk_tc_dispatch_kernel(const __grid_constant__ TcMapsAll maps, float* __restric
   const int f = *prec_sel;
   if (f < 0 || f > 31 || ((fmt_mask >> f) & 1u) == 0) return;
   const TcBatch nb{};
+  // one body per format and epilogue (the K test is uniform over the grid)
+#define TC_BODY(F, MHI, MLO, REXP, MX, LDMX)                                                     \
+  do {                                                                                        \
+    if (tc_wide<F>(k))                                                                        \
+      syrk_tc_body<F, false, true>(MHI, MLO, &maps.c, C, ldc, m, k, REXP, MX, LDMX, st, nb, 0, sel); \
+    else                                                                                      \
+      syrk_tc_body<F, false, false>(MHI, MLO, &maps.c, C, ldc, m, k, REXP, MX, LDMX, st, nb, 0, sel); \
+  } while (0)
   switch (f) {
     case FP16:
-      syrk_tc_body<FP16, false>(&maps.h16, &maps.l16, &maps.c, C, ldc, m, k, rexp_f16, nullptr, 0,
-                                st, nb, 0, sel);
+      TC_BODY(FP16, &maps.h16, &maps.l16, rexp_f16, nullptr, 0);
       break;
-    case FP16X2:
-      syrk_tc_body<FP16X2, false>(&maps.h16, &maps.l16, &maps.c, C, ldc, m, k, rexp_f16, nullptr,
-                                  0, st, nb, 0, sel);
+    case FP16X2:   // reduce-add epilogue at every K
+      syrk_tc_body<FP16X2, false, false>(&maps.h16, &maps.l16, &maps.c, C, ldc, m, k, rexp_f16,
+                                         nullptr, 0, st, nb, 0, sel);
       break;
     case E4M3:
-      syrk_tc_body<E4M3, false>(&maps.h8[0], &maps.h8[0], &maps.c, C, ldc, m, k, rexp_e4m3, nullptr,
-                                0, st, nb, 0, sel);
+      TC_BODY(E4M3, &maps.h8[0], &maps.h8[0], rexp_e4m3, nullptr, 0);
       break;
     case E5M2:
-      syrk_tc_body<E5M2, false>(&maps.h8[1], &maps.h8[1], &maps.c, C, ldc, m, k, rexp_e5m2, nullptr,
-                                0, st, nb, 0, sel);
+      TC_BODY(E5M2, &maps.h8[1], &maps.h8[1], rexp_e5m2, nullptr, 0);
       break;
     case MXFP8:
     case MXFP6E2M3:    // FP6/FP4 element values stored as E4M3 codes: the same body
     case MXFP6E3M2:
     case MXFP4:
-      syrk_tc_body<MXFP8, false>(&maps.h8[2], &maps.h8[2], &maps.c, C, ldc, m, k, nullptr, mxexp,
-                                 ldmx, st, nb, 0, sel);
+      TC_BODY(MXFP8, &maps.h8[2], &maps.h8[2], nullptr, mxexp, ldmx);
       break;
     default:
       break;
   }
+#undef TC_BODY
 }
 
-template <int FMT, bool BATCH>
+template <int FMT, bool BATCH, bool WIDE = false>
 size_t tc_smem() {
   using Cfg = TcCfg<FMT>;
-  using Plan = TcPlan<FMT, BATCH>;
+  using Plan = TcPlan<FMT, BATCH, WIDE>;
   return (size_t)Plan::NSTAGE * (2 * Cfg::NSETS * STRIP + (Cfg::MX ? 2 * SF_BYTES : 0)) +
          (size_t)EPI_WARPS * STAGE_C * Plan::EPI_BOXES + 1024;
+}
+
+template <int FMT>
+size_t tc_smem_k(int k) {
+  return tc_wide<FMT>(k) ? tc_smem<FMT, false, true>() : tc_smem<FMT, false, false>();
 }
 
 int grid_for(int ntiles, int max_sms) {
@@ -581,16 +601,19 @@ cudaError_t launch_fmt(const TcMaps& maps, float* C, int ldc, int m, int k, cons
                        const uint8_t* mxexp, int ldmx, const int* prec_sel, DevStatus* st,
                        const TcBatch& bt, int ntiles_b, cudaStream_t stream,
                        TileSel sel = kAllTiles, int max_sms = 0) {
-  const size_t smem = tc_smem<FMT, BATCH>();
-  cudaError_t e = cudaFuncSetAttribute(syrk_tc_kernel<FMT, BATCH>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
   const int ntiles = BATCH ? ntiles_b : sel_tile_count(ceil_div(m, TM), sel);
   if (ntiles <= 0) return cudaSuccess;
   const int grid = grid_for(ntiles, max_sms);
-  syrk_tc_kernel<FMT, BATCH><<<grid, NTHREADS, smem, stream>>>(maps, C, ldc, m, k, rowexp, mxexp,
-                                                               ldmx, prec_sel, st, bt, ntiles_b, sel);
-  return cudaGetLastError();
+  auto go = [&](auto kernel, size_t smem) -> cudaError_t {
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    kernel<<<grid, NTHREADS, smem, stream>>>(maps, C, ldc, m, k, rowexp, mxexp, ldmx, prec_sel, st,
+                                             bt, ntiles_b, sel);
+    return cudaGetLastError();
+  };
+  if constexpr (!BATCH)
+    if (tc_wide<FMT>(k)) return go(syrk_tc_kernel<FMT, false, true>, tc_smem<FMT, false, true>());
+  return go(syrk_tc_kernel<FMT, BATCH, false>, tc_smem<FMT, BATCH, false>());
 }
 
 }  // namespace
@@ -677,15 +700,17 @@ cudaError_t launch_syrk_tc_dispatch(float* C, int ldc, int m, int k, unsigned fm
       return cudaErrorInvalidValue;
   }
   size_t smem = 0;
-  if ((setup_mask >> FP16) & 1u) smem = std::max(smem, tc_smem<FP16, false>());
-  if ((setup_mask >> E4M3) & 1u) smem = std::max(smem, tc_smem<E4M3, false>());
-  if ((setup_mask >> E5M2) & 1u) smem = std::max(smem, tc_smem<E5M2, false>());
+  if ((setup_mask >> FP16) & 1u) smem = std::max(smem, tc_smem_k<FP16>(k));
+  if ((setup_mask >> E4M3) & 1u) smem = std::max(smem, tc_smem_k<E4M3>(k));
+  if ((setup_mask >> E5M2) & 1u) smem = std::max(smem, tc_smem_k<E5M2>(k));
   if ((setup_mask >> FP16X2) & 1u) smem = std::max(smem, tc_smem<FP16X2, false>());
-  if ((setup_mask >> MXFP8) & 1u) smem = std::max(smem, tc_smem<MXFP8, false>());
+  if ((setup_mask >> MXFP8) & 1u) smem = std::max(smem, tc_smem_k<MXFP8>(k));
   if (smem == 0) return cudaSuccess;
   const size_t smem_all = std::max({tc_smem<FP16, false>(), tc_smem<E4M3, false>(),
                                     tc_smem<E5M2, false>(), tc_smem<FP16X2, false>(),
-                                    tc_smem<MXFP8, false>()});
+                                    tc_smem<MXFP8, false>(), tc_smem<FP16, false, true>(),
+                                    tc_smem<E4M3, false, true>(), tc_smem<E5M2, false, true>(),
+                                    tc_smem<MXFP8, false, true>()});
   cudaError_t e = cudaFuncSetAttribute(syrk_tc_dispatch_kernel,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_all);
   if (e != cudaSuccess) return e;
