@@ -59,6 +59,7 @@ struct mpchol_batch {
   mpchol_opts opts{};
   int count = 0, nrhs = 1, nr = 1, b = 128, fmt = FP16;
   int max_n = 0, nsteps = 0, qrows = 0;
+  int sym_tiles = 0;           // 128-tiles of every system's lower triangle
   std::vector<int> n;          // user order
   std::vector<int> order;      // internal index -> user index (decreasing n)
   std::vector<int> nact, maxm, ntiles;
@@ -147,7 +148,7 @@ mpchol_status precond_all(mpchol_batch* B, int in, int out, int use_skip, cudaSt
 // One PCG iteration of every open system; rho[cur] -> rho[cur ^ 1].
 mpchol_status enqueue_iteration(mpchol_batch* B, int cur, double tol2, cudaStream_t s) {
   const int ns = B->count, nr = B->nr;
-  MPCHOL_CUDA_TRY(launch_symv_batched(B->d_sys, ns, B->max_n, 3, 4, nr, 1, s));
+  MPCHOL_CUDA_TRY(launch_symv_batched(B->d_sys, ns, B->sym_tiles, 3, 4, nr, 1, s));
   MPCHOL_CUDA_TRY(launch_dot_batched(B->d_sys, ns, 3, 4, 0, nr, 1, s));
   MPCHOL_CUDA_TRY(launch_update_xr_batched(B->d_sys, ns, cur, nr, s));
   mpchol_status e = precond_all(B, 1, 2, 1, s);
@@ -292,6 +293,9 @@ mpchol_status mpchol_batch_create(const mpchol_opts* opts, int count, const int*
     S.part = B->part + (size_t)i * 4 * BATCH_VB * 8;
     S.scal = B->scal + (size_t)i * kScal;
     S.done = B->done + (size_t)i * 2;
+    const int t = (n + 127) / 128;
+    S.sym_tile0 = B->sym_tiles;
+    B->sym_tiles += t * (t + 1) / 2;
   }
   if (cudaMemcpy(B->d_sys, B->h_sys.data(), sizeof(BatchSys) * count, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(B->d_steps, B->h_steps.data(), sizeof(BatchStep) * B->h_steps.size(),
@@ -431,7 +435,7 @@ mpchol_status mpchol_batch_pcg(mpchol_batch_t* B, const float* const* dA, const 
   const int max_restarts = 3;
   for (int restart = 0;; ++restart) {
     // true residual r = b - A x; systems within tolerance are marked done
-    MPCHOL_CUDA_TRY(launch_symv_batched(B->d_sys, ns, B->max_n, 0, 4, nr, 0, s));
+    MPCHOL_CUDA_TRY(launch_symv_batched(B->d_sys, ns, B->sym_tiles, 0, 4, nr, 0, s));
     MPCHOL_CUDA_TRY(launch_residual_batched(B->d_sys, ns, nr, s));
     MPCHOL_CUDA_TRY(launch_reduce_batched(B->d_sys, ns, 1, 32, nr, 0, s));
     MPCHOL_CUDA_TRY(launch_check_true_batched(B->d_sys, ns, B->nrhs, tol2, s));

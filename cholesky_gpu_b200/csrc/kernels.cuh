@@ -230,6 +230,7 @@ struct BatchSys {
   double* part;        // partial sums: 4 groups x BATCH_VB x 8
   double* scal;        // 64 scalars (rho[2], alpha, bnorm2, misc)
   int* done;           // [0] converged (recursive residual), [1] iterations
+  int sym_tile0;       // first unit of the system in the batched operator product
 };
 // Per system and factor step.
 struct BatchStep {

@@ -87,7 +87,7 @@ cudaError_t launch_rbf_grad(const float* X, int n, int d, int ldx, double length
 struct BatchSys;
 cudaError_t launch_vec_slot_batched(const BatchSys* sys, int nsys, int src, int dst, int nr,
                                     int use_skip, cudaStream_t stream);
-cudaError_t launch_symv_batched(const BatchSys* sys, int nsys, int max_n, int xslot, int yslot,
+cudaError_t launch_symv_batched(const BatchSys* sys, int nsys, int ntiles, int xslot, int yslot,
                                 int nr, int use_skip, cudaStream_t stream);
 cudaError_t launch_solve_setup_batched(const BatchSys* sys, int nsys, int max_n,
                                        cudaStream_t stream);

@@ -238,6 +238,12 @@ __device__ __forceinline__ void cp_async8(void* dst, const void* src, int src_by
                "l"(src), "r"(src_bytes)
                : "memory");
 }
+__device__ __forceinline__ void cp_async4(void* dst, const void* src, int src_bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(
+                   (uint32_t)__cvta_generic_to_shared(dst)),
+               "l"(src), "r"(src_bytes)
+               : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
@@ -1193,14 +1199,133 @@ __device__ __forceinline__ double* bslot(const BatchSys& S, int slot, int nr) {
   return S.vec + (size_t)slot * S.n * nr;
 }
 
+// A tile whose columns need not start on 16-byte boundaries, by 4-byte
+// copies into the plain (BL = false) or blocked (BL = true) layout.
+template <bool BL>
+__device__ __forceinline__ void stage_tile_4b(float* dst, const float* T, int ld, int rows_valid,
+                                              int cols_valid) {
+#pragma unroll 4
+  for (int e = threadIdx.x; e < TILE_ELEMS; e += NTH) {
+    const int c = e / RB, r = e % RB;
+    const bool ok = c < cols_valid && r < rows_valid;
+    cp_async4(dst + (BL ? bl_off(r, c) : c * RB + r), ok ? T + (size_t)c * ld + r : T, ok ? 4 : 0);
+  }
+}
+
+// One unit of the batched operator product: tile (I, J) of one system's
+// lower triangle.  A == nullptr: the system has converged, nothing to do.
+struct SymvUnit {
+  const float* A;
+  int lda, n, I, J;
+  const double* x;
+  double* y;
+  int al16;             // columns start on 16-byte boundaries
+};
+
+// Unit t -> its system (binary search of the per-system first units; the
+// systems are numbered in order of their first unit) and its tile.
 template <int NR>
-__global__ void __launch_bounds__(NTH)
-symv_batched_kernel(const BatchSys* __restrict__ sys, int xslot, int yslot, int use_skip) {
-  const BatchSys& S = sys[blockIdx.y];
-  const int T = ceil_div(S.n, RB);
-  if ((int)blockIdx.x >= T * (T + 1) / 2) return;
-  symv_body<float, NR>(S.op, S.op_ld, S.n, bslot(S, xslot, NR), bslot(S, yslot, NR),
-                       use_skip ? S.done : nullptr, make_uint3(blockIdx.x, 0, 0));
+__device__ __forceinline__ SymvUnit symv_unit(const BatchSys* __restrict__ sys, int nsys, int t,
+                                              int xslot, int yslot, int use_skip) {
+  int lo = 0, hi = nsys - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (sys[mid].sym_tile0 <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  const BatchSys& S = sys[lo];
+  SymvUnit u;
+  tri_of(t - S.sym_tile0, u.I, u.J);
+  u.A = (use_skip && S.done[0]) ? nullptr : S.op;
+  u.lda = S.op_ld;
+  u.n = S.n;
+  u.x = bslot(S, xslot, NR);
+  u.y = bslot(S, yslot, NR);
+  u.al16 = (reinterpret_cast<uintptr_t>(S.op) & 15) == 0 && S.op_ld % 4 == 0;
+  return u;
+}
+
+// y = A x for every system of a batch, persistent over the concatenated
+// 128-tiles of all systems' lower triangles: the staged operator product's
+// pipeline (each tile copied into shared memory symv_stages - 1 tiles ahead
+// with its two vector segments, used for both A x and A^T x), with the unit's
+// system found per tile.  y slots are zeroed beforehand.
+template <int NR>
+__global__ void __launch_bounds__(NTH, NR >= 8 ? 2 : 1)
+symv_staged_batched_kernel(const BatchSys* __restrict__ sys, int nsys, int ntiles, int xslot,
+                           int yslot, int use_skip) {
+  constexpr int STAGES = symv_stages<NR>();
+  constexpr bool MMA = NR == 8;
+  constexpr int TE = MMA ? BL_TILE : TILE_ELEMS;
+  constexpr int VEC = MMA ? XS * 8 : RB * NR;
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  __shared__ SymvUnit s_unit[STAGES];
+  float* tiles = reinterpret_cast<float*>(sm_raw);
+  double* vecs = reinterpret_cast<double*>(tiles + STAGES * TE);
+  double* s_col = vecs + STAGES * 2 * VEC;
+  auto issue = [&](int t, int stage) {
+    const SymvUnit u = symv_unit<NR>(sys, nsys, t, xslot, yslot, use_skip);
+    if (threadIdx.x == 0) s_unit[stage] = u;
+    if (u.A == nullptr) return;
+    const int i0 = u.I * RB, j0 = u.J * RB;
+    const int ni = min(RB, u.n - i0), nj = min(RB, u.n - j0);
+    const float* T = u.A + (size_t)j0 * u.lda + i0;
+    float* dst = tiles + stage * TE;
+    if (MMA) {
+      if (u.al16) stage_tile_bl(dst, T, u.lda, ni, nj);
+      else stage_tile_4b<true>(dst, T, u.lda, ni, nj);
+      stage_vec_x8(u.x, u.n, j0, nj, vecs + (2 * stage) * VEC);
+      stage_vec_x8(u.x, u.n, i0, ni, vecs + (2 * stage + 1) * VEC);
+    } else {
+      if (u.al16) stage_tile(dst, T, u.lda, ni, nj);
+      else stage_tile_4b<false>(dst, T, u.lda, ni, nj);
+      stage_vec<NR>(u.x, u.n, j0, nj, vecs + (2 * stage) * VEC);
+      stage_vec<NR>(u.x, u.n, i0, ni, vecs + (2 * stage + 1) * VEC);
+    }
+  };
+#pragma unroll
+  for (int st = 0; st < STAGES - 1; ++st) {
+    const int t = blockIdx.x + st * gridDim.x;
+    if (t < ntiles) issue(t, st);
+    cp_async_commit();
+  }
+  int stage = 0;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    {
+      const int tn = t + (STAGES - 1) * gridDim.x;
+      if (tn < ntiles) issue(tn, (stage + STAGES - 1) % STAGES);
+      cp_async_commit();
+    }
+    cp_async_wait<STAGES - 1>();
+    __syncthreads();
+    const SymvUnit u = s_unit[stage];
+    if (u.A != nullptr) {
+      const int i0 = u.I * RB, j0 = u.J * RB;
+      const int ni = min(RB, u.n - i0), nj = min(RB, u.n - j0);
+      float* Ts = tiles + stage * TE;
+      const double* xJ = vecs + (2 * stage) * VEC;
+      const double* xI = xJ + VEC;
+      if (MMA) {
+        if (u.I == u.J)
+          tile_mma_x8<true, false>(Ts, xJ, xI, u.y, i0, ni, u.y, j0, nj, u.n, true, true, 1.0, nullptr);
+        else
+          tile_mma_x8<false, false>(Ts, xJ, xI, u.y, i0, ni, u.y, j0, nj, u.n, true, true, 1.0, nullptr);
+      } else {
+        double acc[4][NR] = {};
+        if (u.I == u.J) tile_pass_staged<NR, true>(Ts, xJ, xI, acc, s_col, true, true);
+        else tile_pass_staged<NR, false>(Ts, xJ, xI, acc, s_col, true, true);
+        __syncthreads();
+        for (int e = threadIdx.x; e < VEC; e += NTH) {
+          const int k = e / RB, c = e % RB;
+          if (c < nj) atomicAdd(&u.y[(size_t)k * u.n + j0 + c], s_col[e]);
+        }
+        flush_rows<NR>(acc, reinterpret_cast<double*>(Ts), u.y, u.n, i0, ni, 1.0);
+      }
+    }
+    __syncthreads();   // the stage, its unit record and s_col are free again
+    stage = (stage + 1) % STAGES;
+  }
+  cp_async_wait<0>();
 }
 
 // dst slot = 0 (src < 0) or a copy of the src slot
@@ -1339,7 +1464,7 @@ cudaError_t solve_set_attributes() {
 #undef SET_NRP
   if ((e = set_dyn(block_inverse_batched_kernel, inv)) != cudaSuccess) return e;
 #define SET_NRB(NRC)                                                                              \
-  if ((e = set_dyn(symv_batched_kernel<NRC>, red_bytes(NRC))) != cudaSuccess) return e;           \
+  if ((e = set_dyn(symv_staged_batched_kernel<NRC>, symv_staged_smem<NRC>())) != cudaSuccess) return e; \
   if ((e = set_dyn(trmv_super_batched_kernel<NRC, false>, red_bytes(NRC))) != cudaSuccess) return e; \
   if ((e = set_dyn(trmv_super_batched_kernel<NRC, true>, red_bytes(NRC))) != cudaSuccess) return e;  \
   if ((e = set_dyn(panel_batched_kernel<NRC, false>, red_bytes(NRC))) != cudaSuccess) return e;      \
@@ -1413,12 +1538,13 @@ cudaError_t launch_vec_slot_batched(const BatchSys* sys, int nsys, int src, int 
   return cudaGetLastError();
 }
 
-cudaError_t launch_symv_batched(const BatchSys* sys, int nsys, int max_n, int xslot, int yslot,
+cudaError_t launch_symv_batched(const BatchSys* sys, int nsys, int ntiles, int xslot, int yslot,
                                 int nr, int use_skip, cudaStream_t stream) {
   cudaError_t e = launch_vec_slot_batched(sys, nsys, -1, yslot, nr, use_skip, stream);
   if (e != cudaSuccess) return e;
-  const int T = ceil_div(max_n, RB);
-  NR_SWITCH(nr, (symv_batched_kernel<NRC><<<dim3(T * (T + 1) / 2, nsys), NTH, red_bytes(NRC), stream>>>(sys, xslot, yslot, use_skip)));
+  if (ntiles <= 0) return cudaSuccess;
+  const int grid = std::min(ntiles, (nr >= 8 ? 2 : 1) * sm_count());
+  NR_SWITCH(nr, (symv_staged_batched_kernel<NRC><<<grid, NTH, symv_staged_smem<NRC>(), stream>>>(sys, nsys, ntiles, xslot, yslot, use_skip)));
   return cudaGetLastError();
 }
 

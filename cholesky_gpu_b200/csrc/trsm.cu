@@ -536,7 +536,7 @@ trsm_panel_kernel(const __grid_constant__ CUtensorMap tmapX, const __grid_consta
 // plain coalesced loads (no per-system tensor maps), the same slab solve;
 // the epilogue keeps the row sums of squares (rounding-shift estimate) and
 // the diagonal tracker.
-__global__ void __launch_bounds__(NTHR, 1)
+__global__ void __launch_bounds__(NTHR, 2)
 trsm_batched_kernel(BatchSys* __restrict__ sys, int s, int b) {
   constexpr int TR = 32;
   const BatchSys& S = sys[blockIdx.y];

@@ -25,7 +25,8 @@ def systems(count, lo, hi, seed, kmax=1e4):
 
 
 @pytest.mark.parametrize("precision,b,nrhs", [("fp16", 128, 4), ("e4m3", 128, 1),
-                                               ("fp16x2", 256, 2), ("mxfp8", 128, 1)])
+                                               ("fp16x2", 256, 2), ("mxfp8", 128, 1),
+                                               ("fp16", 128, 8)])
 def test_batch_factor_equals_single_and_solves(cuda, precision, b, nrhs):
     # FP8 factors need well-conditioned systems for PCG to finish in a few
     # hundred iterations
