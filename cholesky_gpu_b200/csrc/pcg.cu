@@ -14,7 +14,6 @@
 namespace mpchol {
 namespace {
 
-constexpr int RB = 128;      // block rows / tile size
 constexpr int NTH = 256;     // 8 warps
 
 // ---- FP64 vector kernels ----------------------------------------------------
@@ -193,7 +192,7 @@ __global__ void copy_kernel(const double* __restrict__ a, double* __restrict__ b
 // 7 work.  Partial groups: 0 pAp, 1 r^T r, 2 r^T z, 3 misc.  Scalars:
 // rho[0] 0, rho[1] 8, alpha 16, ||b||^2 24, true ||r||^2 32, ||x||^2 40,
 // ||A||_F^2 48, final r^T z 56.
-namespace bslots { constexpr int X = 0, R = 1, Z = 2, P = 3, AP = 4, B = 5, TMP = 6, WORK = 7; }
+namespace bslots { constexpr int X = 0, R = 1, Z = 2, P = 3, AP = 4, B = 5; }   // 6, 7: solve scratch
 
 __device__ __forceinline__ double* bvec(const BatchSys& S, int slot, int nr) {
   return S.vec + (size_t)slot * S.n * nr;
