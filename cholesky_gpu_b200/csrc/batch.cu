@@ -34,16 +34,18 @@ __global__ void batch_load_kernel(const BatchSys* __restrict__ sys, const float*
   const float* a = src[blockIdx.y];
   const int lda = ldsrc[blockIdx.y];
   const int n = S.n;
-  const long long total = (long long)n * n;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
-       e += (long long)gridDim.x * blockDim.x) {
-    const int c = (int)(e / n), r = (int)(e % n);
-    const float v = a[(size_t)c * lda + r];
-    S.A[(size_t)c * S.ld + r] = v;
-    if (r == c) {
-      S.d[r] = v;
-      S.dtilde[r] = v;
-      S.sh[r] = 0.0f;
+  // CTA x copies columns x, x + gridDim.x, ..., its threads run down a column
+  for (int c = blockIdx.x; c < n; c += gridDim.x) {
+    const float* ac = a + (size_t)c * lda;
+    float* dc = S.A + (size_t)c * S.ld;
+    for (int r = threadIdx.x; r < n; r += blockDim.x) {
+      const float v = ac[r];
+      dc[r] = v;
+      if (r == c) {
+        S.d[r] = v;
+        S.dtilde[r] = v;
+        S.sh[r] = 0.0f;
+      }
     }
   }
 }

@@ -400,11 +400,11 @@ frob_batched_kernel(const BatchSys* __restrict__ sys) {
   const BatchSys& S = sys[blockIdx.y];
   const int n = S.n;
   double v[1] = {0.0};
-  const long long total = (long long)n * n;
-  for (long long e = blockIdx.x * (long long)NTH + threadIdx.x; e < total; e += (long long)BATCH_VB * NTH) {
-    const int c = (int)(e / n), r = (int)(e % n);
-    if (r >= c) {
-      const double a = (double)S.op[(size_t)c * S.op_ld + r];
+  // CTA x sums columns x, x + BATCH_VB, ... from the diagonal down
+  for (int c = blockIdx.x; c < n; c += BATCH_VB) {
+    const float* col = S.op + (size_t)c * S.op_ld;
+    for (int r = c + threadIdx.x; r < n; r += NTH) {
+      const double a = (double)col[r];
       v[0] += (r == c ? 1.0 : 2.0) * a * a;
     }
   }
